@@ -1,0 +1,589 @@
+// capi.cu — the extern "C" boundary (include/dvg.h) over the sm_100a kernels.
+//
+// A context owns one CUDA stream, a device status word and grow-only scratch
+// buffers; a scene owns one device arena holding every table of the prepared
+// scene plus its tile lists and a gradient arena sized for it.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/dvg.h"
+#include "kernels.cuh"
+#include "prepare.hpp"
+
+using namespace dvgb;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+dvg_status fail(dvg_status st, const std::string& msg) {
+    g_last_error = msg;
+    return st;
+}
+dvg_status cuda_fail(cudaError_t e, const char* what) {
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? DVG_ERR_OUT_OF_MEMORY : DVG_ERR_LAUNCH;
+}
+#define CK(call)                                           \
+    do {                                                   \
+        cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    ~DevBuf() {
+        if (ptr) cudaFree(ptr);
+    }
+    cudaError_t reserve(size_t n) {
+        if (n <= bytes) return cudaSuccess;
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&ptr, n);
+        if (e == cudaSuccess) bytes = n;
+        return e;
+    }
+    template <typename T>
+    T* as() const {
+        return static_cast<T*>(ptr);
+    }
+};
+
+// Packs several host arrays into one blob with 256-byte aligned offsets.
+struct Blob {
+    std::vector<char> data;
+    template <typename T>
+    size_t add(const std::vector<T>& v) {
+        size_t off = (data.size() + 255) & ~(size_t)255;
+        data.resize(off + std::max<size_t>(v.size() * sizeof(T), 16));
+        if (!v.empty()) std::memcpy(data.data() + off, v.data(), v.size() * sizeof(T));
+        return off;
+    }
+};
+
+}  // namespace
+
+struct dvg_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    unsigned* status = nullptr;  // device word
+    DevBuf accum, wsum, image, d_render, target, loss, bg_grad, trans_grad;
+    uint64_t launches = 0;
+};
+
+struct dvg_scene {
+    dvg_context* ctx = nullptr;
+    HostScene host;
+    DevScene dev{};
+    DevBuf arena;
+    DevBuf tiles;    // counts, offsets
+    DevBuf entries;  // tile entries
+    DevBuf grads;    // gradient arena (device)
+    size_t grad_off[11] = {0};
+    size_t grad_floats = 0;
+    const float4* g_bbox = nullptr;
+};
+
+namespace {
+
+// Offsets of each gradient part inside the scene's gradient arena (in floats).
+void layout_grads(dvg_scene* sc) {
+    const HostScene& h = sc->host;
+    size_t sizes[11] = {4 * (size_t)h.num_shapes, 9 * (size_t)h.num_shapes, h.num_shapes, 2 * (size_t)h.total_points,
+                        h.total_points,           9 * (size_t)h.num_groups, 4 * (size_t)h.num_paints,
+                        h.total_stops,            4 * (size_t)h.total_stops, 1, 4};
+    size_t off = 0;
+    for (int i = 0; i < 11; ++i) {
+        sc->grad_off[i] = off;
+        off += (sizes[i] + 63) & ~(size_t)63;
+    }
+    sc->grad_floats = off;
+}
+GradPtrs device_grads(dvg_scene* sc) {
+    float* b = sc->grads.as<float>();
+    GradPtrs g;
+    g.d_shape_params = b + sc->grad_off[0];
+    g.d_shape_transform = b + sc->grad_off[1];
+    g.d_shape_stroke_width = b + sc->grad_off[2];
+    g.d_points = b + sc->grad_off[3];
+    g.d_thickness = b + sc->grad_off[4];
+    g.d_group_transform = b + sc->grad_off[5];
+    g.d_paint_params = b + sc->grad_off[6];
+    g.d_stop_offsets = b + sc->grad_off[7];
+    g.d_stop_colors = b + sc->grad_off[8];
+    g.d_filter_radius = b + sc->grad_off[9];
+    g.d_background = b + sc->grad_off[10];
+    g.d_background_image = nullptr;
+    g.d_translation = nullptr;
+    return g;
+}
+
+dvg_status check_options(const dvg_render_options* o) {
+    if (!o) return fail(DVG_ERR_INVALID_ARGUMENT, "null render options");
+    if (o->use_prefiltering)
+        return fail(DVG_ERR_INVALID_ARGUMENT,
+                    "use_prefiltering=1 is not implemented by this library yet; pass use_prefiltering=0");
+    return DVG_OK;
+}
+SampleParams sample_params(const dvg_render_options* o) {
+    SampleParams sp;
+    sp.sxn = o->samples_x > 0 ? (int)o->samples_x : 1;
+    sp.syn = o->samples_y > 0 ? (int)o->samples_y : 1;
+    sp.seed = o->seed;
+    sp.jitter = o->jitter != 0 && o->use_prefiltering == 0;
+    return sp;
+}
+dvg_status check_status(dvg_context* ctx) {
+    unsigned st = 0;
+    CK(cudaMemcpyAsync(&st, ctx->status, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (st & ST_FRAGMENT_OVERFLOW) {
+        CK(cudaMemsetAsync(ctx->status, 0, sizeof(unsigned), ctx->stream));
+        return fail(DVG_ERR_DEVICE_LIMIT, "a sample covered more fragments than the per-thread capacity (" +
+                                              std::to_string(MAX_FRAGMENTS) + ")");
+    }
+    return DVG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t dvg_abi_version(void) { return DVG_ABI_VERSION; }
+
+const char* dvg_last_error(void) { return g_last_error.c_str(); }
+
+dvg_status dvg_context_create(int device, dvg_context** out) {
+    if (!out) return fail(DVG_ERR_INVALID_ARGUMENT, "null output pointer");
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) return fail(DVG_ERR_NO_DEVICE, "no CUDA device available");
+    if (device < 0 || device >= count) return fail(DVG_ERR_INVALID_ARGUMENT, "device index out of range");
+    std::unique_ptr<dvg_context> ctx(new dvg_context());
+    ctx->device = device;
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    CK(cudaMalloc(&ctx->status, sizeof(unsigned)));
+    CK(cudaMemsetAsync(ctx->status, 0, sizeof(unsigned), ctx->stream));
+    *out = ctx.release();
+    return DVG_OK;
+}
+
+void dvg_context_destroy(dvg_context* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->status) cudaFree(ctx->status);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+uint64_t dvg_context_launch_count(const dvg_context* ctx) { return ctx ? ctx->launches : 0; }
+
+void* dvg_context_stream(dvg_context* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+dvg_status dvg_scene_upload(dvg_context* ctx, const dvg_scene_desc* desc, dvg_scene** out) {
+    if (!ctx || !desc || !out) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    CK(cudaSetDevice(ctx->device));
+    std::unique_ptr<dvg_scene> sc(new dvg_scene());
+    sc->ctx = ctx;
+    std::string err;
+    dvg_status st = prepare_scene(desc, &sc->host, &err);
+    if (st != DVG_OK) return fail(st, err);
+    const HostScene& h = sc->host;
+    Blob b;
+    size_t o_g_c2s = b.add(h.g_c2s), o_g_s2c = b.add(h.g_s2c), o_g_info = b.add(h.g_info), o_g_bvh = b.add(h.g_bvh),
+           o_g_bbox = b.add(h.g_bbox), o_g_list = b.add(h.g_shape_list), o_gn_b = b.add(h.gn_bounds),
+           o_gn_m = b.add(h.gn_meta), o_gl = b.add(h.gl_shapes), o_s_info = b.add(h.s_info),
+           o_s_prm = b.add(h.s_params), o_s_inv = b.add(h.s_inv), o_s_x = b.add(h.s_xform),
+           o_s_sw = b.add(h.s_stroke), o_p_info = b.add(h.p_info), o_pn_b = b.add(h.pn_bounds),
+           o_pn_m = b.add(h.pn_meta), o_pl = b.add(h.pl_segs), o_seg_p = b.add(h.seg_p), o_seg_r = b.add(h.seg_r),
+           o_seg_m = b.add(h.seg_meta), o_pts = b.add(h.points), o_th = b.add(h.thickness), o_ncp = b.add(h.ncp),
+           o_pi = b.add(h.paint_info), o_pp = b.add(h.paint_params), o_so = b.add(h.stop_offsets),
+           o_sc = b.add(h.stop_colors), o_len = b.add(h.shape_len), o_bcdf = b.add(h.bcdf),
+           o_bpmf = b.add(h.bpmf), o_bs = b.add(h.b_shape), o_bg = b.add(h.b_group),
+           o_pci = b.add(h.path_cdf_info), o_pcdf = b.add(h.path_cdf), o_ppmf = b.add(h.path_pmf),
+           o_ppid = b.add(h.path_pid), o_plen = b.add(h.path_len_arr), o_bgi = b.add(h.bg_image);
+    CK(sc->arena.reserve(b.data.size()));
+    CK(cudaMemcpyAsync(sc->arena.ptr, b.data.data(), b.data.size(), cudaMemcpyHostToDevice, ctx->stream));
+    char* base = sc->arena.as<char>();
+    DevScene& S = sc->dev;
+    S.width = (int)h.width;
+    S.height = (int)h.height;
+    S.num_groups = (int)h.num_groups;
+    S.num_shapes = (int)h.num_shapes;
+    S.num_paints = (int)h.num_paints;
+    S.num_paths = (int)h.num_paths;
+    S.filter_type = (int)h.filter_type;
+    S.filter_radius = h.filter_radius;
+    {
+        float c = std::ceil(h.filter_radius);
+        S.filter_ri = c > 0.0f ? (int)std::min(c, 1024.0f) : 0;
+    }
+    for (int k = 0; k < 4; ++k) S.bg[k] = h.bg[k];
+    S.bg_image = h.bg_image.empty() ? nullptr : (const float*)(base + o_bgi);
+    S.g_c2s = (const float*)(base + o_g_c2s);
+    S.g_s2c = (const float*)(base + o_g_s2c);
+    S.g_info = (const int4*)(base + o_g_info);
+    S.g_bvh = (const int4*)(base + o_g_bvh);
+    S.g_shape_list = (const int*)(base + o_g_list);
+    S.gn_bounds = (const float4*)(base + o_gn_b);
+    S.gn_meta = (const int4*)(base + o_gn_m);
+    S.gl_shapes = (const int*)(base + o_gl);
+    S.s_info = (const int4*)(base + o_s_info);
+    S.s_params = (const float4*)(base + o_s_prm);
+    S.s_inv = (const float*)(base + o_s_inv);
+    S.s_xform = (const float*)(base + o_s_x);
+    S.s_stroke = (const float*)(base + o_s_sw);
+    S.p_info = (const int4*)(base + o_p_info);
+    S.pn_bounds = (const float4*)(base + o_pn_b);
+    S.pn_meta = (const int4*)(base + o_pn_m);
+    S.pl_segs = (const int*)(base + o_pl);
+    S.seg_p = (const float4*)(base + o_seg_p);
+    S.seg_r = (const float4*)(base + o_seg_r);
+    S.seg_meta = (const int4*)(base + o_seg_m);
+    S.points = (const float2*)(base + o_pts);
+    S.thickness = (const float*)(base + o_th);
+    S.ncp = (const uint8_t*)(base + o_ncp);
+    S.paint_info = (const int4*)(base + o_pi);
+    S.paint_params = (const float4*)(base + o_pp);
+    S.stop_offsets = (const float*)(base + o_so);
+    S.stop_colors = (const float4*)(base + o_sc);
+    S.boundary_ok = h.boundary_ok ? 1 : 0;
+    S.bcdf_n = (int)h.bcdf.size();
+    S.shape_len = (const float*)(base + o_len);
+    S.bcdf = (const float*)(base + o_bcdf);
+    S.bpmf = (const float*)(base + o_bpmf);
+    S.b_shape = (const int*)(base + o_bs);
+    S.b_group = (const int*)(base + o_bg);
+    S.path_cdf_info = (const int4*)(base + o_pci);
+    S.path_cdf = (const float*)(base + o_pcdf);
+    S.path_pmf = (const float*)(base + o_ppmf);
+    S.path_pid = (const int*)(base + o_ppid);
+    S.path_len = (const float*)(base + o_plen);
+    sc->g_bbox = (const float4*)(base + o_g_bbox);
+    // tile binning
+    S.tiles_x = (S.width + TILE - 1) / TILE;
+    S.tiles_y = (S.height + TILE - 1) / TILE;
+    const int tiles = S.tiles_x * S.tiles_y;
+    if (tiles > 0) {
+        CK(sc->tiles.reserve(sizeof(int) * (2 * (size_t)tiles + 1)));
+        int* counts = sc->tiles.as<int>();
+        int* offsets = counts + tiles;
+        ctx->launches += launch_binning(S, sc->g_bbox, counts, offsets, nullptr, ctx->stream);
+        CK(cudaGetLastError());
+        int total = 0;
+        CK(cudaMemcpyAsync(&total, offsets + tiles, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        CK(sc->entries.reserve(sizeof(int) * (size_t)std::max(total, 1)));
+        S.tile_offsets = offsets;
+        S.tile_entries = sc->entries.as<int>();
+        ctx->launches += launch_binning(S, sc->g_bbox, counts, offsets, sc->entries.as<int>(), ctx->stream);
+        CK(cudaGetLastError());
+    }
+    layout_grads(sc.get());
+    CK(sc->grads.reserve(sizeof(float) * std::max<size_t>(sc->grad_floats, 64)));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *out = sc.release();
+    return DVG_OK;
+}
+
+void dvg_scene_destroy(dvg_scene* scene) {
+    if (!scene) return;
+    cudaSetDevice(scene->ctx->device);
+    cudaStreamSynchronize(scene->ctx->stream);
+    delete scene;
+}
+
+static dvg_status render_into(dvg_context* ctx, dvg_scene* sc, const dvg_render_options* opts, float* out_dev) {
+    const DevScene& S = sc->dev;
+    const size_t npix = (size_t)S.width * S.height;
+    if (npix == 0) return DVG_OK;
+    if (S.num_groups == 0) {  // Image::solid / background image (src/renderer/renderer.rs:57-66)
+        ctx->launches += launch_fill_background(S, out_dev, ctx->stream);
+        CK(cudaGetLastError());
+        return DVG_OK;
+    }
+    SampleParams sp = sample_params(opts);
+    CK(ctx->accum.reserve(npix * 4 * sizeof(float)));
+    CK(ctx->wsum.reserve(npix * sizeof(float)));
+    CK(cudaMemsetAsync(ctx->accum.ptr, 0, npix * 4 * sizeof(float), ctx->stream));
+    CK(cudaMemsetAsync(ctx->wsum.ptr, 0, npix * sizeof(float), ctx->stream));
+    ctx->launches += launch_forward(S, sp, ctx->accum.as<float>(), ctx->wsum.as<float>(), ctx->status, ctx->stream);
+    CK(cudaGetLastError());
+    ctx->launches += launch_resolve(S, ctx->accum.as<float>(), ctx->wsum.as<float>(), out_dev, ctx->stream);
+    CK(cudaGetLastError());
+    return DVG_OK;
+}
+
+dvg_status dvg_render_device(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts, float* out_rgba) {
+    if (!ctx || !scene || !out_rgba) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    dvg_status st = check_options(opts);
+    if (st != DVG_OK) return st;
+    CK(cudaSetDevice(ctx->device));
+    return render_into(ctx, scene, opts, out_rgba);
+}
+
+dvg_status dvg_render_host(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts, float* out_rgba) {
+    if (!ctx || !scene || !out_rgba) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    dvg_status st = check_options(opts);
+    if (st != DVG_OK) return st;
+    CK(cudaSetDevice(ctx->device));
+    const HostScene& h = scene->host;
+    const size_t npix = (size_t)h.width * h.height;
+    if (npix == 0) return DVG_OK;
+    if (h.num_groups == 0) {  // src/renderer/renderer.rs:57-66
+        for (size_t i = 0; i < npix; ++i)
+            for (int k = 0; k < 4; ++k) out_rgba[4 * i + k] = h.bg_image.empty() ? h.bg[k] : h.bg_image[4 * i + k];
+        return DVG_OK;
+    }
+    CK(ctx->image.reserve(npix * 4 * sizeof(float)));
+    st = render_into(ctx, scene, opts, ctx->image.as<float>());
+    if (st != DVG_OK) return st;
+    CK(cudaMemcpyAsync(out_rgba, ctx->image.ptr, npix * 4 * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return check_status(ctx);
+}
+
+// Backward on device buffers.  `have_weights`: ctx->wsum already holds this scene's weights.
+static dvg_status backward_core(dvg_context* ctx, dvg_scene* sc, const dvg_render_options* opts,
+                                const dvg_backward_options* bopts, const float* d_render, const GradPtrs& G,
+                                bool have_weights) {
+    const DevScene& S = sc->dev;
+    const size_t npix = (size_t)S.width * S.height;
+    if (npix == 0) return DVG_OK;
+    SampleParams sp = sample_params(opts);
+    if (d_render && S.num_groups > 0) {
+        if (!have_weights) {
+            CK(ctx->wsum.reserve(npix * sizeof(float)));
+            CK(cudaMemsetAsync(ctx->wsum.ptr, 0, npix * sizeof(float), ctx->stream));
+            ctx->launches += launch_weights(S, sp, ctx->wsum.as<float>(), ctx->stream);
+            CK(cudaGetLastError());
+        }
+        ctx->launches += launch_interior(S, sp, d_render, ctx->wsum.as<float>(), G, ctx->status, ctx->stream);
+        CK(cudaGetLastError());
+        if (S.boundary_ok) {
+            BoundaryParams bp;
+            uint64_t total = (uint64_t)npix * sp.sxn * sp.syn;
+            bp.num_samples = bopts && bopts->boundary_samples ? bopts->boundary_samples : total;
+            bp.sample_base = 0;
+            bp.seed = (bopts && !bopts->boundary_seed_from_options) ? bopts->boundary_seed : opts->seed;
+            bp.rng = bopts ? (int)bopts->rng : 0;
+            ctx->launches += launch_boundary(S, bp, d_render, ctx->wsum.as<float>(), G, ctx->stream);
+            CK(cudaGetLastError());
+        }
+    } else if (d_render && S.num_groups == 0) {
+        // only the background receives gradient: every sample lands on it.
+        if (!have_weights) {
+            CK(ctx->wsum.reserve(npix * sizeof(float)));
+            CK(cudaMemsetAsync(ctx->wsum.ptr, 0, npix * sizeof(float), ctx->stream));
+            ctx->launches += launch_weights(S, sp, ctx->wsum.as<float>(), ctx->stream);
+        }
+        ctx->launches += launch_interior(S, sp, d_render, ctx->wsum.as<float>(), G, ctx->status, ctx->stream);
+        CK(cudaGetLastError());
+    }
+    ctx->launches += launch_finalize_background(S, G, ctx->stream);
+    CK(cudaGetLastError());
+    return DVG_OK;
+}
+
+static GradPtrs grads_from_user(const dvg_grads* g) {
+    GradPtrs p;
+    p.d_shape_params = g->d_shape_params;
+    p.d_shape_transform = g->d_shape_transform;
+    p.d_shape_stroke_width = g->d_shape_stroke_width;
+    p.d_points = g->d_points;
+    p.d_thickness = g->d_thickness;
+    p.d_group_transform = g->d_group_transform;
+    p.d_paint_params = g->d_paint_params;
+    p.d_stop_offsets = g->d_stop_offsets;
+    p.d_stop_colors = g->d_stop_colors;
+    p.d_filter_radius = g->d_filter_radius;
+    p.d_background = g->d_background;
+    p.d_background_image = g->d_background_image;
+    p.d_translation = g->d_translation;
+    return p;
+}
+
+// Zero every part of a device gradient set (scene arena or caller buffers).
+static dvg_status zero_grads(dvg_context* ctx, dvg_scene* sc, const GradPtrs& G) {
+    const HostScene& h = sc->host;
+    const size_t npix = (size_t)h.width * h.height;
+    struct Part {
+        float* p;
+        size_t n;
+    } parts[] = {{G.d_shape_params, 4 * (size_t)h.num_shapes},
+                 {G.d_shape_transform, 9 * (size_t)h.num_shapes},
+                 {G.d_shape_stroke_width, h.num_shapes},
+                 {G.d_points, 2 * (size_t)h.total_points},
+                 {G.d_thickness, h.total_points},
+                 {G.d_group_transform, 9 * (size_t)h.num_groups},
+                 {G.d_paint_params, 4 * (size_t)h.num_paints},
+                 {G.d_stop_offsets, h.total_stops},
+                 {G.d_stop_colors, 4 * (size_t)h.total_stops},
+                 {G.d_filter_radius, 1},
+                 {G.d_background, 4},
+                 {G.d_background_image, 4 * npix},
+                 {G.d_translation, 2 * npix}};
+    for (auto& p : parts)
+        if (p.p && p.n) CK(cudaMemsetAsync(p.p, 0, p.n * sizeof(float), ctx->stream));
+    return DVG_OK;
+}
+
+static dvg_status check_backward_args(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
+                                      const float* d_sdf, const dvg_grads* grads) {
+    if (!ctx || !scene || !grads) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    if (d_sdf) return fail(DVG_ERR_INVALID_ARGUMENT, "d_sdf_image is not supported by this library yet");
+    dvg_status st = check_options(opts);
+    if (st != DVG_OK) return st;
+    const GradPtrs G = grads_from_user(grads);
+    if (!G.d_shape_params || !G.d_shape_transform || !G.d_shape_stroke_width || !G.d_group_transform ||
+        !G.d_paint_params || !G.d_filter_radius || !G.d_background ||
+        (scene->host.total_points && (!G.d_points || !G.d_thickness)) ||
+        (scene->host.total_stops && (!G.d_stop_offsets || !G.d_stop_colors)))
+        return fail(DVG_ERR_INVALID_ARGUMENT, "missing gradient buffer");
+    return DVG_OK;
+}
+
+dvg_status dvg_render_backward_device(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
+                                      const dvg_backward_options* bopts, const float* d_render, const float* d_sdf,
+                                      dvg_grads* grads) {
+    dvg_status st = check_backward_args(ctx, scene, opts, d_sdf, grads);
+    if (st != DVG_OK) return st;
+    CK(cudaSetDevice(ctx->device));
+    GradPtrs G = grads_from_user(grads);
+    if (!(bopts && bopts->compute_translation)) G.d_translation = nullptr;
+    if (!(d_render && scene->dev.bg_image)) G.d_background_image = nullptr;
+    st = zero_grads(ctx, scene, grads_from_user(grads));
+    if (st != DVG_OK) return st;
+    return backward_core(ctx, scene, opts, bopts, d_render, G, false);
+}
+
+dvg_status dvg_render_backward_host(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
+                                    const dvg_backward_options* bopts, const float* d_render, const float* d_sdf,
+                                    dvg_grads* grads) {
+    dvg_status st = check_backward_args(ctx, scene, opts, d_sdf, grads);
+    if (st != DVG_OK) return st;
+    CK(cudaSetDevice(ctx->device));
+    const HostScene& h = scene->host;
+    const size_t npix = (size_t)h.width * h.height;
+    GradPtrs G = device_grads(scene);
+    CK(cudaMemsetAsync(scene->grads.ptr, 0, scene->grad_floats * sizeof(float), ctx->stream));
+    bool want_bg_img = d_render && !h.bg_image.empty() && grads->d_background_image;
+    bool want_tr = bopts && bopts->compute_translation && grads->d_translation;
+    if (want_bg_img) {
+        CK(ctx->bg_grad.reserve(npix * 4 * sizeof(float)));
+        CK(cudaMemsetAsync(ctx->bg_grad.ptr, 0, npix * 4 * sizeof(float), ctx->stream));
+        G.d_background_image = ctx->bg_grad.as<float>();
+    }
+    if (want_tr) {
+        CK(ctx->trans_grad.reserve(npix * 2 * sizeof(float)));
+        CK(cudaMemsetAsync(ctx->trans_grad.ptr, 0, npix * 2 * sizeof(float), ctx->stream));
+        G.d_translation = ctx->trans_grad.as<float>();
+    }
+    const float* dr = nullptr;
+    if (d_render && npix) {
+        CK(ctx->d_render.reserve(npix * 4 * sizeof(float)));
+        CK(cudaMemcpyAsync(ctx->d_render.ptr, d_render, npix * 4 * sizeof(float), cudaMemcpyHostToDevice,
+                           ctx->stream));
+        dr = ctx->d_render.as<float>();
+    }
+    st = backward_core(ctx, scene, opts, bopts, dr, G, false);
+    if (st != DVG_OK) return st;
+    struct Part {
+        float* dst;
+        const float* src;
+        size_t n;
+    } parts[] = {{grads->d_shape_params, G.d_shape_params, 4 * (size_t)h.num_shapes},
+                 {grads->d_shape_transform, G.d_shape_transform, 9 * (size_t)h.num_shapes},
+                 {grads->d_shape_stroke_width, G.d_shape_stroke_width, h.num_shapes},
+                 {grads->d_points, G.d_points, 2 * (size_t)h.total_points},
+                 {grads->d_thickness, G.d_thickness, h.total_points},
+                 {grads->d_group_transform, G.d_group_transform, 9 * (size_t)h.num_groups},
+                 {grads->d_paint_params, G.d_paint_params, 4 * (size_t)h.num_paints},
+                 {grads->d_stop_offsets, G.d_stop_offsets, h.total_stops},
+                 {grads->d_stop_colors, G.d_stop_colors, 4 * (size_t)h.total_stops},
+                 {grads->d_filter_radius, G.d_filter_radius, 1},
+                 {grads->d_background, G.d_background, 4}};
+    for (auto& p : parts)
+        if (p.dst && p.n) CK(cudaMemcpyAsync(p.dst, p.src, p.n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    if (grads->d_background_image) {
+        if (want_bg_img)
+            CK(cudaMemcpyAsync(grads->d_background_image, G.d_background_image, npix * 4 * sizeof(float),
+                               cudaMemcpyDeviceToHost, ctx->stream));
+        else
+            std::memset(grads->d_background_image, 0, npix * 4 * sizeof(float));
+    }
+    if (grads->d_translation) {
+        if (want_tr)
+            CK(cudaMemcpyAsync(grads->d_translation, G.d_translation, npix * 2 * sizeof(float),
+                               cudaMemcpyDeviceToHost, ctx->stream));
+        else
+            std::memset(grads->d_translation, 0, npix * 2 * sizeof(float));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return check_status(ctx);
+}
+
+dvg_status dvg_render(dvg_context* ctx, const dvg_scene_desc* desc, const dvg_render_options* opts, float* out_rgba) {
+    if (!ctx || !desc || !out_rgba) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    dvg_status st = check_options(opts);
+    if (st != DVG_OK) return st;
+    dvg_scene* sc = nullptr;
+    st = dvg_scene_upload(ctx, desc, &sc);
+    if (st != DVG_OK) return st;
+    st = dvg_render_host(ctx, sc, opts, out_rgba);
+    dvg_scene_destroy(sc);
+    return st;
+}
+
+dvg_status dvg_render_backward(dvg_context* ctx, const dvg_scene_desc* desc, const dvg_render_options* opts,
+                               const dvg_backward_options* bopts, const float* d_render, const float* d_sdf,
+                               dvg_grads* grads) {
+    if (!ctx || !desc || !grads) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    dvg_status st = check_options(opts);
+    if (st != DVG_OK) return st;
+    dvg_scene* sc = nullptr;
+    st = dvg_scene_upload(ctx, desc, &sc);
+    if (st != DVG_OK) return st;
+    st = dvg_render_backward_host(ctx, sc, opts, bopts, d_render, d_sdf, grads);
+    dvg_scene_destroy(sc);
+    return st;
+}
+
+dvg_status dvg_fwd_bwd_l2_device(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
+                                 const dvg_backward_options* bopts, const float* target_rgba, float* out_rgba,
+                                 float* loss_out, dvg_grads* grads) {
+    dvg_status st = check_backward_args(ctx, scene, opts, nullptr, grads);
+    if (st != DVG_OK) return st;
+    if (!target_rgba) return fail(DVG_ERR_INVALID_ARGUMENT, "null target");
+    CK(cudaSetDevice(ctx->device));
+    const size_t npix = (size_t)scene->dev.width * scene->dev.height;
+    if (npix == 0) return DVG_OK;
+    float* img = out_rgba;
+    if (!img) {
+        CK(ctx->image.reserve(npix * 4 * sizeof(float)));
+        img = ctx->image.as<float>();
+    }
+    st = render_into(ctx, scene, opts, img);
+    if (st != DVG_OK) return st;
+    CK(ctx->d_render.reserve(npix * 4 * sizeof(float)));
+    if (loss_out) CK(cudaMemsetAsync(loss_out, 0, sizeof(float), ctx->stream));
+    ctx->launches += launch_l2(img, target_rgba, npix * 4, ctx->d_render.as<float>(), loss_out, ctx->stream);
+    CK(cudaGetLastError());
+    GradPtrs G = grads_from_user(grads);
+    if (!(bopts && bopts->compute_translation)) G.d_translation = nullptr;
+    if (!scene->dev.bg_image) G.d_background_image = nullptr;
+    st = zero_grads(ctx, scene, G);
+    if (st != DVG_OK) return st;
+    return backward_core(ctx, scene, opts, bopts, ctx->d_render.as<float>(), G, true);
+}
+
+}  // extern "C"

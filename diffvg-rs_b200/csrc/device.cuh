@@ -1,0 +1,887 @@
+// device.cuh — device-side scene evaluation for the diffvg hot path (sm_100a).
+//
+// Per-sample evaluation with the crate's CPU semantics (src/backward/sampling.rs,
+// src/distance/*.rs): stroke "within distance" and fill winding-number tests,
+// evaluated over the crate's median-split BVHs (rebuilt on the host with the same
+// topology, walked here with skip links).  Arithmetic mirrors the crate: f32
+// everywhere, f64 exactly where the crate casts to f64 (root solves), and the
+// translation unit is compiled with -fmad=false so that no multiply-add is fused
+// (Rust never fuses), which keeps inside/outside decisions bit-identical.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "prepare.hpp"  // ShapeFlags shared with the host preparation
+
+namespace dvgb {
+
+constexpr int TILE = 16;          // tile edge in pixels (the crate's TILE_SIZE)
+constexpr int TILE_PIXELS = TILE * TILE;
+constexpr float PI_F = 3.14159265358979323846f;
+constexpr float HALF_PI_F = 1.57079632679489661923f;
+
+enum : int { K_CIRCLE = 0, K_RECT = 1, K_PATH = 2, K_ELLIPSE = 3 };
+enum : int { P_NONE = 0, P_SOLID = 1, P_LINEAR = 2, P_RADIAL = 3 };
+enum : int { F_BOX = 0, F_TENT = 1, F_PARABOLIC = 2, F_HANN = 3, F_GAUSSIAN = 4 };
+enum : int { PF_CLOSED = 1, PF_APPROX = 2, PF_THICK = 4 };
+
+// Device status bits written by kernels (never a trap: the host reads them).
+enum : unsigned { ST_FRAGMENT_OVERFLOW = 1u, ST_BVH_LIMIT = 2u };
+
+struct DevScene {
+    int width, height;
+    int num_groups, num_shapes, num_paints, num_paths;
+    int filter_type;
+    float filter_radius;
+    int filter_ri;
+    float bg[4];
+    const float* bg_image;
+    // groups
+    const float* g_c2s;  // 9 per group (full canvas_to_shape)
+    const float* g_s2c;  // 9 per group
+    const int4* g_info;  // fill paint, stroke paint, fill rule, 0
+    const int4* g_bvh;   // node off, node count, list off, list count
+    const int* g_shape_list;
+    const float4* gn_bounds;
+    const int4* gn_meta;  // skip, leaf start, count, 0
+    const int* gl_shapes;
+    // shapes
+    const int4* s_info;  // kind, flags, path index, 0
+    const float4* s_params;
+    const float* s_inv;    // 6 per shape
+    const float* s_xform;  // 9 per shape
+    const float* s_stroke;
+    // paths
+    const int4* p_info;  // 2 per path: (seg off, seg cnt, node off, node cnt), (pt off, pt cnt, ctrl off, flags)
+    const float4* pn_bounds;
+    const int4* pn_meta;
+    const int* pl_segs;
+    const float4* seg_p;  // 2 per segment
+    const float4* seg_r;
+    const int4* seg_meta;  // kind, segment index, point id, shape
+    const float2* points;
+    const float* thickness;
+    const uint8_t* ncp;
+    // paints
+    const int4* paint_info;  // kind, stop off, stop count, 0
+    const float4* paint_params;
+    const float* stop_offsets;
+    const float4* stop_colors;
+    // boundary tables
+    int boundary_ok;
+    int bcdf_n;
+    const float* shape_len;
+    const float* bcdf;
+    const float* bpmf;
+    const int* b_shape;
+    const int* b_group;
+    const int4* path_cdf_info;
+    const float* path_cdf;
+    const float* path_pmf;
+    const int* path_pid;
+    const float* path_len;
+    // tile binning
+    int tiles_x, tiles_y;
+    const int* tile_offsets;
+    const int* tile_entries;
+};
+
+// ------------------------------------------------------------------ small math
+__device__ __forceinline__ float clampf(float v, float lo, float hi) {
+    if (v < lo) v = lo;
+    if (v > hi) v = hi;
+    return v;
+}
+__device__ __forceinline__ float len2(float x, float y) { return sqrtf(x * x + y * y); }
+// Rust `f as i32` (saturating, NaN -> 0) — cvt.rzi.s32.f32 has exactly these semantics.
+__device__ __forceinline__ int f2i(float f) { return __float2int_rz(f); }
+__device__ __forceinline__ float2 xf6(const float* m, float2 p) {  // Mat3::transform_point
+    return make_float2(m[0] * p.x + m[1] * p.y + m[2], m[3] * p.x + m[4] * p.y + m[5]);
+}
+__device__ __forceinline__ float2 xf9(const float* m, float2 p) {
+    return make_float2(m[0] * p.x + m[1] * p.y + m[2], m[3] * p.x + m[4] * p.y + m[5]);
+}
+// distance/utils.rs:7-16: identity shortcut, singular -> unchanged
+__device__ __forceinline__ float2 shape_local_dist(const DevScene& S, int s, float2 p) {
+    int flags = S.s_info[s].y;
+    if (flags & SF_IDENTITY) return p;
+    if (flags & SF_INVERTIBLE) return xf6(S.s_inv + 6 * s, p);
+    return p;
+}
+// backward/math.rs:131-135: no identity shortcut, singular -> identity
+__device__ __forceinline__ float2 shape_local_bwd(const DevScene& S, int s, float2 p) {
+    if (S.s_info[s].y & SF_INVERTIBLE) return xf6(S.s_inv + 6 * s, p);
+    return p;
+}
+
+// ------------------------------------------------------------------ polynomial roots (f64, distance/utils.rs:48-123)
+__device__ __forceinline__ bool solve_quadratic(double a, double b, double c, double t[2]) {
+    const double eps = 1.0e-12;
+    if (fabs(a) < eps) {
+        if (fabs(b) < eps) return false;
+        double root = -c / b;
+        t[0] = root;
+        t[1] = root;
+        return true;
+    }
+    double discrim = b * b - 4.0 * a * c;
+    if (discrim < 0.0) return false;
+    double root = sqrt(discrim);
+    if (fabs(root) < eps) {
+        double r = -0.5 * b / a;
+        t[0] = r;
+        t[1] = r;
+        return true;
+    }
+    double q = (b < 0.0) ? -0.5 * (b - root) : -0.5 * (b + root);
+    if (fabs(q) < eps) {
+        double inv = 0.5 / a;
+        t[0] = (-b - root) * inv;
+        t[1] = (-b + root) * inv;
+    } else {
+        t[0] = q / a;
+        t[1] = c / q;
+    }
+    if (t[0] > t[1]) {
+        double tmp = t[0];
+        t[0] = t[1];
+        t[1] = tmp;
+    }
+    return true;
+}
+__device__ __forceinline__ double cbrt_pow(double x) {
+    if (x > 0.0) return pow(x, 1.0 / 3.0);
+    if (x < 0.0) return -pow(-x, 1.0 / 3.0);
+    return 0.0;
+}
+__device__ __forceinline__ int solve_cubic(double a, double b, double c, double d, double t[3]) {
+    if (fabs(a) < 1.0e-6) {
+        double r2[2];
+        if (solve_quadratic(b, c, d, r2)) {
+            t[0] = r2[0];
+            t[1] = r2[1];
+            return 2;
+        }
+        return 0;
+    }
+    b = b / a;
+    c = c / a;
+    d = d / a;
+    double q = (b * b - 3.0 * c) / 9.0;
+    double r = (2.0 * b * b * b - 9.0 * b * c + 27.0 * d) / 54.0;
+    const double TWO_PI = 6.283185307179586476925286766559;
+    if (r * r < q * q * q) {
+        double theta = acos(r / sqrt(q * q * q));
+        double sq = sqrt(q);
+        t[0] = -2.0 * sq * cos(theta / 3.0) - b / 3.0;
+        t[1] = -2.0 * sq * cos((theta + TWO_PI) / 3.0) - b / 3.0;
+        t[2] = -2.0 * sq * cos((theta - TWO_PI) / 3.0) - b / 3.0;
+        return 3;
+    }
+    double ar = (r > 0.0) ? -cbrt_pow(r + sqrt(r * r - q * q * q)) : cbrt_pow(-r + sqrt(r * r - q * q * q));
+    double br = (fabs(ar) > 1.0e-6) ? q / ar : 0.0;
+    t[0] = (ar + br) - b / 3.0;
+    return 1;
+}
+
+// ------------------------------------------------------------------ closest points (distance/curve.rs)
+struct CPRes {
+    float cx, cy, t, dist;
+};
+__device__ __forceinline__ CPRes closest_line(float2 p, float ax, float ay, float bx, float by) {  // curve.rs:10-21
+    float abx = bx - ax, aby = by - ay;
+    float denom = abx * abx + aby * aby;
+    if (denom <= 1.0e-10f) return CPRes{ax, ay, 0.0f, len2(p.x - ax, p.y - ay)};
+    float t = clampf(((p.x - ax) * abx + (p.y - ay) * aby) / denom, 0.0f, 1.0f);
+    float cx = ax + abx * t, cy = ay + aby * t;
+    return CPRes{cx, cy, t, len2(p.x - cx, p.y - cy)};
+}
+static __device__ __noinline__ CPRes closest_quad_approx(float2 pt, const float* q) {  // curve.rs:267-296
+    float b0x = q[0] - pt.x, b0y = q[1] - pt.y, b1x = q[2] - pt.x, b1y = q[3] - pt.y;
+    float b2x = q[4] - pt.x, b2y = q[5] - pt.y;
+    float a = b0x * b2y - b0y * b2x;
+    float b = 2.0f * (b1x * b0y - b1y * b0x);
+    float d = 2.0f * (b2x * b1y - b2y * b1x);
+    float f = b * d - a * a;
+    float d21x = b2x - b1x, d21y = b2y - b1y, d10x = b1x - b0x, d10y = b1y - b0y, d20x = b2x - b0x, d20y = b2y - b0y;
+    float gx = (d21x * b) + (d10x * d) + (d20x * a);
+    float gy = (d21y * b) + (d10y * d) + (d20y * a);
+    gx = gx * 2.0f;
+    gy = gy * 2.0f;
+    float gfx = gy, gfy = -gx;
+    float t = 0.0f;
+    float denom = gfx * gfx + gfy * gfy;
+    if (denom > 1.0e-8f) {
+        float s = -f / denom;
+        float ppx = gfx * s, ppy = gfy * s;
+        float d0px = b0x - ppx, d0py = b0y - ppy;
+        float ap = d0px * d20y - d0py * d20x;
+        float bp = 2.0f * (d10x * d0py - d10y * d0px);
+        float denom2 = 2.0f * a + b + d;
+        if (fabsf(denom2) > 1.0e-8f) t = clampf((ap + bp) / denom2, 0.0f, 1.0f);
+    }
+    float tt = 1.0f - t;
+    float w0 = tt * tt, w1 = 2.0f * tt * t, w2 = t * t;
+    float cx = q[0] * w0 + q[2] * w1 + q[4] * w2, cy = q[1] * w0 + q[3] * w1 + q[5] * w2;
+    return CPRes{cx, cy, t, len2(pt.x - cx, pt.y - cy)};
+}
+static __device__ __noinline__ CPRes closest_quad(float2 pt, const float* q, bool approx) {  // curve.rs:26-78
+    if (approx) return closest_quad_approx(pt, q);
+    float best_t = 0.0f, bx = q[0], by = q[1];
+    float best = len2(pt.x - q[0], pt.y - q[1]);
+    float de = len2(pt.x - q[4], pt.y - q[5]);
+    if (de < best) {
+        best = de;
+        bx = q[4];
+        by = q[5];
+        best_t = 1.0f;
+    }
+    double ax = (double)(q[0] - 2.0f * q[2] + q[4]);
+    double ay = (double)(q[1] - 2.0f * q[3] + q[5]);
+    double bbx = (double)(-q[0] + q[2]);
+    double bby = (double)(-q[1] + q[3]);
+    double cx = (double)(q[0] - pt.x);
+    double cy = (double)(q[1] - pt.y);
+    double A = ax * ax + ay * ay;
+    double B = 3.0 * (ax * bbx + ay * bby);
+    double Cc = 2.0 * (bbx * bbx + bby * bby) + (ax * cx + ay * cy);
+    double D = bbx * cx + bby * cy;
+    double r[3];
+    int n = solve_cubic(A, B, Cc, D, r);
+    for (int i = 0; i < n; ++i) {
+        double t = r[i];
+        if (t >= 0.0 && t <= 1.0) {
+            float t32 = (float)t;
+            float tt = 1.0f - t32;
+            float w0 = tt * tt, w1 = 2.0f * tt * t32, w2 = t32 * t32;
+            float px = (q[0] * w0 + q[2] * w1) + q[4] * w2;
+            float py = (q[1] * w0 + q[3] * w1) + q[5] * w2;
+            float dist = len2(pt.x - px, pt.y - py);
+            if (dist < best) {
+                best = dist;
+                bx = px;
+                by = py;
+                best_t = t32;
+            }
+        }
+    }
+    return CPRes{bx, by, best_t, best};
+}
+static __device__ __noinline__ CPRes closest_cubic_approx(float2 pt, const float* q) {  // curve.rs:81-119
+    float inv = 1.0f / 8.0f;
+    float prevx = q[0], prevy = q[1], prev_t = 0.0f;
+    float bx = q[0], by = q[1], best_t = 0.0f, best = len2(pt.x - q[0], pt.y - q[1]);
+    for (int i = 1; i <= 8; ++i) {
+        float t = (float)i * inv;
+        float tt = 1.0f - t;
+        float tt2 = tt * tt, t2 = t * t;
+        float a = tt2 * tt, b = 3.0f * tt2 * t, c = 3.0f * tt * t2, d = t2 * t;
+        float cxx = a * q[0] + b * q[2] + c * q[4] + d * q[6];
+        float cyy = a * q[1] + b * q[3] + c * q[5] + d * q[7];
+        CPRes r = closest_line(pt, prevx, prevy, cxx, cyy);
+        float lt = prev_t + r.t * (t - prev_t);
+        if (r.dist < best) {
+            best = r.dist;
+            bx = r.cx;
+            by = r.cy;
+            best_t = lt;
+        }
+        prevx = cxx;
+        prevy = cyy;
+        prev_t = t;
+    }
+    return CPRes{bx, by, best_t, best};
+}
+static __device__ __noinline__ CPRes closest_cubic(float2 pt, const float* q, bool approx) {  // curve.rs:124-264
+    if (approx) return closest_cubic_approx(pt, q);
+    float best_t = 0.0f, bx = q[0], by = q[1];
+    float best = len2(pt.x - q[0], pt.y - q[1]);
+    float de = len2(pt.x - q[6], pt.y - q[7]);
+    if (de < best) {
+        best = de;
+        bx = q[6];
+        by = q[7];
+        best_t = 1.0f;
+    }
+    double ax = (double)(-q[0] + 3.0f * q[2] - 3.0f * q[4] + q[6]);
+    double ay = (double)(-q[1] + 3.0f * q[3] - 3.0f * q[5] + q[7]);
+    double bxx = (double)(3.0f * q[0] - 6.0f * q[2] + 3.0f * q[4]);
+    double byy = (double)(3.0f * q[1] - 6.0f * q[3] + 3.0f * q[5]);
+    double cx = (double)(-3.0f * q[0] + 3.0f * q[2]);
+    double cy = (double)(-3.0f * q[1] + 3.0f * q[3]);
+    double dx = (double)(q[0] - pt.x);
+    double dy = (double)(q[1] - pt.y);
+    double a = 3.0 * (ax * ax + ay * ay);
+    if (fabs(a) < 1.0e-10) return CPRes{bx, by, best_t, best};
+    double b = 5.0 * (ax * bxx + ay * byy);
+    double c = 4.0 * (ax * cx + ay * cy) + 2.0 * (bxx * bxx + byy * byy);
+    double d = 3.0 * ((bxx * cx + byy * cy) + (ax * dx + ay * dy));
+    double e = (cx * cx + cy * cy) + 2.0 * (dx * bxx + dy * byy);
+    double f = dx * cx + dy * cy;
+    b = b / a;
+    c = c / a;
+    d = d / a;
+    e = e / a;
+    f = f / a;
+    double p1a = (2.0 / 5.0) * c - (4.0 / 25.0) * b * b;
+    double p1b = (3.0 / 5.0) * d - (3.0 / 25.0) * b * c;
+    double p1c = (4.0 / 5.0) * e - (2.0 / 25.0) * b * d;
+    double p1d = f - b * e / 25.0;
+    double q_root = -b / 5.0;
+    double pr[3];
+    int num_p = solve_cubic(p1a, p1b, p1c, p1d, pr);
+    double iv[4];
+    int ni = 0;
+    if (q_root >= 0.0 && q_root <= 1.0) iv[ni++] = q_root;
+    for (int i = 0; i < num_p; ++i) iv[ni++] = pr[i];
+    for (int j = 1; j < ni; ++j) {
+        int k = j;
+        while (k > 0 && iv[k - 1] > iv[k]) {
+            double tmp = iv[k - 1];
+            iv[k - 1] = iv[k];
+            iv[k] = tmp;
+            k -= 1;
+        }
+    }
+    double lower = 0.0;
+    for (int j = 0; j <= ni; ++j) {
+        if (j < ni && iv[j] < 0.0) continue;
+        double upper = (j < ni) ? fmin(iv[j], 1.0) : 1.0;
+        double lb = lower, ub = upper;
+        double lbe = ((((lb + b) * lb + c) * lb + d) * lb + e) * lb + f;
+        double ube = ((((ub + b) * ub + c) * ub + d) * ub + e) * ub + f;
+        if (lbe * ube > 0.0) {
+            lower = upper;
+            continue;
+        }
+        if (lbe > ube) {
+            double t0 = lb;
+            lb = ub;
+            ub = t0;
+        }
+        double t = 0.5 * (lb + ub);
+        for (int it = 0; it < 20; ++it) {
+            if (!(t >= lb && t <= ub)) t = 0.5 * (lb + ub);
+            double v = ((((t + b) * t + c) * t + d) * t + e) * t + f;
+            if (fabs(v) < 1.0e-5 || it == 19) break;
+            if (v > 0.0)
+                ub = t;
+            else
+                lb = t;
+            double dv = (((5.0 * t + 4.0 * b) * t + 3.0 * c) * t + 2.0 * d) * t + e;
+            t -= v / dv;
+        }
+        if (t >= 0.0 && t <= 1.0) {
+            float t32 = (float)t;
+            float tt = 1.0f - t32;
+            float w0 = tt * tt * tt, w1 = 3.0f * tt * tt * t32, w2 = 3.0f * tt * t32 * t32, w3 = t32 * t32 * t32;
+            float px = ((q[0] * w0 + q[2] * w1) + q[4] * w2) + q[6] * w3;
+            float py = ((q[1] * w0 + q[3] * w1) + q[5] * w2) + q[7] * w3;
+            float dist = len2(pt.x - px, pt.y - py);
+            if (dist < best) {
+                best = dist;
+                bx = px;
+                by = py;
+                best_t = t32;
+            }
+        }
+        if (upper >= 1.0) break;
+        lower = upper;
+    }
+    return CPRes{bx, by, best_t, best};
+}
+
+// ------------------------------------------------------------------ segments
+struct SegGeom {
+    float q[8];
+    float r[4];
+    int kind;
+};
+__device__ __forceinline__ void load_seg(const DevScene& S, int sidx, SegGeom& sg) {
+    float4 a = __ldg(&S.seg_p[2 * sidx]);
+    float4 b = __ldg(&S.seg_p[2 * sidx + 1]);
+    float4 r = __ldg(&S.seg_r[sidx]);
+    sg.q[0] = a.x; sg.q[1] = a.y; sg.q[2] = a.z; sg.q[3] = a.w;
+    sg.q[4] = b.x; sg.q[5] = b.y; sg.q[6] = b.z; sg.q[7] = b.w;
+    sg.r[0] = r.x; sg.r[1] = r.y; sg.r[2] = r.z; sg.r[3] = r.w;
+    sg.kind = __ldg(&S.seg_meta[sidx].x);
+}
+__device__ __forceinline__ CPRes seg_closest(const SegGeom& sg, float2 p, bool approx) {
+    if (sg.kind == 0) return closest_line(p, sg.q[0], sg.q[1], sg.q[2], sg.q[3]);
+    if (sg.kind == 1) return closest_quad(p, sg.q, approx);
+    return closest_cubic(p, sg.q, approx);
+}
+__device__ __forceinline__ float seg_radius(const SegGeom& s, float t) {  // closest.rs:66-79
+    if (s.kind == 0) return s.r[0] + t * (s.r[1] - s.r[0]);
+    float tt = 1.0f - t;
+    if (s.kind == 1) return tt * tt * s.r[0] + 2.0f * tt * t * s.r[1] + t * t * s.r[2];
+    return tt * tt * tt * s.r[0] + 3.0f * tt * tt * t * s.r[1] + 3.0f * tt * t * t * s.r[2] + t * t * t * s.r[3];
+}
+// winding.rs:118-192
+static __device__ __noinline__ int winding_segment(const SegGeom& s, float2 pt) {
+    const float* q = s.q;
+    if (s.kind == 0) {
+        float dy = q[3] - q[1];
+        if (fabsf(dy) <= 1.0e-8f) return 0;
+        float t = (pt.y - q[1]) / dy;
+        if (t >= 0.0f && t <= 1.0f) {
+            float tp = q[0] - pt.x + t * (q[2] - q[0]);
+            if (tp >= 0.0f) return dy > 0.0f ? 1 : -1;
+        }
+        return 0;
+    }
+    if (s.kind == 1) {
+        double a = (double)(q[1] - 2.0f * q[3] + q[5]);
+        double b = (double)(-2.0f * q[1] + 2.0f * q[3]);
+        double c = (double)(q[1] - pt.y);
+        double r[2];
+        int nr = 0;
+        if (fabs(a) < 1.0e-12) {
+            if (fabs(b) > 1.0e-12) {
+                r[0] = -c / b;
+                nr = 1;
+            }
+        } else if (solve_quadratic(a, b, c, r)) {
+            nr = 2;
+        }
+        double ax = (double)(q[0] - 2.0f * q[2] + q[4]);
+        double bx = (double)(-2.0f * q[0] + 2.0f * q[2]);
+        double cx = (double)(q[0] - pt.x);
+        int w = 0;
+        for (int i = 0; i < nr; ++i) {
+            double t = r[i];
+            if (t >= 0.0 && t <= 1.0) {
+                double tp = ax * t * t + bx * t + cx;
+                if (tp > 0.0) w += (2.0 * a * t + b) > 0.0 ? 1 : -1;
+            }
+        }
+        return w;
+    }
+    double a = (double)(-q[1] + 3.0f * q[3] - 3.0f * q[5] + q[7]);
+    double b = (double)(3.0f * q[1] - 6.0f * q[3] + 3.0f * q[5]);
+    double c = (double)(-3.0f * q[1] + 3.0f * q[3]);
+    double d = (double)(q[1] - pt.y);
+    double r[3];
+    int nr = solve_cubic(a, b, c, d, r);
+    double ax = (double)(-q[0] + 3.0f * q[2] - 3.0f * q[4] + q[6]);
+    double bx = (double)(3.0f * q[0] - 6.0f * q[2] + 3.0f * q[4]);
+    double cx = (double)(-3.0f * q[0] + 3.0f * q[2]);
+    double dx = (double)(q[0] - pt.x);
+    int w = 0;
+    for (int i = 0; i < nr; ++i) {
+        double t = r[i];
+        if (t >= 0.0 && t <= 1.0) {
+            double tp = ax * t * t * t + bx * t * t + cx * t + dx;
+            if (tp > 0.0) w += (3.0 * a * t * t + 2.0 * b * t + c) > 0.0 ? 1 : -1;
+        }
+    }
+    return w;
+}
+
+// ------------------------------------------------------------------ path queries
+// Walks the path's BVH (preorder with skip links).  Node tests are exactly the
+// crate's: ray test for winding (winding.rs:117-126), containment for strokes.
+__device__ __forceinline__ int winding_path(const DevScene& S, int path, float2 p) {
+    int4 pi = __ldg(&S.p_info[2 * path]);
+    int n = pi.z, end = pi.z + pi.w;
+    int w = 0;
+    int guard = 0;
+    while (n < end && guard++ < (1 << 20)) {
+        float4 b = __ldg(&S.pn_bounds[n]);
+        int4 m = __ldg(&S.pn_meta[n]);
+        if (p.y < b.y || p.y > b.w || p.x > b.z) {
+            n = m.x;
+            continue;
+        }
+        if (m.z > 0) {
+            for (int k = m.y; k < m.y + m.z; ++k) {
+                SegGeom sg;
+                load_seg(S, __ldg(&S.pl_segs[k]), sg);
+                w += winding_segment(sg, p);
+            }
+            n = m.x;
+        } else {
+            n = n + 1;
+        }
+    }
+    return w;
+}
+// Brute-force winding over the path's segments (winding.rs:52-70).
+__device__ __forceinline__ int winding_path_list(const DevScene& S, int path, float2 p) {
+    int4 pi = __ldg(&S.p_info[2 * path]);
+    int w = 0;
+    for (int k = 0; k < pi.y; ++k) {
+        SegGeom sg;
+        load_seg(S, pi.x + k, sg);
+        w += winding_segment(sg, p);
+    }
+    return w;
+}
+__device__ __forceinline__ bool within_path_bvh(const DevScene& S, int path, float2 p) {  // closest.rs:20-98
+    int4 pi = __ldg(&S.p_info[2 * path]);
+    bool approx = __ldg(&S.p_info[2 * path + 1].w) & PF_APPROX;
+    int n = pi.z, end = pi.z + pi.w;
+    int guard = 0;
+    while (n < end && guard++ < (1 << 20)) {
+        float4 b = __ldg(&S.pn_bounds[n]);
+        int4 m = __ldg(&S.pn_meta[n]);
+        if (!(p.x >= b.x && p.x <= b.z && p.y >= b.y && p.y <= b.w)) {
+            n = m.x;
+            continue;
+        }
+        if (m.z > 0) {
+            for (int k = m.y; k < m.y + m.z; ++k) {
+                SegGeom sg;
+                load_seg(S, __ldg(&S.pl_segs[k]), sg);
+                CPRes c = seg_closest(sg, p, approx);
+                if (c.dist < seg_radius(sg, c.t)) return true;
+            }
+            n = m.x;
+        } else {
+            n = n + 1;
+        }
+    }
+    return false;
+}
+__device__ __forceinline__ bool within_path_list(const DevScene& S, int path, float2 p) {  // closest.rs:228-377
+    int4 pi = __ldg(&S.p_info[2 * path]);
+    bool approx = __ldg(&S.p_info[2 * path + 1].w) & PF_APPROX;
+    for (int k = 0; k < pi.y; ++k) {
+        SegGeom sg;
+        load_seg(S, pi.x + k, sg);
+        CPRes c = seg_closest(sg, p, approx);
+        if (c.dist < seg_radius(sg, c.t)) return true;
+    }
+    return false;
+}
+
+// ------------------------------------------------------------------ shape queries
+static __device__ __noinline__ float2 closest_point_ellipse(float cx, float cy, float rx, float ry, float2 pt) {  // shape.rs:116-164
+    rx = fabsf(rx);
+    ry = fabsf(ry);
+    const float eps = 1.0e-6f;
+    if (rx < eps && ry < eps) return make_float2(cx, cy);
+    if (rx < eps) return make_float2(cx, cy + clampf(pt.y - cy, -ry, ry));
+    if (ry < eps) return make_float2(cx + clampf(pt.x - cx, -rx, rx), cy);
+    float dx = pt.x - cx, dy = pt.y - cy;
+    if (fabsf(dx) < eps && fabsf(dy) < eps) return make_float2(cx + rx, cy);
+    float sx = dx < 0.0f ? -1.0f : 1.0f, sy = dy < 0.0f ? -1.0f : 1.0f;
+    dx = fabsf(dx);
+    dy = fabsf(dy);
+    float t = atan2f(dy * rx, dx * ry);
+    for (int i = 0; i < 20; ++i) {
+        float s = sinf(t), c = cosf(t);
+        float g = rx * dx * s - ry * dy * c + (ry * ry - rx * rx) * s * c;
+        float gt = rx * dx * c + ry * dy * s + (ry * ry - rx * rx) * (c * c - s * s);
+        if (fabsf(gt) < 1.0e-12f) break;
+        float nx = clampf(t - g / gt, 0.0f, HALF_PI_F);
+        if (fabsf(nx - t) < 1.0e-6f) {
+            t = nx;
+            break;
+        }
+        t = nx;
+    }
+    float s = sinf(t), c = cosf(t);
+    return make_float2(cx + sx * rx * c, cy + sy * ry * s);
+}
+__device__ __forceinline__ float rect_signed_distance(float2 p, float4 r) {  // shape.rs:188-201
+    float dx = fmaxf(fmaxf(r.x - p.x, 0.0f), p.x - r.z);
+    float dy = fmaxf(fmaxf(r.y - p.y, 0.0f), p.y - r.w);
+    float outside = sqrtf(dx * dx + dy * dy);
+    float inside = fminf(fminf(fminf(p.x - r.x, r.z - p.x), p.y - r.y), r.w - p.y);
+    return outside > 0.0f ? outside : -inside;
+}
+__device__ __forceinline__ float ellipse_signed_distance(float2 p, float4 prm) {  // shape.rs:204-212
+    float rx = fmaxf(fabsf(fabsf(prm.z)), 1.0e-6f), ry = fmaxf(fabsf(fabsf(prm.w)), 1.0e-6f);
+    float lx = p.x - prm.x, ly = p.y - prm.y;
+    bool inside = (lx / rx) * (lx / rx) + (ly / ry) * (ly / ry) <= 1.0f;
+    float2 c = closest_point_ellipse(prm.x, prm.y, rx, ry, p);
+    float dist = len2(p.x - c.x, p.y - c.y);
+    return inside ? -dist : dist;
+}
+// within_distance_shape (closest.rs:206-379); lp in group space.
+__device__ __forceinline__ bool within_shape(const DevScene& S, int s, float2 lp, float r) {
+    if (r <= 0.0f) return false;
+    float2 p = shape_local_dist(S, s, lp);
+    int4 si = __ldg(&S.s_info[s]);
+    float4 prm = __ldg(&S.s_params[s]);
+    if (si.x == K_CIRCLE) {
+        float d = len2(p.x - prm.x, p.y - prm.y) - fabsf(prm.z);
+        return fabsf(d) < r;
+    }
+    if (si.x == K_ELLIPSE) return fabsf(ellipse_signed_distance(p, prm)) < r;
+    if (si.x == K_RECT) return fabsf(rect_signed_distance(p, prm)) < r;
+    if (si.z < 0) return false;
+    return within_path_list(S, si.z, p);
+}
+// winding_number_shape (winding.rs:13-48); sp in shape space.
+__device__ __forceinline__ int winding_shape(const DevScene& S, int s, float2 sp, bool use_bvh) {
+    int4 si = __ldg(&S.s_info[s]);
+    float4 prm = __ldg(&S.s_params[s]);
+    if (si.x == K_CIRCLE) {
+        float r = fabsf(prm.z);
+        float dx = sp.x - prm.x, dy = sp.y - prm.y;
+        return (dx * dx + dy * dy) < r * r ? 1 : 0;
+    }
+    if (si.x == K_ELLIPSE) {
+        float rx = fmaxf(fabsf(prm.z), 1.0e-6f), ry = fmaxf(fabsf(prm.w), 1.0e-6f);
+        float dx = (sp.x - prm.x) / rx, dy = (sp.y - prm.y) / ry;
+        return dx * dx + dy * dy < 1.0f ? 1 : 0;
+    }
+    if (si.x == K_RECT) return (sp.x > prm.x && sp.x < prm.z && sp.y > prm.y && sp.y < prm.w) ? 1 : 0;
+    if (si.z < 0) return 0;
+    int4 pi = __ldg(&S.p_info[2 * si.z]);
+    if (use_bvh && pi.w > 0) return winding_path(S, si.z, sp);
+    return winding_path_list(S, si.z, sp);
+}
+__device__ __forceinline__ bool fill_hit(int rule, int w) { return rule == 1 ? ((w < 0 ? -w : w) % 2) == 1 : w != 0; }
+
+// ------------------------------------------------------------------ group queries (distance/api.rs)
+// within_distance_bvh (api.rs:79-135) with the brute-force fallback (api.rs:15-33).
+__device__ __forceinline__ bool group_within(const DevScene& S, int g, float2 lp) {
+    int4 gb = __ldg(&S.g_bvh[g]);
+    if (gb.y == 0) {
+        for (int k = 0; k < gb.w; ++k) {
+            int s = __ldg(&S.g_shape_list[gb.z + k]);
+            float sw = __ldg(&S.s_stroke[s]);
+            if (sw <= 0.0f) continue;
+            if (within_shape(S, s, lp, sw)) return true;
+        }
+        return false;
+    }
+    int n = gb.x, end = gb.x + gb.y;
+    int guard = 0;
+    while (n < end && guard++ < (1 << 20)) {
+        float4 b = __ldg(&S.gn_bounds[n]);
+        int4 m = __ldg(&S.gn_meta[n]);
+        if (!(lp.x >= b.x && lp.x <= b.z && lp.y >= b.y && lp.y <= b.w)) {
+            n = m.x;
+            continue;
+        }
+        if (m.z > 0) {
+            for (int k = m.y; k < m.y + m.z; ++k) {
+                int s = __ldg(&S.gl_shapes[k]);
+                float sw = __ldg(&S.s_stroke[s]);
+                if (sw <= 0.0f) continue;
+                int4 si = __ldg(&S.s_info[s]);
+                if (si.x == K_PATH && si.z >= 0 && __ldg(&S.p_info[2 * si.z].w) > 0) {
+                    if (within_path_bvh(S, si.z, shape_local_dist(S, s, lp))) return true;
+                } else if (within_shape(S, s, lp, sw)) {
+                    return true;
+                }
+            }
+            n = m.x;
+        } else {
+            n = n + 1;
+        }
+    }
+    return false;
+}
+// is_inside_bvh (api.rs:259-309) with the brute-force fallback (api.rs:239-256).
+__device__ __forceinline__ bool group_inside(const DevScene& S, int g, float2 lp, int rule) {
+    int4 gb = __ldg(&S.g_bvh[g]);
+    int w = 0;
+    if (gb.y == 0) {
+        for (int k = 0; k < gb.w; ++k) {
+            int s = __ldg(&S.g_shape_list[gb.z + k]);
+            w += winding_shape(S, s, shape_local_dist(S, s, lp), false);
+        }
+        return fill_hit(rule, w);
+    }
+    {
+        float4 b = __ldg(&S.gn_bounds[gb.x]);
+        if (!(lp.x >= b.x && lp.x <= b.z && lp.y >= b.y && lp.y <= b.w)) return false;
+    }
+    int n = gb.x, end = gb.x + gb.y;
+    int guard = 0;
+    while (n < end && guard++ < (1 << 20)) {
+        float4 b = __ldg(&S.gn_bounds[n]);
+        int4 m = __ldg(&S.gn_meta[n]);
+        if (!(lp.x >= b.x && lp.x <= b.z && lp.y >= b.y && lp.y <= b.w)) {
+            n = m.x;
+            continue;
+        }
+        if (m.z > 0) {
+            for (int k = m.y; k < m.y + m.z; ++k) {
+                int s = __ldg(&S.gl_shapes[k]);
+                w += winding_shape(S, s, shape_local_dist(S, s, lp), true);
+            }
+            n = m.x;
+        } else {
+            n = n + 1;
+        }
+    }
+    return fill_hit(rule, w);
+}
+
+// ------------------------------------------------------------------ paints (backward/paint.rs:8-74)
+__device__ __forceinline__ float4 stops_color(const DevScene& S, int so, int sc, float t) {
+    if (sc <= 0) return make_float4(0, 0, 0, 0);
+    if (t < __ldg(&S.stop_offsets[so])) return __ldg(&S.stop_colors[so]);
+    for (int i = 0; i + 1 < sc; ++i) {
+        float o0 = __ldg(&S.stop_offsets[so + i]), o1 = __ldg(&S.stop_offsets[so + i + 1]);
+        if (t >= o0 && t < o1) {
+            float tt = (t - o0) / (o1 - o0);
+            float4 c0 = __ldg(&S.stop_colors[so + i]), c1 = __ldg(&S.stop_colors[so + i + 1]);
+            return make_float4(c0.x * (1.0f - tt) + c1.x * tt, c0.y * (1.0f - tt) + c1.y * tt,
+                               c0.z * (1.0f - tt) + c1.z * tt, c0.w * (1.0f - tt) + c1.w * tt);
+        }
+    }
+    return __ldg(&S.stop_colors[so + sc - 1]);
+}
+__device__ __forceinline__ float paint_t(const DevScene& S, int kind, float4 pp, float2 pt) {
+    if (kind == P_LINEAR) {
+        float ex = pp.z - pp.x, ey = pp.w - pp.y;
+        float denom = fmaxf(ex * ex + ey * ey, 1.0e-3f);
+        return ((pt.x - pp.x) * ex + (pt.y - pp.y) * ey) / denom;
+    }
+    float nx = (pt.x - pp.x) / pp.z, ny = (pt.y - pp.y) / pp.w;
+    return len2(nx, ny);
+}
+__device__ __forceinline__ float4 paint_color(const DevScene& S, int p, float2 pt) {
+    int4 pi = __ldg(&S.paint_info[p]);
+    float4 pp = __ldg(&S.paint_params[p]);
+    if (pi.x == P_SOLID) return pp;
+    if (pi.x == P_LINEAR || pi.x == P_RADIAL) return stops_color(S, pi.y, pi.z, paint_t(S, pi.x, pp, pt));
+    return make_float4(0, 0, 0, 0);
+}
+
+// ------------------------------------------------------------------ filters (backward/filters.rs:159-239)
+__device__ __forceinline__ float filter_weight(int ft, float radius, float dx, float dy) {
+    if (radius <= 0.0f) return 1.0f;
+    if (fabsf(dx) > radius || fabsf(dy) > radius) return 0.0f;
+    if (ft == F_BOX) return 1.0f / ((2.0f * radius) * (2.0f * radius));
+    if (ft == F_TENT) {
+        float fx = radius - fabsf(dx), fy = radius - fabsf(dy);
+        float norm = 1.0f / (radius * radius);
+        return fx * fy * norm * norm;
+    }
+    if (ft == F_PARABOLIC) {
+        float rx = 1.0f - (dx / radius) * (dx / radius), ry = 1.0f - (dy / radius) * (dy / radius);
+        return (4.0f / 3.0f) * rx * (4.0f / 3.0f) * ry;
+    }
+    if (ft == F_HANN) {
+        float ndx = (dx / (2.0f * radius)) + 0.5f, ndy = (dy / (2.0f * radius)) + 0.5f;
+        float fx = 0.5f * (1.0f - cosf(2.0f * PI_F * ndx)), fy = 0.5f * (1.0f - cosf(2.0f * PI_F * ndy));
+        return fx * fy * (1.0f / (radius * radius));
+    }
+    if (ft == F_GAUSSIAN) {  // this library's Gaussian (sigma = radius/2, square support)
+        float r2 = radius * radius;
+        float q = dx * dx + dy * dy;
+        return (2.0f / (PI_F * r2)) * expf(-2.0f * q / r2);
+    }
+    return 1.0f;
+}
+__device__ __forceinline__ float d_filter_weight(int ft, float radius, float dx, float dy, float d_return) {
+    if (ft == F_BOX) {
+        float denom = 2.0f * radius;
+        return denom != 0.0f ? d_return * (-2.0f) * denom / ((denom * denom) * denom) : 0.0f;
+    }
+    if (ft == F_TENT) {
+        float fx = radius - fabsf(dx), fy = radius - fabsf(dy);
+        float norm = 1.0f / (radius * radius);
+        float d_fx = d_return * fy * norm, d_fy = d_return * fx * norm, d_norm = d_return * fx * fy;
+        float r2 = radius * radius;
+        return radius != 0.0f ? d_fx + d_fy + (-4.0f) * d_norm / ((r2 * r2) * radius) : 0.0f;
+    }
+    if (ft == F_PARABOLIC) {
+        float r3 = radius * radius * radius;
+        return r3 != 0.0f ? -(2.0f * dx * dx + 2.0f * dy * dy) / r3 : 0.0f;
+    }
+    if (ft == F_HANN) {
+        float ndx = (dx / (2.0f * radius)) + 0.5f, ndy = (dy / (2.0f * radius)) + 0.5f;
+        float fx = 0.5f * (1.0f - cosf(2.0f * PI_F * ndx)), fy = 0.5f * (1.0f - cosf(2.0f * PI_F * ndy));
+        float norm = 1.0f / (radius * radius);
+        float d_fx = d_return * fy * norm, d_fy = d_return * fx * norm, d_norm = d_return * fx * fy;
+        float d_ndx = d_fx * 0.5f * sinf(2.0f * PI_F * ndx) * (2.0f * PI_F);
+        float d_ndy = d_fy * 0.5f * sinf(2.0f * PI_F * ndy) * (2.0f * PI_F);
+        float tr = 2.0f * radius;
+        return d_ndx * (-2.0f * dx / (tr * tr)) + d_ndy * (-2.0f * dy / (tr * tr)) +
+               (-2.0f) * d_norm / ((radius * radius) * radius);
+    }
+    if (ft == F_GAUSSIAN) {
+        float r2 = radius * radius;
+        float q = dx * dx + dy * dy;
+        float w = (2.0f / (PI_F * r2)) * expf(-2.0f * q / r2);
+        return radius != 0.0f ? d_return * w * (4.0f * q / (r2 * radius) - 2.0f / radius) : 0.0f;
+    }
+    return 0.0f;
+}
+
+// ------------------------------------------------------------------ random numbers
+// PCG32 exactly as src/renderer/rng.rs:16-43 (native 64-bit arithmetic).
+struct Pcg32 {
+    uint64_t state, inc;
+    __device__ Pcg32(uint64_t idx, uint64_t seed) {
+        state = 0;
+        inc = ((idx + 1) << 1) | 1;
+        next();
+        state += 0x853c49e6748fea9bULL + seed;
+        next();
+    }
+    __device__ __forceinline__ uint32_t next() {
+        uint64_t old = state;
+        state = old * 6364136223846793005ULL + (inc | 1);
+        uint32_t xs = (uint32_t)(((old >> 18) ^ old) >> 27);
+        uint32_t rot = (uint32_t)(old >> 59);
+        return __funnelshift_r(xs, xs, rot);
+    }
+    __device__ __forceinline__ float next_f32() {
+        uint32_t u = next();
+        return __uint_as_float((u >> 9) | 0x3f800000u) - 1.0f;
+    }
+};
+// Philox4x32-10 (Salmon et al., SC'11); counter (idx_lo, idx_hi, 0, 0), key (seed, 0).
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += 0x9E3779B9u;
+        k.y += 0xBB67AE85u;
+    }
+    return c;
+}
+__device__ __forceinline__ float unit_from_u32(uint32_t u) { return (float)(u >> 9) * (1.0f / 8388608.0f); }
+
+// Sample position (src/backward/render.rs:95-111; idx = ((y*W+x)*sy_n+sy)*sx_n+sx).
+__device__ __forceinline__ float2 sample_pos(int x, int y, int sx, int sy, int sxn, int syn, int W, uint32_t seed,
+                                             bool jitter) {
+    float rx = 0.5f, ry = 0.5f;
+    if (jitter) {
+        uint64_t idx = (((uint64_t)y * W + x) * syn + sy) * sxn + sx;
+        Pcg32 rng(idx, (uint64_t)seed);
+        rx = rng.next_f32();
+        ry = rng.next_f32();
+    }
+    return make_float2((float)x + ((float)sx + rx) / (float)sxn, (float)y + ((float)sy + ry) / (float)syn);
+}
+
+__device__ __forceinline__ float4 background_premul(const DevScene& S, int pixel) {  // background.rs:7-26
+    if (S.bg_image) {
+        const float* b = S.bg_image + 4 * (size_t)pixel;
+        return make_float4(b[0] * b[3], b[1] * b[3], b[2] * b[3], b[3]);
+    }
+    return make_float4(S.bg[0] * S.bg[3], S.bg[1] * S.bg[3], S.bg[2] * S.bg[3], S.bg[3]);
+}
+
+// Tile lookup for an arbitrary canvas point (edge tiles extend to infinity in binning).
+__device__ __forceinline__ int tile_of(const DevScene& S, float2 p) {
+    int tx = f2i(floorf(p.x / (float)TILE)), ty = f2i(floorf(p.y / (float)TILE));
+    tx = tx < 0 ? 0 : (tx >= S.tiles_x ? S.tiles_x - 1 : tx);
+    ty = ty < 0 ? 0 : (ty >= S.tiles_y ? S.tiles_y - 1 : ty);
+    return ty * S.tiles_x + tx;
+}
+
+// Premultiplied over (src/backward/sampling.rs:153-154 / forward.rs:370-377).
+__device__ __forceinline__ void over(float4& acc, float4 c) {
+    float a = c.w, inv = 1.0f - a;
+    acc.x = acc.x * inv + c.x * a;
+    acc.y = acc.y * inv + c.y * a;
+    acc.z = acc.z * inv + c.z * a;
+    acc.w = acc.w * inv + a;
+}
+
+}  // namespace dvgb

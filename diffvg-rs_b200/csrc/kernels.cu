@@ -1,0 +1,1209 @@
+// kernels.cu — sm_100a kernels of the render / backward hot path.
+//
+//   k_bin_count / k_bin_scan / k_bin_write  tile binning of groups (group order kept)
+//   k_forward      per (tile, sub-sample) CTA: scene evaluation + filtered splat
+//                  into a shared-memory tile+halo accumulator, flushed once
+//   k_weights      filter-weight image only (backward without a preceding forward)
+//   k_resolve      Σ(c·w)/Σw and un-premultiply            (forward.rs:294-334)
+//   k_interior     interior adjoint per sample             (backward/render.rs:95-169)
+//   k_boundary     edge sampling adjoint per boundary sample (backward/boundary.rs:141-196)
+//   k_l2           L2 loss and d_render
+//
+// Built with -fmad=false (see device.cuh).
+#include "device.cuh"
+#include "kernels.cuh"
+
+namespace dvgb {
+
+// ------------------------------------------------------------------ tile binning
+// One CTA per tile scans all group boxes; the crate bins on the GPU and sorts on
+// the host (src/renderer/renderer.rs:254-384); scanning in group order keeps the
+// compositing order without a sort.  Edge tiles extend to infinity so that any
+// point clamped to an edge tile is covered.
+__device__ __forceinline__ bool tile_hits(const DevScene& S, int tile, float4 b) {
+    int tx = tile % S.tiles_x, ty = tile / S.tiles_x;
+    float x0 = tx == 0 ? -INFINITY : (float)(tx * TILE);
+    float y0 = ty == 0 ? -INFINITY : (float)(ty * TILE);
+    float x1 = tx == S.tiles_x - 1 ? INFINITY : (float)((tx + 1) * TILE);
+    float y1 = ty == S.tiles_y - 1 ? INFINITY : (float)((ty + 1) * TILE);
+    return !(b.z < x0 || b.x > x1 || b.w < y0 || b.y > y1);
+}
+__global__ void __launch_bounds__(256) k_bin_count(DevScene S, const float4* g_bbox, int* counts) {
+    int tile = blockIdx.x;
+    int total = 0;
+    for (int base = 0; base < S.num_groups; base += blockDim.x) {
+        int g = base + threadIdx.x;
+        bool hit = false;
+        if (g < S.num_groups) {
+            int4 gi = S.g_info[g];
+            hit = (gi.x >= 0 || gi.y >= 0) && tile_hits(S, tile, g_bbox[g]);
+        }
+        total += __syncthreads_count(hit);
+    }
+    if (threadIdx.x == 0) counts[tile] = total;
+}
+// Exclusive scan of tile counts (single CTA of 1024 threads, any length).
+__global__ void __launch_bounds__(1024) k_bin_scan(const int* counts, int n, int* offsets) {
+    __shared__ int warp_sums[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int base = 0; base < n; base += 1024) {
+        int i = base + threadIdx.x;
+        int v = i < n ? counts[i] : 0;
+        int x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_sums[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            int w = warp_sums[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                int y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            warp_sums[lane] = w;
+        }
+        __syncthreads();
+        int excl = carry + (wid > 0 ? warp_sums[wid - 1] : 0) + x - v;
+        if (i < n) offsets[i] = excl;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = excl + v;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) offsets[n] = carry;
+}
+__global__ void __launch_bounds__(256) k_bin_write(DevScene S, const float4* g_bbox, const int* offsets,
+                                                   int* entries) {
+    __shared__ int warp_counts[8];
+    int tile = blockIdx.x;
+    int cursor = offsets[tile];
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int base = 0; base < S.num_groups; base += blockDim.x) {
+        int g = base + threadIdx.x;
+        bool hit = false;
+        if (g < S.num_groups) {
+            int4 gi = S.g_info[g];
+            hit = (gi.x >= 0 || gi.y >= 0) && tile_hits(S, tile, g_bbox[g]);
+        }
+        unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (lane == 0) warp_counts[wid] = __popc(m);
+        __syncthreads();
+        int before = 0, total = 0;
+        for (int w = 0; w < 8; ++w) {
+            if (w < wid) before += warp_counts[w];
+            total += warp_counts[w];
+        }
+        if (hit) entries[cursor + before + __popc(m & ((1u << lane) - 1u))] = g;
+        cursor += total;
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------ forward
+// One CTA = one 16x16 tile at one sub-sample (sx, sy); thread = pixel.  Every
+// thread of the CTA walks the same group list, so group data loads are uniform.
+__global__ void __launch_bounds__(256) k_forward(DevScene S, SampleParams sp, float* accum, float* wsum,
+                                                 unsigned* status) {
+    extern __shared__ float sm[];
+    const int ri = S.filter_ri;
+    const int HW = TILE + 2 * ri;
+    const bool use_sm = ri <= MAX_SMEM_RI;
+    const int tile = blockIdx.x;
+    const int sub = blockIdx.y;
+    const int tx = tile % S.tiles_x, ty = tile / S.tiles_x;
+    const int x = tx * TILE + (threadIdx.x % TILE), y = ty * TILE + (threadIdx.x / TILE);
+    if (use_sm)
+        for (int i = threadIdx.x; i < HW * HW * 5; i += blockDim.x) sm[i] = 0.0f;
+    __syncthreads();
+    const int off = S.tile_offsets[tile];
+    const int n = S.tile_offsets[tile + 1] - off;
+    const int* list = S.tile_entries + off;
+    if (x < S.width && y < S.height) {
+        const int sx = sub % sp.sxn, sy = sub / sp.sxn;
+        const float2 pt = sample_pos(x, y, sx, sy, sp.sxn, sp.syn, S.width, sp.seed, sp.jitter);
+        float4 acc = background_premul(S, y * S.width + x);
+        for (int e = 0; e < n; ++e) {
+            const int g = __ldg(&list[e]);
+            const int4 gi = __ldg(&S.g_info[g]);
+            const float2 lp = xf9(S.g_c2s + 9 * g, pt);
+            if (gi.y >= 0 && group_within(S, g, lp)) over(acc, paint_color(S, gi.y, pt));
+            if (gi.x >= 0 && group_inside(S, g, lp, gi.z)) over(acc, paint_color(S, gi.x, pt));
+        }
+        for (int dy = -ri; dy <= ri; ++dy)
+            for (int dx = -ri; dx <= ri; ++dx) {
+                int xx = x + dx, yy = y + dy;
+                if (xx < 0 || yy < 0 || xx >= S.width || yy >= S.height) continue;
+                float w = filter_weight(S.filter_type, S.filter_radius, (float)xx + 0.5f - pt.x,
+                                        (float)yy + 0.5f - pt.y);
+                if (!(w > 0.0f)) continue;
+                if (use_sm) {
+                    int li = (yy - (ty * TILE - ri)) * HW + (xx - (tx * TILE - ri));
+                    float* c = sm + 5 * li;
+                    atomicAdd(c + 0, acc.x * w);
+                    atomicAdd(c + 1, acc.y * w);
+                    atomicAdd(c + 2, acc.z * w);
+                    atomicAdd(c + 3, acc.w * w);
+                    atomicAdd(c + 4, w);
+                } else {
+                    size_t p = (size_t)yy * S.width + xx;
+                    atomicAdd(accum + 4 * p + 0, acc.x * w);
+                    atomicAdd(accum + 4 * p + 1, acc.y * w);
+                    atomicAdd(accum + 4 * p + 2, acc.z * w);
+                    atomicAdd(accum + 4 * p + 3, acc.w * w);
+                    atomicAdd(wsum + p, w);
+                }
+            }
+    }
+    if (!use_sm) return;
+    __syncthreads();
+    for (int i = threadIdx.x; i < HW * HW; i += blockDim.x) {
+        const float* c = sm + 5 * i;
+        if (c[4] == 0.0f) continue;
+        int xx = tx * TILE - ri + i % HW, yy = ty * TILE - ri + i / HW;
+        if (xx < 0 || yy < 0 || xx >= S.width || yy >= S.height) continue;
+        size_t p = (size_t)yy * S.width + xx;
+        atomicAdd(accum + 4 * p + 0, c[0]);
+        atomicAdd(accum + 4 * p + 1, c[1]);
+        atomicAdd(accum + 4 * p + 2, c[2]);
+        atomicAdd(accum + 4 * p + 3, c[3]);
+        atomicAdd(wsum + p, c[4]);
+    }
+}
+
+// Weight image only (rasterize_weights_f32, forward.rs:1505-1564).
+__global__ void __launch_bounds__(256) k_weights(DevScene S, SampleParams sp, float* wsum) {
+    const int tile = blockIdx.x, sub = blockIdx.y;
+    const int tx = tile % S.tiles_x, ty = tile / S.tiles_x;
+    const int x = tx * TILE + (threadIdx.x % TILE), y = ty * TILE + (threadIdx.x / TILE);
+    if (x >= S.width || y >= S.height) return;
+    const int ri = S.filter_ri;
+    const int sx = sub % sp.sxn, sy = sub / sp.sxn;
+    const float2 pt = sample_pos(x, y, sx, sy, sp.sxn, sp.syn, S.width, sp.seed, sp.jitter);
+    for (int dy = -ri; dy <= ri; ++dy)
+        for (int dx = -ri; dx <= ri; ++dx) {
+            int xx = x + dx, yy = y + dy;
+            if (xx < 0 || yy < 0 || xx >= S.width || yy >= S.height) continue;
+            float w = filter_weight(S.filter_type, S.filter_radius, (float)xx + 0.5f - pt.x, (float)yy + 0.5f - pt.y);
+            if (w > 0.0f) atomicAdd(wsum + (size_t)yy * S.width + xx, w);
+        }
+}
+
+__global__ void k_resolve(DevScene S, const float* accum, const float* wsum, float* out) {
+    size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= (size_t)S.width * S.height) return;
+    float r = S.bg[0], g = S.bg[1], b = S.bg[2], a = S.bg[3];
+    float w = wsum[p];
+    if (w > 0.0f) {
+        float4 c = reinterpret_cast<const float4*>(accum)[p];
+        r = c.x / w;
+        g = c.y / w;
+        b = c.z / w;
+        a = c.w / w;
+    }
+    if (a > 1.0e-8f) {
+        r = r / a;
+        g = g / a;
+        b = b / a;
+    }
+    reinterpret_cast<float4*>(out)[p] = make_float4(r, g, b, a);
+}
+
+// ------------------------------------------------------------------ backward helpers
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ void add_if(float* p, float v) {
+    if (v != 0.0f) atomicAdd(p, v);
+}
+
+// d_sample_paint for gradient paints (backward/paint.rs:91-277), per-lane atomics.
+__device__ void d_gradient_paint(const DevScene& S, const GradPtrs& G, int p, float2 pt, float4 dc, float2* dtr) {
+    int4 pi = __ldg(&S.paint_info[p]);
+    float4 pp = __ldg(&S.paint_params[p]);
+    int so = pi.y, sc = pi.z;
+    if (sc <= 0) return;
+    float t, denom = 0.0f, offx = 0.0f, offy = 0.0f, nx = 0.0f, ny = 0.0f;
+    if (pi.x == P_LINEAR) {
+        float ex = pp.z - pp.x, ey = pp.w - pp.y;
+        denom = fmaxf(ex * ex + ey * ey, 1.0e-3f);
+        t = ((pt.x - pp.x) * ex + (pt.y - pp.y) * ey) / denom;
+    } else {
+        offx = pt.x - pp.x;
+        offy = pt.y - pp.y;
+        nx = offx / pp.z;
+        ny = offy / pp.w;
+        t = len2(nx, ny);
+    }
+    if (t < __ldg(&S.stop_offsets[so])) {
+        float* c = G.d_stop_colors + 4 * so;
+        add_if(c + 0, dc.x);
+        add_if(c + 1, dc.y);
+        add_if(c + 2, dc.z);
+        add_if(c + 3, dc.w);
+        return;
+    }
+    for (int i = 0; i + 1 < sc; ++i) {
+        float o0 = __ldg(&S.stop_offsets[so + i]), o1 = __ldg(&S.stop_offsets[so + i + 1]);
+        if (t >= o0 && t < o1) {
+            float tt = (t - o0) / (o1 - o0);
+            float4 c0 = __ldg(&S.stop_colors[so + i]), c1 = __ldg(&S.stop_colors[so + i + 1]);
+            float* a0 = G.d_stop_colors + 4 * (so + i);
+            float* a1 = a0 + 4;
+            add_if(a0 + 0, dc.x * (1.0f - tt));
+            add_if(a0 + 1, dc.y * (1.0f - tt));
+            add_if(a0 + 2, dc.z * (1.0f - tt));
+            add_if(a0 + 3, dc.w * (1.0f - tt));
+            add_if(a1 + 0, dc.x * tt);
+            add_if(a1 + 1, dc.y * tt);
+            add_if(a1 + 2, dc.z * tt);
+            add_if(a1 + 3, dc.w * tt);
+            float d_tt = dc.x * (c1.x - c0.x) + dc.y * (c1.y - c0.y) + dc.z * (c1.z - c0.z) + dc.w * (c1.w - c0.w);
+            float dof = o1 - o0;
+            if (fabsf(dof) > 0.0f) {
+                add_if(G.d_stop_offsets + so + i, d_tt * (tt - 1.0f) / dof);
+                add_if(G.d_stop_offsets + so + i + 1, -d_tt * tt / dof);
+            }
+            float d_t = d_tt / dof;
+            float* dpp = G.d_paint_params + 4 * p;
+            if (pi.x == P_LINEAR) {
+                float bx = d_t * (-(pt.x - pp.x) - (pp.z - pp.x)) / denom;
+                float by = d_t * (-(pt.y - pp.y) - (pp.w - pp.y)) / denom;
+                float ex = d_t * (pt.x - pp.x) / denom;
+                float ey = d_t * (pt.y - pp.y) / denom;
+                float d_l = -d_t * t / denom;
+                float lx = pp.z - pp.x, ly = pp.w - pp.y;
+                if (lx * lx + ly * ly > 1.0e-3f) {
+                    float ax = pp.x - pp.z, ay = pp.y - pp.w;
+                    add_if(dpp + 0, bx + 2.0f * d_l * ax);
+                    add_if(dpp + 1, by + 2.0f * d_l * ay);
+                    add_if(dpp + 2, ex + 2.0f * d_l * lx);
+                    add_if(dpp + 3, ey + 2.0f * d_l * ly);
+                } else {
+                    add_if(dpp + 0, bx);
+                    add_if(dpp + 1, by);
+                    add_if(dpp + 2, ex);
+                    add_if(dpp + 3, ey);
+                }
+                dtr->x += bx + ex;
+                dtr->y += by + ey;
+            } else {
+                // d_length(normalized, d_t) (backward/math.rs:33-41)
+                float l = sqrtf(nx * nx + ny * ny);
+                float dnx = 0.0f, dny = 0.0f;
+                if (l != 0.0f) {
+                    float dls = 0.5f * d_t / l;
+                    dnx = nx * (2.0f * dls);
+                    dny = ny * (2.0f * dls);
+                }
+                float dox = dnx / pp.z, doy = dny / pp.w;
+                float drx = -dnx * offx / (pp.z * pp.z), dry = -dny * offy / (pp.w * pp.w);
+                add_if(dpp + 0, -dox);
+                add_if(dpp + 1, -doy);
+                add_if(dpp + 2, drx);
+                add_if(dpp + 3, dry);
+                dtr->x += -dox;
+                dtr->y += -doy;
+            }
+            return;
+        }
+    }
+    float* c = G.d_stop_colors + 4 * (so + sc - 1);
+    add_if(c + 0, dc.x);
+    add_if(c + 1, dc.y);
+    add_if(c + 2, dc.z);
+    add_if(c + 3, dc.w);
+}
+
+// ------------------------------------------------------------------ interior backward
+// Per sample: gather d_color (filters.rs:70-103), recompute the fragments of
+// sample_color (sampling.rs:76-224) and back-propagate through compositing,
+// paints, background and the filter (filters.rs:106-156).  The fragment list is
+// rebuilt from the BVH; only (fragment code, transmittance) pairs live in
+// per-thread local memory, never in HBM.  The adjoint loop walks the tile's
+// group list in the same order on every lane so solid-paint gradients reduce
+// across the warp before one atomic.
+__global__ void __launch_bounds__(256) k_interior(DevScene S, SampleParams sp, const float* d_render,
+                                                  const float* wsum, GradPtrs G, unsigned* status) {
+    __shared__ float red[8][6];
+    const int tile = blockIdx.x, sub = blockIdx.y;
+    const int tx = tile % S.tiles_x, ty = tile / S.tiles_x;
+    const int x = tx * TILE + (threadIdx.x % TILE), y = ty * TILE + (threadIdx.x / TILE);
+    const bool valid = x < S.width && y < S.height;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int off = S.tile_offsets[tile];
+    const int n = S.tile_offsets[tile + 1] - off;
+    const int* list = S.tile_entries + off;
+    const int W = S.width, H = S.height;
+
+    float2 ps = make_float2(0.0f, 0.0f), pt = make_float2(0.0f, 0.0f);
+    int pixel = 0;
+    float4 dcol = make_float4(0, 0, 0, 0), bg = make_float4(0, 0, 0, 0);
+    if (valid) {
+        const int sx = sub % sp.sxn, sy = sub / sp.sxn;
+        ps = sample_pos(x, y, sx, sy, sp.sxn, sp.syn, W, sp.seed, sp.jitter);
+        float2 npt = make_float2(ps.x / (float)W, ps.y / (float)H);  // render.rs:111
+        pt = make_float2(npt.x * (float)W, npt.y * (float)H);       // sampling.rs:91
+        pixel = y * W + x;
+        bg = background_premul(S, pixel);
+        // gather_d_color (filters.rs:70-103)
+        const int px = f2i(floorf(ps.x)), py = f2i(floorf(ps.y)), ri = S.filter_ri;
+        for (int dy = -ri; dy <= ri; ++dy)
+            for (int dx = -ri; dx <= ri; ++dx) {
+                int xx = px + dx, yy = py + dy;
+                if (xx < 0 || yy < 0 || xx >= W || yy >= H) continue;
+                float w = filter_weight(S.filter_type, S.filter_radius, (float)xx + 0.5f - ps.x,
+                                        (float)yy + 0.5f - ps.y);
+                size_t q = (size_t)yy * W + xx;
+                float ws = wsum[q];
+                if (ws > 0.0f) {
+                    float4 d = reinterpret_cast<const float4*>(d_render)[q];
+                    float k = w / ws;
+                    dcol.x += k * d.x;
+                    dcol.y += k * d.y;
+                    dcol.z += k * d.z;
+                    dcol.w += k * d.w;
+                }
+            }
+    }
+    // Pass 1: fragments in order (stroke before fill within a group).
+    int code[MAX_FRAGMENTS];
+    float tr[MAX_FRAGMENTS];
+    int nf = 0;
+    bool overflow = false;
+    float4 acc = bg;
+    if (valid) {
+        for (int e = 0; e < n; ++e) {
+            const int g = __ldg(&list[e]);
+            const int4 gi = __ldg(&S.g_info[g]);
+            const float2 lp = xf9(S.g_c2s + 9 * g, pt);
+            if (gi.y >= 0 && group_within(S, g, lp)) {
+                float4 c = paint_color(S, gi.y, pt);
+                over(acc, c);
+                if (nf < MAX_FRAGMENTS) {
+                    code[nf] = 2 * e;
+                    tr[nf] = c.w;
+                } else {
+                    overflow = true;
+                }
+                ++nf;
+            }
+            if (gi.x >= 0 && group_inside(S, g, lp, gi.z)) {
+                float4 c = paint_color(S, gi.x, pt);
+                over(acc, c);
+                if (nf < MAX_FRAGMENTS) {
+                    code[nf] = 2 * e + 1;
+                    tr[nf] = c.w;
+                } else {
+                    overflow = true;
+                }
+                ++nf;
+            }
+        }
+    }
+    if (overflow) {
+        atomicOr(status, ST_FRAGMENT_OVERFLOW);
+        nf = 0;
+    }
+    const bool active = valid && !overflow;
+    // Final colour and the adjoint at the end of compositing (sampling.rs:161-174).
+    float4 ret = bg;
+    float dcr = dcol.x, dcg = dcol.y, dcb = dcol.z, dca = dcol.w;
+    if (nf > 0) {
+        float fa = acc.w, fr = acc.x, fg = acc.y, fb = acc.z;
+        if (fa > 1.0e-6f) {
+            float s = 1.0f / fa;
+            fr = fr * s;
+            fg = fg * s;
+            fb = fb * s;
+            float dfr = dcr, dfg = dcg, dfb = dcb;
+            dcr = dcr * s;
+            dcg = dcg * s;
+            dcb = dcb * s;
+            dca -= (dfr * fr + dfg * fg + dfb * fb) / fa;
+        }
+        ret = make_float4(fr, fg, fb, fa);
+        // Pass 2: transmittance after each fragment, T_i = prod_{j>i}(1 - a_j).
+        float run = 1.0f;
+        for (int i = nf - 1; i >= 0; --i) {
+            float a = tr[i];
+            tr[i] = run;
+            run = run * (1.0f - a);
+        }
+        // background adjoint after all fragments
+        float4 dbg = make_float4(dcr * run, dcg * run, dcb * run, dca * run);
+        if (S.bg_image) {
+            float* b = G.d_background_image;
+            if (b) {
+                add_if(b + 4 * (size_t)pixel + 0, dbg.x);
+                add_if(b + 4 * (size_t)pixel + 1, dbg.y);
+                add_if(b + 4 * (size_t)pixel + 2, dbg.z);
+                add_if(b + 4 * (size_t)pixel + 3, dbg.w);
+            }
+            dbg = make_float4(0, 0, 0, 0);
+        }
+        dcol = dbg;  // reused below as this sample's constant-background adjoint
+    } else if (active) {
+        // no fragment: accumulate_background_grad(d_color) (sampling.rs:121-127)
+        if (S.bg_image) {
+            float* b = G.d_background_image;
+            if (b) {
+                add_if(b + 4 * (size_t)pixel + 0, dcol.x);
+                add_if(b + 4 * (size_t)pixel + 1, dcol.y);
+                add_if(b + 4 * (size_t)pixel + 2, dcol.z);
+                add_if(b + 4 * (size_t)pixel + 3, dcol.w);
+            }
+            dcol = make_float4(0, 0, 0, 0);
+        }
+    }
+    if (!active) dcol = make_float4(0, 0, 0, 0);
+
+    // Pass 3: forward over the group list with the compositing adjoint (sampling.rs:175-210).
+    int cur = 0;
+    float4 prev = bg;
+    for (int e = 0; e < n; ++e) {
+        const int g = __ldg(&list[e]);
+        const int4 gi = __ldg(&S.g_info[g]);
+#pragma unroll
+        for (int which = 0; which < 2; ++which) {
+            const int p = which == 0 ? gi.y : gi.x;
+            if (p < 0) continue;
+            const bool has = cur < nf && code[cur] == 2 * e + which;
+            if (!__any_sync(0xffffffffu, has)) continue;
+            float4 dv = make_float4(0, 0, 0, 0);
+            float4 c = make_float4(0, 0, 0, 0);
+            if (has) {
+                c = paint_color(S, p, pt);
+                float T = tr[cur];
+                float r_ = dcr * T, g_ = dcg * T, b_ = dcb * T, a_ = dca * T;
+                float d_alpha = a_ * (1.0f - prev.w);
+                d_alpha += r_ * (c.x - prev.x) + g_ * (c.y - prev.y) + b_ * (c.z - prev.z);
+                dv = make_float4(r_ * c.w, g_ * c.w, b_ * c.w, d_alpha);
+                over(prev, c);
+                ++cur;
+            }
+            const int kind = __ldg(&S.paint_info[p].x);
+            if (kind == P_SOLID) {
+                float s0 = warp_sum(dv.x), s1 = warp_sum(dv.y), s2 = warp_sum(dv.z), s3 = warp_sum(dv.w);
+                if (lane == 0) {
+                    float* d = G.d_paint_params + 4 * p;
+                    add_if(d + 0, s0);
+                    add_if(d + 1, s1);
+                    add_if(d + 2, s2);
+                    add_if(d + 3, s3);
+                }
+            } else if (has) {
+                float2 dtr = make_float2(0.0f, 0.0f);
+                d_gradient_paint(S, G, p, pt, dv, &dtr);
+                if (G.d_translation) {
+                    add_if(G.d_translation + 2 * (size_t)pixel, dtr.x);
+                    add_if(G.d_translation + 2 * (size_t)pixel + 1, dtr.y);
+                }
+            }
+        }
+    }
+    // Filter-radius adjoint (filters.rs:106-156) and the constant-background adjoint.
+    float dradius = 0.0f;
+    if (active) {
+        const int px = f2i(floorf(ps.x)), py = f2i(floorf(ps.y)), ri = S.filter_ri;
+        for (int dy = -ri; dy <= ri; ++dy)
+            for (int dx = -ri; dx <= ri; ++dx) {
+                int xx = px + dx, yy = py + dy;
+                if (xx < 0 || yy < 0 || xx >= W || yy >= H) continue;
+                size_t q = (size_t)yy * W + xx;
+                float ws = wsum[q];
+                if (ws <= 0.0f) continue;
+                float fxc = (float)xx + 0.5f - ps.x, fyc = (float)yy + 0.5f - ps.y;
+                float w = filter_weight(S.filter_type, S.filter_radius, fxc, fyc);
+                if (w <= 0.0f) continue;
+                float4 d = reinterpret_cast<const float4*>(d_render)[q];
+                float dt = d.x * ret.x + d.y * ret.y + d.z * ret.z + d.w * ret.w;
+                float denom = ws * ws;
+                float dw = denom > 0.0f ? (dt * ws - w * dt * (ws - w)) / denom : 0.0f;
+                if (dw != 0.0f) dradius += d_filter_weight(S.filter_type, S.filter_radius, fxc, fyc, dw);
+            }
+    }
+    float v[5] = {dcol.x, dcol.y, dcol.z, dcol.w, dradius};
+#pragma unroll
+    for (int k = 0; k < 5; ++k) v[k] = warp_sum(v[k]);
+    if (lane == 0)
+        for (int k = 0; k < 5; ++k) red[wid][k] = v[k];
+    __syncthreads();
+    if (threadIdx.x < 5) {
+        float s = 0.0f;
+        for (int w = 0; w < 8; ++w) s += red[w][threadIdx.x];
+        if (threadIdx.x < 4)
+            add_if(G.d_background + threadIdx.x, s);
+        else
+            add_if(G.d_filter_radius, s);
+    }
+}
+
+// ------------------------------------------------------------------ boundary sampling
+// sample_color with an EdgeQuery (sampling.rs:76-224, 485-552) at canvas point pt.
+// Returns the un-premultiplied colour (or the premultiplied background when no
+// fragment covers pt) and whether the queried shape is the visible boundary.
+__device__ float4 edge_color(const DevScene& S, float2 pt, float4 bg, int eq_group, int eq_shape, bool* hit_out) {
+    // Edge tests on the queried shape alone (within_distance_edge / is_inside_edge).
+    bool hit0 = false;
+    {
+        const int4 gi = __ldg(&S.g_info[eq_group]);
+        const float2 lp = xf9(S.g_c2s + 9 * eq_group, pt);
+        if (gi.y >= 0) {
+            float sw = __ldg(&S.s_stroke[eq_shape]);
+            if (sw > 0.0f && within_shape(S, eq_shape, lp, sw)) hit0 = true;
+        }
+        if (gi.x >= 0) {
+            float2 sp = shape_local_bwd(S, eq_shape, lp);
+            if (fill_hit(gi.z, winding_shape(S, eq_shape, sp, true))) hit0 = true;
+        }
+    }
+    const int tile = tile_of(S, pt);
+    const int off = S.tile_offsets[tile];
+    const int n = S.tile_offsets[tile + 1] - off;
+    const int* list = S.tile_entries + off;
+    float4 acc = bg;
+    int nfrag = 0, ev = 0;  // ev: 0 none, 1 last event sets the hit, 2 last event clears it
+    for (int e = 0; e < n; ++e) {
+        const int g = __ldg(&list[e]);
+        const int4 gi = __ldg(&S.g_info[g]);
+        const float2 lp = xf9(S.g_c2s + 9 * g, pt);
+        if (gi.y >= 0 && group_within(S, g, lp)) {
+            float4 c = paint_color(S, gi.y, pt);
+            over(acc, c);
+            ++nfrag;
+            if (c.w >= 1.0f) ev = 2;
+            if (g == eq_group) ev = 1;
+        }
+        if (gi.x >= 0 && group_inside(S, g, lp, gi.z)) {
+            float4 c = paint_color(S, gi.x, pt);
+            over(acc, c);
+            ++nfrag;
+            if (c.w >= 1.0f) ev = 2;
+            if (g == eq_group) ev = 1;
+        }
+    }
+    *hit_out = ev == 0 ? hit0 : ev == 1;
+    if (nfrag == 0) return bg;
+    float fa = acc.w, fr = acc.x, fg = acc.y, fb = acc.z;
+    if (fa > 1.0e-6f) {
+        float s = 1.0f / fa;
+        fr = fr * s;
+        fg = fg * s;
+        fb = fb * s;
+    }
+    return make_float4(fr, fg, fb, fa);
+}
+
+__device__ __forceinline__ int lower_bound_cdf(const float* cdf, int n, float u) {
+    // first idx with !(u > cdf[idx]) — the crate's linear scan (boundary.rs:454-469)
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (u > __ldg(&cdf[mid]))
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+__device__ __forceinline__ float cdf_local_t(const float* cdf, int n, int idx, float u) {
+    float prev = idx == 0 ? 0.0f : __ldg(&cdf[idx - 1]);
+    float denom = fmaxf(__ldg(&cdf[idx]) - prev, 1.0e-6f);
+    return clampf((u - prev) / denom, 0.0f, 1.0f);
+}
+__device__ __forceinline__ bool path_pt(const DevScene& S, int po, int pc, bool closed, long idx, float2* p) {
+    if (pc == 0) return false;
+    long i;
+    if (closed)
+        i = idx % pc;
+    else if (idx >= pc)
+        return false;
+    else
+        i = idx;
+    *p = S.points[po + i];
+    return true;
+}
+__device__ __forceinline__ bool path_pt_r(const DevScene& S, int po, int pc, bool closed, bool thick, long idx,
+                                          float def_r, float2* p, float* r) {
+    if (!path_pt(S, po, pc, closed, idx, p)) return false;
+    long i = closed ? idx % pc : idx;
+    *r = (thick && i < pc) ? S.thickness[po + i] * 1.0f : def_r;
+    return true;
+}
+struct BData {
+    int base_point_id, point_id;
+    float t;
+    bool is_stroke;
+};
+__device__ __forceinline__ float2 nrm2(float2 v) {
+    float l = len2(v.x, v.y);
+    return l == 0.0f ? make_float2(0.0f, 0.0f) : make_float2(v.x / l, v.y / l);
+}
+// sample_boundary_path (boundary.rs:630-842)
+__device__ float2 sample_boundary_path(const DevScene& S, int shape, float path_len, float t, float2* normal,
+                                       float* pdf, BData* data, float dir, float srad) {
+    const int path = __ldg(&S.s_info[shape].z);
+    const int4 pi2 = __ldg(&S.p_info[2 * path + 1]);
+    const int po = pi2.x, pc = pi2.y, co = pi2.z;
+    const bool closed = pi2.w & PF_CLOSED;
+    const bool thick = pi2.w & PF_THICK;
+    const int4 cinfo = __ldg(&S.path_cdf_info[shape]);
+    const int nb = cinfo.y;
+    if (pc == 0 || nb == 0) {
+        *pdf = 0.0f;
+        return make_float2(0, 0);
+    }
+    if (dir != 0.0f && !closed) {
+        float cap = 0.0f;
+        if (thick)
+            cap = PI_F * (S.thickness[po] + S.thickness[po + pc - 1]);
+        else
+            cap = 2.0f * PI_F * srad;
+        float denom = cap + path_len;
+        if (denom > 0.0f) {
+            float cp = cap / denom;
+            if (t < cp) {
+                t /= cp;
+                *pdf *= cp;
+                float r0 = srad, r1 = srad;
+                if (thick) {
+                    r0 = S.thickness[po];
+                    r1 = S.thickness[po + pc - 1];
+                }
+                float ang = 2.0f * PI_F * t;
+                if (dir < 0.0f) {
+                    float2 o = make_float2(r0 * cosf(ang), r0 * sinf(ang));
+                    *normal = nrm2(o);
+                    *pdf /= 2.0f * PI_F * r0;
+                    data->base_point_id = 0;
+                    data->point_id = 0;
+                    data->t = 0.0f;
+                    float2 p0 = S.points[po];
+                    return make_float2(p0.x + o.x, p0.y + o.y);
+                }
+                float2 o = make_float2(r1 * cosf(ang), r1 * sinf(ang));
+                *normal = nrm2(o);
+                *pdf /= 2.0f * PI_F * r1;
+                data->base_point_id = nb - 1;
+                int controls = S.ncp[co + nb - 1];
+                data->point_id = pc >= 2 + controls ? pc - (2 + controls) : 0;
+                data->t = 1.0f;
+                float2 pl = S.points[po + pc - 1];
+                return make_float2(pl.x + o.x, pl.y + o.y);
+            }
+            t = (t - cp) / (1.0f - cp);
+            *pdf *= 1.0f - cp;
+        }
+    }
+    const float* cdf = S.path_cdf + cinfo.x;
+    int sid = lower_bound_cdf(cdf, nb, t);
+    if (sid >= nb) sid = nb - 1;
+    float lt = cdf_local_t(cdf, nb, sid, t);
+    int pid = S.path_pid[cinfo.x + sid];
+    data->base_point_id = sid;
+    data->point_id = pid;
+    data->t = lt;
+    if (lt < -1.0e-3f || lt > 1.0f + 1.0e-3f) {
+        *pdf = 0.0f;
+        return make_float2(0, 0);
+    }
+    int nc = S.ncp[co + sid];
+    float pmf = S.path_pmf[cinfo.x + sid];
+    auto nxt = [&](long i) -> long { return closed ? i % pc : (i < pc - 1 ? i : pc - 1); };
+    float2 q[4];
+    float r[4];
+    int np = nc + 2;
+    if (nc > 2) {
+        *pdf = 0.0f;
+        return make_float2(0, 0);
+    }
+    for (int k = 0; k < np; ++k) {
+        long idx = (k == np - 1) ? nxt(pid + k) : (long)(pid + k);
+        if (!path_pt_r(S, po, pc, closed, thick, idx, srad, &q[k], &r[k])) {
+            *pdf = 0.0f;
+            return make_float2(0, 0);
+        }
+    }
+    float tt = 1.0f - lt;
+    float2 ev, tg;
+    float rr;
+    if (nc == 0) {
+        tg = make_float2(q[1].x - q[0].x, q[1].y - q[0].y);
+        ev = make_float2(q[0].x + tg.x * lt, q[0].y + tg.y * lt);
+        rr = r[0] + lt * (r[1] - r[0]);
+    } else if (nc == 1) {
+        float w0 = tt * tt, w1 = 2.0f * tt * lt, w2 = lt * lt;
+        ev = make_float2(q[0].x * w0 + q[1].x * w1 + q[2].x * w2, q[0].y * w0 + q[1].y * w1 + q[2].y * w2);
+        float a = 2.0f * tt, b = 2.0f * lt;
+        tg = make_float2((q[1].x - q[0].x) * a + (q[2].x - q[1].x) * b, (q[1].y - q[0].y) * a + (q[2].y - q[1].y) * b);
+        rr = r[0] * w0 + r[1] * w1 + r[2] * w2;
+    } else {
+        float w0 = tt * tt * tt, w1 = 3.0f * tt * tt * lt, w2 = 3.0f * tt * lt * lt, w3 = lt * lt * lt;
+        ev = make_float2(q[0].x * w0 + q[1].x * w1 + q[2].x * w2 + q[3].x * w3,
+                         q[0].y * w0 + q[1].y * w1 + q[2].y * w2 + q[3].y * w3);
+        float a = 3.0f * tt * tt, b = 6.0f * tt * lt, c = 3.0f * lt * lt;
+        tg = make_float2((q[1].x - q[0].x) * a + (q[2].x - q[1].x) * b + (q[3].x - q[2].x) * c,
+                         (q[1].y - q[0].y) * a + (q[2].y - q[1].y) * b + (q[3].y - q[2].y) * c);
+        rr = r[0] * w0 + r[1] * w1 + r[2] * w2 + r[3] * w3;
+    }
+    float tl = len2(tg.x, tg.y);
+    if (tl == 0.0f) {
+        *pdf = 0.0f;
+        return make_float2(0, 0);
+    }
+    *normal = make_float2(-tg.y / tl, tg.x / tl);
+    *pdf *= pmf / tl;
+    if (dir != 0.0f) {
+        ev.x += normal->x * (dir * rr);
+        ev.y += normal->y * (dir * rr);
+        if (dir < 0.0f) *normal = make_float2(normal->x * -1.0f, normal->y * -1.0f);
+    }
+    return ev;
+}
+// sample_boundary_point (boundary.rs:472-627)
+__device__ bool sample_boundary_point(const DevScene& S, int shape, int group, float t, float shape_len,
+                                      float2* pt_out, float2* normal_out, float* pdf_out, BData* data) {
+    const int4 gi = __ldg(&S.g_info[group]);
+    const bool has_fill = gi.x >= 0, has_stroke = gi.y >= 0;
+    if (!has_fill && !has_stroke) return false;
+    float pdf = 1.0f, lt = t;
+    bool stroke = false;
+    if (has_fill && has_stroke) {
+        if (lt < 0.5f) {
+            lt *= 2.0f;
+        } else {
+            stroke = true;
+            lt = 2.0f * (lt - 0.5f);
+        }
+        pdf = 0.5f;
+    } else if (has_stroke) {
+        stroke = true;
+    }
+    float dir = 0.0f;
+    if (stroke) {
+        if (lt < 0.5f) {
+            dir = -1.0f;
+            lt *= 2.0f;
+        } else {
+            dir = 1.0f;
+            lt = 2.0f * (lt - 0.5f);
+        }
+        pdf *= 0.5f;
+    }
+    data->base_point_id = 0;
+    data->point_id = 0;
+    data->t = 0.0f;
+    data->is_stroke = stroke;
+    const int4 si = __ldg(&S.s_info[shape]);
+    const float4 prm = __ldg(&S.s_params[shape]);
+    const float sw = __ldg(&S.s_stroke[shape]);
+    float2 normal = make_float2(0, 0), out;
+    if (si.x == K_CIRCLE) {
+        float r = fabsf(prm.z);
+        if (r <= 0.0f) return false;
+        float ang = 2.0f * PI_F * lt;
+        float2 o = make_float2(r * cosf(ang), r * sinf(ang));
+        normal = nrm2(o);
+        pdf /= 2.0f * PI_F * r;
+        out = make_float2(prm.x + o.x, prm.y + o.y);
+    } else if (si.x == K_ELLIPSE) {
+        float rx = fabsf(prm.z), ry = fabsf(prm.w);
+        if (rx <= 0.0f || ry <= 0.0f) return false;
+        float ang = 2.0f * PI_F * lt;
+        float s = sinf(ang), c = cosf(ang);
+        float dxdt = -rx * s * 2.0f * PI_F, dydt = ry * c * 2.0f * PI_F;
+        normal = nrm2(make_float2(dydt, -dxdt));
+        pdf /= sqrtf(dxdt * dxdt + dydt * dydt);
+        out = make_float2(prm.x + rx * c, prm.y + ry * s);
+    } else if (si.x == K_RECT) {
+        float w = prm.z - prm.x, h = prm.w - prm.y;
+        if (w == 0.0f && h == 0.0f) return false;
+        pdf /= 2.0f * (w + h);
+        if (lt <= w / (w + h)) {
+            lt *= (w + h) / w;
+            if (lt < 0.5f) {
+                normal = make_float2(0.0f, -1.0f);
+                out = make_float2(prm.x + 2.0f * lt * (prm.z - prm.x), prm.y + 0.0f);
+            } else {
+                normal = make_float2(0.0f, 1.0f);
+                out = make_float2(prm.x + 2.0f * (lt - 0.5f) * (prm.z - prm.x), prm.w + 0.0f);
+            }
+        } else {
+            lt = (lt - w / (w + h)) * (w + h) / h;
+            if (lt < 0.5f) {
+                normal = make_float2(-1.0f, 0.0f);
+                out = make_float2(prm.x + 0.0f, prm.y + 2.0f * lt * (prm.w - prm.y));
+            } else {
+                normal = make_float2(1.0f, 0.0f);
+                out = make_float2(prm.z + 0.0f, prm.y + 2.0f * (lt - 0.5f) * (prm.w - prm.y));
+            }
+        }
+    } else {
+        if (si.z < 0) return false;
+        const int4 ci = __ldg(&S.path_cdf_info[shape]);
+        if (!ci.z) return false;
+        if (S.path_len[shape] <= 0.0f) return false;
+        out = sample_boundary_path(S, shape, shape_len, lt, &normal, &pdf, data, dir, sw);
+        dir = 0.0f;  // the path sampler applies the stroke offset itself
+    }
+    if (dir != 0.0f) {
+        out.x += normal.x * (dir * sw);
+        out.y += normal.y * (dir * sw);
+        if (dir < 0.0f) normal = make_float2(normal.x * -1.0f, normal.y * -1.0f);
+    }
+    if (!isfinite(pdf) || pdf <= 0.0f) return false;
+    *pt_out = out;
+    *normal_out = normal;
+    *pdf_out = pdf;
+    return true;
+}
+__device__ __forceinline__ void mul33(const float* a, const float* b, float* o) {  // Mat3::mul
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) o[3 * r + c] = a[3 * r] * b[c] + a[3 * r + 1] * b[3 + c] + a[3 * r + 2] * b[6 + c];
+}
+// accumulate_boundary_gradient (boundary.rs:970-1148)
+__device__ void accumulate_boundary(const DevScene& S, const GradPtrs& G, int shape, int group, float contrib,
+                                    float t, float2 n, const BData& bd, float2 local_pt) {
+    const int4 si = __ldg(&S.s_info[shape]);
+    int po = 0, pc = 0, co = 0, pflags = 0;
+    if (si.x == K_PATH && si.z >= 0) {
+        int4 pi2 = __ldg(&S.p_info[2 * si.z + 1]);
+        po = pi2.x;
+        pc = pi2.y;
+        co = pi2.z;
+        pflags = pi2.w;
+    }
+    const bool closed = pflags & PF_CLOSED;
+    int nc = 0;  // num_control_points.get(base_point_id).unwrap_or(0)
+    if (si.x == K_PATH) {
+        int ctrl_count = __ldg(&S.path_cdf_info[shape].y);
+        nc = bd.base_point_id < ctrl_count ? S.ncp[co + bd.base_point_id] : 0;
+    }
+    if (bd.is_stroke) {
+        if (si.x == K_PATH && (pflags & PF_THICK)) {
+            float t2 = bd.t, tt = 1.0f - t2;
+            int pid = bd.point_id;
+            auto addt = [&](long i, float v) {
+                if (i < pc) add_if(G.d_thickness + po + i, v);
+            };
+            if (nc == 0) {
+                addt(pid, (1.0f - t2) * contrib);
+                addt(closed ? (pid + 1) % pc : pid + 1, t2 * contrib);
+            } else if (nc == 1) {
+                addt(pid, tt * tt * contrib);
+                addt(pid + 1, 2.0f * tt * t2 * contrib);
+                addt(closed ? (pid + 2) % pc : pid + 2, t2 * t2 * contrib);
+            } else if (nc == 2) {
+                addt(pid, tt * tt * tt * contrib);
+                addt(pid + 1, 3.0f * tt * tt * t2 * contrib);
+                addt(pid + 2, 3.0f * tt * t2 * t2 * contrib);
+                addt(closed ? (pid + 3) % pc : pid + 3, t2 * t2 * t2 * contrib);
+            }
+        } else {
+            add_if(G.d_shape_stroke_width + shape, contrib);
+        }
+    }
+    float* dp = G.d_shape_params + 4 * shape;
+    if (si.x == K_CIRCLE) {
+        add_if(dp + 0, n.x * contrib);
+        add_if(dp + 1, n.y * contrib);
+        add_if(dp + 2, contrib);
+    } else if (si.x == K_ELLIPSE) {
+        add_if(dp + 0, n.x * contrib);
+        add_if(dp + 1, n.y * contrib);
+        float ang = 2.0f * PI_F * t;
+        add_if(dp + 2, cosf(ang) * n.x * contrib);
+        add_if(dp + 3, sinf(ang) * n.y * contrib);
+    } else if (si.x == K_PATH) {
+        float t2 = bd.t, tt = 1.0f - t2;
+        int pid = bd.point_id;
+        auto addp = [&](long idx, float w) {
+            long i = closed ? idx % pc : idx;
+            if (i < pc) {
+                add_if(G.d_points + 2 * (po + i), n.x * (w * contrib));
+                add_if(G.d_points + 2 * (po + i) + 1, n.y * (w * contrib));
+            }
+        };
+        if (nc == 0) {
+            addp(pid, 1.0f - t2);
+            addp(pid + 1, t2);
+        } else if (nc == 1) {
+            addp(pid, tt * tt);
+            addp(pid + 1, 2.0f * tt * t2);
+            addp(pid + 2, t2 * t2);
+        } else if (nc == 2) {
+            addp(pid, tt * tt * tt);
+            addp(pid + 1, 3.0f * tt * tt * t2);
+            addp(pid + 2, 3.0f * tt * t2 * t2);
+            addp(pid + 3, t2 * t2 * t2);
+        }
+    } else if (si.x == K_RECT) {
+        if (n.x == -1.0f && n.y == 0.0f)
+            add_if(dp + 0, -contrib);
+        else if (n.x == 1.0f && n.y == 0.0f)
+            add_if(dp + 2, contrib);
+        else if (n.x == 0.0f && n.y == -1.0f)
+            add_if(dp + 1, -contrib);
+        else if (n.x == 0.0f && n.y == 1.0f)
+            add_if(dp + 3, contrib);
+    }
+    // transforms (boundary.rs:1132-1147) with d_xform_pt (backward/math.rs:109-128)
+    const float* gs = S.g_s2c + 9 * group;
+    const float* sx = S.s_xform + 9 * shape;
+    float m[9];
+    mul33(gs, sx, m);
+    const float2 dout = make_float2(n.x * contrib, n.y * contrib);
+    const float2 p = local_pt;
+    float t0 = m[0] * p.x + m[1] * p.y + m[2];
+    float t1 = m[3] * p.x + m[4] * p.y + m[5];
+    float t2 = m[6] * p.x + m[7] * p.y + m[8];
+    float ox = t0 / t2, oy = t1 / t2;
+    float d0 = dout.x / t2, d1 = dout.y / t2, d2 = -(dout.x * ox + dout.y * oy) / t2;
+    float dm[9] = {d0 * p.x, d0 * p.y, d0, d1 * p.x, d1 * p.y, d1, d2 * p.x, d2 * p.y, d2};
+    // d_group = dm * shape_xform^T ; d_shape = group_s2c^T * dm
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            float dg = dm[3 * r] * sx[3 * c] + dm[3 * r + 1] * sx[3 * c + 1] + dm[3 * r + 2] * sx[3 * c + 2];
+            float ds = gs[r] * dm[c] + gs[3 + r] * dm[3 + c] + gs[6 + r] * dm[6 + c];
+            add_if(G.d_group_transform + 9 * group + 3 * r + c, dg);
+            add_if(G.d_shape_transform + 9 * shape + 3 * r + c, ds);
+        }
+}
+
+__global__ void __launch_bounds__(128) k_boundary(DevScene S, BoundaryParams bp, const float* d_render,
+                                                  const float* wsum, GradPtrs G) {
+    const uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + bp.sample_base;
+    if (idx >= bp.num_samples) return;
+    float u, t;
+    if (bp.rng == 1) {
+        uint4 r = philox4x32_10(make_uint4((uint32_t)idx, (uint32_t)(idx >> 32), 0u, 0u), make_uint2(bp.seed, 0u));
+        u = unit_from_u32(r.x);
+        t = unit_from_u32(r.y);
+    } else {
+        Pcg32 rng(idx, (uint64_t)bp.seed);
+        u = rng.next_f32();
+        t = rng.next_f32();
+    }
+    int sid = lower_bound_cdf(S.bcdf, S.bcdf_n, u);
+    if (sid >= S.bcdf_n) sid = S.bcdf_n - 1;
+    const int shape = S.b_shape[sid], group = S.b_group[sid];
+    const float pmf = S.bpmf[sid];
+    if (pmf <= 0.0f) return;
+    float2 local_pt, normal;
+    float bpdf;
+    BData bd;
+    if (!sample_boundary_point(S, shape, group, t, S.shape_len[shape], &local_pt, &normal, &bpdf, &bd)) return;
+    if (bpdf <= 0.0f) return;
+    // canvas point, canvas normal (boundary.rs:167-175)
+    float s2c[9];
+    mul33(S.g_s2c + 9 * group, S.s_xform + 9 * shape, s2c);
+    float2 bpt = xf9(s2c, local_pt);
+    float sinv[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    if (__ldg(&S.s_info[shape].y) & SF_INVERTIBLE) {
+        const float* iv = S.s_inv + 6 * shape;
+        for (int k = 0; k < 6; ++k) sinv[k] = iv[k];
+    }
+    float cinv[9];
+    mul33(sinv, S.g_c2s + 9 * group, cinv);
+    float2 nc = nrm2(make_float2(cinv[0] * normal.x + cinv[3] * normal.y, cinv[1] * normal.x + cinv[4] * normal.y));
+    const float W = (float)S.width, H = (float)S.height;
+    bpt.x /= W;
+    bpt.y /= H;
+    const float pdf = pmf * bpdf;
+    if (pdf <= 0.0f) return;
+    const int bx = f2i(bpt.x * W), by = f2i(bpt.y * H);
+    if (bx < 0 || bx >= S.width || by < 0 || by >= S.height) return;
+    const int pixel = by * S.width + bx;
+    const float4 bg = background_premul(S, pixel);
+    bool hi, ho;
+    float2 pin = make_float2(bpt.x - nc.x * 1.0e-4f, bpt.y - nc.y * 1.0e-4f);
+    float2 pout = make_float2(bpt.x + nc.x * 1.0e-4f, bpt.y + nc.y * 1.0e-4f);
+    float4 ci = edge_color(S, make_float2(pin.x * W, pin.y * H), bg, group, shape, &hi);
+    float4 co = edge_color(S, make_float2(pout.x * W, pout.y * H), bg, group, shape, &ho);
+    if (!hi && !ho) return;
+    if (!hi) {
+        nc = make_float2(nc.x * -1.0f, nc.y * -1.0f);
+        float4 tmp = ci;
+        ci = co;
+        co = tmp;
+    }
+    // gather_d_color at the boundary pixel, divided by W*H (boundary.rs:913-929)
+    const float2 sb = make_float2(bpt.x * W, bpt.y * H);
+    float4 dc = make_float4(0, 0, 0, 0);
+    {
+        const int px = f2i(floorf(sb.x)), py = f2i(floorf(sb.y)), ri = S.filter_ri;
+        for (int dy = -ri; dy <= ri; ++dy)
+            for (int dx = -ri; dx <= ri; ++dx) {
+                int xx = px + dx, yy = py + dy;
+                if (xx < 0 || yy < 0 || xx >= S.width || yy >= S.height) continue;
+                float w = filter_weight(S.filter_type, S.filter_radius, (float)xx + 0.5f - sb.x,
+                                        (float)yy + 0.5f - sb.y);
+                size_t q = (size_t)yy * S.width + xx;
+                float ws = wsum[q];
+                if (ws > 0.0f) {
+                    float4 d = reinterpret_cast<const float4*>(d_render)[q];
+                    float k = w / ws;
+                    dc.x += k * d.x;
+                    dc.y += k * d.y;
+                    dc.z += k * d.z;
+                    dc.w += k * d.w;
+                }
+            }
+    }
+    const float norm = W * H;
+    if (norm > 0.0f) {
+        dc.x /= norm;
+        dc.y /= norm;
+        dc.z /= norm;
+        dc.w /= norm;
+    }
+    const float contrib =
+        ((ci.x - co.x) * dc.x + (ci.y - co.y) * dc.y + (ci.z - co.z) * dc.z + (ci.w - co.w) * dc.w) / pdf;
+    if (!isfinite(contrib)) return;
+    accumulate_boundary(S, G, shape, group, contrib, t, nc, bd, local_pt);
+    if (G.d_translation) {
+        add_if(G.d_translation + 2 * (size_t)pixel, nc.x * contrib);
+        add_if(G.d_translation + 2 * (size_t)pixel + 1, nc.y * contrib);
+    }
+}
+
+// ------------------------------------------------------------------ background finalisation (background.rs:29-61)
+__global__ void k_finalize_background(DevScene S, GradPtrs G) {
+    size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (S.bg_image) {
+        if (!G.d_background_image || p >= (size_t)S.width * S.height) return;
+        const float* im = S.bg_image + 4 * p;
+        float* c = G.d_background_image + 4 * p;
+        float dr = c[0] * im[3], dg = c[1] * im[3], db = c[2] * im[3];
+        float da = c[0] * im[0] + c[1] * im[1] + c[2] * im[2] + c[3];
+        c[0] = dr;
+        c[1] = dg;
+        c[2] = db;
+        c[3] = da;
+        return;
+    }
+    if (p != 0) return;
+    float* d = G.d_background;
+    float r = S.bg[0], g = S.bg[1], b = S.bg[2], a = S.bg[3];
+    float nr = d[0] * a, ng = d[1] * a, nb = d[2] * a;
+    float na = d[0] * r + d[1] * g + d[2] * b + d[3];
+    d[0] = nr;
+    d[1] = ng;
+    d[2] = nb;
+    d[3] = na;
+}
+
+// Image::solid / background image copy for scenes without groups (renderer.rs:57-66).
+__global__ void k_fill_background(DevScene S, float* out) {
+    size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= (size_t)S.width * S.height) return;
+    float4 v = S.bg_image ? reinterpret_cast<const float4*>(S.bg_image)[p]
+                          : make_float4(S.bg[0], S.bg[1], S.bg[2], S.bg[3]);
+    reinterpret_cast<float4*>(out)[p] = v;
+}
+
+// ------------------------------------------------------------------ L2 loss
+__global__ void k_l2(const float* img, const float* target, size_t n, float* d_render, float* loss) {
+    __shared__ float red[8];
+    float s = 0.0f;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        float d = img[i] - target[i];
+        d_render[i] = 2.0f * d;
+        s += d * d;
+    }
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0 && loss) {
+        float t = 0.0f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        atomicAdd(loss, t);
+    }
+}
+
+}  // namespace dvgb
+
+// ------------------------------------------------------------------ launchers
+namespace dvgb {
+
+int launch_binning(const DevScene& S, const float4* g_bbox, int* counts, int* offsets, int* entries,
+                   cudaStream_t stream) {
+    const int tiles = S.tiles_x * S.tiles_y;
+    if (!entries) {
+        k_bin_count<<<tiles, 256, 0, stream>>>(S, g_bbox, counts);
+        k_bin_scan<<<1, 1024, 0, stream>>>(counts, tiles, offsets);
+        return 2;
+    }
+    k_bin_write<<<tiles, 256, 0, stream>>>(S, g_bbox, offsets, entries);
+    return 1;
+}
+int launch_forward(const DevScene& S, const SampleParams& sp, float* accum, float* wsum, unsigned* status,
+                   cudaStream_t stream) {
+    const int tiles = S.tiles_x * S.tiles_y;
+    const int hw = TILE + 2 * S.filter_ri;
+    size_t smem = S.filter_ri <= MAX_SMEM_RI ? (size_t)hw * hw * 5 * sizeof(float) : 0;
+    dim3 grid(tiles, sp.sxn * sp.syn);
+    k_forward<<<grid, 256, smem, stream>>>(S, sp, accum, wsum, status);
+    return 1;
+}
+int launch_weights(const DevScene& S, const SampleParams& sp, float* wsum, cudaStream_t stream) {
+    dim3 grid(S.tiles_x * S.tiles_y, sp.sxn * sp.syn);
+    k_weights<<<grid, 256, 0, stream>>>(S, sp, wsum);
+    return 1;
+}
+int launch_resolve(const DevScene& S, const float* accum, const float* wsum, float* out, cudaStream_t stream) {
+    size_t n = (size_t)S.width * S.height;
+    k_resolve<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(S, accum, wsum, out);
+    return 1;
+}
+int launch_interior(const DevScene& S, const SampleParams& sp, const float* d_render, const float* wsum,
+                    const GradPtrs& G, unsigned* status, cudaStream_t stream) {
+    dim3 grid(S.tiles_x * S.tiles_y, sp.sxn * sp.syn);
+    k_interior<<<grid, 256, 0, stream>>>(S, sp, d_render, wsum, G, status);
+    return 1;
+}
+int launch_boundary(const DevScene& S, const BoundaryParams& bp, const float* d_render, const float* wsum,
+                    const GradPtrs& G, cudaStream_t stream) {
+    uint64_t n = bp.num_samples;
+    if (n == 0) return 0;
+    int launches = 0;
+    const uint64_t chunk = (uint64_t)1 << 30;  // keep the grid's x extent well inside 2^31
+    for (uint64_t base = 0; base < n; base += chunk) {
+        BoundaryParams b = bp;
+        b.sample_base = base;
+        b.num_samples = base + chunk < n ? base + chunk : n;
+        uint64_t cnt = b.num_samples - base;
+        k_boundary<<<(unsigned)((cnt + 127) / 128), 128, 0, stream>>>(S, b, d_render, wsum, G);
+        ++launches;
+    }
+    return launches;
+}
+int launch_finalize_background(const DevScene& S, const GradPtrs& G, cudaStream_t stream) {
+    size_t n = S.bg_image ? (size_t)S.width * S.height : 1;
+    k_finalize_background<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(S, G);
+    return 1;
+}
+int launch_fill_background(const DevScene& S, float* out, cudaStream_t stream) {
+    size_t n = (size_t)S.width * S.height;
+    k_fill_background<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(S, out);
+    return 1;
+}
+int launch_l2(const float* img, const float* target, size_t n, float* d_render, float* loss, cudaStream_t stream) {
+    unsigned blocks = (unsigned)((n + 255) / 256);
+    if (blocks > 4096) blocks = 4096;
+    if (blocks == 0) blocks = 1;
+    k_l2<<<blocks, 256, 0, stream>>>(img, target, n, d_render, loss);
+    return 1;
+}
+
+}  // namespace dvgb

@@ -1,0 +1,60 @@
+// kernels.cuh — parameters and host launchers of the kernels in kernels.cu.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+
+namespace dvgb {
+
+// Per-thread fragment capacity of the interior adjoint (the crate's GPU kernel
+// used 256, src/gpu/kernels/backward.rs:1657-1662).  Exceeding it sets
+// ST_FRAGMENT_OVERFLOW and the call returns DVG_ERR_DEVICE_LIMIT.
+constexpr int MAX_FRAGMENTS = 96;
+// Filter radii up to this (ceil) use the shared-memory tile+halo splat.
+constexpr int MAX_SMEM_RI = 8;
+
+struct SampleParams {
+    int sxn, syn;
+    uint32_t seed;
+    bool jitter;
+};
+struct BoundaryParams {
+    uint64_t num_samples;
+    uint64_t sample_base;
+    uint32_t seed;
+    int rng;  // 0 PCG32, 1 Philox
+};
+struct GradPtrs {
+    float* d_shape_params;
+    float* d_shape_transform;
+    float* d_shape_stroke_width;
+    float* d_points;
+    float* d_thickness;
+    float* d_group_transform;
+    float* d_paint_params;
+    float* d_stop_offsets;
+    float* d_stop_colors;
+    float* d_filter_radius;
+    float* d_background;
+    float* d_background_image;
+    float* d_translation;
+};
+
+// Launchers (all asynchronous on `stream`).  Each returns the number of kernels launched.
+int launch_binning(const DevScene& S, const float4* g_bbox, int* counts, int* offsets, int* entries_or_null,
+                   cudaStream_t stream);
+int launch_forward(const DevScene& S, const SampleParams& sp, float* accum, float* wsum, unsigned* status,
+                   cudaStream_t stream);
+int launch_weights(const DevScene& S, const SampleParams& sp, float* wsum, cudaStream_t stream);
+int launch_resolve(const DevScene& S, const float* accum, const float* wsum, float* out, cudaStream_t stream);
+int launch_interior(const DevScene& S, const SampleParams& sp, const float* d_render, const float* wsum,
+                    const GradPtrs& G, unsigned* status, cudaStream_t stream);
+int launch_boundary(const DevScene& S, const BoundaryParams& bp, const float* d_render, const float* wsum,
+                    const GradPtrs& G, cudaStream_t stream);
+int launch_finalize_background(const DevScene& S, const GradPtrs& G, cudaStream_t stream);
+int launch_fill_background(const DevScene& S, float* out, cudaStream_t stream);
+int launch_l2(const float* img, const float* target, size_t n, float* d_render, float* loss, cudaStream_t stream);
+
+}  // namespace dvgb

@@ -1,0 +1,403 @@
+"""ctypes mirror of include/dvg.h and the scene packer.
+
+``pack_scene`` flattens a ``Scene`` into the structure-of-arrays
+``dvg_scene_desc`` the C ABI takes (integer indices, one paint entry per group
+fill / stroke).  ``GradBuffers`` allocates the flat ``dvg_grads`` arrays and
+``unflatten_grads`` rebuilds the crate's ``SceneGrad`` shape
+(src/grad.rs:113-126) from them.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional
+
+import numpy as np
+
+from .scene import (
+    BackwardOptions,
+    Circle,
+    Color,
+    Ellipse,
+    LinearGradient,
+    PathGeometry,
+    RadialGradient,
+    Rect,
+    RenderOptions,
+    Scene,
+)
+
+SHAPE_CIRCLE, SHAPE_RECT, SHAPE_PATH, SHAPE_ELLIPSE = 0, 1, 2, 3
+PAINT_NONE, PAINT_SOLID, PAINT_LINEAR, PAINT_RADIAL = 0, 1, 2, 3
+PATH_CLOSED, PATH_DISTANCE_APPROX, PATH_HAS_THICKNESS = 1, 2, 4
+
+_fp = C.POINTER(C.c_float)
+_u32p = C.POINTER(C.c_uint32)
+_i32p = C.POINTER(C.c_int32)
+_u8p = C.POINTER(C.c_uint8)
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("width", C.c_uint32), ("height", C.c_uint32),
+        ("background", C.c_float * 4),
+        ("background_image", _fp),
+        ("filter_type", C.c_uint32), ("filter_radius", C.c_float),
+        ("num_shapes", C.c_uint32),
+        ("shape_kind", _u32p), ("shape_params", _fp), ("shape_transform", _fp),
+        ("shape_stroke_width", _fp), ("shape_stroke_join", _u32p), ("shape_stroke_cap", _u32p),
+        ("shape_miter_limit", _fp),
+        ("path_ctrl_offset", _u32p), ("path_ctrl_count", _u32p),
+        ("path_point_offset", _u32p), ("path_point_count", _u32p), ("path_flags", _u32p),
+        ("num_control_points", _u8p), ("points", _fp), ("thickness", _fp),
+        ("total_ctrl", C.c_uint32), ("total_points", C.c_uint32),
+        ("num_groups", C.c_uint32),
+        ("group_shape_offset", _u32p), ("group_shape_count", _u32p), ("group_shape_ids", _u32p),
+        ("total_group_shapes", C.c_uint32),
+        ("group_fill_rule", _u32p), ("group_shape_to_canvas", _fp), ("group_canvas_to_shape", _fp),
+        ("group_fill_paint", _i32p), ("group_stroke_paint", _i32p),
+        ("num_paints", C.c_uint32),
+        ("paint_kind", _u32p), ("paint_params", _fp), ("paint_stop_offset", _u32p),
+        ("paint_stop_count", _u32p), ("stop_offsets", _fp), ("stop_colors", _fp),
+        ("total_stops", C.c_uint32),
+    ]
+
+
+class RenderOptionsC(C.Structure):
+    _fields_ = [
+        ("aa", C.c_float), ("path_tolerance", C.c_float),
+        ("samples_x", C.c_uint32), ("samples_y", C.c_uint32), ("seed", C.c_uint32),
+        ("jitter", C.c_uint32), ("use_prefiltering", C.c_uint32),
+    ]
+
+
+class BackwardOptionsC(C.Structure):
+    _fields_ = [
+        ("compute_translation", C.c_uint32), ("boundary_samples", C.c_uint32), ("rng", C.c_uint32),
+        ("boundary_seed", C.c_uint32), ("boundary_seed_from_options", C.c_uint32),
+    ]
+
+
+class GradsC(C.Structure):
+    _fields_ = [(n, _fp) for n in (
+        "d_shape_params", "d_shape_transform", "d_shape_stroke_width", "d_points", "d_thickness",
+        "d_group_transform", "d_paint_params", "d_stop_offsets", "d_stop_colors", "d_filter_radius",
+        "d_background", "d_background_image", "d_translation")]
+
+
+def _ptr(a: Optional[np.ndarray], ctype):
+    if a is None:
+        return C.cast(None, C.POINTER(ctype))
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def render_options_c(o: RenderOptions) -> RenderOptionsC:
+    return RenderOptionsC(float(o.aa), float(o.path_tolerance), int(o.samples_x), int(o.samples_y),
+                          int(o.seed) & 0xFFFFFFFF, 1 if o.jitter else 0, 1 if o.use_prefiltering else 0)
+
+
+def backward_options_c(b: Optional[BackwardOptions]) -> BackwardOptionsC:
+    b = b or BackwardOptions()
+    from_opts = 1 if b.boundary_seed is None else 0
+    seed = 0 if b.boundary_seed is None else int(b.boundary_seed) & 0xFFFFFFFF
+    return BackwardOptionsC(1 if b.compute_translation else 0, int(b.boundary_samples), int(b.rng), seed, from_opts)
+
+
+@dataclass
+class PackedScene:
+    """A packed scene: the ctypes description plus the numpy arrays it points into."""
+
+    desc: SceneDesc
+    arrays: Dict[str, np.ndarray]
+    # paint bookkeeping: (group index, "fill"|"stroke") -> paint index
+    paint_of: Dict[tuple, int] = field(default_factory=dict)
+    path_point_offset: List[int] = field(default_factory=list)
+    path_point_count: List[int] = field(default_factory=list)
+    stop_offset: List[int] = field(default_factory=list)
+    stop_count: List[int] = field(default_factory=list)
+
+    def ref(self):
+        return C.byref(self.desc)
+
+
+def _paint_record(p):
+    if isinstance(p, Color):
+        return PAINT_SOLID, [p.r, p.g, p.b, p.a], []
+    if isinstance(p, LinearGradient):
+        return PAINT_LINEAR, [p.start[0], p.start[1], p.end[0], p.end[1]], p.stops
+    if isinstance(p, RadialGradient):
+        return PAINT_RADIAL, [p.center[0], p.center[1], p.radius[0], p.radius[1]], p.stops
+    raise TypeError(f"unsupported paint {type(p)!r}")
+
+
+def pack_scene(scene: Scene) -> PackedScene:
+    ns = len(scene.shapes)
+    kinds = np.zeros(ns, np.uint32)
+    params = np.zeros((ns, 4), np.float32)
+    xforms = np.zeros((ns, 9), np.float32)
+    sw = np.zeros(ns, np.float32)
+    joins = np.zeros(ns, np.uint32)
+    caps = np.zeros(ns, np.uint32)
+    miters = np.zeros(ns, np.float32)
+    ctrl_off = np.zeros(ns, np.uint32)
+    ctrl_cnt = np.zeros(ns, np.uint32)
+    pt_off = np.zeros(ns, np.uint32)
+    pt_cnt = np.zeros(ns, np.uint32)
+    flags = np.zeros(ns, np.uint32)
+    ncp: List[int] = []
+    pts: List[float] = []
+    thick: List[float] = []
+    any_thick = False
+    for i, sh in enumerate(scene.shapes):
+        g = sh.geometry
+        xforms[i] = sh.transform.flat()
+        sw[i] = sh.stroke_width
+        joins[i] = int(sh.stroke_join)
+        caps[i] = int(sh.stroke_cap)
+        miters[i] = sh.stroke_miter_limit
+        if isinstance(g, Circle):
+            kinds[i] = SHAPE_CIRCLE
+            params[i] = [g.center[0], g.center[1], g.radius, 0.0]
+        elif isinstance(g, Ellipse):
+            kinds[i] = SHAPE_ELLIPSE
+            params[i] = [g.center[0], g.center[1], g.radius[0], g.radius[1]]
+        elif isinstance(g, Rect):
+            kinds[i] = SHAPE_RECT
+            params[i] = [g.min[0], g.min[1], g.max[0], g.max[1]]
+        elif isinstance(g, PathGeometry):
+            p = g.path
+            kinds[i] = SHAPE_PATH
+            ctrl_off[i] = len(ncp)
+            ctrl_cnt[i] = len(p.num_control_points)
+            pt_off[i] = len(pts) // 2
+            pt_cnt[i] = len(p.points)
+            ncp += [int(c) for c in p.num_control_points]
+            for q in p.points:
+                pts += [float(q[0]), float(q[1])]
+            f = 0
+            if p.is_closed:
+                f |= PATH_CLOSED
+            if p.use_distance_approx:
+                f |= PATH_DISTANCE_APPROX
+            if p.thickness is not None:
+                f |= PATH_HAS_THICKNESS
+                any_thick = True
+                t = list(p.thickness)[: len(p.points)]
+                t += [0.0] * (len(p.points) - len(t))
+                thick += t
+            else:
+                thick += [0.0] * len(p.points)
+            flags[i] = f
+        else:
+            raise TypeError(f"unsupported geometry {type(g)!r}")
+
+    ng = len(scene.groups)
+    g_off = np.zeros(ng, np.uint32)
+    g_cnt = np.zeros(ng, np.uint32)
+    g_ids: List[int] = []
+    g_rule = np.zeros(ng, np.uint32)
+    g_s2c = np.zeros((ng, 9), np.float32)
+    g_c2s = np.zeros((ng, 9), np.float32)
+    g_fill = np.full(ng, -1, np.int32)
+    g_stroke = np.full(ng, -1, np.int32)
+    p_kind: List[int] = []
+    p_params: List[List[float]] = []
+    p_soff: List[int] = []
+    p_scnt: List[int] = []
+    s_off: List[float] = []
+    s_col: List[float] = []
+    paint_of = {}
+    for gi, grp in enumerate(scene.groups):
+        g_off[gi] = len(g_ids)
+        g_cnt[gi] = len(grp.shape_indices)
+        g_ids += [int(s) for s in grp.shape_indices]
+        g_rule[gi] = int(grp.fill_rule)
+        g_s2c[gi] = grp.shape_to_canvas.flat()
+        g_c2s[gi] = grp.canvas_to_shape.flat()
+        for which, paint, arr in (("stroke", grp.stroke, g_stroke), ("fill", grp.fill, g_fill)):
+            if paint is None:
+                continue
+            k, prm, stops = _paint_record(paint)
+            arr[gi] = len(p_kind)
+            paint_of[(gi, which)] = len(p_kind)
+            p_kind.append(k)
+            p_params.append(prm)
+            p_soff.append(len(s_off))
+            p_scnt.append(len(stops))
+            for st in stops:
+                s_off.append(st.offset)
+                s_col += [st.color.r, st.color.g, st.color.b, st.color.a]
+
+    arrays = dict(
+        kinds=kinds, params=params.reshape(-1), xforms=xforms.reshape(-1), sw=sw, joins=joins, caps=caps,
+        miters=miters, ctrl_off=ctrl_off, ctrl_cnt=ctrl_cnt, pt_off=pt_off, pt_cnt=pt_cnt, flags=flags,
+        ncp=np.asarray(ncp if ncp else [0], np.uint8), pts=np.asarray(pts if pts else [0.0, 0.0], np.float32),
+        thick=np.asarray(thick if thick else [0.0], np.float32),
+        g_off=g_off, g_cnt=g_cnt, g_ids=np.asarray(g_ids if g_ids else [0], np.uint32), g_rule=g_rule,
+        g_s2c=g_s2c.reshape(-1), g_c2s=g_c2s.reshape(-1), g_fill=g_fill, g_stroke=g_stroke,
+        p_kind=np.asarray(p_kind if p_kind else [0], np.uint32),
+        p_params=np.asarray(p_params if p_params else [[0, 0, 0, 0]], np.float32).reshape(-1),
+        p_soff=np.asarray(p_soff if p_soff else [0], np.uint32),
+        p_scnt=np.asarray(p_scnt if p_scnt else [0], np.uint32),
+        s_off=np.asarray(s_off if s_off else [0.0], np.float32),
+        s_col=np.asarray(s_col if s_col else [0.0] * 4, np.float32),
+    )
+    bg_img = None
+    if scene.background_image is not None:
+        bg_img = np.ascontiguousarray(np.asarray(scene.background_image, np.float32).reshape(-1))
+        arrays["bg_img"] = bg_img
+
+    d = SceneDesc()
+    d.width, d.height = int(scene.width), int(scene.height)
+    for k, v in enumerate(scene.background.to_tuple()):
+        d.background[k] = float(v)
+    d.background_image = _ptr(bg_img, C.c_float)
+    d.filter_type = int(scene.filter.filter_type)
+    d.filter_radius = float(scene.filter.radius)
+    d.num_shapes = ns
+    d.shape_kind = _ptr(arrays["kinds"], C.c_uint32)
+    d.shape_params = _ptr(arrays["params"], C.c_float)
+    d.shape_transform = _ptr(arrays["xforms"], C.c_float)
+    d.shape_stroke_width = _ptr(arrays["sw"], C.c_float)
+    d.shape_stroke_join = _ptr(arrays["joins"], C.c_uint32)
+    d.shape_stroke_cap = _ptr(arrays["caps"], C.c_uint32)
+    d.shape_miter_limit = _ptr(arrays["miters"], C.c_float)
+    d.path_ctrl_offset = _ptr(arrays["ctrl_off"], C.c_uint32)
+    d.path_ctrl_count = _ptr(arrays["ctrl_cnt"], C.c_uint32)
+    d.path_point_offset = _ptr(arrays["pt_off"], C.c_uint32)
+    d.path_point_count = _ptr(arrays["pt_cnt"], C.c_uint32)
+    d.path_flags = _ptr(arrays["flags"], C.c_uint32)
+    d.num_control_points = _ptr(arrays["ncp"], C.c_uint8)
+    d.points = _ptr(arrays["pts"], C.c_float)
+    d.thickness = _ptr(arrays["thick"], C.c_float) if any_thick else C.cast(None, _fp)
+    d.total_ctrl = len(ncp)
+    d.total_points = len(pts) // 2
+    d.num_groups = ng
+    d.group_shape_offset = _ptr(g_off, C.c_uint32)
+    d.group_shape_count = _ptr(g_cnt, C.c_uint32)
+    d.group_shape_ids = _ptr(arrays["g_ids"], C.c_uint32)
+    d.total_group_shapes = len(g_ids)
+    d.group_fill_rule = _ptr(g_rule, C.c_uint32)
+    d.group_shape_to_canvas = _ptr(arrays["g_s2c"], C.c_float)
+    d.group_canvas_to_shape = _ptr(arrays["g_c2s"], C.c_float)
+    d.group_fill_paint = _ptr(g_fill, C.c_int32)
+    d.group_stroke_paint = _ptr(g_stroke, C.c_int32)
+    d.num_paints = len(p_kind)
+    d.paint_kind = _ptr(arrays["p_kind"], C.c_uint32)
+    d.paint_params = _ptr(arrays["p_params"], C.c_float)
+    d.paint_stop_offset = _ptr(arrays["p_soff"], C.c_uint32)
+    d.paint_stop_count = _ptr(arrays["p_scnt"], C.c_uint32)
+    d.stop_offsets = _ptr(arrays["s_off"], C.c_float)
+    d.stop_colors = _ptr(arrays["s_col"], C.c_float)
+    d.total_stops = len(s_off)
+    return PackedScene(d, arrays, paint_of, [int(x) for x in pt_off], [int(x) for x in pt_cnt], p_soff, p_scnt)
+
+
+class GradBuffers:
+    """Host arrays behind a dvg_grads struct, sized from a packed scene."""
+
+    NAMES = ("d_shape_params", "d_shape_transform", "d_shape_stroke_width", "d_points", "d_thickness",
+             "d_group_transform", "d_paint_params", "d_stop_offsets", "d_stop_colors", "d_filter_radius",
+             "d_background", "d_background_image", "d_translation")
+
+    def __init__(self, packed: PackedScene, background_image: bool = False, translation: bool = False):
+        d = packed.desc
+        npix = int(d.width) * int(d.height)
+        sizes = dict(
+            d_shape_params=4 * d.num_shapes, d_shape_transform=9 * d.num_shapes,
+            d_shape_stroke_width=d.num_shapes, d_points=2 * d.total_points, d_thickness=d.total_points,
+            d_group_transform=9 * d.num_groups, d_paint_params=4 * d.num_paints, d_stop_offsets=d.total_stops,
+            d_stop_colors=4 * d.total_stops, d_filter_radius=1, d_background=4,
+            d_background_image=4 * npix if background_image else 0, d_translation=2 * npix if translation else 0,
+        )
+        self.arrays: Dict[str, Optional[np.ndarray]] = {}
+        self.c = GradsC()
+        for n in self.NAMES:
+            sz = sizes[n]
+            if n in ("d_background_image", "d_translation") and sz == 0:
+                self.arrays[n] = None
+                setattr(self.c, n, C.cast(None, _fp))
+                continue
+            a = np.zeros(max(int(sz), 1), np.float32)
+            self.arrays[n] = a
+            setattr(self.c, n, _ptr(a, C.c_float))
+
+    def __getitem__(self, k: str) -> Optional[np.ndarray]:
+        return self.arrays[k]
+
+    def flat(self) -> np.ndarray:
+        """All gradient values concatenated (for norms / relative-error checks)."""
+        parts = [a for a in self.arrays.values() if a is not None]
+        return np.concatenate(parts) if parts else np.zeros(0, np.float32)
+
+
+@dataclass
+class DShape:
+    geometry: dict
+    transform: np.ndarray
+    stroke_width: float
+
+
+@dataclass
+class DShapeGroup:
+    shape_to_canvas: np.ndarray
+    fill: Optional[dict]
+    stroke: Optional[dict]
+
+
+@dataclass
+class SceneGrad:
+    """src/grad.rs:113-126, with numpy leaves."""
+
+    shapes: List[DShape]
+    shape_groups: List[DShapeGroup]
+    filter_radius: float
+    background: np.ndarray
+    background_image: Optional[np.ndarray]
+    translation: Optional[np.ndarray]
+    buffers: GradBuffers
+
+
+def _paint_grad(kind_paint, buf: GradBuffers, pi: int, soff: int, scnt: int) -> dict:
+    pp = buf["d_paint_params"][4 * pi: 4 * pi + 4].copy()
+    stops = [dict(offset=float(buf["d_stop_offsets"][soff + k]), color=buf["d_stop_colors"][4 * (soff + k): 4 * (soff + k) + 4].copy())
+             for k in range(scnt)]
+    if isinstance(kind_paint, Color):
+        return dict(kind="solid", color=pp)
+    if isinstance(kind_paint, LinearGradient):
+        return dict(kind="linear", start=pp[:2], end=pp[2:], stops=stops)
+    return dict(kind="radial", center=pp[:2], radius=pp[2:], stops=stops)
+
+
+def unflatten_grads(scene: Scene, packed: PackedScene, buf: GradBuffers) -> SceneGrad:
+    shapes = []
+    for i, sh in enumerate(scene.shapes):
+        g = sh.geometry
+        sp = buf["d_shape_params"][4 * i: 4 * i + 4]
+        if isinstance(g, Circle):
+            geo = dict(kind="circle", center=sp[:2].copy(), radius=float(sp[2]))
+        elif isinstance(g, Ellipse):
+            geo = dict(kind="ellipse", center=sp[:2].copy(), radius=sp[2:].copy())
+        elif isinstance(g, Rect):
+            geo = dict(kind="rect", min=sp[:2].copy(), max=sp[2:].copy())
+        else:
+            o, n = packed.path_point_offset[i], packed.path_point_count[i]
+            pts = buf["d_points"][2 * o: 2 * (o + n)].reshape(-1, 2).copy()
+            th = buf["d_thickness"][o: o + n].copy() if g.path.thickness is not None else None
+            geo = dict(kind="path", points=pts, thickness=th)
+        shapes.append(DShape(geo, buf["d_shape_transform"][9 * i: 9 * i + 9].reshape(3, 3).copy(),
+                             float(buf["d_shape_stroke_width"][i])))
+    groups = []
+    for gi, grp in enumerate(scene.groups):
+        fill = stroke = None
+        if grp.fill is not None:
+            pi = packed.paint_of[(gi, "fill")]
+            fill = _paint_grad(grp.fill, buf, pi, packed.stop_offset[pi], packed.stop_count[pi])
+        if grp.stroke is not None:
+            pi = packed.paint_of[(gi, "stroke")]
+            stroke = _paint_grad(grp.stroke, buf, pi, packed.stop_offset[pi], packed.stop_count[pi])
+        groups.append(DShapeGroup(buf["d_group_transform"][9 * gi: 9 * gi + 9].reshape(3, 3).copy(), fill, stroke))
+    bgi = buf["d_background_image"]
+    tr = buf["d_translation"]
+    return SceneGrad(shapes, groups, float(buf["d_filter_radius"][0]), buf["d_background"].copy(),
+                     None if bgi is None else bgi.copy(), None if tr is None else tr.copy(), buf)

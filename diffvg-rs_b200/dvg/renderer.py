@@ -1,0 +1,270 @@
+"""``Renderer`` over the C ABI of libdvg_b200.so (include/dvg.h).
+
+Mirrors the crate's ``Renderer`` (src/renderer/renderer.rs:20-564):
+``Renderer(device).render(scene, options) -> Image`` and
+``render_backward(scene, options, backward_options, d_render_image, d_sdf_image) -> SceneGrad``.
+Errors raise ``RenderError`` with the crate's kinds (``InvalidScene``,
+``Launch``).  There is no CPU fallback: without the CUDA library or a device
+the constructor raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from .abi import (
+    BackwardOptionsC,
+    GradBuffers,
+    GradsC,
+    PackedScene,
+    RenderOptionsC,
+    SceneDesc,
+    backward_options_c,
+    pack_scene,
+    render_options_c,
+    unflatten_grads,
+)
+from .scene import BackwardOptions, RenderOptions, Scene
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "libdvg_b200.so")
+
+DVG_OK, DVG_ERR_INVALID_SCENE, DVG_ERR_LAUNCH, DVG_ERR_DEVICE_LIMIT = 0, 1, 2, 3
+DVG_ERR_INVALID_ARGUMENT, DVG_ERR_OUT_OF_MEMORY, DVG_ERR_NO_DEVICE = 4, 5, 6
+
+EXPORTED = (
+    "dvg_abi_version", "dvg_last_error", "dvg_context_create", "dvg_context_destroy", "dvg_scene_upload",
+    "dvg_scene_destroy", "dvg_render_host", "dvg_render_device", "dvg_render_backward_host",
+    "dvg_render_backward_device", "dvg_render", "dvg_render_backward", "dvg_fwd_bwd_l2_device",
+    "dvg_context_launch_count", "dvg_context_stream",
+)
+
+
+class RenderError(RuntimeError):
+    """RenderError (src/renderer/types.rs:83-88); ``kind`` is 'InvalidScene', 'Launch', ..."""
+
+    KINDS = {DVG_ERR_INVALID_SCENE: "InvalidScene", DVG_ERR_LAUNCH: "Launch", DVG_ERR_DEVICE_LIMIT: "DeviceLimit",
+             DVG_ERR_INVALID_ARGUMENT: "InvalidArgument", DVG_ERR_OUT_OF_MEMORY: "OutOfMemory",
+             DVG_ERR_NO_DEVICE: "NoDevice"}
+
+    def __init__(self, status: int, message: str):
+        self.status = status
+        self.kind = self.KINDS.get(status, f"Status{status}")
+        super().__init__(f"{self.kind}: {message}")
+
+
+_lib: Optional[C.CDLL] = None
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise OSError(f"{path} is missing: build it with `make -C diffvg-rs_b200` (nvcc, sm_100a)")
+    L = C.CDLL(path)
+    D = C.POINTER(SceneDesc)
+    R = C.POINTER(RenderOptionsC)
+    B = C.POINTER(BackwardOptionsC)
+    Gp = C.POINTER(GradsC)
+    fp = C.POINTER(C.c_float)
+    vp = C.c_void_p
+    L.dvg_abi_version.restype = C.c_uint32
+    L.dvg_last_error.restype = C.c_char_p
+    L.dvg_context_create.argtypes = [C.c_int, C.POINTER(vp)]
+    L.dvg_context_destroy.argtypes = [vp]
+    L.dvg_context_destroy.restype = None
+    L.dvg_scene_upload.argtypes = [vp, D, C.POINTER(vp)]
+    L.dvg_scene_destroy.argtypes = [vp]
+    L.dvg_scene_destroy.restype = None
+    L.dvg_render_host.argtypes = [vp, vp, R, fp]
+    L.dvg_render_device.argtypes = [vp, vp, R, vp]
+    L.dvg_render_backward_host.argtypes = [vp, vp, R, B, fp, fp, Gp]
+    L.dvg_render_backward_device.argtypes = [vp, vp, R, B, vp, vp, Gp]
+    L.dvg_render.argtypes = [vp, D, R, fp]
+    L.dvg_render_backward.argtypes = [vp, D, R, B, fp, fp, Gp]
+    L.dvg_fwd_bwd_l2_device.argtypes = [vp, vp, R, B, vp, vp, vp, Gp]
+    L.dvg_context_launch_count.argtypes = [vp]
+    L.dvg_context_launch_count.restype = C.c_uint64
+    L.dvg_context_stream.argtypes = [vp]
+    L.dvg_context_stream.restype = vp
+    for name in ("dvg_context_create", "dvg_scene_upload", "dvg_render_host", "dvg_render_device",
+                 "dvg_render_backward_host", "dvg_render_backward_device", "dvg_render", "dvg_render_backward",
+                 "dvg_fwd_bwd_l2_device"):
+        getattr(L, name).restype = C.c_int
+    _lib = L
+    return L
+
+
+def _check(status: int) -> None:
+    if status != DVG_OK:
+        msg = load_library().dvg_last_error()
+        raise RenderError(status, msg.decode() if msg else "")
+
+
+def _fp(a: Optional[np.ndarray]):
+    if a is None:
+        return C.cast(None, C.POINTER(C.c_float))
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+@dataclass
+class Image:
+    """Image (src/renderer/types.rs:43-50): linear RGBA, row-major."""
+
+    width: int
+    height: int
+    pixels: np.ndarray  # float32 [height, width, 4]
+
+
+class DeviceGrads:
+    """dvg_grads pointing at caller-owned device buffers (torch tensors)."""
+
+    def __init__(self, packed: PackedScene, torch_device, translation: bool = False):
+        import torch
+
+        d = packed.desc
+        npix = int(d.width) * int(d.height)
+        sizes = dict(
+            d_shape_params=4 * d.num_shapes, d_shape_transform=9 * d.num_shapes,
+            d_shape_stroke_width=d.num_shapes, d_points=2 * d.total_points, d_thickness=d.total_points,
+            d_group_transform=9 * d.num_groups, d_paint_params=4 * d.num_paints, d_stop_offsets=d.total_stops,
+            d_stop_colors=4 * d.total_stops, d_filter_radius=1, d_background=4,
+            d_background_image=4 * npix if packed.desc.background_image else 0,
+            d_translation=2 * npix if translation else 0,
+        )
+        self.tensors = {}
+        self.c = GradsC()
+        for n in GradBuffers.NAMES:
+            sz = int(sizes[n])
+            if n in ("d_background_image", "d_translation") and sz == 0:
+                setattr(self.c, n, C.cast(None, C.POINTER(C.c_float)))
+                continue
+            t = torch.zeros(max(sz, 1), dtype=torch.float32, device=torch_device)
+            self.tensors[n] = t
+            setattr(self.c, n, C.cast(C.c_void_p(t.data_ptr()), C.POINTER(C.c_float)))
+
+    def flat(self):
+        import torch
+
+        return torch.cat([t for t in self.tensors.values()])
+
+
+class UploadedScene:
+    """A scene prepared and resident in HBM (dvg_scene_upload)."""
+
+    def __init__(self, renderer: "Renderer", scene: Scene):
+        self.renderer = renderer
+        self.scene = scene
+        self.packed = pack_scene(scene)
+        self.handle = C.c_void_p()
+        _check(renderer.lib.dvg_scene_upload(renderer.ctx, self.packed.ref(), C.byref(self.handle)))
+
+    def close(self) -> None:
+        if self.handle:
+            self.renderer.lib.dvg_scene_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def render_host(self, options: RenderOptions) -> np.ndarray:
+        out = np.zeros((self.scene.height, self.scene.width, 4), np.float32)
+        o = render_options_c(options)
+        _check(self.renderer.lib.dvg_render_host(self.renderer.ctx, self.handle, C.byref(o), _fp(out)))
+        return out
+
+    def render_device(self, options: RenderOptions, out_ptr: int) -> None:
+        o = render_options_c(options)
+        _check(self.renderer.lib.dvg_render_device(self.renderer.ctx, self.handle, C.byref(o), C.c_void_p(out_ptr)))
+
+    def backward_device(self, options: RenderOptions, bopts: Optional[BackwardOptions], d_render_ptr: int,
+                        grads: DeviceGrads) -> None:
+        o = render_options_c(options)
+        b = backward_options_c(bopts)
+        _check(self.renderer.lib.dvg_render_backward_device(self.renderer.ctx, self.handle, C.byref(o), C.byref(b),
+                                                            C.c_void_p(d_render_ptr), None, C.byref(grads.c)))
+
+    def fwd_bwd_l2_device(self, options: RenderOptions, bopts: Optional[BackwardOptions], target_ptr: int,
+                          out_ptr: Optional[int], loss_ptr: Optional[int], grads: DeviceGrads) -> None:
+        o = render_options_c(options)
+        b = backward_options_c(bopts)
+        _check(self.renderer.lib.dvg_fwd_bwd_l2_device(
+            self.renderer.ctx, self.handle, C.byref(o), C.byref(b), C.c_void_p(target_ptr),
+            C.c_void_p(out_ptr) if out_ptr else None, C.c_void_p(loss_ptr) if loss_ptr else None, C.byref(grads.c)))
+
+
+class Renderer:
+    """Renderer::new / with_device (src/renderer/renderer.rs:25-36) on a CUDA device."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        self.ctx = C.c_void_p()
+        _check(self.lib.dvg_context_create(int(device), C.byref(self.ctx)))
+        self.device = device
+
+    def close(self) -> None:
+        if self.ctx:
+            self.lib.dvg_context_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def launch_count(self) -> int:
+        return int(self.lib.dvg_context_launch_count(self.ctx))
+
+    @property
+    def stream_handle(self) -> int:
+        return int(self.lib.dvg_context_stream(self.ctx) or 0)
+
+    def upload(self, scene: Scene) -> UploadedScene:
+        return UploadedScene(self, scene)
+
+    def render(self, scene: Scene, options: RenderOptions = None) -> Image:
+        """Renderer::render (src/renderer/renderer.rs:39-545)."""
+        options = options or RenderOptions()
+        if scene.background_image is not None:
+            if np.asarray(scene.background_image).size != scene.width * scene.height * 4:
+                raise RenderError(DVG_ERR_INVALID_SCENE, "background image size mismatch")
+        if scene.width == 0 or scene.height == 0:
+            return Image(scene.width, scene.height, np.zeros((0,), np.float32))
+        packed = pack_scene(scene)
+        out = np.zeros((scene.height, scene.width, 4), np.float32)
+        o = render_options_c(options)
+        _check(self.lib.dvg_render(self.ctx, packed.ref(), C.byref(o), _fp(out)))
+        return Image(scene.width, scene.height, out)
+
+    def render_backward(self, scene: Scene, options: RenderOptions = None,
+                        backward_options: Optional[BackwardOptions] = None,
+                        d_render_image: Optional[np.ndarray] = None, d_sdf_image: Optional[np.ndarray] = None):
+        """Renderer::render_backward (src/renderer/renderer.rs:548-564) -> SceneGrad."""
+        options = options or RenderOptions()
+        bopts = backward_options or BackwardOptions()
+        npix = scene.width * scene.height
+        if d_render_image is not None and np.asarray(d_render_image).size != npix * 4:
+            raise RenderError(DVG_ERR_INVALID_SCENE, "d_render_image size mismatch")
+        if d_sdf_image is not None and np.asarray(d_sdf_image).size != npix:
+            raise RenderError(DVG_ERR_INVALID_SCENE, "d_sdf_image size mismatch")
+        packed = pack_scene(scene)
+        has_bg = d_render_image is not None and scene.background_image is not None
+        buf = GradBuffers(packed, background_image=has_bg, translation=bopts.compute_translation)
+        dr = None if d_render_image is None else np.ascontiguousarray(np.asarray(d_render_image, np.float32).reshape(-1))
+        ds = None if d_sdf_image is None else np.ascontiguousarray(np.asarray(d_sdf_image, np.float32).reshape(-1))
+        o = render_options_c(options)
+        b = backward_options_c(bopts)
+        _check(self.lib.dvg_render_backward(self.ctx, packed.ref(), C.byref(o), C.byref(b), _fp(dr), _fp(ds),
+                                            C.byref(buf.c)))
+        return unflatten_grads(scene, packed, buf)

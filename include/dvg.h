@@ -1,0 +1,237 @@
+/*
+ * dvg.h — C ABI of the B200-native differentiable vector-graphics rasteriser.
+ *
+ * This is the drop-in boundary for the render / backward hot path of the
+ * diffvg-rs crate.  Every entry point takes plain pointers and sizes; no
+ * torch or C++ types cross it.  Each declaration names the reference
+ * interface it replaces (file:line inside the diffvg-rs crate).
+ *
+ * Conventions
+ *   - A scene is described by dvg_scene_desc: structure-of-arrays host
+ *     buffers that mirror the crate's Scene / ShapeGroup / Shape / Path /
+ *     Paint types (src/scene.rs:7-291, src/geometry.rs:78-104) with integer
+ *     indices instead of nested Rust enums.
+ *   - Matrices are the crate's Mat3 (src/math.rs:143-146): 9 floats,
+ *     row-major, m[r][c] at index 3*r+c.
+ *   - Colours are linear, non-premultiplied RGBA, as in Color (src/color.rs).
+ *   - Entry points return dvg_status.  On error, dvg_last_error() gives a
+ *     thread-local message; DVG_ERR_INVALID_SCENE carries the same reason
+ *     strings as RenderError::InvalidScene (src/renderer/types.rs:83-88).
+ *   - Calls on one context are serialised on that context's CUDA stream.
+ *     A context may be used from one host thread at a time.
+ */
+#ifndef DVG_H
+#define DVG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DVG_ABI_VERSION 1
+
+typedef enum dvg_status {
+    DVG_OK = 0,
+    DVG_ERR_INVALID_SCENE = 1,    /* RenderError::InvalidScene */
+    DVG_ERR_LAUNCH = 2,           /* RenderError::Launch (CUDA launch / runtime error) */
+    DVG_ERR_DEVICE_LIMIT = 3,     /* a bounded device loop hit its cap; result not written */
+    DVG_ERR_INVALID_ARGUMENT = 4, /* NULL pointer, bad enum, size mismatch in the call itself */
+    DVG_ERR_OUT_OF_MEMORY = 5,
+    DVG_ERR_NO_DEVICE = 6
+} dvg_status;
+
+/* Shape kinds: same ids as the crate's GPU constants (src/gpu/constants.rs:27-34). */
+enum { DVG_SHAPE_CIRCLE = 0, DVG_SHAPE_RECT = 1, DVG_SHAPE_PATH = 2, DVG_SHAPE_ELLIPSE = 3 };
+/* Paint kinds (src/gpu/constants.rs:36-43). */
+enum { DVG_PAINT_NONE = 0, DVG_PAINT_SOLID = 1, DVG_PAINT_LINEAR = 2, DVG_PAINT_RADIAL = 3 };
+/* FilterType (src/scene.rs:6-28); DVG_FILTER_GAUSSIAN is an addition of this library. */
+enum { DVG_FILTER_BOX = 0, DVG_FILTER_TENT = 1, DVG_FILTER_RADIAL_PARABOLIC = 2, DVG_FILTER_HANN = 3,
+       DVG_FILTER_GAUSSIAN = 4 };
+/* FillRule (src/scene.rs:47-63). */
+enum { DVG_FILL_NONZERO = 0, DVG_FILL_EVENODD = 1 };
+/* StrokeJoin / StrokeCap (src/scene.rs:66-107).  Only round joins/caps are rendered,
+ * as in the crate; the other values only widen bounds (miter) like the crate does. */
+enum { DVG_JOIN_MITER = 0, DVG_JOIN_BEVEL = 1, DVG_JOIN_ROUND = 2 };
+enum { DVG_CAP_BUTT = 0, DVG_CAP_SQUARE = 1, DVG_CAP_ROUND = 2 };
+/* Path flags. */
+enum { DVG_PATH_CLOSED = 1u, DVG_PATH_DISTANCE_APPROX = 2u, DVG_PATH_HAS_THICKNESS = 4u };
+/* Boundary-sampling random number generators. */
+enum { DVG_RNG_PCG32 = 0, DVG_RNG_PHILOX = 1 };
+
+/*
+ * Scene description (host memory).  Replaces the Scene value passed by
+ * reference to Renderer::render / render_backward (src/renderer/renderer.rs:39,548).
+ *
+ * shape_params per kind (Shape::geometry, src/scene.rs:151-180):
+ *   CIRCLE  : center.x, center.y, radius, 0
+ *   ELLIPSE : center.x, center.y, radius.x, radius.y
+ *   RECT    : min.x, min.y, max.x, max.y
+ *   PATH    : unused (geometry lives in the path_* arrays)
+ * paint_params per kind (Paint, src/scene.rs:109-149):
+ *   SOLID   : r, g, b, a
+ *   LINEAR  : start.x, start.y, end.x, end.y      (+ stops)
+ *   RADIAL  : center.x, center.y, radius.x, radius.y (+ stops)
+ * Each group's fill and stroke must reference distinct paint entries: paint
+ * gradients are returned per paint entry, which is how SceneGrad keeps one
+ * DPaint per group fill / stroke (src/grad.rs:95-102).
+ */
+typedef struct dvg_scene_desc {
+    uint32_t width, height;
+    float background[4];            /* Scene::background */
+    const float* background_image;  /* NULL, or width*height*4 floats (Scene::background_image) */
+    uint32_t filter_type;           /* Scene::filter.filter_type */
+    float filter_radius;            /* Scene::filter.radius */
+
+    uint32_t num_shapes;
+    const uint32_t* shape_kind;         /* [num_shapes] */
+    const float* shape_params;          /* [num_shapes*4] */
+    const float* shape_transform;       /* [num_shapes*9] Shape::transform */
+    const float* shape_stroke_width;    /* [num_shapes] Shape::stroke_width (a radius, as in the crate) */
+    const uint32_t* shape_stroke_join;  /* [num_shapes] or NULL (= round) */
+    const uint32_t* shape_stroke_cap;   /* [num_shapes] or NULL (= round) */
+    const float* shape_miter_limit;     /* [num_shapes] or NULL (= 4.0) */
+
+    /* Paths (Path, src/geometry.rs:78-89).  Indexed per shape; ignored for other kinds. */
+    const uint32_t* path_ctrl_offset;   /* [num_shapes] start in num_control_points */
+    const uint32_t* path_ctrl_count;    /* [num_shapes] number of segments */
+    const uint32_t* path_point_offset;  /* [num_shapes] start in points / thickness */
+    const uint32_t* path_point_count;   /* [num_shapes] */
+    const uint32_t* path_flags;         /* [num_shapes] DVG_PATH_* */
+    const uint8_t* num_control_points;  /* flat: 0 line, 1 quadratic, 2 cubic */
+    const float* points;                /* flat: 2 floats per point */
+    const float* thickness;             /* flat: 1 float per point, or NULL if no path has thickness */
+    uint32_t total_ctrl;                /* length of num_control_points */
+    uint32_t total_points;              /* number of points (points has 2*total_points floats) */
+
+    uint32_t num_groups;
+    const uint32_t* group_shape_offset; /* [num_groups] start in group_shape_ids */
+    const uint32_t* group_shape_count;  /* [num_groups] */
+    const uint32_t* group_shape_ids;    /* flat ShapeGroup::shape_indices */
+    uint32_t total_group_shapes;
+    const uint32_t* group_fill_rule;    /* [num_groups] */
+    const float* group_shape_to_canvas; /* [num_groups*9] */
+    const float* group_canvas_to_shape; /* [num_groups*9] */
+    const int32_t* group_fill_paint;    /* [num_groups] paint index or -1 */
+    const int32_t* group_stroke_paint;  /* [num_groups] paint index or -1 */
+
+    uint32_t num_paints;
+    const uint32_t* paint_kind;         /* [num_paints] */
+    const float* paint_params;          /* [num_paints*4] */
+    const uint32_t* paint_stop_offset;  /* [num_paints] start in stop arrays */
+    const uint32_t* paint_stop_count;   /* [num_paints] */
+    const float* stop_offsets;          /* flat */
+    const float* stop_colors;           /* flat RGBA */
+    uint32_t total_stops;
+} dvg_scene_desc;
+
+/* RenderOptions (src/renderer/types.rs:10-39). Defaults: aa 1, path_tolerance 0.5,
+ * 2x2 samples, seed 0, jitter 1, use_prefiltering 1. */
+typedef struct dvg_render_options {
+    float aa;
+    float path_tolerance;
+    uint32_t samples_x, samples_y;
+    uint32_t seed;
+    uint32_t jitter;
+    uint32_t use_prefiltering;
+} dvg_render_options;
+
+/* BackwardOptions (src/backward/render.rs:19-32) plus the boundary-sampling knobs. */
+typedef struct dvg_backward_options {
+    uint32_t compute_translation;
+    uint32_t boundary_samples;  /* 0 = width*height*spp, as the crate (src/renderer/backward_gpu.rs:396-398) */
+    uint32_t rng;               /* DVG_RNG_PCG32 (the crate's generator) or DVG_RNG_PHILOX */
+    uint32_t boundary_seed;     /* seed for the boundary pass; the crate uses RenderOptions::seed */
+    uint32_t boundary_seed_from_options; /* 1: use RenderOptions::seed (crate behaviour) */
+} dvg_backward_options;
+
+/*
+ * Gradient buffers (caller-owned, host or device memory depending on the call).
+ * Flattened SceneGrad (src/grad.rs:113-126); every pointer may be NULL when the
+ * caller does not want that part, except where noted.  Buffers are overwritten.
+ */
+typedef struct dvg_grads {
+    float* d_shape_params;       /* [num_shapes*4] DShapeGeometry (circle/ellipse/rect) */
+    float* d_shape_transform;    /* [num_shapes*9] DShape::transform */
+    float* d_shape_stroke_width; /* [num_shapes]   DShape::stroke_width */
+    float* d_points;             /* [total_points*2] DShapeGeometry::Path::points */
+    float* d_thickness;          /* [total_points] DShapeGeometry::Path::thickness */
+    float* d_group_transform;    /* [num_groups*9] DShapeGroup::shape_to_canvas */
+    float* d_paint_params;       /* [num_paints*4] DPaint colour / start,end / center,radius */
+    float* d_stop_offsets;       /* [total_stops] */
+    float* d_stop_colors;        /* [total_stops*4] */
+    float* d_filter_radius;      /* [1] DFilter::radius */
+    float* d_background;         /* [4] SceneGrad::background */
+    float* d_background_image;   /* [w*h*4] or NULL */
+    float* d_translation;        /* [w*h*2] or NULL */
+} dvg_grads;
+
+typedef struct dvg_context dvg_context;
+typedef struct dvg_scene dvg_scene;
+
+/* Version of this ABI (DVG_ABI_VERSION). */
+uint32_t dvg_abi_version(void);
+
+/* Thread-local description of the last error on this thread. */
+const char* dvg_last_error(void);
+
+/* Replaces Renderer::new / Renderer::with_device (src/renderer/renderer.rs:25-36):
+ * binds a CUDA device and creates the context's stream and scratch pool. */
+dvg_status dvg_context_create(int device, dvg_context** out);
+void dvg_context_destroy(dvg_context* ctx);
+
+/* Host preparation + upload.  Replaces prepare_scene / prepare_scene_backward and the
+ * buffer uploads (src/renderer/prepare.rs:114, src/renderer/prepare_backward.rs:45,
+ * src/renderer/renderer.rs:94-144).  The returned scene may be rendered many times. */
+dvg_status dvg_scene_upload(dvg_context* ctx, const dvg_scene_desc* desc, dvg_scene** out);
+void dvg_scene_destroy(dvg_scene* scene);
+
+/* Renderer::render (src/renderer/renderer.rs:39-545) on an uploaded scene.
+ * out_rgba: width*height*4 floats, un-premultiplied linear RGBA, row-major.
+ * *_host variants take host pointers and block until the result is copied back;
+ * *_device variants take device pointers, enqueue on the context stream and return. */
+dvg_status dvg_render_host(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
+                           float* out_rgba);
+dvg_status dvg_render_device(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
+                             float* out_rgba);
+
+/* Renderer::render_backward (src/renderer/renderer.rs:548-564 ->
+ * src/renderer/backward_gpu.rs:21-523) on an uploaded scene.
+ * d_render: width*height*4 floats or NULL; d_sdf must be NULL (the SDF path is not
+ * part of this library yet; passing it returns DVG_ERR_INVALID_ARGUMENT). */
+dvg_status dvg_render_backward_host(dvg_context* ctx, dvg_scene* scene,
+                                    const dvg_render_options* opts,
+                                    const dvg_backward_options* bopts,
+                                    const float* d_render, const float* d_sdf, dvg_grads* grads);
+dvg_status dvg_render_backward_device(dvg_context* ctx, dvg_scene* scene,
+                                      const dvg_render_options* opts,
+                                      const dvg_backward_options* bopts,
+                                      const float* d_render, const float* d_sdf, dvg_grads* grads);
+
+/* One-shot forms mirroring the crate's call shape exactly: scene description in,
+ * host image / host gradients out (upload, launch, read back, release). */
+dvg_status dvg_render(dvg_context* ctx, const dvg_scene_desc* desc, const dvg_render_options* opts,
+                      float* out_rgba);
+dvg_status dvg_render_backward(dvg_context* ctx, const dvg_scene_desc* desc,
+                               const dvg_render_options* opts, const dvg_backward_options* bopts,
+                               const float* d_render, const float* d_sdf, dvg_grads* grads);
+
+/* Forward + L2 loss + backward in one call on an uploaded scene (device pointers):
+ * loss = sum((render - target)^2); d_render = 2*(render - target).
+ * out_rgba (may be NULL), loss_out (device float, may be NULL).  No counterpart in
+ * the crate: it fuses the render -> loss -> render_backward sequence a caller runs. */
+dvg_status dvg_fwd_bwd_l2_device(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
+                                 const dvg_backward_options* bopts, const float* target_rgba,
+                                 float* out_rgba, float* loss_out, dvg_grads* grads);
+
+/* Number of kernels this library launched on the context since creation. */
+uint64_t dvg_context_launch_count(const dvg_context* ctx);
+
+/* The context's CUDA stream (a cudaStream_t) for callers that interleave their own work. */
+void* dvg_context_stream(dvg_context* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DVG_H */

@@ -1,0 +1,3080 @@
+// oracle.cpp — CPU oracle (test infrastructure only; see oracle.h).
+//
+// Restates the diffvg-rs crate's CPU arithmetic function by function.  Each
+// function names the crate file:line it follows.  Arithmetic is f32 where the
+// crate uses f32 and f64 where the crate casts to f64; the file is compiled
+// with -ffp-contract=off so no multiply-add is fused (Rust never fuses).
+// Where the crate has no CPU code (the forward image), the GPU pipeline
+// semantics of src/gpu/kernels/forward.rs are followed (see oracle_render).
+//
+// Parity: pinned by the crate's known-answer tests (tests/test_oracle_kat.py
+// restates src/distance/tests.rs and src/geometry.rs:509-519); render and
+// gradients are "parity unpinned" (no crate tests, crate not buildable here).
+
+#include "oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <thread>
+#include <vector>
+
+namespace orc {
+
+static const float PI_F = 3.14159265358979323846f;       // core::f32::consts::PI
+static const float FRAC_PI_2_F = 1.57079632679489661923f;  // core::f32::consts::FRAC_PI_2
+static const float INF_F = std::numeric_limits<float>::infinity();
+
+// ---------------------------------------------------------------- math (src/math.rs)
+struct V2 {
+    float x, y;
+};
+static inline V2 mk(float x, float y) { return V2{x, y}; }
+static inline V2 operator+(V2 a, V2 b) { return V2{a.x + b.x, a.y + b.y}; }
+static inline V2 operator-(V2 a, V2 b) { return V2{a.x - b.x, a.y - b.y}; }
+static inline V2 operator*(V2 a, float s) { return V2{a.x * s, a.y * s}; }
+static inline V2 operator/(V2 a, float s) { return V2{a.x / s, a.y / s}; }
+static inline V2& operator+=(V2& a, V2 b) {
+    a.x += b.x;
+    a.y += b.y;
+    return a;
+}
+static inline V2& operator-=(V2& a, V2 b) {
+    a.x -= b.x;
+    a.y -= b.y;
+    return a;
+}
+static inline bool operator==(V2 a, V2 b) { return a.x == b.x && a.y == b.y; }
+static inline float dot(V2 a, V2 b) { return a.x * b.x + a.y * b.y; }        // math.rs:24-26
+static inline float cross(V2 a, V2 b) { return a.x * b.y - a.y * b.x; }      // math.rs:29-31
+static inline float length_sq(V2 a) { return dot(a, a); }                    // math.rs:39-41
+static inline float length(V2 a) { return std::sqrt(length_sq(a)); }        // math.rs:34-36
+static inline V2 vmin(V2 a, V2 b) { return V2{std::fmin(a.x, b.x), std::fmin(a.y, b.y)}; }
+static inline V2 vmax(V2 a, V2 b) { return V2{std::fmax(a.x, b.x), std::fmax(a.y, b.y)}; }
+static inline V2 lerp(V2 a, V2 b, float t) {  // math.rs:54-56
+    return V2{a.x + (b.x - a.x) * t, a.y + (b.y - a.y) * t};
+}
+// Rust f32::clamp (panics on min>max, keeps NaN).
+static inline float clampf(float v, float lo, float hi) {
+    if (v < lo) v = lo;
+    if (v > hi) v = hi;
+    return v;
+}
+static inline double clampd(double v, double lo, double hi) {
+    if (v < lo) v = lo;
+    if (v > hi) v = hi;
+    return v;
+}
+// Rust `f as i32`: saturating, NaN -> 0.
+static inline int32_t to_i32(float f) {
+    if (std::isnan(f)) return 0;
+    if (f >= 2147483647.0f) return INT32_MAX;
+    if (f <= -2147483648.0f) return INT32_MIN;
+    return (int32_t)f;
+}
+
+struct V4 {
+    float x, y, z, w;
+};
+static inline float dot4(V4 a, V4 b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
+
+struct M3 {
+    float m[3][3];
+};
+static inline M3 identity3() {
+    M3 r;
+    std::memset(&r, 0, sizeof(r));
+    r.m[0][0] = r.m[1][1] = r.m[2][2] = 1.0f;
+    return r;
+}
+static inline M3 zero3() {
+    M3 r;
+    std::memset(&r, 0, sizeof(r));
+    return r;
+}
+static inline M3 mul3(const M3& a, const M3& b) {  // math.rs:185-195
+    M3 o;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c)
+            o.m[r][c] = a.m[r][0] * b.m[0][c] + a.m[r][1] * b.m[1][c] + a.m[r][2] * b.m[2][c];
+    return o;
+}
+static inline V2 xform_pt(const M3& t, V2 v) {  // math.rs:198-202
+    float x = t.m[0][0] * v.x + t.m[0][1] * v.y + t.m[0][2];
+    float y = t.m[1][0] * v.x + t.m[1][1] * v.y + t.m[1][2];
+    return V2{x, y};
+}
+static const float M3_EPS = 1.0e-6f;  // math.rs:6
+static inline bool is_identity(const M3& t) {  // math.rs:212-222
+    return std::fabs(t.m[0][0] - 1.0f) < M3_EPS && std::fabs(t.m[0][1]) < M3_EPS &&
+           std::fabs(t.m[0][2]) < M3_EPS && std::fabs(t.m[1][0]) < M3_EPS &&
+           std::fabs(t.m[1][1] - 1.0f) < M3_EPS && std::fabs(t.m[1][2]) < M3_EPS &&
+           std::fabs(t.m[2][0]) < M3_EPS && std::fabs(t.m[2][1]) < M3_EPS &&
+           std::fabs(t.m[2][2] - 1.0f) < M3_EPS;
+}
+static inline float max_scale(const M3& t) {  // math.rs:250-266
+    float sx = std::sqrt(t.m[0][0] * t.m[0][0] + t.m[1][0] * t.m[1][0]);
+    float sy = std::sqrt(t.m[0][1] * t.m[0][1] + t.m[1][1] * t.m[1][1]);
+    return std::fmax(sx, sy);
+}
+static inline bool inverse3(const M3& t, M3* out) {  // math.rs:269-290
+    float a = t.m[0][0], b = t.m[0][1], c = t.m[1][0], d = t.m[1][1];
+    float tx = t.m[0][2], ty = t.m[1][2];
+    float det = a * d - b * c;
+    if (std::fabs(det) < M3_EPS) return false;
+    float inv_det = 1.0f / det;
+    float m00 = d * inv_det, m01 = -b * inv_det, m10 = -c * inv_det, m11 = a * inv_det;
+    float m02 = -(m00 * tx + m01 * ty);
+    float m12 = -(m10 * tx + m11 * ty);
+    M3 r;
+    r.m[0][0] = m00; r.m[0][1] = m01; r.m[0][2] = m02;
+    r.m[1][0] = m10; r.m[1][1] = m11; r.m[1][2] = m12;
+    r.m[2][0] = 0.0f; r.m[2][1] = 0.0f; r.m[2][2] = 1.0f;
+    *out = r;
+    return true;
+}
+// distance/utils.rs:7-16 (identity shortcut; singular -> unchanged point)
+static inline V2 xform_inv_dist(const M3& t, V2 pt) {
+    if (is_identity(t)) return pt;
+    M3 inv;
+    if (inverse3(t, &inv)) return xform_pt(inv, pt);
+    return pt;
+}
+// backward/math.rs:131-135 (no identity shortcut; singular -> identity)
+static inline V2 xform_inv_bwd(const M3& t, V2 pt) {
+    M3 inv;
+    if (!inverse3(t, &inv)) inv = identity3();
+    return xform_pt(inv, pt);
+}
+
+// ---------------------------------------------------------------- scene model (src/scene.rs)
+struct Color {
+    float r, g, b, a;
+};
+struct Stop {
+    float offset;
+    Color color;
+};
+struct Paint {
+    uint32_t kind;  // DVG_PAINT_*
+    float p[4];
+    std::vector<Stop> stops;
+};
+struct PathG {  // geometry.rs:78-89
+    std::vector<uint8_t> ncp;
+    std::vector<V2> pts;
+    bool has_thick = false;
+    std::vector<float> thick;
+    bool closed = false;
+    bool approx = false;
+    uint32_t point_base = 0;  // offset of pts[0] in the flat description
+};
+struct Shape {  // scene.rs:184-197
+    uint32_t kind;
+    float prm[4];
+    PathG path;
+    M3 transform;
+    float stroke_width;
+    uint32_t join;
+    float miter;
+};
+struct Group {  // scene.rs:215-230
+    std::vector<size_t> shape_ids;
+    int fill = -1, stroke = -1;  // paint indices
+    uint32_t fill_rule = 0;
+    M3 s2c, c2s;
+};
+struct Scene {  // scene.rs:261-276
+    uint32_t w = 0, h = 0;
+    std::vector<Shape> shapes;
+    std::vector<Group> groups;
+    std::vector<Paint> paints;
+    std::vector<uint32_t> paint_stop_base;
+    Color bg{0, 0, 0, 0};
+    bool has_bg_img = false;
+    std::vector<float> bg_img;
+    uint32_t filter_type = 0;
+    float filter_radius = 0.5f;
+};
+
+static M3 load_m3(const float* p) {
+    M3 r;
+    for (int i = 0; i < 9; ++i) r.m[i / 3][i % 3] = p[i];
+    return r;
+}
+
+static Scene decode(const dvg_scene_desc* d) {
+    Scene s;
+    s.w = d->width;
+    s.h = d->height;
+    s.bg = Color{d->background[0], d->background[1], d->background[2], d->background[3]};
+    if (d->background_image) {
+        s.has_bg_img = true;
+        s.bg_img.assign(d->background_image, d->background_image + (size_t)d->width * d->height * 4);
+    }
+    s.filter_type = d->filter_type;
+    s.filter_radius = d->filter_radius;
+    s.shapes.resize(d->num_shapes);
+    for (uint32_t i = 0; i < d->num_shapes; ++i) {
+        Shape& sh = s.shapes[i];
+        sh.kind = d->shape_kind[i];
+        for (int k = 0; k < 4; ++k) sh.prm[k] = d->shape_params[4 * i + k];
+        sh.transform = load_m3(d->shape_transform + 9 * i);
+        sh.stroke_width = d->shape_stroke_width[i];
+        sh.join = d->shape_stroke_join ? d->shape_stroke_join[i] : (uint32_t)DVG_JOIN_ROUND;
+        sh.miter = d->shape_miter_limit ? d->shape_miter_limit[i] : 4.0f;
+        if (sh.kind == DVG_SHAPE_PATH) {
+            uint32_t co = d->path_ctrl_offset[i], cc = d->path_ctrl_count[i];
+            uint32_t po = d->path_point_offset[i], pc = d->path_point_count[i];
+            uint32_t fl = d->path_flags[i];
+            sh.path.ncp.assign(d->num_control_points + co, d->num_control_points + co + cc);
+            sh.path.pts.resize(pc);
+            for (uint32_t k = 0; k < pc; ++k)
+                sh.path.pts[k] = mk(d->points[2 * (po + k)], d->points[2 * (po + k) + 1]);
+            sh.path.closed = (fl & DVG_PATH_CLOSED) != 0;
+            sh.path.approx = (fl & DVG_PATH_DISTANCE_APPROX) != 0;
+            sh.path.has_thick = (fl & DVG_PATH_HAS_THICKNESS) != 0 && d->thickness != nullptr;
+            if (sh.path.has_thick) sh.path.thick.assign(d->thickness + po, d->thickness + po + pc);
+            sh.path.point_base = po;
+        }
+    }
+    s.paints.resize(d->num_paints);
+    s.paint_stop_base.resize(d->num_paints);
+    for (uint32_t i = 0; i < d->num_paints; ++i) {
+        Paint& p = s.paints[i];
+        p.kind = d->paint_kind[i];
+        for (int k = 0; k < 4; ++k) p.p[k] = d->paint_params[4 * i + k];
+        uint32_t so = d->paint_stop_offset ? d->paint_stop_offset[i] : 0;
+        uint32_t sc = d->paint_stop_count ? d->paint_stop_count[i] : 0;
+        s.paint_stop_base[i] = so;
+        for (uint32_t k = 0; k < sc; ++k) {
+            Stop st;
+            st.offset = d->stop_offsets[so + k];
+            const float* c = d->stop_colors + 4 * (so + k);
+            st.color = Color{c[0], c[1], c[2], c[3]};
+            p.stops.push_back(st);
+        }
+    }
+    s.groups.resize(d->num_groups);
+    for (uint32_t g = 0; g < d->num_groups; ++g) {
+        Group& gr = s.groups[g];
+        uint32_t so = d->group_shape_offset[g], sc = d->group_shape_count[g];
+        for (uint32_t k = 0; k < sc; ++k) gr.shape_ids.push_back(d->group_shape_ids[so + k]);
+        gr.fill = d->group_fill_paint[g];
+        gr.stroke = d->group_stroke_paint[g];
+        gr.fill_rule = d->group_fill_rule[g];
+        gr.s2c = load_m3(d->group_shape_to_canvas + 9 * g);
+        gr.c2s = load_m3(d->group_canvas_to_shape + 9 * g);
+    }
+    return s;
+}
+
+// ---------------------------------------------------------------- path helpers (src/path_utils.rs)
+static bool path_point(const PathG& p, size_t index, V2* out) {  // path_utils.rs:7-16
+    size_t total = p.pts.size();
+    if (total == 0) return false;
+    if (p.closed) {
+        *out = p.pts[index % total];
+        return true;
+    }
+    if (index >= total) return false;
+    *out = p.pts[index];
+    return true;
+}
+static bool path_point_radius(const PathG& p, size_t index, float default_radius, V2* pt,
+                              float* r) {  // path_utils.rs:19-41 (thickness_scale = 1)
+    if (!path_point(p, index, pt)) return false;
+    size_t total = p.pts.size();
+    size_t idx = p.closed ? index % total : index;
+    if (p.has_thick && idx < p.thick.size())
+        *r = p.thick[idx] * 1.0f;
+    else
+        *r = default_radius;
+    return true;
+}
+// distance/utils.rs:24-45
+static bool path_segment_points(const PathG& p, size_t point_id, uint8_t nc, V2* q, size_t* next) {
+    if (!path_point(p, point_id, &q[0])) return false;
+    if (!path_point(p, point_id + 1, &q[1])) return false;
+    if (nc == 0) {
+        q[2] = q[1];
+        q[3] = q[1];
+        *next = point_id + 1;
+        return true;
+    }
+    if (nc == 1) {
+        if (!path_point(p, point_id + 2, &q[2])) return false;
+        q[3] = q[2];
+        *next = point_id + 2;
+        return true;
+    }
+    if (nc == 2) {
+        if (!path_point(p, point_id + 2, &q[2])) return false;
+        if (!path_point(p, point_id + 3, &q[3])) return false;
+        *next = point_id + 3;
+        return true;
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------- polynomial roots (distance/utils.rs:48-123)
+static bool solve_quadratic(double a, double b, double c, double t[2]) {
+    const double eps = 1.0e-12;
+    if (std::fabs(a) < eps) {
+        if (std::fabs(b) < eps) return false;
+        double root = -c / b;
+        t[0] = root;
+        t[1] = root;
+        return true;
+    }
+    double discrim = b * b - 4.0 * a * c;
+    if (discrim < 0.0) return false;
+    double root = std::sqrt(discrim);
+    if (std::fabs(root) < eps) {
+        double r = -0.5 * b / a;
+        t[0] = r;
+        t[1] = r;
+        return true;
+    }
+    double q = (b < 0.0) ? -0.5 * (b - root) : -0.5 * (b + root);
+    if (std::fabs(q) < eps) {
+        double inv = 0.5 / a;
+        t[0] = (-b - root) * inv;
+        t[1] = (-b + root) * inv;
+    } else {
+        t[0] = q / a;
+        t[1] = c / q;
+    }
+    if (t[0] > t[1]) std::swap(t[0], t[1]);
+    return true;
+}
+static double cbrt_ref(double x) {  // distance/utils.rs:115-123
+    if (x > 0.0) return std::pow(x, 1.0 / 3.0);
+    if (x < 0.0) return -std::pow(-x, 1.0 / 3.0);
+    return 0.0;
+}
+static int solve_cubic(double a, double b, double c, double d, double t[3]) {
+    if (std::fabs(a) < 1.0e-6) {
+        double roots[2] = {0.0, 0.0};
+        if (solve_quadratic(b, c, d, roots)) {
+            t[0] = roots[0];
+            t[1] = roots[1];
+            return 2;
+        }
+        return 0;
+    }
+    b = b / a;
+    c = c / a;
+    d = d / a;
+    double q = (b * b - 3.0 * c) / 9.0;
+    double r = (2.0 * b * b * b - 9.0 * b * c + 27.0 * d) / 54.0;
+    if (r * r < q * q * q) {
+        double theta = std::acos(r / std::sqrt(q * q * q));
+        t[0] = -2.0 * std::sqrt(q) * std::cos(theta / 3.0) - b / 3.0;
+        t[1] = -2.0 * std::sqrt(q) * std::cos((theta + 2.0 * M_PI) / 3.0) - b / 3.0;
+        t[2] = -2.0 * std::sqrt(q) * std::cos((theta - 2.0 * M_PI) / 3.0) - b / 3.0;
+        return 3;
+    }
+    double a_root = (r > 0.0) ? -cbrt_ref(r + std::sqrt(r * r - q * q * q))
+                              : cbrt_ref(-r + std::sqrt(r * r - q * q * q));
+    double b_root = (std::fabs(a_root) > 1.0e-6) ? q / a_root : 0.0;
+    t[0] = (a_root + b_root) - b / 3.0;
+    return 1;
+}
+
+// ---------------------------------------------------------------- curve distance (distance/curve.rs)
+struct CP {  // (closest point, t, dist)
+    V2 cp;
+    float t;
+    float dist;
+};
+static inline void distance_to_segment(V2 pt, V2 a, V2 b, float* dist, V2* cp, float* t) {
+    V2 ab = b - a;  // curve.rs:10-21
+    float denom = dot(ab, ab);
+    if (denom <= 1.0e-10f) {
+        *dist = length(pt - a);
+        *cp = a;
+        *t = 0.0f;
+        return;
+    }
+    float tt = clampf(dot(pt - a, ab) / denom, 0.0f, 1.0f);
+    V2 c = a + ab * tt;
+    *dist = length(pt - c);
+    *cp = c;
+    *t = tt;
+}
+static void quadratic_closest_pt_approx(V2 p0, V2 p1, V2 p2, V2 pt, V2* cp_out, float* t_out) {
+    V2 b0 = p0 - pt, b1 = p1 - pt, b2 = p2 - pt;  // curve.rs:267-296
+    float a = cross(b0, b2);
+    float b = 2.0f * cross(b1, b0);
+    float d = 2.0f * cross(b2, b1);
+    float f = b * d - a * a;
+    V2 d21 = b2 - b1, d10 = b1 - b0, d20 = b2 - b0;
+    V2 gf = (d21 * b) + (d10 * d) + (d20 * a);
+    gf = gf * 2.0f;
+    gf = mk(gf.y, -gf.x);
+    float t = 0.0f;
+    float denom = dot(gf, gf);
+    if (denom > 1.0e-8f) {
+        V2 pp = gf * (-f / denom);
+        V2 d0p = b0 - pp;
+        float ap = cross(d0p, d20);
+        float bp = 2.0f * cross(d10, d0p);
+        float denom2 = 2.0f * a + b + d;
+        if (std::fabs(denom2) > 1.0e-8f) t = clampf((ap + bp) / denom2, 0.0f, 1.0f);
+    }
+    float tt = 1.0f - t;
+    *cp_out = p0 * (tt * tt) + p1 * (2.0f * tt * t) + p2 * (t * t);
+    *t_out = t;
+}
+static CP closest_point_quadratic(V2 pt, V2 p0, V2 p1, V2 p2, bool approx) {  // curve.rs:26-78
+    if (approx) {
+        V2 cp;
+        float t;
+        quadratic_closest_pt_approx(p0, p1, p2, pt, &cp, &t);
+        return CP{cp, t, length(pt - cp)};
+    }
+    float best_t = 0.0f;
+    V2 best_pt = p0;
+    float best_dist = length(pt - p0);
+    float dist_end = length(pt - p2);
+    if (dist_end < best_dist) {
+        best_dist = dist_end;
+        best_pt = p2;
+        best_t = 1.0f;
+    }
+    double ax = (double)(p0.x - 2.0f * p1.x + p2.x);
+    double ay = (double)(p0.y - 2.0f * p1.y + p2.y);
+    double bx = (double)(-p0.x + p1.x);
+    double by = (double)(-p0.y + p1.y);
+    double cx = (double)(p0.x - pt.x);
+    double cy = (double)(p0.y - pt.y);
+    double a = ax * ax + ay * ay;
+    double b = 3.0 * (ax * bx + ay * by);
+    double c = 2.0 * (bx * bx + by * by) + (ax * cx + ay * cy);
+    double d = bx * cx + by * cy;
+    double roots[3] = {0, 0, 0};
+    int num = solve_cubic(a, b, c, d, roots);
+    for (int i = 0; i < num; ++i) {
+        double t = roots[i];
+        if (t >= 0.0 && t <= 1.0) {
+            float t32 = (float)t;
+            float tt = 1.0f - t32;
+            V2 cp = (p0 * (tt * tt)) + (p1 * (2.0f * tt * t32)) + (p2 * (t32 * t32));
+            float dist = length(pt - cp);
+            if (dist < best_dist) {
+                best_dist = dist;
+                best_pt = cp;
+                best_t = t32;
+            }
+        }
+    }
+    return CP{best_pt, best_t, best_dist};
+}
+static CP closest_point_cubic_approx(V2 pt, V2 p0, V2 p1, V2 p2, V2 p3) {  // curve.rs:81-119
+    const int steps = 8;
+    float inv = 1.0f / (float)steps;
+    V2 prev = p0;
+    float prev_t = 0.0f;
+    V2 best_pt = p0;
+    float best_t = 0.0f;
+    float best_dist = length(pt - p0);
+    for (int i = 1; i <= steps; ++i) {
+        float t = (float)i * inv;
+        float tt = 1.0f - t;
+        float tt2 = tt * tt, t2 = t * t;
+        float a = tt2 * tt, b = 3.0f * tt2 * t, c = 3.0f * tt * t2, d = t2 * t;
+        V2 curr = mk(a * p0.x + b * p1.x + c * p2.x + d * p3.x, a * p0.y + b * p1.y + c * p2.y + d * p3.y);
+        float dist, seg_t;
+        V2 cp;
+        distance_to_segment(pt, prev, curr, &dist, &cp, &seg_t);
+        float local_t = prev_t + seg_t * (t - prev_t);
+        if (dist < best_dist) {
+            best_dist = dist;
+            best_pt = cp;
+            best_t = local_t;
+        }
+        prev = curr;
+        prev_t = t;
+    }
+    return CP{best_pt, best_t, best_dist};
+}
+static CP closest_point_cubic(V2 pt, V2 p0, V2 p1, V2 p2, V2 p3, bool approx) {  // curve.rs:124-264
+    if (approx) return closest_point_cubic_approx(pt, p0, p1, p2, p3);
+    float best_t = 0.0f;
+    V2 best_pt = p0;
+    float best_dist = length(pt - p0);
+    float dist_end = length(pt - p3);
+    if (dist_end < best_dist) {
+        best_dist = dist_end;
+        best_pt = p3;
+        best_t = 1.0f;
+    }
+    double ax = (double)(-p0.x + 3.0f * p1.x - 3.0f * p2.x + p3.x);
+    double ay = (double)(-p0.y + 3.0f * p1.y - 3.0f * p2.y + p3.y);
+    double bx = (double)(3.0f * p0.x - 6.0f * p1.x + 3.0f * p2.x);
+    double by = (double)(3.0f * p0.y - 6.0f * p1.y + 3.0f * p2.y);
+    double cx = (double)(-3.0f * p0.x + 3.0f * p1.x);
+    double cy = (double)(-3.0f * p0.y + 3.0f * p1.y);
+    double dx = (double)(p0.x - pt.x);
+    double dy = (double)(p0.y - pt.y);
+    double a = 3.0 * (ax * ax + ay * ay);
+    if (std::fabs(a) < 1.0e-10) return CP{best_pt, best_t, best_dist};
+    double b = 5.0 * (ax * bx + ay * by);
+    double c = 4.0 * (ax * cx + ay * cy) + 2.0 * (bx * bx + by * by);
+    double d = 3.0 * ((bx * cx + by * cy) + (ax * dx + ay * dy));
+    double e = (cx * cx + cy * cy) + 2.0 * (dx * bx + dy * by);
+    double f = dx * cx + dy * cy;
+    b = b / a;
+    c = c / a;
+    d = d / a;
+    e = e / a;
+    f = f / a;
+    double p1a = (2.0 / 5.0) * c - (4.0 / 25.0) * b * b;
+    double p1b = (3.0 / 5.0) * d - (3.0 / 25.0) * b * c;
+    double p1c = (4.0 / 5.0) * e - (2.0 / 25.0) * b * d;
+    double p1d = f - b * e / 25.0;
+    double q_root = -b / 5.0;
+    double p_roots[3] = {0, 0, 0};
+    int num_p = solve_cubic(p1a, p1b, p1c, p1d, p_roots);
+    double intervals[4] = {0, 0, 0, 0};
+    int num_intervals = 0;
+    if (q_root >= 0.0 && q_root <= 1.0) intervals[num_intervals++] = q_root;
+    for (int i = 0; i < num_p; ++i) intervals[num_intervals++] = p_roots[i];
+    for (int j = 1; j < num_intervals; ++j) {
+        int k = j;
+        while (k > 0 && intervals[k - 1] > intervals[k]) {
+            std::swap(intervals[k - 1], intervals[k]);
+            k -= 1;
+        }
+    }
+    auto eval_poly = [&](double t) { return ((((t + b) * t + c) * t + d) * t + e) * t + f; };
+    auto eval_deriv = [&](double t) {
+        return (((5.0 * t + 4.0 * b) * t + 3.0 * c) * t + 2.0 * d) * t + e;
+    };
+    double lower = 0.0;
+    for (int j = 0; j <= num_intervals; ++j) {
+        if (j < num_intervals && intervals[j] < 0.0) continue;
+        double upper = (j < num_intervals) ? std::fmin(intervals[j], 1.0) : 1.0;
+        double lb = lower, ub = upper;
+        double lb_eval = eval_poly(lb), ub_eval = eval_poly(ub);
+        if (lb_eval * ub_eval > 0.0) {
+            lower = upper;
+            continue;
+        }
+        if (lb_eval > ub_eval) {
+            std::swap(lb, ub);
+            std::swap(lb_eval, ub_eval);
+        }
+        double t = 0.5 * (lb + ub);
+        for (int it = 0; it < 20; ++it) {
+            if (!(t >= lb && t <= ub)) t = 0.5 * (lb + ub);
+            double value = eval_poly(t);
+            if (std::fabs(value) < 1.0e-5 || it == 19) break;
+            if (value > 0.0)
+                ub = t;
+            else
+                lb = t;
+            double derivative = eval_deriv(t);
+            t -= value / derivative;
+        }
+        if (t >= 0.0 && t <= 1.0) {
+            float t32 = (float)t;
+            float tt = 1.0f - t32;
+            V2 cp = (p0 * (tt * tt * tt)) + (p1 * (3.0f * tt * tt * t32)) +
+                    (p2 * (3.0f * tt * t32 * t32)) + (p3 * (t32 * t32 * t32));
+            float dist = length(pt - cp);
+            if (dist < best_dist) {
+                best_dist = dist;
+                best_pt = cp;
+                best_t = t32;
+            }
+        }
+        if (upper >= 1.0) break;
+        lower = upper;
+    }
+    return CP{best_pt, best_t, best_dist};
+}
+
+// ---------------------------------------------------------------- winding (distance/winding.rs:118-192)
+static int winding_number_segment(uint8_t kind, V2 p0, V2 p1, V2 p2, V2 p3, V2 pt) {
+    if (kind == 0) {
+        float dy = p1.y - p0.y;
+        if (std::fabs(dy) <= 1.0e-8f) return 0;
+        float t = (pt.y - p0.y) / dy;
+        if (t >= 0.0f && t <= 1.0f) {
+            float tp = p0.x - pt.x + t * (p1.x - p0.x);
+            if (tp >= 0.0f) return dy > 0.0f ? 1 : -1;
+        }
+        return 0;
+    }
+    if (kind == 1) {
+        double a = (double)(p0.y - 2.0f * p1.y + p2.y);
+        double b = (double)(-2.0f * p0.y + 2.0f * p1.y);
+        double c = (double)(p0.y - pt.y);
+        double roots[2] = {0, 0};
+        int num_roots = 0;
+        if (std::fabs(a) < 1.0e-12) {
+            if (std::fabs(b) > 1.0e-12) {
+                roots[0] = -c / b;
+                num_roots = 1;
+            }
+        } else if (solve_quadratic(a, b, c, roots)) {
+            num_roots = 2;
+        }
+        int winding = 0;
+        double ax = (double)(p0.x - 2.0f * p1.x + p2.x);
+        double bx = (double)(-2.0f * p0.x + 2.0f * p1.x);
+        double cx = (double)(p0.x - pt.x);
+        for (int i = 0; i < num_roots; ++i) {
+            double t = roots[i];
+            if (t >= 0.0 && t <= 1.0) {
+                double tp = ax * t * t + bx * t + cx;
+                if (tp > 0.0) {
+                    double deriv = 2.0 * a * t + b;
+                    winding += deriv > 0.0 ? 1 : -1;
+                }
+            }
+        }
+        return winding;
+    }
+    if (kind == 2) {
+        double a = (double)(-p0.y + 3.0f * p1.y - 3.0f * p2.y + p3.y);
+        double b = (double)(3.0f * p0.y - 6.0f * p1.y + 3.0f * p2.y);
+        double c = (double)(-3.0f * p0.y + 3.0f * p1.y);
+        double d = (double)(p0.y - pt.y);
+        double roots[3] = {0, 0, 0};
+        int num_roots = solve_cubic(a, b, c, d, roots);
+        double ax = (double)(-p0.x + 3.0f * p1.x - 3.0f * p2.x + p3.x);
+        double bx = (double)(3.0f * p0.x - 6.0f * p1.x + 3.0f * p2.x);
+        double cx = (double)(-3.0f * p0.x + 3.0f * p1.x);
+        double dx = (double)(p0.x - pt.x);
+        int winding = 0;
+        for (int i = 0; i < num_roots; ++i) {
+            double t = roots[i];
+            if (t >= 0.0 && t <= 1.0) {
+                double tp = ax * t * t * t + bx * t * t + cx * t + dx;
+                if (tp > 0.0) {
+                    double deriv = 3.0 * a * t * t + 2.0 * b * t + c;
+                    winding += deriv > 0.0 ? 1 : -1;
+                }
+            }
+        }
+        return winding;
+    }
+    return 0;
+}
+static int winding_number_path(const PathG& p, V2 pt) {  // winding.rs:52-70
+    if (p.pts.empty()) return 0;
+    int winding = 0;
+    size_t point_id = 0;
+    for (uint8_t nc : p.ncp) {
+        V2 q[4];
+        size_t next;
+        if (!path_segment_points(p, point_id, nc, q, &next)) break;
+        winding += winding_number_segment(nc, q[0], q[1], q[2], q[3], pt);
+        point_id = next;
+    }
+    return winding;
+}
+
+// ---------------------------------------------------------------- shapes (distance/shape.rs)
+struct Bounds {  // distance/bvh.rs:70-114
+    V2 min, max;
+    static Bounds empty() { return Bounds{mk(INF_F, INF_F), mk(-INF_F, -INF_F)}; }
+    void include(const Bounds& o) {
+        min = vmin(min, o.min);
+        max = vmax(max, o.max);
+    }
+    V2 center() const { return (min + max) * 0.5f; }
+    V2 extent() const { return max - min; }
+    bool contains(V2 p) const { return p.x >= min.x && p.x <= max.x && p.y >= min.y && p.y <= max.y; }
+    float distance(V2 p) const {
+        float dx = std::fmax(std::fmax(min.x - p.x, 0.0f), p.x - max.x);
+        float dy = std::fmax(std::fmax(min.y - p.y, 0.0f), p.y - max.y);
+        return std::sqrt(dx * dx + dy * dy);
+    }
+};
+static Bounds bounds_from_points(const std::vector<V2>& pts) {  // path_utils.rs:107-115
+    Bounds b = Bounds::empty();
+    for (V2 p : pts) {
+        b.min = vmin(b.min, p);
+        b.max = vmax(b.max, p);
+    }
+    return b;
+}
+static Bounds inflate_bounds(Bounds b, float pad) {  // shape.rs:92-99
+    pad = std::fmax(pad, 0.0f);
+    return Bounds{mk(b.min.x - pad, b.min.y - pad), mk(b.max.x + pad, b.max.y + pad)};
+}
+static V2 ellipse_extents(const M3& t, float rx, float ry) {  // shape.rs:81-89
+    float m00 = t.m[0][0], m01 = t.m[0][1], m10 = t.m[1][0], m11 = t.m[1][1];
+    float ex = std::sqrt((m00 * rx) * (m00 * rx) + (m01 * ry) * (m01 * ry));
+    float ey = std::sqrt((m10 * rx) * (m10 * rx) + (m11 * ry) * (m11 * ry));
+    return mk(ex, ey);
+}
+static bool shape_geom_bounds(const Shape& s, Bounds* out) {  // shape.rs:17-59
+    const M3& t = s.transform;
+    if (s.kind == DVG_SHAPE_CIRCLE || s.kind == DVG_SHAPE_ELLIPSE) {
+        V2 c = xform_pt(t, mk(s.prm[0], s.prm[1]));
+        float rx = std::fabs(s.prm[2]);
+        float ry = s.kind == DVG_SHAPE_CIRCLE ? rx : std::fabs(s.prm[3]);
+        V2 ext = ellipse_extents(t, rx, ry);
+        *out = Bounds{mk(c.x - ext.x, c.y - ext.y), mk(c.x + ext.x, c.y + ext.y)};
+        return true;
+    }
+    if (s.kind == DVG_SHAPE_RECT) {
+        std::vector<V2> corners = {xform_pt(t, mk(s.prm[0], s.prm[1])), xform_pt(t, mk(s.prm[2], s.prm[1])),
+                                   xform_pt(t, mk(s.prm[2], s.prm[3])), xform_pt(t, mk(s.prm[0], s.prm[3]))};
+        *out = bounds_from_points(corners);
+        return true;
+    }
+    if (s.kind == DVG_SHAPE_PATH) {
+        if (s.path.pts.empty()) return false;
+        std::vector<V2> pts = s.path.pts;
+        if (!is_identity(t))  // path_utils.rs:88-104
+            for (auto& p : pts) p = xform_pt(t, p);
+        *out = bounds_from_points(pts);
+        return true;
+    }
+    return false;
+}
+static float max_stroke_radius(const Shape& s) {  // shape.rs:62-78
+    float stroke_scale = std::fmax(max_scale(s.transform), 0.0f);
+    float radius = std::fabs(s.stroke_width) * stroke_scale;
+    if (s.kind == DVG_SHAPE_PATH && s.path.has_thick) {
+        float mt = 0.0f;
+        for (float v : s.path.thick) mt = std::fmax(mt, std::fabs(v));
+        radius = std::fmax(radius, mt * stroke_scale);
+    }
+    if (radius > 0.0f && s.join == DVG_JOIN_MITER) radius *= std::fmax(s.miter, 1.0f);
+    return radius;
+}
+static bool shape_bounds(const Shape& s, Bounds* out) {  // shape.rs:9-14
+    Bounds g;
+    if (!shape_geom_bounds(s, &g)) return false;
+    *out = inflate_bounds(g, max_stroke_radius(s));
+    return true;
+}
+static V2 closest_point_circle(V2 c, float r, V2 pt) {  // shape.rs:106-113
+    V2 d = pt - c;
+    float len = length(d);
+    if (len <= 1.0e-8f) return mk(c.x + r, c.y);
+    return c + d * (r / len);
+}
+static V2 closest_point_ellipse(V2 c, V2 radius, V2 pt) {  // shape.rs:116-164
+    float rx = std::fabs(radius.x), ry = std::fabs(radius.y);
+    const float eps = 1.0e-6f;
+    if (rx < eps && ry < eps) return c;
+    if (rx < eps) return mk(c.x, c.y + clampf(pt.y - c.y, -ry, ry));
+    if (ry < eps) return mk(c.x + clampf(pt.x - c.x, -rx, rx), c.y);
+    float dx = pt.x - c.x, dy = pt.y - c.y;
+    if (std::fabs(dx) < eps && std::fabs(dy) < eps) return mk(c.x + rx, c.y);
+    float sign_x = dx < 0.0f ? -1.0f : 1.0f;
+    float sign_y = dy < 0.0f ? -1.0f : 1.0f;
+    dx = std::fabs(dx);
+    dy = std::fabs(dy);
+    float t = std::atan2(dy * rx, dx * ry);
+    const int max_iter = 20;
+    const float tol = 1.0e-6f;
+    for (int i = 0; i < max_iter; ++i) {
+        float s = std::sin(t), co = std::cos(t);
+        float g = rx * dx * s - ry * dy * co + (ry * ry - rx * rx) * s * co;
+        float g_t = rx * dx * co + ry * dy * s + (ry * ry - rx * rx) * (co * co - s * s);
+        if (std::fabs(g_t) < 1.0e-12f) break;
+        float next = clampf(t - g / g_t, 0.0f, FRAC_PI_2_F);
+        if (std::fabs(next - t) < tol) {
+            t = next;
+            break;
+        }
+        t = next;
+    }
+    float s = std::sin(t), co = std::cos(t);
+    return mk(c.x + sign_x * rx * co, c.y + sign_y * ry * s);
+}
+static V2 closest_point_rect(V2 mn, V2 mx, V2 pt) {  // shape.rs:167-185
+    bool inside = pt.x >= mn.x && pt.x <= mx.x && pt.y >= mn.y && pt.y <= mx.y;
+    if (!inside) return mk(clampf(pt.x, mn.x, mx.x), clampf(pt.y, mn.y, mx.y));
+    float dl = pt.x - mn.x, dr = mx.x - pt.x, db = pt.y - mn.y, dt = mx.y - pt.y;
+    if (dl <= dr && dl <= db && dl <= dt) return mk(mn.x, pt.y);
+    if (dr <= db && dr <= dt) return mk(mx.x, pt.y);
+    if (db <= dt) return mk(pt.x, mn.y);
+    return mk(pt.x, mx.y);
+}
+static float rect_signed_distance(V2 pt, V2 mn, V2 mx) {  // shape.rs:188-201
+    float dx = std::fmax(std::fmax(mn.x - pt.x, 0.0f), pt.x - mx.x);
+    float dy = std::fmax(std::fmax(mn.y - pt.y, 0.0f), pt.y - mx.y);
+    float outside = std::sqrt(dx * dx + dy * dy);
+    float inside = std::fmin(std::fmin(std::fmin(pt.x - mn.x, mx.x - pt.x), pt.y - mn.y), mx.y - pt.y);
+    return outside > 0.0f ? outside : -inside;
+}
+static float ellipse_signed_distance(V2 pt, V2 c, V2 radius) {  // shape.rs:204-212
+    float rx = std::fmax(std::fabs(radius.x), 1.0e-6f);
+    float ry = std::fmax(std::fabs(radius.y), 1.0e-6f);
+    V2 local = pt - c;
+    bool inside = (local.x / rx) * (local.x / rx) + (local.y / ry) * (local.y / ry) <= 1.0f;
+    V2 closest = closest_point_ellipse(c, mk(rx, ry), pt);
+    float dist = length(pt - closest);
+    return inside ? -dist : dist;
+}
+
+// ---------------------------------------------------------------- BVH (distance/bvh.rs)
+static const uint32_t BVH_NONE = 0xffffffffu;
+static const size_t BVH_LEAF_SIZE = 8;
+struct BvhNode {
+    Bounds bounds;
+    uint32_t left, right, start, count;
+};
+struct SegData {  // bvh.rs:130-154
+    size_t segment_index;
+    uint8_t kind;
+    V2 p0, p1, p2, p3;
+    float r0, r1, r2, r3;
+    Bounds bounds;
+};
+struct PathBvh {
+    std::vector<BvhNode> nodes;
+    std::vector<size_t> indices;
+    std::vector<SegData> segments;
+    bool approx = false;
+};
+struct BvhShape {
+    size_t shape_index;
+    Bounds bounds;
+    bool has_path_bvh = false;
+    PathBvh path_bvh;
+};
+struct GroupBvh {
+    std::vector<BvhNode> nodes;
+    std::vector<size_t> indices;
+    std::vector<BvhShape> shapes;
+};
+struct SceneBvh {
+    std::vector<GroupBvh> groups;
+};
+
+template <typename BoundsOf>
+static uint32_t build_node(std::vector<BvhNode>& nodes, BoundsOf bounds_of, std::vector<size_t>& idx,
+                           size_t start, size_t end) {  // bvh.rs:190-238 / 384-432
+    Bounds b = Bounds::empty();
+    for (size_t i = start; i < end; ++i) b.include(bounds_of(idx[i]));
+    size_t count = end - start;
+    uint32_t node_index = (uint32_t)nodes.size();
+    nodes.push_back(BvhNode{b, BVH_NONE, BVH_NONE, (uint32_t)start, (uint32_t)count});
+    if (count <= BVH_LEAF_SIZE) return node_index;
+    V2 ext = b.extent();
+    int axis = ext.x >= ext.y ? 0 : 1;
+    std::stable_sort(idx.begin() + start, idx.begin() + end, [&](size_t a, size_t c) {
+        V2 ca = bounds_of(a).center(), cb = bounds_of(c).center();
+        float va = axis == 0 ? ca.x : ca.y, vb = axis == 0 ? cb.x : cb.y;
+        return va < vb;
+    });
+    size_t mid = start + count / 2;
+    uint32_t l = build_node(nodes, bounds_of, idx, start, mid);
+    uint32_t r = build_node(nodes, bounds_of, idx, mid, end);
+    nodes[node_index].left = l;
+    nodes[node_index].right = r;
+    nodes[node_index].count = 0;
+    return node_index;
+}
+static Bounds segment_bounds(std::initializer_list<V2> pts, float pad) {  // shape.rs:102-105
+    Bounds b = Bounds::empty();
+    for (V2 p : pts) {
+        b.min = vmin(b.min, p);
+        b.max = vmax(b.max, p);
+    }
+    return inflate_bounds(b, pad);
+}
+static bool build_path_bvh(const Shape& s, PathBvh* out) {  // bvh.rs:241-381
+    if (s.kind != DVG_SHAPE_PATH) return false;
+    const PathG& p = s.path;
+    if (p.pts.empty()) return false;
+    float dr = s.stroke_width;
+    size_t point_id = 0;
+    std::vector<SegData> segs;
+    for (size_t si = 0; si < p.ncp.size(); ++si) {
+        uint8_t nc = p.ncp[si];
+        V2 q[4];
+        float r[4];
+        if (nc == 0) {
+            if (!path_point_radius(p, point_id, dr, &q[0], &r[0])) break;
+            if (!path_point_radius(p, point_id + 1, dr, &q[1], &r[1])) break;
+            segs.push_back(SegData{si, 0, q[0], q[1], q[1], q[1], r[0], r[1], r[1], r[1],
+                                   segment_bounds({q[0], q[1]}, std::fmax(r[0], r[1]))});
+            point_id += 1;
+        } else if (nc == 1) {
+            if (!path_point_radius(p, point_id, dr, &q[0], &r[0])) break;
+            if (!path_point_radius(p, point_id + 1, dr, &q[1], &r[1])) break;
+            if (!path_point_radius(p, point_id + 2, dr, &q[2], &r[2])) break;
+            segs.push_back(SegData{si, 1, q[0], q[1], q[2], q[2], r[0], r[1], r[2], r[2],
+                                   segment_bounds({q[0], q[1], q[2]}, std::fmax(std::fmax(r[0], r[1]), r[2]))});
+            point_id += 2;
+        } else if (nc == 2) {
+            if (!path_point_radius(p, point_id, dr, &q[0], &r[0])) break;
+            if (!path_point_radius(p, point_id + 1, dr, &q[1], &r[1])) break;
+            if (!path_point_radius(p, point_id + 2, dr, &q[2], &r[2])) break;
+            if (!path_point_radius(p, point_id + 3, dr, &q[3], &r[3])) break;
+            segs.push_back(SegData{si, 2, q[0], q[1], q[2], q[3], r[0], r[1], r[2], r[3],
+                                   segment_bounds({q[0], q[1], q[2], q[3]},
+                                                  std::fmax(std::fmax(std::fmax(r[0], r[1]), r[2]), r[3]))});
+            point_id += 3;
+        } else {
+            break;
+        }
+    }
+    if (segs.empty()) return false;
+    out->segments = segs;
+    out->indices.resize(segs.size());
+    for (size_t i = 0; i < segs.size(); ++i) out->indices[i] = i;
+    out->nodes.clear();
+    build_node(out->nodes, [&](size_t i) { return out->segments[i].bounds; }, out->indices, 0, segs.size());
+    out->approx = p.approx;
+    return true;
+}
+static GroupBvh build_group_bvh(const Scene& sc, const Group& g) {  // bvh.rs:156-187
+    GroupBvh gb;
+    for (size_t si : g.shape_ids) {
+        if (si >= sc.shapes.size()) continue;
+        const Shape& s = sc.shapes[si];
+        Bounds b;
+        if (shape_bounds(s, &b)) {
+            BvhShape bs;
+            bs.shape_index = si;
+            bs.bounds = b;
+            bs.has_path_bvh = build_path_bvh(s, &bs.path_bvh);
+            gb.shapes.push_back(bs);
+        }
+    }
+    gb.indices.resize(gb.shapes.size());
+    for (size_t i = 0; i < gb.shapes.size(); ++i) gb.indices[i] = i;
+    if (!gb.indices.empty())
+        build_node(gb.nodes, [&](size_t i) { return gb.shapes[i].bounds; }, gb.indices, 0, gb.indices.size());
+    return gb;
+}
+static SceneBvh build_scene_bvh(const Scene& sc) {  // bvh.rs:21-30
+    SceneBvh b;
+    for (const Group& g : sc.groups) b.groups.push_back(build_group_bvh(sc, g));
+    return b;
+}
+
+// ---------------------------------------------------------------- closest / within (distance/closest.rs)
+static float seg_radius(const SegData& s, float t) {  // closest.rs:66-79
+    if (s.kind == 0) return s.r0 + t * (s.r1 - s.r0);
+    float tt = 1.0f - t;
+    if (s.kind == 1) return tt * tt * s.r0 + 2.0f * tt * t * s.r1 + t * t * s.r2;
+    return tt * tt * tt * s.r0 + 3.0f * tt * tt * t * s.r1 + 3.0f * tt * t * t * s.r2 + t * t * t * s.r3;
+}
+static CP seg_closest(const SegData& s, V2 pt, bool approx) {
+    if (s.kind == 0) {
+        CP r;
+        distance_to_segment(pt, s.p0, s.p1, &r.dist, &r.cp, &r.t);
+        return r;
+    }
+    if (s.kind == 1) return closest_point_quadratic(pt, s.p0, s.p1, s.p2, approx);
+    return closest_point_cubic(pt, s.p0, s.p1, s.p2, s.p3, approx);
+}
+static bool within_distance_path_bvh(const PathBvh& pb, V2 pt) {  // closest.rs:20-98
+    if (pb.nodes.empty()) return false;
+    std::vector<size_t> stack{0};
+    while (!stack.empty()) {
+        size_t ni = stack.back();
+        stack.pop_back();
+        const BvhNode& n = pb.nodes[ni];
+        if (!n.bounds.contains(pt)) continue;
+        if (n.count > 0) {
+            for (size_t i = n.start; i < (size_t)n.start + n.count; ++i) {
+                const SegData& s = pb.segments[pb.indices[i]];
+                CP c = seg_closest(s, pt, pb.approx);
+                if (c.dist < seg_radius(s, c.t)) return true;
+            }
+        } else {
+            if (n.left != BVH_NONE) stack.push_back(n.left);
+            if (n.right != BVH_NONE) stack.push_back(n.right);
+        }
+    }
+    return false;
+}
+struct PathHit {
+    bool valid = false;
+    size_t segment_index = 0;
+    float t = 0.0f;
+};
+static bool closest_point_path_bvh(const PathBvh& pb, V2 pt, V2* best_pt_out, PathHit* hit) {  // closest.rs:104-199
+    if (pb.nodes.empty()) return false;
+    float best_dist = INF_F;
+    V2 best_pt = mk(0, 0);
+    size_t best_seg = 0;
+    float best_t = 0.0f;
+    std::vector<size_t> stack{0};
+    while (!stack.empty()) {
+        size_t ni = stack.back();
+        stack.pop_back();
+        const BvhNode& n = pb.nodes[ni];
+        if (n.bounds.distance(pt) > best_dist) continue;
+        if (n.count > 0) {
+            for (size_t i = n.start; i < (size_t)n.start + n.count; ++i) {
+                const SegData& s = pb.segments[pb.indices[i]];
+                CP c = seg_closest(s, pt, pb.approx);
+                if (c.dist < best_dist) {
+                    best_dist = c.dist;
+                    best_pt = c.cp;
+                    best_seg = s.segment_index;
+                    best_t = c.t;
+                }
+            }
+        } else {
+            float ld = INF_F, rd = INF_F;
+            if (n.left != BVH_NONE) ld = pb.nodes[n.left].bounds.distance(pt);
+            if (n.right != BVH_NONE) rd = pb.nodes[n.right].bounds.distance(pt);
+            if (ld < rd) {
+                if (rd <= best_dist) stack.push_back(n.right);
+                if (ld <= best_dist) stack.push_back(n.left);
+            } else {
+                if (ld <= best_dist) stack.push_back(n.left);
+                if (rd <= best_dist) stack.push_back(n.right);
+            }
+        }
+    }
+    if (!std::isfinite(best_dist)) return false;
+    *best_pt_out = best_pt;
+    hit->valid = true;
+    hit->segment_index = best_seg;
+    hit->t = best_t;
+    return true;
+}
+static bool within_distance_shape(const Shape& s, V2 pt, float r) {  // closest.rs:206-379
+    if (r <= 0.0f) return false;
+    V2 lp = xform_inv_dist(s.transform, pt);
+    if (s.kind == DVG_SHAPE_CIRCLE) {
+        float dist = length(lp - mk(s.prm[0], s.prm[1])) - std::fabs(s.prm[2]);
+        return std::fabs(dist) < r;
+    }
+    if (s.kind == DVG_SHAPE_ELLIPSE) {
+        float dist = ellipse_signed_distance(lp, mk(s.prm[0], s.prm[1]), mk(std::fabs(s.prm[2]), std::fabs(s.prm[3])));
+        return std::fabs(dist) < r;
+    }
+    if (s.kind == DVG_SHAPE_RECT) {
+        float dist = rect_signed_distance(lp, mk(s.prm[0], s.prm[1]), mk(s.prm[2], s.prm[3]));
+        return std::fabs(dist) < r;
+    }
+    if (s.kind == DVG_SHAPE_PATH) {
+        const PathG& p = s.path;
+        if (p.pts.empty()) return false;
+        size_t point_id = 0;
+        for (uint8_t nc : p.ncp) {
+            V2 q[4];
+            float rr[4];
+            if (nc == 0) {
+                if (!path_point_radius(p, point_id, r, &q[0], &rr[0])) break;
+                if (!path_point_radius(p, point_id + 1, r, &q[1], &rr[1])) break;
+                float dist, t;
+                V2 cp;
+                distance_to_segment(lp, q[0], q[1], &dist, &cp, &t);
+                float radius = rr[0] + t * (rr[1] - rr[0]);
+                if (dist < radius) return true;
+                point_id += 1;
+            } else if (nc == 1) {
+                if (!path_point_radius(p, point_id, r, &q[0], &rr[0])) break;
+                if (!path_point_radius(p, point_id + 1, r, &q[1], &rr[1])) break;
+                if (!path_point_radius(p, point_id + 2, r, &q[2], &rr[2])) break;
+                CP c = closest_point_quadratic(lp, q[0], q[1], q[2], p.approx);
+                float t = c.t, tt = 1.0f - t;
+                float radius = tt * tt * rr[0] + 2.0f * tt * t * rr[1] + t * t * rr[2];
+                if (c.dist < radius) return true;
+                point_id += 2;
+            } else if (nc == 2) {
+                if (!path_point_radius(p, point_id, r, &q[0], &rr[0])) break;
+                if (!path_point_radius(p, point_id + 1, r, &q[1], &rr[1])) break;
+                if (!path_point_radius(p, point_id + 2, r, &q[2], &rr[2])) break;
+                if (!path_point_radius(p, point_id + 3, r, &q[3], &rr[3])) break;
+                CP c = closest_point_cubic(lp, q[0], q[1], q[2], q[3], p.approx);
+                float t = c.t, tt = 1.0f - t;
+                float radius = tt * tt * tt * rr[0] + 3.0f * tt * tt * t * rr[1] + 3.0f * tt * t * t * rr[2] +
+                               t * t * t * rr[3];
+                if (c.dist < radius) return true;
+                point_id += 3;
+            } else {
+                break;
+            }
+        }
+        return false;
+    }
+    return false;
+}
+static bool closest_point_shape(const Shape& s, V2 pt, V2* out, PathHit* hit) {  // closest.rs:386-456
+    V2 lp = xform_inv_dist(s.transform, pt);
+    hit->valid = false;
+    if (s.kind == DVG_SHAPE_CIRCLE) {
+        *out = xform_pt(s.transform, closest_point_circle(mk(s.prm[0], s.prm[1]), std::fabs(s.prm[2]), lp));
+        return true;
+    }
+    if (s.kind == DVG_SHAPE_ELLIPSE) {
+        *out = xform_pt(s.transform, closest_point_ellipse(mk(s.prm[0], s.prm[1]),
+                                                           mk(std::fabs(s.prm[2]), std::fabs(s.prm[3])), lp));
+        return true;
+    }
+    if (s.kind == DVG_SHAPE_RECT) {
+        *out = xform_pt(s.transform, closest_point_rect(mk(s.prm[0], s.prm[1]), mk(s.prm[2], s.prm[3]), lp));
+        return true;
+    }
+    if (s.kind == DVG_SHAPE_PATH) {
+        const PathG& p = s.path;
+        if (p.pts.empty()) return false;
+        float best_dist = INF_F;
+        V2 best_pt = mk(0, 0);
+        size_t best_seg = 0;
+        float best_t = 0.0f;
+        size_t point_id = 0;
+        for (size_t si = 0; si < p.ncp.size(); ++si) {
+            uint8_t nc = p.ncp[si];
+            V2 q[4];
+            size_t next;
+            if (!path_segment_points(p, point_id, nc, q, &next)) break;
+            CP c;
+            if (nc == 0) {
+                distance_to_segment(lp, q[0], q[1], &c.dist, &c.cp, &c.t);
+            } else if (nc == 1) {
+                c = closest_point_quadratic(lp, q[0], q[1], q[2], p.approx);
+            } else if (nc == 2) {
+                c = closest_point_cubic(lp, q[0], q[1], q[2], q[3], p.approx);
+            } else {
+                break;
+            }
+            if (c.dist < best_dist) {
+                best_dist = c.dist;
+                best_pt = c.cp;
+                best_seg = si;
+                best_t = c.t;
+            }
+            point_id = next;
+        }
+        if (!std::isfinite(best_dist)) return false;
+        *out = xform_pt(s.transform, best_pt);
+        hit->valid = true;
+        hit->segment_index = best_seg;
+        hit->t = best_t;
+        return true;
+    }
+    return false;
+}
+static int winding_number_path_bvh(const PathBvh& pb, V2 pt) {  // winding.rs:73-115
+    if (pb.nodes.empty()) return 0;
+    int winding = 0;
+    std::vector<size_t> stack{0};
+    while (!stack.empty()) {
+        size_t ni = stack.back();
+        stack.pop_back();
+        const BvhNode& n = pb.nodes[ni];
+        if (pt.y < n.bounds.min.y || pt.y > n.bounds.max.y || pt.x > n.bounds.max.x) continue;
+        if (n.count > 0) {
+            for (size_t i = n.start; i < (size_t)n.start + n.count; ++i) {
+                const SegData& s = pb.segments[pb.indices[i]];
+                winding += winding_number_segment(s.kind, s.p0, s.p1, s.p2, s.p3, pt);
+            }
+        } else {
+            if (n.left != BVH_NONE) stack.push_back(n.left);
+            if (n.right != BVH_NONE) stack.push_back(n.right);
+        }
+    }
+    return winding;
+}
+static int winding_number_shape(const Shape& s, const PathBvh* pb, V2 pt) {  // winding.rs:13-48
+    if (s.kind == DVG_SHAPE_CIRCLE) {
+        float r = std::fabs(s.prm[2]);
+        return length_sq(pt - mk(s.prm[0], s.prm[1])) < r * r ? 1 : 0;
+    }
+    if (s.kind == DVG_SHAPE_ELLIPSE) {
+        float rx = std::fmax(std::fabs(s.prm[2]), 1.0e-6f);
+        float ry = std::fmax(std::fabs(s.prm[3]), 1.0e-6f);
+        float dx = (pt.x - s.prm[0]) / rx, dy = (pt.y - s.prm[1]) / ry;
+        return dx * dx + dy * dy < 1.0f ? 1 : 0;
+    }
+    if (s.kind == DVG_SHAPE_RECT) {
+        return (pt.x > s.prm[0] && pt.x < s.prm[2] && pt.y > s.prm[1] && pt.y < s.prm[3]) ? 1 : 0;
+    }
+    if (s.kind == DVG_SHAPE_PATH) return pb ? winding_number_path_bvh(*pb, pt) : winding_number_path(s.path, pt);
+    return 0;
+}
+
+// ---------------------------------------------------------------- distance API (distance/api.rs)
+struct ClosestPoint {
+    size_t shape_index;
+    V2 point;
+    float distance;
+    PathHit path;
+};
+static bool within_distance(const Scene& sc, size_t gi, V2 pt) {  // api.rs:15-33
+    if (gi >= sc.groups.size()) return false;
+    const Group& g = sc.groups[gi];
+    V2 lp = xform_pt(g.c2s, pt);
+    for (size_t si : g.shape_ids) {
+        if (si >= sc.shapes.size()) continue;
+        const Shape& s = sc.shapes[si];
+        if (s.stroke_width <= 0.0f) continue;
+        if (within_distance_shape(s, lp, s.stroke_width)) return true;
+    }
+    return false;
+}
+static bool compute_distance(const Scene& sc, size_t gi, V2 pt, float max_radius, ClosestPoint* best) {  // api.rs:36-76
+    if (gi >= sc.groups.size()) return false;
+    const Group& g = sc.groups[gi];
+    V2 lp = xform_pt(g.c2s, pt);
+    bool have = false;
+    for (size_t si : g.shape_ids) {
+        if (si >= sc.shapes.size()) continue;
+        V2 lc;
+        PathHit ph;
+        if (!closest_point_shape(sc.shapes[si], lp, &lc, &ph)) continue;
+        V2 closest = xform_pt(g.s2c, lc);
+        float distance = length(closest - pt);
+        if (distance <= max_radius) {
+            if (!have || distance < best->distance) {
+                *best = ClosestPoint{si, closest, distance, ph};
+                have = true;
+            }
+        }
+    }
+    return have;
+}
+static bool within_distance_bvh(const Scene& sc, const SceneBvh& bvh, size_t gi, V2 pt) {  // api.rs:79-135
+    if (gi >= sc.groups.size() || gi >= bvh.groups.size()) return false;
+    const Group& g = sc.groups[gi];
+    const GroupBvh& gb = bvh.groups[gi];
+    if (gb.nodes.empty()) return within_distance(sc, gi, pt);
+    V2 lp = xform_pt(g.c2s, pt);
+    std::vector<size_t> stack{0};
+    while (!stack.empty()) {
+        size_t ni = stack.back();
+        stack.pop_back();
+        const BvhNode& n = gb.nodes[ni];
+        if (!n.bounds.contains(lp)) continue;
+        if (n.count > 0) {
+            for (size_t i = n.start; i < (size_t)n.start + n.count; ++i) {
+                const BvhShape& bs = gb.shapes[gb.indices[i]];
+                if (bs.shape_index >= sc.shapes.size()) continue;
+                const Shape& s = sc.shapes[bs.shape_index];
+                if (s.stroke_width <= 0.0f) continue;
+                if (bs.has_path_bvh) {
+                    V2 sp = xform_inv_dist(s.transform, lp);
+                    if (within_distance_path_bvh(bs.path_bvh, sp)) return true;
+                } else if (within_distance_shape(s, lp, s.stroke_width)) {
+                    return true;
+                }
+            }
+        } else {
+            if (n.left != BVH_NONE) stack.push_back(n.left);
+            if (n.right != BVH_NONE) stack.push_back(n.right);
+        }
+    }
+    return false;
+}
+static bool compute_distance_bvh(const Scene& sc, const SceneBvh& bvh, size_t gi, V2 pt, float max_radius,
+                                 ClosestPoint* best) {  // api.rs:138-236
+    if (gi >= sc.groups.size() || gi >= bvh.groups.size()) return false;
+    const Group& g = sc.groups[gi];
+    const GroupBvh& gb = bvh.groups[gi];
+    if (gb.nodes.empty()) return compute_distance(sc, gi, pt, max_radius, best);
+    V2 lp = xform_pt(g.c2s, pt);
+    bool have = false;
+    float best_dist = max_radius;
+    std::vector<size_t> stack{0};
+    while (!stack.empty()) {
+        size_t ni = stack.back();
+        stack.pop_back();
+        const BvhNode& n = gb.nodes[ni];
+        if (n.bounds.distance(lp) > best_dist) continue;
+        if (n.count > 0) {
+            for (size_t i = n.start; i < (size_t)n.start + n.count; ++i) {
+                const BvhShape& bs = gb.shapes[gb.indices[i]];
+                if (bs.shape_index >= sc.shapes.size()) continue;
+                const Shape& s = sc.shapes[bs.shape_index];
+                V2 lc;
+                PathHit ph;
+                bool ok;
+                if (bs.has_path_bvh) {
+                    V2 sp = xform_inv_dist(s.transform, lp);
+                    V2 sc_pt;
+                    ok = closest_point_path_bvh(bs.path_bvh, sp, &sc_pt, &ph);
+                    if (ok) lc = xform_pt(s.transform, sc_pt);
+                } else {
+                    ok = closest_point_shape(s, lp, &lc, &ph);
+                }
+                if (!ok) continue;
+                V2 closest = xform_pt(g.s2c, lc);
+                float distance = length(closest - pt);
+                if (distance <= best_dist) {
+                    best_dist = distance;
+                    *best = ClosestPoint{bs.shape_index, closest, distance, ph};
+                    have = true;
+                }
+            }
+        } else {
+            float ld = INF_F, rd = INF_F;
+            if (n.left != BVH_NONE) ld = gb.nodes[n.left].bounds.distance(lp);
+            if (n.right != BVH_NONE) rd = gb.nodes[n.right].bounds.distance(lp);
+            if (ld < rd) {
+                if (rd <= best_dist) stack.push_back(n.right);
+                if (ld <= best_dist) stack.push_back(n.left);
+            } else {
+                if (ld <= best_dist) stack.push_back(n.left);
+                if (rd <= best_dist) stack.push_back(n.right);
+            }
+        }
+    }
+    return have;
+}
+static bool fill_rule_hit(uint32_t rule, int winding) {
+    if (rule == DVG_FILL_EVENODD) return (std::abs(winding) % 2) == 1;
+    return winding != 0;
+}
+static bool is_inside(const Scene& sc, size_t gi, V2 pt) {  // api.rs:239-256
+    if (gi >= sc.groups.size()) return false;
+    const Group& g = sc.groups[gi];
+    V2 lp = xform_pt(g.c2s, pt);
+    int winding = 0;
+    for (size_t si : g.shape_ids) {
+        if (si >= sc.shapes.size()) continue;
+        const Shape& s = sc.shapes[si];
+        winding += winding_number_shape(s, nullptr, xform_inv_dist(s.transform, lp));
+    }
+    return fill_rule_hit(g.fill_rule, winding);
+}
+static bool is_inside_bvh(const Scene& sc, const SceneBvh& bvh, size_t gi, V2 pt) {  // api.rs:259-309
+    if (gi >= sc.groups.size() || gi >= bvh.groups.size()) return false;
+    const Group& g = sc.groups[gi];
+    const GroupBvh& gb = bvh.groups[gi];
+    if (gb.nodes.empty()) return is_inside(sc, gi, pt);
+    V2 lp = xform_pt(g.c2s, pt);
+    if (!gb.nodes[0].bounds.contains(lp)) return false;
+    int winding = 0;
+    std::vector<size_t> stack{0};
+    while (!stack.empty()) {
+        size_t ni = stack.back();
+        stack.pop_back();
+        const BvhNode& n = gb.nodes[ni];
+        if (!n.bounds.contains(lp)) continue;
+        if (n.count > 0) {
+            for (size_t i = n.start; i < (size_t)n.start + n.count; ++i) {
+                const BvhShape& bs = gb.shapes[gb.indices[i]];
+                if (bs.shape_index >= sc.shapes.size()) continue;
+                const Shape& s = sc.shapes[bs.shape_index];
+                V2 sp = xform_inv_dist(s.transform, lp);
+                winding += winding_number_shape(s, bs.has_path_bvh ? &bs.path_bvh : nullptr, sp);
+            }
+        } else {
+            if (n.left != BVH_NONE) stack.push_back(n.left);
+            if (n.right != BVH_NONE) stack.push_back(n.right);
+        }
+    }
+    return fill_rule_hit(g.fill_rule, winding);
+}
+
+// ---------------------------------------------------------------- gradients (SceneGrad, src/grad.rs:113-126)
+struct Grads {
+    std::vector<float> shape_params, shape_transform, stroke_width, points, thickness, group_transform,
+        paint_params, stop_offsets, stop_colors, bg_image, translation;
+    float filter_radius = 0.0f;
+    float background[4] = {0, 0, 0, 0};
+    bool has_bg_image = false, has_translation = false;
+    void init(const Scene& sc, const dvg_scene_desc* d, bool bg_img, bool trans) {
+        shape_params.assign((size_t)4 * sc.shapes.size(), 0.0f);
+        shape_transform.assign((size_t)9 * sc.shapes.size(), 0.0f);
+        stroke_width.assign(sc.shapes.size(), 0.0f);
+        points.assign((size_t)2 * d->total_points, 0.0f);
+        thickness.assign(d->total_points, 0.0f);
+        group_transform.assign((size_t)9 * sc.groups.size(), 0.0f);
+        paint_params.assign((size_t)4 * sc.paints.size(), 0.0f);
+        stop_offsets.assign(d->total_stops, 0.0f);
+        stop_colors.assign((size_t)4 * d->total_stops, 0.0f);
+        has_bg_image = bg_img;
+        if (bg_img) bg_image.assign((size_t)sc.w * sc.h * 4, 0.0f);
+        has_translation = trans;
+        if (trans) translation.assign((size_t)sc.w * sc.h * 2, 0.0f);
+    }
+    void add(const Grads& o) {
+        auto addv = [](std::vector<float>& a, const std::vector<float>& b) {
+            for (size_t i = 0; i < a.size() && i < b.size(); ++i) a[i] += b[i];
+        };
+        addv(shape_params, o.shape_params);
+        addv(shape_transform, o.shape_transform);
+        addv(stroke_width, o.stroke_width);
+        addv(points, o.points);
+        addv(thickness, o.thickness);
+        addv(group_transform, o.group_transform);
+        addv(paint_params, o.paint_params);
+        addv(stop_offsets, o.stop_offsets);
+        addv(stop_colors, o.stop_colors);
+        addv(bg_image, o.bg_image);
+        addv(translation, o.translation);
+        filter_radius += o.filter_radius;
+        for (int i = 0; i < 4; ++i) background[i] += o.background[i];
+    }
+};
+
+// ---------------------------------------------------------------- backward math (backward/math.rs)
+static inline float smoothstep(float d) {  // math.rs:9-12
+    float t = clampf((d + 1.0f) * 0.5f, 0.0f, 1.0f);
+    return t * t * (3.0f - 2.0f * t);
+}
+static inline V2 normalize(V2 v) {  // math.rs:43-50
+    float len = length(v);
+    if (len == 0.0f) return mk(0, 0);
+    return v / len;
+}
+static void d_xform_pt(const M3& m, V2 pt, V2 d_out, M3* d_m, V2* d_pt) {  // math.rs:109-128
+    float t0 = m.m[0][0] * pt.x + m.m[0][1] * pt.y + m.m[0][2];
+    float t1 = m.m[1][0] * pt.x + m.m[1][1] * pt.y + m.m[1][2];
+    float t2 = m.m[2][0] * pt.x + m.m[2][1] * pt.y + m.m[2][2];
+    V2 out = mk(t0 / t2, t1 / t2);
+    float d_t0 = d_out.x / t2;
+    float d_t1 = d_out.y / t2;
+    float d_t2 = -(d_out.x * out.x + d_out.y * out.y) / t2;
+    d_m->m[0][0] += d_t0 * pt.x;
+    d_m->m[0][1] += d_t0 * pt.y;
+    d_m->m[0][2] += d_t0;
+    d_m->m[1][0] += d_t1 * pt.x;
+    d_m->m[1][1] += d_t1 * pt.y;
+    d_m->m[1][2] += d_t1;
+    d_m->m[2][0] += d_t2 * pt.x;
+    d_m->m[2][1] += d_t2 * pt.y;
+    d_m->m[2][2] += d_t2;
+    d_pt->x += d_t0 * m.m[0][0] + d_t1 * m.m[1][0] + d_t2 * m.m[2][0];
+    d_pt->y += d_t0 * m.m[0][1] + d_t1 * m.m[1][1] + d_t2 * m.m[2][1];
+}
+static V2 xform_normal(const M3& m_inv, V2 n) {  // math.rs:139-143
+    float x = m_inv.m[0][0] * n.x + m_inv.m[1][0] * n.y;
+    float y = m_inv.m[0][1] * n.x + m_inv.m[1][1] * n.y;
+    return normalize(mk(x, y));
+}
+static M3 transpose3(const M3& m) {
+    M3 o;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) o.m[r][c] = m.m[c][r];
+    return o;
+}
+static V2 d_length(V2 v, float d_l) {  // math.rs:33-41
+    float l_sq = dot(v, v);
+    float l = std::sqrt(l_sq);
+    if (l == 0.0f) return mk(0, 0);
+    float d_l_sq = 0.5f * d_l / l;
+    return v * (2.0f * d_l_sq);
+}
+
+// ---------------------------------------------------------------- paint (backward/paint.rs)
+static V4 stops_color(const Paint& p, float t) {  // paint.rs:16-39 (shared by linear / radial)
+    if (p.stops.empty()) return V4{0, 0, 0, 0};
+    if (t < p.stops[0].offset) {
+        Color c = p.stops[0].color;
+        return V4{c.r, c.g, c.b, c.a};
+    }
+    for (size_t i = 0; i + 1 < p.stops.size(); ++i) {
+        const Stop& cu = p.stops[i];
+        const Stop& nx = p.stops[i + 1];
+        if (t >= cu.offset && t < nx.offset) {
+            float tt = (t - cu.offset) / (nx.offset - cu.offset);
+            Color c0 = cu.color, c1 = nx.color;
+            return V4{c0.r * (1.0f - tt) + c1.r * tt, c0.g * (1.0f - tt) + c1.g * tt,
+                      c0.b * (1.0f - tt) + c1.b * tt, c0.a * (1.0f - tt) + c1.a * tt};
+        }
+    }
+    Color l = p.stops.back().color;
+    return V4{l.r, l.g, l.b, l.a};
+}
+static V4 paint_color(const Paint& p, V2 pt) {  // paint.rs:8-74
+    if (p.kind == DVG_PAINT_SOLID) return V4{p.p[0], p.p[1], p.p[2], p.p[3]};
+    if (p.kind == DVG_PAINT_LINEAR) {
+        V2 beg = mk(p.p[0], p.p[1]), end = mk(p.p[2], p.p[3]);
+        float denom = std::fmax(dot(end - beg, end - beg), 1.0e-3f);
+        float t = dot(pt - beg, end - beg) / denom;
+        return stops_color(p, t);
+    }
+    if (p.kind == DVG_PAINT_RADIAL) {
+        V2 off = pt - mk(p.p[0], p.p[1]);
+        V2 nrm = mk(off.x / p.p[2], off.y / p.p[3]);
+        float t = length(nrm);
+        return stops_color(p, t);
+    }
+    return V4{0, 0, 0, 0};
+}
+static void add_stop_color(Grads& g, uint32_t stop_base, size_t i, V4 c) {
+    float* sc = &g.stop_colors[4 * (stop_base + i)];
+    sc[0] += c.x;
+    sc[1] += c.y;
+    sc[2] += c.z;
+    sc[3] += c.w;
+}
+static void d_sample_paint(const Scene& sc, int pi, Grads& g, V2 pt, V4 d_color, V2* d_translation) {  // paint.rs:77-280
+    const Paint& p = sc.paints[pi];
+    float* dp = &g.paint_params[4 * (size_t)pi];
+    uint32_t sb = sc.paint_stop_base[pi];
+    if (p.kind == DVG_PAINT_SOLID) {
+        dp[0] += d_color.x;
+        dp[1] += d_color.y;
+        dp[2] += d_color.z;
+        dp[3] += d_color.w;
+        return;
+    }
+    if (p.kind != DVG_PAINT_LINEAR && p.kind != DVG_PAINT_RADIAL) return;
+    float t;
+    V2 beg, end, off, nrm;
+    float denom = 0.0f;
+    if (p.kind == DVG_PAINT_LINEAR) {
+        beg = mk(p.p[0], p.p[1]);
+        end = mk(p.p[2], p.p[3]);
+        denom = std::fmax(dot(end - beg, end - beg), 1.0e-3f);
+        t = dot(pt - beg, end - beg) / denom;
+    } else {
+        off = pt - mk(p.p[0], p.p[1]);
+        nrm = mk(off.x / p.p[2], off.y / p.p[3]);
+        t = length(nrm);
+    }
+    if (p.stops.empty()) return;
+    if (t < p.stops[0].offset) {
+        add_stop_color(g, sb, 0, d_color);
+        return;
+    }
+    for (size_t i = 0; i + 1 < p.stops.size(); ++i) {
+        const Stop& cu = p.stops[i];
+        const Stop& nx = p.stops[i + 1];
+        if (t >= cu.offset && t < nx.offset) {
+            float tt = (t - cu.offset) / (nx.offset - cu.offset);
+            V4 cc = V4{cu.color.r, cu.color.g, cu.color.b, cu.color.a};
+            V4 cn = V4{nx.color.r, nx.color.g, nx.color.b, nx.color.a};
+            add_stop_color(g, sb, i, V4{d_color.x * (1.0f - tt), d_color.y * (1.0f - tt), d_color.z * (1.0f - tt),
+                                        d_color.w * (1.0f - tt)});
+            add_stop_color(g, sb, i + 1, V4{d_color.x * tt, d_color.y * tt, d_color.z * tt, d_color.w * tt});
+            V4 diff = V4{cn.x - cc.x, cn.y - cc.y, cn.z - cc.z, cn.w - cc.w};
+            float d_tt = dot4(d_color, diff);
+            float denom_offset = nx.offset - cu.offset;
+            if (std::fabs(denom_offset) > 0.0f) {
+                float d_offset_next = -d_tt * tt / denom_offset;
+                float d_offset_curr = d_tt * (tt - 1.0f) / denom_offset;
+                g.stop_offsets[sb + i] += d_offset_curr;
+                g.stop_offsets[sb + i + 1] += d_offset_next;
+            }
+            float d_t = d_tt / denom_offset;
+            if (p.kind == DVG_PAINT_LINEAR) {
+                V2 d_beg = mk(d_t * (-(pt.x - beg.x) - (end.x - beg.x)) / denom,
+                              d_t * (-(pt.y - beg.y) - (end.y - beg.y)) / denom);
+                V2 d_end = mk(d_t * (pt.x - beg.x) / denom, d_t * (pt.y - beg.y) / denom);
+                float d_l = -d_t * t / denom;
+                if (dot(end - beg, end - beg) > 1.0e-3f) {
+                    V2 adjust = mk(beg.x - end.x, beg.y - end.y);
+                    V2 ds = mk(d_beg.x + 2.0f * d_l * adjust.x, d_beg.y + 2.0f * d_l * adjust.y);
+                    V2 de = mk(d_end.x + 2.0f * d_l * (end.x - beg.x), d_end.y + 2.0f * d_l * (end.y - beg.y));
+                    dp[0] += ds.x;
+                    dp[1] += ds.y;
+                    dp[2] += de.x;
+                    dp[3] += de.y;
+                } else {
+                    dp[0] += d_beg.x;
+                    dp[1] += d_beg.y;
+                    dp[2] += d_end.x;
+                    dp[3] += d_end.y;
+                }
+                *d_translation += d_beg + d_end;
+            } else {
+                V2 d_nrm = d_length(nrm, d_t);
+                V2 d_off = mk(d_nrm.x / p.p[2], d_nrm.y / p.p[3]);
+                V2 d_radius = mk(-d_nrm.x * off.x / (p.p[2] * p.p[2]), -d_nrm.y * off.y / (p.p[3] * p.p[3]));
+                V2 d_center = mk(-d_off.x, -d_off.y);
+                dp[0] += d_center.x;
+                dp[1] += d_center.y;
+                dp[2] += d_radius.x;
+                dp[3] += d_radius.y;
+                *d_translation += d_center;
+            }
+            return;
+        }
+    }
+    add_stop_color(g, sb, p.stops.size() - 1, d_color);
+}
+
+// ---------------------------------------------------------------- background (backward/background.rs)
+static V4 sample_background(const Scene& sc, size_t pixel_index) {  // background.rs:7-26
+    if (sc.has_bg_img) {
+        size_t base = pixel_index * 4;
+        if (base + 3 >= sc.bg_img.size()) return V4{0, 0, 0, 0};
+        float r = sc.bg_img[base], g = sc.bg_img[base + 1], b = sc.bg_img[base + 2], a = sc.bg_img[base + 3];
+        return V4{r * a, g * a, b * a, a};
+    }
+    return V4{sc.bg.r * sc.bg.a, sc.bg.g * sc.bg.a, sc.bg.b * sc.bg.a, sc.bg.a};
+}
+static void accumulate_background_grad(const Scene& sc, Grads& g, size_t pixel_index, V4 d) {  // background.rs:64-90
+    if (sc.has_bg_img) {
+        if (g.has_bg_image) {
+            size_t base = pixel_index * 4;
+            if (base + 3 < g.bg_image.size()) {
+                g.bg_image[base] += d.x;
+                g.bg_image[base + 1] += d.y;
+                g.bg_image[base + 2] += d.z;
+                g.bg_image[base + 3] += d.w;
+            }
+        }
+        return;
+    }
+    g.background[0] = g.background[0] + d.x;
+    g.background[1] = g.background[1] + d.y;
+    g.background[2] = g.background[2] + d.z;
+    g.background[3] = g.background[3] + d.w;
+}
+static void finalize_background_gradients(const Scene& sc, Grads& g) {  // background.rs:29-61
+    if (sc.has_bg_img) {
+        if (g.has_bg_image) {
+            for (size_t i = 0; i * 4 < g.bg_image.size(); ++i) {
+                size_t base = i * 4;
+                float r = sc.bg_img[base], gg = sc.bg_img[base + 1], b = sc.bg_img[base + 2], a = sc.bg_img[base + 3];
+                float* c = &g.bg_image[base];
+                float dr = c[0] * a, dg = c[1] * a, db = c[2] * a;
+                float da = c[0] * r + c[1] * gg + c[2] * b + c[3];
+                c[0] = dr;
+                c[1] = dg;
+                c[2] = db;
+                c[3] = da;
+            }
+        }
+    } else {
+        float r = sc.bg.r, gg = sc.bg.g, b = sc.bg.b, a = sc.bg.a;
+        float* d = g.background;
+        float nr = d[0] * a, ng = d[1] * a, nb = d[2] * a;
+        float na = d[0] * r + d[1] * gg + d[2] * b + d[3];
+        d[0] = nr;
+        d[1] = ng;
+        d[2] = nb;
+        d[3] = na;
+    }
+}
+
+// ---------------------------------------------------------------- filters (backward/filters.rs)
+static float compute_filter_weight(uint32_t ft, float radius, float dx, float dy) {  // filters.rs:159-188
+    if (radius <= 0.0f) return 1.0f;
+    if (std::fabs(dx) > radius || std::fabs(dy) > radius) return 0.0f;
+    switch (ft) {
+        case DVG_FILTER_BOX:
+            return 1.0f / ((2.0f * radius) * (2.0f * radius));
+        case DVG_FILTER_TENT: {
+            float fx = radius - std::fabs(dx), fy = radius - std::fabs(dy);
+            float norm = 1.0f / (radius * radius);
+            return fx * fy * norm * norm;
+        }
+        case DVG_FILTER_RADIAL_PARABOLIC: {
+            float rx = 1.0f - (dx / radius) * (dx / radius);
+            float ry = 1.0f - (dy / radius) * (dy / radius);
+            return (4.0f / 3.0f) * rx * (4.0f / 3.0f) * ry;
+        }
+        case DVG_FILTER_HANN: {
+            float ndx = (dx / (2.0f * radius)) + 0.5f, ndy = (dy / (2.0f * radius)) + 0.5f;
+            float fx = 0.5f * (1.0f - std::cos(2.0f * PI_F * ndx));
+            float fy = 0.5f * (1.0f - std::cos(2.0f * PI_F * ndy));
+            float norm = 1.0f / (radius * radius);
+            return fx * fy * norm;
+        }
+        case DVG_FILTER_GAUSSIAN: {
+            // Addition of this library (not in the crate): normalised 2-D Gaussian with
+            // sigma = radius/2 truncated to the square support |dx|,|dy| <= radius:
+            // w = 2/(pi r^2) * exp(-2 (dx^2+dy^2) / r^2).
+            float r2 = radius * radius;
+            float q = dx * dx + dy * dy;
+            return (2.0f / (PI_F * r2)) * std::exp(-2.0f * q / r2);
+        }
+        default:
+            return 1.0f;
+    }
+}
+static void d_compute_filter_weight(uint32_t ft, float radius, float dx, float dy, float d_return,
+                                    float* d_radius) {  // filters.rs:190-239
+    switch (ft) {
+        case DVG_FILTER_BOX: {
+            float denom = 2.0f * radius;
+            if (denom != 0.0f) *d_radius += d_return * (-2.0f) * denom / ((denom * denom) * denom);
+            break;
+        }
+        case DVG_FILTER_TENT: {
+            float fx = radius - std::fabs(dx), fy = radius - std::fabs(dy);
+            float norm = 1.0f / (radius * radius);
+            float d_fx = d_return * fy * norm, d_fy = d_return * fx * norm, d_norm = d_return * fx * fy;
+            float r2 = radius * radius;
+            if (radius != 0.0f) *d_radius += d_fx + d_fy + (-4.0f) * d_norm / ((r2 * r2) * radius);
+            break;
+        }
+        case DVG_FILTER_RADIAL_PARABOLIC: {
+            float r3 = radius * radius * radius;
+            if (r3 != 0.0f) *d_radius += -(2.0f * dx * dx + 2.0f * dy * dy) / r3;
+            break;
+        }
+        case DVG_FILTER_HANN: {
+            float ndx = (dx / (2.0f * radius)) + 0.5f, ndy = (dy / (2.0f * radius)) + 0.5f;
+            float fx = 0.5f * (1.0f - std::cos(2.0f * PI_F * ndx));
+            float fy = 0.5f * (1.0f - std::cos(2.0f * PI_F * ndy));
+            float norm = 1.0f / (radius * radius);
+            float d_fx = d_return * fy * norm, d_fy = d_return * fx * norm, d_norm = d_return * fx * fy;
+            float d_ndx = d_fx * 0.5f * std::sin(2.0f * PI_F * ndx) * (2.0f * PI_F);
+            float d_ndy = d_fy * 0.5f * std::sin(2.0f * PI_F * ndy) * (2.0f * PI_F);
+            float tr = 2.0f * radius;
+            *d_radius += d_ndx * (-2.0f * dx / (tr * tr)) + d_ndy * (-2.0f * dy / (tr * tr)) +
+                         (-2.0f) * d_norm / ((radius * radius) * radius);
+            break;
+        }
+        case DVG_FILTER_GAUSSIAN: {
+            // d/dr of 2/(pi r^2) exp(-2q/r^2) = w * (4q/r^3 - 2/r)
+            float r2 = radius * radius;
+            float q = dx * dx + dy * dy;
+            float w = (2.0f / (PI_F * r2)) * std::exp(-2.0f * q / r2);
+            if (radius != 0.0f) *d_radius += d_return * w * (4.0f * q / (r2 * radius) - 2.0f / radius);
+            break;
+        }
+        default:
+            break;
+    }
+}
+
+// PCG32 (src/renderer/rng.rs:16-43)
+struct Pcg32 {
+    uint64_t state, inc;
+    Pcg32(uint64_t idx, uint64_t seed) {
+        state = 0;
+        inc = ((idx + 1) << 1) | 1;
+        next_u32();
+        state = state + (0x853c49e6748fea9bULL + seed);
+        next_u32();
+    }
+    uint32_t next_u32() {
+        uint64_t old = state;
+        state = old * 6364136223846793005ULL + (inc | 1);
+        uint32_t xorshifted = (uint32_t)(((old >> 18) ^ old) >> 27);
+        uint32_t rot = (uint32_t)(old >> 59);
+        return (xorshifted >> rot) | (xorshifted << ((32 - rot) & 31));
+    }
+    float next_f32() {
+        uint32_t u = next_u32();
+        uint32_t bits = (u >> 9) | 0x3f800000u;
+        float f;
+        std::memcpy(&f, &bits, 4);
+        return f - 1.0f;
+    }
+};
+
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel Random Numbers: As Easy as
+// 1, 2, 3", SC 2011): counter = (idx_lo, idx_hi, 0, 0), key = (seed, 0).
+static void philox4x32_10(uint32_t ctr[4], uint32_t key[2]) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+    uint32_t k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = (uint64_t)M0 * ctr[0];
+        uint64_t p1 = (uint64_t)M1 * ctr[2];
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ ctr[1] ^ k0, n1 = lo1, n2 = hi0 ^ ctr[3] ^ k1, n3 = lo0;
+        ctr[0] = n0;
+        ctr[1] = n1;
+        ctr[2] = n2;
+        ctr[3] = n3;
+        k0 += W0;
+        k1 += W1;
+    }
+}
+static inline float u32_to_unit(uint32_t u) { return (float)(u >> 9) * (1.0f / 8388608.0f); }
+static void boundary_rng(uint32_t kind, uint64_t idx, uint32_t seed, float* u, float* t) {
+    if (kind == DVG_RNG_PHILOX) {
+        uint32_t ctr[4] = {(uint32_t)idx, (uint32_t)(idx >> 32), 0u, 0u};
+        uint32_t key[2] = {seed, 0u};
+        philox4x32_10(ctr, key);
+        *u = u32_to_unit(ctr[0]);
+        *t = u32_to_unit(ctr[1]);
+        return;
+    }
+    Pcg32 rng(idx, (uint64_t)seed);
+    *u = rng.next_f32();
+    *t = rng.next_f32();
+}
+
+struct SampleSpec {
+    uint32_t sx_n, sy_n;
+    bool jitter;
+    bool prefilter;
+    uint32_t seed;
+};
+static void sample_position(const Scene& sc, const SampleSpec& sp, uint64_t idx, V2* pt, size_t* pixel) {  // render.rs:95-111
+    uint64_t sx = idx % sp.sx_n;
+    uint64_t sy = (idx / sp.sx_n) % sp.sy_n;
+    uint64_t x = (idx / ((uint64_t)sp.sx_n * sp.sy_n)) % sc.w;
+    uint64_t y = idx / ((uint64_t)sp.sx_n * sp.sy_n * sc.w);
+    float rx = 0.5f, ry = 0.5f;
+    if (sp.jitter) {
+        Pcg32 rng(idx, (uint64_t)sp.seed);
+        rx = rng.next_f32();
+        ry = rng.next_f32();
+    }
+    if (sp.prefilter) {
+        rx = 0.5f;
+        ry = 0.5f;
+    }
+    float px = (float)x + ((float)sx + rx) / (float)sp.sx_n;
+    float py = (float)y + ((float)sy + ry) / (float)sp.sy_n;
+    *pt = mk(px, py);
+    *pixel = (size_t)(y * sc.w + x);
+}
+
+static std::vector<float> build_weight_image(const Scene& sc, const SampleSpec& sp) {  // filters.rs:11-67
+    int width = (int)sc.w, height = (int)sc.h;
+    std::vector<float> wimg((size_t)width * height, 0.0f);
+    uint64_t total = (uint64_t)width * height * sp.sx_n * sp.sy_n;
+    int ri = to_i32(std::ceil(sc.filter_radius));
+    for (uint64_t idx = 0; idx < total; ++idx) {
+        V2 pt;
+        size_t pix;
+        sample_position(sc, sp, idx, &pt, &pix);
+        int x = (int)(pix % sc.w), y = (int)(pix / sc.w);
+        for (int dy = -ri; dy <= ri; ++dy)
+            for (int dx = -ri; dx <= ri; ++dx) {
+                int xx = x + dx, yy = y + dy;
+                if (xx >= 0 && yy >= 0 && xx < width && yy < height) {
+                    float xc = (float)xx + 0.5f, yc = (float)yy + 0.5f;
+                    float w = compute_filter_weight(sc.filter_type, sc.filter_radius, xc - pt.x, yc - pt.y);
+                    wimg[(size_t)yy * width + xx] += w;
+                }
+            }
+    }
+    return wimg;
+}
+static V4 gather_d_color(const Scene& sc, const float* d_render, const std::vector<float>& wimg, V2 pt) {  // filters.rs:70-103
+    int width = (int)sc.w, height = (int)sc.h;
+    int x = to_i32(std::floor(pt.x)), y = to_i32(std::floor(pt.y));
+    int ri = to_i32(std::ceil(sc.filter_radius));
+    V4 out{0, 0, 0, 0};
+    for (int dy = -ri; dy <= ri; ++dy)
+        for (int dx = -ri; dx <= ri; ++dx) {
+            int xx = x + dx, yy = y + dy;
+            if (xx >= 0 && yy >= 0 && xx < width && yy < height) {
+                float xc = (float)xx + 0.5f, yc = (float)yy + 0.5f;
+                float w = compute_filter_weight(sc.filter_type, sc.filter_radius, xc - pt.x, yc - pt.y);
+                float ws = wimg[(size_t)yy * width + xx];
+                if (ws > 0.0f) {
+                    size_t base = ((size_t)yy * width + xx) * 4;
+                    out.x += (w / ws) * d_render[base];
+                    out.y += (w / ws) * d_render[base + 1];
+                    out.z += (w / ws) * d_render[base + 2];
+                    out.w += (w / ws) * d_render[base + 3];
+                }
+            }
+        }
+    return out;
+}
+static void accumulate_filter_gradient(const Scene& sc, V4 color, const float* d_render,
+                                       const std::vector<float>& wimg, V2 pt, float* d_radius) {  // filters.rs:106-156
+    int width = (int)sc.w, height = (int)sc.h;
+    int x = to_i32(std::floor(pt.x)), y = to_i32(std::floor(pt.y));
+    int ri = to_i32(std::ceil(sc.filter_radius));
+    for (int dy = -ri; dy <= ri; ++dy)
+        for (int dx = -ri; dx <= ri; ++dx) {
+            int xx = x + dx, yy = y + dy;
+            if (xx >= 0 && yy >= 0 && xx < width && yy < height) {
+                float ws = wimg[(size_t)yy * width + xx];
+                if (ws <= 0.0f) continue;
+                float xc = (float)xx + 0.5f, yc = (float)yy + 0.5f;
+                float w = compute_filter_weight(sc.filter_type, sc.filter_radius, xc - pt.x, yc - pt.y);
+                if (w <= 0.0f) continue;
+                size_t base = ((size_t)yy * width + xx) * 4;
+                V4 dpx{d_render[base], d_render[base + 1], d_render[base + 2], d_render[base + 3]};
+                float dt = dot4(dpx, color);
+                float denom = ws * ws;
+                float d_weight = denom > 0.0f ? (dt * ws - w * dt * (ws - w)) / denom : 0.0f;
+                if (d_weight != 0.0f)
+                    d_compute_filter_weight(sc.filter_type, sc.filter_radius, xc - pt.x, yc - pt.y, d_weight,
+                                            d_radius);
+            }
+        }
+}
+
+// ---------------------------------------------------------------- sample colour (backward/sampling.rs)
+struct EdgeQuery {  // types.rs:42-50
+    size_t group_id, shape_id;
+    bool hit;
+};
+struct Fragment {  // types.rs:105-115
+    float r, g, b, a;
+    size_t group_id;
+    bool is_stroke;
+};
+static bool within_distance_edge(const Scene& sc, const SceneBvh& bvh, size_t gi, V2 pt, EdgeQuery* eq) {  // sampling.rs:485-513
+    bool hit = within_distance_bvh(sc, bvh, gi, pt);
+    if (!eq || eq->group_id != gi) return hit;
+    if (gi >= sc.groups.size() || eq->shape_id >= sc.shapes.size()) return hit;
+    const Shape& s = sc.shapes[eq->shape_id];
+    if (s.stroke_width <= 0.0f) return hit;
+    V2 lp = xform_pt(sc.groups[gi].c2s, pt);
+    if (within_distance_shape(s, lp, s.stroke_width)) eq->hit = true;
+    return hit;
+}
+static bool is_inside_edge(const Scene& sc, const SceneBvh& bvh, size_t gi, V2 pt, EdgeQuery* eq) {  // sampling.rs:516-552
+    bool inside = is_inside_bvh(sc, bvh, gi, pt);
+    if (!eq || eq->group_id != gi) return inside;
+    if (gi >= sc.groups.size() || eq->shape_id >= sc.shapes.size()) return inside;
+    const Group& g = sc.groups[gi];
+    const Shape& s = sc.shapes[eq->shape_id];
+    V2 lp = xform_pt(g.c2s, pt);
+    V2 sp = xform_inv_bwd(s.transform, lp);
+    const PathBvh* pb = nullptr;
+    if (gi < bvh.groups.size())
+        for (const BvhShape& bs : bvh.groups[gi].shapes)
+            if (bs.shape_index == eq->shape_id) {
+                pb = bs.has_path_bvh ? &bs.path_bvh : nullptr;
+                break;
+            }
+    int winding = winding_number_shape(s, pb, sp);
+    if (fill_rule_hit(g.fill_rule, winding)) eq->hit = true;
+    return inside;
+}
+static void accumulate_translation(Grads& g, long translation_index, V2 delta) {  // sampling.rs:555-563
+    if (translation_index >= 0 && g.has_translation) {
+        size_t idx = (size_t)translation_index * 2;
+        g.translation[idx] += delta.x;
+        g.translation[idx + 1] += delta.y;
+    }
+}
+
+// Collect fragments (stroke then fill per group, in group order) — sampling.rs:91-119.
+static void collect_fragments(const Scene& sc, const SceneBvh& bvh, V2 pt, EdgeQuery* eq,
+                              std::vector<Fragment>& frags) {
+    frags.clear();
+    for (size_t gi = 0; gi < sc.groups.size(); ++gi) {
+        const Group& g = sc.groups[gi];
+        if (g.stroke >= 0) {
+            if (within_distance_edge(sc, bvh, gi, pt, eq)) {
+                V4 c = paint_color(sc.paints[g.stroke], pt);
+                frags.push_back(Fragment{c.x, c.y, c.z, c.w, gi, true});
+            }
+        }
+        if (g.fill >= 0) {
+            if (is_inside_edge(sc, bvh, gi, pt, eq)) {
+                V4 c = paint_color(sc.paints[g.fill], pt);
+                frags.push_back(Fragment{c.x, c.y, c.z, c.w, gi, false});
+            }
+        }
+    }
+}
+
+// sample_color (sampling.rs:76-224).  screen_pt is in normalised [0,1] canvas units.
+static V4 sample_color(const Scene& sc, const SceneBvh& bvh, V2 screen_pt, const V4* background,
+                       const V4* d_color, EdgeQuery* eq, Grads* grads, long translation_index,
+                       size_t pixel_index) {
+    if (eq) eq->hit = false;
+    V2 pt = mk(screen_pt.x * (float)sc.w, screen_pt.y * (float)sc.h);
+    std::vector<Fragment> frags;
+    collect_fragments(sc, bvh, pt, eq, frags);
+    if (frags.empty()) {
+        if (background) {
+            if (d_color) accumulate_background_grad(sc, *grads, pixel_index, *d_color);
+            return *background;
+        }
+        return V4{0, 0, 0, 0};
+    }
+    // fragments are produced in ascending group order already (stable sort is a no-op)
+    std::vector<V4> accum(frags.size());
+    float pr = 0, pg = 0, pb = 0, pa = 0;
+    if (background) {
+        pr = background->x;
+        pg = background->y;
+        pb = background->z;
+        pa = background->w;
+    }
+    for (size_t i = 0; i < frags.size(); ++i) {
+        const Fragment& f = frags[i];
+        if (eq) {
+            if (f.a >= 1.0f && eq->hit) eq->hit = false;
+            if (eq->group_id == f.group_id) eq->hit = true;
+        }
+        float br = pr * (1.0f - f.a) + f.r * f.a;
+        float bg = pg * (1.0f - f.a) + f.g * f.a;
+        float bb = pb * (1.0f - f.a) + f.b * f.a;
+        float ba = pa * (1.0f - f.a) + f.a;
+        accum[i] = V4{br, bg, bb, ba};
+        pr = br;
+        pg = bg;
+        pb = bb;
+        pa = ba;
+    }
+    V4 fc = accum.back();
+    float final_alpha = fc.w;
+    float fr = fc.x, fg = fc.y, fb = fc.z;
+    if (final_alpha > 1.0e-6f) {
+        float s = 1.0f / final_alpha;
+        fr = fr * s;
+        fg = fg * s;
+        fb = fb * s;
+    }
+    if (d_color) {
+        float dcr = d_color->x, dcg = d_color->y, dcb = d_color->z, dca = d_color->w;
+        if (final_alpha > 1.0e-6f) {
+            float dfr = dcr, dfg = dcg, dfb = dcb;
+            float s = 1.0f / final_alpha;
+            dcr = dcr * s;
+            dcg = dcg * s;
+            dcb = dcb * s;
+            dca -= (dfr * fr + dfg * fg + dfb * fb) / final_alpha;
+        }
+        for (size_t ii = frags.size(); ii-- > 0;) {
+            float prev_a, prev_r, prev_g, prev_b;
+            if (ii > 0) {
+                prev_a = accum[ii - 1].w;
+                prev_r = accum[ii - 1].x;
+                prev_g = accum[ii - 1].y;
+                prev_b = accum[ii - 1].z;
+            } else {
+                prev_a = background ? background->w : 0.0f;
+                prev_r = background ? background->x : 0.0f;
+                prev_g = background ? background->y : 0.0f;
+                prev_b = background ? background->z : 0.0f;
+            }
+            const Fragment& f = frags[ii];
+            float d_prev_alpha = dca * (1.0f - f.a);
+            float d_alpha_i = dca * (1.0f - prev_a);
+            d_alpha_i += dcr * (f.r - prev_r) + dcg * (f.g - prev_g) + dcb * (f.b - prev_b);
+            float s = 1.0f - f.a;
+            float dpr = dcr * s, dpg = dcg * s, dpb = dcb * s;
+            V4 dv{dcr * f.a, dcg * f.a, dcb * f.a, d_alpha_i};
+            V2 tdelta = mk(0, 0);
+            const Group& g = sc.groups[f.group_id];
+            int pi = f.is_stroke ? g.stroke : g.fill;
+            if (pi >= 0) d_sample_paint(sc, pi, *grads, pt, dv, &tdelta);
+            accumulate_translation(*grads, translation_index, tdelta);
+            dcr = dpr;
+            dcg = dpg;
+            dcb = dpb;
+            dca = d_prev_alpha;
+        }
+        if (background) accumulate_background_grad(sc, *grads, pixel_index, V4{dcr, dcg, dcb, dca});
+    }
+    return V4{fr, fg, fb, final_alpha};
+}
+
+// Premultiplied colour at canvas point pt (the crate's eval_scene_tiled output,
+// src/gpu/kernels/forward.rs:1131-1290, with the CPU inside / within tests).
+static V4 eval_premultiplied(const Scene& sc, const SceneBvh& bvh, V2 pt, V4 background) {
+    std::vector<Fragment> frags;
+    collect_fragments(sc, bvh, pt, nullptr, frags);
+    float pr = background.x, pg = background.y, pb = background.z, pa = background.w;
+    for (const Fragment& f : frags) {
+        float br = pr * (1.0f - f.a) + f.r * f.a;
+        float bg = pg * (1.0f - f.a) + f.g * f.a;
+        float bb = pb * (1.0f - f.a) + f.b * f.a;
+        float ba = pa * (1.0f - f.a) + f.a;
+        pr = br;
+        pg = bg;
+        pb = bb;
+        pa = ba;
+    }
+    return V4{pr, pg, pb, pa};
+}
+
+// ---------------------------------------------------------------- boundary sampling (backward/boundary.rs)
+struct ShapeCdf {
+    std::vector<size_t> shape_ids, group_ids;
+    std::vector<float> cdf, pmf;
+};
+struct PathCdf {
+    bool valid = false;
+    std::vector<float> cdf, pmf;
+    std::vector<size_t> point_id_map;
+    float length = 0.0f;
+};
+static V2 bez2(V2 p0, V2 p1, V2 p2, float t) {
+    float tt = 1.0f - t;
+    return p0 * (tt * tt) + p1 * (2.0f * tt * t) + p2 * (t * t);
+}
+static V2 bez3(V2 p0, V2 p1, V2 p2, V2 p3, float t) {
+    float tt = 1.0f - t;
+    return p0 * (tt * tt * tt) + p1 * (3.0f * tt * tt * t) + p2 * (3.0f * tt * t * t) + p3 * (t * t * t);
+}
+static float segment_length_est(const PathG& p, size_t point_id, uint8_t nc, bool* ok) {  // boundary.rs:237-307
+    V2 q0, q1, q2, q3;
+    *ok = true;
+    if (nc == 0) {
+        if (!path_point(p, point_id, &q0) || !path_point(p, point_id + 1, &q1)) {
+            *ok = false;
+            return 0.0f;
+        }
+        return length(q1 - q0);
+    }
+    if (nc == 1) {
+        if (!path_point(p, point_id, &q0) || !path_point(p, point_id + 1, &q1) || !path_point(p, point_id + 2, &q2)) {
+            *ok = false;
+            return 0.0f;
+        }
+        V2 v1 = bez2(q0, q1, q2, 0.5f);
+        return length(v1 - q0) + length(q2 - v1);
+    }
+    if (nc == 2) {
+        if (!path_point(p, point_id, &q0) || !path_point(p, point_id + 1, &q1) || !path_point(p, point_id + 2, &q2) ||
+            !path_point(p, point_id + 3, &q3)) {
+            *ok = false;
+            return 0.0f;
+        }
+        V2 v1 = bez3(q0, q1, q2, q3, 1.0f / 3.0f);
+        V2 v2 = bez3(q0, q1, q2, q3, 2.0f / 3.0f);
+        return length(v1 - q0) + length(v2 - v1) + length(q3 - v2);
+    }
+    *ok = false;
+    return 0.0f;
+}
+static float path_length(const PathG& p) {  // boundary.rs:230-309
+    if (p.pts.empty()) return 0.0f;
+    float len = 0.0f;
+    size_t point_id = 0;
+    for (uint8_t nc : p.ncp) {
+        bool ok;
+        float l = segment_length_est(p, point_id, nc, &ok);
+        if (!ok) break;
+        len += l;
+        point_id += nc == 0 ? 1 : (nc == 1 ? 2 : 3);
+    }
+    return len;
+}
+static std::vector<float> compute_shape_lengths(const Scene& sc) {  // boundary.rs:200-227
+    std::vector<float> out(sc.shapes.size(), 0.0f);
+    for (size_t i = 0; i < sc.shapes.size(); ++i) {
+        const Shape& s = sc.shapes[i];
+        float l = 0.0f;
+        if (s.kind == DVG_SHAPE_CIRCLE) {
+            l = 2.0f * PI_F * std::fabs(s.prm[2]);
+        } else if (s.kind == DVG_SHAPE_ELLIPSE) {
+            float a = std::fabs(s.prm[2]), b = std::fabs(s.prm[3]);
+            l = (a == 0.0f || b == 0.0f) ? 0.0f
+                                         : PI_F * (3.0f * (a + b) - std::sqrt((3.0f * a + b) * (a + 3.0f * b)));
+        } else if (s.kind == DVG_SHAPE_RECT) {
+            float w = std::fabs(s.prm[2] - s.prm[0]), h = std::fabs(s.prm[3] - s.prm[1]);
+            l = 2.0f * (w + h);
+        } else if (s.kind == DVG_SHAPE_PATH) {
+            l = path_length(s.path);
+        }
+        out[i] = l;
+    }
+    return out;
+}
+static bool build_shape_cdf(const Scene& sc, const std::vector<float>& lens, ShapeCdf* out) {  // boundary.rs:312-346
+    float accum = 0.0f;
+    for (size_t gi = 0; gi < sc.groups.size(); ++gi)
+        for (size_t si : sc.groups[gi].shape_ids) {
+            float l = si < lens.size() ? lens[si] : 0.0f;
+            out->shape_ids.push_back(si);
+            out->group_ids.push_back(gi);
+            accum += l;
+            out->cdf.push_back(accum);
+            out->pmf.push_back(l);
+        }
+    if (accum <= 0.0f || !std::isfinite(accum) || out->cdf.empty()) return false;
+    for (float& v : out->cdf) v /= accum;
+    for (float& v : out->pmf) v /= accum;
+    return true;
+}
+static std::vector<PathCdf> build_path_cdfs(const Scene& sc, const std::vector<float>& lens) {  // boundary.rs:349-451
+    std::vector<PathCdf> out(sc.shapes.size());
+    for (size_t si = 0; si < sc.shapes.size(); ++si) {
+        const Shape& s = sc.shapes[si];
+        if (s.kind != DVG_SHAPE_PATH) continue;
+        float l = lens[si];
+        if (l <= 0.0f || !std::isfinite(l)) continue;
+        if (s.path.ncp.empty()) continue;
+        float inv_length = 1.0f / l;
+        PathCdf pc;
+        size_t point_id = 0;
+        for (uint8_t nc : s.path.ncp) {
+            pc.point_id_map.push_back(point_id);
+            bool ok;
+            float seg_len = segment_length_est(s.path, point_id, nc, &ok);
+            if (!ok) seg_len = 0.0f;
+            if (nc == 0)
+                point_id += 1;
+            else if (nc == 1)
+                point_id += 2;
+            else if (nc == 2)
+                point_id += 3;
+            float seg_norm = seg_len * inv_length;
+            pc.pmf.push_back(seg_norm);
+            float acc = seg_norm + (pc.cdf.empty() ? 0.0f : pc.cdf.back());
+            pc.cdf.push_back(acc);
+        }
+        pc.length = l;
+        pc.valid = true;
+        out[si] = pc;
+    }
+    return out;
+}
+static size_t sample_cdf(const std::vector<float>& cdf, float u, float* t_out) {  // boundary.rs:454-469
+    if (cdf.empty()) {
+        *t_out = 0.0f;
+        return 0;
+    }
+    size_t idx = 0;
+    while (idx < cdf.size() && u > cdf[idx]) idx += 1;
+    if (idx >= cdf.size()) idx = cdf.size() - 1;
+    float prev = idx == 0 ? 0.0f : cdf[idx - 1];
+    float denom = std::fmax(cdf[idx] - prev, 1.0e-6f);
+    *t_out = clampf((u - prev) / denom, 0.0f, 1.0f);
+    return idx;
+}
+struct BData {
+    size_t base_point_id = 0, point_id = 0;
+    float t = 0.0f;
+    bool is_stroke = false;
+};
+static V2 sample_boundary_path(const PathG& path, const PathCdf& pc, float path_len, float t, V2* normal, float* pdf,
+                               BData* data, float stroke_direction, float stroke_radius) {  // boundary.rs:630-842
+    size_t num_points = path.pts.size();
+    size_t num_base = path.ncp.size();
+    if (num_points == 0 || num_base == 0) {
+        *pdf = 0.0f;
+        return mk(0, 0);
+    }
+    if (stroke_direction != 0.0f && !path.closed) {
+        float cap_length = 0.0f;
+        if (path.has_thick) {
+            if (!path.thick.empty()) cap_length = PI_F * (path.thick[0] + path.thick.back());
+        } else {
+            cap_length = 2.0f * PI_F * stroke_radius;
+        }
+        float denom = cap_length + path_len;
+        if (denom > 0.0f) {
+            float cap_prob = cap_length / denom;
+            if (t < cap_prob) {
+                t /= cap_prob;
+                *pdf *= cap_prob;
+                float r0 = stroke_radius, r1 = stroke_radius;
+                if (path.has_thick && !path.thick.empty()) {
+                    r0 = path.thick[0];
+                    r1 = path.thick.back();
+                }
+                float angle = 2.0f * PI_F * t;
+                if (stroke_direction < 0.0f) {
+                    V2 p0 = path.pts[0];
+                    V2 off = mk(r0 * std::cos(angle), r0 * std::sin(angle));
+                    *normal = normalize(off);
+                    *pdf /= 2.0f * PI_F * r0;
+                    data->base_point_id = 0;
+                    data->point_id = 0;
+                    data->t = 0.0f;
+                    return p0 + off;
+                } else {
+                    V2 p0 = path.pts[num_points - 1];
+                    V2 off = mk(r1 * std::cos(angle), r1 * std::sin(angle));
+                    *normal = normalize(off);
+                    *pdf /= 2.0f * PI_F * r1;
+                    data->base_point_id = num_base - 1;
+                    size_t controls = path.ncp[data->base_point_id];
+                    data->point_id = num_points >= 2 + controls ? num_points - (2 + controls) : 0;
+                    data->t = 1.0f;
+                    return p0 + off;
+                }
+            } else {
+                t = (t - cap_prob) / (1.0f - cap_prob);
+                *pdf *= 1.0f - cap_prob;
+            }
+        }
+    }
+    float local_t;
+    size_t sample_id = sample_cdf(pc.cdf, t, &local_t);
+    if (sample_id >= pc.point_id_map.size()) {
+        *pdf = 0.0f;
+        return mk(0, 0);
+    }
+    size_t point_id = pc.point_id_map[sample_id];
+    data->base_point_id = sample_id;
+    data->point_id = point_id;
+    data->t = local_t;
+    if (local_t < -1.0e-3f || local_t > 1.0f + 1.0e-3f) {
+        *pdf = 0.0f;
+        return mk(0, 0);
+    }
+    auto next_index = [&](size_t idx) -> size_t {
+        if (path.closed) return idx % num_points;
+        return std::min(idx, num_points >= 1 ? num_points - 1 : 0);
+    };
+    uint8_t nc = sample_id < path.ncp.size() ? path.ncp[sample_id] : 0;
+    float pmf = sample_id < pc.pmf.size() ? pc.pmf[sample_id] : 0.0f;
+    V2 q[4];
+    float r[4];
+    if (nc == 0) {
+        if (!path_point_radius(path, point_id, stroke_radius, &q[0], &r[0]) ||
+            !path_point_radius(path, next_index(point_id + 1), stroke_radius, &q[1], &r[1])) {
+            *pdf = 0.0f;
+            return mk(0, 0);
+        }
+        V2 tangent = q[1] - q[0];
+        float tan_len = length(tangent);
+        if (tan_len == 0.0f) {
+            *pdf = 0.0f;
+            return mk(0, 0);
+        }
+        *normal = mk(-tangent.y, tangent.x) / tan_len;
+        *pdf *= pmf / tan_len;
+        V2 out = q[0] + tangent * local_t;
+        if (stroke_direction != 0.0f) {
+            float rr = r[0] + local_t * (r[1] - r[0]);
+            out += *normal * (stroke_direction * rr);
+            if (stroke_direction < 0.0f) *normal = *normal * -1.0f;
+        }
+        return out;
+    }
+    if (nc == 1) {
+        if (!path_point_radius(path, point_id, stroke_radius, &q[0], &r[0]) ||
+            !path_point_radius(path, point_id + 1, stroke_radius, &q[1], &r[1]) ||
+            !path_point_radius(path, next_index(point_id + 2), stroke_radius, &q[2], &r[2])) {
+            *pdf = 0.0f;
+            return mk(0, 0);
+        }
+        float tt = 1.0f - local_t;
+        V2 ev = q[0] * (tt * tt) + q[1] * (2.0f * tt * local_t) + q[2] * (local_t * local_t);
+        V2 tangent = (q[1] - q[0]) * (2.0f * tt) + (q[2] - q[1]) * (2.0f * local_t);
+        float tan_len = length(tangent);
+        if (tan_len == 0.0f) {
+            *pdf = 0.0f;
+            return mk(0, 0);
+        }
+        *normal = mk(-tangent.y, tangent.x) / tan_len;
+        *pdf *= pmf / tan_len;
+        V2 out = ev;
+        if (stroke_direction != 0.0f) {
+            float rr = r[0] * (tt * tt) + r[1] * (2.0f * tt * local_t) + r[2] * (local_t * local_t);
+            out += *normal * (stroke_direction * rr);
+            if (stroke_direction < 0.0f) *normal = *normal * -1.0f;
+        }
+        return out;
+    }
+    if (nc == 2) {
+        if (!path_point_radius(path, point_id, stroke_radius, &q[0], &r[0]) ||
+            !path_point_radius(path, point_id + 1, stroke_radius, &q[1], &r[1]) ||
+            !path_point_radius(path, point_id + 2, stroke_radius, &q[2], &r[2]) ||
+            !path_point_radius(path, next_index(point_id + 3), stroke_radius, &q[3], &r[3])) {
+            *pdf = 0.0f;
+            return mk(0, 0);
+        }
+        float tt = 1.0f - local_t;
+        V2 ev = q[0] * (tt * tt * tt) + q[1] * (3.0f * tt * tt * local_t) + q[2] * (3.0f * tt * local_t * local_t) +
+                q[3] * (local_t * local_t * local_t);
+        V2 tangent = (q[1] - q[0]) * (3.0f * tt * tt) + (q[2] - q[1]) * (6.0f * tt * local_t) +
+                     (q[3] - q[2]) * (3.0f * local_t * local_t);
+        float tan_len = length(tangent);
+        if (tan_len == 0.0f) {
+            *pdf = 0.0f;
+            return mk(0, 0);
+        }
+        *normal = mk(-tangent.y, tangent.x) / tan_len;
+        *pdf *= pmf / tan_len;
+        V2 out = ev;
+        if (stroke_direction != 0.0f) {
+            float rr = r[0] * (tt * tt * tt) + r[1] * (3.0f * tt * tt * local_t) +
+                       r[2] * (3.0f * tt * local_t * local_t) + r[3] * (local_t * local_t * local_t);
+            out += *normal * (stroke_direction * rr);
+            if (stroke_direction < 0.0f) *normal = *normal * -1.0f;
+        }
+        return out;
+    }
+    *pdf = 0.0f;
+    return mk(0, 0);
+}
+static bool sample_boundary_point(const Scene& sc, size_t shape_id, size_t group_id, float t, float shape_length,
+                                  const PathCdf* pc, V2* pt_out, V2* normal_out, float* pdf_out,
+                                  BData* data) {  // boundary.rs:472-627
+    if (group_id >= sc.groups.size() || shape_id >= sc.shapes.size()) return false;
+    const Group& g = sc.groups[group_id];
+    const Shape& s = sc.shapes[shape_id];
+    if (g.fill < 0 && g.stroke < 0) return false;
+    float pdf = 1.0f;
+    float local_t = t;
+    bool stroke_perturb = false;
+    if (g.fill >= 0 && g.stroke >= 0) {
+        if (local_t < 0.5f) {
+            stroke_perturb = false;
+            local_t *= 2.0f;
+            pdf = 0.5f;
+        } else {
+            stroke_perturb = true;
+            local_t = 2.0f * (local_t - 0.5f);
+            pdf = 0.5f;
+        }
+    } else if (g.stroke >= 0) {
+        stroke_perturb = true;
+    }
+    float stroke_direction = 0.0f;
+    if (stroke_perturb) {
+        if (local_t < 0.5f) {
+            stroke_direction = -1.0f;
+            local_t *= 2.0f;
+            pdf *= 0.5f;
+        } else {
+            stroke_direction = 1.0f;
+            local_t = 2.0f * (local_t - 0.5f);
+            pdf *= 0.5f;
+        }
+    }
+    *data = BData();
+    data->is_stroke = stroke_perturb;
+    V2 normal = mk(0, 0);
+    V2 pt;
+    if (s.kind == DVG_SHAPE_CIRCLE) {
+        float r = std::fabs(s.prm[2]);
+        if (r <= 0.0f) return false;
+        float angle = 2.0f * PI_F * local_t;
+        V2 off = mk(r * std::cos(angle), r * std::sin(angle));
+        normal = normalize(off);
+        pdf /= 2.0f * PI_F * r;
+        V2 out = mk(s.prm[0], s.prm[1]) + off;
+        if (stroke_direction != 0.0f) {
+            out += normal * (stroke_direction * s.stroke_width);
+            if (stroke_direction < 0.0f) normal = normal * -1.0f;
+        }
+        pt = out;
+    } else if (s.kind == DVG_SHAPE_ELLIPSE) {
+        float rx = std::fabs(s.prm[2]), ry = std::fabs(s.prm[3]);
+        if (rx <= 0.0f || ry <= 0.0f) return false;
+        float angle = 2.0f * PI_F * local_t;
+        float sn = std::sin(angle), cs = std::cos(angle);
+        V2 off = mk(rx * cs, ry * sn);
+        float dxdt = -rx * sn * 2.0f * PI_F;
+        float dydt = ry * cs * 2.0f * PI_F;
+        normal = normalize(mk(dydt, -dxdt));
+        pdf /= std::sqrt(dxdt * dxdt + dydt * dydt);
+        V2 out = mk(s.prm[0], s.prm[1]) + off;
+        if (stroke_direction != 0.0f) {
+            out += normal * (stroke_direction * s.stroke_width);
+            if (stroke_direction < 0.0f) normal = normal * -1.0f;
+        }
+        pt = out;
+    } else if (s.kind == DVG_SHAPE_RECT) {
+        V2 mn = mk(s.prm[0], s.prm[1]), mx = mk(s.prm[2], s.prm[3]);
+        float w = mx.x - mn.x, h = mx.y - mn.y;
+        if (w == 0.0f && h == 0.0f) return false;
+        pdf /= 2.0f * (w + h);
+        V2 out = mk(0, 0);
+        if (local_t <= w / (w + h)) {
+            local_t *= (w + h) / w;
+            if (local_t < 0.5f) {
+                normal = mk(0.0f, -1.0f);
+                out = mn + mk(2.0f * local_t * (mx.x - mn.x), 0.0f);
+            } else {
+                normal = mk(0.0f, 1.0f);
+                out = mk(mn.x, mx.y) + mk(2.0f * (local_t - 0.5f) * (mx.x - mn.x), 0.0f);
+            }
+        } else {
+            local_t = (local_t - w / (w + h)) * (w + h) / h;
+            if (local_t < 0.5f) {
+                normal = mk(-1.0f, 0.0f);
+                out = mn + mk(0.0f, 2.0f * local_t * (mx.y - mn.y));
+            } else {
+                normal = mk(1.0f, 0.0f);
+                out = mk(mx.x, mn.y) + mk(0.0f, 2.0f * (local_t - 0.5f) * (mx.y - mn.y));
+            }
+        }
+        if (stroke_direction != 0.0f) {
+            out += normal * (stroke_direction * s.stroke_width);
+            if (stroke_direction < 0.0f) normal = normal * -1.0f;
+        }
+        pt = out;
+    } else if (s.kind == DVG_SHAPE_PATH) {
+        if (!pc || !pc->valid) return false;
+        if (pc->length <= 0.0f) return false;
+        pt = sample_boundary_path(s.path, *pc, shape_length, local_t, &normal, &pdf, data, stroke_direction,
+                                  s.stroke_width);
+    } else {
+        return false;
+    }
+    if (!std::isfinite(pdf) || pdf <= 0.0f) return false;
+    *pt_out = pt;
+    *normal_out = normal;
+    *pdf_out = pdf;
+    return true;
+}
+static void accumulate_boundary_gradient(const Shape& s, size_t shape_id, float contrib, float t, V2 normal,
+                                         const BData& bd, Grads& g, const M3& group_s2c, V2 local_pt,
+                                         size_t group_id) {  // boundary.rs:970-1148
+    if (!std::isfinite(contrib)) return;
+    const PathG& path = s.path;
+    size_t pbase = path.point_base;
+    if (bd.is_stroke) {
+        bool has_thick = s.kind == DVG_SHAPE_PATH && path.has_thick;
+        if (has_thick) {
+            size_t n = path.thick.size();
+            auto addt = [&](size_t i, float v) {
+                if (i < n) g.thickness[pbase + i] += v;
+            };
+            size_t pid = bd.point_id;
+            float t2 = bd.t;
+            uint8_t nc = bd.base_point_id < path.ncp.size() ? path.ncp[bd.base_point_id] : 0;
+            size_t np = path.pts.size();
+            if (nc == 0) {
+                size_t i1 = path.closed ? (pid + 1) % np : pid + 1;
+                addt(pid, (1.0f - t2) * contrib);
+                addt(i1, t2 * contrib);
+            } else if (nc == 1) {
+                size_t i2 = path.closed ? (pid + 2) % np : pid + 2;
+                float tt = 1.0f - t2;
+                addt(pid, tt * tt * contrib);
+                addt(pid + 1, 2.0f * tt * t2 * contrib);
+                addt(i2, t2 * t2 * contrib);
+            } else if (nc == 2) {
+                size_t i3 = path.closed ? (pid + 3) % np : pid + 3;
+                float tt = 1.0f - t2;
+                addt(pid, tt * tt * tt * contrib);
+                addt(pid + 1, 3.0f * tt * tt * t2 * contrib);
+                addt(pid + 2, 3.0f * tt * t2 * t2 * contrib);
+                addt(i3, t2 * t2 * t2 * contrib);
+            }
+        } else {
+            g.stroke_width[shape_id] += contrib;
+        }
+    }
+    float* dp = &g.shape_params[4 * shape_id];
+    if (s.kind == DVG_SHAPE_CIRCLE) {
+        dp[0] += normal.x * contrib;
+        dp[1] += normal.y * contrib;
+        dp[2] += contrib;
+    } else if (s.kind == DVG_SHAPE_ELLIPSE) {
+        dp[0] += normal.x * contrib;
+        dp[1] += normal.y * contrib;
+        float angle = 2.0f * PI_F * t;
+        dp[2] += std::cos(angle) * normal.x * contrib;
+        dp[3] += std::sin(angle) * normal.y * contrib;
+    } else if (s.kind == DVG_SHAPE_PATH) {
+        size_t np = path.pts.size();
+        auto add_point = [&](size_t idx, float w) {
+            size_t index = path.closed ? idx % np : idx;
+            if (index < np) {
+                g.points[2 * (pbase + index)] += normal.x * (w * contrib);
+                g.points[2 * (pbase + index) + 1] += normal.y * (w * contrib);
+            }
+        };
+        size_t pid = bd.point_id;
+        float t2 = bd.t;
+        uint8_t nc = bd.base_point_id < path.ncp.size() ? path.ncp[bd.base_point_id] : 0;
+        if (nc == 0) {
+            add_point(pid, 1.0f - t2);
+            add_point(pid + 1, t2);
+        } else if (nc == 1) {
+            float tt = 1.0f - t2;
+            add_point(pid, tt * tt);
+            add_point(pid + 1, 2.0f * tt * t2);
+            add_point(pid + 2, t2 * t2);
+        } else if (nc == 2) {
+            float tt = 1.0f - t2;
+            add_point(pid, tt * tt * tt);
+            add_point(pid + 1, 3.0f * tt * tt * t2);
+            add_point(pid + 2, 3.0f * tt * t2 * t2);
+            add_point(pid + 3, t2 * t2 * t2);
+        }
+    } else if (s.kind == DVG_SHAPE_RECT) {
+        if (normal == mk(-1.0f, 0.0f))
+            dp[0] += -contrib;
+        else if (normal == mk(1.0f, 0.0f))
+            dp[2] += contrib;
+        else if (normal == mk(0.0f, -1.0f))
+            dp[1] += -contrib;
+        else if (normal == mk(0.0f, 1.0f))
+            dp[3] += contrib;
+    }
+    M3 s2c = mul3(group_s2c, s.transform);
+    M3 d_s2c = zero3();
+    V2 d_lp = mk(0, 0);
+    d_xform_pt(s2c, local_pt, normal * contrib, &d_s2c, &d_lp);
+    M3 d_group = mul3(d_s2c, transpose3(s.transform));
+    M3 d_shape = mul3(transpose3(group_s2c), d_s2c);
+    float* dg = &g.group_transform[9 * group_id];
+    float* ds = &g.shape_transform[9 * shape_id];
+    for (int i = 0; i < 9; ++i) {
+        dg[i] = dg[i] + d_group.m[i / 3][i % 3];
+        ds[i] = ds[i] + d_shape.m[i / 3][i % 3];
+    }
+}
+struct BoundaryTables {
+    std::vector<float> lens;
+    ShapeCdf cdf;
+    bool ok = false;
+    std::vector<PathCdf> path_cdfs;
+};
+static BoundaryTables build_boundary_tables(const Scene& sc) {
+    BoundaryTables bt;
+    if (sc.groups.empty()) return bt;
+    bt.lens = compute_shape_lengths(sc);
+    bt.ok = build_shape_cdf(sc, bt.lens, &bt.cdf);
+    bt.path_cdfs = build_path_cdfs(sc, bt.lens);
+    return bt;
+}
+// One boundary sample (boundary.rs:141-196 + render_edge_sample 845-967).
+static void boundary_sample(const Scene& sc, const SceneBvh& bvh, const BoundaryTables& bt, uint64_t idx,
+                            uint32_t rng_kind, uint32_t seed, const float* d_render, const std::vector<float>& wimg,
+                            Grads& g, bool compute_translation) {
+    float u, t;
+    boundary_rng(rng_kind, idx, seed, &u, &t);
+    float dummy;
+    size_t sample_id = sample_cdf(bt.cdf.cdf, u, &dummy);
+    if (sample_id >= bt.cdf.shape_ids.size()) return;
+    size_t shape_id = bt.cdf.shape_ids[sample_id];
+    size_t group_id = bt.cdf.group_ids[sample_id];
+    float shape_pmf = sample_id < bt.cdf.pmf.size() ? bt.cdf.pmf[sample_id] : 0.0f;
+    if (shape_pmf <= 0.0f) return;
+    float shape_length = shape_id < bt.lens.size() ? bt.lens[shape_id] : 0.0f;
+    const PathCdf* pc = shape_id < bt.path_cdfs.size() ? &bt.path_cdfs[shape_id] : nullptr;
+    V2 local_pt, normal;
+    float bpdf;
+    BData data;
+    if (!sample_boundary_point(sc, shape_id, group_id, t, shape_length, pc, &local_pt, &normal, &bpdf, &data)) return;
+    if (bpdf <= 0.0f) return;
+    const Group& grp = sc.groups[group_id];
+    const Shape& shp = sc.shapes[shape_id];
+    M3 s2c = mul3(grp.s2c, shp.transform);
+    V2 bpt = xform_pt(s2c, local_pt);
+    M3 shape_inv;
+    if (!inverse3(shp.transform, &shape_inv)) shape_inv = identity3();
+    M3 composite_inv = mul3(shape_inv, grp.c2s);
+    V2 normal_canvas = xform_normal(composite_inv, normal);
+    bpt.x /= (float)sc.w;
+    bpt.y /= (float)sc.h;
+    float pdf = shape_pmf * bpdf;
+    // render_edge_sample
+    int width = (int)sc.w, height = (int)sc.h;
+    if (width <= 0 || height <= 0) return;
+    if (pdf <= 0.0f) return;
+    int bx = to_i32(bpt.x * (float)width), by = to_i32(bpt.y * (float)height);
+    if (bx < 0 || bx >= width || by < 0 || by >= height) return;
+    size_t pixel_index = (size_t)by * width + bx;
+    V4 bg = sample_background(sc, pixel_index);
+    EdgeQuery iq{group_id, shape_id, false}, oq{group_id, shape_id, false};
+    V2 n = normal_canvas;
+    V4 ci = sample_color(sc, bvh, bpt - n * 1.0e-4f, &bg, nullptr, &iq, nullptr, -1, pixel_index);
+    V4 co = sample_color(sc, bvh, bpt + n * 1.0e-4f, &bg, nullptr, &oq, nullptr, -1, pixel_index);
+    if (!iq.hit && !oq.hit) return;
+    if (!iq.hit) {
+        n = n * -1.0f;
+        std::swap(ci, co);
+    }
+    V2 sbp = mk(bpt.x * (float)width, bpt.y * (float)height);
+    V4 dc = gather_d_color(sc, d_render, wimg, sbp);
+    float norm = (float)sc.w * (float)sc.h;
+    if (norm > 0.0f) {
+        dc.x /= norm;
+        dc.y /= norm;
+        dc.z /= norm;
+        dc.w /= norm;
+    }
+    V4 diff{ci.x - co.x, ci.y - co.y, ci.z - co.z, ci.w - co.w};
+    float contrib = dot4(diff, dc) / pdf;
+    if (!std::isfinite(contrib)) return;
+    accumulate_boundary_gradient(shp, shape_id, contrib, t, n, data, g, grp.s2c, local_pt, group_id);
+    if (compute_translation && g.has_translation) {
+        size_t ti = pixel_index * 2;
+        if (ti + 1 < g.translation.size()) {
+            g.translation[ti] += n.x * contrib;
+            g.translation[ti + 1] += n.y * contrib;
+        }
+    }
+}
+
+// Interior sample (render.rs:95-169).
+static void interior_sample(const Scene& sc, const SceneBvh& bvh, const SampleSpec& sp, uint64_t idx,
+                            const float* d_render, const std::vector<float>& wimg, Grads& g, bool translation) {
+    V2 pt;
+    size_t pixel_index;
+    sample_position(sc, sp, idx, &pt, &pixel_index);
+    V2 npt = mk(pt.x / (float)sc.w, pt.y / (float)sc.h);
+    V4 bg = sample_background(sc, pixel_index);
+    V4 dcol = gather_d_color(sc, d_render, wimg, pt);
+    V4 color = sample_color(sc, bvh, npt, &bg, &dcol, nullptr, &g, translation ? (long)pixel_index : -1, pixel_index);
+    accumulate_filter_gradient(sc, color, d_render, wimg, pt, &g.filter_radius);
+}
+
+static void export_grads(const Grads& g, dvg_grads* out, const dvg_scene_desc* d) {
+    auto cp = [](float* dst, const std::vector<float>& v) {
+        if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(float));
+    };
+    cp(out->d_shape_params, g.shape_params);
+    cp(out->d_shape_transform, g.shape_transform);
+    cp(out->d_shape_stroke_width, g.stroke_width);
+    cp(out->d_points, g.points);
+    cp(out->d_thickness, g.thickness);
+    cp(out->d_group_transform, g.group_transform);
+    cp(out->d_paint_params, g.paint_params);
+    cp(out->d_stop_offsets, g.stop_offsets);
+    cp(out->d_stop_colors, g.stop_colors);
+    if (out->d_filter_radius) out->d_filter_radius[0] = g.filter_radius;
+    if (out->d_background)
+        for (int i = 0; i < 4; ++i) out->d_background[i] = g.background[i];
+    if (out->d_background_image) {
+        if (g.has_bg_image)
+            cp(out->d_background_image, g.bg_image);
+        else
+            std::memset(out->d_background_image, 0, (size_t)d->width * d->height * 4 * sizeof(float));
+    }
+    if (out->d_translation) {
+        if (g.has_translation)
+            cp(out->d_translation, g.translation);
+        else
+            std::memset(out->d_translation, 0, (size_t)d->width * d->height * 2 * sizeof(float));
+    }
+}
+
+template <typename F>
+static void parallel_for(uint64_t begin, uint64_t end, int threads, F&& body) {
+    if (threads <= 1 || end - begin < 1024) {
+        body(0, begin, end);
+        return;
+    }
+    std::vector<std::thread> pool;
+    uint64_t n = end - begin;
+    for (int t = 0; t < threads; ++t) {
+        uint64_t b = begin + n * t / threads, e = begin + n * (t + 1) / threads;
+        pool.emplace_back([&, t, b, e]() { body(t, b, e); });
+    }
+    for (auto& th : pool) th.join();
+}
+
+}  // namespace orc
+
+using namespace orc;
+
+static SampleSpec make_spec(const dvg_render_options* o) {
+    SampleSpec sp;
+    sp.sx_n = o->samples_x > 0 ? o->samples_x : 1;
+    sp.sy_n = o->samples_y > 0 ? o->samples_y : 1;
+    sp.prefilter = o->use_prefiltering != 0;
+    sp.jitter = o->jitter != 0 && !sp.prefilter;
+    sp.seed = o->seed;
+    return sp;
+}
+
+extern "C" int oracle_weight_image(const dvg_scene_desc* desc, const dvg_render_options* opts, float* out_w) {
+    Scene sc = decode(desc);
+    std::vector<float> w = build_weight_image(sc, make_spec(opts));
+    std::memcpy(out_w, w.data(), w.size() * sizeof(float));
+    return 0;
+}
+
+extern "C" int oracle_sample_premultiplied(const dvg_scene_desc* desc, const dvg_render_options* opts, float px,
+                                           float py, float* out4) {
+    (void)opts;
+    Scene sc = decode(desc);
+    SceneBvh bvh = build_scene_bvh(sc);
+    int x = to_i32(std::floor(px)), y = to_i32(std::floor(py));
+    size_t pix = (x >= 0 && y >= 0 && x < (int)sc.w && y < (int)sc.h) ? (size_t)y * sc.w + x : 0;
+    V4 c = eval_premultiplied(sc, bvh, mk(px, py), sample_background(sc, pix));
+    out4[0] = c.x;
+    out4[1] = c.y;
+    out4[2] = c.z;
+    out4[3] = c.w;
+    return 0;
+}
+
+// Forward image with the crate's GPU semantics: rasterize_weights_f32, rasterize_splat_f32
+// and resolve_splat_f32 (src/gpu/kernels/forward.rs:1505-1735, 294-334), with the early
+// outs of Renderer::render (src/renderer/renderer.rs:40-66).
+extern "C" int oracle_render(const dvg_scene_desc* desc, const dvg_render_options* opts, float* out) {
+    Scene sc = decode(desc);
+    if (sc.w == 0 || sc.h == 0) return 0;
+    size_t npix = (size_t)sc.w * sc.h;
+    if (sc.groups.empty()) {
+        for (size_t i = 0; i < npix; ++i)
+            if (sc.has_bg_img)
+                for (int k = 0; k < 4; ++k) out[4 * i + k] = sc.bg_img[4 * i + k];
+            else {
+                out[4 * i] = sc.bg.r;
+                out[4 * i + 1] = sc.bg.g;
+                out[4 * i + 2] = sc.bg.b;
+                out[4 * i + 3] = sc.bg.a;
+            }
+        return 0;
+    }
+    SampleSpec sp = make_spec(opts);
+    SceneBvh bvh = build_scene_bvh(sc);
+    std::vector<float> wimg((size_t)npix, 0.0f);
+    uint64_t total = (uint64_t)npix * sp.sx_n * sp.sy_n;
+    int ri = to_i32(std::ceil(sc.filter_radius));
+    if (ri < 0) ri = 0;
+    int width = (int)sc.w, height = (int)sc.h;
+    for (uint64_t idx = 0; idx < total; ++idx) {
+        V2 pt;
+        size_t pix;
+        sample_position(sc, sp, idx, &pt, &pix);
+        int x = (int)(pix % sc.w), y = (int)(pix / sc.w);
+        for (int dy = -ri; dy <= ri; ++dy)
+            for (int dx = -ri; dx <= ri; ++dx) {
+                int xx = x + dx, yy = y + dy;
+                if (xx >= 0 && yy >= 0 && xx < width && yy < height) {
+                    float w = compute_filter_weight(sc.filter_type, sc.filter_radius, (float)xx + 0.5f - pt.x,
+                                                    (float)yy + 0.5f - pt.y);
+                    if (w > 0.0f) wimg[(size_t)yy * width + xx] += w;
+                }
+            }
+    }
+    std::vector<float> acc(npix * 4, 0.0f);
+    for (uint64_t idx = 0; idx < total; ++idx) {
+        V2 pt;
+        size_t pix;
+        sample_position(sc, sp, idx, &pt, &pix);
+        int x = (int)(pix % sc.w), y = (int)(pix / sc.w);
+        V4 c = eval_premultiplied(sc, bvh, pt, sample_background(sc, pix));
+        for (int dy = -ri; dy <= ri; ++dy)
+            for (int dx = -ri; dx <= ri; ++dx) {
+                int xx = x + dx, yy = y + dy;
+                if (xx >= 0 && yy >= 0 && xx < width && yy < height) {
+                    size_t b = (size_t)yy * width + xx;
+                    float ws = wimg[b];
+                    if (ws > 0.0f) {
+                        float w = compute_filter_weight(sc.filter_type, sc.filter_radius, (float)xx + 0.5f - pt.x,
+                                                        (float)yy + 0.5f - pt.y);
+                        if (w > 0.0f) {
+                            float wn = w / ws;
+                            acc[4 * b] += c.x * wn;
+                            acc[4 * b + 1] += c.y * wn;
+                            acc[4 * b + 2] += c.z * wn;
+                            acc[4 * b + 3] += c.w * wn;
+                        }
+                    }
+                }
+            }
+    }
+    for (size_t i = 0; i < npix; ++i) {
+        float r = sc.bg.r, g = sc.bg.g, b = sc.bg.b, a = sc.bg.a;
+        if (wimg[i] > 0.0f) {
+            r = acc[4 * i];
+            g = acc[4 * i + 1];
+            b = acc[4 * i + 2];
+            a = acc[4 * i + 3];
+        }
+        if (a > 1.0e-8f) {
+            r = r / a;
+            g = g / a;
+            b = b / a;
+        }
+        out[4 * i] = r;
+        out[4 * i + 1] = g;
+        out[4 * i + 2] = b;
+        out[4 * i + 3] = a;
+    }
+    return 0;
+}
+
+extern "C" int oracle_render_backward_ex(const dvg_scene_desc* desc, const dvg_render_options* opts,
+                                         const dvg_backward_options* bopts, const float* d_render, dvg_grads* out,
+                                         int passes, int threads, unsigned long long sample_begin,
+                                         unsigned long long sample_end) {
+    Scene sc = decode(desc);
+    bool translation = bopts && bopts->compute_translation;
+    bool include_bg_img = d_render != nullptr && sc.has_bg_img;
+    Grads grads;
+    grads.init(sc, desc, include_bg_img, translation);
+    if (sc.w == 0 || sc.h == 0) {
+        export_grads(grads, out, desc);
+        return 0;
+    }
+    SampleSpec sp = make_spec(opts);
+    uint64_t total = (uint64_t)sc.w * sc.h * sp.sx_n * sp.sy_n;
+    SceneBvh bvh = build_scene_bvh(sc);
+    if (d_render) {
+        std::vector<float> wimg = build_weight_image(sc, sp);
+        int nthreads = threads > 1 ? threads : 1;
+        std::vector<Grads> tg(nthreads);
+        for (auto& g : tg) g.init(sc, desc, include_bg_img, translation);
+        if (passes & 1) {
+            uint64_t b = sample_begin, e = sample_end ? std::min<uint64_t>(sample_end, total) : total;
+            parallel_for(b, e, nthreads, [&](int t, uint64_t lo, uint64_t hi) {
+                for (uint64_t idx = lo; idx < hi; ++idx) interior_sample(sc, bvh, sp, idx, d_render, wimg, tg[t], translation);
+            });
+        }
+        if ((passes & 2) && !sp.prefilter) {
+            BoundaryTables bt = build_boundary_tables(sc);
+            if (bt.ok) {
+                uint64_t nb = bopts && bopts->boundary_samples ? bopts->boundary_samples : total;
+                uint32_t rng = bopts ? bopts->rng : 0;
+                uint32_t seed = (bopts && !bopts->boundary_seed_from_options) ? bopts->boundary_seed : opts->seed;
+                uint64_t b = sample_begin, e = sample_end ? std::min<uint64_t>(sample_end, nb) : nb;
+                parallel_for(b, e, nthreads, [&](int t, uint64_t lo, uint64_t hi) {
+                    for (uint64_t idx = lo; idx < hi; ++idx)
+                        boundary_sample(sc, bvh, bt, idx, rng, seed, d_render, wimg, tg[t], translation);
+                });
+            }
+        }
+        for (auto& g : tg) grads.add(g);
+    }
+    finalize_background_gradients(sc, grads);
+    export_grads(grads, out, desc);
+    return 0;
+}
+
+extern "C" int oracle_render_backward(const dvg_scene_desc* desc, const dvg_render_options* opts,
+                                      const dvg_backward_options* bopts, const float* d_render, dvg_grads* out) {
+    return oracle_render_backward_ex(desc, opts, bopts, d_render, out, 3, 1, 0, 0);
+}
+
+extern "C" int oracle_compute_distance(const dvg_scene_desc* desc, uint32_t group, float px, float py,
+                                       float max_radius, int use_bvh, float* out4) {
+    Scene sc = decode(desc);
+    ClosestPoint cp;
+    bool ok;
+    if (use_bvh) {
+        SceneBvh bvh = build_scene_bvh(sc);
+        ok = compute_distance_bvh(sc, bvh, group, mk(px, py), max_radius, &cp);
+    } else {
+        ok = compute_distance(sc, group, mk(px, py), max_radius, &cp);
+    }
+    if (!ok) return 0;
+    out4[0] = (float)cp.shape_index;
+    out4[1] = cp.point.x;
+    out4[2] = cp.point.y;
+    out4[3] = cp.distance;
+    return 1;
+}
+
+extern "C" int oracle_within_distance(const dvg_scene_desc* desc, uint32_t group, float px, float py, int use_bvh) {
+    Scene sc = decode(desc);
+    if (use_bvh) {
+        SceneBvh bvh = build_scene_bvh(sc);
+        return within_distance_bvh(sc, bvh, group, mk(px, py)) ? 1 : 0;
+    }
+    return within_distance(sc, group, mk(px, py)) ? 1 : 0;
+}
+
+extern "C" int oracle_is_inside(const dvg_scene_desc* desc, uint32_t group, float px, float py, int use_bvh) {
+    Scene sc = decode(desc);
+    if (use_bvh) {
+        SceneBvh bvh = build_scene_bvh(sc);
+        return is_inside_bvh(sc, bvh, group, mk(px, py)) ? 1 : 0;
+    }
+    return is_inside(sc, group, mk(px, py)) ? 1 : 0;
+}
+
+// Path::flatten (geometry.rs:206-308) — recursive subdivision of quadratic / cubic segments.
+namespace orc {
+static float distance_point_line(V2 p, V2 a, V2 b) {  // geometry.rs:493-503
+    V2 ab = b - a, ap = p - a;
+    float area = std::fabs(cross(ab, ap));
+    float len = length(ab);
+    return len == 0.0f ? length(ap) : area / len;
+}
+static void flatten_quad(V2 p0, V2 p1, V2 p2, float tol, uint32_t depth, std::vector<V2>& out) {
+    if (depth >= 16 || distance_point_line(p1, p0, p2) <= tol) {
+        out.push_back(p0);
+        out.push_back(p2);
+        return;
+    }
+    V2 p01 = lerp(p0, p1, 0.5f), p12 = lerp(p1, p2, 0.5f), p012 = lerp(p01, p12, 0.5f);
+    flatten_quad(p0, p01, p012, tol, depth + 1, out);
+    flatten_quad(p012, p12, p2, tol, depth + 1, out);
+}
+static void flatten_cubic(V2 p0, V2 p1, V2 p2, V2 p3, float tol, uint32_t depth, std::vector<V2>& out) {
+    float d = std::fmax(distance_point_line(p1, p0, p3), distance_point_line(p2, p0, p3));
+    if (depth >= 16 || d <= tol) {
+        out.push_back(p0);
+        out.push_back(p3);
+        return;
+    }
+    V2 p01 = lerp(p0, p1, 0.5f), p12 = lerp(p1, p2, 0.5f), p23 = lerp(p2, p3, 0.5f);
+    V2 p012 = lerp(p01, p12, 0.5f), p123 = lerp(p12, p23, 0.5f), p0123 = lerp(p012, p123, 0.5f);
+    flatten_cubic(p0, p01, p012, p0123, tol, depth + 1, out);
+    flatten_cubic(p0123, p123, p23, p3, tol, depth + 1, out);
+}
+}  // namespace orc
+
+extern "C" int oracle_flatten(const dvg_scene_desc* desc, uint32_t shape, float tolerance, float* out, int cap) {
+    Scene sc = decode(desc);
+    if (shape >= sc.shapes.size() || sc.shapes[shape].kind != DVG_SHAPE_PATH) return 0;
+    const PathG& p = sc.shapes[shape].path;
+    std::vector<V2> segs;
+    if (p.ncp.empty() || p.pts.empty()) return 0;
+    size_t point_id = 0;
+    for (uint8_t nc : p.ncp) {
+        V2 q[4];
+        if (nc == 0) {
+            if (!path_point(p, point_id, &q[0]) || !path_point(p, point_id + 1, &q[1])) break;
+            segs.push_back(q[0]);
+            segs.push_back(q[1]);
+            point_id += 1;
+        } else if (nc == 1) {
+            if (!path_point(p, point_id, &q[0]) || !path_point(p, point_id + 1, &q[1]) ||
+                !path_point(p, point_id + 2, &q[2]))
+                break;
+            flatten_quad(q[0], q[1], q[2], tolerance, 0, segs);
+            point_id += 2;
+        } else if (nc == 2) {
+            if (!path_point(p, point_id, &q[0]) || !path_point(p, point_id + 1, &q[1]) ||
+                !path_point(p, point_id + 2, &q[2]) || !path_point(p, point_id + 3, &q[3]))
+                break;
+            flatten_cubic(q[0], q[1], q[2], q[3], tolerance, 0, segs);
+            point_id += 3;
+        } else {
+            break;
+        }
+    }
+    int n = (int)(segs.size() / 2);
+    for (int i = 0; i < n && i < cap; ++i) {
+        out[4 * i] = segs[2 * i].x;
+        out[4 * i + 1] = segs[2 * i].y;
+        out[4 * i + 2] = segs[2 * i + 1].x;
+        out[4 * i + 3] = segs[2 * i + 1].y;
+    }
+    return n;
+}
+
+extern "C" void oracle_pcg32_floats(unsigned long long idx, unsigned long long seed, int n, float* out) {
+    Pcg32 rng(idx, seed);
+    for (int i = 0; i < n; ++i) out[i] = rng.next_f32();
+}
+
+extern "C" void oracle_philox_floats(unsigned long long idx, unsigned int seed, float* out2) {
+    boundary_rng(DVG_RNG_PHILOX, idx, seed, &out2[0], &out2[1]);
+}
+
+extern "C" int oracle_path_bvh(const dvg_scene_desc* desc, uint32_t shape, float* nodes, int node_cap, int* indices,
+                               int index_cap, int* num_indices) {
+    Scene sc = decode(desc);
+    if (shape >= sc.shapes.size()) return 0;
+    PathBvh pb;
+    if (!build_path_bvh(sc.shapes[shape], &pb)) return 0;
+    int n = (int)pb.nodes.size();
+    for (int i = 0; i < n && i < node_cap; ++i) {
+        const BvhNode& nd = pb.nodes[i];
+        float* o = nodes + 8 * i;
+        o[0] = nd.bounds.min.x;
+        o[1] = nd.bounds.min.y;
+        o[2] = nd.bounds.max.x;
+        o[3] = nd.bounds.max.y;
+        o[4] = nd.left == BVH_NONE ? -1.0f : (float)nd.left;
+        o[5] = nd.right == BVH_NONE ? -1.0f : (float)nd.right;
+        o[6] = (float)nd.start;
+        o[7] = (float)nd.count;
+    }
+    *num_indices = (int)pb.indices.size();
+    for (int i = 0; i < (int)pb.indices.size() && i < index_cap; ++i) indices[i] = (int)pb.indices[i];
+    return n;
+}
+
+extern "C" int oracle_count_segment_tests(const dvg_scene_desc* desc, const dvg_render_options* opts,
+                                          unsigned long long* out3) {
+    // out3[0..2]: fill ray-test passes per segment kind (line, quad, cubic);
+    // out3[3..5]: stroke padded-bounds hits per kind.
+    Scene sc = decode(desc);
+    SampleSpec sp = make_spec(opts);
+    for (int i = 0; i < 6; ++i) out3[i] = 0;
+    std::vector<PathBvh> pbs(sc.shapes.size());
+    std::vector<char> has(sc.shapes.size(), 0);
+    for (size_t i = 0; i < sc.shapes.size(); ++i) has[i] = build_path_bvh(sc.shapes[i], &pbs[i]);
+    uint64_t total = (uint64_t)sc.w * sc.h * sp.sx_n * sp.sy_n;
+    for (uint64_t idx = 0; idx < total; ++idx) {
+        V2 pt;
+        size_t pix;
+        sample_position(sc, sp, idx, &pt, &pix);
+        for (const Group& g : sc.groups) {
+            V2 lp = xform_pt(g.c2s, pt);
+            for (size_t si : g.shape_ids) {
+                if (si >= sc.shapes.size() || !has[si]) continue;
+                V2 spt = xform_inv_dist(sc.shapes[si].transform, lp);
+                for (const SegData& s : pbs[si].segments) {
+                    if (g.fill >= 0 && !(spt.y < s.bounds.min.y || spt.y > s.bounds.max.y || spt.x > s.bounds.max.x))
+                        out3[s.kind] += 1;
+                    if (g.stroke >= 0 && sc.shapes[si].stroke_width > 0.0f && s.bounds.contains(spt))
+                        out3[3 + s.kind] += 1;
+                }
+            }
+        }
+    }
+    return 0;
+}

@@ -1,0 +1,82 @@
+/*
+ * oracle.h — CPU oracle for the diffvg render / backward hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is a restatement, in C++, of the diffvg-rs
+ * crate's CPU arithmetic (the .rs files under src/backward and src/distance,
+ * src/geometry.rs, src/math.rs, src/renderer/rng.rs) and of its GPU forward
+ * image pipeline (src/gpu/kernels/forward.rs splat + resolve).  It is linked
+ * only by the tests, by __graft_entry__.smoke() and by bench.py's CPU
+ * baseline / reference arm — never by the product library.
+ *
+ * Parity status: pinned against the crate's own known-answer tests
+ * (src/distance/tests.rs:7-136, src/geometry.rs:509-519).  Render and
+ * gradient outputs are otherwise "parity unpinned": the crate has no tests
+ * for them and cannot be built here (no Rust toolchain, no graphics stack).
+ */
+#ifndef DVG_ORACLE_H
+#define DVG_ORACLE_H
+
+#include "../include/dvg.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Forward image with the crate's GPU pipeline semantics (weights -> splat -> resolve). */
+int oracle_render(const dvg_scene_desc* desc, const dvg_render_options* opts, float* out_rgba);
+
+/* Per-sample premultiplied colour at canvas point (px,py) (eval_scene semantics). */
+int oracle_sample_premultiplied(const dvg_scene_desc* desc, const dvg_render_options* opts,
+                                float px, float py, float* out4);
+
+/* The crate's CPU render_backward (src/backward/render.rs:35-210).  grads are host
+ * buffers that are overwritten (NULL parts skipped, sizes as in dvg.h).  bopts->rng
+ * selects the boundary generator (PCG32 as the crate, or Philox4x32-10). */
+int oracle_render_backward(const dvg_scene_desc* desc, const dvg_render_options* opts,
+                           const dvg_backward_options* bopts, const float* d_render,
+                           dvg_grads* grads);
+
+/* Same, with the interior (per-sample) pass and the boundary pass selectable:
+ * passes bit0 = interior, bit1 = boundary; threads > 1 runs the sample loops on
+ * that many host threads with per-thread gradient buffers. */
+int oracle_render_backward_ex(const dvg_scene_desc* desc, const dvg_render_options* opts,
+                              const dvg_backward_options* bopts, const float* d_render,
+                              dvg_grads* grads, int passes, int threads,
+                              unsigned long long sample_begin, unsigned long long sample_end);
+
+/* Weight image (build_weight_image, src/backward/filters.rs:11-67). */
+int oracle_weight_image(const dvg_scene_desc* desc, const dvg_render_options* opts, float* out_w);
+
+/* Distance API (src/distance/api.rs) used by the crate's known-answer tests.
+ * Returns 1 and fills out (shape_index, point.x, point.y, distance) when a hit exists. */
+int oracle_compute_distance(const dvg_scene_desc* desc, uint32_t group, float px, float py,
+                            float max_radius, int use_bvh, float* out4);
+int oracle_within_distance(const dvg_scene_desc* desc, uint32_t group, float px, float py,
+                           int use_bvh);
+int oracle_is_inside(const dvg_scene_desc* desc, uint32_t group, float px, float py, int use_bvh);
+
+/* Path::flatten (src/geometry.rs:206-212) of shape `shape`; writes up to cap segments
+ * as (x0,y0,x1,y1) and returns the number of segments. */
+int oracle_flatten(const dvg_scene_desc* desc, uint32_t shape, float tolerance, float* out,
+                   int cap);
+
+/* PCG32 (src/renderer/rng.rs:16-43): first n floats of Pcg32::new(idx, seed). */
+void oracle_pcg32_floats(unsigned long long idx, unsigned long long seed, int n, float* out);
+/* Philox4x32-10 floats for sample idx / seed (the boundary generator alternative). */
+void oracle_philox_floats(unsigned long long idx, unsigned int seed, float* out2);
+
+/* Reference median-split BVH (src/distance/bvh.rs:149-238) of one path shape:
+ * writes per node (min.x,min.y,max.x,max.y,left,right,start,count) into nodes
+ * (8 floats each, ints stored as floats) and the leaf index order into indices. */
+int oracle_path_bvh(const dvg_scene_desc* desc, uint32_t shape, float* nodes, int node_cap,
+                    int* indices, int index_cap, int* num_indices);
+
+/* Work units: number of (sample, path segment) pairs whose padded segment bounds
+ * contain the sample in shape space, split by segment kind (line, quad, cubic). */
+int oracle_count_segment_tests(const dvg_scene_desc* desc, const dvg_render_options* opts,
+                               unsigned long long* out3);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

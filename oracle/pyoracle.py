@@ -1,0 +1,173 @@
+"""ctypes binding of the CPU oracle (test infrastructure only).
+
+Imported only by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline /
+reference arm.  It builds oracle/_build/liboracle.so with the committed
+Makefile when the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import sys
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_REPO = os.path.dirname(_HERE)
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+sys.path.insert(0, os.path.join(_REPO, "diffvg-rs_b200"))
+
+from dvg.abi import (  # noqa: E402
+    BackwardOptionsC,
+    GradBuffers,
+    GradsC,
+    RenderOptionsC,
+    SceneDesc,
+    backward_options_c,
+    pack_scene,
+    render_options_c,
+    unflatten_grads,
+)
+from dvg.scene import BackwardOptions, RenderOptions, Scene  # noqa: E402
+
+_lib: Optional[C.CDLL] = None
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        src = os.path.join(_HERE, "oracle.cpp")
+        if not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        D = C.POINTER(SceneDesc)
+        R = C.POINTER(RenderOptionsC)
+        B = C.POINTER(BackwardOptionsC)
+        fp = C.POINTER(C.c_float)
+        L.oracle_render.argtypes = [D, R, fp]
+        L.oracle_sample_premultiplied.argtypes = [D, R, C.c_float, C.c_float, fp]
+        L.oracle_render_backward.argtypes = [D, R, B, fp, C.POINTER(GradsC)]
+        L.oracle_render_backward_ex.argtypes = [D, R, B, fp, C.POINTER(GradsC), C.c_int, C.c_int,
+                                                C.c_ulonglong, C.c_ulonglong]
+        L.oracle_weight_image.argtypes = [D, R, fp]
+        L.oracle_compute_distance.argtypes = [D, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_int, fp]
+        L.oracle_within_distance.argtypes = [D, C.c_uint32, C.c_float, C.c_float, C.c_int]
+        L.oracle_is_inside.argtypes = [D, C.c_uint32, C.c_float, C.c_float, C.c_int]
+        L.oracle_flatten.argtypes = [D, C.c_uint32, C.c_float, fp, C.c_int]
+        L.oracle_pcg32_floats.argtypes = [C.c_ulonglong, C.c_ulonglong, C.c_int, fp]
+        L.oracle_philox_floats.argtypes = [C.c_ulonglong, C.c_uint, fp]
+        L.oracle_path_bvh.argtypes = [D, C.c_uint32, fp, C.c_int, C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int)]
+        L.oracle_count_segment_tests.argtypes = [D, R, C.POINTER(C.c_ulonglong)]
+        _lib = L
+    return _lib
+
+
+def _fp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def render(scene: Scene, options: RenderOptions) -> np.ndarray:
+    ps = pack_scene(scene)
+    out = np.zeros(int(scene.width) * int(scene.height) * 4, np.float32)
+    o = render_options_c(options)
+    lib().oracle_render(ps.ref(), C.byref(o), _fp(out))
+    return out.reshape(int(scene.height), int(scene.width), 4)
+
+
+def sample_premultiplied(scene: Scene, px: float, py: float) -> np.ndarray:
+    ps = pack_scene(scene)
+    out = np.zeros(4, np.float32)
+    o = render_options_c(RenderOptions())
+    lib().oracle_sample_premultiplied(ps.ref(), C.byref(o), px, py, _fp(out))
+    return out
+
+
+def weight_image(scene: Scene, options: RenderOptions) -> np.ndarray:
+    ps = pack_scene(scene)
+    out = np.zeros(int(scene.width) * int(scene.height), np.float32)
+    o = render_options_c(options)
+    lib().oracle_weight_image(ps.ref(), C.byref(o), _fp(out))
+    return out.reshape(int(scene.height), int(scene.width))
+
+
+def render_backward(scene: Scene, options: RenderOptions, bopts: Optional[BackwardOptions] = None,
+                    d_render: Optional[np.ndarray] = None, passes: int = 3, threads: int = 1,
+                    sample_begin: int = 0, sample_end: int = 0):
+    """The crate's CPU render_backward; returns (SceneGrad, GradBuffers)."""
+    bopts = bopts or BackwardOptions()
+    ps = pack_scene(scene)
+    has_bg = d_render is not None and scene.background_image is not None
+    buf = GradBuffers(ps, background_image=has_bg, translation=bopts.compute_translation)
+    o = render_options_c(options)
+    b = backward_options_c(bopts)
+    dr = None
+    if d_render is not None:
+        dr = np.ascontiguousarray(np.asarray(d_render, np.float32).reshape(-1))
+    lib().oracle_render_backward_ex(ps.ref(), C.byref(o), C.byref(b),
+                                    _fp(dr) if dr is not None else C.cast(None, C.POINTER(C.c_float)),
+                                    C.byref(buf.c), passes, threads, sample_begin, sample_end)
+    return unflatten_grads(scene, ps, buf), buf
+
+
+def compute_distance(scene: Scene, group: int, pt, max_radius: float = float("inf"), use_bvh: bool = False):
+    ps = pack_scene(scene)
+    out = np.zeros(4, np.float32)
+    ok = lib().oracle_compute_distance(ps.ref(), group, pt[0], pt[1], max_radius, 1 if use_bvh else 0, _fp(out))
+    if not ok:
+        return None
+    return dict(shape_index=int(out[0]), point=(float(out[1]), float(out[2])), distance=float(out[3]))
+
+
+def within_distance(scene: Scene, group: int, pt, use_bvh: bool = False) -> bool:
+    ps = pack_scene(scene)
+    return bool(lib().oracle_within_distance(ps.ref(), group, pt[0], pt[1], 1 if use_bvh else 0))
+
+
+def is_inside(scene: Scene, group: int, pt, use_bvh: bool = False) -> bool:
+    ps = pack_scene(scene)
+    return bool(lib().oracle_is_inside(ps.ref(), group, pt[0], pt[1], 1 if use_bvh else 0))
+
+
+def flatten(scene: Scene, shape: int, tolerance: float) -> np.ndarray:
+    ps = pack_scene(scene)
+    cap = 1 << 16
+    out = np.zeros(cap * 4, np.float32)
+    n = lib().oracle_flatten(ps.ref(), shape, tolerance, _fp(out), cap)
+    return out[: 4 * min(n, cap)].reshape(-1, 4)
+
+
+def pcg32_floats(idx: int, seed: int, n: int) -> np.ndarray:
+    out = np.zeros(n, np.float32)
+    lib().oracle_pcg32_floats(idx, seed, n, _fp(out))
+    return out
+
+
+def philox_floats(idx: int, seed: int) -> np.ndarray:
+    out = np.zeros(2, np.float32)
+    lib().oracle_philox_floats(idx, seed, _fp(out))
+    return out
+
+
+def path_bvh(scene: Scene, shape: int):
+    ps = pack_scene(scene)
+    nodes = np.zeros(8 * 4096, np.float32)
+    idx = np.zeros(4096, np.int32)
+    ni = C.c_int(0)
+    n = lib().oracle_path_bvh(ps.ref(), shape, _fp(nodes), 4096, idx.ctypes.data_as(C.POINTER(C.c_int)), 4096,
+                              C.byref(ni))
+    return nodes[: 8 * n].reshape(-1, 8), idx[: ni.value]
+
+
+def count_segment_tests(scene: Scene, options: RenderOptions) -> np.ndarray:
+    ps = pack_scene(scene)
+    out = (C.c_ulonglong * 6)()
+    o = render_options_c(options)
+    lib().oracle_count_segment_tests(ps.ref(), C.byref(o), out)
+    return np.array(list(out), np.uint64)
