@@ -70,11 +70,25 @@ struct Blob {
 
 }  // namespace
 
+struct ProfEvent {
+    const char* name;
+    cudaEvent_t a, b;
+};
+struct ProfStat {
+    const char* name;
+    double ms;
+    uint64_t count;
+};
+
 struct dvg_context {
     int device = 0;
+    bool profiling = false;
+    std::vector<ProfEvent> pending;
+    std::vector<ProfStat> stats;
     cudaStream_t stream = nullptr;
     unsigned* status = nullptr;  // device word
     DevBuf accum, wsum, image, d_render, target, loss, bg_grad, trans_grad;
+    DevBuf bsamples, bkey, border, bcounts;  // boundary-pass scratch
     uint64_t launches = 0;
 };
 
@@ -152,9 +166,72 @@ dvg_status check_status(dvg_context* ctx) {
     return DVG_OK;
 }
 
+// Brackets one launcher call with CUDA events on the context stream when profiling is on.
+struct Prof {
+    dvg_context* ctx;
+    ProfEvent ev{};
+    Prof(dvg_context* c, const char* name) : ctx(c) {
+        ev.name = name;
+        if (!ctx->profiling) return;
+        cudaEventCreate(&ev.a);
+        cudaEventCreate(&ev.b);
+        cudaEventRecord(ev.a, ctx->stream);
+    }
+    ~Prof() {
+        if (!ctx->profiling) return;
+        cudaEventRecord(ev.b, ctx->stream);
+        ctx->pending.push_back(ev);
+    }
+};
+void resolve_profile(dvg_context* ctx) {
+    for (auto& e : ctx->pending) {
+        cudaEventSynchronize(e.b);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e.a, e.b);
+        bool found = false;
+        for (auto& st : ctx->stats)
+            if (std::strcmp(st.name, e.name) == 0) {
+                st.ms += ms;
+                st.count += 1;
+                found = true;
+            }
+        if (!found) ctx->stats.push_back(ProfStat{e.name, (double)ms, 1});
+        cudaEventDestroy(e.a);
+        cudaEventDestroy(e.b);
+    }
+    ctx->pending.clear();
+}
+
 }  // namespace
 
 extern "C" {
+
+dvg_status dvg_context_set_profiling(dvg_context* ctx, int enable) {
+    if (!ctx) return fail(DVG_ERR_INVALID_ARGUMENT, "null context");
+    ctx->profiling = enable != 0;
+    return DVG_OK;
+}
+
+int dvg_context_profile(dvg_context* ctx, const char** names, double* total_ms, uint64_t* launches, int cap) {
+    if (!ctx) return 0;
+    cudaSetDevice(ctx->device);
+    resolve_profile(ctx);
+    int n = (int)ctx->stats.size();
+    for (int i = 0; i < n && i < cap; ++i) {
+        if (names) names[i] = ctx->stats[i].name;
+        if (total_ms) total_ms[i] = ctx->stats[i].ms;
+        if (launches) launches[i] = ctx->stats[i].count;
+    }
+    return n;
+}
+
+void dvg_context_profile_reset(dvg_context* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    resolve_profile(ctx);
+    ctx->stats.clear();
+}
+
 
 uint32_t dvg_abi_version(void) { return DVG_ABI_VERSION; }
 
@@ -307,7 +384,10 @@ static dvg_status render_into(dvg_context* ctx, dvg_scene* sc, const dvg_render_
     const size_t npix = (size_t)S.width * S.height;
     if (npix == 0) return DVG_OK;
     if (S.num_groups == 0) {  // Image::solid / background image (src/renderer/renderer.rs:57-66)
-        ctx->launches += launch_fill_background(S, out_dev, ctx->stream);
+        {
+            Prof prof_(ctx, "fill_background");
+            ctx->launches += launch_fill_background(S, out_dev, ctx->stream);
+        }
         CK(cudaGetLastError());
         return DVG_OK;
     }
@@ -316,9 +396,15 @@ static dvg_status render_into(dvg_context* ctx, dvg_scene* sc, const dvg_render_
     CK(ctx->wsum.reserve(npix * sizeof(float)));
     CK(cudaMemsetAsync(ctx->accum.ptr, 0, npix * 4 * sizeof(float), ctx->stream));
     CK(cudaMemsetAsync(ctx->wsum.ptr, 0, npix * sizeof(float), ctx->stream));
-    ctx->launches += launch_forward(S, sp, ctx->accum.as<float>(), ctx->wsum.as<float>(), ctx->status, ctx->stream);
+    {
+        Prof prof_(ctx, "forward");
+        ctx->launches += launch_forward(S, sp, ctx->accum.as<float>(), ctx->wsum.as<float>(), ctx->status, ctx->stream);
+    }
     CK(cudaGetLastError());
-    ctx->launches += launch_resolve(S, ctx->accum.as<float>(), ctx->wsum.as<float>(), out_dev, ctx->stream);
+    {
+        Prof prof_(ctx, "resolve");
+        ctx->launches += launch_resolve(S, ctx->accum.as<float>(), ctx->wsum.as<float>(), out_dev, ctx->stream);
+    }
     CK(cudaGetLastError());
     return DVG_OK;
 }
@@ -364,19 +450,33 @@ static dvg_status backward_core(dvg_context* ctx, dvg_scene* sc, const dvg_rende
         if (!have_weights) {
             CK(ctx->wsum.reserve(npix * sizeof(float)));
             CK(cudaMemsetAsync(ctx->wsum.ptr, 0, npix * sizeof(float), ctx->stream));
+            Prof prof_(ctx, "weights");
             ctx->launches += launch_weights(S, sp, ctx->wsum.as<float>(), ctx->stream);
             CK(cudaGetLastError());
         }
-        ctx->launches += launch_interior(S, sp, d_render, ctx->wsum.as<float>(), G, ctx->status, ctx->stream);
+        {
+            Prof prof_(ctx, "interior");
+            ctx->launches += launch_interior(S, sp, d_render, ctx->wsum.as<float>(), G, ctx->status, ctx->stream);
+        }
         CK(cudaGetLastError());
         if (S.boundary_ok) {
             BoundaryParams bp;
             uint64_t total = (uint64_t)npix * sp.sxn * sp.syn;
             bp.num_samples = bopts && bopts->boundary_samples ? bopts->boundary_samples : total;
             bp.sample_base = 0;
+            bp.slot_base = 0;
             bp.seed = (bopts && !bopts->boundary_seed_from_options) ? bopts->boundary_seed : opts->seed;
             bp.rng = bopts ? (int)bopts->rng : 0;
-            ctx->launches += launch_boundary(S, bp, d_render, ctx->wsum.as<float>(), G, ctx->stream);
+            const uint64_t cap = std::min<uint64_t>(bp.num_samples, (uint64_t)1 << 24);
+            const int tiles = S.tiles_x * S.tiles_y;
+            CK(ctx->bsamples.reserve(cap * sizeof(BSample)));
+            CK(ctx->bkey.reserve(cap * sizeof(int)));
+            CK(ctx->border.reserve(cap * sizeof(int)));
+            CK(ctx->bcounts.reserve((2 * (size_t)tiles + 1) * sizeof(int)));
+            Prof prof_(ctx, "boundary");
+            ctx->launches += launch_boundary(S, bp, d_render, ctx->wsum.as<float>(), G, ctx->bsamples.as<BSample>(),
+                                             ctx->bkey.as<int>(), ctx->bcounts.as<int>(), ctx->border.as<int>(), cap,
+                                             ctx->stream);
             CK(cudaGetLastError());
         }
     } else if (d_render && S.num_groups == 0) {
@@ -384,12 +484,19 @@ static dvg_status backward_core(dvg_context* ctx, dvg_scene* sc, const dvg_rende
         if (!have_weights) {
             CK(ctx->wsum.reserve(npix * sizeof(float)));
             CK(cudaMemsetAsync(ctx->wsum.ptr, 0, npix * sizeof(float), ctx->stream));
+            Prof prof_(ctx, "weights");
             ctx->launches += launch_weights(S, sp, ctx->wsum.as<float>(), ctx->stream);
         }
-        ctx->launches += launch_interior(S, sp, d_render, ctx->wsum.as<float>(), G, ctx->status, ctx->stream);
+        {
+            Prof prof_(ctx, "interior");
+            ctx->launches += launch_interior(S, sp, d_render, ctx->wsum.as<float>(), G, ctx->status, ctx->stream);
+        }
         CK(cudaGetLastError());
     }
-    ctx->launches += launch_finalize_background(S, G, ctx->stream);
+    {
+        Prof prof_(ctx, "finalize_background");
+        ctx->launches += launch_finalize_background(S, G, ctx->stream);
+    }
     CK(cudaGetLastError());
     return DVG_OK;
 }
@@ -576,7 +683,10 @@ dvg_status dvg_fwd_bwd_l2_device(dvg_context* ctx, dvg_scene* scene, const dvg_r
     if (st != DVG_OK) return st;
     CK(ctx->d_render.reserve(npix * 4 * sizeof(float)));
     if (loss_out) CK(cudaMemsetAsync(loss_out, 0, sizeof(float), ctx->stream));
-    ctx->launches += launch_l2(img, target_rgba, npix * 4, ctx->d_render.as<float>(), loss_out, ctx->stream);
+    {
+        Prof prof_(ctx, "l2_loss");
+        ctx->launches += launch_l2(img, target_rgba, npix * 4, ctx->d_render.as<float>(), loss_out, ctx->stream);
+    }
     CK(cudaGetLastError());
     GradPtrs G = grads_from_user(grads);
     if (!(bopts && bopts->compute_translation)) G.d_translation = nullptr;

@@ -548,7 +548,8 @@ __global__ void __launch_bounds__(256) k_interior(DevScene S, SampleParams sp, c
 // sample_color with an EdgeQuery (sampling.rs:76-224, 485-552) at canvas point pt.
 // Returns the un-premultiplied colour (or the premultiplied background when no
 // fragment covers pt) and whether the queried shape is the visible boundary.
-__device__ float4 edge_color(const DevScene& S, float2 pt, float4 bg, int eq_group, int eq_shape, bool* hit_out) {
+__device__ float4 edge_color(const DevScene& S, int tile, float2 pt, float4 bg, int eq_group, int eq_shape,
+                             bool* hit_out) {
     // Edge tests on the queried shape alone (within_distance_edge / is_inside_edge).
     bool hit0 = false;
     {
@@ -563,7 +564,6 @@ __device__ float4 edge_color(const DevScene& S, float2 pt, float4 bg, int eq_gro
             if (fill_hit(gi.z, winding_shape(S, eq_shape, sp, true))) hit0 = true;
         }
     }
-    const int tile = tile_of(S, pt);
     const int off = S.tile_offsets[tile];
     const int n = S.tile_offsets[tile + 1] - off;
     const int* list = S.tile_entries + off;
@@ -980,10 +980,14 @@ __device__ void accumulate_boundary(const DevScene& S, const GradPtrs& G, int sh
         }
 }
 
-__global__ void __launch_bounds__(128) k_boundary(DevScene S, BoundaryParams bp, const float* d_render,
-                                                  const float* wsum, GradPtrs G) {
+// Boundary pass, stage 1: draw every edge sample (boundary.rs:141-175), keep
+// the valid ones with the tile of their boundary pixel as sort key.
+__global__ void __launch_bounds__(256) k_boundary_gen(DevScene S, BoundaryParams bp, BSample* out, int* key,
+                                                      int* tile_counts) {
     const uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + bp.sample_base;
     if (idx >= bp.num_samples) return;
+    const uint64_t slot = idx - bp.slot_base;
+    key[slot] = -1;
     float u, t;
     if (bp.rng == 1) {
         uint4 r = philox4x32_10(make_uint4((uint32_t)idx, (uint32_t)(idx >> 32), 0u, 0u), make_uint2(bp.seed, 0u));
@@ -1004,7 +1008,6 @@ __global__ void __launch_bounds__(128) k_boundary(DevScene S, BoundaryParams bp,
     BData bd;
     if (!sample_boundary_point(S, shape, group, t, S.shape_len[shape], &local_pt, &normal, &bpdf, &bd)) return;
     if (bpdf <= 0.0f) return;
-    // canvas point, canvas normal (boundary.rs:167-175)
     float s2c[9];
     mul33(S.g_s2c + 9 * group, S.s_xform + 9 * shape, s2c);
     float2 bpt = xf9(s2c, local_pt);
@@ -1023,13 +1026,53 @@ __global__ void __launch_bounds__(128) k_boundary(DevScene S, BoundaryParams bp,
     if (pdf <= 0.0f) return;
     const int bx = f2i(bpt.x * W), by = f2i(bpt.y * H);
     if (bx < 0 || bx >= S.width || by < 0 || by >= S.height) return;
-    const int pixel = by * S.width + bx;
-    const float4 bg = background_premul(S, pixel);
+    BSample r;
+    r.bx = bpt.x;
+    r.by = bpt.y;
+    r.nx = nc.x;
+    r.ny = nc.y;
+    r.lx = local_pt.x;
+    r.ly = local_pt.y;
+    r.pdf = pdf;
+    r.t = t;
+    r.shape = shape;
+    r.group = group;
+    r.pixel = by * S.width + bx;
+    r.base_point_id = bd.base_point_id;
+    r.point_id = bd.point_id;
+    r.bt = bd.t;
+    r.is_stroke = bd.is_stroke ? 1 : 0;
+    r.pad = 0;
+    out[slot] = r;
+    const int tile = (by / TILE) * S.tiles_x + (bx / TILE);
+    key[slot] = tile;
+    atomicAdd(tile_counts + tile, 1);
+}
+// Stage 2: counting-sort scatter of sample slots by tile.
+__global__ void k_boundary_scatter(const int* key, uint64_t n, int* cursor, int* order) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int k = key[i];
+    if (k < 0) return;
+    order[atomicAdd(cursor + k, 1)] = (int)i;
+}
+// Stage 3: evaluate both sides of every edge sample in tile order, so that the
+// lanes of a warp share one group list (render_edge_sample, boundary.rs:845-967).
+__global__ void __launch_bounds__(128) k_boundary_eval(DevScene S, const BSample* samples, const int* order,
+                                                       const int* offsets, int tiles, const float* d_render,
+                                                       const float* wsum, GradPtrs G) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= offsets[tiles]) return;
+    const BSample r = samples[order[i]];
+    const float W = (float)S.width, H = (float)S.height;
+    const float4 bg = background_premul(S, r.pixel);
+    const int tile = ((r.pixel / S.width) / TILE) * S.tiles_x + ((r.pixel % S.width) / TILE);
+    float2 nc = make_float2(r.nx, r.ny);
     bool hi, ho;
-    float2 pin = make_float2(bpt.x - nc.x * 1.0e-4f, bpt.y - nc.y * 1.0e-4f);
-    float2 pout = make_float2(bpt.x + nc.x * 1.0e-4f, bpt.y + nc.y * 1.0e-4f);
-    float4 ci = edge_color(S, make_float2(pin.x * W, pin.y * H), bg, group, shape, &hi);
-    float4 co = edge_color(S, make_float2(pout.x * W, pout.y * H), bg, group, shape, &ho);
+    const float2 pin = make_float2(r.bx - nc.x * 1.0e-4f, r.by - nc.y * 1.0e-4f);
+    const float2 pout = make_float2(r.bx + nc.x * 1.0e-4f, r.by + nc.y * 1.0e-4f);
+    float4 ci = edge_color(S, tile, make_float2(pin.x * W, pin.y * H), bg, r.group, r.shape, &hi);
+    float4 co = edge_color(S, tile, make_float2(pout.x * W, pout.y * H), bg, r.group, r.shape, &ho);
     if (!hi && !ho) return;
     if (!hi) {
         nc = make_float2(nc.x * -1.0f, nc.y * -1.0f);
@@ -1038,7 +1081,7 @@ __global__ void __launch_bounds__(128) k_boundary(DevScene S, BoundaryParams bp,
         co = tmp;
     }
     // gather_d_color at the boundary pixel, divided by W*H (boundary.rs:913-929)
-    const float2 sb = make_float2(bpt.x * W, bpt.y * H);
+    const float2 sb = make_float2(r.bx * W, r.by * H);
     float4 dc = make_float4(0, 0, 0, 0);
     {
         const int px = f2i(floorf(sb.x)), py = f2i(floorf(sb.y)), ri = S.filter_ri;
@@ -1068,12 +1111,17 @@ __global__ void __launch_bounds__(128) k_boundary(DevScene S, BoundaryParams bp,
         dc.w /= norm;
     }
     const float contrib =
-        ((ci.x - co.x) * dc.x + (ci.y - co.y) * dc.y + (ci.z - co.z) * dc.z + (ci.w - co.w) * dc.w) / pdf;
+        ((ci.x - co.x) * dc.x + (ci.y - co.y) * dc.y + (ci.z - co.z) * dc.z + (ci.w - co.w) * dc.w) / r.pdf;
     if (!isfinite(contrib)) return;
-    accumulate_boundary(S, G, shape, group, contrib, t, nc, bd, local_pt);
+    BData bd;
+    bd.base_point_id = r.base_point_id;
+    bd.point_id = r.point_id;
+    bd.t = r.bt;
+    bd.is_stroke = r.is_stroke != 0;
+    accumulate_boundary(S, G, r.shape, r.group, contrib, r.t, nc, bd, make_float2(r.lx, r.ly));
     if (G.d_translation) {
-        add_if(G.d_translation + 2 * (size_t)pixel, nc.x * contrib);
-        add_if(G.d_translation + 2 * (size_t)pixel + 1, nc.y * contrib);
+        add_if(G.d_translation + 2 * (size_t)r.pixel, nc.x * contrib);
+        add_if(G.d_translation + 2 * (size_t)r.pixel + 1, nc.y * contrib);
     }
 }
 
@@ -1173,18 +1221,27 @@ int launch_interior(const DevScene& S, const SampleParams& sp, const float* d_re
     return 1;
 }
 int launch_boundary(const DevScene& S, const BoundaryParams& bp, const float* d_render, const float* wsum,
-                    const GradPtrs& G, cudaStream_t stream) {
-    uint64_t n = bp.num_samples;
-    if (n == 0) return 0;
+                    const GradPtrs& G, BSample* samples, int* key, int* counts, int* order, uint64_t capacity,
+                    cudaStream_t stream) {
+    const uint64_t n = bp.num_samples;
+    const int tiles = S.tiles_x * S.tiles_y;
     int launches = 0;
-    const uint64_t chunk = (uint64_t)1 << 30;  // keep the grid's x extent well inside 2^31
-    for (uint64_t base = 0; base < n; base += chunk) {
+    for (uint64_t base = 0; base < n; base += capacity) {
+        const uint64_t cnt = base + capacity < n ? capacity : n - base;
         BoundaryParams b = bp;
         b.sample_base = base;
-        b.num_samples = base + chunk < n ? base + chunk : n;
-        uint64_t cnt = b.num_samples - base;
-        k_boundary<<<(unsigned)((cnt + 127) / 128), 128, 0, stream>>>(S, b, d_render, wsum, G);
-        ++launches;
+        b.slot_base = base;
+        b.num_samples = base + cnt;
+        cudaMemsetAsync(counts, 0, sizeof(int) * (2 * (size_t)tiles + 1), stream);
+        k_boundary_gen<<<(unsigned)((cnt + 255) / 256), 256, 0, stream>>>(S, b, samples, key, counts);
+        int* offsets = counts + tiles;  // tiles + 1 entries
+        k_bin_scan<<<1, 1024, 0, stream>>>(counts, tiles, offsets);
+        // reuse the count array as the scatter cursor (a copy of the exclusive offsets)
+        cudaMemcpyAsync(counts, offsets, sizeof(int) * (size_t)tiles, cudaMemcpyDeviceToDevice, stream);
+        k_boundary_scatter<<<(unsigned)((cnt + 255) / 256), 256, 0, stream>>>(key, cnt, counts, order);
+        k_boundary_eval<<<(unsigned)((cnt + 127) / 128), 128, 0, stream>>>(S, samples, order, offsets, tiles,
+                                                                            d_render, wsum, G);
+        launches += 4;
     }
     return launches;
 }

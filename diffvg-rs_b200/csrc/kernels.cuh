@@ -21,10 +21,22 @@ struct SampleParams {
     bool jitter;
 };
 struct BoundaryParams {
-    uint64_t num_samples;
-    uint64_t sample_base;
+    uint64_t num_samples;  // one past the last sample index of this launch
+    uint64_t sample_base;  // first sample index of this launch
+    uint64_t slot_base;    // sample index stored in scratch slot 0
     uint32_t seed;
     int rng;  // 0 PCG32, 1 Philox
+};
+// One drawn edge sample (64 bytes), kept in scratch between the boundary stages.
+struct BSample {
+    float bx, by;  // boundary point, normalised canvas units
+    float nx, ny;  // canvas-space normal
+    float lx, ly;  // shape-space boundary point
+    float pdf, t;  // combined pdf, raw random t
+    int shape, group, pixel;
+    int base_point_id, point_id;
+    float bt;
+    int is_stroke, pad;
 };
 struct GradPtrs {
     float* d_shape_params;
@@ -51,8 +63,11 @@ int launch_weights(const DevScene& S, const SampleParams& sp, float* wsum, cudaS
 int launch_resolve(const DevScene& S, const float* accum, const float* wsum, float* out, cudaStream_t stream);
 int launch_interior(const DevScene& S, const SampleParams& sp, const float* d_render, const float* wsum,
                     const GradPtrs& G, unsigned* status, cudaStream_t stream);
+// Boundary pass in chunks of at most `capacity` samples; scratch: samples[capacity],
+// key[capacity], order[capacity], counts[2*tiles+1].
 int launch_boundary(const DevScene& S, const BoundaryParams& bp, const float* d_render, const float* wsum,
-                    const GradPtrs& G, cudaStream_t stream);
+                    const GradPtrs& G, BSample* samples, int* key, int* counts, int* order, uint64_t capacity,
+                    cudaStream_t stream);
 int launch_finalize_background(const DevScene& S, const GradPtrs& G, cudaStream_t stream);
 int launch_fill_background(const DevScene& S, float* out, cudaStream_t stream);
 int launch_l2(const float* img, const float* target, size_t n, float* d_render, float* loss, cudaStream_t stream);

@@ -40,7 +40,8 @@ EXPORTED = (
     "dvg_abi_version", "dvg_last_error", "dvg_context_create", "dvg_context_destroy", "dvg_scene_upload",
     "dvg_scene_destroy", "dvg_render_host", "dvg_render_device", "dvg_render_backward_host",
     "dvg_render_backward_device", "dvg_render", "dvg_render_backward", "dvg_fwd_bwd_l2_device",
-    "dvg_context_launch_count", "dvg_context_stream",
+    "dvg_context_launch_count", "dvg_context_stream", "dvg_context_set_profiling", "dvg_context_profile",
+    "dvg_context_profile_reset",
 )
 
 
@@ -93,6 +94,13 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.dvg_context_launch_count.restype = C.c_uint64
     L.dvg_context_stream.argtypes = [vp]
     L.dvg_context_stream.restype = vp
+    L.dvg_context_set_profiling.argtypes = [vp, C.c_int]
+    L.dvg_context_set_profiling.restype = C.c_int
+    L.dvg_context_profile.argtypes = [vp, C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.POINTER(C.c_uint64),
+                                      C.c_int]
+    L.dvg_context_profile.restype = C.c_int
+    L.dvg_context_profile_reset.argtypes = [vp]
+    L.dvg_context_profile_reset.restype = None
     for name in ("dvg_context_create", "dvg_scene_upload", "dvg_render_host", "dvg_render_device",
                  "dvg_render_backward_host", "dvg_render_backward_device", "dvg_render", "dvg_render_backward",
                  "dvg_fwd_bwd_l2_device"):
@@ -229,6 +237,21 @@ class Renderer:
     @property
     def stream_handle(self) -> int:
         return int(self.lib.dvg_context_stream(self.ctx) or 0)
+
+    def set_profiling(self, enable: bool) -> None:
+        _check(self.lib.dvg_context_set_profiling(self.ctx, 1 if enable else 0))
+
+    def profile(self, reset: bool = True) -> dict:
+        """{launcher name: (total ms, calls)} from the context's CUDA-event timing."""
+        cap = 64
+        names = (C.c_char_p * cap)()
+        ms = (C.c_double * cap)()
+        calls = (C.c_uint64 * cap)()
+        n = self.lib.dvg_context_profile(self.ctx, names, ms, calls, cap)
+        out = {names[i].decode(): (float(ms[i]), int(calls[i])) for i in range(min(n, cap))}
+        if reset:
+            self.lib.dvg_context_profile_reset(self.ctx)
+        return out
 
     def upload(self, scene: Scene) -> UploadedScene:
         return UploadedScene(self, scene)

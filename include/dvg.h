@@ -231,6 +231,15 @@ uint64_t dvg_context_launch_count(const dvg_context* ctx);
 /* The context's CUDA stream (a cudaStream_t) for callers that interleave their own work. */
 void* dvg_context_stream(dvg_context* ctx);
 
+/* Kernel timing (no counterpart in the crate, which has no tracing): when enabled,
+ * every launcher call of this library on the context is bracketed by CUDA events on
+ * the context stream.  dvg_context_profile synchronises, then fills up to cap entries
+ * of (launcher name, total milliseconds, calls) accumulated since the last reset and
+ * returns the number of distinct launchers.  Names are static strings. */
+dvg_status dvg_context_set_profiling(dvg_context* ctx, int enable);
+int dvg_context_profile(dvg_context* ctx, const char** names, double* total_ms, uint64_t* calls, int cap);
+void dvg_context_profile_reset(dvg_context* ctx);
+
 #ifdef __cplusplus
 }
 #endif

@@ -14,6 +14,7 @@
 #include "oracle.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -3077,4 +3078,82 @@ extern "C" int oracle_count_segment_tests(const dvg_scene_desc* desc, const dvg_
         }
     }
     return 0;
+}
+
+// Bounded-sample forward + backward for CPU timing: `count` samples spread evenly
+// over the W*H*spp sample sequence (idx = k*stride), each doing the forward
+// per-sample evaluation (premultiplied colour and filtered splat) and the interior
+// adjoint, plus count*nb/total boundary samples spread the same way over the
+// nb-sample boundary pass.  Runs on `threads` host threads with per-thread gradient
+// buffers, as a parallel port of the crate's serial loops
+// (src/backward/render.rs:95-205).  Writes the per-call set-up time (BVH, weight
+// image, CDF tables) and the sample-loop time in seconds to times[0..1].
+extern "C" unsigned long long oracle_fwd_bwd_sample(const dvg_scene_desc* desc, const dvg_render_options* opts,
+                                                    const dvg_backward_options* bopts, const float* d_render,
+                                                    unsigned long long count, int threads, double* times) {
+    auto now = []() { return std::chrono::steady_clock::now(); };
+    auto t0 = now();
+    Scene sc = decode(desc);
+    if (sc.w == 0 || sc.h == 0 || sc.groups.empty()) return 0;
+    SampleSpec sp = make_spec(opts);
+    uint64_t total = (uint64_t)sc.w * sc.h * sp.sx_n * sp.sy_n;
+    if (count > total) count = total;
+    if (count == 0) return 0;
+    uint64_t stride = total / count;
+    SceneBvh bvh = build_scene_bvh(sc);
+    std::vector<float> wimg = build_weight_image(sc, sp);
+    BoundaryTables bt = build_boundary_tables(sc);
+    int nthreads = threads > 1 ? threads : 1;
+    std::vector<Grads> tg(nthreads);
+    std::vector<std::vector<float>> acc(nthreads);
+    for (int t = 0; t < nthreads; ++t) {
+        tg[t].init(sc, desc, false, false);
+        acc[t].assign((size_t)sc.w * sc.h * 4, 0.0f);
+    }
+    auto t1 = now();
+    int ri = std::max(0, to_i32(std::ceil(sc.filter_radius)));
+    int width = (int)sc.w, height = (int)sc.h;
+    parallel_for(0, count, nthreads, [&](int t, uint64_t lo, uint64_t hi) {
+        for (uint64_t k = lo; k < hi; ++k) {
+            uint64_t idx = k * stride;
+            V2 pt;
+            size_t pix;
+            sample_position(sc, sp, idx, &pt, &pix);
+            V4 c = eval_premultiplied(sc, bvh, pt, sample_background(sc, pix));
+            int x = (int)(pix % sc.w), y = (int)(pix / sc.w);
+            for (int dy = -ri; dy <= ri; ++dy)
+                for (int dx = -ri; dx <= ri; ++dx) {
+                    int xx = x + dx, yy = y + dy;
+                    if (xx < 0 || yy < 0 || xx >= width || yy >= height) continue;
+                    size_t b = (size_t)yy * width + xx;
+                    float w = compute_filter_weight(sc.filter_type, sc.filter_radius, (float)xx + 0.5f - pt.x,
+                                                    (float)yy + 0.5f - pt.y);
+                    if (w > 0.0f && wimg[b] > 0.0f) {
+                        float wn = w / wimg[b];
+                        acc[t][4 * b] += c.x * wn;
+                        acc[t][4 * b + 1] += c.y * wn;
+                        acc[t][4 * b + 2] += c.z * wn;
+                        acc[t][4 * b + 3] += c.w * wn;
+                    }
+                }
+            interior_sample(sc, bvh, sp, idx, d_render, wimg, tg[t], false);
+        }
+    });
+    if (bt.ok && !sp.prefilter) {
+        uint64_t nb = bopts && bopts->boundary_samples ? bopts->boundary_samples : total;
+        uint64_t bcount = count * nb / total;
+        uint64_t bstride = bcount ? nb / bcount : 1;
+        uint32_t rng = bopts ? bopts->rng : 0;
+        uint32_t seed = (bopts && !bopts->boundary_seed_from_options) ? bopts->boundary_seed : opts->seed;
+        parallel_for(0, bcount, nthreads, [&](int t, uint64_t lo, uint64_t hi) {
+            for (uint64_t k = lo; k < hi; ++k)
+                boundary_sample(sc, bvh, bt, k * bstride, rng, seed, d_render, wimg, tg[t], false);
+        });
+    }
+    auto t2 = now();
+    if (times) {
+        times[0] = std::chrono::duration<double>(t1 - t0).count();
+        times[1] = std::chrono::duration<double>(t2 - t1).count();
+    }
+    return count;
 }

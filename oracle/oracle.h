@@ -73,6 +73,13 @@ int oracle_path_bvh(const dvg_scene_desc* desc, uint32_t shape, float* nodes, in
 
 /* Work units: number of (sample, path segment) pairs whose padded segment bounds
  * contain the sample in shape space, split by segment kind (line, quad, cubic). */
+/* Bounded-sample CPU forward + backward (timing workload): `count` samples spread
+ * evenly over the sample sequence plus the proportional share of boundary samples,
+ * on `threads` threads; times[0] = set-up seconds, times[1] = sample-loop seconds. */
+unsigned long long oracle_fwd_bwd_sample(const dvg_scene_desc* desc, const dvg_render_options* opts,
+                                         const dvg_backward_options* bopts, const float* d_render,
+                                         unsigned long long count, int threads, double* times);
+
 int oracle_count_segment_tests(const dvg_scene_desc* desc, const dvg_render_options* opts,
                                unsigned long long* out3);
 

@@ -65,6 +65,8 @@ def lib() -> C.CDLL:
         L.oracle_philox_floats.argtypes = [C.c_ulonglong, C.c_uint, fp]
         L.oracle_path_bvh.argtypes = [D, C.c_uint32, fp, C.c_int, C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int)]
         L.oracle_count_segment_tests.argtypes = [D, R, C.POINTER(C.c_ulonglong)]
+        L.oracle_fwd_bwd_sample.argtypes = [D, R, B, fp, C.c_ulonglong, C.c_int, C.POINTER(C.c_double)]
+        L.oracle_fwd_bwd_sample.restype = C.c_ulonglong
         _lib = L
     return _lib
 
@@ -171,3 +173,17 @@ def count_segment_tests(scene: Scene, options: RenderOptions) -> np.ndarray:
     o = render_options_c(options)
     lib().oracle_count_segment_tests(ps.ref(), C.byref(o), out)
     return np.array(list(out), np.uint64)
+
+
+def fwd_bwd_sample(scene: Scene, options: RenderOptions, bopts: Optional[BackwardOptions], d_render: np.ndarray,
+                   count: int, threads: int):
+    """Bounded-sample CPU forward + backward (the CPU baseline workload).
+
+    Returns (samples done, set-up seconds, sample-loop seconds)."""
+    ps = pack_scene(scene)
+    o = render_options_c(options)
+    b = backward_options_c(bopts or BackwardOptions())
+    dr = np.ascontiguousarray(np.asarray(d_render, np.float32).reshape(-1))
+    t = (C.c_double * 2)()
+    n = int(lib().oracle_fwd_bwd_sample(ps.ref(), C.byref(o), C.byref(b), _fp(dr), count, threads, t))
+    return n, float(t[0]), float(t[1])
