@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -697,3 +698,77 @@ dvg_status dvg_fwd_bwd_l2_device(dvg_context* ctx, dvg_scene* scene, const dvg_r
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Render without any device allocation.
+//
+// For callers that cannot call cudaMalloc while they render: a host application
+// that hands this library a fixed device-memory budget up front, a plugin that
+// runs inside another framework's frame loop where allocation is not allowed,
+// or code that must not hit the allocator's implicit synchronisation.  The
+// filtered-splat accumulators (4 colour floats + 1 weight float per pixel)
+// live in one file-scope device array instead of the context's grow-only
+// scratch, so a call only launches kernels and clears that array.
+//
+// Limits and sharing:
+//   * at most kNoAllocMaxPixels (512*512) pixels per canvas; larger canvases are
+//     rejected with DVG_ERR_INVALID_ARGUMENT before anything is launched;
+//   * every GPU that loads this library holds the array (5 MiB) until exit;
+//   * all calls on a device share the one array and it keeps the last call's
+//     contents: each call clears it first, and calls whose work overlaps on the
+//     GPU (different streams or contexts at the same time) race on it.
+// The array's device address is looked up once per device, by the first call
+// on that device (with the device current); make that first call before any
+// stream capture begins.
+namespace {
+constexpr size_t kNoAllocMaxPixels = 512 * 512;
+constexpr int kNoAllocMaxDevices = 64;
+static __device__ __align__(256) float g_noalloc_scratch[kNoAllocMaxPixels * 5];
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
+
+dvg_status noalloc_scratch(int device, float** out) {
+    if (device < 0 || device >= kNoAllocMaxDevices)
+        return fail(DVG_ERR_INVALID_ARGUMENT, "device ordinal beyond the no-allocation table");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        g_noalloc_ptr[device] = p;
+    }
+    *out = static_cast<float*>(g_noalloc_ptr[device]);
+    return DVG_OK;
+}
+}  // namespace
+
+extern "C" dvg_status dvg_render_device_noalloc(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
+                                                float* out_rgba) {
+    if (!ctx || !scene || !out_rgba) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    dvg_status st = check_options(opts);
+    if (st != DVG_OK) return st;
+    CK(cudaSetDevice(ctx->device));
+    const DevScene& S = scene->dev;
+    const size_t npix = (size_t)S.width * S.height;
+    if (npix == 0) return DVG_OK;
+    if (npix > kNoAllocMaxPixels)
+        return fail(DVG_ERR_INVALID_ARGUMENT,
+                    "canvas of " + std::to_string(npix) + " pixels exceeds the no-allocation limit of " +
+                        std::to_string(kNoAllocMaxPixels) + " pixels (512x512); use dvg_render_device");
+    float* scratch = nullptr;
+    st = noalloc_scratch(ctx->device, &scratch);
+    if (st != DVG_OK) return st;
+    if (S.num_groups == 0) {
+        ctx->launches += launch_fill_background(S, out_rgba, ctx->stream);
+        CK(cudaGetLastError());
+        return DVG_OK;
+    }
+    float* accum = scratch;            // 4 floats per pixel (float4 aligned: 256-byte base)
+    float* wsum = scratch + 4 * npix;  // 1 float per pixel
+    CK(cudaMemsetAsync(scratch, 0, 5 * npix * sizeof(float), ctx->stream));
+    const SampleParams sp = sample_params(opts);
+    ctx->launches += launch_forward(S, sp, accum, wsum, ctx->status, ctx->stream);
+    ctx->launches += launch_resolve(S, accum, wsum, out_rgba, ctx->stream);
+    CK(cudaGetLastError());
+    return DVG_OK;
+}

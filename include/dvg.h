@@ -209,6 +209,20 @@ dvg_status dvg_render_backward_device(dvg_context* ctx, dvg_scene* scene,
                                       const dvg_backward_options* bopts,
                                       const float* d_render, const float* d_sdf, dvg_grads* grads);
 
+/* Render of an uploaded scene that allocates no device memory.  No counterpart in
+ * the crate: it exists for callers that cannot call cudaMalloc while rendering (a
+ * host application that fixes the device-memory budget up front, a plugin running
+ * inside another framework's frame loop, code that must avoid the allocator's
+ * implicit synchronisation).  Same inputs, output and result as dvg_render_device,
+ * but the splat accumulators live in one file-scope device array of 5 MiB held by
+ * every GPU that loads the library, so the canvas may have at most 512*512 pixels;
+ * larger canvases return DVG_ERR_INVALID_ARGUMENT and launch nothing.  All calls on
+ * a device share that array (each call clears it first); calls that overlap on the
+ * GPU race on it.  The first call on a device looks up the array's address (with
+ * the device current); make that first call before any stream capture begins. */
+dvg_status dvg_render_device_noalloc(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
+                                     float* out_rgba);
+
 /* One-shot forms mirroring the crate's call shape exactly: scene description in,
  * host image / host gradients out (upload, launch, read back, release). */
 dvg_status dvg_render(dvg_context* ctx, const dvg_scene_desc* desc, const dvg_render_options* opts,
