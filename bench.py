@@ -249,7 +249,7 @@ def main():
 
     # end to end through the host API (scene description in, host image / host gradients out)
     e2e = None
-    if rank == 0 or world > 1:
+    if args.e2e_steps > 0:
         tgt_host = target.view(H, W, 4).cpu().numpy()
         ts = []
         img_h = None

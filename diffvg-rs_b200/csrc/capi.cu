@@ -142,9 +142,6 @@ GradPtrs device_grads(dvg_scene* sc) {
 
 dvg_status check_options(const dvg_render_options* o) {
     if (!o) return fail(DVG_ERR_INVALID_ARGUMENT, "null render options");
-    if (o->use_prefiltering)
-        return fail(DVG_ERR_INVALID_ARGUMENT,
-                    "use_prefiltering=1 is not implemented by this library yet; pass use_prefiltering=0");
     return DVG_OK;
 }
 SampleParams sample_params(const dvg_render_options* o) {
@@ -163,6 +160,10 @@ dvg_status check_status(dvg_context* ctx) {
         CK(cudaMemsetAsync(ctx->status, 0, sizeof(unsigned), ctx->stream));
         return fail(DVG_ERR_DEVICE_LIMIT, "a sample covered more fragments than the per-thread capacity (" +
                                               std::to_string(MAX_FRAGMENTS) + ")");
+    }
+    if (st & ST_BVH_LIMIT) {
+        CK(cudaMemsetAsync(ctx->status, 0, sizeof(unsigned), ctx->stream));
+        return fail(DVG_ERR_DEVICE_LIMIT, "a BVH traversal exceeded its stack depth");
     }
     return DVG_OK;
 }
@@ -398,8 +399,13 @@ static dvg_status render_into(dvg_context* ctx, dvg_scene* sc, const dvg_render_
     CK(cudaMemsetAsync(ctx->accum.ptr, 0, npix * 4 * sizeof(float), ctx->stream));
     CK(cudaMemsetAsync(ctx->wsum.ptr, 0, npix * sizeof(float), ctx->stream));
     {
-        Prof prof_(ctx, "forward");
-        ctx->launches += launch_forward(S, sp, ctx->accum.as<float>(), ctx->wsum.as<float>(), ctx->status, ctx->stream);
+        Prof prof_(ctx, opts->use_prefiltering ? "forward_prefilter" : "forward");
+        if (opts->use_prefiltering)
+            ctx->launches += launch_forward_prefilter(S, sp, ctx->accum.as<float>(), ctx->wsum.as<float>(), ctx->status,
+                                                      ctx->stream);
+        else
+            ctx->launches += launch_forward(S, sp, ctx->accum.as<float>(), ctx->wsum.as<float>(), ctx->status,
+                                            ctx->stream);
     }
     CK(cudaGetLastError());
     {
@@ -456,11 +462,15 @@ static dvg_status backward_core(dvg_context* ctx, dvg_scene* sc, const dvg_rende
             CK(cudaGetLastError());
         }
         {
-            Prof prof_(ctx, "interior");
-            ctx->launches += launch_interior(S, sp, d_render, ctx->wsum.as<float>(), G, ctx->status, ctx->stream);
+            Prof prof_(ctx, opts->use_prefiltering ? "interior_prefilter" : "interior");
+            if (opts->use_prefiltering)
+                ctx->launches +=
+                    launch_interior_prefilter(S, sp, d_render, ctx->wsum.as<float>(), G, ctx->status, ctx->stream);
+            else
+                ctx->launches += launch_interior(S, sp, d_render, ctx->wsum.as<float>(), G, ctx->status, ctx->stream);
         }
         CK(cudaGetLastError());
-        if (S.boundary_ok) {
+        if (S.boundary_ok && !opts->use_prefiltering) {  // src/backward/render.rs:191
             BoundaryParams bp;
             uint64_t total = (uint64_t)npix * sp.sxn * sp.syn;
             bp.num_samples = bopts && bopts->boundary_samples ? bopts->boundary_samples : total;
@@ -767,7 +777,10 @@ extern "C" dvg_status dvg_render_device_noalloc(dvg_context* ctx, dvg_scene* sce
     float* wsum = scratch + 4 * npix;  // 1 float per pixel
     CK(cudaMemsetAsync(scratch, 0, 5 * npix * sizeof(float), ctx->stream));
     const SampleParams sp = sample_params(opts);
-    ctx->launches += launch_forward(S, sp, accum, wsum, ctx->status, ctx->stream);
+    if (opts->use_prefiltering)
+        ctx->launches += launch_forward_prefilter(S, sp, accum, wsum, ctx->status, ctx->stream);
+    else
+        ctx->launches += launch_forward(S, sp, accum, wsum, ctx->status, ctx->stream);
     ctx->launches += launch_resolve(S, accum, wsum, out_rgba, ctx->stream);
     CK(cudaGetLastError());
     return DVG_OK;

@@ -44,7 +44,7 @@ struct DevScene {
     const int4* g_bvh;   // node off, node count, list off, list count
     const int* g_shape_list;
     const float4* gn_bounds;
-    const int4* gn_meta;  // skip, leaf start, count, 0
+    const int4* gn_meta;  // skip, leaf start, count, right child (left child = node + 1)
     const int* gl_shapes;
     // shapes
     const int4* s_info;  // kind, flags, path index, 0
@@ -479,6 +479,38 @@ static __device__ __noinline__ int winding_segment(const SegGeom& s, float2 pt) 
     return w;
 }
 
+// ------------------------------------------------------------------ exact-result culling
+// A segment whose control-point hull lies strictly beyond the +x ray by more than
+// the rounding of the crate's root solve cannot add a crossing: the computed
+// polynomial then has no root in [0,1] with x(t) > pt.x, so winding_segment would
+// return 0.  The margin is ~300x the worst-case f32 coefficient error
+// (~3e-6 * max |coordinate|), so skipping such segments never changes a result.
+__device__ __forceinline__ float cull_margin(const SegGeom& s, float2 p) {
+    float m = fmaxf(fabsf(p.x), fabsf(p.y));
+#pragma unroll
+    for (int k = 0; k < 8; ++k) m = fmaxf(m, fabsf(s.q[k]));
+    return 1.0e-3f * (1.0f + m);
+}
+__device__ __forceinline__ bool ray_misses_segment(const SegGeom& s, float2 p) {
+    float ymin = fminf(fminf(s.q[1], s.q[3]), fminf(s.q[5], s.q[7]));
+    float ymax = fmaxf(fmaxf(s.q[1], s.q[3]), fmaxf(s.q[5], s.q[7]));
+    float xmax = fmaxf(fmaxf(s.q[0], s.q[2]), fmaxf(s.q[4], s.q[6]));
+    float m = cull_margin(s, p);
+    return p.y < ymin - m || p.y > ymax + m || p.x > xmax + m;
+}
+// A point farther than max radius (+margin) outside the control-point box of a
+// segment cannot satisfy dist < radius(t): the closest point lies in the hull.
+__device__ __forceinline__ bool stroke_misses_segment(const SegGeom& s, float2 p) {
+    float xmin = fminf(fminf(s.q[0], s.q[2]), fminf(s.q[4], s.q[6]));
+    float xmax = fmaxf(fmaxf(s.q[0], s.q[2]), fmaxf(s.q[4], s.q[6]));
+    float ymin = fminf(fminf(s.q[1], s.q[3]), fminf(s.q[5], s.q[7]));
+    float ymax = fmaxf(fmaxf(s.q[1], s.q[3]), fmaxf(s.q[5], s.q[7]));
+    float r = fmaxf(fmaxf(s.r[0], s.r[1]), fmaxf(s.r[2], s.r[3]));
+    float m = cull_margin(s, p) + 1.0e-5f * fabsf(r);
+    r = r + m;
+    return p.x < xmin - r || p.x > xmax + r || p.y < ymin - r || p.y > ymax + r;
+}
+
 // ------------------------------------------------------------------ path queries
 // Walks the path's BVH (preorder with skip links).  Node tests are exactly the
 // crate's: ray test for winding (winding.rs:117-126), containment for strokes.
@@ -498,7 +530,7 @@ __device__ __forceinline__ int winding_path(const DevScene& S, int path, float2 
             for (int k = m.y; k < m.y + m.z; ++k) {
                 SegGeom sg;
                 load_seg(S, __ldg(&S.pl_segs[k]), sg);
-                w += winding_segment(sg, p);
+                if (!ray_misses_segment(sg, p)) w += winding_segment(sg, p);
             }
             n = m.x;
         } else {
@@ -514,7 +546,7 @@ __device__ __forceinline__ int winding_path_list(const DevScene& S, int path, fl
     for (int k = 0; k < pi.y; ++k) {
         SegGeom sg;
         load_seg(S, pi.x + k, sg);
-        w += winding_segment(sg, p);
+        if (!ray_misses_segment(sg, p)) w += winding_segment(sg, p);
     }
     return w;
 }
@@ -534,6 +566,7 @@ __device__ __forceinline__ bool within_path_bvh(const DevScene& S, int path, flo
             for (int k = m.y; k < m.y + m.z; ++k) {
                 SegGeom sg;
                 load_seg(S, __ldg(&S.pl_segs[k]), sg);
+                if (stroke_misses_segment(sg, p)) continue;
                 CPRes c = seg_closest(sg, p, approx);
                 if (c.dist < seg_radius(sg, c.t)) return true;
             }
@@ -550,6 +583,7 @@ __device__ __forceinline__ bool within_path_list(const DevScene& S, int path, fl
     for (int k = 0; k < pi.y; ++k) {
         SegGeom sg;
         load_seg(S, pi.x + k, sg);
+        if (stroke_misses_segment(sg, p)) continue;
         CPRes c = seg_closest(sg, p, approx);
         if (c.dist < seg_radius(sg, c.t)) return true;
     }
@@ -882,6 +916,225 @@ __device__ __forceinline__ void over(float4& acc, float4 c) {
     acc.y = acc.y * inv + c.y * a;
     acc.z = acc.z * inv + c.z * a;
     acc.w = acc.w * inv + a;
+}
+
+// ------------------------------------------------------------------ gradients
+struct GradPtrs {
+    float* d_shape_params;
+    float* d_shape_transform;
+    float* d_shape_stroke_width;
+    float* d_points;
+    float* d_thickness;
+    float* d_group_transform;
+    float* d_paint_params;
+    float* d_stop_offsets;
+    float* d_stop_colors;
+    float* d_filter_radius;
+    float* d_background;
+    float* d_background_image;
+    float* d_translation;
+};
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ void add_if(float* p, float v) {
+    if (v != 0.0f) atomicAdd(p, v);
+}
+
+// d_sample_paint for gradient paints (backward/paint.rs:91-277), per-lane atomics.
+static __device__ void d_gradient_paint(const DevScene& S, const GradPtrs& G, int p, float2 pt, float4 dc, float2* dtr) {
+    int4 pi = __ldg(&S.paint_info[p]);
+    float4 pp = __ldg(&S.paint_params[p]);
+    int so = pi.y, sc = pi.z;
+    if (sc <= 0) return;
+    float t, denom = 0.0f, offx = 0.0f, offy = 0.0f, nx = 0.0f, ny = 0.0f;
+    if (pi.x == P_LINEAR) {
+        float ex = pp.z - pp.x, ey = pp.w - pp.y;
+        denom = fmaxf(ex * ex + ey * ey, 1.0e-3f);
+        t = ((pt.x - pp.x) * ex + (pt.y - pp.y) * ey) / denom;
+    } else {
+        offx = pt.x - pp.x;
+        offy = pt.y - pp.y;
+        nx = offx / pp.z;
+        ny = offy / pp.w;
+        t = len2(nx, ny);
+    }
+    if (t < __ldg(&S.stop_offsets[so])) {
+        float* c = G.d_stop_colors + 4 * so;
+        add_if(c + 0, dc.x);
+        add_if(c + 1, dc.y);
+        add_if(c + 2, dc.z);
+        add_if(c + 3, dc.w);
+        return;
+    }
+    for (int i = 0; i + 1 < sc; ++i) {
+        float o0 = __ldg(&S.stop_offsets[so + i]), o1 = __ldg(&S.stop_offsets[so + i + 1]);
+        if (t >= o0 && t < o1) {
+            float tt = (t - o0) / (o1 - o0);
+            float4 c0 = __ldg(&S.stop_colors[so + i]), c1 = __ldg(&S.stop_colors[so + i + 1]);
+            float* a0 = G.d_stop_colors + 4 * (so + i);
+            float* a1 = a0 + 4;
+            add_if(a0 + 0, dc.x * (1.0f - tt));
+            add_if(a0 + 1, dc.y * (1.0f - tt));
+            add_if(a0 + 2, dc.z * (1.0f - tt));
+            add_if(a0 + 3, dc.w * (1.0f - tt));
+            add_if(a1 + 0, dc.x * tt);
+            add_if(a1 + 1, dc.y * tt);
+            add_if(a1 + 2, dc.z * tt);
+            add_if(a1 + 3, dc.w * tt);
+            float d_tt = dc.x * (c1.x - c0.x) + dc.y * (c1.y - c0.y) + dc.z * (c1.z - c0.z) + dc.w * (c1.w - c0.w);
+            float dof = o1 - o0;
+            if (fabsf(dof) > 0.0f) {
+                add_if(G.d_stop_offsets + so + i, d_tt * (tt - 1.0f) / dof);
+                add_if(G.d_stop_offsets + so + i + 1, -d_tt * tt / dof);
+            }
+            float d_t = d_tt / dof;
+            float* dpp = G.d_paint_params + 4 * p;
+            if (pi.x == P_LINEAR) {
+                float bx = d_t * (-(pt.x - pp.x) - (pp.z - pp.x)) / denom;
+                float by = d_t * (-(pt.y - pp.y) - (pp.w - pp.y)) / denom;
+                float ex = d_t * (pt.x - pp.x) / denom;
+                float ey = d_t * (pt.y - pp.y) / denom;
+                float d_l = -d_t * t / denom;
+                float lx = pp.z - pp.x, ly = pp.w - pp.y;
+                if (lx * lx + ly * ly > 1.0e-3f) {
+                    float ax = pp.x - pp.z, ay = pp.y - pp.w;
+                    add_if(dpp + 0, bx + 2.0f * d_l * ax);
+                    add_if(dpp + 1, by + 2.0f * d_l * ay);
+                    add_if(dpp + 2, ex + 2.0f * d_l * lx);
+                    add_if(dpp + 3, ey + 2.0f * d_l * ly);
+                } else {
+                    add_if(dpp + 0, bx);
+                    add_if(dpp + 1, by);
+                    add_if(dpp + 2, ex);
+                    add_if(dpp + 3, ey);
+                }
+                dtr->x += bx + ex;
+                dtr->y += by + ey;
+            } else {
+                // d_length(normalized, d_t) (backward/math.rs:33-41)
+                float l = sqrtf(nx * nx + ny * ny);
+                float dnx = 0.0f, dny = 0.0f;
+                if (l != 0.0f) {
+                    float dls = 0.5f * d_t / l;
+                    dnx = nx * (2.0f * dls);
+                    dny = ny * (2.0f * dls);
+                }
+                float dox = dnx / pp.z, doy = dny / pp.w;
+                float drx = -dnx * offx / (pp.z * pp.z), dry = -dny * offy / (pp.w * pp.w);
+                add_if(dpp + 0, -dox);
+                add_if(dpp + 1, -doy);
+                add_if(dpp + 2, drx);
+                add_if(dpp + 3, dry);
+                dtr->x += -dox;
+                dtr->y += -doy;
+            }
+            return;
+        }
+    }
+    float* c = G.d_stop_colors + 4 * (so + sc - 1);
+    add_if(c + 0, dc.x);
+    add_if(c + 1, dc.y);
+    add_if(c + 2, dc.z);
+    add_if(c + 3, dc.w);
+}
+
+
+// ------------------------------------------------------------------ filtered splat / gather
+// Adds the sample's premultiplied colour times the filter weight (and the weight)
+// to every pixel of its (2*ri+1)^2 footprint: into the CTA's shared tile+halo
+// accumulator when it fits, else straight to global memory.
+__device__ __forceinline__ void splat_sample(const DevScene& S, int x, int y, int tx, int ty, int ri, int HW,
+                                             bool use_sm, float2 pt, float4 acc, float* sm, float* accum,
+                                             float* wsum) {
+    for (int dy = -ri; dy <= ri; ++dy)
+        for (int dx = -ri; dx <= ri; ++dx) {
+            int xx = x + dx, yy = y + dy;
+            if (xx < 0 || yy < 0 || xx >= S.width || yy >= S.height) continue;
+            float w = filter_weight(S.filter_type, S.filter_radius, (float)xx + 0.5f - pt.x, (float)yy + 0.5f - pt.y);
+            if (!(w > 0.0f)) continue;
+            if (use_sm) {
+                int li = (yy - (ty * TILE - ri)) * HW + (xx - (tx * TILE - ri));
+                float* c = sm + 5 * li;
+                atomicAdd(c + 0, acc.x * w);
+                atomicAdd(c + 1, acc.y * w);
+                atomicAdd(c + 2, acc.z * w);
+                atomicAdd(c + 3, acc.w * w);
+                atomicAdd(c + 4, w);
+            } else {
+                size_t p = (size_t)yy * S.width + xx;
+                atomicAdd(accum + 4 * p + 0, acc.x * w);
+                atomicAdd(accum + 4 * p + 1, acc.y * w);
+                atomicAdd(accum + 4 * p + 2, acc.z * w);
+                atomicAdd(accum + 4 * p + 3, acc.w * w);
+                atomicAdd(wsum + p, w);
+            }
+        }
+}
+// Flushes the CTA's tile+halo accumulator to global memory (one atomic per value).
+__device__ __forceinline__ void flush_splat(const DevScene& S, int tx, int ty, int ri, int HW, const float* sm,
+                                            float* accum, float* wsum) {
+    for (int i = threadIdx.x; i < HW * HW; i += blockDim.x) {
+        const float* c = sm + 5 * i;
+        if (c[4] == 0.0f) continue;
+        int xx = tx * TILE - ri + i % HW, yy = ty * TILE - ri + i / HW;
+        if (xx < 0 || yy < 0 || xx >= S.width || yy >= S.height) continue;
+        size_t p = (size_t)yy * S.width + xx;
+        atomicAdd(accum + 4 * p + 0, c[0]);
+        atomicAdd(accum + 4 * p + 1, c[1]);
+        atomicAdd(accum + 4 * p + 2, c[2]);
+        atomicAdd(accum + 4 * p + 3, c[3]);
+        atomicAdd(wsum + p, c[4]);
+    }
+}
+// gather_d_color (src/backward/filters.rs:70-103)
+__device__ __forceinline__ float4 gather_d_color(const DevScene& S, const float* d_render, const float* wsum,
+                                                 float2 ps) {
+    float4 out = make_float4(0, 0, 0, 0);
+    const int px = f2i(floorf(ps.x)), py = f2i(floorf(ps.y)), ri = S.filter_ri;
+    for (int dy = -ri; dy <= ri; ++dy)
+        for (int dx = -ri; dx <= ri; ++dx) {
+            int xx = px + dx, yy = py + dy;
+            if (xx < 0 || yy < 0 || xx >= S.width || yy >= S.height) continue;
+            float w = filter_weight(S.filter_type, S.filter_radius, (float)xx + 0.5f - ps.x, (float)yy + 0.5f - ps.y);
+            size_t q = (size_t)yy * S.width + xx;
+            float ws = wsum[q];
+            if (ws > 0.0f) {
+                float4 d = reinterpret_cast<const float4*>(d_render)[q];
+                float k = w / ws;
+                out.x += k * d.x;
+                out.y += k * d.y;
+                out.z += k * d.z;
+                out.w += k * d.w;
+            }
+        }
+    return out;
+}
+// accumulate_filter_gradient (src/backward/filters.rs:106-156) for one sample; returns d radius.
+__device__ __forceinline__ float filter_radius_adjoint(const DevScene& S, const float* d_render, const float* wsum,
+                                                       float2 ps, float4 color) {
+    float dradius = 0.0f;
+    const int px = f2i(floorf(ps.x)), py = f2i(floorf(ps.y)), ri = S.filter_ri;
+    for (int dy = -ri; dy <= ri; ++dy)
+        for (int dx = -ri; dx <= ri; ++dx) {
+            int xx = px + dx, yy = py + dy;
+            if (xx < 0 || yy < 0 || xx >= S.width || yy >= S.height) continue;
+            size_t q = (size_t)yy * S.width + xx;
+            float ws = wsum[q];
+            if (ws <= 0.0f) continue;
+            float fxc = (float)xx + 0.5f - ps.x, fyc = (float)yy + 0.5f - ps.y;
+            float w = filter_weight(S.filter_type, S.filter_radius, fxc, fyc);
+            if (w <= 0.0f) continue;
+            float4 d = reinterpret_cast<const float4*>(d_render)[q];
+            float dt = d.x * color.x + d.y * color.y + d.z * color.z + d.w * color.w;
+            float denom = ws * ws;
+            float dw = denom > 0.0f ? (dt * ws - w * dt * (ws - w)) / denom : 0.0f;
+            if (dw != 0.0f) dradius += d_filter_weight(S.filter_type, S.filter_radius, fxc, fyc, dw);
+        }
+    return dradius;
 }
 
 }  // namespace dvgb

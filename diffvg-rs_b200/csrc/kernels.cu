@@ -13,6 +13,18 @@
 #include "device.cuh"
 #include "kernels.cuh"
 
+// Minimum resident CTAs per SM for the scene-evaluation kernels (register cap =
+// 65536 / (threads * value)); chosen by measurement on B200.
+#ifndef DVG_MINB_FWD
+#define DVG_MINB_FWD 2
+#endif
+#ifndef DVG_MINB_INT
+#define DVG_MINB_INT 2
+#endif
+#ifndef DVG_MINB_BND
+#define DVG_MINB_BND 4
+#endif
+
 namespace dvgb {
 
 // ------------------------------------------------------------------ tile binning
@@ -106,7 +118,7 @@ __global__ void __launch_bounds__(256) k_bin_write(DevScene S, const float4* g_b
 // ------------------------------------------------------------------ forward
 // One CTA = one 16x16 tile at one sub-sample (sx, sy); thread = pixel.  Every
 // thread of the CTA walks the same group list, so group data loads are uniform.
-__global__ void __launch_bounds__(256) k_forward(DevScene S, SampleParams sp, float* accum, float* wsum,
+__global__ void __launch_bounds__(256, DVG_MINB_FWD) k_forward(DevScene S, SampleParams sp, float* accum, float* wsum,
                                                  unsigned* status) {
     extern __shared__ float sm[];
     const int ri = S.filter_ri;
@@ -133,45 +145,11 @@ __global__ void __launch_bounds__(256) k_forward(DevScene S, SampleParams sp, fl
             if (gi.y >= 0 && group_within(S, g, lp)) over(acc, paint_color(S, gi.y, pt));
             if (gi.x >= 0 && group_inside(S, g, lp, gi.z)) over(acc, paint_color(S, gi.x, pt));
         }
-        for (int dy = -ri; dy <= ri; ++dy)
-            for (int dx = -ri; dx <= ri; ++dx) {
-                int xx = x + dx, yy = y + dy;
-                if (xx < 0 || yy < 0 || xx >= S.width || yy >= S.height) continue;
-                float w = filter_weight(S.filter_type, S.filter_radius, (float)xx + 0.5f - pt.x,
-                                        (float)yy + 0.5f - pt.y);
-                if (!(w > 0.0f)) continue;
-                if (use_sm) {
-                    int li = (yy - (ty * TILE - ri)) * HW + (xx - (tx * TILE - ri));
-                    float* c = sm + 5 * li;
-                    atomicAdd(c + 0, acc.x * w);
-                    atomicAdd(c + 1, acc.y * w);
-                    atomicAdd(c + 2, acc.z * w);
-                    atomicAdd(c + 3, acc.w * w);
-                    atomicAdd(c + 4, w);
-                } else {
-                    size_t p = (size_t)yy * S.width + xx;
-                    atomicAdd(accum + 4 * p + 0, acc.x * w);
-                    atomicAdd(accum + 4 * p + 1, acc.y * w);
-                    atomicAdd(accum + 4 * p + 2, acc.z * w);
-                    atomicAdd(accum + 4 * p + 3, acc.w * w);
-                    atomicAdd(wsum + p, w);
-                }
-            }
+        splat_sample(S, x, y, tx, ty, ri, HW, use_sm, pt, acc, sm, accum, wsum);
     }
     if (!use_sm) return;
     __syncthreads();
-    for (int i = threadIdx.x; i < HW * HW; i += blockDim.x) {
-        const float* c = sm + 5 * i;
-        if (c[4] == 0.0f) continue;
-        int xx = tx * TILE - ri + i % HW, yy = ty * TILE - ri + i / HW;
-        if (xx < 0 || yy < 0 || xx >= S.width || yy >= S.height) continue;
-        size_t p = (size_t)yy * S.width + xx;
-        atomicAdd(accum + 4 * p + 0, c[0]);
-        atomicAdd(accum + 4 * p + 1, c[1]);
-        atomicAdd(accum + 4 * p + 2, c[2]);
-        atomicAdd(accum + 4 * p + 3, c[3]);
-        atomicAdd(wsum + p, c[4]);
-    }
+    flush_splat(S, tx, ty, ri, HW, sm, accum, wsum);
 }
 
 // Weight image only (rasterize_weights_f32, forward.rs:1505-1564).
@@ -213,113 +191,6 @@ __global__ void k_resolve(DevScene S, const float* accum, const float* wsum, flo
 }
 
 // ------------------------------------------------------------------ backward helpers
-__device__ __forceinline__ float warp_sum(float v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-__device__ __forceinline__ void add_if(float* p, float v) {
-    if (v != 0.0f) atomicAdd(p, v);
-}
-
-// d_sample_paint for gradient paints (backward/paint.rs:91-277), per-lane atomics.
-__device__ void d_gradient_paint(const DevScene& S, const GradPtrs& G, int p, float2 pt, float4 dc, float2* dtr) {
-    int4 pi = __ldg(&S.paint_info[p]);
-    float4 pp = __ldg(&S.paint_params[p]);
-    int so = pi.y, sc = pi.z;
-    if (sc <= 0) return;
-    float t, denom = 0.0f, offx = 0.0f, offy = 0.0f, nx = 0.0f, ny = 0.0f;
-    if (pi.x == P_LINEAR) {
-        float ex = pp.z - pp.x, ey = pp.w - pp.y;
-        denom = fmaxf(ex * ex + ey * ey, 1.0e-3f);
-        t = ((pt.x - pp.x) * ex + (pt.y - pp.y) * ey) / denom;
-    } else {
-        offx = pt.x - pp.x;
-        offy = pt.y - pp.y;
-        nx = offx / pp.z;
-        ny = offy / pp.w;
-        t = len2(nx, ny);
-    }
-    if (t < __ldg(&S.stop_offsets[so])) {
-        float* c = G.d_stop_colors + 4 * so;
-        add_if(c + 0, dc.x);
-        add_if(c + 1, dc.y);
-        add_if(c + 2, dc.z);
-        add_if(c + 3, dc.w);
-        return;
-    }
-    for (int i = 0; i + 1 < sc; ++i) {
-        float o0 = __ldg(&S.stop_offsets[so + i]), o1 = __ldg(&S.stop_offsets[so + i + 1]);
-        if (t >= o0 && t < o1) {
-            float tt = (t - o0) / (o1 - o0);
-            float4 c0 = __ldg(&S.stop_colors[so + i]), c1 = __ldg(&S.stop_colors[so + i + 1]);
-            float* a0 = G.d_stop_colors + 4 * (so + i);
-            float* a1 = a0 + 4;
-            add_if(a0 + 0, dc.x * (1.0f - tt));
-            add_if(a0 + 1, dc.y * (1.0f - tt));
-            add_if(a0 + 2, dc.z * (1.0f - tt));
-            add_if(a0 + 3, dc.w * (1.0f - tt));
-            add_if(a1 + 0, dc.x * tt);
-            add_if(a1 + 1, dc.y * tt);
-            add_if(a1 + 2, dc.z * tt);
-            add_if(a1 + 3, dc.w * tt);
-            float d_tt = dc.x * (c1.x - c0.x) + dc.y * (c1.y - c0.y) + dc.z * (c1.z - c0.z) + dc.w * (c1.w - c0.w);
-            float dof = o1 - o0;
-            if (fabsf(dof) > 0.0f) {
-                add_if(G.d_stop_offsets + so + i, d_tt * (tt - 1.0f) / dof);
-                add_if(G.d_stop_offsets + so + i + 1, -d_tt * tt / dof);
-            }
-            float d_t = d_tt / dof;
-            float* dpp = G.d_paint_params + 4 * p;
-            if (pi.x == P_LINEAR) {
-                float bx = d_t * (-(pt.x - pp.x) - (pp.z - pp.x)) / denom;
-                float by = d_t * (-(pt.y - pp.y) - (pp.w - pp.y)) / denom;
-                float ex = d_t * (pt.x - pp.x) / denom;
-                float ey = d_t * (pt.y - pp.y) / denom;
-                float d_l = -d_t * t / denom;
-                float lx = pp.z - pp.x, ly = pp.w - pp.y;
-                if (lx * lx + ly * ly > 1.0e-3f) {
-                    float ax = pp.x - pp.z, ay = pp.y - pp.w;
-                    add_if(dpp + 0, bx + 2.0f * d_l * ax);
-                    add_if(dpp + 1, by + 2.0f * d_l * ay);
-                    add_if(dpp + 2, ex + 2.0f * d_l * lx);
-                    add_if(dpp + 3, ey + 2.0f * d_l * ly);
-                } else {
-                    add_if(dpp + 0, bx);
-                    add_if(dpp + 1, by);
-                    add_if(dpp + 2, ex);
-                    add_if(dpp + 3, ey);
-                }
-                dtr->x += bx + ex;
-                dtr->y += by + ey;
-            } else {
-                // d_length(normalized, d_t) (backward/math.rs:33-41)
-                float l = sqrtf(nx * nx + ny * ny);
-                float dnx = 0.0f, dny = 0.0f;
-                if (l != 0.0f) {
-                    float dls = 0.5f * d_t / l;
-                    dnx = nx * (2.0f * dls);
-                    dny = ny * (2.0f * dls);
-                }
-                float dox = dnx / pp.z, doy = dny / pp.w;
-                float drx = -dnx * offx / (pp.z * pp.z), dry = -dny * offy / (pp.w * pp.w);
-                add_if(dpp + 0, -dox);
-                add_if(dpp + 1, -doy);
-                add_if(dpp + 2, drx);
-                add_if(dpp + 3, dry);
-                dtr->x += -dox;
-                dtr->y += -doy;
-            }
-            return;
-        }
-    }
-    float* c = G.d_stop_colors + 4 * (so + sc - 1);
-    add_if(c + 0, dc.x);
-    add_if(c + 1, dc.y);
-    add_if(c + 2, dc.z);
-    add_if(c + 3, dc.w);
-}
-
 // ------------------------------------------------------------------ interior backward
 // Per sample: gather d_color (filters.rs:70-103), recompute the fragments of
 // sample_color (sampling.rs:76-224) and back-propagate through compositing,
@@ -328,7 +199,7 @@ __device__ void d_gradient_paint(const DevScene& S, const GradPtrs& G, int p, fl
 // per-thread local memory, never in HBM.  The adjoint loop walks the tile's
 // group list in the same order on every lane so solid-paint gradients reduce
 // across the warp before one atomic.
-__global__ void __launch_bounds__(256) k_interior(DevScene S, SampleParams sp, const float* d_render,
+__global__ void __launch_bounds__(256, DVG_MINB_INT) k_interior(DevScene S, SampleParams sp, const float* d_render,
                                                   const float* wsum, GradPtrs G, unsigned* status) {
     __shared__ float red[8][6];
     const int tile = blockIdx.x, sub = blockIdx.y;
@@ -351,25 +222,7 @@ __global__ void __launch_bounds__(256) k_interior(DevScene S, SampleParams sp, c
         pt = make_float2(npt.x * (float)W, npt.y * (float)H);       // sampling.rs:91
         pixel = y * W + x;
         bg = background_premul(S, pixel);
-        // gather_d_color (filters.rs:70-103)
-        const int px = f2i(floorf(ps.x)), py = f2i(floorf(ps.y)), ri = S.filter_ri;
-        for (int dy = -ri; dy <= ri; ++dy)
-            for (int dx = -ri; dx <= ri; ++dx) {
-                int xx = px + dx, yy = py + dy;
-                if (xx < 0 || yy < 0 || xx >= W || yy >= H) continue;
-                float w = filter_weight(S.filter_type, S.filter_radius, (float)xx + 0.5f - ps.x,
-                                        (float)yy + 0.5f - ps.y);
-                size_t q = (size_t)yy * W + xx;
-                float ws = wsum[q];
-                if (ws > 0.0f) {
-                    float4 d = reinterpret_cast<const float4*>(d_render)[q];
-                    float k = w / ws;
-                    dcol.x += k * d.x;
-                    dcol.y += k * d.y;
-                    dcol.z += k * d.z;
-                    dcol.w += k * d.w;
-                }
-            }
+        dcol = gather_d_color(S, d_render, wsum, ps);
     }
     // Pass 1: fragments in order (stroke before fill within a group).
     int code[MAX_FRAGMENTS];
@@ -508,26 +361,7 @@ __global__ void __launch_bounds__(256) k_interior(DevScene S, SampleParams sp, c
         }
     }
     // Filter-radius adjoint (filters.rs:106-156) and the constant-background adjoint.
-    float dradius = 0.0f;
-    if (active) {
-        const int px = f2i(floorf(ps.x)), py = f2i(floorf(ps.y)), ri = S.filter_ri;
-        for (int dy = -ri; dy <= ri; ++dy)
-            for (int dx = -ri; dx <= ri; ++dx) {
-                int xx = px + dx, yy = py + dy;
-                if (xx < 0 || yy < 0 || xx >= W || yy >= H) continue;
-                size_t q = (size_t)yy * W + xx;
-                float ws = wsum[q];
-                if (ws <= 0.0f) continue;
-                float fxc = (float)xx + 0.5f - ps.x, fyc = (float)yy + 0.5f - ps.y;
-                float w = filter_weight(S.filter_type, S.filter_radius, fxc, fyc);
-                if (w <= 0.0f) continue;
-                float4 d = reinterpret_cast<const float4*>(d_render)[q];
-                float dt = d.x * ret.x + d.y * ret.y + d.z * ret.z + d.w * ret.w;
-                float denom = ws * ws;
-                float dw = denom > 0.0f ? (dt * ws - w * dt * (ws - w)) / denom : 0.0f;
-                if (dw != 0.0f) dradius += d_filter_weight(S.filter_type, S.filter_radius, fxc, fyc, dw);
-            }
-    }
+    const float dradius = active ? filter_radius_adjoint(S, d_render, wsum, ps, ret) : 0.0f;
     float v[5] = {dcol.x, dcol.y, dcol.z, dcol.w, dradius};
 #pragma unroll
     for (int k = 0; k < 5; ++k) v[k] = warp_sum(v[k]);
@@ -1058,7 +892,7 @@ __global__ void k_boundary_scatter(const int* key, uint64_t n, int* cursor, int*
 }
 // Stage 3: evaluate both sides of every edge sample in tile order, so that the
 // lanes of a warp share one group list (render_edge_sample, boundary.rs:845-967).
-__global__ void __launch_bounds__(128) k_boundary_eval(DevScene S, const BSample* samples, const int* order,
+__global__ void __launch_bounds__(128, DVG_MINB_BND) k_boundary_eval(DevScene S, const BSample* samples, const int* order,
                                                        const int* offsets, int tiles, const float* d_render,
                                                        const float* wsum, GradPtrs G) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -38,31 +38,21 @@ struct BSample {
     float bt;
     int is_stroke, pad;
 };
-struct GradPtrs {
-    float* d_shape_params;
-    float* d_shape_transform;
-    float* d_shape_stroke_width;
-    float* d_points;
-    float* d_thickness;
-    float* d_group_transform;
-    float* d_paint_params;
-    float* d_stop_offsets;
-    float* d_stop_colors;
-    float* d_filter_radius;
-    float* d_background;
-    float* d_background_image;
-    float* d_translation;
-};
+
 
 // Launchers (all asynchronous on `stream`).  Each returns the number of kernels launched.
 int launch_binning(const DevScene& S, const float4* g_bbox, int* counts, int* offsets, int* entries_or_null,
                    cudaStream_t stream);
 int launch_forward(const DevScene& S, const SampleParams& sp, float* accum, float* wsum, unsigned* status,
                    cudaStream_t stream);
+int launch_forward_prefilter(const DevScene& S, const SampleParams& sp, float* accum, float* wsum, unsigned* status,
+                             cudaStream_t stream);
 int launch_weights(const DevScene& S, const SampleParams& sp, float* wsum, cudaStream_t stream);
 int launch_resolve(const DevScene& S, const float* accum, const float* wsum, float* out, cudaStream_t stream);
 int launch_interior(const DevScene& S, const SampleParams& sp, const float* d_render, const float* wsum,
                     const GradPtrs& G, unsigned* status, cudaStream_t stream);
+int launch_interior_prefilter(const DevScene& S, const SampleParams& sp, const float* d_render, const float* wsum,
+                              const GradPtrs& G, unsigned* status, cudaStream_t stream);
 // Boundary pass in chunks of at most `capacity` samples; scratch: samples[capacity],
 // key[capacity], order[capacity], counts[2*tiles+1].
 int launch_boundary(const DevScene& S, const BoundaryParams& bp, const float* d_render, const float* wsum,

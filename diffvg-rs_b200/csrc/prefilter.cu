@@ -1,0 +1,932 @@
+// prefilter.cu — prefiltered (smoothstep-coverage) forward and interior adjoint.
+//
+// RenderOptions::use_prefiltering (the crate's default): coverage comes from
+// the signed distance to the closest boundary (src/backward/sampling.rs:227-482)
+// instead of point sampling, so the interior adjoint also reaches the geometry
+// through d_compute_distance (src/backward/distance.rs:50-561).  The closest-point
+// search walks the crate's BVHs with an explicit stack in the crate's order
+// (closer child first, src/distance/api.rs:138-236, closest.rs:104-199): the
+// order only matters for exact distance ties, which it resolves the same way.
+// Built with -fmad=false like kernels.cu.
+#include "device.cuh"
+#include "kernels.cuh"
+
+namespace dvgb {
+
+constexpr int BVH_STACK = 64;
+constexpr float INF_F = __builtin_huge_valf();
+
+__device__ __forceinline__ float box_distance(float4 b, float2 p) {  // Bounds::distance (bvh.rs:109-113)
+    float dx = fmaxf(fmaxf(b.x - p.x, 0.0f), p.x - b.z);
+    float dy = fmaxf(fmaxf(b.y - p.y, 0.0f), p.y - b.w);
+    return sqrtf(dx * dx + dy * dy);
+}
+
+struct ClosestD {
+    int shape;
+    float2 point;  // canvas space
+    float dist;
+    int seg;  // segment index within the path, -1 when the shape is not a path
+    float t;
+};
+
+// closest_point_path_bvh (closest.rs:104-199); cp in shape space.
+__device__ bool closest_path_bvh(const DevScene& S, int path, float2 p, float2* cp, int* seg, float* tt,
+                                 unsigned* status) {
+    const int4 pi = __ldg(&S.p_info[2 * path]);
+    if (pi.w == 0) return false;
+    const bool approx = __ldg(&S.p_info[2 * path + 1].w) & PF_APPROX;
+    float best = INF_F, bt = 0.0f;
+    float2 bp = make_float2(0.0f, 0.0f);
+    int bseg = 0;
+    int stk[BVH_STACK];
+    int sp = 0;
+    stk[sp++] = pi.z;
+    int guard = 0;
+    while (sp > 0 && guard++ < (1 << 20)) {
+        const int n = stk[--sp];
+        const int4 m = __ldg(&S.pn_meta[n]);
+        if (box_distance(__ldg(&S.pn_bounds[n]), p) > best) continue;
+        if (m.z > 0) {
+            for (int k = m.y; k < m.y + m.z; ++k) {
+                const int sidx = __ldg(&S.pl_segs[k]);
+                SegGeom sg;
+                load_seg(S, sidx, sg);
+                CPRes c = seg_closest(sg, p, approx);
+                if (c.dist < best) {
+                    best = c.dist;
+                    bp = make_float2(c.cx, c.cy);
+                    bseg = __ldg(&S.seg_meta[sidx].y);
+                    bt = c.t;
+                }
+            }
+        } else {
+            const int l = n + 1, r = m.w;
+            const float ld = box_distance(__ldg(&S.pn_bounds[l]), p);
+            const float rd = r >= 0 ? box_distance(__ldg(&S.pn_bounds[r]), p) : INF_F;
+            if (sp + 2 > BVH_STACK) {
+                atomicOr(status, ST_BVH_LIMIT);
+                break;
+            }
+            if (ld < rd) {
+                if (rd <= best) stk[sp++] = r;
+                if (ld <= best) stk[sp++] = l;
+            } else {
+                if (ld <= best) stk[sp++] = l;
+                if (rd <= best) stk[sp++] = r;
+            }
+        }
+    }
+    if (!isfinite(best)) return false;
+    *cp = bp;
+    *seg = bseg;
+    *tt = bt;
+    return true;
+}
+
+__device__ __forceinline__ float2 closest_point_rect(float4 r, float2 p) {  // shape.rs:167-185
+    bool inside = p.x >= r.x && p.x <= r.z && p.y >= r.y && p.y <= r.w;
+    if (!inside) return make_float2(clampf(p.x, r.x, r.z), clampf(p.y, r.y, r.w));
+    float dl = p.x - r.x, dr = r.z - p.x, db = p.y - r.y, dt = r.w - p.y;
+    if (dl <= dr && dl <= db && dl <= dt) return make_float2(r.x, p.y);
+    if (dr <= db && dr <= dt) return make_float2(r.z, p.y);
+    if (db <= dt) return make_float2(p.x, r.y);
+    return make_float2(p.x, r.w);
+}
+
+// closest_point_shape (closest.rs:386-456); lp and the result in group space.
+__device__ bool closest_shape(const DevScene& S, int s, float2 lp, float2* out, int* seg, float* t) {
+    const float2 p = shape_local_dist(S, s, lp);
+    const int4 si = __ldg(&S.s_info[s]);
+    const float4 prm = __ldg(&S.s_params[s]);
+    const float* X = S.s_xform + 9 * s;
+    *seg = -1;
+    *t = 0.0f;
+    float2 c;
+    if (si.x == K_CIRCLE) {
+        float r = fabsf(prm.z);
+        float dx = p.x - prm.x, dy = p.y - prm.y;
+        float len = len2(dx, dy);
+        if (len <= 1.0e-8f)
+            c = make_float2(prm.x + r, prm.y);
+        else {
+            float k = r / len;
+            c = make_float2(prm.x + dx * k, prm.y + dy * k);
+        }
+    } else if (si.x == K_ELLIPSE) {
+        c = closest_point_ellipse(prm.x, prm.y, fabsf(prm.z), fabsf(prm.w), p);
+    } else if (si.x == K_RECT) {
+        c = closest_point_rect(prm, p);
+    } else {
+        if (si.z < 0) return false;
+        const int4 pi = __ldg(&S.p_info[2 * si.z]);
+        const int4 pi2 = __ldg(&S.p_info[2 * si.z + 1]);
+        if (pi2.y == 0) return false;
+        const bool approx = pi2.w & PF_APPROX;
+        float best = INF_F, bt = 0.0f;
+        float2 bp = make_float2(0.0f, 0.0f);
+        int bseg = 0;
+        for (int k = 0; k < pi.y; ++k) {
+            SegGeom sg;
+            load_seg(S, pi.x + k, sg);
+            CPRes cc = seg_closest(sg, p, approx);
+            if (cc.dist < best) {
+                best = cc.dist;
+                bp = make_float2(cc.cx, cc.cy);
+                bseg = k;
+                bt = cc.t;
+            }
+        }
+        if (!isfinite(best)) return false;
+        c = bp;
+        *seg = bseg;
+        *t = bt;
+    }
+    *out = xf9(X, c);
+    return true;
+}
+
+// compute_distance_bvh (api.rs:138-236) with the brute-force fallback compute_distance (api.rs:36-76).
+__device__ bool compute_distance_group(const DevScene& S, int g, float2 pt, float max_radius, ClosestD* best,
+                                       unsigned* status) {
+    const int4 gb = __ldg(&S.g_bvh[g]);
+    const float* s2c = S.g_s2c + 9 * g;
+    const float2 lp = xf9(S.g_c2s + 9 * g, pt);
+    if (gb.y == 0) {
+        bool have = false;
+        for (int k = 0; k < gb.w; ++k) {
+            const int s = __ldg(&S.g_shape_list[gb.z + k]);
+            float2 lc;
+            int seg;
+            float t;
+            if (!closest_shape(S, s, lp, &lc, &seg, &t)) continue;
+            const float2 cl = xf9(s2c, lc);
+            const float d = len2(cl.x - pt.x, cl.y - pt.y);
+            if (d <= max_radius && (!have || d < best->dist)) {
+                *best = ClosestD{s, cl, d, seg, t};
+                have = true;
+            }
+        }
+        return have;
+    }
+    float best_dist = max_radius;
+    bool have = false;
+    int stk[BVH_STACK];
+    int sp = 0;
+    stk[sp++] = gb.x;
+    int guard = 0;
+    while (sp > 0 && guard++ < (1 << 20)) {
+        const int n = stk[--sp];
+        const int4 m = __ldg(&S.gn_meta[n]);
+        if (box_distance(__ldg(&S.gn_bounds[n]), lp) > best_dist) continue;
+        if (m.z > 0) {
+            for (int k = m.y; k < m.y + m.z; ++k) {
+                const int s = __ldg(&S.gl_shapes[k]);
+                const int4 si = __ldg(&S.s_info[s]);
+                float2 lc;
+                int seg = -1;
+                float t = 0.0f;
+                bool ok;
+                if (si.x == K_PATH && si.z >= 0 && __ldg(&S.p_info[2 * si.z].w) > 0) {
+                    float2 scp;
+                    ok = closest_path_bvh(S, si.z, shape_local_dist(S, s, lp), &scp, &seg, &t, status);
+                    if (ok) lc = xf9(S.s_xform + 9 * s, scp);
+                } else {
+                    ok = closest_shape(S, s, lp, &lc, &seg, &t);
+                }
+                if (!ok) continue;
+                const float2 cl = xf9(s2c, lc);
+                const float d = len2(cl.x - pt.x, cl.y - pt.y);
+                if (d <= best_dist) {
+                    best_dist = d;
+                    *best = ClosestD{s, cl, d, seg, t};
+                    have = true;
+                }
+            }
+        } else {
+            const int l = n + 1, r = m.w;
+            const float ld = box_distance(__ldg(&S.gn_bounds[l]), lp);
+            const float rd = r >= 0 ? box_distance(__ldg(&S.gn_bounds[r]), lp) : INF_F;
+            if (sp + 2 > BVH_STACK) {
+                atomicOr(status, ST_BVH_LIMIT);
+                break;
+            }
+            if (ld < rd) {
+                if (rd <= best_dist) stk[sp++] = r;
+                if (ld <= best_dist) stk[sp++] = l;
+            } else {
+                if (ld <= best_dist) stk[sp++] = l;
+                if (rd <= best_dist) stk[sp++] = r;
+            }
+        }
+    }
+    return have;
+}
+
+__device__ __forceinline__ float smoothstep1(float d) {  // backward/math.rs:9-12
+    float t = clampf((d + 1.0f) * 0.5f, 0.0f, 1.0f);
+    return t * t * (3.0f - 2.0f * t);
+}
+__device__ __forceinline__ float d_smoothstep(float d, float d_ret) {  // backward/math.rs:15-22
+    if (d < -1.0f || d > 1.0f) return 0.0f;
+    float t = (d + 1.0f) * 0.5f;
+    float d_t = d_ret * (6.0f * t - 6.0f * t * t);
+    return d_t * 0.5f;
+}
+
+// One prefiltered fragment (sampling.rs:240-300).
+struct PFragD {
+    bool hit;
+    float4 c;  // paint colour with alpha already scaled by the coverage w
+    int shape;
+    float dist;  // signed distance used for the coverage
+    float2 cp;   // closest point, canvas space
+    int seg;     // path segment of the closest point or -1
+    float t;
+    bool within;
+};
+__device__ __forceinline__ PFragD prefilter_stroke(const DevScene& S, int g, int paint, float2 pt, unsigned* status) {
+    PFragD f;
+    f.hit = false;
+    ClosestD h;
+    if (!compute_distance_group(S, g, pt, INF_F, &h, status)) return f;
+    const float sw = __ldg(&S.s_stroke[h.shape]);
+    const float d = h.dist;
+    const float w = smoothstep1(fabsf(d) + sw) - smoothstep1(fabsf(d) - sw);
+    if (!(w > 0.0f)) return f;
+    f.c = paint_color(S, paint, pt);
+    f.c.w *= w;
+    f.hit = true;
+    f.shape = h.shape;
+    f.dist = d;
+    f.cp = h.point;
+    f.seg = h.seg;
+    f.t = h.t;
+    f.within = true;
+    return f;
+}
+__device__ __forceinline__ PFragD prefilter_fill(const DevScene& S, int g, int paint, int rule, float2 pt,
+                                                 unsigned* status) {
+    PFragD f;
+    f.hit = false;
+    ClosestD h;
+    const bool have = compute_distance_group(S, g, pt, 1.0f, &h, status);
+    const bool inside = group_inside(S, g, xf9(S.g_c2s + 9 * g, pt), rule);
+    if (!have && !inside) return f;
+    float d = have ? h.dist : 1.0f;
+    if (!inside) d = -d;
+    const float w = smoothstep1(d);
+    if (!(w > 0.0f)) return f;
+    f.c = paint_color(S, paint, pt);
+    f.c.w *= w;
+    f.hit = true;
+    f.shape = have ? h.shape : 0;
+    f.dist = d;
+    f.cp = have ? h.point : make_float2(0.0f, 0.0f);
+    f.seg = have ? h.seg : -1;
+    f.t = have ? h.t : 0.0f;
+    f.within = have;
+    return f;
+}
+
+// ------------------------------------------------------------------ forward
+__global__ void __launch_bounds__(256, 2) k_forward_prefilter(DevScene S, SampleParams sp, float* accum, float* wsum,
+                                                              unsigned* status) {
+    extern __shared__ float sm[];
+    const int ri = S.filter_ri;
+    const int HW = TILE + 2 * ri;
+    const bool use_sm = ri <= MAX_SMEM_RI;
+    const int tile = blockIdx.x, sub = blockIdx.y;
+    const int tx = tile % S.tiles_x, ty = tile / S.tiles_x;
+    const int x = tx * TILE + (threadIdx.x % TILE), y = ty * TILE + (threadIdx.x / TILE);
+    if (use_sm)
+        for (int i = threadIdx.x; i < HW * HW * 5; i += blockDim.x) sm[i] = 0.0f;
+    __syncthreads();
+    const int off = S.tile_offsets[tile];
+    const int n = S.tile_offsets[tile + 1] - off;
+    const int* list = S.tile_entries + off;
+    if (x < S.width && y < S.height) {
+        const int sx = sub % sp.sxn, sy = sub / sp.sxn;
+        const float2 pt = sample_pos(x, y, sx, sy, sp.sxn, sp.syn, S.width, sp.seed, false);
+        float4 acc = background_premul(S, y * S.width + x);
+        for (int e = 0; e < n; ++e) {
+            const int g = __ldg(&list[e]);
+            const int4 gi = __ldg(&S.g_info[g]);
+            if (gi.y >= 0) {
+                PFragD f = prefilter_stroke(S, g, gi.y, pt, status);
+                if (f.hit) over(acc, f.c);
+            }
+            if (gi.x >= 0) {
+                PFragD f = prefilter_fill(S, g, gi.x, gi.z, pt, status);
+                if (f.hit) over(acc, f.c);
+            }
+        }
+        splat_sample(S, x, y, tx, ty, ri, HW, use_sm, pt, acc, sm, accum, wsum);
+    }
+    if (!use_sm) return;
+    __syncthreads();
+    flush_splat(S, tx, ty, ri, HW, sm, accum, wsum);
+}
+
+// ------------------------------------------------------------------ distance adjoint (backward/distance.rs)
+__device__ __forceinline__ void d_xform_pt(const float* m, float2 p, float2 d_out, float* dm, float2* d_p) {
+    float t0 = m[0] * p.x + m[1] * p.y + m[2];
+    float t1 = m[3] * p.x + m[4] * p.y + m[5];
+    float t2 = m[6] * p.x + m[7] * p.y + m[8];
+    float ox = t0 / t2, oy = t1 / t2;
+    float d0 = d_out.x / t2, d1 = d_out.y / t2, d2 = -(d_out.x * ox + d_out.y * oy) / t2;
+    dm[0] += d0 * p.x;
+    dm[1] += d0 * p.y;
+    dm[2] += d0;
+    dm[3] += d1 * p.x;
+    dm[4] += d1 * p.y;
+    dm[5] += d1;
+    dm[6] += d2 * p.x;
+    dm[7] += d2 * p.y;
+    dm[8] += d2;
+    d_p->x += d0 * m[0] + d1 * m[3] + d2 * m[6];
+    d_p->y += d0 * m[1] + d1 * m[4] + d2 * m[7];
+}
+__device__ __forceinline__ float2 d_length2(float2 v, float d_l) {
+    float l = sqrtf(v.x * v.x + v.y * v.y);
+    if (l == 0.0f) return make_float2(0.0f, 0.0f);
+    float k = 2.0f * (0.5f * d_l / l);
+    return make_float2(v.x * k, v.y * k);
+}
+__device__ __forceinline__ float dot2(float2 a, float2 b) { return a.x * b.x + a.y * b.y; }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 mul2(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+
+__device__ void add_point_grad(const GradPtrs& G, int po, int pc, bool closed, long idx, float2 d) {
+    long i = closed ? idx % pc : idx;
+    if (i < pc) {
+        add_if(G.d_points + 2 * (po + i), d.x);
+        add_if(G.d_points + 2 * (po + i) + 1, d.y);
+    }
+}
+// d_closest_point_path (distance.rs:190-394)
+__device__ void d_closest_point_path(const DevScene& S, const GradPtrs& G, int s, float2 pt, float2 d_cp, int seg,
+                                     float min_t, float2* d_pt) {
+    const int path = __ldg(&S.s_info[s].z);
+    const int4 pi = __ldg(&S.p_info[2 * path]);
+    const int4 pi2 = __ldg(&S.p_info[2 * path + 1]);
+    const int po = pi2.x, np = pi2.y, co = pi2.z;
+    const bool closed = pi2.w & PF_CLOSED;
+    if (np == 0) return;
+    const int pid = __ldg(&S.seg_meta[pi.x + seg].z);
+    auto gp = [&](long idx) { return S.points[po + (closed ? idx % np : (idx < np - 1 ? idx : np - 1))]; };
+    const int nc = seg < __ldg(&S.path_cdf_info[s].y) ? S.ncp[co + seg] : 0;
+    if (nc == 0) {
+        long i0 = pid, i1 = (pid + 1) % np;
+        float2 p0 = gp(i0), p1 = gp(i1);
+        float2 e = sub2(p1, p0);
+        float t = dot2(sub2(pt, p0), e) / dot2(e, e);
+        if (t < 0.0f) {
+            add_point_grad(G, po, np, closed, i0, d_cp);
+        } else if (t > 1.0f) {
+            add_point_grad(G, po, np, closed, i1, d_cp);
+        } else {
+            add_point_grad(G, po, np, closed, i0, mul2(d_cp, 1.0f - t));
+            add_point_grad(G, po, np, closed, i1, mul2(d_cp, t));
+        }
+    } else if (nc == 1) {
+        long i0 = pid, i1 = pid + 1, i2 = (pid + 2) % np;
+        float2 p0 = gp(i0), p1 = gp(i1), p2 = gp(i2);
+        float t = min_t;
+        float2 d0 = make_float2(0, 0), d1 = d0, d2 = d0;
+        if (t == 0.0f) {
+            d0 = add2(d0, d_cp);
+        } else if (t == 1.0f) {
+            d2 = add2(d2, d_cp);
+        } else {
+            float2 a = add2(sub2(p0, mul2(p1, 2.0f)), p2);
+            float2 b = sub2(p1, p0);
+            float2 q = sub2(p0, pt);
+            float A = dot2(a, a), B = 3.0f * dot2(a, b), C = 2.0f * dot2(b, b) + dot2(a, q);
+            float tt = 1.0f - t;
+            float d_tt = 2.0f * tt * dot2(d_cp, p0) + 2.0f * t * dot2(d_cp, p1);
+            float d_t = -d_tt + 2.0f * tt * dot2(d_cp, p1) + 2.0f * t * dot2(d_cp, p2);
+            d0 = add2(d0, mul2(d_cp, tt * tt));
+            d1 = add2(d1, mul2(d_cp, 2.0f * tt * t));
+            d2 = add2(d2, mul2(d_cp, t * t));
+            float pd = 3.0f * A * t * t + 2.0f * B * t + C;
+            if (fabsf(pd) > 1.0e-6f) {
+                float dA = -(d_t / pd) * t * t * t, dB = -(d_t / pd) * t * t, dC = -(d_t / pd) * t,
+                      dD = -(d_t / pd);
+                d0 = add2(d0, add2(add2(add2(add2(mul2(a, 2.0f * dA), mul2(sub2(b, a), 3.0f * dB)),
+                                             mul2(mul2(b, -4.0f), dC)),
+                                        mul2(add2(q, a), dC)),
+                                   mul2(sub2(b, q), 2.0f * dD)));
+                d1 = add2(d1, add2(add2(add2(add2(mul2(a, -4.0f * dA), mul2(add2(a, mul2(b, -2.0f)), 3.0f * dB)),
+                                             mul2(mul2(b, 4.0f), dC)),
+                                        mul2(q, -2.0f * dC)),
+                                   mul2(q, dD)));
+                d2 = add2(d2, add2(add2(mul2(a, 2.0f * dA), mul2(b, 3.0f * dB)), mul2(q, dC)));
+                *d_pt = add2(*d_pt, add2(mul2(a, -dC), mul2(b, dD)));
+            }
+        }
+        add_point_grad(G, po, np, closed, i0, d0);
+        add_point_grad(G, po, np, closed, i1, d1);
+        add_point_grad(G, po, np, closed, i2, d2);
+    } else if (nc == 2) {
+        long i0 = pid, i1 = pid + 1, i2 = pid + 2, i3 = (pid + 3) % np;
+        float2 p0 = gp(i0), p1 = gp(i1), p2 = gp(i2), p3 = gp(i3);
+        float t = min_t;
+        float2 d0 = make_float2(0, 0), d1 = d0, d2 = d0, d3 = d0;
+        if (t == 0.0f) {
+            d0 = add2(d0, d_cp);
+        } else if (t == 1.0f) {
+            d3 = add2(d3, d_cp);
+        } else {
+            float2 a = add2(add2(add2(mul2(p0, -1.0f), mul2(p1, 3.0f)), mul2(p2, -3.0f)), p3);
+            float2 b = add2(add2(mul2(p0, 3.0f), mul2(p1, -6.0f)), mul2(p2, 3.0f));
+            float2 c = add2(mul2(p0, -3.0f), mul2(p1, 3.0f));
+            float2 q = sub2(p0, pt);
+            float A = 3.0f * dot2(a, a);
+            if (fabsf(A) < 1.0e-10f) return;
+            float B = 5.0f * dot2(a, b);
+            float C = 4.0f * dot2(a, c) + 2.0f * dot2(b, b);
+            float D = 3.0f * (dot2(b, c) + dot2(a, q));
+            float E = dot2(c, c) + 2.0f * dot2(q, b);
+            float F = dot2(q, c);
+            B = B / A;
+            C = C / A;
+            D = D / A;
+            E = E / A;
+            F = F / A;
+            float tt = 1.0f - t;
+            float d_tt = 3.0f * tt * tt * dot2(d_cp, p0) + 6.0f * tt * t * dot2(d_cp, p1) +
+                         3.0f * t * t * dot2(d_cp, p2);
+            float d_t = -d_tt + 3.0f * tt * tt * dot2(d_cp, p1) + 6.0f * tt * t * dot2(d_cp, p2) +
+                        3.0f * t * t * dot2(d_cp, p3);
+            d0 = add2(d0, mul2(d_cp, tt * tt * tt));
+            d1 = add2(d1, mul2(d_cp, 3.0f * tt * tt * t));
+            d2 = add2(d2, mul2(d_cp, 3.0f * tt * t * t));
+            d3 = add2(d3, mul2(d_cp, t * t * t));
+            float pd = 5.0f * t * t * t * t + 4.0f * B * t * t * t + 3.0f * C * t * t + 2.0f * D * t + E;
+            if (fabsf(pd) > 1.0e-10f) {
+                float dB = -(d_t / pd) * t * t * t * t, dC = -(d_t / pd) * t * t * t, dD = -(d_t / pd) * t * t,
+                      dE = -(d_t / pd) * t, dF = -(d_t / pd);
+                float dA = -dB * B / A - dC * C / A - dD * D / A - dE * E / A - dF * F / A;
+                dB /= A;
+                dC /= A;
+                dD /= A;
+                dE /= A;
+                dF /= A;
+                d0 = add2(d0, mul2(a, 3.0f * -1.0f * 2.0f * dA));
+                d1 = add2(d1, mul2(a, 3.0f * 3.0f * 2.0f * dA));
+                d2 = add2(d2, mul2(a, 3.0f * -3.0f * 2.0f * dA));
+                d3 = add2(d3, mul2(a, 3.0f * 1.0f * 2.0f * dA));
+                d0 = add2(d0, mul2(add2(mul2(b, -1.0f), mul2(a, 3.0f)), 5.0f * dB));
+                d1 = add2(d1, mul2(add2(mul2(b, 3.0f), mul2(a, -6.0f)), 5.0f * dB));
+                d2 = add2(d2, mul2(add2(mul2(b, -3.0f), mul2(a, 3.0f)), 5.0f * dB));
+                d3 = add2(d3, mul2(b, 5.0f * dB));
+                d0 = add2(d0, add2(mul2(add2(mul2(c, -1.0f), mul2(a, -3.0f)), 4.0f * dC), mul2(b, 3.0f * 2.0f * dC)));
+                d1 = add2(d1, add2(mul2(add2(mul2(c, 3.0f), mul2(a, 3.0f)), 4.0f * dC), mul2(b, -6.0f * 2.0f * dC)));
+                d2 = add2(d2, add2(mul2(c, -3.0f * dC * 4.0f), mul2(b, 3.0f * 2.0f * dC)));
+                d3 = add2(d3, mul2(c, 4.0f * dC));
+                d0 = add2(d0, add2(mul2(add2(mul2(c, 3.0f), mul2(b, -3.0f)), 3.0f * dD), mul2(sub2(a, q), 3.0f * dD)));
+                d1 = add2(d1, add2(mul2(add2(mul2(c, -6.0f), mul2(b, 3.0f)), 3.0f * dD), mul2(q, 3.0f * 3.0f * dD)));
+                d2 = add2(d2, add2(mul2(c, 3.0f * 3.0f * dD), mul2(q, -3.0f * 3.0f * dD)));
+                *d_pt = add2(*d_pt, mul2(a, -1.0f * 3.0f * dD));
+                d0 = add2(d0, add2(mul2(c, -3.0f * 2.0f * dE), mul2(add2(b, mul2(q, 3.0f)), 2.0f * dE)));
+                d1 = add2(d1, add2(mul2(c, 3.0f * 2.0f * dE), mul2(q, -6.0f * 2.0f * dE)));
+                d2 = add2(d2, mul2(q, 3.0f * 2.0f * dE));
+                *d_pt = add2(*d_pt, mul2(b, -1.0f * 2.0f * dE));
+                d0 = add2(d0, add2(mul2(c, dF), mul2(q, -3.0f * dF)));
+                d1 = add2(d1, mul2(q, 3.0f * dF));
+                *d_pt = add2(*d_pt, mul2(c, -1.0f * dF));
+            }
+        }
+        add_point_grad(G, po, np, closed, i0, d0);
+        add_point_grad(G, po, np, closed, i1, d1);
+        add_point_grad(G, po, np, closed, i2, d2);
+        add_point_grad(G, po, np, closed, i3, d3);
+    }
+}
+// d_closest_point_ellipse (distance.rs:479-561)
+__device__ void d_closest_point_ellipse(float4 prm, float2 pt, float2 d_cp, float2* dc, float2* dr, float2* d_pt) {
+    float rx = fabsf(prm.z), ry = fabsf(prm.w);
+    const float eps = 1.0e-6f;
+    float lx = pt.x - prm.x, ly = pt.y - prm.y;
+    if (rx < eps && ry < eps) {
+        *dc = add2(*dc, d_cp);
+        return;
+    }
+    if (rx < eps) {
+        float hit = (ly >= -ry && ly <= ry) ? 1.0f : 0.0f;
+        *dc = add2(*dc, d_cp);
+        d_pt->y += d_cp.y * hit;
+        if (ly > ry)
+            dr->y += d_cp.y;
+        else if (ly < -ry)
+            dr->y -= d_cp.y;
+        return;
+    }
+    if (ry < eps) {
+        float hit = (lx >= -rx && lx <= rx) ? 1.0f : 0.0f;
+        *dc = add2(*dc, d_cp);
+        d_pt->x += d_cp.x * hit;
+        if (lx > rx)
+            dr->x += d_cp.x;
+        else if (lx < -rx)
+            dr->x -= d_cp.x;
+        return;
+    }
+    float sx = lx < 0.0f ? -1.0f : 1.0f, sy = ly < 0.0f ? -1.0f : 1.0f;
+    float x = fabsf(lx), y = fabsf(ly);
+    float t = atan2f(y * rx, x * ry);
+    float g_t = 0.0f;
+    for (int i = 0; i < 20; ++i) {
+        float sn = sinf(t), cs = cosf(t);
+        float gg = rx * x * sn - ry * y * cs + (ry * ry - rx * rx) * sn * cs;
+        g_t = rx * x * cs + ry * y * sn + (ry * ry - rx * rx) * (cs * cs - sn * sn);
+        if (fabsf(g_t) < 1.0e-12f) break;
+        float nx = clampf(t - gg / g_t, 0.0f, HALF_PI_F);
+        if (fabsf(nx - t) < 1.0e-6f) {
+            t = nx;
+            break;
+        }
+        t = nx;
+    }
+    float sn = sinf(t), cs = cosf(t);
+    float d_t = 0.0f;
+    dr->x += d_cp.x * sx * cs;
+    d_t += d_cp.x * sx * (-rx * sn);
+    dr->y += d_cp.y * sy * sn;
+    d_t += d_cp.y * sy * (ry * cs);
+    float g_a = x * sn - 2.0f * rx * sn * cs, g_b = -y * cs + 2.0f * ry * sn * cs, g_x = rx * sn, g_y = -ry * cs;
+    if (fabsf(g_t) > 1.0e-12f) {
+        float inv = -d_t / g_t;
+        dr->x += inv * g_a;
+        dr->y += inv * g_b;
+        float d_x = inv * g_x, d_y = inv * g_y;
+        d_pt->x += d_x * sx;
+        d_pt->y += d_y * sy;
+        dc->x -= d_x * sx;
+        dc->y -= d_y * sy;
+    }
+}
+// d_closest_point_rect (distance.rs:397-476)
+__device__ void d_closest_point_rect(float4 r, float2 pt, float2 d_cp, float2* d_min, float2* d_max, float2* d_pt) {
+    auto dist_to_seg = [&](float2 p0, float2 p1) {
+        float2 e = sub2(p1, p0);
+        float t = dot2(sub2(pt, p0), e) / dot2(e, e);
+        if (t < 0.0f) return len2(p0.x - pt.x, p0.y - pt.y);
+        if (t > 1.0f) return len2(p1.x - pt.x, p1.y - pt.y);
+        float2 q = sub2(add2(p0, mul2(e, t)), pt);
+        return len2(q.x, q.y);
+    };
+    float2 lt = make_float2(r.x, r.y), rt = make_float2(r.z, r.y), lb = make_float2(r.x, r.w), rb = make_float2(r.z, r.w);
+    int id = 0;
+    float md = dist_to_seg(lt, lb);
+    float top = dist_to_seg(lt, rt), right = dist_to_seg(rt, rb), bottom = dist_to_seg(lb, rb);
+    if (top < md) {
+        md = top;
+        id = 1;
+    }
+    if (right < md) {
+        md = right;
+        id = 2;
+    }
+    if (bottom < md) {
+        md = bottom;
+        id = 3;
+    }
+    float2 a = id == 0 ? lt : (id == 1 ? lt : (id == 2 ? rt : lb));
+    float2 b = id == 0 ? lb : (id == 1 ? rt : rb);
+    float2 da = make_float2(0, 0), db = make_float2(0, 0);
+    float2 e = sub2(b, a);
+    float t = dot2(sub2(pt, a), e) / dot2(e, e);
+    if (t < 0.0f) {
+        da = add2(da, d_cp);
+    } else if (t > 1.0f) {
+        db = add2(db, d_cp);
+    } else {
+        da = add2(da, mul2(d_cp, 1.0f - t));
+        db = add2(db, mul2(d_cp, t));
+        float d_t = dot2(d_cp, e);
+        float denom = dot2(e, e);
+        float d_num = d_t / denom, d_den = d_t * (-t) / denom;
+        *d_pt = add2(*d_pt, mul2(e, d_num));
+        db = add2(db, mul2(sub2(pt, a), d_num));
+        da = add2(da, mul2(sub2(add2(sub2(a, b), a), pt), d_num));
+        db = add2(db, mul2(e, 2.0f * d_den));
+        da = add2(da, mul2(sub2(a, b), 2.0f * d_den));
+    }
+    float2 dlt = make_float2(0, 0), drt = dlt, dlb = dlt, drb = dlt;
+    if (id == 0) {
+        dlt = da;
+        dlb = db;
+    } else if (id == 1) {
+        dlt = da;
+        drt = db;
+    } else if (id == 2) {
+        drt = da;
+        drb = db;
+    } else {
+        dlb = da;
+        drb = db;
+    }
+    *d_min = add2(*d_min, dlt);
+    d_max->x += drt.x;
+    d_min->y += drt.y;
+    d_min->x += dlb.x;
+    d_max->y += dlb.y;
+    *d_max = add2(*d_max, drb);
+}
+// d_compute_distance (distance.rs:50-136): geometry, shape and group transform
+// gradients by atomics; returns d_pt (for the translation adjoint).
+__device__ float2 d_compute_distance(const DevScene& S, const GradPtrs& G, int g, int s, float2 pt, float2 cp,
+                                     int seg, float seg_t, float d_dist) {
+    float dx = pt.x - cp.x, dy = pt.y - cp.y;
+    if (dx * dx + dy * dy < 1.0e-10f) return make_float2(0.0f, 0.0f);
+    const float* c2s = S.g_c2s + 9 * g;
+    const float* s2c = S.g_s2c + 9 * g;
+    const float* X = S.s_xform + 9 * s;
+    float inv[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    if (__ldg(&S.s_info[s].y) & SF_INVERTIBLE)
+        for (int k = 0; k < 6; ++k) inv[k] = S.s_inv[6 * s + k];
+    const float2 lpg = xf9(c2s, pt), lcg = xf9(c2s, cp);
+    const float2 lps = xf9(inv, lpg), lcs = xf9(inv, lcg);
+    float2 dl = d_length2(make_float2(pt.x - cp.x, pt.y - cp.y), d_dist);
+    float2 d_pt = dl;
+    float2 d_closest = make_float2(-dl.x, -dl.y);
+    float d_s2c[9] = {0}, d_st[9] = {0}, d_sinv[9] = {0}, d_c2s[9] = {0};
+    float2 d_lcg = make_float2(0, 0), d_lcs = make_float2(0, 0), d_lps = make_float2(0, 0), d_lpg = make_float2(0, 0);
+    d_xform_pt(s2c, lcg, d_closest, d_s2c, &d_lcg);
+    d_xform_pt(X, lcs, d_lcg, d_st, &d_lcs);
+    // d_closest_point (distance.rs:139-187)
+    const int4 si = __ldg(&S.s_info[s]);
+    const float4 prm = __ldg(&S.s_params[s]);
+    float* dp = G.d_shape_params + 4 * s;
+    if (si.x == K_CIRCLE) {
+        float2 v = make_float2(lps.x - prm.x, lps.y - prm.y);
+        float l = len2(v.x, v.y);
+        float2 n = l == 0.0f ? make_float2(0, 0) : make_float2(v.x / l, v.y / l);
+        float2 d_center = d_lcs;
+        float d_radius = dot2(d_lcs, n);
+        float2 d_n = mul2(d_lcs, prm.z);
+        float2 d_v = make_float2(0, 0);
+        if (l != 0.0f) {  // d_normalize (backward/math.rs:53-63)
+            d_v = make_float2(d_n.x / l, d_n.y / l);
+            float d_l = -dot2(d_n, n) / l;
+            d_v = add2(d_v, d_length2(v, d_l));
+        }
+        d_center = sub2(d_center, d_v);
+        d_lps = add2(d_lps, d_v);
+        add_if(dp + 0, d_center.x);
+        add_if(dp + 1, d_center.y);
+        add_if(dp + 2, d_radius);
+    } else if (si.x == K_ELLIPSE) {
+        float2 dc = make_float2(0, 0), dr = make_float2(0, 0);
+        d_closest_point_ellipse(prm, lps, d_lcs, &dc, &dr, &d_lps);
+        add_if(dp + 0, dc.x);
+        add_if(dp + 1, dc.y);
+        add_if(dp + 2, dr.x);
+        add_if(dp + 3, dr.y);
+    } else if (si.x == K_RECT) {
+        float2 dmn = make_float2(0, 0), dmx = make_float2(0, 0);
+        d_closest_point_rect(prm, lps, d_lcs, &dmn, &dmx, &d_lps);
+        add_if(dp + 0, dmn.x);
+        add_if(dp + 1, dmn.y);
+        add_if(dp + 2, dmx.x);
+        add_if(dp + 3, dmx.y);
+    } else if (si.x == K_PATH && seg >= 0 && si.z >= 0) {
+        d_closest_point_path(S, G, s, lps, d_lcs, seg, seg_t, &d_lps);
+    }
+    d_xform_pt(inv, lpg, d_lps, d_sinv, &d_lpg);
+    d_xform_pt(c2s, pt, d_lpg, d_c2s, &d_pt);
+    // d_group += d_s2c + (-c2s^T) d_c2s c2s^T ; d_shape += (-inv^T) d_sinv inv^T + d_st
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            float cg = 0.0f, cs = 0.0f;
+            for (int k = 0; k < 3; ++k) {
+                // (-A^T M)[r][k] summed against A^T[k][c] = A[c][k]
+                float mg = (-c2s[0 * 3 + r]) * d_c2s[0 * 3 + k] + (-c2s[1 * 3 + r]) * d_c2s[1 * 3 + k] +
+                           (-c2s[2 * 3 + r]) * d_c2s[2 * 3 + k];
+                float ms = (-inv[0 * 3 + r]) * d_sinv[0 * 3 + k] + (-inv[1 * 3 + r]) * d_sinv[1 * 3 + k] +
+                           (-inv[2 * 3 + r]) * d_sinv[2 * 3 + k];
+                cg += mg * c2s[3 * c + k];
+                cs += ms * inv[3 * c + k];
+            }
+            add_if(G.d_group_transform + 9 * g + 3 * r + c, (0.0f + d_s2c[3 * r + c]) + cg);
+            add_if(G.d_shape_transform + 9 * s + 3 * r + c, (0.0f + cs) + d_st[3 * r + c]);
+        }
+    return d_pt;
+}
+
+// ------------------------------------------------------------------ interior adjoint (sampling.rs:227-482)
+constexpr int MAX_PF = 48;
+__global__ void __launch_bounds__(256) k_interior_prefilter(DevScene S, SampleParams sp, const float* d_render,
+                                                            const float* wsum, GradPtrs G, unsigned* status) {
+    __shared__ float red[8][6];
+    const int tile = blockIdx.x, sub = blockIdx.y;
+    const int tx = tile % S.tiles_x, ty = tile / S.tiles_x;
+    const int x = tx * TILE + (threadIdx.x % TILE), y = ty * TILE + (threadIdx.x / TILE);
+    const bool valid = x < S.width && y < S.height;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int off = S.tile_offsets[tile];
+    const int n = S.tile_offsets[tile + 1] - off;
+    const int* list = S.tile_entries + off;
+    const int W = S.width, H = S.height;
+    float2 ps = make_float2(0.0f, 0.0f), pt = ps;
+    int pixel = 0;
+    float4 dcol = make_float4(0, 0, 0, 0), bg = dcol;
+    if (valid) {
+        const int sx = sub % sp.sxn, sy = sub / sp.sxn;
+        ps = sample_pos(x, y, sx, sy, sp.sxn, sp.syn, W, sp.seed, false);
+        pt = make_float2((ps.x / (float)W) * (float)W, (ps.y / (float)H) * (float)H);
+        pixel = y * W + x;
+        bg = background_premul(S, pixel);
+        dcol = gather_d_color(S, d_render, wsum, ps);
+    }
+    // pass 1: fragments with their distance data
+    int code[MAX_PF], fshape[MAX_PF], fseg[MAX_PF];
+    float tr[MAX_PF], fdist[MAX_PF], fcx[MAX_PF], fcy[MAX_PF], ft[MAX_PF];
+    bool fwithin[MAX_PF];
+    int nf = 0;
+    bool overflow = false;
+    float4 acc = bg;
+    if (valid) {
+        for (int e = 0; e < n; ++e) {
+            const int g = __ldg(&list[e]);
+            const int4 gi = __ldg(&S.g_info[g]);
+#pragma unroll
+            for (int which = 0; which < 2; ++which) {
+                PFragD f;
+                f.hit = false;
+                if (which == 0 && gi.y >= 0) f = prefilter_stroke(S, g, gi.y, pt, status);
+                if (which == 1 && gi.x >= 0) f = prefilter_fill(S, g, gi.x, gi.z, pt, status);
+                if (!f.hit) continue;
+                over(acc, f.c);
+                if (nf < MAX_PF) {
+                    code[nf] = 2 * e + which;
+                    tr[nf] = f.c.w;
+                    fshape[nf] = f.shape;
+                    fdist[nf] = f.dist;
+                    fcx[nf] = f.cp.x;
+                    fcy[nf] = f.cp.y;
+                    fseg[nf] = f.seg;
+                    ft[nf] = f.t;
+                    fwithin[nf] = f.within;
+                } else {
+                    overflow = true;
+                }
+                ++nf;
+            }
+        }
+    }
+    if (overflow) {
+        atomicOr(status, ST_FRAGMENT_OVERFLOW);
+        nf = 0;
+    }
+    const bool active = valid && !overflow;
+    float4 ret = bg;
+    float dcr = dcol.x, dcg = dcol.y, dcb = dcol.z, dca = dcol.w;
+    if (nf > 0) {
+        float fa = acc.w, fr = acc.x, fg = acc.y, fb = acc.z;
+        if (fa > 1.0e-6f) {
+            float s = 1.0f / fa;
+            fr = fr * s;
+            fg = fg * s;
+            fb = fb * s;
+            float dfr = dcr, dfg = dcg, dfb = dcb;
+            dcr = dcr * s;
+            dcg = dcg * s;
+            dcb = dcb * s;
+            dca -= (dfr * fr + dfg * fg + dfb * fb) / fa;
+        }
+        ret = make_float4(fr, fg, fb, fa);
+        float run = 1.0f;
+        for (int i = nf - 1; i >= 0; --i) {
+            float a = tr[i];
+            tr[i] = run;
+            run = run * (1.0f - a);
+        }
+        dcol = make_float4(dcr * run, dcg * run, dcb * run, dca * run);
+    }
+    if (active && S.bg_image) {
+        if (G.d_background_image) {
+            float* b = G.d_background_image + 4 * (size_t)pixel;
+            add_if(b + 0, dcol.x);
+            add_if(b + 1, dcol.y);
+            add_if(b + 2, dcol.z);
+            add_if(b + 3, dcol.w);
+        }
+        dcol = make_float4(0, 0, 0, 0);
+    }
+    if (!active) dcol = make_float4(0, 0, 0, 0);
+    // pass 3: compositing adjoint with coverage and distance derivatives
+    int cur = 0;
+    float4 prev = bg;
+    for (int e = 0; e < n; ++e) {
+        const int g = __ldg(&list[e]);
+        const int4 gi = __ldg(&S.g_info[g]);
+#pragma unroll
+        for (int which = 0; which < 2; ++which) {
+            const int p = which == 0 ? gi.y : gi.x;
+            if (p < 0) continue;
+            const bool has = cur < nf && code[cur] == 2 * e + which;
+            if (!__any_sync(0xffffffffu, has)) continue;
+            float4 dv = make_float4(0, 0, 0, 0);
+            int i = cur;
+            float w = 0.0f, d_w = 0.0f;
+            if (has) {
+                float4 c = paint_color(S, p, pt);
+                const float d = fdist[i];
+                if (which == 0) {
+                    const float sw = __ldg(&S.s_stroke[fshape[i]]);
+                    w = smoothstep1(fabsf(d) + sw) - smoothstep1(fabsf(d) - sw);
+                } else {
+                    w = smoothstep1(d);
+                }
+                c.w *= w;
+                const float T = tr[i];
+                const float r_ = dcr * T, g_ = dcg * T, b_ = dcb * T, a_ = dca * T;
+                float d_alpha = a_ * (1.0f - prev.w);
+                d_alpha += r_ * (c.x - prev.x) + g_ * (c.y - prev.y) + b_ * (c.z - prev.z);
+                if (w != 0.0f) {
+                    d_w = w > 0.0f ? (c.w / w) * d_alpha : 0.0f;
+                    dv = make_float4(r_ * c.w, g_ * c.w, b_ * c.w, d_alpha * w);
+                }
+                over(prev, c);
+                ++cur;
+            }
+            const int kind = __ldg(&S.paint_info[p].x);
+            if (kind == P_SOLID) {
+                float s0 = warp_sum(dv.x), s1 = warp_sum(dv.y), s2 = warp_sum(dv.z), s3 = warp_sum(dv.w);
+                if (lane == 0) {
+                    float* d = G.d_paint_params + 4 * p;
+                    add_if(d + 0, s0);
+                    add_if(d + 1, s1);
+                    add_if(d + 2, s2);
+                    add_if(d + 3, s3);
+                }
+            }
+            if (!has || w == 0.0f) continue;
+            float2 tdelta = make_float2(0.0f, 0.0f);
+            if (kind != P_SOLID) d_gradient_paint(S, G, p, pt, dv, &tdelta);
+            const float d = fdist[i];
+            float d_d;
+            bool geom = true;
+            if (which == 0) {
+                const float sw = __ldg(&S.s_stroke[fshape[i]]);
+                const float ap = fabsf(d) + sw, am = fabsf(d) - sw;
+                const float dap = d_smoothstep(ap, d_w), dam = -d_smoothstep(am, d_w);
+                d_d = dap + dam;
+                if (d < 0.0f) d_d = -d_d;
+                add_if(G.d_shape_stroke_width + fshape[i], dap - dam);
+            } else {
+                d_d = d_smoothstep(d, d_w);
+                if (d < 0.0f) d_d = -d_d;
+                geom = fwithin[i];
+            }
+            if (fabsf(d_d) > 1.0e-10f && geom) {
+                float2 dpt = d_compute_distance(S, G, g, fshape[i], pt, make_float2(fcx[i], fcy[i]), fseg[i], ft[i],
+                                                d_d);
+                tdelta.x += -dpt.x;
+                tdelta.y += -dpt.y;
+            }
+            if (G.d_translation) {
+                add_if(G.d_translation + 2 * (size_t)pixel, tdelta.x);
+                add_if(G.d_translation + 2 * (size_t)pixel + 1, tdelta.y);
+            }
+        }
+    }
+    float dradius = active ? filter_radius_adjoint(S, d_render, wsum, ps, ret) : 0.0f;
+    float v[5] = {dcol.x, dcol.y, dcol.z, dcol.w, dradius};
+#pragma unroll
+    for (int k = 0; k < 5; ++k) v[k] = warp_sum(v[k]);
+    if (lane == 0)
+        for (int k = 0; k < 5; ++k) red[wid][k] = v[k];
+    __syncthreads();
+    if (threadIdx.x < 5) {
+        float s = 0.0f;
+        for (int w2 = 0; w2 < 8; ++w2) s += red[w2][threadIdx.x];
+        if (threadIdx.x < 4)
+            add_if(G.d_background + threadIdx.x, s);
+        else
+            add_if(G.d_filter_radius, s);
+    }
+}
+
+int launch_forward_prefilter(const DevScene& S, const SampleParams& sp, float* accum, float* wsum, unsigned* status,
+                             cudaStream_t stream) {
+    const int hw = TILE + 2 * S.filter_ri;
+    size_t smem = S.filter_ri <= MAX_SMEM_RI ? (size_t)hw * hw * 5 * sizeof(float) : 0;
+    dim3 grid(S.tiles_x * S.tiles_y, sp.sxn * sp.syn);
+    k_forward_prefilter<<<grid, 256, smem, stream>>>(S, sp, accum, wsum, status);
+    return 1;
+}
+int launch_interior_prefilter(const DevScene& S, const SampleParams& sp, const float* d_render, const float* wsum,
+                              const GradPtrs& G, unsigned* status, cudaStream_t stream) {
+    dim3 grid(S.tiles_x * S.tiles_y, sp.sxn * sp.syn);
+    k_interior_prefilter<<<grid, 256, 0, stream>>>(S, sp, d_render, wsum, G, status);
+    return 1;
+}
+
+}  // namespace dvgb

@@ -308,8 +308,8 @@ dvg_status prepare_scene(const dvg_scene_desc* d, HostScene* out, std::string* e
                 for (size_t n = 0; n < bo.bounds.size(); ++n) {
                     const Box& b = bo.bounds[n];
                     h.pn_bounds.insert(h.pn_bounds.end(), {b.x0, b.y0, b.x1, b.y1});
-                    h.pn_meta.insert(h.pn_meta.end(),
-                                     {node_off + skip[n], leaf_base + bo.start[n], bo.count[n], 0});
+                    h.pn_meta.insert(h.pn_meta.end(), {node_off + skip[n], leaf_base + bo.start[n], bo.count[n],
+                                                       bo.right[n] >= 0 ? node_off + bo.right[n] : -1});
                 }
                 node_cnt = (int32_t)bo.bounds.size();
                 for (const Seg& sg : segs) {
@@ -418,7 +418,8 @@ dvg_status prepare_scene(const dvg_scene_desc* d, HostScene* out, std::string* e
             for (size_t n = 0; n < bo.bounds.size(); ++n) {
                 const Box& b = bo.bounds[n];
                 h.gn_bounds.insert(h.gn_bounds.end(), {b.x0, b.y0, b.x1, b.y1});
-                h.gn_meta.insert(h.gn_meta.end(), {node_off + skip[n], leaf_base + bo.start[n], bo.count[n], 0});
+                h.gn_meta.insert(h.gn_meta.end(), {node_off + skip[n], leaf_base + bo.start[n], bo.count[n],
+                                                   bo.right[n] >= 0 ? node_off + bo.right[n] : -1});
             }
             node_cnt = (int32_t)bo.bounds.size();
             root = bo.bounds[0];

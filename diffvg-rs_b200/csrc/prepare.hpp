@@ -38,7 +38,8 @@ struct HostScene {
     std::vector<int32_t> g_shape_list; // flat ShapeGroup::shape_indices (valid ids only)
     // group BVH nodes (global), preorder with skip links
     std::vector<float> gn_bounds;      // 4 per node
-    std::vector<int32_t> gn_meta;      // 4 per node: skip (absolute), leaf start (into gl_shapes), count, 0
+    std::vector<int32_t> gn_meta;      // 4 per node: skip, leaf start (into gl_shapes), count, right child
+                                       // (absolute indices; left child of an inner node = node + 1; -1 none)
     std::vector<int32_t> gl_shapes;    // leaf order: shape id, per entry
 
     // shapes
@@ -52,7 +53,7 @@ struct HostScene {
     std::vector<int32_t> p_info;       // 8 per path: seg off, seg count, node off, node count,
                                        //             point off, point count, ctrl off, flags
     std::vector<float> pn_bounds;      // 4 per path-BVH node
-    std::vector<int32_t> pn_meta;      // 4 per node: skip (absolute), leaf start (into pl_segs), count, 0
+    std::vector<int32_t> pn_meta;      // 4 per node: skip, leaf start (into pl_segs), count, right child
     std::vector<int32_t> pl_segs;      // leaf order: global segment index
     std::vector<float> seg_p;          // 8 per segment: p0..p3
     std::vector<float> seg_r;          // 4 per segment: r0..r3

@@ -2051,6 +2051,606 @@ static V4 sample_color(const Scene& sc, const SceneBvh& bvh, V2 screen_pt, const
     return V4{fr, fg, fb, final_alpha};
 }
 
+// ---------------------------------------------------------------- prefiltered sampling (backward/sampling.rs:227-482)
+struct PathInfo {  // types.rs:33-41
+    bool valid = false;
+    size_t base_point_id = 0, point_id = 0;
+    float t = 0.0f;
+};
+static size_t path_point_id(const PathG& p, size_t base_point_id) {  // backward/distance.rs:35-47
+    size_t point_id = 0;
+    size_t count = std::min(base_point_id, p.ncp.size());
+    for (size_t i = 0; i < count; ++i) {
+        uint8_t c = p.ncp[i];
+        point_id += c == 0 ? 1 : (c == 1 ? 2 : (c == 2 ? 3 : 0));
+    }
+    return point_id;
+}
+static PathInfo path_info_from_closest(const Scene& sc, size_t shape_index, const PathHit& h) {  // distance.rs:14-32
+    PathInfo pi;
+    if (sc.shapes[shape_index].kind != DVG_SHAPE_PATH || !h.valid) return pi;
+    pi.valid = true;
+    pi.base_point_id = h.segment_index;
+    pi.point_id = path_point_id(sc.shapes[shape_index].path, h.segment_index);
+    pi.t = h.t;
+    return pi;
+}
+static float d_smoothstep(float d, float d_ret) {  // backward/math.rs:15-22
+    if (d < -1.0f || d > 1.0f) return 0.0f;
+    float t = (d + 1.0f) * 0.5f;
+    float d_t = d_ret * (6.0f * t - 6.0f * t * t);
+    return d_t * 0.5f;
+}
+static void d_distance(V2 a, V2 b, float d_out, V2* d_a, V2* d_b) {  // math.rs:25-30
+    V2 d = d_length(b - a, d_out);
+    *d_a -= d;
+    *d_b += d;
+}
+static V2 d_normalize(V2 v, V2 d_n) {  // math.rs:53-63
+    float l = length(v);
+    if (l == 0.0f) return mk(0, 0);
+    V2 n = v / l;
+    V2 d_v = d_n / l;
+    float d_l = -dot(d_n, n) / l;
+    d_v += d_length(v, d_l);
+    return d_v;
+}
+static M3 scale3(const M3& m, float s) {
+    M3 o = m;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) o.m[r][c] *= s;
+    return o;
+}
+static M3 add3(const M3& a, const M3& b) {
+    M3 o = a;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) o.m[r][c] += b.m[r][c];
+    return o;
+}
+static void add_shape_transform(Grads& g, size_t shape_id, const M3& m) {
+    float* ds = &g.shape_transform[9 * shape_id];
+    for (int i = 0; i < 9; ++i) ds[i] = ds[i] + m.m[i / 3][i % 3];
+}
+static void add_group_transform(Grads& g, size_t group_id, const M3& m) {
+    float* dg = &g.group_transform[9 * group_id];
+    for (int i = 0; i < 9; ++i) dg[i] = dg[i] + m.m[i / 3][i % 3];
+}
+static void d_closest_point_path(const Shape& s, size_t shape_id, V2 pt, V2 d_cp, const PathInfo& info, Grads& g,
+                                 V2* d_pt) {  // backward/distance.rs:190-394
+    const PathG& path = s.path;
+    size_t bpid = info.base_point_id, pid = info.point_id;
+    float min_t = info.t;
+    size_t np = path.pts.size();
+    if (np == 0) return;
+    auto get_point = [&](size_t idx) { return path.closed ? path.pts[idx % np] : path.pts[std::min(idx, np - 1)]; };
+    auto add_point = [&](size_t idx, V2 delta) {
+        size_t index = path.closed ? idx % np : idx;
+        if (index < np) {
+            g.points[2 * (path.point_base + index)] += delta.x;
+            g.points[2 * (path.point_base + index) + 1] += delta.y;
+        }
+    };
+    uint8_t nc = bpid < path.ncp.size() ? path.ncp[bpid] : 0;
+    if (nc == 0) {
+        size_t i0 = pid, i1 = (pid + 1) % np;
+        V2 p0 = get_point(i0), p1 = get_point(i1);
+        float t = dot(pt - p0, p1 - p0) / dot(p1 - p0, p1 - p0);
+        if (t < 0.0f) {
+            add_point(i0, d_cp);
+        } else if (t > 1.0f) {
+            add_point(i1, d_cp);
+        } else {
+            add_point(i0, d_cp * (1.0f - t));
+            add_point(i1, d_cp * t);
+        }
+    } else if (nc == 1) {
+        size_t i0 = pid, i1 = pid + 1, i2 = (pid + 2) % np;
+        V2 p0 = get_point(i0), p1 = get_point(i1), p2 = get_point(i2);
+        float t = min_t;
+        V2 d_p0 = mk(0, 0), d_p1 = mk(0, 0), d_p2 = mk(0, 0);
+        if (t == 0.0f) {
+            d_p0 += d_cp;
+        } else if (t == 1.0f) {
+            d_p2 += d_cp;
+        } else {
+            V2 a = p0 - p1 * 2.0f + p2;
+            V2 b = p1 - p0;
+            float A = dot(a, a);
+            float B = 3.0f * dot(a, b);
+            float C = 2.0f * dot(b, b) + dot(a, p0 - pt);
+            float tt = 1.0f - t;
+            V2 d_p = d_cp;
+            float d_tt = 2.0f * tt * dot(d_p, p0) + 2.0f * t * dot(d_p, p1);
+            float d_t = -d_tt + 2.0f * tt * dot(d_p, p1) + 2.0f * t * dot(d_p, p2);
+            d_p0 += d_p * (tt * tt);
+            d_p1 += d_p * (2.0f * tt * t);
+            d_p2 += d_p * (t * t);
+            float poly_deriv_t = 3.0f * A * t * t + 2.0f * B * t + C;
+            if (std::fabs(poly_deriv_t) > 1.0e-6f) {
+                float d_A = -(d_t / poly_deriv_t) * t * t * t;
+                float d_B = -(d_t / poly_deriv_t) * t * t;
+                float d_C = -(d_t / poly_deriv_t) * t;
+                float d_D = -(d_t / poly_deriv_t);
+                d_p0 += a * (2.0f * d_A) + (b - a) * (3.0f * d_B) + (b * -4.0f) * d_C + (p0 - pt + a) * d_C +
+                        (b - (p0 - pt)) * (2.0f * d_D);
+                d_p1 += a * (-4.0f * d_A) + (a + b * -2.0f) * (3.0f * d_B) + (b * 4.0f) * d_C +
+                        (p0 - pt) * (-2.0f * d_C) + (p0 - pt) * d_D;
+                d_p2 += a * (2.0f * d_A) + b * (3.0f * d_B) + (p0 - pt) * d_C;
+                *d_pt += a * (-d_C) + b * d_D;
+            }
+        }
+        add_point(i0, d_p0);
+        add_point(i1, d_p1);
+        add_point(i2, d_p2);
+    } else if (nc == 2) {
+        size_t i0 = pid, i1 = pid + 1, i2 = pid + 2, i3 = (pid + 3) % np;
+        V2 p0 = get_point(i0), p1 = get_point(i1), p2 = get_point(i2), p3 = get_point(i3);
+        float t = min_t;
+        V2 d_p0 = mk(0, 0), d_p1 = mk(0, 0), d_p2 = mk(0, 0), d_p3 = mk(0, 0);
+        if (t == 0.0f) {
+            d_p0 += d_cp;
+        } else if (t == 1.0f) {
+            d_p3 += d_cp;
+        } else {
+            V2 a = p0 * -1.0f + p1 * 3.0f + p2 * -3.0f + p3;
+            V2 b = p0 * 3.0f + p1 * -6.0f + p2 * 3.0f;
+            V2 c = p0 * -3.0f + p1 * 3.0f;
+            float A = 3.0f * dot(a, a);
+            if (std::fabs(A) < 1.0e-10f) return;
+            float B = 5.0f * dot(a, b);
+            float C = 4.0f * dot(a, c) + 2.0f * dot(b, b);
+            float D = 3.0f * (dot(b, c) + dot(a, p0 - pt));
+            float E = dot(c, c) + 2.0f * dot(p0 - pt, b);
+            float F = dot(p0 - pt, c);
+            B = B / A;
+            C = C / A;
+            D = D / A;
+            E = E / A;
+            F = F / A;
+            float tt = 1.0f - t;
+            V2 d_p = d_cp;
+            float d_tt = 3.0f * tt * tt * dot(d_p, p0) + 6.0f * tt * t * dot(d_p, p1) + 3.0f * t * t * dot(d_p, p2);
+            float d_t = -d_tt + 3.0f * tt * tt * dot(d_p, p1) + 6.0f * tt * t * dot(d_p, p2) +
+                        3.0f * t * t * dot(d_p, p3);
+            d_p0 += d_p * (tt * tt * tt);
+            d_p1 += d_p * (3.0f * tt * tt * t);
+            d_p2 += d_p * (3.0f * tt * t * t);
+            d_p3 += d_p * (t * t * t);
+            float pd = 5.0f * t * t * t * t + 4.0f * B * t * t * t + 3.0f * C * t * t + 2.0f * D * t + E;
+            if (std::fabs(pd) > 1.0e-10f) {
+                float d_B = -(d_t / pd) * t * t * t * t;
+                float d_C = -(d_t / pd) * t * t * t;
+                float d_D = -(d_t / pd) * t * t;
+                float d_E = -(d_t / pd) * t;
+                float d_F = -(d_t / pd);
+                float d_A = -d_B * B / A - d_C * C / A - d_D * D / A - d_E * E / A - d_F * F / A;
+                d_B /= A;
+                d_C /= A;
+                d_D /= A;
+                d_E /= A;
+                d_F /= A;
+                d_p0 += a * (3.0f * -1.0f * 2.0f * d_A);
+                d_p1 += a * (3.0f * 3.0f * 2.0f * d_A);
+                d_p2 += a * (3.0f * -3.0f * 2.0f * d_A);
+                d_p3 += a * (3.0f * 1.0f * 2.0f * d_A);
+                d_p0 += (b * -1.0f + a * 3.0f) * (5.0f * d_B);
+                d_p1 += (b * 3.0f + a * -6.0f) * (5.0f * d_B);
+                d_p2 += (b * -3.0f + a * 3.0f) * (5.0f * d_B);
+                d_p3 += b * (5.0f * d_B);
+                d_p0 += (c * -1.0f + a * -3.0f) * (4.0f * d_C) + b * (3.0f * 2.0f * d_C);
+                d_p1 += (c * 3.0f + a * 3.0f) * (4.0f * d_C) + b * (-6.0f * 2.0f * d_C);
+                d_p2 += c * (-3.0f * d_C * 4.0f) + b * (3.0f * 2.0f * d_C);
+                d_p3 += c * (4.0f * d_C);
+                d_p0 += (c * 3.0f + b * -3.0f) * (3.0f * d_D) + (a - (p0 - pt)) * (3.0f * d_D);
+                d_p1 += (c * -6.0f + b * 3.0f) * (3.0f * d_D) + (p0 - pt) * (3.0f * 3.0f * d_D);
+                d_p2 += c * (3.0f * 3.0f * d_D) + (p0 - pt) * (-3.0f * 3.0f * d_D);
+                *d_pt += a * (-1.0f * 3.0f * d_D);
+                d_p0 += c * (-3.0f * 2.0f * d_E) + (b + (p0 - pt) * 3.0f) * (2.0f * d_E);
+                d_p1 += c * (3.0f * 2.0f * d_E) + (p0 - pt) * (-6.0f * 2.0f * d_E);
+                d_p2 += (p0 - pt) * (3.0f * 2.0f * d_E);
+                *d_pt += b * (-1.0f * 2.0f * d_E);
+                d_p0 += c * d_F + (p0 - pt) * (-3.0f * d_F);
+                d_p1 += (p0 - pt) * (3.0f * d_F);
+                *d_pt += c * (-1.0f * d_F);
+            }
+        }
+        add_point(i0, d_p0);
+        add_point(i1, d_p1);
+        add_point(i2, d_p2);
+        add_point(i3, d_p3);
+    }
+    (void)shape_id;
+}
+static void d_closest_point_rect(V2 mn, V2 mx, V2 pt, V2 d_cp, V2* d_min, V2* d_max, V2* d_pt) {  // distance.rs:397-476
+    auto dist_to_seg = [&](V2 p0, V2 p1) {
+        float t = dot(pt - p0, p1 - p0) / dot(p1 - p0, p1 - p0);
+        if (t < 0.0f) return length(p0 - pt);
+        if (t > 1.0f) return length(p1 - pt);
+        return length(p0 + (p1 - p0) * t - pt);
+    };
+    V2 lt = mn, rt = mk(mx.x, mn.y), lb = mk(mn.x, mx.y), rb = mx;
+    int min_id = 0;
+    float min_dist = dist_to_seg(lt, lb);
+    float top = dist_to_seg(lt, rt), right = dist_to_seg(rt, rb), bottom = dist_to_seg(lb, rb);
+    if (top < min_dist) {
+        min_dist = top;
+        min_id = 1;
+    }
+    if (right < min_dist) {
+        min_dist = right;
+        min_id = 2;
+    }
+    if (bottom < min_dist) {
+        min_dist = bottom;
+        min_id = 3;
+    }
+    auto update = [&](V2 p0, V2 p1, V2* d_p0, V2* d_p1) {
+        float t = dot(pt - p0, p1 - p0) / dot(p1 - p0, p1 - p0);
+        if (t < 0.0f) {
+            *d_p0 += d_cp;
+        } else if (t > 1.0f) {
+            *d_p1 += d_cp;
+        } else {
+            V2 d_p = d_cp;
+            *d_p0 += d_p * (1.0f - t);
+            *d_p1 += d_p * t;
+            float d_t = dot(d_p, p1 - p0);
+            float denom = dot(p1 - p0, p1 - p0);
+            float d_num = d_t / denom;
+            float d_den = d_t * (-t) / denom;
+            *d_pt += (p1 - p0) * d_num;
+            *d_p1 += (pt - p0) * d_num;
+            *d_p0 += (p0 - p1 + p0 - pt) * d_num;
+            *d_p1 += (p1 - p0) * (2.0f * d_den);
+            *d_p0 += (p0 - p1) * (2.0f * d_den);
+        }
+    };
+    V2 d_lt = mk(0, 0), d_rt = mk(0, 0), d_lb = mk(0, 0), d_rb = mk(0, 0);
+    if (min_id == 0)
+        update(lt, lb, &d_lt, &d_lb);
+    else if (min_id == 1)
+        update(lt, rt, &d_lt, &d_rt);
+    else if (min_id == 2)
+        update(rt, rb, &d_rt, &d_rb);
+    else
+        update(lb, rb, &d_lb, &d_rb);
+    *d_min += d_lt;
+    d_max->x += d_rt.x;
+    d_min->y += d_rt.y;
+    d_min->x += d_lb.x;
+    d_max->y += d_lb.y;
+    *d_max += d_rb;
+}
+static void d_closest_point_ellipse(V2 center, V2 radius, V2 pt, V2 d_cp, V2* d_center, V2* d_radius,
+                                    V2* d_pt) {  // distance.rs:479-561
+    float rx = std::fabs(radius.x), ry = std::fabs(radius.y);
+    const float eps = 1.0e-6f;
+    V2 local = pt - center;
+    if (rx < eps && ry < eps) {
+        *d_center += d_cp;
+        return;
+    }
+    if (rx < eps) {
+        float hit = (local.y >= -ry && local.y <= ry) ? 1.0f : 0.0f;
+        *d_center += mk(d_cp.x, d_cp.y);
+        d_pt->y += d_cp.y * hit;
+        if (local.y > ry)
+            d_radius->y += d_cp.y;
+        else if (local.y < -ry)
+            d_radius->y -= d_cp.y;
+        return;
+    }
+    if (ry < eps) {
+        float hit = (local.x >= -rx && local.x <= rx) ? 1.0f : 0.0f;
+        *d_center += mk(d_cp.x, d_cp.y);
+        d_pt->x += d_cp.x * hit;
+        if (local.x > rx)
+            d_radius->x += d_cp.x;
+        else if (local.x < -rx)
+            d_radius->x -= d_cp.x;
+        return;
+    }
+    float sign_x = local.x < 0.0f ? -1.0f : 1.0f, sign_y = local.y < 0.0f ? -1.0f : 1.0f;
+    float x = std::fabs(local.x), y = std::fabs(local.y);
+    float t = std::atan2(y * rx, x * ry);
+    float g_t = 0.0f;
+    for (int i = 0; i < 20; ++i) {
+        float sn = std::sin(t), cs = std::cos(t);
+        float gg = rx * x * sn - ry * y * cs + (ry * ry - rx * rx) * sn * cs;
+        g_t = rx * x * cs + ry * y * sn + (ry * ry - rx * rx) * (cs * cs - sn * sn);
+        if (std::fabs(g_t) < 1.0e-12f) break;
+        float next = clampf(t - gg / g_t, 0.0f, FRAC_PI_2_F);
+        if (std::fabs(next - t) < 1.0e-6f) {
+            t = next;
+            break;
+        }
+        t = next;
+    }
+    float sn = std::sin(t), cs = std::cos(t);
+    float d_t = 0.0f;
+    d_radius->x += d_cp.x * sign_x * cs;
+    d_t += d_cp.x * sign_x * (-rx * sn);
+    d_radius->y += d_cp.y * sign_y * sn;
+    d_t += d_cp.y * sign_y * (ry * cs);
+    float g_a = x * sn - 2.0f * rx * sn * cs;
+    float g_b = -y * cs + 2.0f * ry * sn * cs;
+    float g_x = rx * sn;
+    float g_y = -ry * cs;
+    if (std::fabs(g_t) > 1.0e-12f) {
+        float inv = -d_t / g_t;
+        d_radius->x += inv * g_a;
+        d_radius->y += inv * g_b;
+        float d_x = inv * g_x, d_y = inv * g_y;
+        d_pt->x += d_x * sign_x;
+        d_pt->y += d_y * sign_y;
+        d_center->x -= d_x * sign_x;
+        d_center->y -= d_y * sign_y;
+    }
+}
+static void d_closest_point(const Shape& s, size_t shape_id, V2 pt, V2 d_cp, const PathInfo& pinfo, Grads& g,
+                            V2* d_pt) {  // distance.rs:139-187
+    float* dp = &g.shape_params[4 * shape_id];
+    if (s.kind == DVG_SHAPE_CIRCLE) {
+        V2 center = mk(s.prm[0], s.prm[1]);
+        float radius = s.prm[2];
+        V2 v = pt - center;
+        V2 n = normalize(v);
+        V2 d_center = d_cp;
+        float d_radius = dot(d_cp, n);
+        V2 d_n = d_cp * radius;
+        V2 d_v = d_normalize(v, d_n);
+        d_center -= d_v;
+        *d_pt += d_v;
+        dp[0] += d_center.x;
+        dp[1] += d_center.y;
+        dp[2] += d_radius;
+    } else if (s.kind == DVG_SHAPE_ELLIPSE) {
+        V2 dc = mk(0, 0), dr = mk(0, 0);
+        d_closest_point_ellipse(mk(s.prm[0], s.prm[1]), mk(s.prm[2], s.prm[3]), pt, d_cp, &dc, &dr, d_pt);
+        dp[0] += dc.x;
+        dp[1] += dc.y;
+        dp[2] += dr.x;
+        dp[3] += dr.y;
+    } else if (s.kind == DVG_SHAPE_RECT) {
+        V2 dmn = mk(0, 0), dmx = mk(0, 0);
+        d_closest_point_rect(mk(s.prm[0], s.prm[1]), mk(s.prm[2], s.prm[3]), pt, d_cp, &dmn, &dmx, d_pt);
+        dp[0] += dmn.x;
+        dp[1] += dmn.y;
+        dp[2] += dmx.x;
+        dp[3] += dmx.y;
+    } else if (s.kind == DVG_SHAPE_PATH) {
+        if (!pinfo.valid) return;
+        d_closest_point_path(s, shape_id, pt, d_cp, pinfo, g, d_pt);
+    }
+}
+static V2 d_compute_distance(const Group& grp, size_t group_id, const Shape& s, size_t shape_id, V2 pt, V2 closest_pt,
+                             const PathInfo& pinfo, float d_dist, Grads& g) {  // distance.rs:50-136
+    if (length_sq(pt - closest_pt) < 1.0e-10f) return mk(0, 0);
+    V2 lpg = xform_pt(grp.c2s, pt);
+    V2 lcg = xform_pt(grp.c2s, closest_pt);
+    M3 shape_inv;
+    if (!inverse3(s.transform, &shape_inv)) shape_inv = identity3();
+    V2 lps = xform_pt(shape_inv, lpg);
+    V2 lcs = xform_pt(shape_inv, lcg);
+    V2 d_pt = mk(0, 0), d_closest = mk(0, 0);
+    d_distance(closest_pt, pt, d_dist, &d_closest, &d_pt);
+    M3 d_s2c = zero3();
+    V2 d_lcg = mk(0, 0);
+    d_xform_pt(grp.s2c, lcg, d_closest, &d_s2c, &d_lcg);
+    M3 d_st = zero3();
+    V2 d_lcs = mk(0, 0);
+    d_xform_pt(s.transform, lcs, d_lcg, &d_st, &d_lcs);
+    V2 d_lps = mk(0, 0);
+    d_closest_point(s, shape_id, lps, d_lcs, pinfo, g, &d_lps);
+    M3 d_sinv = zero3();
+    V2 d_lpg = mk(0, 0);
+    d_xform_pt(shape_inv, lpg, d_lps, &d_sinv, &d_lpg);
+    M3 d_c2s = zero3();
+    d_xform_pt(grp.c2s, pt, d_lpg, &d_c2s, &d_pt);
+    M3 tc2s = transpose3(grp.c2s);
+    M3 corr = mul3(mul3(scale3(tc2s, -1.0f), d_c2s), tc2s);
+    M3 dg = zero3();
+    dg = add3(dg, d_s2c);
+    dg = add3(dg, corr);
+    add_group_transform(g, group_id, dg);
+    M3 tsi = transpose3(shape_inv);
+    M3 corr_s = mul3(mul3(scale3(tsi, -1.0f), d_sinv), tsi);
+    M3 ds = zero3();
+    ds = add3(ds, corr_s);
+    ds = add3(ds, d_st);
+    add_shape_transform(g, shape_id, ds);
+    return d_pt;
+}
+struct PFrag {  // types.rs:118-136
+    float r, g, b, a;
+    size_t group_id, shape_id;
+    float distance;
+    V2 closest;
+    PathInfo pinfo;
+    bool within, is_stroke;
+};
+static void collect_prefiltered(const Scene& sc, const SceneBvh& bvh, V2 pt, std::vector<PFrag>& frags) {
+    frags.clear();
+    for (size_t gi = 0; gi < sc.groups.size(); ++gi) {
+        const Group& g = sc.groups[gi];
+        if (g.stroke >= 0) {
+            ClosestPoint hit;
+            if (compute_distance_bvh(sc, bvh, gi, pt, INF_F, &hit)) {
+                const Shape& shp = sc.shapes[hit.shape_index];
+                float d = hit.distance;
+                float w = smoothstep(std::fabs(d) + shp.stroke_width) - smoothstep(std::fabs(d) - shp.stroke_width);
+                if (w > 0.0f) {
+                    V4 c = paint_color(sc.paints[g.stroke], pt);
+                    c.w *= w;
+                    frags.push_back(PFrag{c.x, c.y, c.z, c.w, gi, hit.shape_index, d, hit.point,
+                                          path_info_from_closest(sc, hit.shape_index, hit.path), true, true});
+                }
+            }
+        }
+        if (g.fill >= 0) {
+            ClosestPoint hit;
+            bool have = compute_distance_bvh(sc, bvh, gi, pt, 1.0f, &hit);
+            bool inside = is_inside_bvh(sc, bvh, gi, pt);
+            if (have || inside) {
+                size_t shape_id = 0;
+                V2 cp = mk(0, 0);
+                PathInfo pinfo;
+                float d = 1.0f;
+                if (have) {
+                    shape_id = hit.shape_index;
+                    cp = hit.point;
+                    pinfo = path_info_from_closest(sc, hit.shape_index, hit.path);
+                    d = hit.distance;
+                }
+                if (!inside) d = -d;
+                float w = smoothstep(d);
+                if (w > 0.0f) {
+                    V4 c = paint_color(sc.paints[g.fill], pt);
+                    c.w *= w;
+                    frags.push_back(PFrag{c.x, c.y, c.z, c.w, gi, shape_id, d, cp, pinfo, have, false});
+                }
+            }
+        }
+    }
+}
+static V4 sample_color_prefiltered(const Scene& sc, const SceneBvh& bvh, V2 screen_pt, const V4* background,
+                                   const V4* d_color, Grads* grads, long translation_index, size_t pixel_index) {
+    V2 pt = mk(screen_pt.x * (float)sc.w, screen_pt.y * (float)sc.h);
+    std::vector<PFrag> frags;
+    collect_prefiltered(sc, bvh, pt, frags);
+    if (frags.empty()) {
+        if (background) {
+            if (d_color) accumulate_background_grad(sc, *grads, pixel_index, *d_color);
+            return *background;
+        }
+        return V4{0, 0, 0, 0};
+    }
+    std::vector<V4> accum(frags.size());
+    float pr = 0, pg = 0, pb = 0, pa = 0;
+    if (background) {
+        pr = background->x;
+        pg = background->y;
+        pb = background->z;
+        pa = background->w;
+    }
+    for (size_t i = 0; i < frags.size(); ++i) {
+        const PFrag& f = frags[i];
+        float br = pr * (1.0f - f.a) + f.r * f.a;
+        float bg = pg * (1.0f - f.a) + f.g * f.a;
+        float bb = pb * (1.0f - f.a) + f.b * f.a;
+        float ba = pa * (1.0f - f.a) + f.a;
+        accum[i] = V4{br, bg, bb, ba};
+        pr = br;
+        pg = bg;
+        pb = bb;
+        pa = ba;
+    }
+    V4 fc = accum.back();
+    float final_alpha = fc.w, fr = fc.x, fg = fc.y, fb = fc.z;
+    if (final_alpha > 1.0e-6f) {
+        float s = 1.0f / final_alpha;
+        fr = fr * s;
+        fg = fg * s;
+        fb = fb * s;
+    }
+    if (d_color) {
+        float dcr = d_color->x, dcg = d_color->y, dcb = d_color->z, dca = d_color->w;
+        if (final_alpha > 1.0e-6f) {
+            float dfr = dcr, dfg = dcg, dfb = dcb;
+            float s = 1.0f / final_alpha;
+            dcr = dcr * s;
+            dcg = dcg * s;
+            dcb = dcb * s;
+            dca -= (dfr * fr + dfg * fg + dfb * fb) / final_alpha;
+        }
+        for (size_t ii = frags.size(); ii-- > 0;) {
+            float prev_a, prev_r, prev_g, prev_b;
+            if (ii > 0) {
+                prev_a = accum[ii - 1].w;
+                prev_r = accum[ii - 1].x;
+                prev_g = accum[ii - 1].y;
+                prev_b = accum[ii - 1].z;
+            } else {
+                prev_a = background ? background->w : 0.0f;
+                prev_r = background ? background->x : 0.0f;
+                prev_g = background ? background->y : 0.0f;
+                prev_b = background ? background->z : 0.0f;
+            }
+            const PFrag& f = frags[ii];
+            float d_prev_alpha = dca * (1.0f - f.a);
+            float d_alpha_i = dca * (1.0f - prev_a);
+            d_alpha_i += dcr * (f.r - prev_r) + dcg * (f.g - prev_g) + dcb * (f.b - prev_b);
+            float s = 1.0f - f.a;
+            float dpr = dcr * s, dpg = dcg * s, dpb = dcb * s;
+            float dci_r = dcr * f.a, dci_g = dcg * f.a, dci_b = dcb * f.a;
+            const Group& grp = sc.groups[f.group_id];
+            if (f.is_stroke) {
+                const Shape& shp = sc.shapes[f.shape_id];
+                float d = f.distance;
+                float abs_plus = std::fabs(d) + shp.stroke_width, abs_minus = std::fabs(d) - shp.stroke_width;
+                float w = smoothstep(abs_plus) - smoothstep(abs_minus);
+                if (w != 0.0f) {
+                    float d_w = w > 0.0f ? (f.a / w) * d_alpha_i : 0.0f;
+                    float dai = d_alpha_i * w;
+                    V2 tdelta = mk(0, 0);
+                    if (grp.stroke >= 0) d_sample_paint(sc, grp.stroke, *grads, pt, V4{dci_r, dci_g, dci_b, dai}, &tdelta);
+                    accumulate_translation(*grads, translation_index, tdelta);
+                    float d_abs_plus = d_smoothstep(abs_plus, d_w);
+                    float d_abs_minus = -d_smoothstep(abs_minus, d_w);
+                    float d_d = d_abs_plus + d_abs_minus;
+                    if (d < 0.0f) d_d = -d_d;
+                    float d_sw = d_abs_plus - d_abs_minus;
+                    grads->stroke_width[f.shape_id] += d_sw;
+                    if (std::fabs(d_d) > 1.0e-10f) {
+                        V2 d_pt = d_compute_distance(grp, f.group_id, shp, f.shape_id, pt, f.closest, f.pinfo, d_d,
+                                                     *grads);
+                        accumulate_translation(*grads, translation_index, d_pt * -1.0f);
+                    }
+                }
+            } else {
+                float d = f.distance;
+                float w = smoothstep(d);
+                if (w != 0.0f) {
+                    float d_w = w > 0.0f ? (f.a / w) * d_alpha_i : 0.0f;
+                    float dai = d_alpha_i * w;
+                    V2 tdelta = mk(0, 0);
+                    if (grp.fill >= 0) d_sample_paint(sc, grp.fill, *grads, pt, V4{dci_r, dci_g, dci_b, dai}, &tdelta);
+                    accumulate_translation(*grads, translation_index, tdelta);
+                    float d_d = d_smoothstep(d, d_w);
+                    if (d < 0.0f) d_d = -d_d;
+                    if (std::fabs(d_d) > 1.0e-10f && f.within) {
+                        V2 d_pt = d_compute_distance(grp, f.group_id, sc.shapes[f.shape_id], f.shape_id, pt, f.closest,
+                                                     f.pinfo, d_d, *grads);
+                        accumulate_translation(*grads, translation_index, d_pt * -1.0f);
+                    }
+                }
+            }
+            dcr = dpr;
+            dcg = dpg;
+            dcb = dpb;
+            dca = d_prev_alpha;
+        }
+        if (background) accumulate_background_grad(sc, *grads, pixel_index, V4{dcr, dcg, dcb, dca});
+    }
+    return V4{fr, fg, fb, final_alpha};
+}
+static V4 eval_premultiplied_prefiltered(const Scene& sc, const SceneBvh& bvh, V2 pt, V4 background) {
+    std::vector<PFrag> frags;
+    collect_prefiltered(sc, bvh, pt, frags);
+    float pr = background.x, pg = background.y, pb = background.z, pa = background.w;
+    for (const PFrag& f : frags) {
+        float br = pr * (1.0f - f.a) + f.r * f.a;
+        float bg = pg * (1.0f - f.a) + f.g * f.a;
+        float bb = pb * (1.0f - f.a) + f.b * f.a;
+        float ba = pa * (1.0f - f.a) + f.a;
+        pr = br;
+        pg = bg;
+        pb = bb;
+        pa = ba;
+    }
+    return V4{pr, pg, pb, pa};
+}
+
 // Premultiplied colour at canvas point pt (the crate's eval_scene_tiled output,
 // src/gpu/kernels/forward.rs:1131-1290, with the CPU inside / within tests).
 static V4 eval_premultiplied(const Scene& sc, const SceneBvh& bvh, V2 pt, V4 background) {
@@ -2680,7 +3280,11 @@ static void interior_sample(const Scene& sc, const SceneBvh& bvh, const SampleSp
     V2 npt = mk(pt.x / (float)sc.w, pt.y / (float)sc.h);
     V4 bg = sample_background(sc, pixel_index);
     V4 dcol = gather_d_color(sc, d_render, wimg, pt);
-    V4 color = sample_color(sc, bvh, npt, &bg, &dcol, nullptr, &g, translation ? (long)pixel_index : -1, pixel_index);
+    V4 color = sp.prefilter
+                   ? sample_color_prefiltered(sc, bvh, npt, &bg, &dcol, &g, translation ? (long)pixel_index : -1,
+                                              pixel_index)
+                   : sample_color(sc, bvh, npt, &bg, &dcol, nullptr, &g, translation ? (long)pixel_index : -1,
+                                  pixel_index);
     accumulate_filter_gradient(sc, color, d_render, wimg, pt, &g.filter_radius);
 }
 
@@ -2812,7 +3416,8 @@ extern "C" int oracle_render(const dvg_scene_desc* desc, const dvg_render_option
         size_t pix;
         sample_position(sc, sp, idx, &pt, &pix);
         int x = (int)(pix % sc.w), y = (int)(pix / sc.w);
-        V4 c = eval_premultiplied(sc, bvh, pt, sample_background(sc, pix));
+        V4 c = sp.prefilter ? eval_premultiplied_prefiltered(sc, bvh, pt, sample_background(sc, pix))
+                            : eval_premultiplied(sc, bvh, pt, sample_background(sc, pix));
         for (int dy = -ri; dy <= ri; ++dy)
             for (int dx = -ri; dx <= ri; ++dx) {
                 int xx = x + dx, yy = y + dy;
@@ -3119,7 +3724,8 @@ extern "C" unsigned long long oracle_fwd_bwd_sample(const dvg_scene_desc* desc, 
             V2 pt;
             size_t pix;
             sample_position(sc, sp, idx, &pt, &pix);
-            V4 c = eval_premultiplied(sc, bvh, pt, sample_background(sc, pix));
+            V4 c = sp.prefilter ? eval_premultiplied_prefiltered(sc, bvh, pt, sample_background(sc, pix))
+                                : eval_premultiplied(sc, bvh, pt, sample_background(sc, pix));
             int x = (int)(pix % sc.w), y = (int)(pix / sc.w);
             for (int dy = -ri; dy <= ri; ++dy)
                 for (int dx = -ri; dx <= ri; ++dx) {

@@ -164,3 +164,33 @@ def test_backward_background_image(renderer):
     sc.background_image = np.random.default_rng(1).uniform(0, 1, (32, 32, 4)).astype(np.float32)
     gpu, ref = _backward_case(renderer, sc, synth.plain_options())
     _grad_check(gpu, ref)
+
+
+# ---------------------------------------------------------------- prefiltering (the crate's default mode)
+def _prefilter_opts(n=2, seed=0):
+    return RenderOptions(samples_x=n, samples_y=n, seed=seed, jitter=True, use_prefiltering=True)
+
+
+def test_render_prefilter_matches_oracle(renderer):
+    for sc in (synth.plain_scene(1, 48, 48, 6), _primitives_scene(),
+               synth.mixed_scene(6, 96, 96, scale=0.1, size_scale=0.25)):
+        opts = _prefilter_opts()
+        assert _img_err(renderer.render(sc, opts).pixels, orc.render(sc, opts)) <= IMG_TOL
+
+
+def test_backward_prefilter_plain_matches_oracle(renderer):
+    sc = synth.plain_scene(2, 40, 40, 5)
+    gpu, ref = _backward_case(renderer, sc, _prefilter_opts())
+    _grad_check(gpu, ref)
+
+
+def test_backward_prefilter_primitives_matches_oracle(renderer):
+    sc = _primitives_scene()
+    gpu, ref = _backward_case(renderer, sc, _prefilter_opts(), BackwardOptions(compute_translation=True))
+    _grad_check(gpu, ref)
+
+
+def test_backward_prefilter_mixed_matches_oracle(renderer):
+    sc = synth.mixed_scene(7, 80, 80, scale=0.08, size_scale=0.25)
+    gpu, ref = _backward_case(renderer, sc, _prefilter_opts())
+    _grad_check(gpu, ref)
