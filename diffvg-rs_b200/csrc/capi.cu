@@ -785,3 +785,229 @@ extern "C" dvg_status dvg_render_device_noalloc(dvg_context* ctx, dvg_scene* sce
     CK(cudaGetLastError());
     return DVG_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Batches: many uploaded scenes stepped together (forward + L2 + backward), one
+// kernel launch per stage for all scenes, optionally replayed as one CUDA graph.
+struct dvg_batch {
+    dvg_context* ctx = nullptr;
+    std::vector<dvg_scene*> scenes;
+    dvg_render_options opts{};
+    dvg_backward_options bopts{};
+    std::vector<BatchEntry> host_entries;
+    std::vector<size_t> pix_off;      // float offset of each scene's 4-channel image region
+    std::vector<size_t> wpix_off;     // float offset of each scene's 1-channel region
+    std::vector<size_t> grad_base;    // float offset of each scene's gradient block
+    size_t total_pix4 = 0, total_pix = 0, total_grads = 0, max_pixels = 0;
+    int items = 0, total_tiles = 0, max_ri = 0;
+    uint64_t total_bsamples = 0;
+    DevBuf entries, item_scene, accum, wsum, image, target, d_render, loss, grads, bsamples, bkey, border, bcounts;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t steps = 0;
+};
+
+namespace {
+dvg_status batch_enqueue(dvg_batch* b) {
+    dvg_context* ctx = b->ctx;
+    const int n = (int)b->scenes.size();
+    const BatchEntry* B = b->entries.as<BatchEntry>();
+    CK(cudaMemsetAsync(b->accum.ptr, 0, b->total_pix4 * sizeof(float), ctx->stream));
+    CK(cudaMemsetAsync(b->wsum.ptr, 0, b->total_pix * sizeof(float), ctx->stream));
+    CK(cudaMemsetAsync(b->loss.ptr, 0, (size_t)n * sizeof(float), ctx->stream));
+    CK(cudaMemsetAsync(b->grads.ptr, 0, b->total_grads * sizeof(float), ctx->stream));
+    const bool pre = b->opts.use_prefiltering != 0;
+    if (pre)
+        ctx->launches += launch_forward_prefilter_batch(B, b->item_scene.as<int>(), b->items, b->max_ri, ctx->status,
+                                                        ctx->stream);
+    else
+        ctx->launches += launch_forward_batch(B, b->item_scene.as<int>(), b->items, b->max_ri, ctx->stream);
+    ctx->launches += launch_pixels_batch(B, n, b->max_pixels, 0, ctx->stream);
+    ctx->launches += launch_pixels_batch(B, n, b->max_pixels, 1, ctx->stream);
+    if (pre)
+        ctx->launches += launch_interior_prefilter_batch(B, b->item_scene.as<int>(), b->items, ctx->status, ctx->stream);
+    else
+        ctx->launches += launch_interior_batch(B, b->item_scene.as<int>(), b->items, ctx->status, ctx->stream);
+    if (!pre)
+        ctx->launches += launch_boundary_batch(B, n, b->total_bsamples, b->total_tiles, b->bsamples.as<BSample>(),
+                                               b->bkey.as<int>(), b->bcounts.as<int>(), b->border.as<int>(),
+                                               ctx->stream);
+    ctx->launches += launch_pixels_batch(B, n, b->max_pixels, 2, ctx->stream);
+    CK(cudaGetLastError());
+    return DVG_OK;
+}
+}  // namespace
+
+extern "C" dvg_status dvg_batch_create(dvg_context* ctx, dvg_scene* const* scenes, uint32_t count,
+                                       const dvg_render_options* opts, const dvg_backward_options* bopts,
+                                       dvg_batch** out) {
+    if (!ctx || !scenes || !opts || !out || count == 0) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    dvg_status st = check_options(opts);
+    if (st != DVG_OK) return st;
+    CK(cudaSetDevice(ctx->device));
+    std::unique_ptr<dvg_batch> b(new dvg_batch());
+    b->ctx = ctx;
+    b->opts = *opts;
+    if (bopts) b->bopts = *bopts;
+    else {
+        b->bopts.boundary_seed_from_options = 1;
+    }
+    const SampleParams sp = sample_params(opts);
+    std::vector<int> item_scene;
+    for (uint32_t i = 0; i < count; ++i) {
+        dvg_scene* sc = scenes[i];
+        if (!sc || sc->ctx != ctx) return fail(DVG_ERR_INVALID_ARGUMENT, "batch scene is null or from another context");
+        const DevScene& S = sc->dev;
+        const size_t npix = (size_t)S.width * S.height;
+        if (npix == 0 || S.num_groups == 0)
+            return fail(DVG_ERR_INVALID_ARGUMENT, "batch scenes need a non-empty canvas and at least one group");
+        b->scenes.push_back(sc);
+        b->pix_off.push_back(b->total_pix4);
+        b->wpix_off.push_back(b->total_pix);
+        b->total_pix4 += (npix * 4 + 63) & ~(size_t)63;
+        b->total_pix += (npix + 63) & ~(size_t)63;
+        b->max_pixels = std::max(b->max_pixels, npix);
+        b->grad_base.push_back(b->total_grads);
+        b->total_grads += (sc->grad_floats + 63) & ~(size_t)63;
+        b->max_ri = std::max(b->max_ri, S.filter_ri);
+        BatchEntry e{};
+        e.S = S;
+        e.sp = sp;
+        e.item_off = b->items;
+        const int tiles = S.tiles_x * S.tiles_y;
+        e.tile_off = b->total_tiles;
+        const uint64_t spp = (uint64_t)sp.sxn * sp.syn;
+        e.nb = b->bopts.boundary_samples ? b->bopts.boundary_samples : (uint64_t)npix * spp;
+        if (!S.boundary_ok) e.nb = 0;
+        e.b_off = b->total_bsamples;
+        e.bseed = b->bopts.boundary_seed_from_options ? opts->seed : b->bopts.boundary_seed;
+        e.rng = (int)b->bopts.rng;
+        const int items = tiles * (int)spp;
+        for (int k = 0; k < items; ++k) item_scene.push_back((int)i);
+        b->items += items;
+        b->total_tiles += tiles;
+        b->total_bsamples += e.nb;
+        b->host_entries.push_back(e);
+    }
+    CK(b->accum.reserve(b->total_pix4 * sizeof(float)));
+    CK(b->image.reserve(b->total_pix4 * sizeof(float)));
+    CK(b->target.reserve(b->total_pix4 * sizeof(float)));
+    CK(b->d_render.reserve(b->total_pix4 * sizeof(float)));
+    CK(b->wsum.reserve(b->total_pix * sizeof(float)));
+    CK(b->loss.reserve(count * sizeof(float)));
+    CK(b->grads.reserve(std::max<size_t>(b->total_grads, 64) * sizeof(float)));
+    CK(b->item_scene.reserve(item_scene.size() * sizeof(int)));
+    const uint64_t nbs = std::max<uint64_t>(b->total_bsamples, 1);
+    CK(b->bsamples.reserve(nbs * sizeof(BSample)));
+    CK(b->bkey.reserve(nbs * sizeof(int)));
+    CK(b->border.reserve(nbs * sizeof(int)));
+    CK(b->bcounts.reserve((2 * (size_t)b->total_tiles + 1) * sizeof(int)));
+    CK(cudaMemsetAsync(b->target.ptr, 0, b->total_pix4 * sizeof(float), ctx->stream));
+    float* acc = b->accum.as<float>();
+    float* img = b->image.as<float>();
+    float* tgt = b->target.as<float>();
+    float* dr = b->d_render.as<float>();
+    float* ws = b->wsum.as<float>();
+    float* gb = b->grads.as<float>();
+    for (uint32_t i = 0; i < count; ++i) {
+        BatchEntry& e = b->host_entries[i];
+        dvg_scene* sc = b->scenes[i];
+        e.accum = acc + b->pix_off[i];
+        e.image = img + b->pix_off[i];
+        e.target = tgt + b->pix_off[i];
+        e.d_render = dr + b->pix_off[i];
+        e.wsum = ws + b->wpix_off[i];
+        e.loss = b->loss.as<float>() + i;
+        float* g = gb + b->grad_base[i];
+        e.G.d_shape_params = g + sc->grad_off[0];
+        e.G.d_shape_transform = g + sc->grad_off[1];
+        e.G.d_shape_stroke_width = g + sc->grad_off[2];
+        e.G.d_points = g + sc->grad_off[3];
+        e.G.d_thickness = g + sc->grad_off[4];
+        e.G.d_group_transform = g + sc->grad_off[5];
+        e.G.d_paint_params = g + sc->grad_off[6];
+        e.G.d_stop_offsets = g + sc->grad_off[7];
+        e.G.d_stop_colors = g + sc->grad_off[8];
+        e.G.d_filter_radius = g + sc->grad_off[9];
+        e.G.d_background = g + sc->grad_off[10];
+        e.G.d_background_image = nullptr;
+        e.G.d_translation = nullptr;
+    }
+    CK(b->entries.reserve(count * sizeof(BatchEntry)));
+    CK(cudaMemcpyAsync(b->entries.ptr, b->host_entries.data(), count * sizeof(BatchEntry), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(cudaMemcpyAsync(b->item_scene.ptr, item_scene.data(), item_scene.size() * sizeof(int), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *out = b.release();
+    return DVG_OK;
+}
+
+extern "C" void dvg_batch_destroy(dvg_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->ctx->device);
+    cudaStreamSynchronize(b->ctx->stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    delete b;
+}
+
+extern "C" dvg_status dvg_batch_buffers(dvg_batch* b, uint32_t index, float** image, float** target,
+                                        dvg_grads* grads) {
+    if (!b || index >= b->scenes.size()) return fail(DVG_ERR_INVALID_ARGUMENT, "batch index out of range");
+    const BatchEntry& e = b->host_entries[index];
+    if (image) *image = e.image;
+    if (target) *target = const_cast<float*>(e.target);
+    if (grads) {
+        grads->d_shape_params = e.G.d_shape_params;
+        grads->d_shape_transform = e.G.d_shape_transform;
+        grads->d_shape_stroke_width = e.G.d_shape_stroke_width;
+        grads->d_points = e.G.d_points;
+        grads->d_thickness = e.G.d_thickness;
+        grads->d_group_transform = e.G.d_group_transform;
+        grads->d_paint_params = e.G.d_paint_params;
+        grads->d_stop_offsets = e.G.d_stop_offsets;
+        grads->d_stop_colors = e.G.d_stop_colors;
+        grads->d_filter_radius = e.G.d_filter_radius;
+        grads->d_background = e.G.d_background;
+        grads->d_background_image = nullptr;
+        grads->d_translation = nullptr;
+    }
+    return DVG_OK;
+}
+
+extern "C" dvg_status dvg_batch_step(dvg_batch* b, int use_graph) {
+    if (!b) return fail(DVG_ERR_INVALID_ARGUMENT, "null batch");
+    dvg_context* ctx = b->ctx;
+    CK(cudaSetDevice(ctx->device));
+    if (!use_graph) {
+        b->steps++;
+        return batch_enqueue(b);
+    }
+    if (!b->exec) {
+        CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        dvg_status st = batch_enqueue(b);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+        if (st != DVG_OK) {
+            if (g) cudaGraphDestroy(g);
+            return st;
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        b->graph = g;
+        CK(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    }
+    CK(cudaGraphLaunch(b->exec, ctx->stream));
+    b->steps++;
+    return DVG_OK;
+}
+
+extern "C" dvg_status dvg_batch_losses(dvg_batch* b, float* host_losses) {
+    if (!b || !host_losses) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    dvg_context* ctx = b->ctx;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(host_losses, b->loss.ptr, b->scenes.size() * sizeof(float), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return check_status(ctx);
+}

@@ -118,14 +118,11 @@ __global__ void __launch_bounds__(256) k_bin_write(DevScene S, const float4* g_b
 // ------------------------------------------------------------------ forward
 // One CTA = one 16x16 tile at one sub-sample (sx, sy); thread = pixel.  Every
 // thread of the CTA walks the same group list, so group data loads are uniform.
-__global__ void __launch_bounds__(256, DVG_MINB_FWD) k_forward(DevScene S, SampleParams sp, float* accum, float* wsum,
-                                                 unsigned* status) {
-    extern __shared__ float sm[];
+__device__ __forceinline__ void forward_body(const DevScene& S, const SampleParams& sp, int tile, int sub,
+                                             float* accum, float* wsum, float* sm) {
     const int ri = S.filter_ri;
     const int HW = TILE + 2 * ri;
     const bool use_sm = ri <= MAX_SMEM_RI;
-    const int tile = blockIdx.x;
-    const int sub = blockIdx.y;
     const int tx = tile % S.tiles_x, ty = tile / S.tiles_x;
     const int x = tx * TILE + (threadIdx.x % TILE), y = ty * TILE + (threadIdx.x / TILE);
     if (use_sm)
@@ -150,6 +147,22 @@ __global__ void __launch_bounds__(256, DVG_MINB_FWD) k_forward(DevScene S, Sampl
     if (!use_sm) return;
     __syncthreads();
     flush_splat(S, tx, ty, ri, HW, sm, accum, wsum);
+}
+__global__ void __launch_bounds__(256, DVG_MINB_FWD) k_forward(DevScene S, SampleParams sp, float* accum, float* wsum,
+                                                               unsigned* status) {
+    extern __shared__ float sm[];
+    (void)status;
+    forward_body(S, sp, blockIdx.x, blockIdx.y, accum, wsum, sm);
+}
+// Batched forward: one flat grid over every (scene, tile, sub-sample) work item.
+__global__ void __launch_bounds__(256, DVG_MINB_FWD) k_forward_batch(const BatchEntry* __restrict__ B,
+                                                                     const int* __restrict__ item_scene) {
+    extern __shared__ float sm[];
+    const int item = blockIdx.x;
+    const BatchEntry& E = B[item_scene[item]];
+    const int local = item - E.item_off;
+    const int tiles = E.S.tiles_x * E.S.tiles_y;
+    forward_body(E.S, E.sp, local % tiles, local / tiles, E.accum, E.wsum, sm);
 }
 
 // Weight image only (rasterize_weights_f32, forward.rs:1505-1564).
@@ -199,10 +212,10 @@ __global__ void k_resolve(DevScene S, const float* accum, const float* wsum, flo
 // per-thread local memory, never in HBM.  The adjoint loop walks the tile's
 // group list in the same order on every lane so solid-paint gradients reduce
 // across the warp before one atomic.
-__global__ void __launch_bounds__(256, DVG_MINB_INT) k_interior(DevScene S, SampleParams sp, const float* d_render,
-                                                  const float* wsum, GradPtrs G, unsigned* status) {
+__device__ __forceinline__ void interior_body(const DevScene& S, const SampleParams& sp, int tile, int sub,
+                                              const float* d_render, const float* wsum, const GradPtrs& G,
+                                              unsigned* status) {
     __shared__ float red[8][6];
-    const int tile = blockIdx.x, sub = blockIdx.y;
     const int tx = tile % S.tiles_x, ty = tile / S.tiles_x;
     const int x = tx * TILE + (threadIdx.x % TILE), y = ty * TILE + (threadIdx.x / TILE);
     const bool valid = x < S.width && y < S.height;
@@ -376,6 +389,20 @@ __global__ void __launch_bounds__(256, DVG_MINB_INT) k_interior(DevScene S, Samp
         else
             add_if(G.d_filter_radius, s);
     }
+}
+
+__global__ void __launch_bounds__(256, DVG_MINB_INT) k_interior(DevScene S, SampleParams sp, const float* d_render,
+                                                                const float* wsum, GradPtrs G, unsigned* status) {
+    interior_body(S, sp, blockIdx.x, blockIdx.y, d_render, wsum, G, status);
+}
+__global__ void __launch_bounds__(256, DVG_MINB_INT) k_interior_batch(const BatchEntry* __restrict__ B,
+                                                                      const int* __restrict__ item_scene,
+                                                                      unsigned* status) {
+    const int item = blockIdx.x;
+    const BatchEntry& E = B[item_scene[item]];
+    const int local = item - E.item_off;
+    const int tiles = E.S.tiles_x * E.S.tiles_y;
+    interior_body(E.S, E.sp, local % tiles, local / tiles, E.d_render, E.wsum, E.G, status);
 }
 
 // ------------------------------------------------------------------ boundary sampling
@@ -816,19 +843,17 @@ __device__ void accumulate_boundary(const DevScene& S, const GradPtrs& G, int sh
 
 // Boundary pass, stage 1: draw every edge sample (boundary.rs:141-175), keep
 // the valid ones with the tile of their boundary pixel as sort key.
-__global__ void __launch_bounds__(256) k_boundary_gen(DevScene S, BoundaryParams bp, BSample* out, int* key,
-                                                      int* tile_counts) {
-    const uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + bp.sample_base;
-    if (idx >= bp.num_samples) return;
-    const uint64_t slot = idx - bp.slot_base;
+__device__ __forceinline__ void boundary_gen_one(const DevScene& S, uint64_t idx, uint64_t slot, uint32_t seed,
+                                                 int rng_kind, int tile_off, int scene, BSample* out, int* key,
+                                                 int* tile_counts) {
     key[slot] = -1;
     float u, t;
-    if (bp.rng == 1) {
-        uint4 r = philox4x32_10(make_uint4((uint32_t)idx, (uint32_t)(idx >> 32), 0u, 0u), make_uint2(bp.seed, 0u));
+    if (rng_kind == 1) {
+        uint4 r = philox4x32_10(make_uint4((uint32_t)idx, (uint32_t)(idx >> 32), 0u, 0u), make_uint2(seed, 0u));
         u = unit_from_u32(r.x);
         t = unit_from_u32(r.y);
     } else {
-        Pcg32 rng(idx, (uint64_t)bp.seed);
+        Pcg32 rng(idx, (uint64_t)seed);
         u = rng.next_f32();
         t = rng.next_f32();
     }
@@ -876,11 +901,36 @@ __global__ void __launch_bounds__(256) k_boundary_gen(DevScene S, BoundaryParams
     r.point_id = bd.point_id;
     r.bt = bd.t;
     r.is_stroke = bd.is_stroke ? 1 : 0;
-    r.pad = 0;
+    r.scene = scene;
     out[slot] = r;
-    const int tile = (by / TILE) * S.tiles_x + (bx / TILE);
+    const int tile = tile_off + (by / TILE) * S.tiles_x + (bx / TILE);
     key[slot] = tile;
     atomicAdd(tile_counts + tile, 1);
+}
+__global__ void __launch_bounds__(256) k_boundary_gen(DevScene S, BoundaryParams bp, BSample* out, int* key,
+                                                      int* tile_counts) {
+    const uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + bp.sample_base;
+    if (idx >= bp.num_samples) return;
+    boundary_gen_one(S, idx, idx - bp.slot_base, bp.seed, bp.rng, 0, 0, out, key, tile_counts);
+}
+// Batched stage 1: one flat index over all scenes' boundary samples; the scene is
+// found by binary search over the per-scene sample offsets.
+__global__ void __launch_bounds__(256) k_boundary_gen_batch(const BatchEntry* __restrict__ B, int nscenes,
+                                                            uint64_t total, BSample* out, int* key, int* tile_counts) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    int lo = 0, hi = nscenes - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (B[mid].b_off <= g)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const BatchEntry& E = B[lo];
+    key[g] = -1;
+    if (!E.S.boundary_ok || g - E.b_off >= E.nb) return;
+    boundary_gen_one(E.S, g - E.b_off, g, E.bseed, E.rng, E.tile_off, lo, out, key, tile_counts);
 }
 // Stage 2: counting-sort scatter of sample slots by tile.
 __global__ void k_boundary_scatter(const int* key, uint64_t n, int* cursor, int* order) {
@@ -892,12 +942,8 @@ __global__ void k_boundary_scatter(const int* key, uint64_t n, int* cursor, int*
 }
 // Stage 3: evaluate both sides of every edge sample in tile order, so that the
 // lanes of a warp share one group list (render_edge_sample, boundary.rs:845-967).
-__global__ void __launch_bounds__(128, DVG_MINB_BND) k_boundary_eval(DevScene S, const BSample* samples, const int* order,
-                                                       const int* offsets, int tiles, const float* d_render,
-                                                       const float* wsum, GradPtrs G) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= offsets[tiles]) return;
-    const BSample r = samples[order[i]];
+__device__ __forceinline__ void boundary_eval_one(const DevScene& S, const BSample& r, const float* d_render,
+                                                  const float* wsum, const GradPtrs& G) {
     const float W = (float)S.width, H = (float)S.height;
     const float4 bg = background_premul(S, r.pixel);
     const int tile = ((r.pixel / S.width) / TILE) * S.tiles_x + ((r.pixel % S.width) / TILE);
@@ -958,6 +1004,23 @@ __global__ void __launch_bounds__(128, DVG_MINB_BND) k_boundary_eval(DevScene S,
         add_if(G.d_translation + 2 * (size_t)r.pixel + 1, nc.y * contrib);
     }
 }
+__global__ void __launch_bounds__(128, DVG_MINB_BND) k_boundary_eval(DevScene S, const BSample* samples,
+                                                                     const int* order, const int* offsets, int tiles,
+                                                                     const float* d_render, const float* wsum,
+                                                                     GradPtrs G) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= offsets[tiles]) return;
+    boundary_eval_one(S, samples[order[i]], d_render, wsum, G);
+}
+__global__ void __launch_bounds__(128, DVG_MINB_BND) k_boundary_eval_batch(const BatchEntry* __restrict__ B,
+                                                                           const BSample* samples, const int* order,
+                                                                           const int* offsets, int tiles) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= offsets[tiles]) return;
+    const BSample r = samples[order[i]];
+    const BatchEntry& E = B[r.scene];
+    boundary_eval_one(E.S, r, E.d_render, E.wsum, E.G);
+}
 
 // ------------------------------------------------------------------ background finalisation (background.rs:29-61)
 __global__ void k_finalize_background(DevScene S, GradPtrs G) {
@@ -1011,6 +1074,72 @@ __global__ void k_l2(const float* img, const float* target, size_t n, float* d_r
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
         atomicAdd(loss, t);
     }
+}
+
+// ------------------------------------------------------------------ batched per-pixel kernels (grid.y = scene)
+__global__ void k_resolve_batch(const BatchEntry* __restrict__ B) {
+    const BatchEntry& E = B[blockIdx.y];
+    size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= (size_t)E.S.width * E.S.height) return;
+    float r = E.S.bg[0], g = E.S.bg[1], b = E.S.bg[2], a = E.S.bg[3];
+    float w = E.wsum[p];
+    if (w > 0.0f) {
+        float4 c = reinterpret_cast<const float4*>(E.accum)[p];
+        r = c.x / w;
+        g = c.y / w;
+        b = c.z / w;
+        a = c.w / w;
+    }
+    if (a > 1.0e-8f) {
+        r = r / a;
+        g = g / a;
+        b = b / a;
+    }
+    reinterpret_cast<float4*>(E.image)[p] = make_float4(r, g, b, a);
+}
+__global__ void k_l2_batch(const BatchEntry* __restrict__ B) {
+    __shared__ float red[8];
+    const BatchEntry& E = B[blockIdx.y];
+    const size_t n = (size_t)E.S.width * E.S.height * 4;
+    float s = 0.0f;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        float d = E.image[i] - E.target[i];
+        E.d_render[i] = 2.0f * d;
+        s += d * d;
+    }
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.0f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        atomicAdd(E.loss, t);
+    }
+}
+__global__ void k_finalize_background_batch(const BatchEntry* __restrict__ B) {
+    const BatchEntry& E = B[blockIdx.y];
+    size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (E.S.bg_image) {
+        if (!E.G.d_background_image || p >= (size_t)E.S.width * E.S.height) return;
+        const float* im = E.S.bg_image + 4 * p;
+        float* c = E.G.d_background_image + 4 * p;
+        float dr = c[0] * im[3], dg = c[1] * im[3], db = c[2] * im[3];
+        float da = c[0] * im[0] + c[1] * im[1] + c[2] * im[2] + c[3];
+        c[0] = dr;
+        c[1] = dg;
+        c[2] = db;
+        c[3] = da;
+        return;
+    }
+    if (p != 0) return;
+    float* d = E.G.d_background;
+    float r = E.S.bg[0], g = E.S.bg[1], b = E.S.bg[2], a = E.S.bg[3];
+    float nr = d[0] * a, ng = d[1] * a, nb = d[2] * a;
+    float na = d[0] * r + d[1] * g + d[2] * b + d[3];
+    d[0] = nr;
+    d[1] = ng;
+    d[2] = nb;
+    d[3] = na;
 }
 
 }  // namespace dvgb
@@ -1084,6 +1213,48 @@ int launch_finalize_background(const DevScene& S, const GradPtrs& G, cudaStream_
     k_finalize_background<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(S, G);
     return 1;
 }
+// Batched step launchers (one launch per stage for all scenes).
+int launch_forward_batch(const BatchEntry* B, const int* item_scene, int items, int max_ri, cudaStream_t stream) {
+    const int hw = TILE + 2 * max_ri;
+    size_t smem = max_ri <= MAX_SMEM_RI ? (size_t)hw * hw * 5 * sizeof(float) : 0;
+    k_forward_batch<<<items, 256, smem, stream>>>(B, item_scene);
+    return 1;
+}
+int launch_pixels_batch(const BatchEntry* B, int nscenes, size_t max_pixels, int which, cudaStream_t stream) {
+    if (which == 0) {
+        dim3 grid((unsigned)((max_pixels + 255) / 256), nscenes);
+        k_resolve_batch<<<grid, 256, 0, stream>>>(B);
+    } else if (which == 1) {
+        unsigned bx = (unsigned)((max_pixels * 4 + 255) / 256);
+        if (bx > 512) bx = 512;
+        dim3 grid(bx, nscenes);
+        k_l2_batch<<<grid, 256, 0, stream>>>(B);
+    } else {
+        dim3 grid((unsigned)((max_pixels + 255) / 256), nscenes);
+        k_finalize_background_batch<<<grid, 256, 0, stream>>>(B);
+    }
+    return 1;
+}
+int launch_interior_batch(const BatchEntry* B, const int* item_scene, int items, unsigned* status,
+                          cudaStream_t stream) {
+    k_interior_batch<<<items, 256, 0, stream>>>(B, item_scene, status);
+    return 1;
+}
+int launch_boundary_batch(const BatchEntry* B, int nscenes, uint64_t total, int total_tiles, BSample* samples, int* key,
+                          int* counts, int* order, cudaStream_t stream) {
+    if (total == 0) return 0;
+    cudaMemsetAsync(counts, 0, sizeof(int) * (2 * (size_t)total_tiles + 1), stream);
+    k_boundary_gen_batch<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(B, nscenes, total, samples, key,
+                                                                              counts);
+    int* offsets = counts + total_tiles;
+    k_bin_scan<<<1, 1024, 0, stream>>>(counts, total_tiles, offsets);
+    cudaMemcpyAsync(counts, offsets, sizeof(int) * (size_t)total_tiles, cudaMemcpyDeviceToDevice, stream);
+    k_boundary_scatter<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(key, total, counts, order);
+    k_boundary_eval_batch<<<(unsigned)((total + 127) / 128), 128, 0, stream>>>(B, samples, order, offsets,
+                                                                               total_tiles);
+    return 4;
+}
+
 int launch_fill_background(const DevScene& S, float* out, cudaStream_t stream) {
     size_t n = (size_t)S.width * S.height;
     k_fill_background<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(S, out);

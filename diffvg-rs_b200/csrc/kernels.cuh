@@ -36,7 +36,26 @@ struct BSample {
     int shape, group, pixel;
     int base_point_id, point_id;
     float bt;
-    int is_stroke, pad;
+    int is_stroke, scene;  // scene: index in a batch (0 for single-scene calls)
+};
+// One scene of a batch: its tables, options, gradient pointers, per-scene
+// output buffers and its ranges in the batch-wide work numbering.
+struct BatchEntry {
+    DevScene S;
+    SampleParams sp;
+    GradPtrs G;
+    float* accum;
+    float* wsum;
+    float* image;
+    const float* target;
+    float* d_render;
+    float* loss;
+    int item_off;    // first (tile, sub-sample) work item
+    int tile_off;    // first tile in the batch-wide tile numbering
+    uint64_t b_off;  // first boundary sample in the batch-wide numbering
+    uint64_t nb;     // boundary samples of this scene
+    uint32_t bseed;
+    int rng;
 };
 
 
@@ -60,6 +79,18 @@ int launch_boundary(const DevScene& S, const BoundaryParams& bp, const float* d_
                     cudaStream_t stream);
 int launch_finalize_background(const DevScene& S, const GradPtrs& G, cudaStream_t stream);
 int launch_fill_background(const DevScene& S, float* out, cudaStream_t stream);
+// Batched launchers: B (device) holds one BatchEntry per scene; item_scene maps each
+// (scene, tile, sub-sample) work item to its scene.  which: 0 resolve, 1 L2, 2 background.
+int launch_forward_batch(const BatchEntry* B, const int* item_scene, int items, int max_ri, cudaStream_t stream);
+int launch_forward_prefilter_batch(const BatchEntry* B, const int* item_scene, int items, int max_ri,
+                                   unsigned* status, cudaStream_t stream);
+int launch_pixels_batch(const BatchEntry* B, int nscenes, size_t max_pixels, int which, cudaStream_t stream);
+int launch_interior_batch(const BatchEntry* B, const int* item_scene, int items, unsigned* status,
+                          cudaStream_t stream);
+int launch_interior_prefilter_batch(const BatchEntry* B, const int* item_scene, int items, unsigned* status,
+                                    cudaStream_t stream);
+int launch_boundary_batch(const BatchEntry* B, int nscenes, uint64_t total, int total_tiles, BSample* samples, int* key,
+                          int* counts, int* order, cudaStream_t stream);
 int launch_l2(const float* img, const float* target, size_t n, float* d_render, float* loss, cudaStream_t stream);
 
 }  // namespace dvgb

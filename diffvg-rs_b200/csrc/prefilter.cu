@@ -290,13 +290,11 @@ __device__ __forceinline__ PFragD prefilter_fill(const DevScene& S, int g, int p
 }
 
 // ------------------------------------------------------------------ forward
-__global__ void __launch_bounds__(256, 2) k_forward_prefilter(DevScene S, SampleParams sp, float* accum, float* wsum,
-                                                              unsigned* status) {
-    extern __shared__ float sm[];
+__device__ __forceinline__ void forward_prefilter_body(const DevScene& S, const SampleParams& sp, int tile, int sub,
+                                                       float* accum, float* wsum, unsigned* status, float* sm) {
     const int ri = S.filter_ri;
     const int HW = TILE + 2 * ri;
     const bool use_sm = ri <= MAX_SMEM_RI;
-    const int tile = blockIdx.x, sub = blockIdx.y;
     const int tx = tile % S.tiles_x, ty = tile / S.tiles_x;
     const int x = tx * TILE + (threadIdx.x % TILE), y = ty * TILE + (threadIdx.x / TILE);
     if (use_sm)
@@ -326,6 +324,21 @@ __global__ void __launch_bounds__(256, 2) k_forward_prefilter(DevScene S, Sample
     if (!use_sm) return;
     __syncthreads();
     flush_splat(S, tx, ty, ri, HW, sm, accum, wsum);
+}
+__global__ void __launch_bounds__(256, 2) k_forward_prefilter(DevScene S, SampleParams sp, float* accum, float* wsum,
+                                                              unsigned* status) {
+    extern __shared__ float sm[];
+    forward_prefilter_body(S, sp, blockIdx.x, blockIdx.y, accum, wsum, status, sm);
+}
+__global__ void __launch_bounds__(256, 2) k_forward_prefilter_batch(const BatchEntry* __restrict__ B,
+                                                                    const int* __restrict__ item_scene,
+                                                                    unsigned* status) {
+    extern __shared__ float sm[];
+    const int item = blockIdx.x;
+    const BatchEntry& E = B[item_scene[item]];
+    const int local = item - E.item_off;
+    const int tiles = E.S.tiles_x * E.S.tiles_y;
+    forward_prefilter_body(E.S, E.sp, local % tiles, local / tiles, E.accum, E.wsum, status, sm);
 }
 
 // ------------------------------------------------------------------ distance adjoint (backward/distance.rs)
@@ -721,10 +734,10 @@ __device__ float2 d_compute_distance(const DevScene& S, const GradPtrs& G, int g
 
 // ------------------------------------------------------------------ interior adjoint (sampling.rs:227-482)
 constexpr int MAX_PF = 48;
-__global__ void __launch_bounds__(256) k_interior_prefilter(DevScene S, SampleParams sp, const float* d_render,
-                                                            const float* wsum, GradPtrs G, unsigned* status) {
+__device__ __forceinline__ void interior_prefilter_body(const DevScene& S, const SampleParams& sp, int tile, int sub,
+                                                        const float* d_render, const float* wsum, const GradPtrs& G,
+                                                        unsigned* status) {
     __shared__ float red[8][6];
-    const int tile = blockIdx.x, sub = blockIdx.y;
     const int tx = tile % S.tiles_x, ty = tile / S.tiles_x;
     const int x = tx * TILE + (threadIdx.x % TILE), y = ty * TILE + (threadIdx.x / TILE);
     const bool valid = x < S.width && y < S.height;
@@ -914,6 +927,20 @@ __global__ void __launch_bounds__(256) k_interior_prefilter(DevScene S, SamplePa
     }
 }
 
+__global__ void __launch_bounds__(256) k_interior_prefilter(DevScene S, SampleParams sp, const float* d_render,
+                                                            const float* wsum, GradPtrs G, unsigned* status) {
+    interior_prefilter_body(S, sp, blockIdx.x, blockIdx.y, d_render, wsum, G, status);
+}
+__global__ void __launch_bounds__(256) k_interior_prefilter_batch(const BatchEntry* __restrict__ B,
+                                                                  const int* __restrict__ item_scene,
+                                                                  unsigned* status) {
+    const int item = blockIdx.x;
+    const BatchEntry& E = B[item_scene[item]];
+    const int local = item - E.item_off;
+    const int tiles = E.S.tiles_x * E.S.tiles_y;
+    interior_prefilter_body(E.S, E.sp, local % tiles, local / tiles, E.d_render, E.wsum, E.G, status);
+}
+
 int launch_forward_prefilter(const DevScene& S, const SampleParams& sp, float* accum, float* wsum, unsigned* status,
                              cudaStream_t stream) {
     const int hw = TILE + 2 * S.filter_ri;
@@ -926,6 +953,19 @@ int launch_interior_prefilter(const DevScene& S, const SampleParams& sp, const f
                               const GradPtrs& G, unsigned* status, cudaStream_t stream) {
     dim3 grid(S.tiles_x * S.tiles_y, sp.sxn * sp.syn);
     k_interior_prefilter<<<grid, 256, 0, stream>>>(S, sp, d_render, wsum, G, status);
+    return 1;
+}
+
+int launch_forward_prefilter_batch(const BatchEntry* B, const int* item_scene, int items, int max_ri,
+                                   unsigned* status, cudaStream_t stream) {
+    const int hw = TILE + 2 * max_ri;
+    size_t smem = max_ri <= MAX_SMEM_RI ? (size_t)hw * hw * 5 * sizeof(float) : 0;
+    k_forward_prefilter_batch<<<items, 256, smem, stream>>>(B, item_scene, status);
+    return 1;
+}
+int launch_interior_prefilter_batch(const BatchEntry* B, const int* item_scene, int items, unsigned* status,
+                                    cudaStream_t stream) {
+    k_interior_prefilter_batch<<<items, 256, 0, stream>>>(B, item_scene, status);
     return 1;
 }
 

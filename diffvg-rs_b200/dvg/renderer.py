@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import weakref
 from dataclasses import dataclass
 from typing import Optional
 
@@ -41,7 +42,8 @@ EXPORTED = (
     "dvg_scene_destroy", "dvg_render_host", "dvg_render_device", "dvg_render_backward_host",
     "dvg_render_backward_device", "dvg_render", "dvg_render_backward", "dvg_fwd_bwd_l2_device",
     "dvg_context_launch_count", "dvg_context_stream", "dvg_context_set_profiling", "dvg_context_profile",
-    "dvg_context_profile_reset",
+    "dvg_context_profile_reset", "dvg_batch_create", "dvg_batch_destroy", "dvg_batch_buffers", "dvg_batch_step",
+    "dvg_batch_losses", "dvg_render_device_noalloc",
 )
 
 
@@ -101,6 +103,14 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.dvg_context_profile.restype = C.c_int
     L.dvg_context_profile_reset.argtypes = [vp]
     L.dvg_context_profile_reset.restype = None
+    L.dvg_batch_create.argtypes = [vp, C.POINTER(vp), C.c_uint32, R, B, C.POINTER(vp)]
+    L.dvg_batch_destroy.argtypes = [vp]
+    L.dvg_batch_destroy.restype = None
+    L.dvg_batch_buffers.argtypes = [vp, C.c_uint32, C.POINTER(vp), C.POINTER(vp), Gp]
+    L.dvg_batch_step.argtypes = [vp, C.c_int]
+    L.dvg_batch_losses.argtypes = [vp, fp]
+    for name in ("dvg_batch_create", "dvg_batch_buffers", "dvg_batch_step", "dvg_batch_losses"):
+        getattr(L, name).restype = C.c_int
     for name in ("dvg_context_create", "dvg_scene_upload", "dvg_render_host", "dvg_render_device",
                  "dvg_render_backward_host", "dvg_render_backward_device", "dvg_render", "dvg_render_backward",
                  "dvg_fwd_bwd_l2_device"):
@@ -172,11 +182,12 @@ class UploadedScene:
         self.packed = pack_scene(scene)
         self.handle = C.c_void_p()
         _check(renderer.lib.dvg_scene_upload(renderer.ctx, self.packed.ref(), C.byref(self.handle)))
+        renderer._children.add(self)
 
     def close(self) -> None:
-        if self.handle:
+        if self.handle and self.renderer.ctx:
             self.renderer.lib.dvg_scene_destroy(self.handle)
-            self.handle = C.c_void_p()
+        self.handle = C.c_void_p()
 
     def __del__(self):
         try:
@@ -215,12 +226,15 @@ class Renderer:
 
     def __init__(self, device: int = 0):
         self.lib = load_library()
+        self._children = weakref.WeakSet()  # scenes and batches: destroyed before the context
         self.ctx = C.c_void_p()
         _check(self.lib.dvg_context_create(int(device), C.byref(self.ctx)))
         self.device = device
 
     def close(self) -> None:
         if self.ctx:
+            for child in sorted(list(self._children), key=lambda c: 0 if isinstance(c, Batch) else 1):
+                child.close()
             self.lib.dvg_context_destroy(self.ctx)
             self.ctx = C.c_void_p()
 
@@ -291,3 +305,59 @@ class Renderer:
         _check(self.lib.dvg_render_backward(self.ctx, packed.ref(), C.byref(o), C.byref(b), _fp(dr), _fp(ds),
                                             C.byref(buf.c)))
         return unflatten_grads(scene, packed, buf)
+
+
+def device_view(ptr: int, count: int, device=None):
+    """A float32 torch tensor aliasing `count` floats of device memory at `ptr`."""
+    import torch
+
+    class _Iface:
+        __cuda_array_interface__ = {"shape": (int(count),), "typestr": "<f4", "data": (int(ptr), False),
+                                    "version": 3, "strides": None}
+
+    return torch.as_tensor(_Iface(), device=device or "cuda")
+
+
+class Batch:
+    """dvg_batch: many uploaded scenes stepped together (one launch per stage, CUDA graph)."""
+
+    def __init__(self, renderer: "Renderer", scenes, options: RenderOptions,
+                 backward_options: Optional[BackwardOptions] = None):
+        self.renderer = renderer
+        self.scenes = list(scenes)
+        arr = (C.c_void_p * len(self.scenes))(*[u.handle.value for u in self.scenes])
+        o = render_options_c(options)
+        b = backward_options_c(backward_options)
+        self.handle = C.c_void_p()
+        _check(renderer.lib.dvg_batch_create(renderer.ctx, arr, len(self.scenes), C.byref(o), C.byref(b),
+                                             C.byref(self.handle)))
+        renderer._children.add(self)
+
+    def buffers(self, index: int):
+        """(image tensor, target tensor, GradsC) aliasing the batch's device buffers of scene `index`."""
+        img = C.c_void_p()
+        tgt = C.c_void_p()
+        g = GradsC()
+        _check(self.renderer.lib.dvg_batch_buffers(self.handle, index, C.byref(img), C.byref(tgt), C.byref(g)))
+        sc = self.scenes[index].scene
+        n = sc.width * sc.height * 4
+        return device_view(img.value, n), device_view(tgt.value, n), g
+
+    def step(self, use_graph: bool = True) -> None:
+        _check(self.renderer.lib.dvg_batch_step(self.handle, 1 if use_graph else 0))
+
+    def losses(self) -> np.ndarray:
+        out = np.zeros(len(self.scenes), np.float32)
+        _check(self.renderer.lib.dvg_batch_losses(self.handle, _fp(out)))
+        return out
+
+    def close(self) -> None:
+        if self.handle and self.renderer.ctx:
+            self.renderer.lib.dvg_batch_destroy(self.handle)
+        self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

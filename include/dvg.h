@@ -19,6 +19,8 @@
  *     strings as RenderError::InvalidScene (src/renderer/types.rs:83-88).
  *   - Calls on one context are serialised on that context's CUDA stream.
  *     A context may be used from one host thread at a time.
+ *   - Scenes and batches belong to the context they were created on: destroy
+ *     them before that context.
  */
 #ifndef DVG_H
 #define DVG_H
@@ -238,6 +240,26 @@ dvg_status dvg_render_backward(dvg_context* ctx, const dvg_scene_desc* desc,
 dvg_status dvg_fwd_bwd_l2_device(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
                                  const dvg_backward_options* bopts, const float* target_rgba,
                                  float* out_rgba, float* loss_out, dvg_grads* grads);
+
+/* Batches (no counterpart in the crate): many uploaded scenes stepped together.
+ * A step renders every scene, forms the L2 loss against that scene's target, and
+ * runs the backward pass — one kernel launch per stage for all scenes (work items
+ * are (scene, tile, sub-sample) triples; boundary samples of all scenes are sorted
+ * together by tile).  All scenes share opts / bopts.  The batch owns the images,
+ * targets, gradients and scratch of every scene; dvg_batch_buffers returns device
+ * pointers into them (write the targets there before stepping).
+ * dvg_batch_step(use_graph=1) captures the step into a CUDA graph on its first call
+ * and replays it afterwards; use_graph=0 enqueues the kernels directly. */
+typedef struct dvg_batch dvg_batch;
+dvg_status dvg_batch_create(dvg_context* ctx, dvg_scene* const* scenes, uint32_t count,
+                            const dvg_render_options* opts, const dvg_backward_options* bopts,
+                            dvg_batch** out);
+void dvg_batch_destroy(dvg_batch* batch);
+dvg_status dvg_batch_buffers(dvg_batch* batch, uint32_t index, float** image, float** target,
+                             dvg_grads* grads);
+dvg_status dvg_batch_step(dvg_batch* batch, int use_graph);
+/* Copies the per-scene L2 losses of the last step to host memory (synchronises). */
+dvg_status dvg_batch_losses(dvg_batch* batch, float* host_losses);
 
 /* Number of kernels this library launched on the context since creation. */
 uint64_t dvg_context_launch_count(const dvg_context* ctx);
