@@ -31,7 +31,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "diffvg-rs_b200"))
 
-from dvg import BackwardOptions, DeviceGrads, Renderer, synth  # noqa: E402
+from dvg import BackwardOptions, Batch, DeviceGrads, Renderer, synth  # noqa: E402
 
 METRIC = "fwd+bwd Msamples/s (ms/iter), plain single-scene launch loop on one B200"
 UNIT = "Msamples/s"
@@ -129,6 +129,61 @@ def cpu_baseline(sc, opts, bopts, target_img, img, seconds: float):
             "ms_per_step_extrapolated": t * total / n * 1e3}
 
 
+def batched_vs_plain(r, dev, lib_stream, flush, count, steps, rank):
+    """64 uneven scenes (sides 128/256/512, 4-1024 paths, 4x4 spp): one batched
+    CUDA-graph step against the loop of single-scene fused calls, same work."""
+    import torch
+
+    scenes = synth.batched_scenes(seed=rank, count=count)
+    opts = synth.batched_options()
+    bopts = BackwardOptions(boundary_samples=0)
+    ups = [r.upload(s) for s in scenes]
+    tgts = [r.upload(synth.plain_scene(1000 + i, s.width, s.height, 16)) for i, s in enumerate(scenes)]
+    batch = Batch(r, ups, opts, bopts)
+    plain = []
+    for i, (up, tu) in enumerate(zip(ups, tgts)):
+        _, tgt_b, _ = batch.buffers(i)
+        tu.render_device(opts, tgt_b.data_ptr())
+        n = up.scene.width * up.scene.height * 4
+        plain.append((up, tgt_b, torch.empty(n, device=dev), torch.zeros(1, device=dev), DeviceGrads(up.packed, dev)))
+    torch.cuda.synchronize(dev)
+
+    def plain_step():
+        for up, tgt, out, loss, g in plain:
+            up.fwd_bwd_l2_device(opts, bopts, tgt.data_ptr(), out.data_ptr(), loss.data_ptr(), g)
+
+    def timed(fn):
+        fn()
+        fn()
+        torch.cuda.synchronize(dev)
+        ms = []
+        for _ in range(steps):
+            with torch.cuda.stream(lib_stream):
+                flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(lib_stream)
+            fn()
+            e1.record(lib_stream)
+            torch.cuda.synchronize(dev)
+            ms.append(e0.elapsed_time(e1))
+        return float(np.median(ms))
+
+    t_plain = timed(plain_step)
+    t_batch = timed(lambda: batch.step(True))
+    samples = sum(s.width * s.height * 16 for s in scenes)
+    out = {"scenes": count, "samples_per_step": samples,
+           "batched_ms_per_step": t_batch, "plain_ms_per_step": t_plain,
+           "scenes_per_s_batched_graph": count / (t_batch / 1e3), "scenes_per_s_plain_loop": count / (t_plain / 1e3),
+           "msamples_per_s_batched": samples / (t_batch / 1e3) / 1e6, "speedup": t_plain / t_batch,
+           "workload": "64 uneven scenes: side in {128,256,512}, log-uniform 4-1024 closed cubic paths (plain mix, "
+                       "paths shrink as sqrt(16/n)), 4x4 spp, box r=0.5, W*H*spp boundary samples, fwd+L2+bwd"}
+    batch.close()
+    for u in ups + tgts:
+        u.close()
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -167,6 +222,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-scenes", type=int, default=64)
+    ap.add_argument("--batch-steps", type=int, default=5)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -270,6 +327,18 @@ def main():
                "d2h_bytes_per_step": int(img_h.nbytes + grad_bytes), "ms_per_step": e2e_s * 1e3,
                "path": "dvg_render + dvg_render_backward (host buffers, per-call scene preparation)"}
 
+    batched = None
+    if args.batch_scenes > 0:
+        batched = batched_vs_plain(r, dev, lib_stream, flush, args.batch_scenes, args.batch_steps, rank)
+        if world > 1:
+            t = torch.tensor([batched["batched_ms_per_step"], batched["plain_ms_per_step"]], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            batched["batched_ms_per_step"], batched["plain_ms_per_step"] = float(t[0]), float(t[1])
+            n = batched["scenes"] * world
+            batched["scenes_per_s_batched_graph"] = n / (batched["batched_ms_per_step"] / 1e3)
+            batched["scenes_per_s_plain_loop"] = n / (batched["plain_ms_per_step"] / 1e3)
+            batched["speedup"] = batched["plain_ms_per_step"] / batched["batched_ms_per_step"]
+
     dominant = max(prof.items(), key=lambda kv: kv[1][0]) if prof else ("none", (0.0, 1))
     name, (ms_tot, calls) = dominant
     avg_ms = ms_tot / max(calls, 1)
@@ -302,6 +371,7 @@ def main():
                              "as required, see profiles/ for the issue-slot view"},
         "kernel_ms_per_step": prof_json,
         "gpu_launches": int(timed_launches), "clocks": clocks.summary(), "e2e": e2e,
+        "batched_vs_plain": batched,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         img = out.view(H, W, 4).cpu().numpy()

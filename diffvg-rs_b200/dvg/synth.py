@@ -46,14 +46,25 @@ def _stops(rng: np.random.Generator, n: int) -> List[GradientStop]:
     return [GradientStop(float(o), _solid(rng)) for o in offs]
 
 
-def plain_scene(seed: int = 0, width: int = 256, height: int = 256, num_paths: int = 16) -> Scene:
+def plain_scene(seed: int = 0, width: int = 256, height: int = 256, num_paths: int = 16,
+                extent: float = 1.0) -> Scene:
+    """``extent`` < 1 confines each path's control points to a random square of that
+    fraction of the canvas (1.0: points uniform over the whole canvas)."""
     rng = np.random.default_rng(seed)
     sc = Scene(width, height)
     sc.background = Color(1.0, 1.0, 1.0, 1.0)
     sc.filter = Filter(FilterType.BOX, 0.5)
+    side = float(max(width, height))
     for i in range(num_paths):
         nseg = int(rng.integers(4, 9))
-        sc.shapes.append(Shape(PathGeometry(_closed_cubic(rng, nseg, 0.0, float(max(width, height))))))
+        if extent >= 1.0:
+            path = _closed_cubic(rng, nseg, 0.0, side)
+        else:
+            size = extent * side
+            ox, oy = rng.uniform(0.0, side - size, 2)
+            path = _closed_cubic(rng, nseg, 0.0, size)
+            path.points = [(float(np.float32(x + ox)), float(np.float32(y + oy))) for x, y in path.points]
+        sc.shapes.append(Shape(PathGeometry(path)))
         sc.groups.append(ShapeGroup([i], _solid(rng), None))
     return sc
 
@@ -160,14 +171,22 @@ def adjoint_options() -> RenderOptions:
 
 
 def batched_scenes(seed: int = 0, count: int = 64) -> List[Scene]:
+    """Uneven batch: side in {128,256,512}, log-uniform 4-1024 paths of the plain mix.
+    Paths shrink as sqrt(16/n) of the canvas above 16 paths, which keeps the depth
+    complexity of the 16-path plain scene instead of stacking hundreds of
+    full-canvas paths on every pixel."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(count):
         side = int(rng.choice([128, 256, 512]))
         n = int(round(math.exp(rng.uniform(math.log(4), math.log(1024)))))
-        sub = plain_scene(int(rng.integers(0, 2 ** 31)), side, side, n)
-        out.append(sub)
+        extent = min(1.0, math.sqrt(16.0 / n))
+        out.append(plain_scene(int(rng.integers(0, 2 ** 31)), side, side, n, extent))
     return out
+
+
+def batched_options() -> RenderOptions:
+    return RenderOptions(samples_x=4, samples_y=4, seed=0, jitter=True, use_prefiltering=False)
 
 
 def large_scene(seed: int = 0, width: int = 1024, height: int = 1024, num_paths: int = 4096) -> Scene:
