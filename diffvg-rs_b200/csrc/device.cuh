@@ -116,6 +116,14 @@ __device__ __forceinline__ float2 shape_local_bwd(const DevScene& S, int s, floa
 }
 
 // ------------------------------------------------------------------ polynomial roots (f64, distance/utils.rs:48-123)
+// Out-of-line wrappers: one copy of each libm body per kernel instead of one per call site.
+static __device__ __noinline__ double dvg_acos(double x) { return acos(x); }
+static __device__ __noinline__ double dvg_cos(double x) { return cos(x); }
+static __device__ __noinline__ double dvg_pow(double x, double y) { return pow(x, y); }
+static __device__ __noinline__ float dvg_sinf(float x) { return sinf(x); }
+static __device__ __noinline__ float dvg_cosf(float x) { return cosf(x); }
+static __device__ __noinline__ float dvg_expf(float x) { return expf(x); }
+static __device__ __noinline__ float dvg_atan2f(float y, float x) { return atan2f(y, x); }
 __device__ __forceinline__ bool solve_quadratic(double a, double b, double c, double t[2]) {
     const double eps = 1.0e-12;
     if (fabs(a) < eps) {
@@ -151,11 +159,11 @@ __device__ __forceinline__ bool solve_quadratic(double a, double b, double c, do
     return true;
 }
 __device__ __forceinline__ double cbrt_pow(double x) {
-    if (x > 0.0) return pow(x, 1.0 / 3.0);
-    if (x < 0.0) return -pow(-x, 1.0 / 3.0);
+    if (x > 0.0) return dvg_pow(x, 1.0 / 3.0);
+    if (x < 0.0) return -dvg_pow(-x, 1.0 / 3.0);
     return 0.0;
 }
-__device__ __forceinline__ int solve_cubic(double a, double b, double c, double d, double t[3]) {
+static __device__ __noinline__ int solve_cubic(double a, double b, double c, double d, double t[3]) {
     if (fabs(a) < 1.0e-6) {
         double r2[2];
         if (solve_quadratic(b, c, d, r2)) {
@@ -172,11 +180,11 @@ __device__ __forceinline__ int solve_cubic(double a, double b, double c, double 
     double r = (2.0 * b * b * b - 9.0 * b * c + 27.0 * d) / 54.0;
     const double TWO_PI = 6.283185307179586476925286766559;
     if (r * r < q * q * q) {
-        double theta = acos(r / sqrt(q * q * q));
+        double theta = dvg_acos(r / sqrt(q * q * q));
         double sq = sqrt(q);
-        t[0] = -2.0 * sq * cos(theta / 3.0) - b / 3.0;
-        t[1] = -2.0 * sq * cos((theta + TWO_PI) / 3.0) - b / 3.0;
-        t[2] = -2.0 * sq * cos((theta - TWO_PI) / 3.0) - b / 3.0;
+        t[0] = -2.0 * sq * dvg_cos(theta / 3.0) - b / 3.0;
+        t[1] = -2.0 * sq * dvg_cos((theta + TWO_PI) / 3.0) - b / 3.0;
+        t[2] = -2.0 * sq * dvg_cos((theta - TWO_PI) / 3.0) - b / 3.0;
         return 3;
     }
     double ar = (r > 0.0) ? -cbrt_pow(r + sqrt(r * r - q * q * q)) : cbrt_pow(-r + sqrt(r * r - q * q * q));
@@ -603,9 +611,9 @@ static __device__ __noinline__ float2 closest_point_ellipse(float cx, float cy, 
     float sx = dx < 0.0f ? -1.0f : 1.0f, sy = dy < 0.0f ? -1.0f : 1.0f;
     dx = fabsf(dx);
     dy = fabsf(dy);
-    float t = atan2f(dy * rx, dx * ry);
+    float t = dvg_atan2f(dy * rx, dx * ry);
     for (int i = 0; i < 20; ++i) {
-        float s = sinf(t), c = cosf(t);
+        float s = dvg_sinf(t), c = dvg_cosf(t);
         float g = rx * dx * s - ry * dy * c + (ry * ry - rx * rx) * s * c;
         float gt = rx * dx * c + ry * dy * s + (ry * ry - rx * rx) * (c * c - s * s);
         if (fabsf(gt) < 1.0e-12f) break;
@@ -616,7 +624,7 @@ static __device__ __noinline__ float2 closest_point_ellipse(float cx, float cy, 
         }
         t = nx;
     }
-    float s = sinf(t), c = cosf(t);
+    float s = dvg_sinf(t), c = dvg_cosf(t);
     return make_float2(cx + sx * rx * c, cy + sy * ry * s);
 }
 __device__ __forceinline__ float rect_signed_distance(float2 p, float4 r) {  // shape.rs:188-201
@@ -797,13 +805,13 @@ __device__ __forceinline__ float filter_weight(int ft, float radius, float dx, f
     }
     if (ft == F_HANN) {
         float ndx = (dx / (2.0f * radius)) + 0.5f, ndy = (dy / (2.0f * radius)) + 0.5f;
-        float fx = 0.5f * (1.0f - cosf(2.0f * PI_F * ndx)), fy = 0.5f * (1.0f - cosf(2.0f * PI_F * ndy));
+        float fx = 0.5f * (1.0f - dvg_cosf(2.0f * PI_F * ndx)), fy = 0.5f * (1.0f - dvg_cosf(2.0f * PI_F * ndy));
         return fx * fy * (1.0f / (radius * radius));
     }
     if (ft == F_GAUSSIAN) {  // this library's Gaussian (sigma = radius/2, square support)
         float r2 = radius * radius;
         float q = dx * dx + dy * dy;
-        return (2.0f / (PI_F * r2)) * expf(-2.0f * q / r2);
+        return (2.0f / (PI_F * r2)) * dvg_expf(-2.0f * q / r2);
     }
     return 1.0f;
 }
@@ -825,11 +833,11 @@ __device__ __forceinline__ float d_filter_weight(int ft, float radius, float dx,
     }
     if (ft == F_HANN) {
         float ndx = (dx / (2.0f * radius)) + 0.5f, ndy = (dy / (2.0f * radius)) + 0.5f;
-        float fx = 0.5f * (1.0f - cosf(2.0f * PI_F * ndx)), fy = 0.5f * (1.0f - cosf(2.0f * PI_F * ndy));
+        float fx = 0.5f * (1.0f - dvg_cosf(2.0f * PI_F * ndx)), fy = 0.5f * (1.0f - dvg_cosf(2.0f * PI_F * ndy));
         float norm = 1.0f / (radius * radius);
         float d_fx = d_return * fy * norm, d_fy = d_return * fx * norm, d_norm = d_return * fx * fy;
-        float d_ndx = d_fx * 0.5f * sinf(2.0f * PI_F * ndx) * (2.0f * PI_F);
-        float d_ndy = d_fy * 0.5f * sinf(2.0f * PI_F * ndy) * (2.0f * PI_F);
+        float d_ndx = d_fx * 0.5f * dvg_sinf(2.0f * PI_F * ndx) * (2.0f * PI_F);
+        float d_ndy = d_fy * 0.5f * dvg_sinf(2.0f * PI_F * ndy) * (2.0f * PI_F);
         float tr = 2.0f * radius;
         return d_ndx * (-2.0f * dx / (tr * tr)) + d_ndy * (-2.0f * dy / (tr * tr)) +
                (-2.0f) * d_norm / ((radius * radius) * radius);
@@ -837,7 +845,7 @@ __device__ __forceinline__ float d_filter_weight(int ft, float radius, float dx,
     if (ft == F_GAUSSIAN) {
         float r2 = radius * radius;
         float q = dx * dx + dy * dy;
-        float w = (2.0f / (PI_F * r2)) * expf(-2.0f * q / r2);
+        float w = (2.0f / (PI_F * r2)) * dvg_expf(-2.0f * q / r2);
         return radius != 0.0f ? d_return * w * (4.0f * q / (r2 * radius) - 2.0f / radius) : 0.0f;
     }
     return 0.0f;

@@ -539,7 +539,7 @@ __device__ float2 sample_boundary_path(const DevScene& S, int shape, float path_
                 }
                 float ang = 2.0f * PI_F * t;
                 if (dir < 0.0f) {
-                    float2 o = make_float2(r0 * cosf(ang), r0 * sinf(ang));
+                    float2 o = make_float2(r0 * dvg_cosf(ang), r0 * dvg_sinf(ang));
                     *normal = nrm2(o);
                     *pdf /= 2.0f * PI_F * r0;
                     data->base_point_id = 0;
@@ -548,7 +548,7 @@ __device__ float2 sample_boundary_path(const DevScene& S, int shape, float path_
                     float2 p0 = S.points[po];
                     return make_float2(p0.x + o.x, p0.y + o.y);
                 }
-                float2 o = make_float2(r1 * cosf(ang), r1 * sinf(ang));
+                float2 o = make_float2(r1 * dvg_cosf(ang), r1 * dvg_sinf(ang));
                 *normal = nrm2(o);
                 *pdf /= 2.0f * PI_F * r1;
                 data->base_point_id = nb - 1;
@@ -669,7 +669,7 @@ __device__ bool sample_boundary_point(const DevScene& S, int shape, int group, f
         float r = fabsf(prm.z);
         if (r <= 0.0f) return false;
         float ang = 2.0f * PI_F * lt;
-        float2 o = make_float2(r * cosf(ang), r * sinf(ang));
+        float2 o = make_float2(r * dvg_cosf(ang), r * dvg_sinf(ang));
         normal = nrm2(o);
         pdf /= 2.0f * PI_F * r;
         out = make_float2(prm.x + o.x, prm.y + o.y);
@@ -677,7 +677,7 @@ __device__ bool sample_boundary_point(const DevScene& S, int shape, int group, f
         float rx = fabsf(prm.z), ry = fabsf(prm.w);
         if (rx <= 0.0f || ry <= 0.0f) return false;
         float ang = 2.0f * PI_F * lt;
-        float s = sinf(ang), c = cosf(ang);
+        float s = dvg_sinf(ang), c = dvg_cosf(ang);
         float dxdt = -rx * s * 2.0f * PI_F, dydt = ry * c * 2.0f * PI_F;
         normal = nrm2(make_float2(dydt, -dxdt));
         pdf /= sqrtf(dxdt * dxdt + dydt * dydt);
@@ -781,8 +781,8 @@ __device__ void accumulate_boundary(const DevScene& S, const GradPtrs& G, int sh
         add_if(dp + 0, n.x * contrib);
         add_if(dp + 1, n.y * contrib);
         float ang = 2.0f * PI_F * t;
-        add_if(dp + 2, cosf(ang) * n.x * contrib);
-        add_if(dp + 3, sinf(ang) * n.y * contrib);
+        add_if(dp + 2, dvg_cosf(ang) * n.x * contrib);
+        add_if(dp + 3, dvg_sinf(ang) * n.y * contrib);
     } else if (si.x == K_PATH) {
         float t2 = bd.t, tt = 1.0f - t2;
         int pid = bd.point_id;

@@ -549,10 +549,10 @@ __device__ void d_closest_point_ellipse(float4 prm, float2 pt, float2 d_cp, floa
     }
     float sx = lx < 0.0f ? -1.0f : 1.0f, sy = ly < 0.0f ? -1.0f : 1.0f;
     float x = fabsf(lx), y = fabsf(ly);
-    float t = atan2f(y * rx, x * ry);
+    float t = dvg_atan2f(y * rx, x * ry);
     float g_t = 0.0f;
     for (int i = 0; i < 20; ++i) {
-        float sn = sinf(t), cs = cosf(t);
+        float sn = dvg_sinf(t), cs = dvg_cosf(t);
         float gg = rx * x * sn - ry * y * cs + (ry * ry - rx * rx) * sn * cs;
         g_t = rx * x * cs + ry * y * sn + (ry * ry - rx * rx) * (cs * cs - sn * sn);
         if (fabsf(g_t) < 1.0e-12f) break;
@@ -563,7 +563,7 @@ __device__ void d_closest_point_ellipse(float4 prm, float2 pt, float2 d_cp, floa
         }
         t = nx;
     }
-    float sn = sinf(t), cs = cosf(t);
+    float sn = dvg_sinf(t), cs = dvg_cosf(t);
     float d_t = 0.0f;
     dr->x += d_cp.x * sx * cs;
     d_t += d_cp.x * sx * (-rx * sn);
