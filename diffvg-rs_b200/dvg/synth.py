@@ -15,6 +15,10 @@ PCG64 generator and a fixed seed).
                        paths (width U[2,4]), solid colours.
 * ``batched_scenes``   side in {128,256,512}, log-uniform shape count 4-1024 of
                        the plain mix, 4x4 spp.
+* ``primitives_scene`` 64x64: one of each primitive (circle, stroked ellipse,
+                       rotated rect, mixed-order closed path, open path with
+                       per-point thickness), linear / radial / solid paints,
+                       even-odd group with a shape-to-canvas transform.
 * ``large_scene``      1024x1024, 4x4 spp, 4096 closed cubic paths of 16
                        segments, 25% stroked (width U[0.5,8]), radial 3-stop
                        fills, group and shape transforms.
@@ -27,7 +31,7 @@ from typing import List, Tuple
 import numpy as np
 
 from .scene import (Circle, Color, Ellipse, Filter, FilterType, FillRule, GradientStop, LinearGradient, Mat3,
-                    Path, PathGeometry, RadialGradient, RenderOptions, Scene, Shape, ShapeGroup)
+                    Path, PathGeometry, RadialGradient, Rect, RenderOptions, Scene, Shape, ShapeGroup)
 
 
 def _closed_cubic(rng: np.random.Generator, nseg: int, lo, hi) -> Path:
@@ -208,4 +212,36 @@ def large_scene(seed: int = 0, width: int = 1024, height: int = 1024, num_paths:
         grp = ShapeGroup([i], fill, _solid(rng) if stroked else None)
         grp.set_shape_to_canvas(Mat3.translate(cx, cy).mul(Mat3.rotate(float(rng.uniform(0, 2 * math.pi)))))
         sc.groups.append(grp)
+    return sc
+
+
+def primitives_scene() -> Scene:
+    """Every primitive and paint kind once on a 64x64 canvas (edge-case coverage)."""
+    sc = Scene(64, 64)
+    sc.background = Color(0.9, 0.9, 0.9, 1.0)
+    sc.shapes.append(Shape(Circle((20.0, 20.0), 12.0)))
+    e = Shape(Ellipse((44.0, 24.0), (14.0, 8.0)))
+    e.stroke_width = 2.0
+    sc.shapes.append(e)
+    r = Shape(Rect((10.0, 36.0), (30.0, 58.0)))
+    r.transform = Mat3.rotate(0.3)
+    sc.shapes.append(r)
+    p = Path([1, 0, 2], [(36.0, 40.0), (60.0, 30.0), (58.0, 60.0), (40.0, 62.0), (30.0, 50.0), (38.0, 46.0)],
+             None, True, False)
+    ps = Shape(PathGeometry(p))
+    ps.stroke_width = 1.5
+    sc.shapes.append(ps)
+    open_path = Path([0, 0], [(4.0, 4.0), (30.0, 10.0), (60.0, 4.0)], [1.0, 3.0, 0.5], False, False)
+    os_ = Shape(PathGeometry(open_path))
+    os_.stroke_width = 1.0
+    sc.shapes.append(os_)
+    stops = [GradientStop(0.1, Color(1, 0, 0, 1)), GradientStop(0.6, Color(0, 1, 0, 0.7)),
+             GradientStop(0.9, Color(0, 0, 1, 1))]
+    sc.groups.append(ShapeGroup([0], LinearGradient((8.0, 8.0), (32.0, 30.0), stops), None))
+    sc.groups.append(ShapeGroup([1], RadialGradient((44.0, 24.0), (14.0, 9.0), stops), Color(0.1, 0.2, 0.3, 1.0)))
+    g = ShapeGroup([2, 3], Color(0.3, 0.6, 0.2, 0.6), Color(0.0, 0.0, 0.0, 0.9))
+    g.fill_rule = FillRule.EVEN_ODD
+    g.set_shape_to_canvas(Mat3.translate(2.0, -1.0).mul(Mat3.scale(1.05, 0.95)))
+    sc.groups.append(g)
+    sc.groups.append(ShapeGroup([4], None, Color(0.8, 0.1, 0.5, 1.0)))
     return sc

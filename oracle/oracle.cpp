@@ -3506,6 +3506,49 @@ extern "C" int oracle_render_backward_ex(const dvg_scene_desc* desc, const dvg_r
     return 0;
 }
 
+// The image the crate's render_backward differentiates: per pixel, the filter-
+// weighted average of the CPU sample colours (un-premultiplied per sample, as
+// backward/sampling.rs:76-224 returns them), with the weights gather_d_color
+// uses (backward/filters.rs:70-103).  It equals the forward image wherever every
+// sample of a pixel has alpha 1; pixels with no weight are 0.
+extern "C" int oracle_render_differentiated(const dvg_scene_desc* desc, const dvg_render_options* opts, float* out) {
+    Scene sc = decode(desc);
+    if (sc.w == 0 || sc.h == 0) return 0;
+    size_t npix = (size_t)sc.w * sc.h;
+    std::fill(out, out + 4 * npix, 0.0f);
+    SampleSpec sp = make_spec(opts);
+    SceneBvh bvh = build_scene_bvh(sc);
+    std::vector<float> wimg = build_weight_image(sc, sp);
+    uint64_t total = (uint64_t)npix * sp.sx_n * sp.sy_n;
+    int width = (int)sc.w, height = (int)sc.h;
+    int ri = to_i32(std::ceil(sc.filter_radius));
+    for (uint64_t idx = 0; idx < total; ++idx) {
+        V2 pt;
+        size_t pixel_index;
+        sample_position(sc, sp, idx, &pt, &pixel_index);
+        V2 npt = mk(pt.x / (float)sc.w, pt.y / (float)sc.h);
+        V4 bg = sample_background(sc, pixel_index);
+        V4 c = sp.prefilter ? sample_color_prefiltered(sc, bvh, npt, &bg, nullptr, nullptr, -1, pixel_index)
+                            : sample_color(sc, bvh, npt, &bg, nullptr, nullptr, nullptr, -1, pixel_index);
+        int x = to_i32(std::floor(pt.x)), y = to_i32(std::floor(pt.y));
+        for (int dy = -ri; dy <= ri; ++dy)
+            for (int dx = -ri; dx <= ri; ++dx) {
+                int xx = x + dx, yy = y + dy;
+                if (xx < 0 || yy < 0 || xx >= width || yy >= height) continue;
+                float ws = wimg[(size_t)yy * width + xx];
+                if (!(ws > 0.0f)) continue;
+                float w = compute_filter_weight(sc.filter_type, sc.filter_radius, (float)xx + 0.5f - pt.x,
+                                                (float)yy + 0.5f - pt.y);
+                float* o = out + 4 * ((size_t)yy * width + xx);
+                o[0] += (w / ws) * c.x;
+                o[1] += (w / ws) * c.y;
+                o[2] += (w / ws) * c.z;
+                o[3] += (w / ws) * c.w;
+            }
+    }
+    return 0;
+}
+
 extern "C" int oracle_render_backward(const dvg_scene_desc* desc, const dvg_render_options* opts,
                                       const dvg_backward_options* bopts, const float* d_render, dvg_grads* out) {
     return oracle_render_backward_ex(desc, opts, bopts, d_render, out, 3, 1, 0, 0);

@@ -29,6 +29,10 @@ int oracle_render(const dvg_scene_desc* desc, const dvg_render_options* opts, fl
 int oracle_sample_premultiplied(const dvg_scene_desc* desc, const dvg_render_options* opts,
                                 float px, float py, float* out4);
 
+/* The image render_backward differentiates (per-sample un-premultiplied colours,
+ * filter-weighted per pixel); test infrastructure for finite differences. */
+int oracle_render_differentiated(const dvg_scene_desc* desc, const dvg_render_options* opts, float* out);
+
 /* The crate's CPU render_backward (src/backward/render.rs:35-210).  grads are host
  * buffers that are overwritten (NULL parts skipped, sizes as in dvg.h).  bopts->rng
  * selects the boundary generator (PCG32 as the crate, or Philox4x32-10). */

@@ -52,6 +52,7 @@ def lib() -> C.CDLL:
         B = C.POINTER(BackwardOptionsC)
         fp = C.POINTER(C.c_float)
         L.oracle_render.argtypes = [D, R, fp]
+        L.oracle_render_differentiated.argtypes = [D, R, fp]
         L.oracle_sample_premultiplied.argtypes = [D, R, C.c_float, C.c_float, fp]
         L.oracle_render_backward.argtypes = [D, R, B, fp, C.POINTER(GradsC)]
         L.oracle_render_backward_ex.argtypes = [D, R, B, fp, C.POINTER(GradsC), C.c_int, C.c_int,
@@ -80,6 +81,17 @@ def render(scene: Scene, options: RenderOptions) -> np.ndarray:
     out = np.zeros(int(scene.width) * int(scene.height) * 4, np.float32)
     o = render_options_c(options)
     lib().oracle_render(ps.ref(), C.byref(o), _fp(out))
+    return out.reshape(int(scene.height), int(scene.width), 4)
+
+
+def render_differentiated(scene: Scene, options: RenderOptions) -> np.ndarray:
+    """The image render_backward differentiates: per pixel, the filter-weighted
+    average of per-sample un-premultiplied colours (equal to render() wherever
+    every sample of a pixel is opaque)."""
+    ps = pack_scene(scene)
+    out = np.zeros(int(scene.width) * int(scene.height) * 4, np.float32)
+    o = render_options_c(options)
+    lib().oracle_render_differentiated(ps.ref(), C.byref(o), _fp(out))
     return out.reshape(int(scene.height), int(scene.width), 4)
 
 

@@ -10,8 +10,7 @@ import pytest
 
 import pyoracle as orc
 from dvg import BackwardOptions, Color, Renderer, RenderOptions, Rng, synth
-from dvg.scene import (Circle, Ellipse, FillRule, LinearGradient, GradientStop, Mat3, Path, PathGeometry,
-                       RadialGradient, Rect, Scene, Shape, ShapeGroup)
+from dvg.scene import Scene
 
 pytestmark = pytest.mark.gpu
 
@@ -85,34 +84,7 @@ def test_render_edge_cases(renderer):
 
 
 def _primitives_scene():
-    sc = Scene(64, 64)
-    sc.background = Color(0.9, 0.9, 0.9, 1.0)
-    sc.shapes.append(Shape(Circle((20.0, 20.0), 12.0)))
-    e = Shape(Ellipse((44.0, 24.0), (14.0, 8.0)))
-    e.stroke_width = 2.0
-    sc.shapes.append(e)
-    r = Shape(Rect((10.0, 36.0), (30.0, 58.0)))
-    r.transform = Mat3.rotate(0.3)
-    sc.shapes.append(r)
-    p = Path([1, 0, 2], [(36.0, 40.0), (60.0, 30.0), (58.0, 60.0), (40.0, 62.0), (30.0, 50.0), (38.0, 46.0)],
-             None, True, False)
-    ps = Shape(PathGeometry(p))
-    ps.stroke_width = 1.5
-    sc.shapes.append(ps)
-    open_path = Path([0, 0], [(4.0, 4.0), (30.0, 10.0), (60.0, 4.0)], [1.0, 3.0, 0.5], False, False)
-    os_ = Shape(PathGeometry(open_path))
-    os_.stroke_width = 1.0
-    sc.shapes.append(os_)
-    stops = [GradientStop(0.1, Color(1, 0, 0, 1)), GradientStop(0.6, Color(0, 1, 0, 0.7)),
-             GradientStop(0.9, Color(0, 0, 1, 1))]
-    sc.groups.append(ShapeGroup([0], LinearGradient((8.0, 8.0), (32.0, 30.0), stops), None))
-    sc.groups.append(ShapeGroup([1], RadialGradient((44.0, 24.0), (14.0, 9.0), stops), Color(0.1, 0.2, 0.3, 1.0)))
-    g = ShapeGroup([2, 3], Color(0.3, 0.6, 0.2, 0.6), Color(0.0, 0.0, 0.0, 0.9))
-    g.fill_rule = FillRule.EVEN_ODD
-    g.set_shape_to_canvas(Mat3.translate(2.0, -1.0).mul(Mat3.scale(1.05, 0.95)))
-    sc.groups.append(g)
-    sc.groups.append(ShapeGroup([4], None, Color(0.8, 0.1, 0.5, 1.0)))
-    return sc
+    return synth.primitives_scene()
 
 
 def test_render_primitives_matches_oracle(renderer):
