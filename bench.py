@@ -355,6 +355,9 @@ def main():
         peak = float(json.load(open(peaks_path)).get("hbm_gbs", peak))
         peak_src = "measured"
     achieved = alg_bytes / (avg_ms / 1e3) / 1e9
+    # DRAM bytes (read + write) per launch from one ncu capture of this workload
+    # (profiles/k_*_mixed512.md); only the default workload has a capture.
+    ncu_traffic = {"interior": 7315200, "forward": 7385856, "boundary": 25160192} if args.workload == "mixed" else {}
     prof_json = {k: {"ms_per_step": v[0] / 3.0, "calls_per_step": v[1] / 3.0} for k, v in prof.items()}
 
     line = {
@@ -365,7 +368,10 @@ def main():
         "config": {**cfg, "boundary_samples": bopts.boundary_samples, "l2": "flushed between timed steps "
                    "(256 MiB write outside the timed events)", "parallelism": f"weak, {world} independent scene(s)"},
         "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
+                     "frac": achieved / peak, "traffic": ncu_traffic.get(name), "peak_source": peak_src,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch "
+                                       f"(profiles/k_{'boundary_eval' if name == 'boundary' else name}_mixed512.md)"
+                                       if name in ncu_traffic else None,
                      "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
                      "note": "compute-bound path (f64 root solves, divergent BVH walks); HBM roofline reported "
                              "as required, see profiles/ for the issue-slot view"},
