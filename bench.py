@@ -32,6 +32,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "diffvg-rs_b200"))
 
 from dvg import BackwardOptions, Batch, DeviceGrads, Renderer, synth  # noqa: E402
+from dvg.abi import pack_scene as synth_pack  # noqa: E402
 
 METRIC = "fwd+bwd Msamples/s (ms/iter), plain single-scene launch loop on one B200"
 UNIT = "Msamples/s"
@@ -171,11 +172,48 @@ def batched_vs_plain(r, dev, lib_stream, flush, count, steps, rank):
 
     t_plain = timed(plain_step)
     t_batch = timed(lambda: batch.step(True))
+
+    # Full optimisation step (forward, L2, backward, Adam lr 1e-2 on path points).
+    # Batched: Adam and the scene re-preparation run on device inside the graph.
+    # Plain: the crate's loop shape — per scene, host preparation + upload of the
+    # current points, the fused device call, gradient read-back and a host Adam.
+    batch.set_adam(1e-2, (0.9, 0.999), 1e-8, points=True)
+    t_batch_opt = timed(lambda: batch.step(True))
+    state = []
+    for up in ups:
+        pk = synth_pack(up.scene)
+        n = pk.arrays["pts"].size
+        state.append((up.scene, pk, np.zeros(n, np.float32), np.zeros(n, np.float32), [0]))
+
+    def plain_opt_step():
+        for k, (scene, pk, m, v, t) in enumerate(state):
+            _, tgt_b, out_b, loss_b, g = plain[k][0], plain[k][1], plain[k][2], plain[k][3], plain[k][4]
+            up = r.upload(scene, packed=pk)
+            up.fwd_bwd_l2_device(opts, bopts, tgt_b.data_ptr(), out_b.data_ptr(), loss_b.data_ptr(), g)
+            torch.cuda.synchronize(dev)
+            grad = g.tensors["d_points"][: m.size].cpu().numpy()
+            t[0] += 1
+            m *= 0.9
+            m += 0.1 * grad
+            v *= 0.999
+            v += 0.001 * grad * grad
+            denom = np.sqrt(v) / np.sqrt(1.0 - 0.999 ** t[0]) + 1e-8
+            pk.arrays["pts"] -= (1e-2 / (1.0 - 0.9 ** t[0])) * m / denom
+            up.close()
+
+    t_plain_opt = timed(plain_opt_step)
     samples = sum(s.width * s.height * 16 for s in scenes)
     out = {"scenes": count, "samples_per_step": samples,
            "batched_ms_per_step": t_batch, "plain_ms_per_step": t_plain,
            "scenes_per_s_batched_graph": count / (t_batch / 1e3), "scenes_per_s_plain_loop": count / (t_plain / 1e3),
            "msamples_per_s_batched": samples / (t_batch / 1e3) / 1e6, "speedup": t_plain / t_batch,
+           "optimisation_step": {
+               "batched_graph_ms": t_batch_opt, "plain_loop_ms": t_plain_opt,
+               "scenes_per_s_batched_graph": count / (t_batch_opt / 1e3),
+               "scenes_per_s_plain_loop": count / (t_plain_opt / 1e3), "speedup": t_plain_opt / t_batch_opt,
+               "what": "fwd + L2 + bwd + Adam(lr 1e-2) on path points per scene; batched = one graph replay with "
+                       "on-device Adam and scene re-preparation; plain = per scene host preparation + upload, "
+                       "fused device call, gradient read-back, host Adam"},
            "workload": "64 uneven scenes: side in {128,256,512}, log-uniform 4-1024 closed cubic paths (plain mix, "
                        "paths shrink as sqrt(16/n)), 4x4 spp, box r=0.5, W*H*spp boundary samples, fwd+L2+bwd"}
     batch.close()

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -103,6 +104,7 @@ struct dvg_scene {
     DevBuf grads;    // gradient arena (device)
     size_t grad_off[11] = {0};
     size_t grad_floats = 0;
+    size_t arena_bytes = 0;  // bytes of prepared tables in `arena`
     const float4* g_bbox = nullptr;
 };
 
@@ -164,6 +166,10 @@ dvg_status check_status(dvg_context* ctx) {
     if (st & ST_BVH_LIMIT) {
         CK(cudaMemsetAsync(ctx->status, 0, sizeof(unsigned), ctx->stream));
         return fail(DVG_ERR_DEVICE_LIMIT, "a BVH traversal exceeded its stack depth");
+    }
+    if (st & ST_REFIT_LAYOUT) {
+        CK(cudaMemsetAsync(ctx->status, 0, sizeof(unsigned), ctx->stream));
+        return fail(DVG_ERR_LAUNCH, "on-device scene re-preparation found a BVH layout it did not build");
     }
     return DVG_OK;
 }
@@ -282,7 +288,8 @@ dvg_status dvg_scene_upload(dvg_context* ctx, const dvg_scene_desc* desc, dvg_sc
            o_g_bbox = b.add(h.g_bbox), o_g_list = b.add(h.g_shape_list), o_gn_b = b.add(h.gn_bounds),
            o_gn_m = b.add(h.gn_meta), o_gl = b.add(h.gl_shapes), o_s_info = b.add(h.s_info),
            o_s_prm = b.add(h.s_params), o_s_inv = b.add(h.s_inv), o_s_x = b.add(h.s_xform),
-           o_s_sw = b.add(h.s_stroke), o_p_info = b.add(h.p_info), o_pn_b = b.add(h.pn_bounds),
+           o_s_sw = b.add(h.s_stroke), o_s_box = b.add(h.s_box), o_s_pm = b.add(h.s_padmul),
+           o_p_shape = b.add(h.p_shape), o_p_info = b.add(h.p_info), o_pn_b = b.add(h.pn_bounds),
            o_pn_m = b.add(h.pn_meta), o_pl = b.add(h.pl_segs), o_seg_p = b.add(h.seg_p), o_seg_r = b.add(h.seg_r),
            o_seg_m = b.add(h.seg_meta), o_pts = b.add(h.points), o_th = b.add(h.thickness), o_ncp = b.add(h.ncp),
            o_pi = b.add(h.paint_info), o_pp = b.add(h.paint_params), o_so = b.add(h.stop_offsets),
@@ -291,6 +298,7 @@ dvg_status dvg_scene_upload(dvg_context* ctx, const dvg_scene_desc* desc, dvg_sc
            o_pci = b.add(h.path_cdf_info), o_pcdf = b.add(h.path_cdf), o_ppmf = b.add(h.path_pmf),
            o_ppid = b.add(h.path_pid), o_plen = b.add(h.path_len_arr), o_bgi = b.add(h.bg_image);
     CK(sc->arena.reserve(b.data.size()));
+    sc->arena_bytes = b.data.size();
     CK(cudaMemcpyAsync(sc->arena.ptr, b.data.data(), b.data.size(), cudaMemcpyHostToDevice, ctx->stream));
     char* base = sc->arena.as<char>();
     DevScene& S = sc->dev;
@@ -321,6 +329,9 @@ dvg_status dvg_scene_upload(dvg_context* ctx, const dvg_scene_desc* desc, dvg_sc
     S.s_inv = (const float*)(base + o_s_inv);
     S.s_xform = (const float*)(base + o_s_x);
     S.s_stroke = (const float*)(base + o_s_sw);
+    S.s_box = (const float4*)(base + o_s_box);
+    S.s_padmul = (const float*)(base + o_s_pm);
+    S.p_shape = (const int*)(base + o_p_shape);
     S.p_info = (const int4*)(base + o_p_info);
     S.pn_bounds = (const float4*)(base + o_pn_b);
     S.pn_meta = (const int4*)(base + o_pn_m);
@@ -805,6 +816,11 @@ struct dvg_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     uint64_t steps = 0;
+    // on-device optimisation step (dvg_batch_set_adam)
+    bool adam = false;
+    AdamParams ap{};
+    DevBuf refit, adam_state, sort_ids, sort_keys, opt_step;
+    int max_params = 0, max_paths = 0, max_groups = 0;
 };
 
 namespace {
@@ -833,8 +849,26 @@ dvg_status batch_enqueue(dvg_batch* b) {
                                                b->bkey.as<int>(), b->bcounts.as<int>(), b->border.as<int>(),
                                                ctx->stream);
     ctx->launches += launch_pixels_batch(B, n, b->max_pixels, 2, ctx->stream);
+    if (b->adam) {
+        BatchEntry* Bm = b->entries.as<BatchEntry>();
+        const RefitEntry* R = b->refit.as<RefitEntry>();
+        ctx->launches += launch_adam_batch(Bm, R, n, b->max_params, b->ap, b->opt_step.as<int>(), ctx->stream);
+        ctx->launches += launch_refit_batch(Bm, R, n, b->max_paths, b->max_groups, ctx->status, ctx->stream);
+        for (dvg_scene* sc : b->scenes) {
+            int* counts = sc->tiles.as<int>();
+            int* offsets = counts + sc->dev.tiles_x * sc->dev.tiles_y;
+            ctx->launches += launch_binning(sc->dev, sc->g_bbox, counts, offsets, nullptr, ctx->stream);
+            ctx->launches += launch_binning(sc->dev, sc->g_bbox, counts, offsets, sc->entries.as<int>(), ctx->stream);
+        }
+    }
     CK(cudaGetLastError());
     return DVG_OK;
+}
+void batch_drop_graph(dvg_batch* b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
 }
 }  // namespace
 
@@ -878,7 +912,8 @@ extern "C" dvg_status dvg_batch_create(dvg_context* ctx, dvg_scene* const* scene
         e.tile_off = b->total_tiles;
         const uint64_t spp = (uint64_t)sp.sxn * sp.syn;
         e.nb = b->bopts.boundary_samples ? b->bopts.boundary_samples : (uint64_t)npix * spp;
-        if (!S.boundary_ok) e.nb = 0;
+        // (scenes without boundary tables draw no samples: the generator checks the flag,
+        // which the on-device optimisation step may turn on or off)
         e.b_off = b->total_bsamples;
         e.bseed = b->bopts.boundary_seed_from_options ? opts->seed : b->bopts.boundary_seed;
         e.rng = (int)b->bopts.rng;
@@ -947,8 +982,7 @@ extern "C" void dvg_batch_destroy(dvg_batch* b) {
     if (!b) return;
     cudaSetDevice(b->ctx->device);
     cudaStreamSynchronize(b->ctx->stream);
-    if (b->exec) cudaGraphExecDestroy(b->exec);
-    if (b->graph) cudaGraphDestroy(b->graph);
+    batch_drop_graph(b);
     delete b;
 }
 
@@ -1010,4 +1044,152 @@ extern "C" dvg_status dvg_batch_losses(dvg_batch* b, float* host_losses) {
                        ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return check_status(ctx);
+}
+
+extern "C" dvg_status dvg_batch_set_adam(dvg_batch* b, const dvg_adam_options* o) {
+    if (!b) return fail(DVG_ERR_INVALID_ARGUMENT, "null batch");
+    dvg_context* ctx = b->ctx;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    batch_drop_graph(b);
+    if (!o) {
+        b->adam = false;
+        return DVG_OK;
+    }
+    if (!(std::isfinite(o->lr) && o->lr >= 0.0f && o->beta1 >= 0.0f && o->beta1 < 1.0f && o->beta2 >= 0.0f &&
+          o->beta2 < 1.0f && std::isfinite(o->eps) && o->eps >= 0.0f) ||
+        (o->params & ~(uint32_t)(DVG_OPT_POINTS | DVG_OPT_PAINTS)) || !o->params)
+        return fail(DVG_ERR_INVALID_ARGUMENT, "invalid Adam options");
+    const int n = (int)b->scenes.size();
+    AdamParams ap{o->lr, o->beta1, o->beta2, o->eps, (o->params & DVG_OPT_POINTS) ? 1 : 0,
+                  (o->params & DVG_OPT_PAINTS) ? 1 : 0};
+    // Tile lists must hold any binning the moved geometry can produce: every group in
+    // every tile at worst.
+    for (int i = 0; i < n; ++i) {
+        dvg_scene* sc = b->scenes[i];
+        const size_t tiles = (size_t)sc->dev.tiles_x * sc->dev.tiles_y;
+        const size_t need = std::max<size_t>(tiles * (size_t)std::max(sc->dev.num_groups, 1), 1);
+        if (need > ((size_t)1 << 28))
+            return fail(DVG_ERR_DEVICE_LIMIT, "tile lists of an optimised scene would exceed 2^28 entries");
+        if (sc->entries.bytes < need * sizeof(int)) {
+            CK(sc->entries.reserve(need * sizeof(int)));
+            sc->dev.tile_entries = sc->entries.as<int>();
+            int* counts = sc->tiles.as<int>();
+            int* offsets = counts + tiles;
+            ctx->launches += launch_binning(sc->dev, sc->g_bbox, counts, offsets, nullptr, ctx->stream);
+            ctx->launches += launch_binning(sc->dev, sc->g_bbox, counts, offsets, sc->entries.as<int>(), ctx->stream);
+            CK(cudaGetLastError());
+        }
+        b->host_entries[i].S.tile_entries = sc->dev.tile_entries;
+    }
+    // Adam moments and sort scratch, one block per scene.
+    std::vector<size_t> st_off(n), so_off(n);
+    size_t st_total = 0, so_total = 0;
+    int max_params = 0, max_paths = 0, max_groups = 0;
+    for (int i = 0; i < n; ++i) {
+        const HostScene& h = b->scenes[i]->host;
+        const size_t np = ap.points ? 2 * (size_t)h.total_points : 0;
+        const size_t nq = ap.paints ? 4 * (size_t)h.num_paints : 0;
+        st_off[i] = st_total;
+        st_total += 2 * ((np + nq + 63) & ~(size_t)63);
+        const size_t sort_n = std::max(h.seg_meta.size() / 4, h.g_shape_list.size());
+        so_off[i] = so_total;
+        so_total += 2 * ((sort_n + 63) & ~(size_t)63);
+        max_params = std::max(max_params, (int)(np + nq));
+        max_paths = std::max(max_paths, (int)h.num_paths);
+        max_groups = std::max(max_groups, (int)h.num_groups);
+    }
+    CK(b->adam_state.reserve(std::max<size_t>(st_total, 64) * sizeof(float)));
+    CK(b->sort_ids.reserve(std::max<size_t>(so_total, 64) * sizeof(int)));
+    CK(b->sort_keys.reserve(std::max<size_t>(so_total, 64) * sizeof(float)));
+    CK(b->opt_step.reserve(sizeof(int)));
+    CK(cudaMemsetAsync(b->adam_state.ptr, 0, std::max<size_t>(st_total, 64) * sizeof(float), ctx->stream));
+    CK(cudaMemsetAsync(b->opt_step.ptr, 0, sizeof(int), ctx->stream));
+    std::vector<RefitEntry> re(n);
+    for (int i = 0; i < n; ++i) {
+        dvg_scene* sc = b->scenes[i];
+        const HostScene& h = sc->host;
+        const size_t np = ap.points ? 2 * (size_t)h.total_points : 0;
+        const size_t nq = ap.paints ? 4 * (size_t)h.num_paints : 0;
+        const size_t half = (np + nq + 63) & ~(size_t)63;
+        float* base = b->adam_state.as<float>() + st_off[i];
+        RefitEntry& r = re[i];
+        r.m_points = base;
+        r.v_points = base + half;
+        r.m_paints = base + np;
+        r.v_paints = base + half + np;
+        r.sort_n = (int)std::max(h.seg_meta.size() / 4, h.g_shape_list.size());
+        r.sort_ids = b->sort_ids.as<int>() + so_off[i];
+        r.sort_keys = b->sort_keys.as<float>() + so_off[i];
+        r.n_points = (int)h.total_points;
+        r.n_paints = (int)h.num_paints;
+        r.g_bbox = const_cast<float4*>(sc->g_bbox);
+    }
+    CK(b->refit.reserve(n * sizeof(RefitEntry)));
+    CK(cudaMemcpyAsync(b->refit.ptr, re.data(), n * sizeof(RefitEntry), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(b->entries.ptr, b->host_entries.data(), n * sizeof(BatchEntry), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    b->ap = ap;
+    b->max_params = max_params;
+    b->max_paths = max_paths;
+    b->max_groups = max_groups;
+    b->adam = true;
+    return DVG_OK;
+}
+
+extern "C" dvg_status dvg_batch_scene_params(dvg_batch* b, uint32_t index, float* host_points,
+                                             float* host_paint_params) {
+    if (!b || index >= b->scenes.size()) return fail(DVG_ERR_INVALID_ARGUMENT, "batch index out of range");
+    dvg_context* ctx = b->ctx;
+    CK(cudaSetDevice(ctx->device));
+    dvg_scene* sc = b->scenes[index];
+    const HostScene& h = sc->host;
+    if (host_points && h.total_points)
+        CK(cudaMemcpyAsync(host_points, sc->dev.points, 2 * (size_t)h.total_points * sizeof(float),
+                           cudaMemcpyDeviceToHost, ctx->stream));
+    if (host_paint_params && h.num_paints)
+        CK(cudaMemcpyAsync(host_paint_params, sc->dev.paint_params, 4 * (size_t)h.num_paints * sizeof(float),
+                           cudaMemcpyDeviceToHost, ctx->stream));
+    int ok = sc->dev.boundary_ok;
+    const BatchEntry* E = b->entries.as<BatchEntry>() + index;
+    CK(cudaMemcpyAsync(&ok, &E->S.boundary_ok, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    sc->dev.boundary_ok = ok;
+    b->host_entries[index].S.boundary_ok = ok;
+    return check_status(ctx);
+}
+
+extern "C" dvg_status dvg_scene_digest(dvg_context* ctx, dvg_scene* sc, uint64_t* digest) {
+    if (!ctx || !sc || !digest) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    CK(cudaSetDevice(ctx->device));
+    const int tiles = sc->dev.tiles_x * sc->dev.tiles_y;
+    std::vector<char> arena(sc->arena_bytes);
+    std::vector<int> tl(tiles > 0 ? 2 * (size_t)tiles + 1 : 0);
+    if (!arena.empty())
+        CK(cudaMemcpyAsync(arena.data(), sc->arena.ptr, arena.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    if (!tl.empty())
+        CK(cudaMemcpyAsync(tl.data(), sc->tiles.ptr, tl.size() * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    std::vector<int> entries(tiles > 0 ? (size_t)std::max(tl[2 * (size_t)tiles], 0) : 0);
+    if (!entries.empty()) {
+        CK(cudaMemcpyAsync(entries.data(), sc->entries.ptr, entries.size() * sizeof(int), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    uint64_t h = 1469598103934665603ull;  // FNV-1a, 64 bit
+    auto mix = [&h](const void* p, size_t n) {
+        const unsigned char* c = static_cast<const unsigned char*>(p);
+        for (size_t i = 0; i < n; ++i) {
+            h ^= c[i];
+            h *= 1099511628211ull;
+        }
+    };
+    mix(arena.data(), arena.size());
+    if (tiles > 0) mix(tl.data() + tiles, ((size_t)tiles + 1) * sizeof(int));  // offsets (counts are scratch)
+    mix(entries.data(), entries.size() * sizeof(int));
+    int flags[1] = {sc->dev.boundary_ok};
+    mix(flags, sizeof(flags));
+    *digest = h;
+    return DVG_OK;
 }

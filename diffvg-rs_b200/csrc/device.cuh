@@ -27,7 +27,7 @@ enum : int { F_BOX = 0, F_TENT = 1, F_PARABOLIC = 2, F_HANN = 3, F_GAUSSIAN = 4 
 enum : int { PF_CLOSED = 1, PF_APPROX = 2, PF_THICK = 4 };
 
 // Device status bits written by kernels (never a trap: the host reads them).
-enum : unsigned { ST_FRAGMENT_OVERFLOW = 1u, ST_BVH_LIMIT = 2u };
+enum : unsigned { ST_FRAGMENT_OVERFLOW = 1u, ST_BVH_LIMIT = 2u, ST_REFIT_LAYOUT = 4u };
 
 struct DevScene {
     int width, height;
@@ -52,8 +52,11 @@ struct DevScene {
     const float* s_inv;    // 6 per shape
     const float* s_xform;  // 9 per shape
     const float* s_stroke;
+    const float4* s_box;     // padded group-space bounds (scene re-preparation only)
+    const float* s_padmul;   // stroke-pad multiplier (scene re-preparation only)
     // paths
     const int4* p_info;  // 2 per path: (seg off, seg cnt, node off, node cnt), (pt off, pt cnt, ctrl off, flags)
+    const int* p_shape;  // shape id per path
     const float4* pn_bounds;
     const int4* pn_meta;
     const int* pl_segs;

@@ -58,6 +58,22 @@ struct BatchEntry {
     int rng;
 };
 
+// Per-scene state of the on-device optimisation step (Adam + scene re-preparation).
+struct RefitEntry {
+    float* m_points;  // Adam first / second moments, 2 per point
+    float* v_points;
+    float* m_paints;  // 4 per paint (NULL when paints are not optimised)
+    float* v_paints;
+    int* sort_ids;     // scratch: 2 * sort_n ints
+    float* sort_keys;  // scratch: 2 * sort_n floats
+    int sort_n;        // max(total segments, total group shape entries)
+    int n_points, n_paints;
+    float4* g_bbox;    // the scene's canvas-space group boxes (tile binning input)
+};
+struct AdamParams {
+    float lr, beta1, beta2, eps;
+    int points, paints;  // which parameter sets are stepped
+};
 
 // Launchers (all asynchronous on `stream`).  Each returns the number of kernels launched.
 int launch_binning(const DevScene& S, const float4* g_bbox, int* counts, int* offsets, int* entries_or_null,
@@ -91,6 +107,14 @@ int launch_interior_prefilter_batch(const BatchEntry* B, const int* item_scene, 
                                     cudaStream_t stream);
 int launch_boundary_batch(const BatchEntry* B, int nscenes, uint64_t total, int total_tiles, BSample* samples, int* key,
                           int* counts, int* order, cudaStream_t stream);
+// Optimisation step: Adam on the selected parameters of every scene, then the
+// scene tables that depend on path points are rebuilt in place (segments, path and
+// group BVHs, group canvas boxes, boundary-sampling tables).  Tile binning is
+// re-run per scene by the caller afterwards.
+int launch_adam_batch(BatchEntry* B, const RefitEntry* R, int nscenes, int max_params, const AdamParams& ap,
+                      int* step, cudaStream_t stream);
+int launch_refit_batch(BatchEntry* B, const RefitEntry* R, int nscenes, int max_paths, int max_groups,
+                       unsigned* status, cudaStream_t stream);
 int launch_l2(const float* img, const float* target, size_t n, float* d_render, float* loss, cudaStream_t stream);
 
 }  // namespace dvgb

@@ -200,6 +200,7 @@ dvg_status prepare_scene(const dvg_scene_desc* d, HostScene* out, std::string* e
     h.s_inv.assign(6 * (size_t)S, 0.0f);
     h.s_xform.assign(9 * (size_t)S, 0.0f);
     h.s_stroke.assign(S, 0.0f);
+    h.s_padmul.assign(S, 1.0f);
     std::vector<Box> shape_box(S, empty_box());
     for (uint32_t s = 0; s < S; ++s) {
         uint32_t kind = d->shape_kind[s];
@@ -264,6 +265,7 @@ dvg_status prepare_scene(const dvg_scene_desc* d, HostScene* out, std::string* e
                 }
             }
             path_index = (int32_t)(h.p_info.size() / 8);
+            h.p_shape.push_back((int32_t)s);
             // Segments in path order (src/distance/bvh.rs:255-364).
             std::vector<Seg> segs;
             size_t pid = 0;
@@ -336,13 +338,24 @@ dvg_status prepare_scene(const dvg_scene_desc* d, HostScene* out, std::string* e
             }
             uint32_t join = d->shape_stroke_join ? d->shape_stroke_join[s] : (uint32_t)DVG_JOIN_ROUND;
             float miter = d->shape_miter_limit ? d->shape_miter_limit[s] : 4.0f;
-            if (rad > 0.0f && join == DVG_JOIN_MITER) rad *= std::fmax(miter, 1.0f);
+            if (join == DVG_JOIN_MITER) h.s_padmul[s] = std::fmax(miter, 1.0f);
+            if (rad > 0.0f && join == DVG_JOIN_MITER) rad *= h.s_padmul[s];
             shape_box[s] = inflate(gb, rad);
             flags |= SF_HAS_BOUNDS;
         }
         h.s_info[4 * (size_t)s] = (int32_t)kind;
         h.s_info[4 * (size_t)s + 1] = flags;
         h.s_info[4 * (size_t)s + 2] = path_index;
+    }
+
+    h.s_box.assign(4 * (size_t)S, 0.0f);
+    for (uint32_t s = 0; s < S; ++s) {
+        const Box& b = shape_box[s];
+        float* o = &h.s_box[4 * (size_t)s];
+        o[0] = b.x0;
+        o[1] = b.y0;
+        o[2] = b.x1;
+        o[3] = b.y1;
     }
 
     // ---- paints
@@ -548,10 +561,11 @@ dvg_status prepare_scene(const dvg_scene_desc* d, HostScene* out, std::string* e
         if (d->shape_kind[s] != DVG_SHAPE_PATH) continue;
         float l = h.shape_len[s];
         uint32_t co = d->path_ctrl_offset[s], cc = d->path_ctrl_count[s];
-        if (l <= 0.0f || !std::isfinite(l) || cc == 0) continue;
+        if (cc == 0) continue;
+        const bool valid = l > 0.0f && std::isfinite(l);
         uint32_t po = d->path_point_offset[s], pc = d->path_point_count[s];
         bool closed = d->path_flags[s] & DVG_PATH_CLOSED;
-        float inv_length = 1.0f / l;
+        float inv_length = valid ? 1.0f / l : 0.0f;
         int32_t off = (int32_t)h.path_cdf.size();
         size_t pid = 0;
         float prev = 0.0f;
@@ -575,8 +589,8 @@ dvg_status prepare_scene(const dvg_scene_desc* d, HostScene* out, std::string* e
         }
         h.path_cdf_info[4 * (size_t)s] = off;
         h.path_cdf_info[4 * (size_t)s + 1] = (int32_t)cc;
-        h.path_cdf_info[4 * (size_t)s + 2] = 1;
-        h.path_len_arr[s] = l;
+        h.path_cdf_info[4 * (size_t)s + 2] = valid ? 1 : 0;
+        h.path_len_arr[s] = valid ? l : 0.0f;
     }
     return DVG_OK;
 }

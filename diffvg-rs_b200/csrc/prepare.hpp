@@ -48,10 +48,13 @@ struct HostScene {
     std::vector<float> s_inv;          // 6 per shape: inverse of Shape::transform (rows 0..1)
     std::vector<float> s_xform;        // 9 per shape
     std::vector<float> s_stroke;       // 1 per shape
+    std::vector<float> s_box;          // 4 per shape: padded group-space bounds (the group BVH's leaf boxes)
+    std::vector<float> s_padmul;       // 1 per shape: stroke-pad multiplier (miter limit for miter joins, else 1)
 
     // paths (one record per path shape)
     std::vector<int32_t> p_info;       // 8 per path: seg off, seg count, node off, node count,
                                        //             point off, point count, ctrl off, flags
+    std::vector<int32_t> p_shape;      // 1 per path: its shape id
     std::vector<float> pn_bounds;      // 4 per path-BVH node
     std::vector<int32_t> pn_meta;      // 4 per node: skip, leaf start (into pl_segs), count, right child
     std::vector<int32_t> pl_segs;      // leaf order: global segment index
@@ -73,7 +76,8 @@ struct HostScene {
     std::vector<float> shape_len;      // per shape
     std::vector<float> bcdf, bpmf;     // over (group, shape) pairs in group order
     std::vector<int32_t> b_shape, b_group;
-    std::vector<int32_t> path_cdf_info;  // 4 per shape: cdf offset, count, valid, 0
+    std::vector<int32_t> path_cdf_info;  // 4 per shape: cdf offset, count, valid, 0 (a slot for every path,
+                                         // so the tables can be rebuilt in place when points move)
     std::vector<float> path_cdf, path_pmf, path_len_arr;
     std::vector<int32_t> path_pid;       // point id per cdf entry
 };

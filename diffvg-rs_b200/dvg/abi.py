@@ -401,3 +401,32 @@ def unflatten_grads(scene: Scene, packed: PackedScene, buf: GradBuffers) -> Scen
     tr = buf["d_translation"]
     return SceneGrad(shapes, groups, float(buf["d_filter_radius"][0]), buf["d_background"].copy(),
                      None if bgi is None else bgi.copy(), None if tr is None else tr.copy(), buf)
+
+
+def scene_with_params(scene: Scene, packed: PackedScene, points: np.ndarray,
+                      paint_params: Optional[np.ndarray] = None) -> Scene:
+    """A copy of `scene` whose path points (flat [total_points, 2], as packed) and,
+    if given, paint parameters ([num_paints, 4], as packed) are replaced — e.g. with
+    the values a batch's on-device optimisation step reached."""
+    import copy
+
+    out = copy.deepcopy(scene)
+    pts = np.asarray(points, np.float32).reshape(-1, 2)
+    for si, shp in enumerate(out.shapes):
+        path = getattr(shp.geometry, "path", None)
+        if path is None:
+            continue
+        o = packed.path_point_offset[si]
+        path.points = [(float(x), float(y)) for x, y in pts[o:o + len(path.points)]]
+    if paint_params is not None:
+        pp = np.asarray(paint_params, np.float32).reshape(-1, 4)
+        for (gi, which), pi in packed.paint_of.items():
+            paint = getattr(out.groups[gi], which)
+            v = [float(x) for x in pp[pi]]
+            if isinstance(paint, Color):
+                paint.r, paint.g, paint.b, paint.a = v
+            elif isinstance(paint, LinearGradient):
+                paint.start, paint.end = (v[0], v[1]), (v[2], v[3])
+            elif isinstance(paint, RadialGradient):
+                paint.center, paint.radius = (v[0], v[1]), (v[2], v[3])
+    return out

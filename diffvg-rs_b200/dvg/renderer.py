@@ -43,8 +43,18 @@ EXPORTED = (
     "dvg_render_backward_device", "dvg_render", "dvg_render_backward", "dvg_fwd_bwd_l2_device",
     "dvg_context_launch_count", "dvg_context_stream", "dvg_context_set_profiling", "dvg_context_profile",
     "dvg_context_profile_reset", "dvg_batch_create", "dvg_batch_destroy", "dvg_batch_buffers", "dvg_batch_step",
-    "dvg_batch_losses", "dvg_render_device_noalloc",
+    "dvg_batch_losses", "dvg_render_device_noalloc", "dvg_batch_set_adam", "dvg_batch_scene_params",
+    "dvg_scene_digest",
 )
+
+
+class AdamOptionsC(C.Structure):
+    _fields_ = [("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float),
+                ("params", C.c_uint32)]
+
+
+OPT_POINTS = 1
+OPT_PAINTS = 2
 
 
 class RenderError(RuntimeError):
@@ -109,7 +119,12 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.dvg_batch_buffers.argtypes = [vp, C.c_uint32, C.POINTER(vp), C.POINTER(vp), Gp]
     L.dvg_batch_step.argtypes = [vp, C.c_int]
     L.dvg_batch_losses.argtypes = [vp, fp]
-    for name in ("dvg_batch_create", "dvg_batch_buffers", "dvg_batch_step", "dvg_batch_losses"):
+    L.dvg_batch_set_adam.argtypes = [vp, C.POINTER(AdamOptionsC)]
+    L.dvg_scene_digest.argtypes = [vp, vp, C.POINTER(C.c_uint64)]
+    L.dvg_scene_digest.restype = C.c_int
+    L.dvg_batch_scene_params.argtypes = [vp, C.c_uint32, fp, fp]
+    for name in ("dvg_batch_create", "dvg_batch_buffers", "dvg_batch_step", "dvg_batch_losses", "dvg_batch_set_adam",
+                 "dvg_batch_scene_params"):
         getattr(L, name).restype = C.c_int
     for name in ("dvg_context_create", "dvg_scene_upload", "dvg_render_host", "dvg_render_device",
                  "dvg_render_backward_host", "dvg_render_backward_device", "dvg_render", "dvg_render_backward",
@@ -176,10 +191,10 @@ class DeviceGrads:
 class UploadedScene:
     """A scene prepared and resident in HBM (dvg_scene_upload)."""
 
-    def __init__(self, renderer: "Renderer", scene: Scene):
+    def __init__(self, renderer: "Renderer", scene: Scene, packed: Optional[PackedScene] = None):
         self.renderer = renderer
         self.scene = scene
-        self.packed = pack_scene(scene)
+        self.packed = packed if packed is not None else pack_scene(scene)
         self.handle = C.c_void_p()
         _check(renderer.lib.dvg_scene_upload(renderer.ctx, self.packed.ref(), C.byref(self.handle)))
         renderer._children.add(self)
@@ -211,6 +226,12 @@ class UploadedScene:
         b = backward_options_c(bopts)
         _check(self.renderer.lib.dvg_render_backward_device(self.renderer.ctx, self.handle, C.byref(o), C.byref(b),
                                                             C.c_void_p(d_render_ptr), None, C.byref(grads.c)))
+
+    def digest(self) -> int:
+        """dvg_scene_digest: hash of the prepared device tables."""
+        out = C.c_uint64()
+        _check(self.renderer.lib.dvg_scene_digest(self.renderer.ctx, self.handle, C.byref(out)))
+        return int(out.value)
 
     def fwd_bwd_l2_device(self, options: RenderOptions, bopts: Optional[BackwardOptions], target_ptr: int,
                           out_ptr: Optional[int], loss_ptr: Optional[int], grads: DeviceGrads) -> None:
@@ -267,8 +288,10 @@ class Renderer:
             self.lib.dvg_context_profile_reset(self.ctx)
         return out
 
-    def upload(self, scene: Scene) -> UploadedScene:
-        return UploadedScene(self, scene)
+    def upload(self, scene: Scene, packed: Optional[PackedScene] = None) -> UploadedScene:
+        """dvg_scene_upload.  `packed`: a pack_scene(scene) result to upload instead of
+        packing again (e.g. after editing its arrays in place)."""
+        return UploadedScene(self, scene, packed)
 
     def render(self, scene: Scene, options: RenderOptions = None) -> Image:
         """Renderer::render (src/renderer/renderer.rs:39-545)."""
@@ -350,6 +373,24 @@ class Batch:
         out = np.zeros(len(self.scenes), np.float32)
         _check(self.renderer.lib.dvg_batch_losses(self.handle, _fp(out)))
         return out
+
+    def set_adam(self, lr: float = 1e-2, betas=(0.9, 0.999), eps: float = 1e-8, points: bool = True,
+                 paints: bool = False) -> None:
+        """Adds Adam + on-device scene re-preparation to every step (dvg_batch_set_adam);
+        lr=None clears it."""
+        if lr is None:
+            _check(self.renderer.lib.dvg_batch_set_adam(self.handle, None))
+            return
+        o = AdamOptionsC(lr, betas[0], betas[1], eps, (OPT_POINTS if points else 0) | (OPT_PAINTS if paints else 0))
+        _check(self.renderer.lib.dvg_batch_set_adam(self.handle, C.byref(o)))
+
+    def scene_params(self, index: int):
+        """(points [total_points, 2], paint params [num_paints, 4]) of scene `index` as stepped so far."""
+        d = self.scenes[index].packed.desc
+        pts = np.zeros(2 * d.total_points, np.float32)
+        pp = np.zeros(4 * d.num_paints, np.float32)
+        _check(self.renderer.lib.dvg_batch_scene_params(self.handle, index, _fp(pts), _fp(pp)))
+        return pts.reshape(-1, 2), pp.reshape(-1, 4)
 
     def close(self) -> None:
         if self.handle and self.renderer.ctx:

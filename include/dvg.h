@@ -261,6 +261,37 @@ dvg_status dvg_batch_step(dvg_batch* batch, int use_graph);
 /* Copies the per-scene L2 losses of the last step to host memory (synchronises). */
 dvg_status dvg_batch_losses(dvg_batch* batch, float* host_losses);
 
+/* On-device optimisation step (no counterpart in the crate, whose callers update
+ * parameters on the host and re-prepare the scene on every call).  Once set, every
+ * dvg_batch_step also runs, after the backward pass: Adam (PyTorch's default form,
+ * no weight decay) on the selected parameters of every scene, then rebuilds in
+ * place every scene table derived from path points — segments, path and group
+ * BVHs (the crate's median split, same leaf order), group canvas boxes, tile lists,
+ * boundary-sampling lengths and CDFs — exactly as a fresh dvg_scene_upload of the
+ * updated scene would build them.  The scenes' points / paint parameters are
+ * updated in place.  Setting (or clearing, opts = NULL) resets the Adam moments and
+ * step count and drops a captured graph (the next graph step recaptures).  Tile
+ * lists of the batch's scenes are grown to their worst case (every group in every
+ * tile); scenes for which that exceeds 2^28 entries return DVG_ERR_DEVICE_LIMIT. */
+enum { DVG_OPT_POINTS = 1u, DVG_OPT_PAINTS = 2u };
+typedef struct dvg_adam_options {
+    float lr, beta1, beta2, eps;
+    uint32_t params; /* DVG_OPT_POINTS | DVG_OPT_PAINTS */
+} dvg_adam_options;
+dvg_status dvg_batch_set_adam(dvg_batch* batch, const dvg_adam_options* opts);
+/* Current path points (2*total_points floats) and paint parameters (4*num_paints)
+ * of batch scene `index`, copied to host memory (either pointer may be NULL);
+ * synchronises, and brings the scene's own handle up to date so it can be rendered
+ * or differentiated outside the batch. */
+dvg_status dvg_batch_scene_params(dvg_batch* batch, uint32_t index, float* host_points, float* host_paint_params);
+
+/* 64-bit FNV-1a digest of an uploaded scene's prepared device tables (every table of
+ * the scene arena, the tile offsets and the used tile entries, the boundary flag).
+ * No counterpart in the crate: it lets a caller check that the on-device
+ * re-preparation of an optimised scene built exactly the tables a fresh
+ * dvg_scene_upload of the same parameters builds.  Synchronises. */
+dvg_status dvg_scene_digest(dvg_context* ctx, dvg_scene* scene, uint64_t* digest);
+
 /* Number of kernels this library launched on the context since creation. */
 uint64_t dvg_context_launch_count(const dvg_context* ctx);
 
