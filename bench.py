@@ -33,6 +33,7 @@ sys.path.insert(0, os.path.join(ROOT, "diffvg-rs_b200"))
 
 from dvg import BackwardOptions, Batch, DeviceGrads, Renderer, synth  # noqa: E402
 from dvg.abi import pack_scene as synth_pack  # noqa: E402
+from dvg.shard import max_over_ranks, rank_seed, weak_scaling_rate  # noqa: E402
 
 METRIC = "fwd+bwd Msamples/s (ms/iter), plain single-scene launch loop on one B200"
 UNIT = "Msamples/s"
@@ -135,7 +136,7 @@ def batched_vs_plain(r, dev, lib_stream, flush, count, steps, rank):
     CUDA-graph step against the loop of single-scene fused calls, same work."""
     import torch
 
-    scenes = synth.batched_scenes(seed=rank, count=count)
+    scenes = synth.batched_scenes(seed=rank_seed(0, rank), count=count)
     opts = synth.batched_options()
     bopts = BackwardOptions(boundary_samples=0)
     ups = [r.upload(s) for s in scenes]
@@ -281,7 +282,7 @@ def main():
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
-    sc, target_scene, opts, bopts, cfg = workload(args.workload, rank)
+    sc, target_scene, opts, bopts, cfg = workload(args.workload, rank_seed(0, rank))
     W, H = sc.width, sc.height
     spp = opts.samples_x * opts.samples_y
     samples = W * H * spp
@@ -324,12 +325,10 @@ def main():
     timed_launches = r.launch_count - launches_before
     step_ms = [a.elapsed_time(b) for a, b in evs]
     total_ms = float(sum(step_ms))
+    total_ms = max_over_ranks([total_ms], dev)[0]
     if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
         dist.barrier()
-    value = args.steps * samples * world / (total_ms / 1e3) / 1e6
+    value = weak_scaling_rate(args.steps * samples, world, total_ms) / 1e6
 
     # per-launcher device time (CUDA events inside the library), 3 extra untimed steps
     r.set_profiling(True)
@@ -350,14 +349,17 @@ def main():
         img_h = None
         for i in range(args.e2e_steps + 1):
             torch.cuda.synchronize(dev)
-            t0 = time.perf_counter()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(lib_stream)
             img_h = r.render(sc, opts).pixels
             d_render = 2.0 * (img_h - tgt_host)
             g = r.render_backward(sc, opts, bopts, d_render)
-            t1 = time.perf_counter()
+            e1.record(lib_stream)  # the calls block, so the events bracket host and device work
+            torch.cuda.synchronize(dev)
             if i > 0:  # first call pays the one-time allocation of scratch buffers
-                ts.append(t1 - t0)
-        e2e_s = float(np.median(ts))
+                ts.append(e0.elapsed_time(e1) / 1e3)
+        e2e_s = max_over_ranks([float(np.median(ts))], dev)[0]
         desc_bytes = sum(a.nbytes for a in up.packed.arrays.values())
         grad_bytes = int(g.buffers.flat().nbytes)
         e2e = {"value": samples * world / e2e_s / 1e6, "unit": UNIT,
@@ -369,10 +371,15 @@ def main():
     if args.batch_scenes > 0:
         batched = batched_vs_plain(r, dev, lib_stream, flush, args.batch_scenes, args.batch_steps, rank)
         if world > 1:
-            t = torch.tensor([batched["batched_ms_per_step"], batched["plain_ms_per_step"]], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            batched["batched_ms_per_step"], batched["plain_ms_per_step"] = float(t[0]), float(t[1])
+            o = batched["optimisation_step"]
+            mx = max_over_ranks([batched["batched_ms_per_step"], batched["plain_ms_per_step"],
+                                 o["batched_graph_ms"], o["plain_loop_ms"]], dev)
+            batched["batched_ms_per_step"], batched["plain_ms_per_step"] = mx[0], mx[1]
+            o["batched_graph_ms"], o["plain_loop_ms"] = mx[2], mx[3]
             n = batched["scenes"] * world
+            o["scenes_per_s_batched_graph"] = n / (mx[2] / 1e3)
+            o["scenes_per_s_plain_loop"] = n / (mx[3] / 1e3)
+            o["speedup"] = mx[3] / mx[2]
             batched["scenes_per_s_batched_graph"] = n / (batched["batched_ms_per_step"] / 1e3)
             batched["scenes_per_s_plain_loop"] = n / (batched["plain_ms_per_step"] / 1e3)
             batched["speedup"] = batched["plain_ms_per_step"] / batched["batched_ms_per_step"]
