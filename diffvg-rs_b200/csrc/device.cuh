@@ -208,7 +208,12 @@ __device__ __forceinline__ CPRes closest_line(float2 p, float ax, float ay, floa
     float cx = ax + abx * t, cy = ay + aby * t;
     return CPRes{cx, cy, t, len2(p.x - cx, p.y - cy)};
 }
-static __device__ __noinline__ CPRes closest_quad_approx(float2 pt, const float* q) {  // curve.rs:267-296
+static __device__ __noinline__ CPRes closest_quad_approx_v(float2 pt, float a0, float a1, float a2, float a3, float a4, float a5, float a6, float a7);
+__device__ __forceinline__ CPRes closest_quad_approx(float2 pt, const float* q) {
+    return closest_quad_approx_v(pt, q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7]);
+}
+static __device__ __noinline__ CPRes closest_quad_approx_v(float2 pt, float a0, float a1, float a2, float a3, float a4, float a5, float a6, float a7) {
+    const float q[8] = {a0, a1, a2, a3, a4, a5, a6, a7};  // curve.rs:267-296
     float b0x = q[0] - pt.x, b0y = q[1] - pt.y, b1x = q[2] - pt.x, b1y = q[3] - pt.y;
     float b2x = q[4] - pt.x, b2y = q[5] - pt.y;
     float a = b0x * b2y - b0y * b2x;
@@ -237,7 +242,12 @@ static __device__ __noinline__ CPRes closest_quad_approx(float2 pt, const float*
     float cx = q[0] * w0 + q[2] * w1 + q[4] * w2, cy = q[1] * w0 + q[3] * w1 + q[5] * w2;
     return CPRes{cx, cy, t, len2(pt.x - cx, pt.y - cy)};
 }
-static __device__ __noinline__ CPRes closest_quad(float2 pt, const float* q, bool approx) {  // curve.rs:26-78
+static __device__ __noinline__ CPRes closest_quad_v(float2 pt, float a0, float a1, float a2, float a3, float a4, float a5, float a6, float a7, bool approx);
+__device__ __forceinline__ CPRes closest_quad(float2 pt, const float* q, bool approx) {
+    return closest_quad_v(pt, q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], approx);
+}
+static __device__ __noinline__ CPRes closest_quad_v(float2 pt, float a0, float a1, float a2, float a3, float a4, float a5, float a6, float a7, bool approx) {
+    const float q[8] = {a0, a1, a2, a3, a4, a5, a6, a7};  // curve.rs:26-78
     if (approx) return closest_quad_approx(pt, q);
     float best_t = 0.0f, bx = q[0], by = q[1];
     float best = len2(pt.x - q[0], pt.y - q[1]);
@@ -279,7 +289,12 @@ static __device__ __noinline__ CPRes closest_quad(float2 pt, const float* q, boo
     }
     return CPRes{bx, by, best_t, best};
 }
-static __device__ __noinline__ CPRes closest_cubic_approx(float2 pt, const float* q) {  // curve.rs:81-119
+static __device__ __noinline__ CPRes closest_cubic_approx_v(float2 pt, float a0, float a1, float a2, float a3, float a4, float a5, float a6, float a7);
+__device__ __forceinline__ CPRes closest_cubic_approx(float2 pt, const float* q) {
+    return closest_cubic_approx_v(pt, q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7]);
+}
+static __device__ __noinline__ CPRes closest_cubic_approx_v(float2 pt, float a0, float a1, float a2, float a3, float a4, float a5, float a6, float a7) {
+    const float q[8] = {a0, a1, a2, a3, a4, a5, a6, a7};  // curve.rs:81-119
     float inv = 1.0f / 8.0f;
     float prevx = q[0], prevy = q[1], prev_t = 0.0f;
     float bx = q[0], by = q[1], best_t = 0.0f, best = len2(pt.x - q[0], pt.y - q[1]);
@@ -304,7 +319,12 @@ static __device__ __noinline__ CPRes closest_cubic_approx(float2 pt, const float
     }
     return CPRes{bx, by, best_t, best};
 }
-static __device__ __noinline__ CPRes closest_cubic(float2 pt, const float* q, bool approx) {  // curve.rs:124-264
+static __device__ __noinline__ CPRes closest_cubic_v(float2 pt, float a0, float a1, float a2, float a3, float a4, float a5, float a6, float a7, bool approx);
+__device__ __forceinline__ CPRes closest_cubic(float2 pt, const float* q, bool approx) {
+    return closest_cubic_v(pt, q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], approx);
+}
+static __device__ __noinline__ CPRes closest_cubic_v(float2 pt, float a0, float a1, float a2, float a3, float a4, float a5, float a6, float a7, bool approx) {
+    const float q[8] = {a0, a1, a2, a3, a4, a5, a6, a7};  // curve.rs:124-264
     if (approx) return closest_cubic_approx(pt, q);
     float best_t = 0.0f, bx = q[0], by = q[1];
     float best = len2(pt.x - q[0], pt.y - q[1]);
@@ -430,9 +450,9 @@ __device__ __forceinline__ float seg_radius(const SegGeom& s, float t) {  // clo
     return tt * tt * tt * s.r[0] + 3.0f * tt * tt * t * s.r[1] + 3.0f * tt * t * t * s.r[2] + t * t * t * s.r[3];
 }
 // winding.rs:118-192
-static __device__ __noinline__ int winding_segment(const SegGeom& s, float2 pt) {
-    const float* q = s.q;
-    if (s.kind == 0) {
+static __device__ __noinline__ int winding_segment_v(int kind, float a0, float a1, float a2, float a3, float a4, float a5, float a6, float a7, float2 pt) {
+    const float q[8] = {a0, a1, a2, a3, a4, a5, a6, a7};
+    if (kind == 0) {
         float dy = q[3] - q[1];
         if (fabsf(dy) <= 1.0e-8f) return 0;
         float t = (pt.y - q[1]) / dy;
@@ -442,7 +462,7 @@ static __device__ __noinline__ int winding_segment(const SegGeom& s, float2 pt) 
         }
         return 0;
     }
-    if (s.kind == 1) {
+    if (kind == 1) {
         double a = (double)(q[1] - 2.0f * q[3] + q[5]);
         double b = (double)(-2.0f * q[1] + 2.0f * q[3]);
         double c = (double)(q[1] - pt.y);
@@ -488,6 +508,9 @@ static __device__ __noinline__ int winding_segment(const SegGeom& s, float2 pt) 
         }
     }
     return w;
+}
+__device__ __forceinline__ int winding_segment(const SegGeom& s, float2 pt) {
+    return winding_segment_v(s.kind, s.q[0], s.q[1], s.q[2], s.q[3], s.q[4], s.q[5], s.q[6], s.q[7], pt);
 }
 
 // ------------------------------------------------------------------ exact-result culling
