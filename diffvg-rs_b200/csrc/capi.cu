@@ -91,6 +91,7 @@ struct dvg_context {
     unsigned* status = nullptr;  // device word
     DevBuf accum, wsum, image, d_render, target, loss, bg_grad, trans_grad;
     DevBuf bsamples, bkey, border, bcounts;  // boundary-pass scratch
+    DevBuf sdf, positions, dvalues;          // signed-distance host calls
     uint64_t launches = 0;
 };
 
@@ -458,8 +459,8 @@ dvg_status dvg_render_host(dvg_context* ctx, dvg_scene* scene, const dvg_render_
 
 // Backward on device buffers.  `have_weights`: ctx->wsum already holds this scene's weights.
 static dvg_status backward_core(dvg_context* ctx, dvg_scene* sc, const dvg_render_options* opts,
-                                const dvg_backward_options* bopts, const float* d_render, const GradPtrs& G,
-                                bool have_weights) {
+                                const dvg_backward_options* bopts, const float* d_render, const float* d_sdf,
+                                const GradPtrs& G, bool have_weights) {
     const DevScene& S = sc->dev;
     const size_t npix = (size_t)S.width * S.height;
     if (npix == 0) return DVG_OK;
@@ -513,6 +514,12 @@ static dvg_status backward_core(dvg_context* ctx, dvg_scene* sc, const dvg_rende
             Prof prof_(ctx, "interior");
             ctx->launches += launch_interior(S, sp, d_render, ctx->wsum.as<float>(), G, ctx->status, ctx->stream);
         }
+        CK(cudaGetLastError());
+    }
+    if (d_sdf && S.num_groups > 0) {  // the d_sdf_image part (src/renderer/backward_gpu.rs:512-520)
+        Prof prof_(ctx, "sdf_backward");
+        ctx->launches += launch_sdf_backward(S, sp, d_sdf, G, bopts && bopts->compute_translation && G.d_translation,
+                                             ctx->status, ctx->stream);
         CK(cudaGetLastError());
     }
     {
@@ -569,7 +576,6 @@ static dvg_status zero_grads(dvg_context* ctx, dvg_scene* sc, const GradPtrs& G)
 static dvg_status check_backward_args(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
                                       const float* d_sdf, const dvg_grads* grads) {
     if (!ctx || !scene || !grads) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
-    if (d_sdf) return fail(DVG_ERR_INVALID_ARGUMENT, "d_sdf_image is not supported by this library yet");
     dvg_status st = check_options(opts);
     if (st != DVG_OK) return st;
     const GradPtrs G = grads_from_user(grads);
@@ -592,7 +598,7 @@ dvg_status dvg_render_backward_device(dvg_context* ctx, dvg_scene* scene, const 
     if (!(d_render && scene->dev.bg_image)) G.d_background_image = nullptr;
     st = zero_grads(ctx, scene, grads_from_user(grads));
     if (st != DVG_OK) return st;
-    return backward_core(ctx, scene, opts, bopts, d_render, G, false);
+    return backward_core(ctx, scene, opts, bopts, d_render, d_sdf, G, false);
 }
 
 dvg_status dvg_render_backward_host(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
@@ -624,7 +630,13 @@ dvg_status dvg_render_backward_host(dvg_context* ctx, dvg_scene* scene, const dv
                            ctx->stream));
         dr = ctx->d_render.as<float>();
     }
-    st = backward_core(ctx, scene, opts, bopts, dr, G, false);
+    const float* ds = nullptr;
+    if (d_sdf && npix) {
+        CK(ctx->sdf.reserve(npix * sizeof(float)));
+        CK(cudaMemcpyAsync(ctx->sdf.ptr, d_sdf, npix * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+        ds = ctx->sdf.as<float>();
+    }
+    st = backward_core(ctx, scene, opts, bopts, dr, ds, G, false);
     if (st != DVG_OK) return st;
     struct Part {
         float* dst;
@@ -715,7 +727,7 @@ dvg_status dvg_fwd_bwd_l2_device(dvg_context* ctx, dvg_scene* scene, const dvg_r
     if (!scene->dev.bg_image) G.d_background_image = nullptr;
     st = zero_grads(ctx, scene, G);
     if (st != DVG_OK) return st;
-    return backward_core(ctx, scene, opts, bopts, ctx->d_render.as<float>(), G, true);
+    return backward_core(ctx, scene, opts, bopts, ctx->d_render.as<float>(), nullptr, G, true);
 }
 
 }  // extern "C"
@@ -1192,4 +1204,191 @@ extern "C" dvg_status dvg_scene_digest(dvg_context* ctx, dvg_scene* sc, uint64_t
     mix(flags, sizeof(flags));
     *digest = h;
     return DVG_OK;
+}
+
+// ------------------------------------------------------------------ signed distance field
+extern "C" dvg_status dvg_render_sdf_device(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
+                                            float* out) {
+    if (!ctx || !scene || !out) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    dvg_status st = check_options(opts);
+    if (st != DVG_OK) return st;
+    CK(cudaSetDevice(ctx->device));
+    const DevScene& S = scene->dev;
+    const size_t npix = (size_t)S.width * S.height;
+    if (npix == 0) return DVG_OK;
+    if (S.num_groups == 0) {
+        CK(cudaMemsetAsync(out, 0, npix * sizeof(float), ctx->stream));
+        return DVG_OK;
+    }
+    {
+        Prof prof_(ctx, "render_sdf");
+        ctx->launches += launch_render_sdf(S, sample_params(opts), out, ctx->status, ctx->stream);
+    }
+    CK(cudaGetLastError());
+    return DVG_OK;
+}
+
+extern "C" dvg_status dvg_render_sdf_host(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
+                                          float* out) {
+    if (!ctx || !scene || !out) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    CK(cudaSetDevice(ctx->device));
+    const size_t npix = (size_t)scene->dev.width * scene->dev.height;
+    if (npix == 0) return check_options(opts);
+    CK(ctx->sdf.reserve(npix * sizeof(float)));
+    dvg_status st = dvg_render_sdf_device(ctx, scene, opts, ctx->sdf.as<float>());
+    if (st != DVG_OK) return st;
+    CK(cudaMemcpyAsync(out, ctx->sdf.ptr, npix * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return check_status(ctx);
+}
+
+extern "C" dvg_status dvg_render_sdf(dvg_context* ctx, const dvg_scene_desc* desc, const dvg_render_options* opts,
+                                     float* out) {
+    if (!ctx || !desc || !out) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    dvg_status st = check_options(opts);
+    if (st != DVG_OK) return st;
+    dvg_scene* sc = nullptr;
+    st = dvg_scene_upload(ctx, desc, &sc);
+    if (st != DVG_OK) return st;
+    st = dvg_render_sdf_host(ctx, sc, opts, out);
+    dvg_scene_destroy(sc);
+    return st;
+}
+
+extern "C" dvg_status dvg_eval_positions_device(dvg_context* ctx, dvg_scene* scene, const float* positions,
+                                                uint64_t count, float* out) {
+    if (!ctx || !scene || (count && (!positions || !out))) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    CK(cudaSetDevice(ctx->device));
+    if (count == 0) return DVG_OK;
+    if (scene->dev.num_groups == 0) {
+        CK(cudaMemsetAsync(out, 0, count * sizeof(float), ctx->stream));
+        return DVG_OK;
+    }
+    {
+        Prof prof_(ctx, "eval_positions");
+        ctx->launches += launch_eval_positions(scene->dev, reinterpret_cast<const float2*>(positions), count, out,
+                                               ctx->status, ctx->stream);
+    }
+    CK(cudaGetLastError());
+    return DVG_OK;
+}
+
+extern "C" dvg_status dvg_eval_positions_host(dvg_context* ctx, dvg_scene* scene, const float* positions,
+                                              uint64_t count, float* out) {
+    if (!ctx || !scene || (count && (!positions || !out))) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    CK(cudaSetDevice(ctx->device));
+    if (count == 0) return DVG_OK;
+    CK(ctx->positions.reserve(count * 2 * sizeof(float)));
+    CK(ctx->dvalues.reserve(count * sizeof(float)));
+    CK(cudaMemcpyAsync(ctx->positions.ptr, positions, count * 2 * sizeof(float), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    dvg_status st = dvg_eval_positions_device(ctx, scene, ctx->positions.as<float>(), count, ctx->dvalues.as<float>());
+    if (st != DVG_OK) return st;
+    CK(cudaMemcpyAsync(out, ctx->dvalues.ptr, count * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return check_status(ctx);
+}
+
+extern "C" dvg_status dvg_eval_positions(dvg_context* ctx, const dvg_scene_desc* desc, const float* positions,
+                                         uint64_t count, float* out) {
+    if (!ctx || !desc) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    if (count == 0) return DVG_OK;
+    dvg_scene* sc = nullptr;
+    dvg_status st = dvg_scene_upload(ctx, desc, &sc);
+    if (st != DVG_OK) return st;
+    st = dvg_eval_positions_host(ctx, sc, positions, count, out);
+    dvg_scene_destroy(sc);
+    return st;
+}
+
+extern "C" dvg_status dvg_eval_positions_backward_device(dvg_context* ctx, dvg_scene* scene,
+                                                         const dvg_backward_options* bopts, const float* positions,
+                                                         uint64_t count, const float* d_values, dvg_grads* grads) {
+    if (!ctx || !scene || !grads || (count && (!positions || !d_values)))
+        return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    CK(cudaSetDevice(ctx->device));
+    GradPtrs G = grads_from_user(grads);
+    const bool tr = bopts && bopts->compute_translation && G.d_translation;
+    if (!tr) G.d_translation = nullptr;
+    G.d_background_image = nullptr;
+    dvg_status st = zero_grads(ctx, scene, grads_from_user(grads));
+    if (st != DVG_OK) return st;
+    if (count == 0 || scene->dev.num_groups == 0) return DVG_OK;
+    {
+        Prof prof_(ctx, "positions_backward");
+        ctx->launches += launch_positions_backward(scene->dev, reinterpret_cast<const float2*>(positions), count,
+                                                   d_values, G, tr, ctx->status, ctx->stream);
+    }
+    CK(cudaGetLastError());
+    return DVG_OK;
+}
+
+extern "C" dvg_status dvg_eval_positions_backward_host(dvg_context* ctx, dvg_scene* scene,
+                                                       const dvg_backward_options* bopts, const float* positions,
+                                                       uint64_t count, const float* d_values, dvg_grads* grads) {
+    if (!ctx || !scene || !grads || (count && (!positions || !d_values)))
+        return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    CK(cudaSetDevice(ctx->device));
+    const HostScene& h = scene->host;
+    const size_t npix = (size_t)h.width * h.height;
+    GradPtrs G = device_grads(scene);
+    CK(cudaMemsetAsync(scene->grads.ptr, 0, scene->grad_floats * sizeof(float), ctx->stream));
+    const bool want_tr = bopts && bopts->compute_translation && grads->d_translation && npix;
+    G.d_background_image = nullptr;
+    G.d_translation = nullptr;
+    if (want_tr) {
+        CK(ctx->trans_grad.reserve(npix * 2 * sizeof(float)));
+        CK(cudaMemsetAsync(ctx->trans_grad.ptr, 0, npix * 2 * sizeof(float), ctx->stream));
+        G.d_translation = ctx->trans_grad.as<float>();
+    }
+    if (count && scene->dev.num_groups > 0) {
+        CK(ctx->positions.reserve(count * 2 * sizeof(float)));
+        CK(ctx->dvalues.reserve(count * sizeof(float)));
+        CK(cudaMemcpyAsync(ctx->positions.ptr, positions, count * 2 * sizeof(float), cudaMemcpyHostToDevice,
+                           ctx->stream));
+        CK(cudaMemcpyAsync(ctx->dvalues.ptr, d_values, count * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+        Prof prof_(ctx, "positions_backward");
+        ctx->launches += launch_positions_backward(scene->dev, ctx->positions.as<float2>(), count,
+                                                   ctx->dvalues.as<float>(), G, want_tr, ctx->status, ctx->stream);
+        CK(cudaGetLastError());
+    }
+    struct Part {
+        float* dst;
+        const float* src;
+        size_t n;
+    } parts[] = {{grads->d_shape_params, G.d_shape_params, 4 * (size_t)h.num_shapes},
+                 {grads->d_shape_transform, G.d_shape_transform, 9 * (size_t)h.num_shapes},
+                 {grads->d_shape_stroke_width, G.d_shape_stroke_width, h.num_shapes},
+                 {grads->d_points, G.d_points, 2 * (size_t)h.total_points},
+                 {grads->d_thickness, G.d_thickness, h.total_points},
+                 {grads->d_group_transform, G.d_group_transform, 9 * (size_t)h.num_groups},
+                 {grads->d_paint_params, G.d_paint_params, 4 * (size_t)h.num_paints},
+                 {grads->d_stop_offsets, G.d_stop_offsets, h.total_stops},
+                 {grads->d_stop_colors, G.d_stop_colors, 4 * (size_t)h.total_stops},
+                 {grads->d_filter_radius, G.d_filter_radius, 1},
+                 {grads->d_background, G.d_background, 4}};
+    for (auto& p : parts)
+        if (p.dst && p.n) CK(cudaMemcpyAsync(p.dst, p.src, p.n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    if (grads->d_background_image) std::memset(grads->d_background_image, 0, npix * 4 * sizeof(float));
+    if (grads->d_translation) {
+        if (want_tr)
+            CK(cudaMemcpyAsync(grads->d_translation, G.d_translation, npix * 2 * sizeof(float),
+                               cudaMemcpyDeviceToHost, ctx->stream));
+        else
+            std::memset(grads->d_translation, 0, npix * 2 * sizeof(float));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return check_status(ctx);
+}
+
+extern "C" dvg_status dvg_eval_positions_backward(dvg_context* ctx, const dvg_scene_desc* desc,
+                                                  const dvg_backward_options* bopts, const float* positions,
+                                                  uint64_t count, const float* d_values, dvg_grads* grads) {
+    if (!ctx || !desc || !grads) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    dvg_scene* sc = nullptr;
+    dvg_status st = dvg_scene_upload(ctx, desc, &sc);
+    if (st != DVG_OK) return st;
+    st = dvg_eval_positions_backward_host(ctx, sc, bopts, positions, count, d_values, grads);
+    dvg_scene_destroy(sc);
+    return st;
 }

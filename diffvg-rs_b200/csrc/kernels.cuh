@@ -115,6 +115,15 @@ int launch_adam_batch(BatchEntry* B, const RefitEntry* R, int nscenes, int max_p
                       int* step, cudaStream_t stream);
 int launch_refit_batch(BatchEntry* B, const RefitEntry* R, int nscenes, int max_paths, int max_groups,
                        unsigned* status, cudaStream_t stream);
+// Signed distance field: per-pixel mean over samples, per-point values, and the
+// adjoints of both (d_sdf image / per-point d_values) into G.
+int launch_render_sdf(const DevScene& S, const SampleParams& sp, float* out, unsigned* status, cudaStream_t stream);
+int launch_eval_positions(const DevScene& S, const float2* pos, uint64_t n, float* out, unsigned* status,
+                          cudaStream_t stream);
+int launch_sdf_backward(const DevScene& S, const SampleParams& sp, const float* d_sdf, const GradPtrs& G,
+                        bool translation, unsigned* status, cudaStream_t stream);
+int launch_positions_backward(const DevScene& S, const float2* pos, uint64_t n, const float* d_values,
+                              const GradPtrs& G, bool translation, unsigned* status, cudaStream_t stream);
 int launch_l2(const float* img, const float* target, size_t n, float* d_render, float* loss, cudaStream_t stream);
 
 }  // namespace dvgb

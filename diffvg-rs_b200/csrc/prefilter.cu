@@ -969,4 +969,142 @@ int launch_interior_prefilter_batch(const BatchEntry* B, const int* item_scene, 
     return 1;
 }
 
+
+// ------------------------------------------------------------------ signed distance field
+// The closest boundary over all groups, last group first, with a strict `<` between
+// groups (gpu/kernels/sdf.rs:8-115 forward, backward/sampling.rs:14-68 backward).
+// `init` is the starting bound: 1e20 in the crate's forward kernel, infinity in its
+// backward.  Every group is searched (the closest boundary may be far from the
+// point), pruned by each group's BVH against the best distance so far.
+__device__ bool sdf_closest(const DevScene& S, float2 pt, float init, ClosestD* best, int* group, unsigned* status) {
+    float best_dist = init;
+    bool found = false;
+    for (int g = S.num_groups - 1; g >= 0; --g) {
+        ClosestD h;
+        if (compute_distance_group(S, g, pt, best_dist, &h, status) && h.dist < best_dist) {
+            best_dist = h.dist;
+            *best = h;
+            *group = g;
+            found = true;
+        }
+    }
+    return found;
+}
+// Sign from the closest group's fill: negative inside (fill_inside_group / is_inside_bvh).
+__device__ __forceinline__ bool sdf_inside(const DevScene& S, int g, float2 pt) {
+    const int4 gi = __ldg(&S.g_info[g]);
+    return gi.x >= 0 && group_inside(S, g, xf9(S.g_c2s + 9 * g, pt), gi.z);
+}
+__device__ float sdf_signed(const DevScene& S, float2 pt, unsigned* status) {
+    ClosestD b;
+    int g = 0;
+    if (!sdf_closest(S, pt, 1.0e20f, &b, &g, status)) return 0.0f;
+    return sdf_inside(S, g, pt) ? -b.dist : b.dist;
+}
+
+// Renderer::render_sdf (gpu/kernels/sdf.rs:118-200): thread = pixel; mean signed
+// distance of the pixel's samples at the kernel's positions x + (sx + r) * (1/sx_n).
+__global__ void __launch_bounds__(256) k_render_sdf(DevScene S, SampleParams sp, float* out, unsigned* status) {
+    const int x = blockIdx.x * 16 + (threadIdx.x & 15), y = blockIdx.y * 16 + (threadIdx.x >> 4);
+    if (x >= S.width || y >= S.height) return;
+    const float inv_sx = 1.0f / (float)sp.sxn, inv_sy = 1.0f / (float)sp.syn;
+    float acc = 0.0f;
+    for (int sy = 0; sy < sp.syn; ++sy)
+        for (int sx = 0; sx < sp.sxn; ++sx) {
+            float rx = 0.5f, ry = 0.5f;
+            if (sp.jitter) {
+                const uint64_t idx = (((uint64_t)y * S.width + x) * sp.syn + sy) * sp.sxn + sx;
+                Pcg32 rng(idx, (uint64_t)sp.seed);
+                rx = rng.next_f32();
+                ry = rng.next_f32();
+            }
+            const float2 pt = make_float2((float)x + ((float)sx + rx) * inv_sx, (float)y + ((float)sy + ry) * inv_sy);
+            acc += sdf_signed(S, pt, status);
+        }
+    out[(size_t)y * S.width + x] = acc * (1.0f / (float)(sp.sxn * sp.syn));
+}
+
+// Renderer::eval_positions (gpu/kernels/sdf.rs:203-262): thread = point.
+__global__ void __launch_bounds__(256) k_eval_positions(DevScene S, const float2* pos, uint64_t n, float* out,
+                                                        unsigned* status) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = sdf_signed(S, pos[i], status);
+}
+
+// sample_distance (backward/sampling.rs:14-68) at one point with adjoint d_dist.
+__device__ __forceinline__ void sdf_adjoint(const DevScene& S, const GradPtrs& G, float2 pt, float d_dist,
+                                            int translation_pixel, unsigned* status) {
+    ClosestD b;
+    int g = 0;
+    if (!sdf_closest(S, pt, INF_F, &b, &g, status)) return;
+    const float d_abs = sdf_inside(S, g, pt) ? -d_dist : d_dist;
+    const float2 dpt = d_compute_distance(S, G, g, b.shape, pt, b.point, b.seg, b.t, d_abs);
+    if (translation_pixel >= 0 && G.d_translation) {
+        add_if(G.d_translation + 2 * (size_t)translation_pixel, -dpt.x);
+        add_if(G.d_translation + 2 * (size_t)translation_pixel + 1, -dpt.y);
+    }
+}
+
+// The d_sdf_image part of render_backward (backward/render.rs:95-188): thread = sample
+// at the CPU sample position; every sample passes its pixel's full d_sdf (the crate
+// does not divide it by the sample count).
+__global__ void __launch_bounds__(256) k_sdf_backward(DevScene S, SampleParams sp, const float* d_sdf, GradPtrs G,
+                                                      int translation, unsigned* status) {
+    const uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t spp = (uint64_t)sp.sxn * sp.syn;
+    if (idx >= (uint64_t)S.width * S.height * spp) return;
+    const int sx = (int)(idx % sp.sxn), sy = (int)((idx / sp.sxn) % sp.syn);
+    const uint64_t p = idx / spp;
+    const int x = (int)(p % S.width), y = (int)(p / S.width);
+    const float d = d_sdf[p];
+    if (d == 0.0f) return;
+    const float2 pt = sample_pos(x, y, sx, sy, sp.sxn, sp.syn, S.width, sp.seed, sp.jitter);
+    sdf_adjoint(S, G, pt, d, translation ? (int)p : -1, status);
+}
+
+// render_backward_positions (backward/render.rs:213-281): thread = point.
+__global__ void __launch_bounds__(256) k_positions_backward(DevScene S, const float2* pos, uint64_t n,
+                                                            const float* d_values, GradPtrs G, int translation,
+                                                            unsigned* status) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float d = d_values[i];
+    if (d == 0.0f) return;
+    const float2 pt = pos[i];
+    int tp = -1;
+    if (translation) {  // translation_index_for_point
+        const int x = f2i(pt.x), y = f2i(pt.y);
+        if (x >= 0 && y >= 0 && x < S.width && y < S.height) tp = y * S.width + x;
+    }
+    sdf_adjoint(S, G, pt, d, tp, status);
+}
+
+int launch_render_sdf(const DevScene& S, const SampleParams& sp, float* out, unsigned* status, cudaStream_t stream) {
+    if (S.width <= 0 || S.height <= 0) return 0;
+    dim3 grid((unsigned)((S.width + 15) / 16), (unsigned)((S.height + 15) / 16));
+    k_render_sdf<<<grid, 256, 0, stream>>>(S, sp, out, status);
+    return 1;
+}
+int launch_eval_positions(const DevScene& S, const float2* pos, uint64_t n, float* out, unsigned* status,
+                          cudaStream_t stream) {
+    if (n == 0) return 0;
+    k_eval_positions<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(S, pos, n, out, status);
+    return 1;
+}
+int launch_sdf_backward(const DevScene& S, const SampleParams& sp, const float* d_sdf, const GradPtrs& G,
+                        bool translation, unsigned* status, cudaStream_t stream) {
+    const uint64_t total = (uint64_t)S.width * S.height * sp.sxn * sp.syn;
+    if (total == 0) return 0;
+    k_sdf_backward<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(S, sp, d_sdf, G, translation ? 1 : 0, status);
+    return 1;
+}
+int launch_positions_backward(const DevScene& S, const float2* pos, uint64_t n, const float* d_values,
+                              const GradPtrs& G, bool translation, unsigned* status, cudaStream_t stream) {
+    if (n == 0) return 0;
+    k_positions_backward<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(S, pos, n, d_values, G,
+                                                                          translation ? 1 : 0, status);
+    return 1;
+}
+
 }  // namespace dvgb

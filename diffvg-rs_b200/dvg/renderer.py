@@ -44,7 +44,9 @@ EXPORTED = (
     "dvg_context_launch_count", "dvg_context_stream", "dvg_context_set_profiling", "dvg_context_profile",
     "dvg_context_profile_reset", "dvg_batch_create", "dvg_batch_destroy", "dvg_batch_buffers", "dvg_batch_step",
     "dvg_batch_losses", "dvg_render_device_noalloc", "dvg_batch_set_adam", "dvg_batch_scene_params",
-    "dvg_scene_digest",
+    "dvg_scene_digest", "dvg_render_sdf_host", "dvg_render_sdf_device", "dvg_render_sdf",
+    "dvg_eval_positions_host", "dvg_eval_positions_device", "dvg_eval_positions",
+    "dvg_eval_positions_backward_host", "dvg_eval_positions_backward_device", "dvg_eval_positions_backward",
 )
 
 
@@ -121,6 +123,19 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.dvg_batch_losses.argtypes = [vp, fp]
     L.dvg_batch_set_adam.argtypes = [vp, C.POINTER(AdamOptionsC)]
     L.dvg_scene_digest.argtypes = [vp, vp, C.POINTER(C.c_uint64)]
+    L.dvg_render_sdf_host.argtypes = [vp, vp, R, fp]
+    L.dvg_render_sdf_device.argtypes = [vp, vp, R, vp]
+    L.dvg_render_sdf.argtypes = [vp, D, R, fp]
+    L.dvg_eval_positions_host.argtypes = [vp, vp, fp, C.c_uint64, fp]
+    L.dvg_eval_positions_device.argtypes = [vp, vp, vp, C.c_uint64, vp]
+    L.dvg_eval_positions.argtypes = [vp, D, fp, C.c_uint64, fp]
+    L.dvg_eval_positions_backward_host.argtypes = [vp, vp, B, fp, C.c_uint64, fp, Gp]
+    L.dvg_eval_positions_backward_device.argtypes = [vp, vp, B, vp, C.c_uint64, vp, Gp]
+    L.dvg_eval_positions_backward.argtypes = [vp, D, B, fp, C.c_uint64, fp, Gp]
+    for name in ("dvg_render_sdf_host", "dvg_render_sdf_device", "dvg_render_sdf", "dvg_eval_positions_host",
+                 "dvg_eval_positions_device", "dvg_eval_positions", "dvg_eval_positions_backward_host",
+                 "dvg_eval_positions_backward_device", "dvg_eval_positions_backward"):
+        getattr(L, name).restype = C.c_int
     L.dvg_scene_digest.restype = C.c_int
     L.dvg_batch_scene_params.argtypes = [vp, C.c_uint32, fp, fp]
     for name in ("dvg_batch_create", "dvg_batch_buffers", "dvg_batch_step", "dvg_batch_losses", "dvg_batch_set_adam",
@@ -153,6 +168,15 @@ class Image:
     width: int
     height: int
     pixels: np.ndarray  # float32 [height, width, 4]
+
+
+@dataclass
+class SdfImage:
+    """SdfImage (src/renderer/types.rs): per-pixel signed distance, row-major."""
+
+    width: int
+    height: int
+    values: np.ndarray  # float32 [height, width]
 
 
 class DeviceGrads:
@@ -226,6 +250,11 @@ class UploadedScene:
         b = backward_options_c(bopts)
         _check(self.renderer.lib.dvg_render_backward_device(self.renderer.ctx, self.handle, C.byref(o), C.byref(b),
                                                             C.c_void_p(d_render_ptr), None, C.byref(grads.c)))
+
+    def render_sdf_device(self, options: RenderOptions, out_ptr: int) -> None:
+        """dvg_render_sdf_device into width*height floats of device memory."""
+        o = render_options_c(options)
+        _check(self.renderer.lib.dvg_render_sdf_device(self.renderer.ctx, self.handle, C.byref(o), C.c_void_p(out_ptr)))
 
     def digest(self) -> int:
         """dvg_scene_digest: hash of the prepared device tables."""
@@ -327,6 +356,45 @@ class Renderer:
         b = backward_options_c(bopts)
         _check(self.lib.dvg_render_backward(self.ctx, packed.ref(), C.byref(o), C.byref(b), _fp(dr), _fp(ds),
                                             C.byref(buf.c)))
+        return unflatten_grads(scene, packed, buf)
+
+
+    def render_sdf(self, scene: Scene, options: RenderOptions = None) -> SdfImage:
+        """Renderer::render_sdf (src/renderer/renderer.rs:586-716)."""
+        options = options or RenderOptions()
+        out = np.zeros((scene.height, scene.width), np.float32)
+        if scene.width == 0 or scene.height == 0:
+            return SdfImage(scene.width, scene.height, out.reshape(-1))
+        packed = pack_scene(scene)
+        o = render_options_c(options)
+        _check(self.lib.dvg_render_sdf(self.ctx, packed.ref(), C.byref(o), _fp(out)))
+        return SdfImage(scene.width, scene.height, out)
+
+    def eval_positions(self, scene: Scene, positions, options: RenderOptions = None) -> np.ndarray:
+        """Renderer::eval_positions (src/renderer/renderer.rs:719-848): signed distances at [n, 2] points."""
+        pos = np.ascontiguousarray(np.asarray(positions, np.float32).reshape(-1))
+        out = np.zeros(pos.size // 2, np.float32)
+        if out.size == 0:
+            return out
+        packed = pack_scene(scene)
+        _check(self.lib.dvg_eval_positions(self.ctx, packed.ref(), _fp(pos), out.size, _fp(out)))
+        return out
+
+    def eval_positions_backward(self, scene: Scene, positions, options: RenderOptions = None,
+                                backward_options: Optional[BackwardOptions] = None, d_sdf_values=None):
+        """Renderer::eval_positions_backward (src/renderer/renderer.rs:567-583) -> SceneGrad."""
+        bopts = backward_options or BackwardOptions()
+        pos = np.ascontiguousarray(np.asarray(positions, np.float32).reshape(-1))
+        n = pos.size // 2
+        if d_sdf_values is not None and np.asarray(d_sdf_values).size != n:
+            raise RenderError(DVG_ERR_INVALID_SCENE, "d_sdf_image size mismatch for eval_positions")
+        packed = pack_scene(scene)
+        buf = GradBuffers(packed, background_image=False, translation=bopts.compute_translation)
+        if d_sdf_values is not None and n:
+            d = np.ascontiguousarray(np.asarray(d_sdf_values, np.float32).reshape(-1))
+            b = backward_options_c(bopts)
+            _check(self.lib.dvg_eval_positions_backward(self.ctx, packed.ref(), C.byref(b), _fp(pos), n, _fp(d),
+                                                        C.byref(buf.c)))
         return unflatten_grads(scene, packed, buf)
 
 

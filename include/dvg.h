@@ -200,8 +200,10 @@ dvg_status dvg_render_device(dvg_context* ctx, dvg_scene* scene, const dvg_rende
 
 /* Renderer::render_backward (src/renderer/renderer.rs:548-564 ->
  * src/renderer/backward_gpu.rs:21-523) on an uploaded scene.
- * d_render: width*height*4 floats or NULL; d_sdf must be NULL (the SDF path is not
- * part of this library yet; passing it returns DVG_ERR_INVALID_ARGUMENT). */
+ * d_render: width*height*4 floats or NULL.  d_sdf: width*height floats or NULL, the
+ * adjoint of dvg_render_sdf; as in the crate (src/backward/render.rs:171-188), every
+ * sample of a pixel passes that pixel's full d_sdf to the closest-boundary adjoint
+ * (it is not divided by the sample count). */
 dvg_status dvg_render_backward_host(dvg_context* ctx, dvg_scene* scene,
                                     const dvg_render_options* opts,
                                     const dvg_backward_options* bopts,
@@ -210,6 +212,35 @@ dvg_status dvg_render_backward_device(dvg_context* ctx, dvg_scene* scene,
                                       const dvg_render_options* opts,
                                       const dvg_backward_options* bopts,
                                       const float* d_render, const float* d_sdf, dvg_grads* grads);
+
+/* Signed distance field.  Replaces Renderer::render_sdf (src/renderer/renderer.rs:586-716,
+ * src/gpu/kernels/sdf.rs:118-200): out = width*height floats, per pixel the mean over
+ * its samples of the signed distance to the closest boundary of any group (searched
+ * last group first), negative inside that group's fill; 0 without groups. */
+dvg_status dvg_render_sdf_host(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts, float* out);
+dvg_status dvg_render_sdf_device(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts, float* out);
+dvg_status dvg_render_sdf(dvg_context* ctx, const dvg_scene_desc* desc, const dvg_render_options* opts, float* out);
+/* Renderer::eval_positions (src/renderer/renderer.rs:719-848): the signed distance at
+ * `count` canvas points (positions: 2*count floats, x then y). */
+dvg_status dvg_eval_positions_host(dvg_context* ctx, dvg_scene* scene, const float* positions, uint64_t count,
+                                   float* out);
+dvg_status dvg_eval_positions_device(dvg_context* ctx, dvg_scene* scene, const float* positions, uint64_t count,
+                                     float* out);
+dvg_status dvg_eval_positions(dvg_context* ctx, const dvg_scene_desc* desc, const float* positions, uint64_t count,
+                              float* out);
+/* Renderer::eval_positions_backward -> render_backward_positions
+ * (src/renderer/renderer.rs:567-583, src/backward/render.rs:213-281): gradients of
+ * sum(d_values * sdf(positions)); points with d_value 0 are skipped; translation
+ * gradients land on the pixel containing the point. */
+dvg_status dvg_eval_positions_backward_host(dvg_context* ctx, dvg_scene* scene, const dvg_backward_options* bopts,
+                                            const float* positions, uint64_t count, const float* d_values,
+                                            dvg_grads* grads);
+dvg_status dvg_eval_positions_backward_device(dvg_context* ctx, dvg_scene* scene, const dvg_backward_options* bopts,
+                                              const float* positions, uint64_t count, const float* d_values,
+                                              dvg_grads* grads);
+dvg_status dvg_eval_positions_backward(dvg_context* ctx, const dvg_scene_desc* desc, const dvg_backward_options* bopts,
+                                       const float* positions, uint64_t count, const float* d_values,
+                                       dvg_grads* grads);
 
 /* Render of an uploaded scene that allocates no device memory.  No counterpart in
  * the crate: it exists for callers that cannot call cudaMalloc while rendering (a

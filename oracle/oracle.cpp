@@ -3506,6 +3506,140 @@ extern "C" int oracle_render_backward_ex(const dvg_scene_desc* desc, const dvg_r
     return 0;
 }
 
+// ---------------------------------------------------------------- signed distance field
+// Closest boundary over all groups, last group first (gpu/kernels/sdf.rs:8-115 for the
+// forward, backward/sampling.rs:14-68 for the backward; same search, strict `<`
+// between groups).  `init` is the starting bound: 1e20 in the GPU forward kernel,
+// infinity in the CPU backward.
+static bool sdf_closest(const Scene& sc, const SceneBvh& bvh, V2 pt, float init, ClosestPoint* best, size_t* group) {
+    float best_dist = init;
+    bool found = false;
+    for (size_t gi = sc.groups.size(); gi-- > 0;) {
+        ClosestPoint hit;
+        if (compute_distance_bvh(sc, bvh, gi, pt, best_dist, &hit) && hit.distance < best_dist) {
+            best_dist = hit.distance;
+            *best = hit;
+            *group = gi;
+            found = true;
+        }
+    }
+    return found;
+}
+static float sdf_signed(const Scene& sc, const SceneBvh& bvh, V2 pt) {  // compute_signed_distance
+    ClosestPoint best;
+    size_t g = 0;
+    if (!sdf_closest(sc, bvh, pt, 1.0e20f, &best, &g)) return 0.0f;
+    const bool inside = sc.groups[g].fill >= 0 && is_inside_bvh(sc, bvh, g, pt);
+    return inside ? -best.distance : best.distance;
+}
+// sample_distance (backward/sampling.rs:14-68): every sample passes the pixel's full
+// d_dist (the crate does not divide it by the sample count).
+static void sample_distance(const Scene& sc, const SceneBvh& bvh, V2 pt, float d_dist, Grads& g, long translation_index) {
+    ClosestPoint best;
+    size_t gi = 0;
+    if (!sdf_closest(sc, bvh, pt, INF_F, &best, &gi)) return;
+    const bool inside = sc.groups[gi].fill >= 0 && is_inside_bvh(sc, bvh, gi, pt);
+    const float d_abs = inside ? -d_dist : d_dist;
+    PathInfo pinfo = path_info_from_closest(sc, best.shape_index, best.path);
+    V2 d_pt = d_compute_distance(sc.groups[gi], gi, sc.shapes[best.shape_index], best.shape_index, pt, best.point, pinfo,
+                                 d_abs, g);
+    accumulate_translation(g, translation_index, d_pt * -1.0f);
+}
+
+// Renderer::render_sdf (renderer.rs:586-716, gpu/kernels/sdf.rs:118-200): per pixel the
+// mean signed distance of its samples, at the GPU kernel's sample positions
+// (x + (sx + r) * (1/sx_n)), jitter off when prefiltering.
+extern "C" int oracle_render_sdf(const dvg_scene_desc* desc, const dvg_render_options* opts, float* out) {
+    Scene sc = decode(desc);
+    const size_t npix = (size_t)sc.w * sc.h;
+    for (size_t i = 0; i < npix; ++i) out[i] = 0.0f;
+    if (npix == 0 || sc.groups.empty()) return 0;
+    SceneBvh bvh = build_scene_bvh(sc);
+    const uint32_t sxn = opts->samples_x ? opts->samples_x : 1, syn = opts->samples_y ? opts->samples_y : 1;
+    const bool jitter = !opts->use_prefiltering && opts->jitter;
+    const float inv_sx = 1.0f / (float)sxn, inv_sy = 1.0f / (float)syn;
+    const float inv_n = 1.0f / (float)(sxn * syn);
+    for (uint32_t y = 0; y < sc.h; ++y)
+        for (uint32_t x = 0; x < sc.w; ++x) {
+            float acc = 0.0f;
+            for (uint32_t sy = 0; sy < syn; ++sy)
+                for (uint32_t sx = 0; sx < sxn; ++sx) {
+                    float rx = 0.5f, ry = 0.5f;
+                    if (jitter) {
+                        uint64_t idx = (((uint64_t)y * sc.w + x) * syn + sy) * sxn + sx;
+                        Pcg32 rng(idx, (uint64_t)opts->seed);
+                        rx = rng.next_f32();
+                        ry = rng.next_f32();
+                    }
+                    V2 pt = mk((float)x + ((float)sx + rx) * inv_sx, (float)y + ((float)sy + ry) * inv_sy);
+                    acc += sdf_signed(sc, bvh, pt);
+                }
+            out[(size_t)y * sc.w + x] = acc * inv_n;
+        }
+    return 0;
+}
+
+// Renderer::eval_positions (renderer.rs:719-848, gpu/kernels/sdf.rs:203-262).
+extern "C" int oracle_eval_positions(const dvg_scene_desc* desc, const float* positions, uint64_t n, float* out) {
+    Scene sc = decode(desc);
+    if (sc.groups.empty()) {
+        for (uint64_t i = 0; i < n; ++i) out[i] = 0.0f;
+        return 0;
+    }
+    SceneBvh bvh = build_scene_bvh(sc);
+    for (uint64_t i = 0; i < n; ++i) out[i] = sdf_signed(sc, bvh, mk(positions[2 * i], positions[2 * i + 1]));
+    return 0;
+}
+
+// The d_sdf_image part of render_backward (backward/render.rs:171-188): every sample of
+// pixel p (CPU sample positions) passes d_sdf[p] to sample_distance.
+extern "C" int oracle_sdf_backward(const dvg_scene_desc* desc, const dvg_render_options* opts,
+                                   const dvg_backward_options* bopts, const float* d_sdf, dvg_grads* out) {
+    Scene sc = decode(desc);
+    bool translation = bopts && bopts->compute_translation;
+    Grads grads;
+    grads.init(sc, desc, false, translation);
+    if (sc.w && sc.h && d_sdf) {
+        SampleSpec sp = make_spec(opts);
+        SceneBvh bvh = build_scene_bvh(sc);
+        uint64_t total = (uint64_t)sc.w * sc.h * sp.sx_n * sp.sy_n;
+        for (uint64_t idx = 0; idx < total; ++idx) {
+            V2 pt;
+            size_t pixel;
+            sample_position(sc, sp, idx, &pt, &pixel);
+            sample_distance(sc, bvh, pt, d_sdf[pixel], grads, translation ? (long)pixel : -1);
+        }
+    }
+    finalize_background_gradients(sc, grads);
+    export_grads(grads, out, desc);
+    return 0;
+}
+
+// render_backward_positions (backward/render.rs:213-265).
+extern "C" int oracle_positions_backward(const dvg_scene_desc* desc, const dvg_backward_options* bopts,
+                                         const float* positions, uint64_t n, const float* d_values, dvg_grads* out) {
+    Scene sc = decode(desc);
+    bool translation = bopts && bopts->compute_translation;
+    Grads grads;
+    grads.init(sc, desc, false, translation);
+    if (n && d_values) {
+        SceneBvh bvh = build_scene_bvh(sc);
+        for (uint64_t i = 0; i < n; ++i) {
+            const float d = d_values[i];
+            if (d == 0.0f) continue;
+            V2 pt = mk(positions[2 * i], positions[2 * i + 1]);
+            long ti = -1;
+            if (translation) {  // translation_index_for_point (render.rs:267-281)
+                int32_t x = to_i32(pt.x), y = to_i32(pt.y);
+                if (x >= 0 && y >= 0 && x < (int32_t)sc.w && y < (int32_t)sc.h) ti = (long)y * (long)sc.w + x;
+            }
+            sample_distance(sc, bvh, pt, d, grads, ti);
+        }
+    }
+    export_grads(grads, out, desc);
+    return 0;
+}
+
 // The image the crate's render_backward differentiates: per pixel, the filter-
 // weighted average of the CPU sample colours (un-premultiplied per sample, as
 // backward/sampling.rs:76-224 returns them), with the weights gather_d_color

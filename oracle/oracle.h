@@ -33,6 +33,16 @@ int oracle_sample_premultiplied(const dvg_scene_desc* desc, const dvg_render_opt
  * filter-weighted per pixel); test infrastructure for finite differences. */
 int oracle_render_differentiated(const dvg_scene_desc* desc, const dvg_render_options* opts, float* out);
 
+/* Signed distance field (Renderer::render_sdf, src/renderer/renderer.rs:586), per-point
+ * signed distances (Renderer::eval_positions, :719), the d_sdf part of render_backward
+ * (src/backward/render.rs:171-188) and render_backward_positions (:213-265). */
+int oracle_render_sdf(const dvg_scene_desc* desc, const dvg_render_options* opts, float* out);
+int oracle_eval_positions(const dvg_scene_desc* desc, const float* positions, uint64_t n, float* out);
+int oracle_sdf_backward(const dvg_scene_desc* desc, const dvg_render_options* opts,
+                        const dvg_backward_options* bopts, const float* d_sdf, dvg_grads* grads);
+int oracle_positions_backward(const dvg_scene_desc* desc, const dvg_backward_options* bopts,
+                              const float* positions, uint64_t n, const float* d_values, dvg_grads* grads);
+
 /* The crate's CPU render_backward (src/backward/render.rs:35-210).  grads are host
  * buffers that are overwritten (NULL parts skipped, sizes as in dvg.h).  bopts->rng
  * selects the boundary generator (PCG32 as the crate, or Philox4x32-10). */

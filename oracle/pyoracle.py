@@ -53,6 +53,10 @@ def lib() -> C.CDLL:
         fp = C.POINTER(C.c_float)
         L.oracle_render.argtypes = [D, R, fp]
         L.oracle_render_differentiated.argtypes = [D, R, fp]
+        L.oracle_render_sdf.argtypes = [D, R, fp]
+        L.oracle_eval_positions.argtypes = [D, fp, C.c_uint64, fp]
+        L.oracle_sdf_backward.argtypes = [D, R, B, fp, C.POINTER(GradsC)]
+        L.oracle_positions_backward.argtypes = [D, B, fp, C.c_uint64, fp, C.POINTER(GradsC)]
         L.oracle_sample_premultiplied.argtypes = [D, R, C.c_float, C.c_float, fp]
         L.oracle_render_backward.argtypes = [D, R, B, fp, C.POINTER(GradsC)]
         L.oracle_render_backward_ex.argtypes = [D, R, B, fp, C.POINTER(GradsC), C.c_int, C.c_int,
@@ -127,6 +131,48 @@ def render_backward(scene: Scene, options: RenderOptions, bopts: Optional[Backwa
     lib().oracle_render_backward_ex(ps.ref(), C.byref(o), C.byref(b),
                                     _fp(dr) if dr is not None else C.cast(None, C.POINTER(C.c_float)),
                                     C.byref(buf.c), passes, threads, sample_begin, sample_end)
+    return unflatten_grads(scene, ps, buf), buf
+
+
+def render_sdf(scene: Scene, options: RenderOptions) -> np.ndarray:
+    """Renderer::render_sdf: per-pixel mean signed distance, [height, width]."""
+    ps = pack_scene(scene)
+    out = np.zeros(int(scene.width) * int(scene.height), np.float32)
+    o = render_options_c(options)
+    lib().oracle_render_sdf(ps.ref(), C.byref(o), _fp(out))
+    return out.reshape(int(scene.height), int(scene.width))
+
+
+def eval_positions(scene: Scene, positions) -> np.ndarray:
+    """Renderer::eval_positions: signed distance at each canvas point ([n, 2] -> [n])."""
+    ps = pack_scene(scene)
+    pos = np.ascontiguousarray(np.asarray(positions, np.float32).reshape(-1))
+    out = np.zeros(pos.size // 2, np.float32)
+    lib().oracle_eval_positions(ps.ref(), _fp(pos), out.size, _fp(out))
+    return out
+
+
+def sdf_backward(scene: Scene, options: RenderOptions, bopts: Optional[BackwardOptions], d_sdf: np.ndarray):
+    """The d_sdf_image part of the crate's render_backward; returns (SceneGrad, GradBuffers)."""
+    bopts = bopts or BackwardOptions()
+    ps = pack_scene(scene)
+    buf = GradBuffers(ps, background_image=False, translation=bopts.compute_translation)
+    o = render_options_c(options)
+    b = backward_options_c(bopts)
+    d = np.ascontiguousarray(np.asarray(d_sdf, np.float32).reshape(-1))
+    lib().oracle_sdf_backward(ps.ref(), C.byref(o), C.byref(b), _fp(d), C.byref(buf.c))
+    return unflatten_grads(scene, ps, buf), buf
+
+
+def eval_positions_backward(scene: Scene, positions, bopts: Optional[BackwardOptions], d_values):
+    """render_backward_positions; returns (SceneGrad, GradBuffers)."""
+    bopts = bopts or BackwardOptions()
+    ps = pack_scene(scene)
+    buf = GradBuffers(ps, background_image=False, translation=bopts.compute_translation)
+    b = backward_options_c(bopts)
+    pos = np.ascontiguousarray(np.asarray(positions, np.float32).reshape(-1))
+    d = np.ascontiguousarray(np.asarray(d_values, np.float32).reshape(-1))
+    lib().oracle_positions_backward(ps.ref(), C.byref(b), _fp(pos), d.size, _fp(d), C.byref(buf.c))
     return unflatten_grads(scene, ps, buf), buf
 
 
