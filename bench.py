@@ -31,7 +31,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "diffvg-rs_b200"))
 
-from dvg import BackwardOptions, Batch, DeviceGrads, Renderer, synth  # noqa: E402
+from dvg import BackwardOptions, Batch, DeviceGrads, Renderer, RenderOptions, synth  # noqa: E402
 from dvg.abi import pack_scene as synth_pack  # noqa: E402
 from dvg.shard import max_over_ranks, rank_seed, weak_scaling_rate  # noqa: E402
 
@@ -129,6 +129,45 @@ def cpu_baseline(sc, opts, bopts, target_img, img, seconds: float):
             "sample": f"{n} of {total} pixel samples spread evenly over the image (+ the same fraction of the "
                       f"{bopts.boundary_samples} boundary samples); set-up {setup:.2f}s amortised by that fraction",
             "ms_per_step_extrapolated": t * total / n * 1e3}
+
+
+def large_fit(r, dev, lib_stream, steps, warmup, rank):
+    """Large fitting loop: 1024x1024, 4x4 spp, 4096 closed cubic paths of 16 segments
+    (25 % stroked, radial 3-stop fills, group and shape transforms); every iteration
+    is one CUDA-graph replay of forward + L2 + backward + Adam (lr 1e-2 on points) +
+    on-device scene re-preparation, with no host work between iterations."""
+    import torch
+
+    sc = synth.large_scene(rank_seed(0, rank))
+    tgt_sc = synth.large_scene(rank_seed(1, rank) + 7)
+    opts = RenderOptions(samples_x=4, samples_y=4, seed=0, jitter=True, use_prefiltering=False)
+    up = r.upload(sc)
+    tu = r.upload(tgt_sc)
+    batch = Batch(r, [up], opts, BackwardOptions())
+    _, tgt, _ = batch.buffers(0)
+    tu.render_device(opts, tgt.data_ptr())
+    torch.cuda.synchronize(dev)
+    tu.close()
+    batch.set_adam(1e-2, (0.9, 0.999), 1e-8, points=True)
+    for _ in range(warmup):
+        batch.step(True)
+    first = float(batch.losses()[0])
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(lib_stream)
+    for _ in range(steps):
+        batch.step(True)
+    e1.record(lib_stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / steps
+    last = float(batch.losses()[0])
+    samples = sc.width * sc.height * 16
+    batch.close()
+    up.close()
+    return {"workload": "1024x1024, 4x4 spp, 4096 closed cubic paths x 16 segments, 25% stroked, radial 3-stop "
+                        "fills, W*H*spp boundary samples; fwd + L2 + bwd + Adam + re-preparation per graph replay",
+            "iterations": steps, "warmup": warmup, "ms_per_iter": ms, "msamples_per_s": samples / (ms / 1e3) / 1e6,
+            "loss_after_warmup": first, "loss_last": last}
 
 
 def batched_vs_plain(r, dev, lib_stream, flush, count, steps, rank):
@@ -263,6 +302,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-scenes", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=5)
+    ap.add_argument("--large-fit-steps", type=int, default=20)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -367,6 +407,12 @@ def main():
                "d2h_bytes_per_step": int(img_h.nbytes + grad_bytes), "ms_per_step": e2e_s * 1e3,
                "path": "dvg_render + dvg_render_backward (host buffers, per-call scene preparation)"}
 
+    fit = None
+    if args.large_fit_steps > 0:
+        fit = large_fit(r, dev, lib_stream, args.large_fit_steps, 3, rank)
+        if world > 1:
+            fit["ms_per_iter"] = max_over_ranks([fit["ms_per_iter"]], dev)[0]
+
     batched = None
     if args.batch_scenes > 0:
         batched = batched_vs_plain(r, dev, lib_stream, flush, args.batch_scenes, args.batch_steps, rank)
@@ -422,7 +468,7 @@ def main():
                              "as required, see profiles/ for the issue-slot view"},
         "kernel_ms_per_step": prof_json,
         "gpu_launches": int(timed_launches), "clocks": clocks.summary(), "e2e": e2e,
-        "batched_vs_plain": batched,
+        "batched_vs_plain": batched, "large_fit": fit,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         img = out.view(H, W, 4).cpu().numpy()

@@ -357,6 +357,62 @@ class SceneGrad:
     translation: Optional[np.ndarray]
     buffers: GradBuffers
 
+    def to_diffvg_layout(self, scene: Scene) -> "DiffvgSceneGrad":
+        return to_diffvg_layout(self, scene)
+
+
+@dataclass
+class DiffvgShapeGrad:
+    """src/grad.rs (DiffvgShapeGrad): geometry gradient with path metadata."""
+
+    geometry: dict
+    transform: np.ndarray
+    stroke_width: float
+
+
+@dataclass
+class DiffvgSceneGrad:
+    """src/grad.rs:451-466: the diffvg-compatible gradient layout."""
+
+    shapes: List[DiffvgShapeGrad]
+    shape_groups: List[DShapeGroup]
+    filter_radius: float
+    background: np.ndarray
+    background_image: Optional[np.ndarray]
+    translation: Optional[np.ndarray]
+
+
+def to_diffvg_layout(grad: "SceneGrad", scene: Scene) -> DiffvgSceneGrad:
+    """SceneGrad::to_diffvg_layout (src/grad.rs:474-553): path gradients carry the
+    path's control-point counts, closure and distance-approximation flag, and
+    per-point buffers take the source path's lengths (zero-padded or truncated)."""
+    shapes = []
+    for idx, ds in enumerate(grad.shapes):
+        g = dict(ds.geometry)
+        src = scene.shapes[idx].geometry if idx < len(scene.shapes) else None
+        if g["kind"] == "path":
+            path = getattr(src, "path", None)
+            if path is not None:
+                pts = np.zeros((len(path.points), 2), np.float32)
+                n = min(len(path.points), len(g["points"]))
+                pts[:n] = g["points"][:n]
+                th = g.get("thickness")
+                if path.thickness is not None:
+                    out_th = np.zeros(len(path.thickness), np.float32)
+                    if th is not None:
+                        m = min(len(out_th), len(th))
+                        out_th[:m] = th[:m]
+                    th = out_th
+                g = dict(kind="path", num_control_points=list(path.num_control_points), points=pts, thickness=th,
+                         is_closed=bool(path.is_closed), use_distance_approx=bool(path.use_distance_approx))
+            else:
+                g = dict(kind="path", num_control_points=[], points=g["points"], thickness=g.get("thickness"),
+                         is_closed=False, use_distance_approx=False)
+        shapes.append(DiffvgShapeGrad(g, ds.transform, ds.stroke_width))
+    groups = [DShapeGroup(gg.shape_to_canvas, gg.fill, gg.stroke) for gg in grad.shape_groups]
+    return DiffvgSceneGrad(shapes, groups, grad.filter_radius, grad.background, grad.background_image,
+                           grad.translation)
+
 
 def _paint_grad(kind_paint, buf: GradBuffers, pi: int, soff: int, scnt: int) -> dict:
     pp = buf["d_paint_params"][4 * pi: 4 * pi + 4].copy()
