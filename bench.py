@@ -302,7 +302,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-scenes", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=5)
-    ap.add_argument("--large-fit-steps", type=int, default=20)
+    ap.add_argument("--large-fit-steps", type=int, default=5)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
