@@ -360,6 +360,7 @@ dvg_status dvg_scene_upload(dvg_context* ctx, const dvg_scene_desc* desc, dvg_sc
     S.path_pid = (const int*)(base + o_ppid);
     S.path_len = (const float*)(base + o_plen);
     sc->g_bbox = (const float4*)(base + o_g_bbox);
+    S.g_bbox = sc->g_bbox;
     // tile binning
     S.tiles_x = (S.width + TILE - 1) / TILE;
     S.tiles_y = (S.height + TILE - 1) / TILE;
@@ -1391,4 +1392,41 @@ extern "C" dvg_status dvg_eval_positions_backward(dvg_context* ctx, const dvg_sc
     st = dvg_eval_positions_backward_host(ctx, sc, bopts, positions, count, d_values, grads);
     dvg_scene_destroy(sc);
     return st;
+}
+
+extern "C" dvg_status dvg_lbvh_build(dvg_context* ctx, const float* boxes, uint32_t count, uint64_t* keys_out,
+                                     int32_t* children_out, float* bounds_out) {
+    if (!ctx || (count && !boxes)) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    if (count > (1u << 24)) return fail(DVG_ERR_INVALID_ARGUMENT, "more than 2^24 boxes");
+    CK(cudaSetDevice(ctx->device));
+    if (count == 0) return DVG_OK;
+    const int n = (int)count;
+    const size_t padded = (size_t)lbvh_padded(n);
+    DevBuf buf;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        size_t o = (off + 255) & ~(size_t)255;
+        off = o + std::max<size_t>(bytes, 16);
+        return o;
+    };
+    const size_t o_box = take(sizeof(float4) * n), o_keys = take(padded * 8),
+                 o_child = take(sizeof(int2) * (size_t)std::max(n - 1, 0)), o_par = take(sizeof(int) * (2 * n - 1)),
+                 o_flag = take(sizeof(int) * (size_t)std::max(n - 1, 0)), o_bnd = take(sizeof(float4) * (2 * n - 1)),
+                 o_leaf = take(sizeof(int) * n), o_ext = take(sizeof(float4));
+    CK(buf.reserve(off));
+    char* b = buf.as<char>();
+    LbvhBufs L{(uint64_t*)(b + o_keys), (int2*)(b + o_child), (int*)(b + o_par), (int*)(b + o_flag),
+               (float4*)(b + o_bnd), (int*)(b + o_leaf), (float4*)(b + o_ext)};
+    CK(cudaMemcpyAsync(b + o_box, boxes, sizeof(float4) * n, cudaMemcpyHostToDevice, ctx->stream));
+    ctx->launches += launch_lbvh_build((const float4*)(b + o_box), n, nullptr, L, ctx->stream);
+    CK(cudaGetLastError());
+    if (keys_out) CK(cudaMemcpyAsync(keys_out, L.keys, 8 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+    if (children_out && n > 1)
+        CK(cudaMemcpyAsync(children_out, L.children, sizeof(int2) * (size_t)(n - 1), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    if (bounds_out)
+        CK(cudaMemcpyAsync(bounds_out, L.bounds, sizeof(float4) * (size_t)(2 * n - 1), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return DVG_OK;
 }

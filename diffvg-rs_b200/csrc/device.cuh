@@ -84,6 +84,7 @@ struct DevScene {
     const float* path_pmf;
     const int* path_pid;
     const float* path_len;
+    const float4* g_bbox;  // conservative canvas-space group boxes (binning, distance search skips)
     // tile binning
     int tiles_x, tiles_y;
     const int* tile_offsets;

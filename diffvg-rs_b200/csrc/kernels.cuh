@@ -75,6 +75,19 @@ struct AdamParams {
     int points, paints;  // which parameter sets are stepped
 };
 
+// Device buffers of one linear BVH over n boxes (lbvh.cu): keys[lbvh_padded(n)],
+// children[n-1], parent[2n-1], flags[n-1], bounds[2n-1], leaf_item[n], extent[1].
+struct LbvhBufs {
+    uint64_t* keys;
+    int2* children;
+    int* parent;
+    int* flags;
+    float4* bounds;
+    int* leaf_item;
+    float4* extent;
+};
+int lbvh_padded(int n);
+
 // Launchers (all asynchronous on `stream`).  Each returns the number of kernels launched.
 int launch_binning(const DevScene& S, const float4* g_bbox, int* counts, int* offsets, int* entries_or_null,
                    cudaStream_t stream);
@@ -124,6 +137,9 @@ int launch_sdf_backward(const DevScene& S, const SampleParams& sp, const float* 
                         bool translation, unsigned* status, cudaStream_t stream);
 int launch_positions_backward(const DevScene& S, const float2* pos, uint64_t n, const float* d_values,
                               const GradPtrs& G, bool translation, unsigned* status, cudaStream_t stream);
+// Linear BVH over n boxes into L (leaf_item[k] = item_map[box index], or the box
+// index without a map).
+int launch_lbvh_build(const float4* boxes, int n, const int* item_map, LbvhBufs& L, cudaStream_t stream);
 int launch_l2(const float* img, const float* target, size_t n, float* d_render, float* loss, cudaStream_t stream);
 
 }  // namespace dvgb

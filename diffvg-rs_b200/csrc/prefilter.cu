@@ -971,15 +971,22 @@ int launch_interior_prefilter_batch(const BatchEntry* B, const int* item_scene, 
 
 
 // ------------------------------------------------------------------ signed distance field
-// The closest boundary over all groups, last group first, with a strict `<` between
-// groups (gpu/kernels/sdf.rs:8-115 forward, backward/sampling.rs:14-68 backward).
-// `init` is the starting bound: 1e20 in the crate's forward kernel, infinity in its
-// backward.  Every group is searched (the closest boundary may be far from the
-// point), pruned by each group's BVH against the best distance so far.
-__device__ bool sdf_closest(const DevScene& S, float2 pt, float init, ClosestD* best, int* group, unsigned* status) {
+// The closest boundary over all groups (gpu/kernels/sdf.rs:8-115 forward,
+// backward/sampling.rs:14-68 backward): groups last to first, each searched with the
+// best distance so far as its bound and kept only when strictly closer; `init` is
+// the starting bound (1e20 in the crate's forward kernel, infinity in its backward).
+// The order matters: inside a group the crate prunes BVH nodes by their distance in
+// the group's local frame against that canvas-space bound, so a group whose
+// transform enlarges distances can return a different point under a different
+// bound; the loop therefore keeps the crate's order.  A group whose conservative
+// canvas box is farther than the bound is skipped without its transform (it cannot
+// return a point within the bound, which is all the crate's search would accept).
+__device__ bool sdf_closest(const DevScene& S, const float4* g_bbox, float2 pt, float init, ClosestD* best,
+                            int* group, unsigned* status) {
     float best_dist = init;
     bool found = false;
     for (int g = S.num_groups - 1; g >= 0; --g) {
+        if (box_distance(__ldg(&g_bbox[g]), pt) > best_dist) continue;
         ClosestD h;
         if (compute_distance_group(S, g, pt, best_dist, &h, status) && h.dist < best_dist) {
             best_dist = h.dist;
@@ -998,7 +1005,7 @@ __device__ __forceinline__ bool sdf_inside(const DevScene& S, int g, float2 pt) 
 __device__ float sdf_signed(const DevScene& S, float2 pt, unsigned* status) {
     ClosestD b;
     int g = 0;
-    if (!sdf_closest(S, pt, 1.0e20f, &b, &g, status)) return 0.0f;
+    if (!sdf_closest(S, S.g_bbox, pt, 1.0e20f, &b, &g, status)) return 0.0f;
     return sdf_inside(S, g, pt) ? -b.dist : b.dist;
 }
 
@@ -1037,7 +1044,7 @@ __device__ __forceinline__ void sdf_adjoint(const DevScene& S, const GradPtrs& G
                                             int translation_pixel, unsigned* status) {
     ClosestD b;
     int g = 0;
-    if (!sdf_closest(S, pt, INF_F, &b, &g, status)) return;
+    if (!sdf_closest(S, S.g_bbox, pt, INF_F, &b, &g, status)) return;
     const float d_abs = sdf_inside(S, g, pt) ? -d_dist : d_dist;
     const float2 dpt = d_compute_distance(S, G, g, b.shape, pt, b.point, b.seg, b.t, d_abs);
     if (translation_pixel >= 0 && G.d_translation) {

@@ -47,6 +47,7 @@ EXPORTED = (
     "dvg_scene_digest", "dvg_render_sdf_host", "dvg_render_sdf_device", "dvg_render_sdf",
     "dvg_eval_positions_host", "dvg_eval_positions_device", "dvg_eval_positions",
     "dvg_eval_positions_backward_host", "dvg_eval_positions_backward_device", "dvg_eval_positions_backward",
+    "dvg_lbvh_build",
 )
 
 
@@ -123,6 +124,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.dvg_batch_losses.argtypes = [vp, fp]
     L.dvg_batch_set_adam.argtypes = [vp, C.POINTER(AdamOptionsC)]
     L.dvg_scene_digest.argtypes = [vp, vp, C.POINTER(C.c_uint64)]
+    L.dvg_lbvh_build.argtypes = [vp, fp, C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(C.c_int32), fp]
+    L.dvg_lbvh_build.restype = C.c_int
     L.dvg_render_sdf_host.argtypes = [vp, vp, R, fp]
     L.dvg_render_sdf_device.argtypes = [vp, vp, R, vp]
     L.dvg_render_sdf.argtypes = [vp, D, R, fp]
@@ -358,6 +361,17 @@ class Renderer:
                                             C.byref(buf.c)))
         return unflatten_grads(scene, packed, buf)
 
+
+    def lbvh_build(self, boxes):
+        """dvg_lbvh_build on [n, 4] boxes: (sorted keys [n], children [n-1, 2], bounds [2n-1, 4])."""
+        b = np.ascontiguousarray(np.asarray(boxes, np.float32).reshape(-1, 4))
+        n = b.shape[0]
+        keys = np.zeros(n, np.uint64)
+        ch = np.zeros((max(n - 1, 0), 2), np.int32)
+        bounds = np.zeros((max(2 * n - 1, 0), 4), np.float32)
+        _check(self.lib.dvg_lbvh_build(self.ctx, _fp(b), n, keys.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                       ch.ctypes.data_as(C.POINTER(C.c_int32)), _fp(bounds)))
+        return keys, ch, bounds
 
     def render_sdf(self, scene: Scene, options: RenderOptions = None) -> SdfImage:
         """Renderer::render_sdf (src/renderer/renderer.rs:586-716)."""

@@ -323,6 +323,18 @@ dvg_status dvg_batch_scene_params(dvg_batch* batch, uint32_t index, float* host_
  * dvg_scene_upload of the same parameters builds.  Synchronises. */
 dvg_status dvg_scene_digest(dvg_context* ctx, dvg_scene* scene, uint64_t* digest);
 
+/* Linear BVH (Morton codes, bitonic key sort, Karras topology, bottom-up bounds) over
+ * `count` boxes (4 floats each: min x, min y, max x, max y), built on the GPU.  No
+ * counterpart in the crate, whose BVHs are median splits built on the host (the
+ * scene tables keep those: the crate's closest-point search breaks exact distance
+ * ties by their traversal order).  A building block for callers that need a BVH over
+ * many boxes built on the device; its tree equals a CPU build of the same steps.  Outputs (host memory, each may be NULL): keys_out[count] sorted keys
+ * (Morton code << 32 | box index), children_out[2*(count-1)] (left, right) of the
+ * internal nodes 0..count-2 (node ids >= count-1 are leaves count-1+k, k = sorted
+ * position), bounds_out[4*(2*count-1)].  At most 2^24 boxes.  Synchronises. */
+dvg_status dvg_lbvh_build(dvg_context* ctx, const float* boxes, uint32_t count, uint64_t* keys_out,
+                          int32_t* children_out, float* bounds_out);
+
 /* Number of kernels this library launched on the context since creation. */
 uint64_t dvg_context_launch_count(const dvg_context* ctx);
 

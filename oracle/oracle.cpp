@@ -3640,6 +3640,105 @@ extern "C" int oracle_positions_backward(const dvg_scene_desc* desc, const dvg_b
     return 0;
 }
 
+// ---------------------------------------------------------------- linear BVH (CPU twin)
+// The same steps as the library's GPU build (Karras 2012): 16-bit-per-axis Morton
+// codes of the box centres normalised to the centres' bounds (f32, no contraction),
+// keys code << 32 | index sorted ascending, per-node range / split from common prefix
+// lengths, bounds as exact unions.  Used to check the GPU tree bit for bit.
+static uint32_t lb_spread16(uint32_t v) {
+    v &= 0xffffu;
+    v = (v | (v << 8)) & 0x00ff00ffu;
+    v = (v | (v << 4)) & 0x0f0f0f0fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+static uint32_t lb_quantise(float c, float lo, float ext) {
+    float u = ext > 0.0f ? (c - lo) / ext : 0.0f;
+    u = std::fmin(std::fmax(u, 0.0f), 1.0f);
+    const float s = u * 65536.0f;
+    return s >= 65535.0f ? 65535u : (uint32_t)s;
+}
+static int lb_prefix(const std::vector<uint64_t>& k, int i, int j) {
+    if (j < 0 || j >= (int)k.size()) return -1;
+    return __builtin_clzll(k[i] ^ k[j]);
+}
+extern "C" int oracle_lbvh_build(const float* boxes, uint32_t count, uint64_t* keys_out, int32_t* children_out,
+                                 float* bounds_out) {
+    const int n = (int)count;
+    if (n == 0) return 0;
+    float x0 = INF_F, y0 = INF_F, x1 = -INF_F, y1 = -INF_F;
+    for (int i = 0; i < n; ++i) {
+        const float* b = boxes + 4 * i;
+        const float cx = (b[0] + b[2]) * 0.5f, cy = (b[1] + b[3]) * 0.5f;
+        x0 = std::fmin(x0, cx);
+        y0 = std::fmin(y0, cy);
+        x1 = std::fmax(x1, cx);
+        y1 = std::fmax(y1, cy);
+    }
+    std::vector<uint64_t> keys(n);
+    for (int i = 0; i < n; ++i) {
+        const float* b = boxes + 4 * i;
+        const float cx = (b[0] + b[2]) * 0.5f, cy = (b[1] + b[3]) * 0.5f;
+        const uint32_t code = lb_spread16(lb_quantise(cx, x0, x1 - x0)) | (lb_spread16(lb_quantise(cy, y0, y1 - y0)) << 1);
+        keys[i] = ((uint64_t)code << 32) | (uint32_t)i;
+    }
+    std::sort(keys.begin(), keys.end());
+    std::vector<int> left(std::max(n - 1, 0)), right(std::max(n - 1, 0));
+    for (int i = 0; i < n - 1; ++i) {
+        const int d = lb_prefix(keys, i, i + 1) - lb_prefix(keys, i, i - 1) >= 0 ? 1 : -1;
+        const int dmin = lb_prefix(keys, i, i - d);
+        int lmax = 2;
+        while (lb_prefix(keys, i, i + lmax * d) > dmin) lmax *= 2;
+        int l = 0;
+        for (int t = lmax / 2; t >= 1; t /= 2)
+            if (lb_prefix(keys, i, i + (l + t) * d) > dmin) l += t;
+        const int j = i + l * d;
+        const int dnode = lb_prefix(keys, i, j);
+        int s = 0;
+        for (int div = 2;; div *= 2) {
+            const int t = (l + div - 1) / div;
+            if (lb_prefix(keys, i, i + (s + t) * d) > dnode) s += t;
+            if (t <= 1) break;
+        }
+        const int gamma = i + s * d + (d < 0 ? -1 : 0);
+        left[i] = std::min(i, j) == gamma ? (n - 1) + gamma : gamma;
+        right[i] = std::max(i, j) == gamma + 1 ? (n - 1) + gamma + 1 : gamma + 1;
+    }
+    std::vector<float> bounds(4 * (size_t)(2 * n - 1), 0.0f);
+    for (int k = 0; k < n; ++k) {
+        const float* b = boxes + 4 * (keys[k] & 0xffffffffu);
+        for (int c = 0; c < 4; ++c) bounds[4 * (size_t)(n - 1 + k) + c] = b[c];
+    }
+    std::vector<int> stack, post;
+    if (n > 1) stack.push_back(0);
+    while (!stack.empty()) {  // post-order so children come before parents
+        const int v = stack.back();
+        stack.pop_back();
+        post.push_back(v);
+        if (left[v] < n - 1) stack.push_back(left[v]);
+        if (right[v] < n - 1) stack.push_back(right[v]);
+    }
+    for (size_t q = post.size(); q-- > 0;) {
+        const int v = post[q];
+        const float* a = &bounds[4 * (size_t)left[v]];
+        const float* b = &bounds[4 * (size_t)right[v]];
+        float* o = &bounds[4 * (size_t)v];
+        o[0] = std::fmin(a[0], b[0]);
+        o[1] = std::fmin(a[1], b[1]);
+        o[2] = std::fmax(a[2], b[2]);
+        o[3] = std::fmax(a[3], b[3]);
+    }
+    if (keys_out) std::memcpy(keys_out, keys.data(), 8 * (size_t)n);
+    if (children_out)
+        for (int i = 0; i < n - 1; ++i) {
+            children_out[2 * i] = left[i];
+            children_out[2 * i + 1] = right[i];
+        }
+    if (bounds_out) std::memcpy(bounds_out, bounds.data(), bounds.size() * sizeof(float));
+    return 0;
+}
+
 // The image the crate's render_backward differentiates: per pixel, the filter-
 // weighted average of the CPU sample colours (un-premultiplied per sample, as
 // backward/sampling.rs:76-224 returns them), with the weights gather_d_color

@@ -43,6 +43,10 @@ int oracle_sdf_backward(const dvg_scene_desc* desc, const dvg_render_options* op
 int oracle_positions_backward(const dvg_scene_desc* desc, const dvg_backward_options* bopts,
                               const float* positions, uint64_t n, const float* d_values, dvg_grads* grads);
 
+/* CPU twin of the library's linear BVH build (same outputs as dvg_lbvh_build). */
+int oracle_lbvh_build(const float* boxes, uint32_t count, uint64_t* keys_out, int32_t* children_out,
+                      float* bounds_out);
+
 /* The crate's CPU render_backward (src/backward/render.rs:35-210).  grads are host
  * buffers that are overwritten (NULL parts skipped, sizes as in dvg.h).  bopts->rng
  * selects the boundary generator (PCG32 as the crate, or Philox4x32-10). */

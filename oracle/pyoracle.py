@@ -54,6 +54,7 @@ def lib() -> C.CDLL:
         L.oracle_render.argtypes = [D, R, fp]
         L.oracle_render_differentiated.argtypes = [D, R, fp]
         L.oracle_render_sdf.argtypes = [D, R, fp]
+        L.oracle_lbvh_build.argtypes = [fp, C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(C.c_int32), fp]
         L.oracle_eval_positions.argtypes = [D, fp, C.c_uint64, fp]
         L.oracle_sdf_backward.argtypes = [D, R, B, fp, C.POINTER(GradsC)]
         L.oracle_positions_backward.argtypes = [D, B, fp, C.c_uint64, fp, C.POINTER(GradsC)]
@@ -174,6 +175,18 @@ def eval_positions_backward(scene: Scene, positions, bopts: Optional[BackwardOpt
     d = np.ascontiguousarray(np.asarray(d_values, np.float32).reshape(-1))
     lib().oracle_positions_backward(ps.ref(), C.byref(b), _fp(pos), d.size, _fp(d), C.byref(buf.c))
     return unflatten_grads(scene, ps, buf), buf
+
+
+def lbvh_build(boxes: np.ndarray):
+    """CPU twin of dvg_lbvh_build: (sorted keys [n], children [n-1, 2], bounds [2n-1, 4])."""
+    b = np.ascontiguousarray(np.asarray(boxes, np.float32).reshape(-1, 4))
+    n = b.shape[0]
+    keys = np.zeros(n, np.uint64)
+    ch = np.zeros((max(n - 1, 0), 2), np.int32)
+    bounds = np.zeros((max(2 * n - 1, 0), 4), np.float32)
+    lib().oracle_lbvh_build(_fp(b), n, keys.ctypes.data_as(C.POINTER(C.c_uint64)),
+                            ch.ctypes.data_as(C.POINTER(C.c_int32)), _fp(bounds))
+    return keys, ch, bounds
 
 
 def compute_distance(scene: Scene, group: int, pt, max_radius: float = float("inf"), use_bvh: bool = False):

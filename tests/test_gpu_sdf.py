@@ -90,3 +90,16 @@ def test_eval_positions_backward_matches_oracle(renderer):
         g = renderer.eval_positions_backward(sc, pos, None, bo, d).buffers
         _, ref = orc.eval_positions_backward(sc, pos, bo, d)
         _grad_check(g, ref)
+
+
+def test_sdf_many_groups_matches_oracle(renderer):
+    """200 groups: the closest-group search walks the linear BVH over group boxes."""
+    sc = synth.large_scene(2, 112, 96, 200)
+    opts = RenderOptions(samples_x=2, samples_y=1, seed=6, jitter=True, use_prefiltering=False)
+    assert _close(renderer.render_sdf(sc, opts).values, orc.render_sdf(sc, opts)) <= 1e-5
+    pos = np.random.default_rng(4).uniform(-20.0, 130.0, (400, 2)).astype(np.float32)
+    assert _close(renderer.eval_positions(sc, pos), orc.eval_positions(sc, pos)) <= 1e-5
+    d = np.random.default_rng(5).normal(0, 1, 400).astype(np.float32)
+    bo = BackwardOptions()
+    _grad_check(renderer.eval_positions_backward(sc, pos, None, bo, d).buffers,
+                orc.eval_positions_backward(sc, pos, bo, d)[1])
