@@ -170,12 +170,13 @@ def large_fit(r, dev, lib_stream, steps, warmup, rank):
             "loss_after_warmup": first, "loss_last": last}
 
 
-def batched_vs_plain(r, dev, lib_stream, flush, count, steps, rank):
-    """64 uneven scenes (sides 128/256/512, 4-1024 paths, 4x4 spp): one batched
-    CUDA-graph step against the loop of single-scene fused calls, same work."""
+def batched_vs_plain(r, dev, lib_stream, flush, scenes, steps, label):
+    """One batched CUDA-graph step over `scenes` against the loop of single-scene
+    calls doing the same work (forward + L2 + backward, then the full optimisation
+    step with Adam)."""
     import torch
 
-    scenes = synth.batched_scenes(seed=rank_seed(0, rank), count=count)
+    count = len(scenes)
     opts = synth.batched_options()
     bopts = BackwardOptions(boundary_samples=0)
     ups = [r.upload(s) for s in scenes]
@@ -254,8 +255,7 @@ def batched_vs_plain(r, dev, lib_stream, flush, count, steps, rank):
                "what": "fwd + L2 + bwd + Adam(lr 1e-2) on path points per scene; batched = one graph replay with "
                        "on-device Adam and scene re-preparation; plain = per scene host preparation + upload, "
                        "fused device call, gradient read-back, host Adam"},
-           "workload": "64 uneven scenes: side in {128,256,512}, log-uniform 4-1024 closed cubic paths (plain mix, "
-                       "paths shrink as sqrt(16/n)), 4x4 spp, box r=0.5, W*H*spp boundary samples, fwd+L2+bwd"}
+           "workload": label}
     batch.close()
     for u in ups + tgts:
         u.close()
@@ -415,7 +415,13 @@ def main():
 
     batched = None
     if args.batch_scenes > 0:
-        batched = batched_vs_plain(r, dev, lib_stream, flush, args.batch_scenes, args.batch_steps, rank)
+        batched = batched_vs_plain(
+            r, dev, lib_stream, flush, synth.batched_scenes(seed=rank_seed(0, rank), count=args.batch_scenes),
+            args.batch_steps, f"{args.batch_scenes} uneven scenes: side in {{128,256,512}}, log-uniform 4-1024 closed "
+            "cubic paths (plain mix, paths shrink as sqrt(16/n)), 4x4 spp, box r=0.5, W*H*spp boundary samples")
+        batched["small_scenes"] = batched_vs_plain(
+            r, dev, lib_stream, flush, synth.small_scenes(seed=rank_seed(2, rank), count=256), args.batch_steps,
+            "256 scenes of 64x64, 4-16 closed cubic paths (plain mix), 4x4 spp, box r=0.5, W*H*spp boundary samples")
         if world > 1:
             o = batched["optimisation_step"]
             mx = max_over_ranks([batched["batched_ms_per_step"], batched["plain_ms_per_step"],
@@ -426,6 +432,10 @@ def main():
             o["scenes_per_s_batched_graph"] = n / (mx[2] / 1e3)
             o["scenes_per_s_plain_loop"] = n / (mx[3] / 1e3)
             o["speedup"] = mx[3] / mx[2]
+            sm = batched["small_scenes"]
+            mx = max_over_ranks([sm["batched_ms_per_step"], sm["plain_ms_per_step"]], dev)
+            sm["batched_ms_per_step"], sm["plain_ms_per_step"] = mx[0], mx[1]
+            sm["speedup"] = mx[1] / mx[0]
             batched["scenes_per_s_batched_graph"] = n / (batched["batched_ms_per_step"] / 1e3)
             batched["scenes_per_s_plain_loop"] = n / (batched["plain_ms_per_step"] / 1e3)
             batched["speedup"] = batched["plain_ms_per_step"] / batched["batched_ms_per_step"]

@@ -189,6 +189,13 @@ def batched_scenes(seed: int = 0, count: int = 64) -> List[Scene]:
     return out
 
 
+def small_scenes(seed: int = 0, count: int = 256) -> List[Scene]:
+    """Many small scenes (64x64, 4-16 paths of the plain mix): the regime where one
+    batched graph replay replaces hundreds of short per-scene launches."""
+    rng = np.random.default_rng(seed)
+    return [plain_scene(int(rng.integers(0, 2 ** 31)), 64, 64, int(rng.integers(4, 17))) for _ in range(count)]
+
+
 def batched_options() -> RenderOptions:
     return RenderOptions(samples_x=4, samples_y=4, seed=0, jitter=True, use_prefiltering=False)
 
