@@ -329,47 +329,48 @@ __device__ __forceinline__ void interior_body(const DevScene& S, const SamplePar
     }
     if (!active) dcol = make_float4(0, 0, 0, 0);
 
-    // Pass 3: forward over the group list with the compositing adjoint (sampling.rs:175-210).
+    // Pass 3: forward over the fragments with the compositing adjoint (sampling.rs:175-210).
+    // The warp visits only the (group, stroke/fill) entries some lane hit: each round
+    // takes the smallest next fragment code over the warp, so lanes stay in step for
+    // the warp-reduced solid-paint gradients while entries nobody hit cost nothing.
     int cur = 0;
     float4 prev = bg;
-    for (int e = 0; e < n; ++e) {
+    while (true) {
+        const int mine = cur < nf ? code[cur] : 0x7fffffff;
+        const int nxt = __reduce_min_sync(0xffffffffu, mine);
+        if (nxt == 0x7fffffff) break;
+        const int e = nxt >> 1, which = nxt & 1;  // code = 2 * entry + (0 stroke, 1 fill)
         const int g = __ldg(&list[e]);
         const int4 gi = __ldg(&S.g_info[g]);
-#pragma unroll
-        for (int which = 0; which < 2; ++which) {
-            const int p = which == 0 ? gi.y : gi.x;
-            if (p < 0) continue;
-            const bool has = cur < nf && code[cur] == 2 * e + which;
-            if (!__any_sync(0xffffffffu, has)) continue;
-            float4 dv = make_float4(0, 0, 0, 0);
-            float4 c = make_float4(0, 0, 0, 0);
-            if (has) {
-                c = paint_color(S, p, pt);
-                float T = tr[cur];
-                float r_ = dcr * T, g_ = dcg * T, b_ = dcb * T, a_ = dca * T;
-                float d_alpha = a_ * (1.0f - prev.w);
-                d_alpha += r_ * (c.x - prev.x) + g_ * (c.y - prev.y) + b_ * (c.z - prev.z);
-                dv = make_float4(r_ * c.w, g_ * c.w, b_ * c.w, d_alpha);
-                over(prev, c);
-                ++cur;
+        const int p = which == 0 ? gi.y : gi.x;
+        const bool has = mine == nxt;
+        float4 dv = make_float4(0, 0, 0, 0);
+        if (has) {
+            const float4 c = paint_color(S, p, pt);
+            float T = tr[cur];
+            float r_ = dcr * T, g_ = dcg * T, b_ = dcb * T, a_ = dca * T;
+            float d_alpha = a_ * (1.0f - prev.w);
+            d_alpha += r_ * (c.x - prev.x) + g_ * (c.y - prev.y) + b_ * (c.z - prev.z);
+            dv = make_float4(r_ * c.w, g_ * c.w, b_ * c.w, d_alpha);
+            over(prev, c);
+            ++cur;
+        }
+        const int kind = __ldg(&S.paint_info[p].x);
+        if (kind == P_SOLID) {
+            float s0 = warp_sum(dv.x), s1 = warp_sum(dv.y), s2 = warp_sum(dv.z), s3 = warp_sum(dv.w);
+            if (lane == 0) {
+                float* d = G.d_paint_params + 4 * p;
+                add_if(d + 0, s0);
+                add_if(d + 1, s1);
+                add_if(d + 2, s2);
+                add_if(d + 3, s3);
             }
-            const int kind = __ldg(&S.paint_info[p].x);
-            if (kind == P_SOLID) {
-                float s0 = warp_sum(dv.x), s1 = warp_sum(dv.y), s2 = warp_sum(dv.z), s3 = warp_sum(dv.w);
-                if (lane == 0) {
-                    float* d = G.d_paint_params + 4 * p;
-                    add_if(d + 0, s0);
-                    add_if(d + 1, s1);
-                    add_if(d + 2, s2);
-                    add_if(d + 3, s3);
-                }
-            } else if (has) {
-                float2 dtr = make_float2(0.0f, 0.0f);
-                d_gradient_paint(S, G, p, pt, dv, &dtr);
-                if (G.d_translation) {
-                    add_if(G.d_translation + 2 * (size_t)pixel, dtr.x);
-                    add_if(G.d_translation + 2 * (size_t)pixel + 1, dtr.y);
-                }
+        } else if (has) {
+            float2 dtr = make_float2(0.0f, 0.0f);
+            d_gradient_paint(S, G, p, pt, dv, &dtr);
+            if (G.d_translation) {
+                add_if(G.d_translation + 2 * (size_t)pixel, dtr.x);
+                add_if(G.d_translation + 2 * (size_t)pixel + 1, dtr.y);
             }
         }
     }

@@ -833,18 +833,20 @@ __device__ __forceinline__ void interior_prefilter_body(const DevScene& S, const
         dcol = make_float4(0, 0, 0, 0);
     }
     if (!active) dcol = make_float4(0, 0, 0, 0);
-    // pass 3: compositing adjoint with coverage and distance derivatives
+    // pass 3: compositing adjoint with coverage and distance derivatives; the warp
+    // visits only entries some lane hit (smallest next fragment code over the warp).
     int cur = 0;
     float4 prev = bg;
-    for (int e = 0; e < n; ++e) {
+    while (true) {
+        const int mine = cur < nf ? code[cur] : 0x7fffffff;
+        const int nxt = __reduce_min_sync(0xffffffffu, mine);
+        if (nxt == 0x7fffffff) break;
+        const int e = nxt >> 1, which = nxt & 1;  // code = 2 * entry + (0 stroke, 1 fill)
         const int g = __ldg(&list[e]);
         const int4 gi = __ldg(&S.g_info[g]);
-#pragma unroll
-        for (int which = 0; which < 2; ++which) {
-            const int p = which == 0 ? gi.y : gi.x;
-            if (p < 0) continue;
-            const bool has = cur < nf && code[cur] == 2 * e + which;
-            if (!__any_sync(0xffffffffu, has)) continue;
+        const int p = which == 0 ? gi.y : gi.x;
+        const bool has = mine == nxt;
+        {
             float4 dv = make_float4(0, 0, 0, 0);
             int i = cur;
             float w = 0.0f, d_w = 0.0f;
