@@ -118,13 +118,16 @@ __global__ void __launch_bounds__(256) k_bin_write(DevScene S, const float4* g_b
 // ------------------------------------------------------------------ forward
 // One CTA = one 16x16 tile at one sub-sample (sx, sy); thread = pixel.  Every
 // thread of the CTA walks the same group list, so group data loads are uniform.
-__device__ __forceinline__ void forward_body(const DevScene& S, const SampleParams& sp, int tile, int sub,
+__device__ __forceinline__ void forward_body(const DevScene& S, const SampleParams& sp, int tile, int round,
                                              float* accum, float* wsum, float* sm) {
     const int ri = S.filter_ri;
     const int HW = TILE + 2 * ri;
     const bool use_sm = ri <= MAX_SMEM_RI;
     const int tx = tile % S.tiles_x, ty = tile / S.tiles_x;
-    const int x = tx * TILE + (threadIdx.x % TILE), y = ty * TILE + (threadIdx.x / TILE);
+    const int spp = sp.sxn * sp.syn;
+    const int s_in_tile = round * 256 + (int)threadIdx.x;
+    const int pix = s_in_tile / spp, sub = s_in_tile % spp;
+    const int x = tx * TILE + (pix % TILE), y = ty * TILE + (pix / TILE);
     if (use_sm)
         for (int i = threadIdx.x; i < HW * HW * 5; i += blockDim.x) sm[i] = 0.0f;
     __syncthreads();
@@ -212,12 +215,15 @@ __global__ void k_resolve(DevScene S, const float* accum, const float* wsum, flo
 // per-thread local memory, never in HBM.  The adjoint loop walks the tile's
 // group list in the same order on every lane so solid-paint gradients reduce
 // across the warp before one atomic.
-__device__ __forceinline__ void interior_body(const DevScene& S, const SampleParams& sp, int tile, int sub,
+__device__ __forceinline__ void interior_body(const DevScene& S, const SampleParams& sp, int tile, int round,
                                               const float* d_render, const float* wsum, const GradPtrs& G,
                                               unsigned* status) {
     __shared__ float red[8][6];
     const int tx = tile % S.tiles_x, ty = tile / S.tiles_x;
-    const int x = tx * TILE + (threadIdx.x % TILE), y = ty * TILE + (threadIdx.x / TILE);
+    const int spp = sp.sxn * sp.syn;
+    const int s_in_tile = round * 256 + (int)threadIdx.x;
+    const int pix = s_in_tile / spp, sub = s_in_tile % spp;
+    const int x = tx * TILE + (pix % TILE), y = ty * TILE + (pix / TILE);
     const bool valid = x < S.width && y < S.height;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int off = S.tile_offsets[tile];

@@ -290,13 +290,16 @@ __device__ __forceinline__ PFragD prefilter_fill(const DevScene& S, int g, int p
 }
 
 // ------------------------------------------------------------------ forward
-__device__ __forceinline__ void forward_prefilter_body(const DevScene& S, const SampleParams& sp, int tile, int sub,
+__device__ __forceinline__ void forward_prefilter_body(const DevScene& S, const SampleParams& sp, int tile, int round,
                                                        float* accum, float* wsum, unsigned* status, float* sm) {
     const int ri = S.filter_ri;
     const int HW = TILE + 2 * ri;
     const bool use_sm = ri <= MAX_SMEM_RI;
     const int tx = tile % S.tiles_x, ty = tile / S.tiles_x;
-    const int x = tx * TILE + (threadIdx.x % TILE), y = ty * TILE + (threadIdx.x / TILE);
+    const int spp = sp.sxn * sp.syn;
+    const int s_in_tile = round * 256 + (int)threadIdx.x;
+    const int pix = s_in_tile / spp, sub = s_in_tile % spp;
+    const int x = tx * TILE + (pix % TILE), y = ty * TILE + (pix / TILE);
     if (use_sm)
         for (int i = threadIdx.x; i < HW * HW * 5; i += blockDim.x) sm[i] = 0.0f;
     __syncthreads();
@@ -734,12 +737,15 @@ __device__ float2 d_compute_distance(const DevScene& S, const GradPtrs& G, int g
 
 // ------------------------------------------------------------------ interior adjoint (sampling.rs:227-482)
 constexpr int MAX_PF = 48;
-__device__ __forceinline__ void interior_prefilter_body(const DevScene& S, const SampleParams& sp, int tile, int sub,
+__device__ __forceinline__ void interior_prefilter_body(const DevScene& S, const SampleParams& sp, int tile, int round,
                                                         const float* d_render, const float* wsum, const GradPtrs& G,
                                                         unsigned* status) {
     __shared__ float red[8][6];
     const int tx = tile % S.tiles_x, ty = tile / S.tiles_x;
-    const int x = tx * TILE + (threadIdx.x % TILE), y = ty * TILE + (threadIdx.x / TILE);
+    const int spp = sp.sxn * sp.syn;
+    const int s_in_tile = round * 256 + (int)threadIdx.x;
+    const int pix = s_in_tile / spp, sub = s_in_tile % spp;
+    const int x = tx * TILE + (pix % TILE), y = ty * TILE + (pix / TILE);
     const bool valid = x < S.width && y < S.height;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int off = S.tile_offsets[tile];
