@@ -496,7 +496,7 @@ static dvg_status backward_core(dvg_context* ctx, dvg_scene* sc, const dvg_rende
             CK(ctx->bsamples.reserve(cap * sizeof(BSample)));
             CK(ctx->bkey.reserve(cap * sizeof(int)));
             CK(ctx->border.reserve(cap * sizeof(int)));
-            CK(ctx->bcounts.reserve((2 * (size_t)tiles + 1) * sizeof(int)));
+            CK(ctx->bcounts.reserve((2 * (size_t)tiles * BND_BUCKETS + 1) * sizeof(int)));
             Prof prof_(ctx, "boundary");
             ctx->launches += launch_boundary(S, bp, d_render, ctx->wsum.as<float>(), G, ctx->bsamples.as<BSample>(),
                                              ctx->bkey.as<int>(), ctx->bcounts.as<int>(), ctx->border.as<int>(), cap,
@@ -949,7 +949,7 @@ extern "C" dvg_status dvg_batch_create(dvg_context* ctx, dvg_scene* const* scene
     CK(b->bsamples.reserve(nbs * sizeof(BSample)));
     CK(b->bkey.reserve(nbs * sizeof(int)));
     CK(b->border.reserve(nbs * sizeof(int)));
-    CK(b->bcounts.reserve((2 * (size_t)b->total_tiles + 1) * sizeof(int)));
+    CK(b->bcounts.reserve((2 * (size_t)b->total_tiles * BND_BUCKETS + 1) * sizeof(int)));
     CK(cudaMemsetAsync(b->target.ptr, 0, b->total_pix4 * sizeof(float), ctx->stream));
     float* acc = b->accum.as<float>();
     float* img = b->image.as<float>();

@@ -910,9 +910,13 @@ __device__ __forceinline__ void boundary_gen_one(const DevScene& S, uint64_t idx
     r.is_stroke = bd.is_stroke ? 1 : 0;
     r.scene = scene;
     out[slot] = r;
+    // sort bucket: the 4x4-pixel cell of the boundary pixel inside its tile, so that a
+    // warp evaluates edge points that lie close together (coherent group walks)
     const int tile = tile_off + (by / TILE) * S.tiles_x + (bx / TILE);
-    key[slot] = tile;
-    atomicAdd(tile_counts + tile, 1);
+    const int cell = ((by % TILE) / BND_CELL) * (TILE / BND_CELL) + (bx % TILE) / BND_CELL;
+    const int bucket = tile * BND_BUCKETS + cell;
+    key[slot] = bucket;
+    atomicAdd(tile_counts + bucket, 1);
 }
 __global__ void __launch_bounds__(256) k_boundary_gen(DevScene S, BoundaryParams bp, BSample* out, int* key,
                                                       int* tile_counts) {
@@ -1194,7 +1198,7 @@ int launch_boundary(const DevScene& S, const BoundaryParams& bp, const float* d_
                     const GradPtrs& G, BSample* samples, int* key, int* counts, int* order, uint64_t capacity,
                     cudaStream_t stream) {
     const uint64_t n = bp.num_samples;
-    const int tiles = S.tiles_x * S.tiles_y;
+    const int tiles = S.tiles_x * S.tiles_y * BND_BUCKETS;  // sort buckets
     int launches = 0;
     for (uint64_t base = 0; base < n; base += capacity) {
         const uint64_t cnt = base + capacity < n ? capacity : n - base;
@@ -1250,6 +1254,7 @@ int launch_interior_batch(const BatchEntry* B, const int* item_scene, int items,
 int launch_boundary_batch(const BatchEntry* B, int nscenes, uint64_t total, int total_tiles, BSample* samples, int* key,
                           int* counts, int* order, cudaStream_t stream) {
     if (total == 0) return 0;
+    total_tiles *= BND_BUCKETS;  // sort buckets
     cudaMemsetAsync(counts, 0, sizeof(int) * (2 * (size_t)total_tiles + 1), stream);
     k_boundary_gen_batch<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(B, nscenes, total, samples, key,
                                                                               counts);

@@ -14,6 +14,10 @@ namespace dvgb {
 constexpr int MAX_FRAGMENTS = 96;
 // Filter radii up to this (ceil) use the shared-memory tile+halo splat.
 constexpr int MAX_SMEM_RI = 8;
+// Boundary samples are counting-sorted by BND_CELL x BND_CELL-pixel cells of their
+// tile (BND_BUCKETS buckets per tile); scratch counts hold 2 * tiles * BND_BUCKETS + 1.
+constexpr int BND_CELL = 4;
+constexpr int BND_BUCKETS = (16 / BND_CELL) * (16 / BND_CELL);
 
 struct SampleParams {
     int sxn, syn;
@@ -102,7 +106,7 @@ int launch_interior(const DevScene& S, const SampleParams& sp, const float* d_re
 int launch_interior_prefilter(const DevScene& S, const SampleParams& sp, const float* d_render, const float* wsum,
                               const GradPtrs& G, unsigned* status, cudaStream_t stream);
 // Boundary pass in chunks of at most `capacity` samples; scratch: samples[capacity],
-// key[capacity], order[capacity], counts[2*tiles+1].
+// key[capacity], order[capacity], counts[2*tiles*BND_BUCKETS+1].
 int launch_boundary(const DevScene& S, const BoundaryParams& bp, const float* d_render, const float* wsum,
                     const GradPtrs& G, BSample* samples, int* key, int* counts, int* order, uint64_t capacity,
                     cudaStream_t stream);
