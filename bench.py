@@ -458,7 +458,7 @@ def main():
     achieved = alg_bytes / (avg_ms / 1e3) / 1e9
     # DRAM bytes (read + write) per launch from one ncu capture of this workload
     # (profiles/k_*_mixed512.md); only the default workload has a capture.
-    ncu_traffic = {"interior": 7315200, "forward": 7385856, "boundary": 25160192} if args.workload == "mixed" else {}
+    ncu_traffic = {"interior": 6066944, "forward": 5911808, "boundary": 23650304} if args.workload == "mixed" else {}
     prof_json = {k: {"ms_per_step": v[0] / 3.0, "calls_per_step": v[1] / 3.0} for k, v in prof.items()}
 
     line = {
