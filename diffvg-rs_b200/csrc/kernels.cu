@@ -962,8 +962,16 @@ __device__ __forceinline__ void boundary_eval_one(const DevScene& S, const BSamp
     bool hi, ho;
     const float2 pin = make_float2(r.bx - nc.x * 1.0e-4f, r.by - nc.y * 1.0e-4f);
     const float2 pout = make_float2(r.bx + nc.x * 1.0e-4f, r.by + nc.y * 1.0e-4f);
-    float4 ci = edge_color(S, tile, make_float2(pin.x * W, pin.y * H), bg, r.group, r.shape, &hi);
-    float4 co = edge_color(S, tile, make_float2(pout.x * W, pout.y * H), bg, r.group, r.shape, &ho);
+    float4 cc[2];
+    bool hh[2];
+#pragma unroll 1
+    for (int side = 0; side < 2; ++side) {
+        const float2 q = side == 0 ? pin : pout;
+        cc[side] = edge_color(S, tile, make_float2(q.x * W, q.y * H), bg, r.group, r.shape, &hh[side]);
+    }
+    float4 ci = cc[0], co = cc[1];
+    hi = hh[0];
+    ho = hh[1];
     if (!hi && !ho) return;
     if (!hi) {
         nc = make_float2(nc.x * -1.0f, nc.y * -1.0f);
