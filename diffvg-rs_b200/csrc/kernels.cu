@@ -142,8 +142,13 @@ __device__ __forceinline__ void forward_body(const DevScene& S, const SamplePara
             const int g = __ldg(&list[e]);
             const int4 gi = __ldg(&S.g_info[g]);
             const float2 lp = xf9(S.g_c2s + 9 * g, pt);
-            if (gi.y >= 0 && group_within(S, g, lp)) over(acc, paint_color(S, gi.y, pt));
-            if (gi.x >= 0 && group_inside(S, g, lp, gi.z)) over(acc, paint_color(S, gi.x, pt));
+            // stroke first, then fill; one paint call site for both
+            int hitp[2];
+            hitp[0] = gi.y >= 0 && group_within(S, g, lp) ? gi.y : -1;
+            hitp[1] = gi.x >= 0 && group_inside(S, g, lp, gi.z) ? gi.x : -1;
+#pragma unroll 1
+            for (int which = 0; which < 2; ++which)
+                if (hitp[which] >= 0) over(acc, paint_color(S, hitp[which], pt));
         }
         splat_sample(S, x, y, tx, ty, ri, HW, use_sm, pt, acc, sm, accum, wsum);
     }
@@ -254,22 +259,16 @@ __device__ __forceinline__ void interior_body(const DevScene& S, const SamplePar
             const int g = __ldg(&list[e]);
             const int4 gi = __ldg(&S.g_info[g]);
             const float2 lp = xf9(S.g_c2s + 9 * g, pt);
-            if (gi.y >= 0 && group_within(S, g, lp)) {
-                float4 c = paint_color(S, gi.y, pt);
+            int hitp[2];
+            hitp[0] = gi.y >= 0 && group_within(S, g, lp) ? gi.y : -1;
+            hitp[1] = gi.x >= 0 && group_inside(S, g, lp, gi.z) ? gi.x : -1;
+#pragma unroll 1
+            for (int which = 0; which < 2; ++which) {
+                if (hitp[which] < 0) continue;
+                float4 c = paint_color(S, hitp[which], pt);
                 over(acc, c);
                 if (nf < MAX_FRAGMENTS) {
-                    code[nf] = 2 * e;
-                    tr[nf] = c.w;
-                } else {
-                    overflow = true;
-                }
-                ++nf;
-            }
-            if (gi.x >= 0 && group_inside(S, g, lp, gi.z)) {
-                float4 c = paint_color(S, gi.x, pt);
-                over(acc, c);
-                if (nf < MAX_FRAGMENTS) {
-                    code[nf] = 2 * e + 1;
+                    code[nf] = 2 * e + which;
                     tr[nf] = c.w;
                 } else {
                     overflow = true;
