@@ -245,37 +245,27 @@ struct PFragD {
     float t;
     bool within;
 };
-__device__ __forceinline__ PFragD prefilter_stroke(const DevScene& S, int g, int paint, float2 pt, unsigned* status) {
-    PFragD f;
-    f.hit = false;
-    ClosestD h;
-    if (!compute_distance_group(S, g, pt, INF_F, &h, status)) return f;
-    const float sw = __ldg(&S.s_stroke[h.shape]);
-    const float d = h.dist;
-    const float w = smoothstep1(fabsf(d) + sw) - smoothstep1(fabsf(d) - sw);
-    if (!(w > 0.0f)) return f;
-    f.c = paint_color(S, paint, pt);
-    f.c.w *= w;
-    f.hit = true;
-    f.shape = h.shape;
-    f.dist = d;
-    f.cp = h.point;
-    f.seg = h.seg;
-    f.t = h.t;
-    f.within = true;
-    return f;
-}
-__device__ __forceinline__ PFragD prefilter_fill(const DevScene& S, int g, int paint, int rule, float2 pt,
+// Stroke (which = 0) or fill (which = 1) fragment of group g, through one call
+// site each of the closest-point search, the inside test and the paint.
+__device__ __forceinline__ PFragD prefilter_frag(const DevScene& S, int g, int which, int paint, int rule, float2 pt,
                                                  unsigned* status) {
     PFragD f;
     f.hit = false;
     ClosestD h;
-    const bool have = compute_distance_group(S, g, pt, 1.0f, &h, status);
-    const bool inside = group_inside(S, g, xf9(S.g_c2s + 9 * g, pt), rule);
-    if (!have && !inside) return f;
-    float d = have ? h.dist : 1.0f;
-    if (!inside) d = -d;
-    const float w = smoothstep1(d);
+    const bool have = compute_distance_group(S, g, pt, which == 0 ? INF_F : 1.0f, &h, status);
+    float d, w;
+    if (which == 0) {
+        if (!have) return f;
+        const float sw = __ldg(&S.s_stroke[h.shape]);
+        d = h.dist;
+        w = smoothstep1(fabsf(d) + sw) - smoothstep1(fabsf(d) - sw);
+    } else {
+        const bool inside = group_inside(S, g, xf9(S.g_c2s + 9 * g, pt), rule);
+        if (!have && !inside) return f;
+        d = have ? h.dist : 1.0f;
+        if (!inside) d = -d;
+        w = smoothstep1(d);
+    }
     if (!(w > 0.0f)) return f;
     f.c = paint_color(S, paint, pt);
     f.c.w *= w;
@@ -285,7 +275,7 @@ __device__ __forceinline__ PFragD prefilter_fill(const DevScene& S, int g, int p
     f.cp = have ? h.point : make_float2(0.0f, 0.0f);
     f.seg = have ? h.seg : -1;
     f.t = have ? h.t : 0.0f;
-    f.within = have;
+    f.within = which == 0 ? true : have;
     return f;
 }
 
@@ -313,12 +303,11 @@ __device__ __forceinline__ void forward_prefilter_body(const DevScene& S, const 
         for (int e = 0; e < n; ++e) {
             const int g = __ldg(&list[e]);
             const int4 gi = __ldg(&S.g_info[g]);
-            if (gi.y >= 0) {
-                PFragD f = prefilter_stroke(S, g, gi.y, pt, status);
-                if (f.hit) over(acc, f.c);
-            }
-            if (gi.x >= 0) {
-                PFragD f = prefilter_fill(S, g, gi.x, gi.z, pt, status);
+#pragma unroll 1
+            for (int which = 0; which < 2; ++which) {
+                const int p = which == 0 ? gi.y : gi.x;
+                if (p < 0) continue;
+                PFragD f = prefilter_frag(S, g, which, p, gi.z, pt, status);
                 if (f.hit) over(acc, f.c);
             }
         }
@@ -774,12 +763,11 @@ __device__ __forceinline__ void interior_prefilter_body(const DevScene& S, const
         for (int e = 0; e < n; ++e) {
             const int g = __ldg(&list[e]);
             const int4 gi = __ldg(&S.g_info[g]);
-#pragma unroll
+#pragma unroll 1
             for (int which = 0; which < 2; ++which) {
-                PFragD f;
-                f.hit = false;
-                if (which == 0 && gi.y >= 0) f = prefilter_stroke(S, g, gi.y, pt, status);
-                if (which == 1 && gi.x >= 0) f = prefilter_fill(S, g, gi.x, gi.z, pt, status);
+                const int p = which == 0 ? gi.y : gi.x;
+                if (p < 0) continue;
+                PFragD f = prefilter_frag(S, g, which, p, gi.z, pt, status);
                 if (!f.hit) continue;
                 over(acc, f.c);
                 if (nf < MAX_PF) {
