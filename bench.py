@@ -148,6 +148,7 @@ def large_fit(r, dev, lib_stream, steps, warmup, rank):
     tu.render_device(opts, tgt.data_ptr())
     torch.cuda.synchronize(dev)
     tu.close()
+    tuning = batch.autotune()
     batch.set_adam(1e-2, (0.9, 0.999), 1e-8, points=True)
     for _ in range(warmup):
         batch.step(True)
@@ -167,7 +168,8 @@ def large_fit(r, dev, lib_stream, steps, warmup, rank):
     return {"workload": "1024x1024, 4x4 spp, 4096 closed cubic paths x 16 segments, 25% stroked, radial 3-stop "
                         "fills, W*H*spp boundary samples; fwd + L2 + bwd + Adam + re-preparation per graph replay",
             "iterations": steps, "warmup": warmup, "ms_per_iter": ms, "msamples_per_s": samples / (ms / 1e3) / 1e6,
-            "loss_after_warmup": first, "loss_last": last}
+            "loss_after_warmup": first, "loss_last": last,
+            "launch_shape": {"sample_layout": tuning[0], "boundary_cell": tuning[1]}}
 
 
 def batched_vs_plain(r, dev, lib_stream, flush, scenes, steps, label):
@@ -211,6 +213,7 @@ def batched_vs_plain(r, dev, lib_stream, flush, scenes, steps, label):
             ms.append(e0.elapsed_time(e1))
         return float(np.median(ms))
 
+    tuning = batch.autotune()
     t_plain = timed(plain_step)
     t_batch = timed(lambda: batch.step(True))
 
@@ -255,7 +258,7 @@ def batched_vs_plain(r, dev, lib_stream, flush, scenes, steps, label):
                "what": "fwd + L2 + bwd + Adam(lr 1e-2) on path points per scene; batched = one graph replay with "
                        "on-device Adam and scene re-preparation; plain = per scene host preparation + upload, "
                        "fused device call, gradient read-back, host Adam"},
-           "workload": label}
+           "workload": label, "launch_shape": {"sample_layout": tuning[0], "boundary_cell": tuning[1]}}
     batch.close()
     for u in ups + tgts:
         u.close()
@@ -336,6 +339,8 @@ def main():
     grads = DeviceGrads(up.packed, dev)
     lib_stream = torch.cuda.ExternalStream(r.stream_handle, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+
+    tuning = up.autotune(opts, bopts, target.data_ptr())  # launch shape for this scene (dvg_scene_autotune)
 
     def step():
         up.fwd_bwd_l2_device(opts, bopts, target.data_ptr(), out.data_ptr(), loss.data_ptr(), grads)
@@ -467,7 +472,8 @@ def main():
         "vs_baseline": None, "dtype": "f32 (f64 root solves, as the crate)",
         "data": "synthetic (seeded scene generator, no dataset)",
         "config": {**cfg, "boundary_samples": bopts.boundary_samples, "l2": "flushed between timed steps "
-                   "(256 MiB write outside the timed events)", "parallelism": f"weak, {world} independent scene(s)"},
+                   "(256 MiB write outside the timed events)", "parallelism": f"weak, {world} independent scene(s)",
+                   "launch_shape": {"sample_layout": tuning[0], "boundary_cell": tuning[1], "chosen_by": "dvg_scene_autotune"}},
         "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": ncu_traffic.get(name), "peak_source": peak_src,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch "

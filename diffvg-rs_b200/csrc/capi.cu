@@ -107,6 +107,7 @@ struct dvg_scene {
     size_t grad_floats = 0;
     size_t arena_bytes = 0;  // bytes of prepared tables in `arena`
     const float4* g_bbox = nullptr;
+    dvg_tuning tune{1, 4};   // launch shape (dvg_scene_set_tuning / dvg_scene_autotune)
 };
 
 namespace {
@@ -147,8 +148,9 @@ dvg_status check_options(const dvg_render_options* o) {
     if (!o) return fail(DVG_ERR_INVALID_ARGUMENT, "null render options");
     return DVG_OK;
 }
-SampleParams sample_params(const dvg_render_options* o) {
+SampleParams sample_params(const dvg_render_options* o, int layout = 1) {
     SampleParams sp;
+    sp.layout = layout;
     sp.sxn = o->samples_x > 0 ? (int)o->samples_x : 1;
     sp.syn = o->samples_y > 0 ? (int)o->samples_y : 1;
     sp.seed = o->seed;
@@ -406,7 +408,7 @@ static dvg_status render_into(dvg_context* ctx, dvg_scene* sc, const dvg_render_
         CK(cudaGetLastError());
         return DVG_OK;
     }
-    SampleParams sp = sample_params(opts);
+    SampleParams sp = sample_params(opts, (int)sc->tune.sample_layout);
     CK(ctx->accum.reserve(npix * 4 * sizeof(float)));
     CK(ctx->wsum.reserve(npix * sizeof(float)));
     CK(cudaMemsetAsync(ctx->accum.ptr, 0, npix * 4 * sizeof(float), ctx->stream));
@@ -465,7 +467,7 @@ static dvg_status backward_core(dvg_context* ctx, dvg_scene* sc, const dvg_rende
     const DevScene& S = sc->dev;
     const size_t npix = (size_t)S.width * S.height;
     if (npix == 0) return DVG_OK;
-    SampleParams sp = sample_params(opts);
+    SampleParams sp = sample_params(opts, (int)sc->tune.sample_layout);
     if (d_render && S.num_groups > 0) {
         if (!have_weights) {
             CK(ctx->wsum.reserve(npix * sizeof(float)));
@@ -491,12 +493,13 @@ static dvg_status backward_core(dvg_context* ctx, dvg_scene* sc, const dvg_rende
             bp.slot_base = 0;
             bp.seed = (bopts && !bopts->boundary_seed_from_options) ? bopts->boundary_seed : opts->seed;
             bp.rng = bopts ? (int)bopts->rng : 0;
+            bp.cell = (int)sc->tune.boundary_cell;
             const uint64_t cap = std::min<uint64_t>(bp.num_samples, (uint64_t)1 << 24);
             const int tiles = S.tiles_x * S.tiles_y;
             CK(ctx->bsamples.reserve(cap * sizeof(BSample)));
             CK(ctx->bkey.reserve(cap * sizeof(int)));
             CK(ctx->border.reserve(cap * sizeof(int)));
-            CK(ctx->bcounts.reserve((2 * (size_t)tiles * BND_BUCKETS + 1) * sizeof(int)));
+            CK(ctx->bcounts.reserve((2 * (size_t)tiles * BND_MAX_BUCKETS + 1) * sizeof(int)));
             Prof prof_(ctx, "boundary");
             ctx->launches += launch_boundary(S, bp, d_render, ctx->wsum.as<float>(), G, ctx->bsamples.as<BSample>(),
                                              ctx->bkey.as<int>(), ctx->bcounts.as<int>(), ctx->border.as<int>(), cap,
@@ -800,7 +803,7 @@ extern "C" dvg_status dvg_render_device_noalloc(dvg_context* ctx, dvg_scene* sce
     float* accum = scratch;            // 4 floats per pixel (float4 aligned: 256-byte base)
     float* wsum = scratch + 4 * npix;  // 1 float per pixel
     CK(cudaMemsetAsync(scratch, 0, 5 * npix * sizeof(float), ctx->stream));
-    const SampleParams sp = sample_params(opts);
+    const SampleParams sp = sample_params(opts, (int)scene->tune.sample_layout);
     if (opts->use_prefiltering)
         ctx->launches += launch_forward_prefilter(S, sp, accum, wsum, ctx->status, ctx->stream);
     else
@@ -829,6 +832,7 @@ struct dvg_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     uint64_t steps = 0;
+    dvg_tuning tune{1, 4};  // launch shape (dvg_batch_autotune)
     // on-device optimisation step (dvg_batch_set_adam)
     bool adam = false;
     AdamParams ap{};
@@ -858,7 +862,8 @@ dvg_status batch_enqueue(dvg_batch* b) {
     else
         ctx->launches += launch_interior_batch(B, b->item_scene.as<int>(), b->items, ctx->status, ctx->stream);
     if (!pre)
-        ctx->launches += launch_boundary_batch(B, n, b->total_bsamples, b->total_tiles, b->bsamples.as<BSample>(),
+        ctx->launches += launch_boundary_batch(B, n, b->total_bsamples, b->total_tiles, (int)b->tune.boundary_cell,
+                                               b->bsamples.as<BSample>(),
                                                b->bkey.as<int>(), b->bcounts.as<int>(), b->border.as<int>(),
                                                ctx->stream);
     ctx->launches += launch_pixels_batch(B, n, b->max_pixels, 2, ctx->stream);
@@ -949,7 +954,7 @@ extern "C" dvg_status dvg_batch_create(dvg_context* ctx, dvg_scene* const* scene
     CK(b->bsamples.reserve(nbs * sizeof(BSample)));
     CK(b->bkey.reserve(nbs * sizeof(int)));
     CK(b->border.reserve(nbs * sizeof(int)));
-    CK(b->bcounts.reserve((2 * (size_t)b->total_tiles * BND_BUCKETS + 1) * sizeof(int)));
+    CK(b->bcounts.reserve((2 * (size_t)b->total_tiles * BND_MAX_BUCKETS + 1) * sizeof(int)));
     CK(cudaMemsetAsync(b->target.ptr, 0, b->total_pix4 * sizeof(float), ctx->stream));
     float* acc = b->accum.as<float>();
     float* img = b->image.as<float>();
@@ -1429,4 +1434,125 @@ extern "C" dvg_status dvg_lbvh_build(dvg_context* ctx, const float* boxes, uint3
                            ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return DVG_OK;
+}
+
+// ------------------------------------------------------------------ launch-shape tuning
+namespace {
+bool tuning_valid(const dvg_tuning* t) {
+    return t && t->sample_layout <= 1 &&
+           (t->boundary_cell == 2 || t->boundary_cell == 4 || t->boundary_cell == 8 || t->boundary_cell == 16);
+}
+// The candidates: both warp layouts with the default cell, then every cell with the
+// better layout (the boundary pass does not depend on the layout).
+template <typename Apply, typename Run>
+dvg_status autotune_loop(dvg_context* ctx, dvg_tuning* tune, Apply apply, Run run) {
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    auto time_of = [&](dvg_tuning t, float* ms) -> dvg_status {
+        *tune = t;
+        dvg_status st = apply();
+        if (st != DVG_OK) return st;
+        st = run();  // warm
+        if (st != DVG_OK) return st;
+        CK(cudaEventRecord(e0, ctx->stream));
+        st = run();
+        if (st != DVG_OK) return st;
+        CK(cudaEventRecord(e1, ctx->stream));
+        CK(cudaEventSynchronize(e1));
+        CK(cudaEventElapsedTime(ms, e0, e1));
+        return DVG_OK;
+    };
+    dvg_status st = DVG_OK;
+    dvg_tuning best{1, 4};
+    float best_ms = 0.0f, ms = 0.0f;
+    st = time_of(dvg_tuning{1, 4}, &best_ms);
+    if (st == DVG_OK) st = time_of(dvg_tuning{0, 4}, &ms);
+    if (st == DVG_OK && ms < best_ms) {
+        best = dvg_tuning{0, 4};
+        best_ms = ms;
+    }
+    const uint32_t cells[3] = {2, 8, 16};
+    for (int k = 0; k < 3 && st == DVG_OK; ++k) {
+        st = time_of(dvg_tuning{best.sample_layout, cells[k]}, &ms);
+        if (st == DVG_OK && ms < best_ms) {
+            best = dvg_tuning{best.sample_layout, cells[k]};
+            best_ms = ms;
+        }
+    }
+    *tune = best;
+    if (st == DVG_OK) st = apply();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return st;
+}
+}  // namespace
+
+extern "C" dvg_status dvg_scene_set_tuning(dvg_scene* scene, const dvg_tuning* tuning) {
+    if (!scene || !tuning_valid(tuning)) return fail(DVG_ERR_INVALID_ARGUMENT, "invalid tuning");
+    scene->tune = *tuning;
+    return DVG_OK;
+}
+extern "C" dvg_status dvg_scene_get_tuning(const dvg_scene* scene, dvg_tuning* tuning) {
+    if (!scene || !tuning) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    *tuning = scene->tune;
+    return DVG_OK;
+}
+extern "C" dvg_status dvg_scene_autotune(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
+                                         const dvg_backward_options* bopts, const float* target_rgba,
+                                         dvg_tuning* out) {
+    if (!ctx || !scene || !target_rgba) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    dvg_status st = check_options(opts);
+    if (st != DVG_OK) return st;
+    CK(cudaSetDevice(ctx->device));
+    const GradPtrs G = device_grads(scene);
+    dvg_grads g{};
+    g.d_shape_params = G.d_shape_params;
+    g.d_shape_transform = G.d_shape_transform;
+    g.d_shape_stroke_width = G.d_shape_stroke_width;
+    g.d_points = G.d_points;
+    g.d_thickness = G.d_thickness;
+    g.d_group_transform = G.d_group_transform;
+    g.d_paint_params = G.d_paint_params;
+    g.d_stop_offsets = G.d_stop_offsets;
+    g.d_stop_colors = G.d_stop_colors;
+    g.d_filter_radius = G.d_filter_radius;
+    g.d_background = G.d_background;
+    st = autotune_loop(
+        ctx, &scene->tune, []() { return DVG_OK; },
+        [&]() { return dvg_fwd_bwd_l2_device(ctx, scene, opts, bopts, target_rgba, nullptr, nullptr, &g); });
+    if (st != DVG_OK) return st;
+    if (out) *out = scene->tune;
+    return check_status(ctx);
+}
+
+extern "C" dvg_status dvg_batch_set_tuning(dvg_batch* b, const dvg_tuning* tuning) {
+    if (!b || !tuning_valid(tuning)) return fail(DVG_ERR_INVALID_ARGUMENT, "invalid tuning");
+    dvg_context* ctx = b->ctx;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    batch_drop_graph(b);
+    b->tune = *tuning;
+    for (auto& e : b->host_entries) e.sp.layout = (int)tuning->sample_layout;
+    CK(cudaMemcpyAsync(b->entries.ptr, b->host_entries.data(), b->host_entries.size() * sizeof(BatchEntry),
+                       cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return DVG_OK;
+}
+
+extern "C" dvg_status dvg_batch_autotune(dvg_batch* b, dvg_tuning* out) {
+    if (!b) return fail(DVG_ERR_INVALID_ARGUMENT, "null batch");
+    dvg_context* ctx = b->ctx;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    batch_drop_graph(b);
+    dvg_tuning t = b->tune;
+    const bool adam = b->adam;
+    b->adam = false;  // time forward + loss + backward only: the parameters must not move
+    dvg_status st = autotune_loop(
+        ctx, &t, [&]() { return dvg_batch_set_tuning(b, &t); }, [&]() { return batch_enqueue(b); });
+    b->adam = adam;
+    if (st != DVG_OK) return st;
+    if (out) *out = b->tune;
+    return check_status(ctx);
 }

@@ -126,7 +126,7 @@ __device__ __forceinline__ void forward_body(const DevScene& S, const SamplePara
     const int tx = tile % S.tiles_x, ty = tile / S.tiles_x;
     const int spp = sp.sxn * sp.syn;
     const int s_in_tile = round * 256 + (int)threadIdx.x;
-    const int pix = s_in_tile / spp, sub = s_in_tile % spp;
+    const int pix = sp.layout ? s_in_tile / spp : (int)threadIdx.x, sub = sp.layout ? s_in_tile % spp : round;
     const int x = tx * TILE + (pix % TILE), y = ty * TILE + (pix / TILE);
     if (use_sm)
         for (int i = threadIdx.x; i < HW * HW * 5; i += blockDim.x) sm[i] = 0.0f;
@@ -227,7 +227,7 @@ __device__ __forceinline__ void interior_body(const DevScene& S, const SamplePar
     const int tx = tile % S.tiles_x, ty = tile / S.tiles_x;
     const int spp = sp.sxn * sp.syn;
     const int s_in_tile = round * 256 + (int)threadIdx.x;
-    const int pix = s_in_tile / spp, sub = s_in_tile % spp;
+    const int pix = sp.layout ? s_in_tile / spp : (int)threadIdx.x, sub = sp.layout ? s_in_tile % spp : round;
     const int x = tx * TILE + (pix % TILE), y = ty * TILE + (pix / TILE);
     const bool valid = x < S.width && y < S.height;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -850,8 +850,8 @@ __device__ void accumulate_boundary(const DevScene& S, const GradPtrs& G, int sh
 // Boundary pass, stage 1: draw every edge sample (boundary.rs:141-175), keep
 // the valid ones with the tile of their boundary pixel as sort key.
 __device__ __forceinline__ void boundary_gen_one(const DevScene& S, uint64_t idx, uint64_t slot, uint32_t seed,
-                                                 int rng_kind, int tile_off, int scene, BSample* out, int* key,
-                                                 int* tile_counts) {
+                                                 int rng_kind, int tile_off, int scene, int cell, BSample* out,
+                                                 int* key, int* tile_counts) {
     key[slot] = -1;
     float u, t;
     if (rng_kind == 1) {
@@ -912,8 +912,8 @@ __device__ __forceinline__ void boundary_gen_one(const DevScene& S, uint64_t idx
     // sort bucket: the 4x4-pixel cell of the boundary pixel inside its tile, so that a
     // warp evaluates edge points that lie close together (coherent group walks)
     const int tile = tile_off + (by / TILE) * S.tiles_x + (bx / TILE);
-    const int cell = ((by % TILE) / BND_CELL) * (TILE / BND_CELL) + (bx % TILE) / BND_CELL;
-    const int bucket = tile * BND_BUCKETS + cell;
+    const int per_row = TILE / cell;
+    const int bucket = tile * (per_row * per_row) + ((by % TILE) / cell) * per_row + (bx % TILE) / cell;
     key[slot] = bucket;
     atomicAdd(tile_counts + bucket, 1);
 }
@@ -921,12 +921,13 @@ __global__ void __launch_bounds__(256) k_boundary_gen(DevScene S, BoundaryParams
                                                       int* tile_counts) {
     const uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + bp.sample_base;
     if (idx >= bp.num_samples) return;
-    boundary_gen_one(S, idx, idx - bp.slot_base, bp.seed, bp.rng, 0, 0, out, key, tile_counts);
+    boundary_gen_one(S, idx, idx - bp.slot_base, bp.seed, bp.rng, 0, 0, bp.cell, out, key, tile_counts);
 }
 // Batched stage 1: one flat index over all scenes' boundary samples; the scene is
 // found by binary search over the per-scene sample offsets.
 __global__ void __launch_bounds__(256) k_boundary_gen_batch(const BatchEntry* __restrict__ B, int nscenes,
-                                                            uint64_t total, BSample* out, int* key, int* tile_counts) {
+                                                            uint64_t total, int cell, BSample* out, int* key,
+                                                            int* tile_counts) {
     const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= total) return;
     int lo = 0, hi = nscenes - 1;
@@ -940,7 +941,7 @@ __global__ void __launch_bounds__(256) k_boundary_gen_batch(const BatchEntry* __
     const BatchEntry& E = B[lo];
     key[g] = -1;
     if (!E.S.boundary_ok || g - E.b_off >= E.nb) return;
-    boundary_gen_one(E.S, g - E.b_off, g, E.bseed, E.rng, E.tile_off, lo, out, key, tile_counts);
+    boundary_gen_one(E.S, g - E.b_off, g, E.bseed, E.rng, E.tile_off, lo, cell, out, key, tile_counts);
 }
 // Stage 2: counting-sort scatter of sample slots by tile.
 __global__ void k_boundary_scatter(const int* key, uint64_t n, int* cursor, int* order) {
@@ -1205,7 +1206,7 @@ int launch_boundary(const DevScene& S, const BoundaryParams& bp, const float* d_
                     const GradPtrs& G, BSample* samples, int* key, int* counts, int* order, uint64_t capacity,
                     cudaStream_t stream) {
     const uint64_t n = bp.num_samples;
-    const int tiles = S.tiles_x * S.tiles_y * BND_BUCKETS;  // sort buckets
+    const int tiles = S.tiles_x * S.tiles_y * bnd_buckets(bp.cell);  // sort buckets
     int launches = 0;
     for (uint64_t base = 0; base < n; base += capacity) {
         const uint64_t cnt = base + capacity < n ? capacity : n - base;
@@ -1258,13 +1259,13 @@ int launch_interior_batch(const BatchEntry* B, const int* item_scene, int items,
     k_interior_batch<<<items, 256, 0, stream>>>(B, item_scene, status);
     return 1;
 }
-int launch_boundary_batch(const BatchEntry* B, int nscenes, uint64_t total, int total_tiles, BSample* samples, int* key,
-                          int* counts, int* order, cudaStream_t stream) {
+int launch_boundary_batch(const BatchEntry* B, int nscenes, uint64_t total, int total_tiles, int cell,
+                          BSample* samples, int* key, int* counts, int* order, cudaStream_t stream) {
     if (total == 0) return 0;
-    total_tiles *= BND_BUCKETS;  // sort buckets
+    total_tiles *= bnd_buckets(cell);  // sort buckets
     cudaMemsetAsync(counts, 0, sizeof(int) * (2 * (size_t)total_tiles + 1), stream);
-    k_boundary_gen_batch<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(B, nscenes, total, samples, key,
-                                                                              counts);
+    k_boundary_gen_batch<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(B, nscenes, total, cell, samples,
+                                                                              key, counts);
     int* offsets = counts + total_tiles;
     k_bin_scan<<<1, 1024, 0, stream>>>(counts, total_tiles, offsets);
     cudaMemcpyAsync(counts, offsets, sizeof(int) * (size_t)total_tiles, cudaMemcpyDeviceToDevice, stream);

@@ -14,22 +14,25 @@ namespace dvgb {
 constexpr int MAX_FRAGMENTS = 96;
 // Filter radii up to this (ceil) use the shared-memory tile+halo splat.
 constexpr int MAX_SMEM_RI = 8;
-// Boundary samples are counting-sorted by BND_CELL x BND_CELL-pixel cells of their
-// tile (BND_BUCKETS buckets per tile); scratch counts hold 2 * tiles * BND_BUCKETS + 1.
-constexpr int BND_CELL = 4;
-constexpr int BND_BUCKETS = (16 / BND_CELL) * (16 / BND_CELL);
+// Boundary samples are counting-sorted by cell x cell-pixel cells of their tile
+// (cell in {2, 4, 8, 16}: bnd_buckets(cell) buckets per tile); scratch counts hold
+// 2 * tiles * BND_MAX_BUCKETS + 1.
+constexpr int BND_MAX_BUCKETS = (16 / 2) * (16 / 2);
+inline int bnd_buckets(int cell) { return (16 / cell) * (16 / cell); }
 
 struct SampleParams {
     int sxn, syn;
     uint32_t seed;
     bool jitter;
+    int layout;  // 1: a warp holds all sub-samples of 32/spp pixels; 0: one sub-sample of 32 pixels
 };
 struct BoundaryParams {
     uint64_t num_samples;  // one past the last sample index of this launch
     uint64_t sample_base;  // first sample index of this launch
     uint64_t slot_base;    // sample index stored in scratch slot 0
     uint32_t seed;
-    int rng;  // 0 PCG32, 1 Philox
+    int rng;   // 0 PCG32, 1 Philox
+    int cell;  // boundary sort cell edge in pixels (2, 4, 8 or 16)
 };
 // One drawn edge sample (64 bytes), kept in scratch between the boundary stages.
 struct BSample {
@@ -106,7 +109,7 @@ int launch_interior(const DevScene& S, const SampleParams& sp, const float* d_re
 int launch_interior_prefilter(const DevScene& S, const SampleParams& sp, const float* d_render, const float* wsum,
                               const GradPtrs& G, unsigned* status, cudaStream_t stream);
 // Boundary pass in chunks of at most `capacity` samples; scratch: samples[capacity],
-// key[capacity], order[capacity], counts[2*tiles*BND_BUCKETS+1].
+// key[capacity], order[capacity], counts[2*tiles*BND_MAX_BUCKETS+1].
 int launch_boundary(const DevScene& S, const BoundaryParams& bp, const float* d_render, const float* wsum,
                     const GradPtrs& G, BSample* samples, int* key, int* counts, int* order, uint64_t capacity,
                     cudaStream_t stream);
@@ -122,8 +125,8 @@ int launch_interior_batch(const BatchEntry* B, const int* item_scene, int items,
                           cudaStream_t stream);
 int launch_interior_prefilter_batch(const BatchEntry* B, const int* item_scene, int items, unsigned* status,
                                     cudaStream_t stream);
-int launch_boundary_batch(const BatchEntry* B, int nscenes, uint64_t total, int total_tiles, BSample* samples, int* key,
-                          int* counts, int* order, cudaStream_t stream);
+int launch_boundary_batch(const BatchEntry* B, int nscenes, uint64_t total, int total_tiles, int cell,
+                          BSample* samples, int* key, int* counts, int* order, cudaStream_t stream);
 // Optimisation step: Adam on the selected parameters of every scene, then the
 // scene tables that depend on path points are rebuilt in place (segments, path and
 // group BVHs, group canvas boxes, boundary-sampling tables).  Tile binning is

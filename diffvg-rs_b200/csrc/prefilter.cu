@@ -288,7 +288,7 @@ __device__ __forceinline__ void forward_prefilter_body(const DevScene& S, const 
     const int tx = tile % S.tiles_x, ty = tile / S.tiles_x;
     const int spp = sp.sxn * sp.syn;
     const int s_in_tile = round * 256 + (int)threadIdx.x;
-    const int pix = s_in_tile / spp, sub = s_in_tile % spp;
+    const int pix = sp.layout ? s_in_tile / spp : (int)threadIdx.x, sub = sp.layout ? s_in_tile % spp : round;
     const int x = tx * TILE + (pix % TILE), y = ty * TILE + (pix / TILE);
     if (use_sm)
         for (int i = threadIdx.x; i < HW * HW * 5; i += blockDim.x) sm[i] = 0.0f;
@@ -733,7 +733,7 @@ __device__ __forceinline__ void interior_prefilter_body(const DevScene& S, const
     const int tx = tile % S.tiles_x, ty = tile / S.tiles_x;
     const int spp = sp.sxn * sp.syn;
     const int s_in_tile = round * 256 + (int)threadIdx.x;
-    const int pix = s_in_tile / spp, sub = s_in_tile % spp;
+    const int pix = sp.layout ? s_in_tile / spp : (int)threadIdx.x, sub = sp.layout ? s_in_tile % spp : round;
     const int x = tx * TILE + (pix % TILE), y = ty * TILE + (pix / TILE);
     const bool valid = x < S.width && y < S.height;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;

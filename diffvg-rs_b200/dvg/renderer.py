@@ -47,8 +47,13 @@ EXPORTED = (
     "dvg_scene_digest", "dvg_render_sdf_host", "dvg_render_sdf_device", "dvg_render_sdf",
     "dvg_eval_positions_host", "dvg_eval_positions_device", "dvg_eval_positions",
     "dvg_eval_positions_backward_host", "dvg_eval_positions_backward_device", "dvg_eval_positions_backward",
-    "dvg_lbvh_build",
+    "dvg_lbvh_build", "dvg_scene_set_tuning", "dvg_scene_get_tuning", "dvg_scene_autotune", "dvg_batch_set_tuning",
+    "dvg_batch_autotune",
 )
+
+
+class TuningC(C.Structure):
+    _fields_ = [("sample_layout", C.c_uint32), ("boundary_cell", C.c_uint32)]
 
 
 class AdamOptionsC(C.Structure):
@@ -126,6 +131,14 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.dvg_scene_digest.argtypes = [vp, vp, C.POINTER(C.c_uint64)]
     L.dvg_lbvh_build.argtypes = [vp, fp, C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(C.c_int32), fp]
     L.dvg_lbvh_build.restype = C.c_int
+    L.dvg_scene_set_tuning.argtypes = [vp, C.POINTER(TuningC)]
+    L.dvg_scene_get_tuning.argtypes = [vp, C.POINTER(TuningC)]
+    L.dvg_scene_autotune.argtypes = [vp, vp, R, B, vp, C.POINTER(TuningC)]
+    L.dvg_batch_set_tuning.argtypes = [vp, C.POINTER(TuningC)]
+    L.dvg_batch_autotune.argtypes = [vp, C.POINTER(TuningC)]
+    for name in ("dvg_scene_set_tuning", "dvg_scene_get_tuning", "dvg_scene_autotune", "dvg_batch_set_tuning",
+                 "dvg_batch_autotune"):
+        getattr(L, name).restype = C.c_int
     L.dvg_render_sdf_host.argtypes = [vp, vp, R, fp]
     L.dvg_render_sdf_device.argtypes = [vp, vp, R, vp]
     L.dvg_render_sdf.argtypes = [vp, D, R, fp]
@@ -253,6 +266,25 @@ class UploadedScene:
         b = backward_options_c(bopts)
         _check(self.renderer.lib.dvg_render_backward_device(self.renderer.ctx, self.handle, C.byref(o), C.byref(b),
                                                             C.c_void_p(d_render_ptr), None, C.byref(grads.c)))
+
+    def tuning(self):
+        """(sample_layout, boundary_cell) used by this scene's launches."""
+        t = TuningC()
+        _check(self.renderer.lib.dvg_scene_get_tuning(self.handle, C.byref(t)))
+        return int(t.sample_layout), int(t.boundary_cell)
+
+    def set_tuning(self, sample_layout: int, boundary_cell: int) -> None:
+        t = TuningC(sample_layout, boundary_cell)
+        _check(self.renderer.lib.dvg_scene_set_tuning(self.handle, C.byref(t)))
+
+    def autotune(self, options: RenderOptions, bopts: Optional[BackwardOptions], target_ptr: int):
+        """dvg_scene_autotune against a device target image; returns the chosen tuning."""
+        o = render_options_c(options)
+        b = backward_options_c(bopts)
+        t = TuningC()
+        _check(self.renderer.lib.dvg_scene_autotune(self.renderer.ctx, self.handle, C.byref(o), C.byref(b),
+                                                    C.c_void_p(target_ptr), C.byref(t)))
+        return int(t.sample_layout), int(t.boundary_cell)
 
     def render_sdf_device(self, options: RenderOptions, out_ptr: int) -> None:
         """dvg_render_sdf_device into width*height floats of device memory."""
@@ -455,6 +487,16 @@ class Batch:
         out = np.zeros(len(self.scenes), np.float32)
         _check(self.renderer.lib.dvg_batch_losses(self.handle, _fp(out)))
         return out
+
+    def autotune(self):
+        """dvg_batch_autotune: returns the chosen (sample_layout, boundary_cell)."""
+        t = TuningC()
+        _check(self.renderer.lib.dvg_batch_autotune(self.handle, C.byref(t)))
+        return int(t.sample_layout), int(t.boundary_cell)
+
+    def set_tuning(self, sample_layout: int, boundary_cell: int) -> None:
+        t = TuningC(sample_layout, boundary_cell)
+        _check(self.renderer.lib.dvg_batch_set_tuning(self.handle, C.byref(t)))
 
     def set_adam(self, lr: float = 1e-2, betas=(0.9, 0.999), eps: float = 1e-8, points: bool = True,
                  paints: bool = False) -> None:

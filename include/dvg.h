@@ -172,6 +172,17 @@ typedef struct dvg_grads {
 typedef struct dvg_context dvg_context;
 typedef struct dvg_scene dvg_scene;
 
+/* Launch shape of the sample and boundary kernels (no counterpart in the crate; the
+ * results do not depend on it beyond float summation order).
+ * sample_layout: 1 = a warp holds all sub-samples of 32/spp neighbouring pixels
+ *                (default), 0 = a warp holds one sub-sample of 32 pixels.
+ * boundary_cell: boundary samples are sorted by cells of this many pixels square
+ *                inside their 16x16 tile before evaluation: 2, 4 (default), 8 or 16. */
+typedef struct dvg_tuning {
+    uint32_t sample_layout;
+    uint32_t boundary_cell;
+} dvg_tuning;
+
 /* Version of this ABI (DVG_ABI_VERSION). */
 uint32_t dvg_abi_version(void);
 
@@ -315,6 +326,19 @@ dvg_status dvg_batch_set_adam(dvg_batch* batch, const dvg_adam_options* opts);
  * synchronises, and brings the scene's own handle up to date so it can be rendered
  * or differentiated outside the batch. */
 dvg_status dvg_batch_scene_params(dvg_batch* batch, uint32_t index, float* host_points, float* host_paint_params);
+
+/* Launch-shape tuning of an uploaded scene (see dvg_tuning).  dvg_scene_autotune times
+ * dvg_fwd_bwd_l2_device on the scene with each warp layout and each boundary cell
+ * (device target image, width*height*4 floats; the scene's own gradient buffers are
+ * used as scratch), keeps the fastest for later calls and returns it.  Synchronises. */
+dvg_status dvg_scene_set_tuning(dvg_scene* scene, const dvg_tuning* tuning);
+dvg_status dvg_scene_get_tuning(const dvg_scene* scene, dvg_tuning* tuning);
+dvg_status dvg_scene_autotune(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
+                              const dvg_backward_options* bopts, const float* target_rgba, dvg_tuning* out);
+/* The same for a batch: times directly enqueued steps (targets as set in the batch),
+ * keeps the fastest and drops a captured graph so the next graph step recaptures. */
+dvg_status dvg_batch_set_tuning(dvg_batch* batch, const dvg_tuning* tuning);
+dvg_status dvg_batch_autotune(dvg_batch* batch, dvg_tuning* out);
 
 /* 64-bit FNV-1a digest of an uploaded scene's prepared device tables (every table of
  * the scene arena, the tile offsets and the used tile entries, the boundary flag).
