@@ -22,7 +22,7 @@
 #define DVG_MINB_INT 2
 #endif
 #ifndef DVG_MINB_BND
-#define DVG_MINB_BND 4
+#define DVG_MINB_BND 6
 #endif
 
 namespace dvgb {
