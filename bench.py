@@ -169,7 +169,7 @@ def large_fit(r, dev, lib_stream, steps, warmup, rank):
                         "fills, W*H*spp boundary samples; fwd + L2 + bwd + Adam + re-preparation per graph replay",
             "iterations": steps, "warmup": warmup, "ms_per_iter": ms, "msamples_per_s": samples / (ms / 1e3) / 1e6,
             "loss_after_warmup": first, "loss_last": last,
-            "launch_shape": {"sample_layout": tuning[0], "boundary_cell": tuning[1]}}
+            "launch_shape": {"sample_layout": tuning[0], "boundary_cell": tuning[1], "fragment_slots": tuning[2]}}
 
 
 def batched_vs_plain(r, dev, lib_stream, flush, scenes, steps, label):
@@ -258,7 +258,7 @@ def batched_vs_plain(r, dev, lib_stream, flush, scenes, steps, label):
                "what": "fwd + L2 + bwd + Adam(lr 1e-2) on path points per scene; batched = one graph replay with "
                        "on-device Adam and scene re-preparation; plain = per scene host preparation + upload, "
                        "fused device call, gradient read-back, host Adam"},
-           "workload": label, "launch_shape": {"sample_layout": tuning[0], "boundary_cell": tuning[1]}}
+           "workload": label, "launch_shape": {"sample_layout": tuning[0], "boundary_cell": tuning[1], "fragment_slots": tuning[2]}}
     batch.close()
     for u in ups + tgts:
         u.close()
@@ -473,7 +473,8 @@ def main():
         "data": "synthetic (seeded scene generator, no dataset)",
         "config": {**cfg, "boundary_samples": bopts.boundary_samples, "l2": "flushed between timed steps "
                    "(256 MiB write outside the timed events)", "parallelism": f"weak, {world} independent scene(s)",
-                   "launch_shape": {"sample_layout": tuning[0], "boundary_cell": tuning[1], "chosen_by": "dvg_scene_autotune"}},
+                   "launch_shape": {"sample_layout": tuning[0], "boundary_cell": tuning[1],
+                                    "fragment_slots": tuning[2], "chosen_by": "dvg_scene_autotune"}},
         "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": ncu_traffic.get(name), "peak_source": peak_src,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch "

@@ -92,6 +92,7 @@ struct dvg_context {
     DevBuf accum, wsum, image, d_render, target, loss, bg_grad, trans_grad;
     DevBuf bsamples, bkey, border, bcounts;  // boundary-pass scratch
     DevBuf sdf, positions, dvalues;          // signed-distance host calls
+    DevBuf frag;                             // fragment cache of dvg_fwd_bwd_l2_device
     uint64_t launches = 0;
 };
 
@@ -107,7 +108,7 @@ struct dvg_scene {
     size_t grad_floats = 0;
     size_t arena_bytes = 0;  // bytes of prepared tables in `arena`
     const float4* g_bbox = nullptr;
-    dvg_tuning tune{1, 4};   // launch shape (dvg_scene_set_tuning / dvg_scene_autotune)
+    dvg_tuning tune{1, 4, 16};  // launch shape (dvg_scene_set_tuning / dvg_scene_autotune)
 };
 
 namespace {
@@ -155,7 +156,17 @@ SampleParams sample_params(const dvg_render_options* o, int layout = 1) {
     sp.syn = o->samples_y > 0 ? (int)o->samples_y : 1;
     sp.seed = o->seed;
     sp.jitter = o->jitter != 0 && o->use_prefiltering == 0;
+    sp.frag = nullptr;
+    sp.frag_n = nullptr;
+    sp.frag_slots = 0;
     return sp;
+}
+// Points sp at a fragment cache of frag_cache_bytes(tiles, spp, slots) bytes at `base`.
+void attach_frag(SampleParams& sp, void* base, int tiles, int slots) {
+    const size_t samples = (size_t)tiles * sp.sxn * sp.syn * 256;
+    sp.frag = static_cast<uint16_t*>(base);
+    sp.frag_n = reinterpret_cast<uint8_t*>(sp.frag + samples * (size_t)slots);
+    sp.frag_slots = slots;
 }
 dvg_status check_status(dvg_context* ctx) {
     unsigned st = 0;
@@ -396,8 +407,13 @@ void dvg_scene_destroy(dvg_scene* scene) {
     delete scene;
 }
 
-static dvg_status render_into(dvg_context* ctx, dvg_scene* sc, const dvg_render_options* opts, float* out_dev) {
+// `frag_out` non-null: the forward also fills the context's fragment cache for the
+// interior pass that follows (non-prefiltered, cache enabled by the scene's tuning);
+// *frag_out tells whether it did.
+static dvg_status render_into(dvg_context* ctx, dvg_scene* sc, const dvg_render_options* opts, float* out_dev,
+                              bool* frag_out = nullptr) {
     const DevScene& S = sc->dev;
+    if (frag_out) *frag_out = false;
     const size_t npix = (size_t)S.width * S.height;
     if (npix == 0) return DVG_OK;
     if (S.num_groups == 0) {  // Image::solid / background image (src/renderer/renderer.rs:57-66)
@@ -409,6 +425,12 @@ static dvg_status render_into(dvg_context* ctx, dvg_scene* sc, const dvg_render_
         return DVG_OK;
     }
     SampleParams sp = sample_params(opts, (int)sc->tune.sample_layout);
+    if (frag_out && !opts->use_prefiltering && sc->tune.fragment_slots > 0) {
+        const int tiles = S.tiles_x * S.tiles_y, slots = (int)sc->tune.fragment_slots;
+        CK(ctx->frag.reserve(frag_cache_bytes(tiles, sp.sxn * sp.syn, slots)));
+        attach_frag(sp, ctx->frag.ptr, tiles, slots);
+        *frag_out = true;
+    }
     CK(ctx->accum.reserve(npix * 4 * sizeof(float)));
     CK(ctx->wsum.reserve(npix * sizeof(float)));
     CK(cudaMemsetAsync(ctx->accum.ptr, 0, npix * 4 * sizeof(float), ctx->stream));
@@ -460,14 +482,16 @@ dvg_status dvg_render_host(dvg_context* ctx, dvg_scene* scene, const dvg_render_
     return check_status(ctx);
 }
 
-// Backward on device buffers.  `have_weights`: ctx->wsum already holds this scene's weights.
+// Backward on device buffers.  `have_weights`: ctx->wsum already holds this scene's
+// weights; `frag_ready`: the forward just filled ctx->frag for these options.
 static dvg_status backward_core(dvg_context* ctx, dvg_scene* sc, const dvg_render_options* opts,
                                 const dvg_backward_options* bopts, const float* d_render, const float* d_sdf,
-                                const GradPtrs& G, bool have_weights) {
+                                const GradPtrs& G, bool have_weights, bool frag_ready = false) {
     const DevScene& S = sc->dev;
     const size_t npix = (size_t)S.width * S.height;
     if (npix == 0) return DVG_OK;
     SampleParams sp = sample_params(opts, (int)sc->tune.sample_layout);
+    if (frag_ready) attach_frag(sp, ctx->frag.ptr, S.tiles_x * S.tiles_y, (int)sc->tune.fragment_slots);
     if (d_render && S.num_groups > 0) {
         if (!have_weights) {
             CK(ctx->wsum.reserve(npix * sizeof(float)));
@@ -717,7 +741,8 @@ dvg_status dvg_fwd_bwd_l2_device(dvg_context* ctx, dvg_scene* scene, const dvg_r
         CK(ctx->image.reserve(npix * 4 * sizeof(float)));
         img = ctx->image.as<float>();
     }
-    st = render_into(ctx, scene, opts, img);
+    bool frag = false;
+    st = render_into(ctx, scene, opts, img, &frag);
     if (st != DVG_OK) return st;
     CK(ctx->d_render.reserve(npix * 4 * sizeof(float)));
     if (loss_out) CK(cudaMemsetAsync(loss_out, 0, sizeof(float), ctx->stream));
@@ -731,7 +756,7 @@ dvg_status dvg_fwd_bwd_l2_device(dvg_context* ctx, dvg_scene* scene, const dvg_r
     if (!scene->dev.bg_image) G.d_background_image = nullptr;
     st = zero_grads(ctx, scene, G);
     if (st != DVG_OK) return st;
-    return backward_core(ctx, scene, opts, bopts, ctx->d_render.as<float>(), nullptr, G, true);
+    return backward_core(ctx, scene, opts, bopts, ctx->d_render.as<float>(), nullptr, G, true, frag);
 }
 
 }  // extern "C"
@@ -829,10 +854,11 @@ struct dvg_batch {
     int items = 0, total_tiles = 0, max_ri = 0;
     uint64_t total_bsamples = 0;
     DevBuf entries, item_scene, accum, wsum, image, target, d_render, loss, grads, bsamples, bkey, border, bcounts;
+    DevBuf frag;  // per-scene fragment caches (forward -> interior)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     uint64_t steps = 0;
-    dvg_tuning tune{1, 4};  // launch shape (dvg_batch_autotune)
+    dvg_tuning tune{1, 4, 16};  // launch shape (dvg_batch_autotune)
     // on-device optimisation step (dvg_batch_set_adam)
     bool adam = false;
     AdamParams ap{};
@@ -880,6 +906,27 @@ dvg_status batch_enqueue(dvg_batch* b) {
         }
     }
     CK(cudaGetLastError());
+    return DVG_OK;
+}
+// Applies b->tune to the host entries: warp layout, and one fragment cache per scene
+// inside b->frag (none when prefiltering or with zero slots).
+dvg_status batch_apply_tuning(dvg_batch* b) {
+    const int slots = b->opts.use_prefiltering ? 0 : (int)b->tune.fragment_slots;
+    std::vector<size_t> off;
+    size_t total = 0;
+    for (const BatchEntry& e : b->host_entries) {
+        off.push_back(total);
+        total += (frag_cache_bytes(e.S.tiles_x * e.S.tiles_y, e.sp.sxn * e.sp.syn, slots) + 255) & ~(size_t)255;
+    }
+    if (slots > 0) CK(b->frag.reserve(total));
+    for (size_t i = 0; i < b->host_entries.size(); ++i) {
+        BatchEntry& e = b->host_entries[i];
+        e.sp.layout = (int)b->tune.sample_layout;
+        e.sp.frag = nullptr;
+        e.sp.frag_n = nullptr;
+        e.sp.frag_slots = 0;
+        if (slots > 0) attach_frag(e.sp, b->frag.as<char>() + off[i], e.S.tiles_x * e.S.tiles_y, slots);
+    }
     return DVG_OK;
 }
 void batch_drop_graph(dvg_batch* b) {
@@ -986,6 +1033,8 @@ extern "C" dvg_status dvg_batch_create(dvg_context* ctx, dvg_scene* const* scene
         e.G.d_background_image = nullptr;
         e.G.d_translation = nullptr;
     }
+    st = batch_apply_tuning(b.get());
+    if (st != DVG_OK) return st;
     CK(b->entries.reserve(count * sizeof(BatchEntry)));
     CK(cudaMemcpyAsync(b->entries.ptr, b->host_entries.data(), count * sizeof(BatchEntry), cudaMemcpyHostToDevice,
                        ctx->stream));
@@ -1440,12 +1489,14 @@ extern "C" dvg_status dvg_lbvh_build(dvg_context* ctx, const float* boxes, uint3
 namespace {
 bool tuning_valid(const dvg_tuning* t) {
     return t && t->sample_layout <= 1 &&
-           (t->boundary_cell == 2 || t->boundary_cell == 4 || t->boundary_cell == 8 || t->boundary_cell == 16);
+           (t->boundary_cell == 2 || t->boundary_cell == 4 || t->boundary_cell == 8 || t->boundary_cell == 16) &&
+           t->fragment_slots <= (uint32_t)FRAG_MAX_SLOTS;
 }
-// The candidates: both warp layouts with the default cell, then every cell with the
-// better layout (the boundary pass does not depend on the layout).
+// The candidates: both warp layouts with the default cell and cache, then every cell
+// with the better layout (the boundary pass does not depend on the layout), then the
+// fragment-cache sizes (`try_slots`: only where the cache is used, non-prefiltered).
 template <typename Apply, typename Run>
-dvg_status autotune_loop(dvg_context* ctx, dvg_tuning* tune, Apply apply, Run run) {
+dvg_status autotune_loop(dvg_context* ctx, dvg_tuning* tune, bool try_slots, Apply apply, Run run) {
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -1463,22 +1514,27 @@ dvg_status autotune_loop(dvg_context* ctx, dvg_tuning* tune, Apply apply, Run ru
         CK(cudaEventElapsedTime(ms, e0, e1));
         return DVG_OK;
     };
+    const uint32_t slots0 = try_slots ? 16 : 0;
     dvg_status st = DVG_OK;
-    dvg_tuning best{1, 4};
+    dvg_tuning best{1, 4, slots0};
     float best_ms = 0.0f, ms = 0.0f;
-    st = time_of(dvg_tuning{1, 4}, &best_ms);
-    if (st == DVG_OK) st = time_of(dvg_tuning{0, 4}, &ms);
-    if (st == DVG_OK && ms < best_ms) {
-        best = dvg_tuning{0, 4};
-        best_ms = ms;
-    }
-    const uint32_t cells[3] = {2, 8, 16};
-    for (int k = 0; k < 3 && st == DVG_OK; ++k) {
-        st = time_of(dvg_tuning{best.sample_layout, cells[k]}, &ms);
+    auto consider = [&](dvg_tuning t) {
+        if (st != DVG_OK) return;
+        st = time_of(t, &ms);
         if (st == DVG_OK && ms < best_ms) {
-            best = dvg_tuning{best.sample_layout, cells[k]};
+            best = t;
             best_ms = ms;
         }
+    };
+    st = time_of(best, &best_ms);
+    consider(dvg_tuning{0, 4, slots0});
+    const uint32_t cells[3] = {2, 8, 16};
+    const dvg_tuning base = best;
+    for (int k = 0; k < 3; ++k) consider(dvg_tuning{base.sample_layout, cells[k], slots0});
+    if (try_slots) {
+        const uint32_t slots[3] = {0, 8, 32};
+        const dvg_tuning b2 = best;
+        for (int k = 0; k < 3; ++k) consider(dvg_tuning{b2.sample_layout, b2.boundary_cell, slots[k]});
     }
     *tune = best;
     if (st == DVG_OK) st = apply();
@@ -1519,7 +1575,7 @@ extern "C" dvg_status dvg_scene_autotune(dvg_context* ctx, dvg_scene* scene, con
     g.d_filter_radius = G.d_filter_radius;
     g.d_background = G.d_background;
     st = autotune_loop(
-        ctx, &scene->tune, []() { return DVG_OK; },
+        ctx, &scene->tune, opts->use_prefiltering == 0, []() { return DVG_OK; },
         [&]() { return dvg_fwd_bwd_l2_device(ctx, scene, opts, bopts, target_rgba, nullptr, nullptr, &g); });
     if (st != DVG_OK) return st;
     if (out) *out = scene->tune;
@@ -1533,9 +1589,13 @@ extern "C" dvg_status dvg_batch_set_tuning(dvg_batch* b, const dvg_tuning* tunin
     CK(cudaStreamSynchronize(ctx->stream));
     batch_drop_graph(b);
     b->tune = *tuning;
-    for (auto& e : b->host_entries) e.sp.layout = (int)tuning->sample_layout;
-    CK(cudaMemcpyAsync(b->entries.ptr, b->host_entries.data(), b->host_entries.size() * sizeof(BatchEntry),
-                       cudaMemcpyHostToDevice, ctx->stream));
+    // start from the device entries: the optimisation step updates some of their fields
+    const size_t eb = b->host_entries.size() * sizeof(BatchEntry);
+    CK(cudaMemcpyAsync(b->host_entries.data(), b->entries.ptr, eb, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    dvg_status st = batch_apply_tuning(b);
+    if (st != DVG_OK) return st;
+    CK(cudaMemcpyAsync(b->entries.ptr, b->host_entries.data(), eb, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return DVG_OK;
 }
@@ -1550,7 +1610,8 @@ extern "C" dvg_status dvg_batch_autotune(dvg_batch* b, dvg_tuning* out) {
     const bool adam = b->adam;
     b->adam = false;  // time forward + loss + backward only: the parameters must not move
     dvg_status st = autotune_loop(
-        ctx, &t, [&]() { return dvg_batch_set_tuning(b, &t); }, [&]() { return batch_enqueue(b); });
+        ctx, &t, b->opts.use_prefiltering == 0, [&]() { return dvg_batch_set_tuning(b, &t); },
+        [&]() { return batch_enqueue(b); });
     b->adam = adam;
     if (st != DVG_OK) return st;
     if (out) *out = b->tune;

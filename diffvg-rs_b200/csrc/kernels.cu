@@ -137,6 +137,15 @@ __device__ __forceinline__ void forward_body(const DevScene& S, const SamplePara
     if (x < S.width && y < S.height) {
         const int sx = sub % sp.sxn, sy = sub / sp.sxn;
         const float2 pt = sample_pos(x, y, sx, sy, sp.sxn, sp.syn, S.width, sp.seed, sp.jitter);
+        // Fragment cache (see SampleParams): kept only where the interior pass, which
+        // normalises the sample point by the canvas size and scales it back
+        // (src/backward/render.rs:111, src/backward/sampling.rs:91), tests the same point.
+        const size_t fstride = (size_t)S.tiles_x * S.tiles_y * spp * 256;
+        const size_t sid = ((size_t)tile * spp + round) * 256 + threadIdx.x;
+        const bool cache = sp.frag != nullptr && n <= FRAG_MAX_ENTRIES &&
+                           (pt.x / (float)S.width) * (float)S.width == pt.x &&
+                           (pt.y / (float)S.height) * (float)S.height == pt.y;
+        int nf = 0;
         float4 acc = background_premul(S, y * S.width + x);
         for (int e = 0; e < n; ++e) {
             const int g = __ldg(&list[e]);
@@ -148,8 +157,15 @@ __device__ __forceinline__ void forward_body(const DevScene& S, const SamplePara
             hitp[1] = gi.x >= 0 && group_inside(S, g, lp, gi.z) ? gi.x : -1;
 #pragma unroll 1
             for (int which = 0; which < 2; ++which)
-                if (hitp[which] >= 0) over(acc, paint_color(S, hitp[which], pt));
+                if (hitp[which] >= 0) {
+                    over(acc, paint_color(S, hitp[which], pt));
+                    if (cache) {
+                        if (nf < sp.frag_slots) sp.frag[(size_t)nf * fstride + sid] = (uint16_t)(2 * e + which);
+                        ++nf;
+                    }
+                }
         }
+        if (sp.frag) sp.frag_n[sid] = cache && nf <= sp.frag_slots ? (uint8_t)nf : FRAG_NONE;
         splat_sample(S, x, y, tx, ty, ri, HW, use_sm, pt, acc, sm, accum, wsum);
     }
     if (!use_sm) return;
@@ -255,13 +271,29 @@ __device__ __forceinline__ void interior_body(const DevScene& S, const SamplePar
     bool overflow = false;
     float4 acc = bg;
     if (valid) {
-        for (int e = 0; e < n; ++e) {
-            const int g = __ldg(&list[e]);
-            const int4 gi = __ldg(&S.g_info[g]);
-            const float2 lp = xf9(S.g_c2s + 9 * g, pt);
-            int hitp[2];
-            hitp[0] = gi.y >= 0 && group_within(S, g, lp) ? gi.y : -1;
-            hitp[1] = gi.x >= 0 && group_inside(S, g, lp, gi.z) ? gi.x : -1;
+        // Either the forward's cached fragment codes (one fragment per step) or the
+        // tile's group list with both hit tests (up to two fragments per step).
+        const size_t fstride = (size_t)S.tiles_x * S.tiles_y * spp * 256;
+        const size_t sid = ((size_t)tile * spp + round) * 256 + threadIdx.x;
+        const int cn = sp.frag ? (int)__ldcs(&sp.frag_n[sid]) : (int)FRAG_NONE;
+        const bool cached = cn != (int)FRAG_NONE;
+        const int steps = cached ? cn : n;
+        for (int k = 0; k < steps; ++k) {
+            int e, hitp[2];
+            if (cached) {
+                const int c0 = __ldcs(&sp.frag[(size_t)k * fstride + sid]);
+                e = c0 >> 1;
+                const int4 gi = __ldg(&S.g_info[__ldg(&list[e])]);
+                hitp[0] = (c0 & 1) ? -1 : gi.y;
+                hitp[1] = (c0 & 1) ? gi.x : -1;
+            } else {
+                e = k;
+                const int g = __ldg(&list[e]);
+                const int4 gi = __ldg(&S.g_info[g]);
+                const float2 lp = xf9(S.g_c2s + 9 * g, pt);
+                hitp[0] = gi.y >= 0 && group_within(S, g, lp) ? gi.y : -1;
+                hitp[1] = gi.x >= 0 && group_inside(S, g, lp, gi.z) ? gi.x : -1;
+            }
 #pragma unroll 1
             for (int which = 0; which < 2; ++which) {
                 if (hitp[which] < 0) continue;

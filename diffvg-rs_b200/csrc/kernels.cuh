@@ -20,12 +20,32 @@ constexpr int MAX_SMEM_RI = 8;
 constexpr int BND_MAX_BUCKETS = (16 / 2) * (16 / 2);
 inline int bnd_buckets(int cell) { return (16 / cell) * (16 / cell); }
 
+// Fragment cache of the fused forward -> interior paths: the forward stores, per
+// pixel sample, the codes (2 * tile-list entry + 0 stroke / 1 fill) of the fragments
+// it composited, and the interior adjoint reads them back instead of repeating the
+// hit tests.  Codes are 16-bit (tile lists up to FRAG_MAX_ENTRIES entries), stored
+// slot-major (slot k of sample s at k * samples + s, samples = tiles * spp * 256) so
+// a warp's lanes touch consecutive halves; a count of FRAG_NONE marks a sample the
+// interior re-tests (more fragments than slots, a longer tile list, or a sample
+// point that the interior's normalise-and-rescale does not reproduce exactly).
+constexpr int FRAG_MAX_ENTRIES = 32767;
+constexpr uint8_t FRAG_NONE = 0xff;
+constexpr int FRAG_MAX_SLOTS = 64;
+
 struct SampleParams {
     int sxn, syn;
     uint32_t seed;
     bool jitter;
     int layout;  // 1: a warp holds all sub-samples of 32/spp pixels; 0: one sub-sample of 32 pixels
+    uint16_t* frag;  // fragment codes (NULL: no cache)
+    uint8_t* frag_n; // per-sample code count or FRAG_NONE
+    int frag_slots;  // codes kept per sample (<= FRAG_MAX_SLOTS)
 };
+// Bytes of a fragment cache with `slots` codes per sample for one scene.
+inline size_t frag_cache_bytes(int tiles, int spp, int slots) {
+    const size_t samples = (size_t)tiles * spp * 256;
+    return samples * (2 * (size_t)slots + 1);
+}
 struct BoundaryParams {
     uint64_t num_samples;  // one past the last sample index of this launch
     uint64_t sample_base;  // first sample index of this launch

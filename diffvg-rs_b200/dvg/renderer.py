@@ -52,8 +52,12 @@ EXPORTED = (
 )
 
 
+def _tuple(t):
+    return int(t.sample_layout), int(t.boundary_cell), int(t.fragment_slots)
+
+
 class TuningC(C.Structure):
-    _fields_ = [("sample_layout", C.c_uint32), ("boundary_cell", C.c_uint32)]
+    _fields_ = [("sample_layout", C.c_uint32), ("boundary_cell", C.c_uint32), ("fragment_slots", C.c_uint32)]
 
 
 class AdamOptionsC(C.Structure):
@@ -268,13 +272,13 @@ class UploadedScene:
                                                             C.c_void_p(d_render_ptr), None, C.byref(grads.c)))
 
     def tuning(self):
-        """(sample_layout, boundary_cell) used by this scene's launches."""
+        """(sample_layout, boundary_cell, fragment_slots) used by this scene's launches."""
         t = TuningC()
         _check(self.renderer.lib.dvg_scene_get_tuning(self.handle, C.byref(t)))
-        return int(t.sample_layout), int(t.boundary_cell)
+        return _tuple(t)
 
-    def set_tuning(self, sample_layout: int, boundary_cell: int) -> None:
-        t = TuningC(sample_layout, boundary_cell)
+    def set_tuning(self, sample_layout: int, boundary_cell: int, fragment_slots: int = 16) -> None:
+        t = TuningC(sample_layout, boundary_cell, fragment_slots)
         _check(self.renderer.lib.dvg_scene_set_tuning(self.handle, C.byref(t)))
 
     def autotune(self, options: RenderOptions, bopts: Optional[BackwardOptions], target_ptr: int):
@@ -284,7 +288,7 @@ class UploadedScene:
         t = TuningC()
         _check(self.renderer.lib.dvg_scene_autotune(self.renderer.ctx, self.handle, C.byref(o), C.byref(b),
                                                     C.c_void_p(target_ptr), C.byref(t)))
-        return int(t.sample_layout), int(t.boundary_cell)
+        return _tuple(t)
 
     def render_sdf_device(self, options: RenderOptions, out_ptr: int) -> None:
         """dvg_render_sdf_device into width*height floats of device memory."""
@@ -489,13 +493,13 @@ class Batch:
         return out
 
     def autotune(self):
-        """dvg_batch_autotune: returns the chosen (sample_layout, boundary_cell)."""
+        """dvg_batch_autotune: returns the chosen (sample_layout, boundary_cell, fragment_slots)."""
         t = TuningC()
         _check(self.renderer.lib.dvg_batch_autotune(self.handle, C.byref(t)))
-        return int(t.sample_layout), int(t.boundary_cell)
+        return _tuple(t)
 
-    def set_tuning(self, sample_layout: int, boundary_cell: int) -> None:
-        t = TuningC(sample_layout, boundary_cell)
+    def set_tuning(self, sample_layout: int, boundary_cell: int, fragment_slots: int = 16) -> None:
+        t = TuningC(sample_layout, boundary_cell, fragment_slots)
         _check(self.renderer.lib.dvg_batch_set_tuning(self.handle, C.byref(t)))
 
     def set_adam(self, lr: float = 1e-2, betas=(0.9, 0.999), eps: float = 1e-8, points: bool = True,

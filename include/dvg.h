@@ -177,10 +177,17 @@ typedef struct dvg_scene dvg_scene;
  * sample_layout: 1 = a warp holds all sub-samples of 32/spp neighbouring pixels
  *                (default), 0 = a warp holds one sub-sample of 32 pixels.
  * boundary_cell: boundary samples are sorted by cells of this many pixels square
- *                inside their 16x16 tile before evaluation: 2, 4 (default), 8 or 16. */
+ *                inside their 16x16 tile before evaluation: 2, 4 (default), 8 or 16.
+ * fragment_slots: fragment codes kept per pixel sample by the forward pass of the
+ *                fused calls (dvg_fwd_bwd_l2_device, batch steps) for the interior
+ *                adjoint, which then skips its own hit tests for samples with at most
+ *                this many fragments; 0 disables the cache, at most 64, default 16.
+ *                Device memory: (2 * slots + 1) bytes per pixel sample of the scene
+ *                (W * H * spp, rounded up to whole 16x16 tiles). */
 typedef struct dvg_tuning {
     uint32_t sample_layout;
     uint32_t boundary_cell;
+    uint32_t fragment_slots;
 } dvg_tuning;
 
 /* Version of this ABI (DVG_ABI_VERSION). */

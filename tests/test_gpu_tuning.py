@@ -1,6 +1,8 @@
-"""Launch-shape tuning (dvg_tuning): every warp layout and boundary cell gives the
-same image (to float-atomic order, 2e-6) and gradients (1e-4 of scale) as the
-default; the autotuners pick a valid shape, for a scene and for a batch."""
+"""Launch-shape tuning (dvg_tuning): every warp layout, boundary cell and
+fragment-cache size gives the same image (to float-atomic order, 2e-6) and
+gradients (1e-4 of scale) as the default; the autotuners pick a valid shape, for a
+scene and for a batch.  Cache sizes of 1 and 2 slots leave many samples over the
+cap, so warps mix cached samples with samples that repeat the hit tests."""
 import numpy as np
 import pytest
 import torch
@@ -9,7 +11,8 @@ from dvg import BackwardOptions, Batch, DeviceGrads, Renderer, RenderOptions, sy
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [(1, 4), (0, 4), (1, 2), (1, 8), (1, 16), (0, 16)]
+SHAPES = [(1, 4, 16), (0, 4, 16), (1, 2, 16), (1, 8, 16), (1, 16, 16), (0, 16, 16), (1, 4, 0), (0, 4, 0),
+          (1, 4, 1), (0, 4, 2), (1, 4, 8), (1, 4, 64)]
 
 
 def _run(up, opts, bo, tgt):
@@ -35,22 +38,34 @@ def test_every_launch_shape_gives_the_same_result(prefilter):
         tgt = torch.empty(96 * 80 * 4, device="cuda")
         t.render_device(opts, tgt.data_ptr())
         ref_img, ref_g = _run(up, opts, bo, tgt)
-        for layout, cell in SHAPES:
-            up.set_tuning(layout, cell)
-            assert up.tuning() == (layout, cell)
+        for shape in SHAPES:
+            up.set_tuning(*shape)
+            assert up.tuning() == shape
             img, g = _run(up, opts, bo, tgt)
-            assert float(np.max(np.abs(img - ref_img))) <= 2e-6, (layout, cell)
+            assert float(np.max(np.abs(img - ref_img))) <= 2e-6, shape
             for k, v in ref_g.items():
                 scale = float(np.max(np.abs(v))) if v.size else 0.0
-                assert float(np.max(np.abs(g[k] - v))) <= 1e-4 * (scale + 1e-6) + 1e-6, (layout, cell, k)
+                assert float(np.max(np.abs(g[k] - v))) <= 1e-4 * (scale + 1e-6) + 1e-6, (shape, k)
         chosen = up.autotune(opts, bo, tgt.data_ptr())
-        assert chosen[0] in (0, 1) and chosen[1] in (2, 4, 8, 16) and up.tuning() == chosen
+        assert chosen[0] in (0, 1) and chosen[1] in (2, 4, 8, 16) and chosen[2] <= 64 and up.tuning() == chosen
         img, _ = _run(up, opts, bo, tgt)
         assert float(np.max(np.abs(img - ref_img))) <= 2e-6
         t.close()
         up.close()
     finally:
         r.close()
+
+
+def _batch_grads(batch, i, ups):
+    import ctypes as C
+
+    from dvg import device_view
+
+    _, _, g = batch.buffers(i)
+    d = ups[i].packed.desc
+    pts = device_view(C.cast(g.d_points, C.c_void_p).value, 2 * d.total_points).cpu().numpy()
+    pp = device_view(C.cast(g.d_paint_params, C.c_void_p).value, 4 * d.num_paints).cpu().numpy()
+    return pts, pp
 
 
 def test_batch_autotune_keeps_results():
@@ -69,9 +84,21 @@ def test_batch_autotune_keeps_results():
         b.step(False)
         ref = b.losses().copy()
         chosen = b.autotune()
-        assert chosen[0] in (0, 1) and chosen[1] in (2, 4, 8, 16)
+        assert chosen[0] in (0, 1) and chosen[1] in (2, 4, 8, 16) and chosen[2] in (0, 8, 16, 32)
         b.step(True)
         assert np.allclose(b.losses(), ref, rtol=1e-5, atol=1e-6)
+        # gradients with and without the fragment cache
+        grads = []
+        for slots in (0, 2, 16):
+            b.set_tuning(1, 4, slots)
+            b.step(True)
+            b.losses()
+            grads.append([(lambda g: (g[0].copy(), g[1].copy()))(_batch_grads(b, i, ups)) for i in range(3)])
+        for other in grads[1:]:
+            for (p0, c0), (p1, c1) in zip(grads[0], other):
+                for x, y in ((p1, p0), (c1, c0)):
+                    scale = float(np.max(np.abs(y))) if y.size else 0.0
+                    assert float(np.max(np.abs(x - y))) <= 1e-4 * (scale + 1e-6) + 1e-6
         b.close()
         for u in ups:
             u.close()
