@@ -546,6 +546,56 @@ __device__ __forceinline__ bool stroke_misses_segment(const SegGeom& s, float2 p
     return p.x < xmin - r || p.x > xmax + r || p.y < ymin - r || p.y > ymax + r;
 }
 
+// Lower bound on the distance from p to a cubic segment, for rejecting stroke
+// tests before the exact closest-point solve.  The 16-chord polyline through
+// B(k/16) lies within e = (h^2/8) max|B''| = (3 / (4 * 16^2)) max(|q0-2q1+q2|,
+// |q1-2q2+q3|) of the curve (linear-interpolation error, |B''| <= 6 max|second
+// difference|), so dist(p, curve) >= dist(p, polyline) - e.  Whenever this bound
+// exceeds the segment's largest radius by the culling margin (far above the f32
+// rounding of the polyline and of the crate's closest point), the crate's
+// `dist < radius(t)` test is false, so skipping the solve never changes a result.
+static __device__ __noinline__ float cubic_dist_lower(float px, float py, float a0, float a1, float a2, float a3,
+                                                     float a4, float a5, float a6, float a7) {
+    const float ax = -a0 + 3.0f * a2 - 3.0f * a4 + a6, ay = -a1 + 3.0f * a3 - 3.0f * a5 + a7;
+    const float bx = 3.0f * a0 - 6.0f * a2 + 3.0f * a4, by = 3.0f * a1 - 6.0f * a3 + 3.0f * a5;
+    const float cx = -3.0f * a0 + 3.0f * a2, cy = -3.0f * a1 + 3.0f * a3;
+    float best = INFINITY;  // squared distance to the polyline
+    float vx = a0 - px, vy = a1 - py;
+#pragma unroll 4
+    for (int k = 1; k <= 16; ++k) {
+        const float t = (float)k * (1.0f / 16.0f);
+        const float wx = (k == 16 ? a6 : ((ax * t + bx) * t + cx) * t + a0) - px;
+        const float wy = (k == 16 ? a7 : ((ay * t + by) * t + cy) * t + a1) - py;
+        const float ex = wx - vx, ey = wy - vy;
+        const float ee = ex * ex + ey * ey, de = -(vx * ex + vy * ey);
+        float d2;
+        if (de <= 0.0f || ee <= 0.0f) d2 = vx * vx + vy * vy;
+        else if (de >= ee) d2 = wx * wx + wy * wy;
+        else d2 = fmaxf(vx * vx + vy * vy - de * (de / ee), 0.0f);
+        best = fminf(best, d2);
+        vx = wx;
+        vy = wy;
+    }
+    const float s0x = a0 - 2.0f * a2 + a4, s0y = a1 - 2.0f * a3 + a5;
+    const float s1x = a2 - 2.0f * a4 + a6, s1y = a3 - 2.0f * a5 + a7;
+    const float e = (3.0f / 1024.0f) * sqrtf(fmaxf(s0x * s0x + s0y * s0y, s1x * s1x + s1y * s1y));
+    return sqrtf(best) - e;
+}
+__device__ __forceinline__ bool stroke_far_from_cubic(const SegGeom& s, float2 p) {
+    float r = fmaxf(fmaxf(s.r[0], s.r[1]), fmaxf(s.r[2], s.r[3]));
+    float m = cull_margin(s, p) + 1.0e-5f * fabsf(r);
+    return cubic_dist_lower(p.x, p.y, s.q[0], s.q[1], s.q[2], s.q[3], s.q[4], s.q[5], s.q[6], s.q[7]) > r + m;
+}
+
+// Nearest-segment searches keep a segment only when its distance is strictly below
+// the best so far; a cubic whose lower bound exceeds that by the culling margin
+// cannot be kept, so its exact solve is skipped (same argument as above).
+__device__ __forceinline__ bool cubic_cannot_beat(const SegGeom& s, float2 p, bool approx, float best) {
+    if (s.kind != 2 || approx || !(best < INFINITY)) return false;
+    return cubic_dist_lower(p.x, p.y, s.q[0], s.q[1], s.q[2], s.q[3], s.q[4], s.q[5], s.q[6], s.q[7]) >
+           best + cull_margin(s, p);
+}
+
 // ------------------------------------------------------------------ path queries
 // Walks the path's BVH (preorder with skip links).  Node tests are exactly the
 // crate's: ray test for winding (winding.rs:117-126), containment for strokes.
@@ -602,6 +652,7 @@ __device__ __forceinline__ bool within_path_bvh(const DevScene& S, int path, flo
                 SegGeom sg;
                 load_seg(S, __ldg(&S.pl_segs[k]), sg);
                 if (stroke_misses_segment(sg, p)) continue;
+                if (sg.kind == 2 && !approx && stroke_far_from_cubic(sg, p)) continue;
                 CPRes c = seg_closest(sg, p, approx);
                 if (c.dist < seg_radius(sg, c.t)) return true;
             }
@@ -619,6 +670,7 @@ __device__ __forceinline__ bool within_path_list(const DevScene& S, int path, fl
         SegGeom sg;
         load_seg(S, pi.x + k, sg);
         if (stroke_misses_segment(sg, p)) continue;
+        if (sg.kind == 2 && !approx && stroke_far_from_cubic(sg, p)) continue;
         CPRes c = seg_closest(sg, p, approx);
         if (c.dist < seg_radius(sg, c.t)) return true;
     }

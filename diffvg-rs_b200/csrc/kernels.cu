@@ -6,6 +6,7 @@
 //   k_weights      filter-weight image only (backward without a preceding forward)
 //   k_resolve      Σ(c·w)/Σw and un-premultiply            (forward.rs:294-334)
 //   k_interior     interior adjoint per sample             (backward/render.rs:95-169)
+//   k_interior_cached  the same for samples whose fragments the forward cached
 //   k_boundary     edge sampling adjoint per boundary sample (backward/boundary.rs:141-196)
 //   k_l2           L2 loss and d_render
 //
@@ -23,6 +24,9 @@
 #endif
 #ifndef DVG_MINB_BND
 #define DVG_MINB_BND 6
+#endif
+#ifndef DVG_MINB_LEAN
+#define DVG_MINB_LEAN 4
 #endif
 
 namespace dvgb {
@@ -231,11 +235,17 @@ __global__ void k_resolve(DevScene S, const float* accum, const float* wsum, flo
 // ------------------------------------------------------------------ interior backward
 // Per sample: gather d_color (filters.rs:70-103), recompute the fragments of
 // sample_color (sampling.rs:76-224) and back-propagate through compositing,
-// paints, background and the filter (filters.rs:106-156).  The fragment list is
-// rebuilt from the BVH; only (fragment code, transmittance) pairs live in
-// per-thread local memory, never in HBM.  The adjoint loop walks the tile's
-// group list in the same order on every lane so solid-paint gradients reduce
-// across the warp before one atomic.
+// paints, background and the filter (filters.rs:106-156).  The fragment list comes
+// from the forward's fragment cache or is rebuilt from the BVHs; only (fragment
+// code, transmittance) pairs live in per-thread local memory.  The adjoint loop
+// walks the tile's group list in the same order on every lane so solid-paint
+// gradients reduce across the warp before one atomic.
+//
+// LEAN: the kernel takes only the samples with cached fragments and carries no hit
+// tests (fewer registers, more resident warps for its load chains); otherwise it
+// takes every sample without a cache entry (all samples when there is no cache).
+// Each sample is handled by exactly one of the two launches.
+template <bool LEAN>
 __device__ __forceinline__ void interior_body(const DevScene& S, const SampleParams& sp, int tile, int round,
                                               const float* d_render, const float* wsum, const GradPtrs& G,
                                               unsigned* status) {
@@ -245,7 +255,12 @@ __device__ __forceinline__ void interior_body(const DevScene& S, const SamplePar
     const int s_in_tile = round * 256 + (int)threadIdx.x;
     const int pix = sp.layout ? s_in_tile / spp : (int)threadIdx.x, sub = sp.layout ? s_in_tile % spp : round;
     const int x = tx * TILE + (pix % TILE), y = ty * TILE + (pix / TILE);
-    const bool valid = x < S.width && y < S.height;
+    const size_t fstride = (size_t)S.tiles_x * S.tiles_y * spp * 256;
+    const size_t sid = ((size_t)tile * spp + round) * 256 + threadIdx.x;
+    const bool inside = x < S.width && y < S.height;
+    const int cn = inside && sp.frag ? (int)__ldcs(&sp.frag_n[sid]) : (int)FRAG_NONE;
+    const bool valid = inside && (LEAN ? cn != (int)FRAG_NONE : cn == (int)FRAG_NONE);
+    if (!__syncthreads_or(valid)) return;  // uniform per CTA
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int off = S.tile_offsets[tile];
     const int n = S.tile_offsets[tile + 1] - off;
@@ -273,14 +288,10 @@ __device__ __forceinline__ void interior_body(const DevScene& S, const SamplePar
     if (valid) {
         // Either the forward's cached fragment codes (one fragment per step) or the
         // tile's group list with both hit tests (up to two fragments per step).
-        const size_t fstride = (size_t)S.tiles_x * S.tiles_y * spp * 256;
-        const size_t sid = ((size_t)tile * spp + round) * 256 + threadIdx.x;
-        const int cn = sp.frag ? (int)__ldcs(&sp.frag_n[sid]) : (int)FRAG_NONE;
-        const bool cached = cn != (int)FRAG_NONE;
-        const int steps = cached ? cn : n;
+        const int steps = LEAN ? cn : n;
         for (int k = 0; k < steps; ++k) {
             int e, hitp[2];
-            if (cached) {
+            if constexpr (LEAN) {
                 const int c0 = __ldcs(&sp.frag[(size_t)k * fstride + sid]);
                 e = c0 >> 1;
                 const int4 gi = __ldg(&S.g_info[__ldg(&list[e])]);
@@ -431,7 +442,12 @@ __device__ __forceinline__ void interior_body(const DevScene& S, const SamplePar
 
 __global__ void __launch_bounds__(256, DVG_MINB_INT) k_interior(DevScene S, SampleParams sp, const float* d_render,
                                                                 const float* wsum, GradPtrs G, unsigned* status) {
-    interior_body(S, sp, blockIdx.x, blockIdx.y, d_render, wsum, G, status);
+    interior_body<false>(S, sp, blockIdx.x, blockIdx.y, d_render, wsum, G, status);
+}
+__global__ void __launch_bounds__(256, DVG_MINB_LEAN) k_interior_cached(DevScene S, SampleParams sp,
+                                                                        const float* d_render, const float* wsum,
+                                                                        GradPtrs G, unsigned* status) {
+    interior_body<true>(S, sp, blockIdx.x, blockIdx.y, d_render, wsum, G, status);
 }
 __global__ void __launch_bounds__(256, DVG_MINB_INT) k_interior_batch(const BatchEntry* __restrict__ B,
                                                                       const int* __restrict__ item_scene,
@@ -440,7 +456,17 @@ __global__ void __launch_bounds__(256, DVG_MINB_INT) k_interior_batch(const Batc
     const BatchEntry& E = B[item_scene[item]];
     const int local = item - E.item_off;
     const int tiles = E.S.tiles_x * E.S.tiles_y;
-    interior_body(E.S, E.sp, local % tiles, local / tiles, E.d_render, E.wsum, E.G, status);
+    interior_body<false>(E.S, E.sp, local % tiles, local / tiles, E.d_render, E.wsum, E.G, status);
+}
+__global__ void __launch_bounds__(256, DVG_MINB_LEAN) k_interior_cached_batch(const BatchEntry* __restrict__ B,
+                                                                              const int* __restrict__ item_scene,
+                                                                              unsigned* status) {
+    const int item = blockIdx.x;
+    const BatchEntry& E = B[item_scene[item]];
+    if (!E.sp.frag) return;  // uniform per CTA
+    const int local = item - E.item_off;
+    const int tiles = E.S.tiles_x * E.S.tiles_y;
+    interior_body<true>(E.S, E.sp, local % tiles, local / tiles, E.d_render, E.wsum, E.G, status);
 }
 
 // ------------------------------------------------------------------ boundary sampling
@@ -1231,8 +1257,9 @@ int launch_resolve(const DevScene& S, const float* accum, const float* wsum, flo
 int launch_interior(const DevScene& S, const SampleParams& sp, const float* d_render, const float* wsum,
                     const GradPtrs& G, unsigned* status, cudaStream_t stream) {
     dim3 grid(S.tiles_x * S.tiles_y, sp.sxn * sp.syn);
+    if (sp.frag) k_interior_cached<<<grid, 256, 0, stream>>>(S, sp, d_render, wsum, G, status);
     k_interior<<<grid, 256, 0, stream>>>(S, sp, d_render, wsum, G, status);
-    return 1;
+    return sp.frag ? 2 : 1;
 }
 int launch_boundary(const DevScene& S, const BoundaryParams& bp, const float* d_render, const float* wsum,
                     const GradPtrs& G, BSample* samples, int* key, int* counts, int* order, uint64_t capacity,
@@ -1288,8 +1315,9 @@ int launch_pixels_batch(const BatchEntry* B, int nscenes, size_t max_pixels, int
 }
 int launch_interior_batch(const BatchEntry* B, const int* item_scene, int items, unsigned* status,
                           cudaStream_t stream) {
+    k_interior_cached_batch<<<items, 256, 0, stream>>>(B, item_scene, status);
     k_interior_batch<<<items, 256, 0, stream>>>(B, item_scene, status);
-    return 1;
+    return 2;
 }
 int launch_boundary_batch(const BatchEntry* B, int nscenes, uint64_t total, int total_tiles, int cell,
                           BSample* samples, int* key, int* counts, int* order, cudaStream_t stream) {

@@ -52,6 +52,7 @@ __device__ bool closest_path_bvh(const DevScene& S, int path, float2 p, float2* 
                 const int sidx = __ldg(&S.pl_segs[k]);
                 SegGeom sg;
                 load_seg(S, sidx, sg);
+                if (cubic_cannot_beat(sg, p, approx, best)) continue;
                 CPRes c = seg_closest(sg, p, approx);
                 if (c.dist < best) {
                     best = c.dist;
@@ -129,6 +130,7 @@ __device__ bool closest_shape(const DevScene& S, int s, float2 lp, float2* out, 
         for (int k = 0; k < pi.y; ++k) {
             SegGeom sg;
             load_seg(S, pi.x + k, sg);
+            if (cubic_cannot_beat(sg, p, approx, best)) continue;
             CPRes cc = seg_closest(sg, p, approx);
             if (cc.dist < best) {
                 best = cc.dist;
