@@ -92,8 +92,19 @@ struct dvg_context {
     DevBuf accum, wsum, image, d_render, target, loss, bg_grad, trans_grad;
     DevBuf bsamples, bkey, border, bcounts;  // boundary-pass scratch
     DevBuf sdf, positions, dvalues;          // signed-distance host calls
-    DevBuf frag;                             // fragment cache of dvg_fwd_bwd_l2_device
+    DevBuf frag;                             // fragment cache of the fused calls
     uint64_t launches = 0;
+    // Retained render: dvg_render keeps its prepared scene, and its weight image and
+    // fragment cache stay valid until the next call that writes them (gen counts
+    // those calls), so a dvg_render_backward of the same description and options
+    // reuses all three instead of preparing, uploading and re-testing again.
+    bool retain = true;
+    uint64_t gen = 0;
+    dvg_scene* kept = nullptr;
+    std::vector<char> kept_key;
+    dvg_render_options kept_opts{};
+    uint64_t kept_gen = 0;
+    bool kept_weights = false, kept_frag = false;
 };
 
 struct dvg_scene {
@@ -143,6 +154,65 @@ GradPtrs device_grads(dvg_scene* sc) {
     g.d_background_image = nullptr;
     g.d_translation = nullptr;
     return g;
+}
+
+// Byte image of a scene description: every scalar and every array it points to
+// (a marker byte for each optional array left NULL).  Equal images prepare to the
+// same device scene.
+void desc_key(const dvg_scene_desc* d, std::vector<char>& k) {
+    k.clear();
+    auto put = [&](const void* p, size_t n) {
+        const char* c = static_cast<const char*>(p);
+        k.insert(k.end(), c, c + n);
+    };
+    auto arr = [&](const void* p, size_t n) {
+        const char mark = p ? 1 : 0;
+        put(&mark, 1);
+        if (p && n) put(p, n);
+    };
+    const size_t ns = d->num_shapes, ng = d->num_groups, np = d->num_paints;
+    put(&d->width, sizeof d->width);
+    put(&d->height, sizeof d->height);
+    put(d->background, sizeof d->background);
+    put(&d->filter_type, sizeof d->filter_type);
+    put(&d->filter_radius, sizeof d->filter_radius);
+    put(&d->num_shapes, sizeof d->num_shapes);
+    put(&d->total_ctrl, sizeof d->total_ctrl);
+    put(&d->total_points, sizeof d->total_points);
+    put(&d->num_groups, sizeof d->num_groups);
+    put(&d->total_group_shapes, sizeof d->total_group_shapes);
+    put(&d->num_paints, sizeof d->num_paints);
+    put(&d->total_stops, sizeof d->total_stops);
+    arr(d->background_image, d->background_image ? (size_t)d->width * d->height * 4 * sizeof(float) : 0);
+    arr(d->shape_kind, ns * 4);
+    arr(d->shape_params, ns * 16);
+    arr(d->shape_transform, ns * 36);
+    arr(d->shape_stroke_width, ns * 4);
+    arr(d->shape_stroke_join, ns * 4);
+    arr(d->shape_stroke_cap, ns * 4);
+    arr(d->shape_miter_limit, ns * 4);
+    arr(d->path_ctrl_offset, ns * 4);
+    arr(d->path_ctrl_count, ns * 4);
+    arr(d->path_point_offset, ns * 4);
+    arr(d->path_point_count, ns * 4);
+    arr(d->path_flags, ns * 4);
+    arr(d->num_control_points, d->total_ctrl);
+    arr(d->points, (size_t)d->total_points * 8);
+    arr(d->thickness, (size_t)d->total_points * 4);
+    arr(d->group_shape_offset, ng * 4);
+    arr(d->group_shape_count, ng * 4);
+    arr(d->group_shape_ids, (size_t)d->total_group_shapes * 4);
+    arr(d->group_fill_rule, ng * 4);
+    arr(d->group_shape_to_canvas, ng * 36);
+    arr(d->group_canvas_to_shape, ng * 36);
+    arr(d->group_fill_paint, ng * 4);
+    arr(d->group_stroke_paint, ng * 4);
+    arr(d->paint_kind, np * 4);
+    arr(d->paint_params, np * 16);
+    arr(d->paint_stop_offset, np * 4);
+    arr(d->paint_stop_count, np * 4);
+    arr(d->stop_offsets, (size_t)d->total_stops * 4);
+    arr(d->stop_colors, (size_t)d->total_stops * 16);
 }
 
 dvg_status check_options(const dvg_render_options* o) {
@@ -275,9 +345,22 @@ dvg_status dvg_context_create(int device, dvg_context** out) {
     return DVG_OK;
 }
 
+dvg_status dvg_context_set_retain(dvg_context* ctx, int enable) {
+    if (!ctx) return fail(DVG_ERR_INVALID_ARGUMENT, "null context");
+    ctx->retain = enable != 0;
+    if (!ctx->retain && ctx->kept) {
+        CK(cudaSetDevice(ctx->device));
+        dvg_scene_destroy(ctx->kept);
+        ctx->kept = nullptr;
+    }
+    return DVG_OK;
+}
+
 void dvg_context_destroy(dvg_context* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
+    if (ctx->kept) dvg_scene_destroy(ctx->kept);
+    ctx->kept = nullptr;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->status) cudaFree(ctx->status);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -410,10 +493,12 @@ void dvg_scene_destroy(dvg_scene* scene) {
 // `frag_out` non-null: the forward also fills the context's fragment cache for the
 // interior pass that follows (non-prefiltered, cache enabled by the scene's tuning);
 // *frag_out tells whether it did.
+// *weights_out: whether ctx->wsum now holds this scene's weight image.
 static dvg_status render_into(dvg_context* ctx, dvg_scene* sc, const dvg_render_options* opts, float* out_dev,
-                              bool* frag_out = nullptr) {
+                              bool* frag_out = nullptr, bool* weights_out = nullptr) {
     const DevScene& S = sc->dev;
     if (frag_out) *frag_out = false;
+    if (weights_out) *weights_out = false;
     const size_t npix = (size_t)S.width * S.height;
     if (npix == 0) return DVG_OK;
     if (S.num_groups == 0) {  // Image::solid / background image (src/renderer/renderer.rs:57-66)
@@ -424,6 +509,7 @@ static dvg_status render_into(dvg_context* ctx, dvg_scene* sc, const dvg_render_
         CK(cudaGetLastError());
         return DVG_OK;
     }
+    ++ctx->gen;  // accum, wsum and the fragment cache are rewritten below
     SampleParams sp = sample_params(opts, (int)sc->tune.sample_layout);
     if (frag_out && !opts->use_prefiltering && sc->tune.fragment_slots > 0) {
         const int tiles = S.tiles_x * S.tiles_y, slots = (int)sc->tune.fragment_slots;
@@ -450,6 +536,7 @@ static dvg_status render_into(dvg_context* ctx, dvg_scene* sc, const dvg_render_
         ctx->launches += launch_resolve(S, ctx->accum.as<float>(), ctx->wsum.as<float>(), out_dev, ctx->stream);
     }
     CK(cudaGetLastError());
+    if (weights_out) *weights_out = true;
     return DVG_OK;
 }
 
@@ -461,7 +548,15 @@ dvg_status dvg_render_device(dvg_context* ctx, dvg_scene* scene, const dvg_rende
     return render_into(ctx, scene, opts, out_rgba);
 }
 
+static dvg_status render_host_impl(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
+                                   float* out_rgba, bool* frag_out, bool* weights_out);
 dvg_status dvg_render_host(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts, float* out_rgba) {
+    return render_host_impl(ctx, scene, opts, out_rgba, nullptr, nullptr);
+}
+static dvg_status render_host_impl(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
+                                   float* out_rgba, bool* frag_out, bool* weights_out) {
+    if (frag_out) *frag_out = false;
+    if (weights_out) *weights_out = false;
     if (!ctx || !scene || !out_rgba) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
     dvg_status st = check_options(opts);
     if (st != DVG_OK) return st;
@@ -475,7 +570,7 @@ dvg_status dvg_render_host(dvg_context* ctx, dvg_scene* scene, const dvg_render_
         return DVG_OK;
     }
     CK(ctx->image.reserve(npix * 4 * sizeof(float)));
-    st = render_into(ctx, scene, opts, ctx->image.as<float>());
+    st = render_into(ctx, scene, opts, ctx->image.as<float>(), frag_out, weights_out);
     if (st != DVG_OK) return st;
     CK(cudaMemcpyAsync(out_rgba, ctx->image.ptr, npix * 4 * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -494,6 +589,7 @@ static dvg_status backward_core(dvg_context* ctx, dvg_scene* sc, const dvg_rende
     if (frag_ready) attach_frag(sp, ctx->frag.ptr, S.tiles_x * S.tiles_y, (int)sc->tune.fragment_slots);
     if (d_render && S.num_groups > 0) {
         if (!have_weights) {
+            ++ctx->gen;
             CK(ctx->wsum.reserve(npix * sizeof(float)));
             CK(cudaMemsetAsync(ctx->wsum.ptr, 0, npix * sizeof(float), ctx->stream));
             Prof prof_(ctx, "weights");
@@ -533,6 +629,7 @@ static dvg_status backward_core(dvg_context* ctx, dvg_scene* sc, const dvg_rende
     } else if (d_render && S.num_groups == 0) {
         // only the background receives gradient: every sample lands on it.
         if (!have_weights) {
+            ++ctx->gen;
             CK(ctx->wsum.reserve(npix * sizeof(float)));
             CK(cudaMemsetAsync(ctx->wsum.ptr, 0, npix * sizeof(float), ctx->stream));
             Prof prof_(ctx, "weights");
@@ -629,9 +726,17 @@ dvg_status dvg_render_backward_device(dvg_context* ctx, dvg_scene* scene, const 
     return backward_core(ctx, scene, opts, bopts, d_render, d_sdf, G, false);
 }
 
+static dvg_status backward_host_impl(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
+                                     const dvg_backward_options* bopts, const float* d_render, const float* d_sdf,
+                                     dvg_grads* grads, bool have_weights, bool frag_ready);
 dvg_status dvg_render_backward_host(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
                                     const dvg_backward_options* bopts, const float* d_render, const float* d_sdf,
                                     dvg_grads* grads) {
+    return backward_host_impl(ctx, scene, opts, bopts, d_render, d_sdf, grads, false, false);
+}
+static dvg_status backward_host_impl(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
+                                     const dvg_backward_options* bopts, const float* d_render, const float* d_sdf,
+                                     dvg_grads* grads, bool have_weights, bool frag_ready) {
     dvg_status st = check_backward_args(ctx, scene, opts, d_sdf, grads);
     if (st != DVG_OK) return st;
     CK(cudaSetDevice(ctx->device));
@@ -664,7 +769,7 @@ dvg_status dvg_render_backward_host(dvg_context* ctx, dvg_scene* scene, const dv
         CK(cudaMemcpyAsync(ctx->sdf.ptr, d_sdf, npix * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
         ds = ctx->sdf.as<float>();
     }
-    st = backward_core(ctx, scene, opts, bopts, dr, ds, G, false);
+    st = backward_core(ctx, scene, opts, bopts, dr, ds, G, have_weights, frag_ready);
     if (st != DVG_OK) return st;
     struct Part {
         float* dst;
@@ -708,8 +813,25 @@ dvg_status dvg_render(dvg_context* ctx, const dvg_scene_desc* desc, const dvg_re
     dvg_scene* sc = nullptr;
     st = dvg_scene_upload(ctx, desc, &sc);
     if (st != DVG_OK) return st;
-    st = dvg_render_host(ctx, sc, opts, out_rgba);
-    dvg_scene_destroy(sc);
+    if (!ctx->retain) {
+        st = dvg_render_host(ctx, sc, opts, out_rgba);
+        dvg_scene_destroy(sc);
+        return st;
+    }
+    bool frag = false, weights = false;
+    st = render_host_impl(ctx, sc, opts, out_rgba, &frag, &weights);
+    if (ctx->kept) dvg_scene_destroy(ctx->kept);
+    ctx->kept = nullptr;
+    if (st != DVG_OK) {
+        dvg_scene_destroy(sc);
+        return st;
+    }
+    ctx->kept = sc;
+    desc_key(desc, ctx->kept_key);
+    ctx->kept_opts = *opts;
+    ctx->kept_gen = ctx->gen;
+    ctx->kept_weights = weights;
+    ctx->kept_frag = frag;
     return st;
 }
 
@@ -719,6 +841,14 @@ dvg_status dvg_render_backward(dvg_context* ctx, const dvg_scene_desc* desc, con
     if (!ctx || !desc || !grads) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
     dvg_status st = check_options(opts);
     if (st != DVG_OK) return st;
+    if (ctx->retain && ctx->kept && ctx->kept_gen == ctx->gen &&
+        std::memcmp(&ctx->kept_opts, opts, sizeof(dvg_render_options)) == 0) {
+        std::vector<char> key;
+        desc_key(desc, key);
+        if (key == ctx->kept_key)  // the scene, weights and fragments of the last dvg_render
+            return backward_host_impl(ctx, ctx->kept, opts, bopts, d_render, d_sdf, grads, ctx->kept_weights,
+                                      ctx->kept_frag);
+    }
     dvg_scene* sc = nullptr;
     st = dvg_scene_upload(ctx, desc, &sc);
     if (st != DVG_OK) return st;

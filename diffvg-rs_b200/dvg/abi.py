@@ -12,6 +12,8 @@ import ctypes as C
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional
 
+import itertools
+
 import numpy as np
 
 from .scene import (
@@ -131,75 +133,90 @@ def _paint_record(p):
 
 
 def pack_scene(scene: Scene) -> PackedScene:
+    """Scene -> dvg_scene_desc arrays (one Python pass collecting plain lists, one
+    numpy conversion per array)."""
     ns = len(scene.shapes)
-    kinds = np.zeros(ns, np.uint32)
-    params = np.zeros((ns, 4), np.float32)
-    xforms = np.zeros((ns, 9), np.float32)
-    sw = np.zeros(ns, np.float32)
-    joins = np.zeros(ns, np.uint32)
-    caps = np.zeros(ns, np.uint32)
-    miters = np.zeros(ns, np.float32)
-    ctrl_off = np.zeros(ns, np.uint32)
-    ctrl_cnt = np.zeros(ns, np.uint32)
-    pt_off = np.zeros(ns, np.uint32)
-    pt_cnt = np.zeros(ns, np.uint32)
-    flags = np.zeros(ns, np.uint32)
-    ncp: List[int] = []
-    pts: List[float] = []
-    thick: List[float] = []
+    kinds: List[int] = []
+    params: List[tuple] = []
+    xf: List[np.ndarray] = []
+    sw: List[float] = []
+    joins: List[int] = []
+    caps: List[int] = []
+    miters: List[float] = []
+    ctrl_off: List[int] = []
+    ctrl_cnt: List[int] = []
+    pt_off: List[int] = []
+    pt_cnt: List[int] = []
+    flags: List[int] = []
+    ncp_l: List[int] = []
+    pts_l: list = []
+    th_l: List[float] = []
     any_thick = False
-    for i, sh in enumerate(scene.shapes):
+    zero4 = (0.0, 0.0, 0.0, 0.0)
+    for sh in scene.shapes:
         g = sh.geometry
-        xforms[i] = sh.transform.flat()
-        sw[i] = sh.stroke_width
-        joins[i] = int(sh.stroke_join)
-        caps[i] = int(sh.stroke_cap)
-        miters[i] = sh.stroke_miter_limit
-        if isinstance(g, Circle):
-            kinds[i] = SHAPE_CIRCLE
-            params[i] = [g.center[0], g.center[1], g.radius, 0.0]
-        elif isinstance(g, Ellipse):
-            kinds[i] = SHAPE_ELLIPSE
-            params[i] = [g.center[0], g.center[1], g.radius[0], g.radius[1]]
-        elif isinstance(g, Rect):
-            kinds[i] = SHAPE_RECT
-            params[i] = [g.min[0], g.min[1], g.max[0], g.max[1]]
-        elif isinstance(g, PathGeometry):
+        xf.append(sh.transform.m)
+        sw.append(sh.stroke_width)
+        joins.append(int(sh.stroke_join))
+        caps.append(int(sh.stroke_cap))
+        miters.append(sh.stroke_miter_limit)
+        if isinstance(g, PathGeometry):
             p = g.path
-            kinds[i] = SHAPE_PATH
-            ctrl_off[i] = len(ncp)
-            ctrl_cnt[i] = len(p.num_control_points)
-            pt_off[i] = len(pts) // 2
-            pt_cnt[i] = len(p.points)
-            ncp += [int(c) for c in p.num_control_points]
-            for q in p.points:
-                pts += [float(q[0]), float(q[1])]
-            f = 0
-            if p.is_closed:
-                f |= PATH_CLOSED
-            if p.use_distance_approx:
-                f |= PATH_DISTANCE_APPROX
+            npt = len(p.points)
+            kinds.append(SHAPE_PATH)
+            params.append(zero4)
+            ctrl_off.append(len(ncp_l))
+            ctrl_cnt.append(len(p.num_control_points))
+            pt_off.append(len(pts_l))
+            pt_cnt.append(npt)
+            ncp_l.extend(p.num_control_points)
+            pts_l.extend(p.points)
+            f = (PATH_CLOSED if p.is_closed else 0) | (PATH_DISTANCE_APPROX if p.use_distance_approx else 0)
             if p.thickness is not None:
                 f |= PATH_HAS_THICKNESS
                 any_thick = True
-                t = list(p.thickness)[: len(p.points)]
-                t += [0.0] * (len(p.points) - len(t))
-                thick += t
+                t = [float(x) for x in list(p.thickness)[:npt]]
+                th_l.extend(t + [0.0] * (npt - len(t)))
             else:
-                thick += [0.0] * len(p.points)
-            flags[i] = f
+                th_l.extend([0.0] * npt)
+            flags.append(f)
+            continue
+        ctrl_off.append(0)
+        ctrl_cnt.append(0)
+        pt_off.append(0)
+        pt_cnt.append(0)
+        flags.append(0)
+        if isinstance(g, Circle):
+            kinds.append(SHAPE_CIRCLE)
+            params.append((g.center[0], g.center[1], g.radius, 0.0))
+        elif isinstance(g, Ellipse):
+            kinds.append(SHAPE_ELLIPSE)
+            params.append((g.center[0], g.center[1], g.radius[0], g.radius[1]))
+        elif isinstance(g, Rect):
+            kinds.append(SHAPE_RECT)
+            params.append((g.min[0], g.min[1], g.max[0], g.max[1]))
         else:
             raise TypeError(f"unsupported geometry {type(g)!r}")
+    n_ncp, n_pts = len(ncp_l), len(pts_l)
+    u32 = lambda v: np.asarray(v, np.uint32).reshape(-1)  # noqa: E731
+    f32 = lambda v: np.asarray(v, np.float32).reshape(-1)  # noqa: E731
+    kinds, sw, joins, caps, miters = u32(kinds), f32(sw), u32(joins), u32(caps), f32(miters)
+    ctrl_off, ctrl_cnt, pt_off, pt_cnt, flags = u32(ctrl_off), u32(ctrl_cnt), u32(pt_off), u32(pt_cnt), u32(flags)
+    params = np.asarray(params, np.float32).reshape(ns, 4) if ns else np.zeros((0, 4), np.float32)
+    xforms = np.stack(xf).astype(np.float32, copy=False).reshape(ns, 9) if ns else np.zeros((0, 9), np.float32)
+    ncp = np.asarray(ncp_l, np.int64).astype(np.uint8) if n_ncp else np.zeros(1, np.uint8)
+    pts = np.fromiter(itertools.chain.from_iterable(pts_l), np.float32, 2 * n_pts) if n_pts else np.zeros(2, np.float32)
+    thick = np.asarray(th_l, np.float32) if n_pts else np.zeros(1, np.float32)
 
     ng = len(scene.groups)
-    g_off = np.zeros(ng, np.uint32)
-    g_cnt = np.zeros(ng, np.uint32)
+    g_off: List[int] = []
+    g_cnt: List[int] = []
     g_ids: List[int] = []
-    g_rule = np.zeros(ng, np.uint32)
-    g_s2c = np.zeros((ng, 9), np.float32)
-    g_c2s = np.zeros((ng, 9), np.float32)
-    g_fill = np.full(ng, -1, np.int32)
-    g_stroke = np.full(ng, -1, np.int32)
+    g_rule: List[int] = []
+    s2c: List[np.ndarray] = []
+    c2s: List[np.ndarray] = []
+    g_fill: List[int] = []
+    g_stroke: List[int] = []
     p_kind: List[int] = []
     p_params: List[List[float]] = []
     p_soff: List[int] = []
@@ -208,17 +225,18 @@ def pack_scene(scene: Scene) -> PackedScene:
     s_col: List[float] = []
     paint_of = {}
     for gi, grp in enumerate(scene.groups):
-        g_off[gi] = len(g_ids)
-        g_cnt[gi] = len(grp.shape_indices)
-        g_ids += [int(s) for s in grp.shape_indices]
-        g_rule[gi] = int(grp.fill_rule)
-        g_s2c[gi] = grp.shape_to_canvas.flat()
-        g_c2s[gi] = grp.canvas_to_shape.flat()
+        g_off.append(len(g_ids))
+        g_cnt.append(len(grp.shape_indices))
+        g_ids.extend(int(s) for s in grp.shape_indices)
+        g_rule.append(int(grp.fill_rule))
+        s2c.append(grp.shape_to_canvas.m)
+        c2s.append(grp.canvas_to_shape.m)
         for which, paint, arr in (("stroke", grp.stroke, g_stroke), ("fill", grp.fill, g_fill)):
             if paint is None:
+                arr.append(-1)
                 continue
             k, prm, stops = _paint_record(paint)
-            arr[gi] = len(p_kind)
+            arr.append(len(p_kind))
             paint_of[(gi, which)] = len(p_kind)
             p_kind.append(k)
             p_params.append(prm)
@@ -227,12 +245,15 @@ def pack_scene(scene: Scene) -> PackedScene:
             for st in stops:
                 s_off.append(st.offset)
                 s_col += [st.color.r, st.color.g, st.color.b, st.color.a]
+    g_off, g_cnt, g_rule = u32(g_off), u32(g_cnt), u32(g_rule)
+    g_fill, g_stroke = np.asarray(g_fill, np.int32).reshape(-1), np.asarray(g_stroke, np.int32).reshape(-1)
+    g_s2c = np.stack(s2c).astype(np.float32, copy=False).reshape(ng, 9) if ng else np.zeros((0, 9), np.float32)
+    g_c2s = np.stack(c2s).astype(np.float32, copy=False).reshape(ng, 9) if ng else np.zeros((0, 9), np.float32)
 
     arrays = dict(
         kinds=kinds, params=params.reshape(-1), xforms=xforms.reshape(-1), sw=sw, joins=joins, caps=caps,
         miters=miters, ctrl_off=ctrl_off, ctrl_cnt=ctrl_cnt, pt_off=pt_off, pt_cnt=pt_cnt, flags=flags,
-        ncp=np.asarray(ncp if ncp else [0], np.uint8), pts=np.asarray(pts if pts else [0.0, 0.0], np.float32),
-        thick=np.asarray(thick if thick else [0.0], np.float32),
+        ncp=ncp, pts=pts, thick=thick,
         g_off=g_off, g_cnt=g_cnt, g_ids=np.asarray(g_ids if g_ids else [0], np.uint32), g_rule=g_rule,
         g_s2c=g_s2c.reshape(-1), g_c2s=g_c2s.reshape(-1), g_fill=g_fill, g_stroke=g_stroke,
         p_kind=np.asarray(p_kind if p_kind else [0], np.uint32),
@@ -270,8 +291,8 @@ def pack_scene(scene: Scene) -> PackedScene:
     d.num_control_points = _ptr(arrays["ncp"], C.c_uint8)
     d.points = _ptr(arrays["pts"], C.c_float)
     d.thickness = _ptr(arrays["thick"], C.c_float) if any_thick else C.cast(None, _fp)
-    d.total_ctrl = len(ncp)
-    d.total_points = len(pts) // 2
+    d.total_ctrl = n_ncp
+    d.total_points = n_pts
     d.num_groups = ng
     d.group_shape_offset = _ptr(g_off, C.c_uint32)
     d.group_shape_count = _ptr(g_cnt, C.c_uint32)
@@ -290,7 +311,7 @@ def pack_scene(scene: Scene) -> PackedScene:
     d.stop_offsets = _ptr(arrays["s_off"], C.c_float)
     d.stop_colors = _ptr(arrays["s_col"], C.c_float)
     d.total_stops = len(s_off)
-    return PackedScene(d, arrays, paint_of, [int(x) for x in pt_off], [int(x) for x in pt_cnt], p_soff, p_scnt)
+    return PackedScene(d, arrays, paint_of, pt_off.tolist(), pt_cnt.tolist(), p_soff, p_scnt)
 
 
 class GradBuffers:

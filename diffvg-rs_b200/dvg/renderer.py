@@ -120,6 +120,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.dvg_context_stream.restype = vp
     L.dvg_context_set_profiling.argtypes = [vp, C.c_int]
     L.dvg_context_set_profiling.restype = C.c_int
+    L.dvg_context_set_retain.argtypes = [vp, C.c_int]
+    L.dvg_context_set_retain.restype = C.c_int
     L.dvg_context_profile.argtypes = [vp, C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.POINTER(C.c_uint64),
                                       C.c_int]
     L.dvg_context_profile.restype = C.c_int
@@ -341,6 +343,10 @@ class Renderer:
     def stream_handle(self) -> int:
         return int(self.lib.dvg_context_stream(self.ctx) or 0)
 
+    def set_retain(self, enable: bool) -> None:
+        """dvg_context_set_retain: keep the last render for a following render_backward."""
+        _check(self.lib.dvg_context_set_retain(self.ctx, 1 if enable else 0))
+
     def set_profiling(self, enable: bool) -> None:
         _check(self.lib.dvg_context_set_profiling(self.ctx, 1 if enable else 0))
 
@@ -361,23 +367,25 @@ class Renderer:
         packing again (e.g. after editing its arrays in place)."""
         return UploadedScene(self, scene, packed)
 
-    def render(self, scene: Scene, options: RenderOptions = None) -> Image:
-        """Renderer::render (src/renderer/renderer.rs:39-545)."""
+    def render(self, scene: Scene, options: RenderOptions = None, packed: Optional[PackedScene] = None) -> Image:
+        """Renderer::render (src/renderer/renderer.rs:39-545).  `packed`: pack_scene(scene)
+        made by the caller (one packing for a render and the render_backward after it)."""
         options = options or RenderOptions()
         if scene.background_image is not None:
             if np.asarray(scene.background_image).size != scene.width * scene.height * 4:
                 raise RenderError(DVG_ERR_INVALID_SCENE, "background image size mismatch")
         if scene.width == 0 or scene.height == 0:
             return Image(scene.width, scene.height, np.zeros((0,), np.float32))
-        packed = pack_scene(scene)
-        out = np.zeros((scene.height, scene.width, 4), np.float32)
+        packed = packed or pack_scene(scene)
+        out = np.empty((scene.height, scene.width, 4), np.float32)
         o = render_options_c(options)
         _check(self.lib.dvg_render(self.ctx, packed.ref(), C.byref(o), _fp(out)))
         return Image(scene.width, scene.height, out)
 
     def render_backward(self, scene: Scene, options: RenderOptions = None,
                         backward_options: Optional[BackwardOptions] = None,
-                        d_render_image: Optional[np.ndarray] = None, d_sdf_image: Optional[np.ndarray] = None):
+                        d_render_image: Optional[np.ndarray] = None, d_sdf_image: Optional[np.ndarray] = None,
+                        packed: Optional[PackedScene] = None):
         """Renderer::render_backward (src/renderer/renderer.rs:548-564) -> SceneGrad."""
         options = options or RenderOptions()
         bopts = backward_options or BackwardOptions()
@@ -386,7 +394,7 @@ class Renderer:
             raise RenderError(DVG_ERR_INVALID_SCENE, "d_render_image size mismatch")
         if d_sdf_image is not None and np.asarray(d_sdf_image).size != npix:
             raise RenderError(DVG_ERR_INVALID_SCENE, "d_sdf_image size mismatch")
-        packed = pack_scene(scene)
+        packed = packed or pack_scene(scene)
         has_bg = d_render_image is not None and scene.background_image is not None
         buf = GradBuffers(packed, background_image=has_bg, translation=bopts.compute_translation)
         dr = None if d_render_image is None else np.ascontiguousarray(np.asarray(d_render_image, np.float32).reshape(-1))

@@ -200,6 +200,10 @@ const char* dvg_last_error(void);
  * binds a CUDA device and creates the context's stream and scratch pool. */
 dvg_status dvg_context_create(int device, dvg_context** out);
 void dvg_context_destroy(dvg_context* ctx);
+/* Retention of the last dvg_render for dvg_render_backward (see dvg_render); 1 by
+ * default.  Turning it off releases the retained scene; with it off, dvg_render
+ * writes no fragment codes and frees its scene at once. */
+dvg_status dvg_context_set_retain(dvg_context* ctx, int enable);
 
 /* Host preparation + upload.  Replaces prepare_scene / prepare_scene_backward and the
  * buffer uploads (src/renderer/prepare.rs:114, src/renderer/prepare_backward.rs:45,
@@ -275,7 +279,13 @@ dvg_status dvg_render_device_noalloc(dvg_context* ctx, dvg_scene* scene, const d
                                      float* out_rgba);
 
 /* One-shot forms mirroring the crate's call shape exactly: scene description in,
- * host image / host gradients out (upload, launch, read back, release). */
+ * host image / host gradients out (upload, launch, read back).  With retention on
+ * (the default, dvg_context_set_retain), dvg_render keeps its prepared scene, its
+ * weight image and the per-sample fragment codes of its forward pass in the
+ * context; a following dvg_render_backward whose description has the same bytes
+ * (every scalar and array) and whose options are equal reuses them, as long as no
+ * other call on the context rendered or drew weights in between.  Results are the
+ * same either way (to float summation order). */
 dvg_status dvg_render(dvg_context* ctx, const dvg_scene_desc* desc, const dvg_render_options* opts,
                       float* out_rgba);
 dvg_status dvg_render_backward(dvg_context* ctx, const dvg_scene_desc* desc,
