@@ -465,7 +465,9 @@ def main():
     achieved = alg_bytes / (avg_ms / 1e3) / 1e9
     # DRAM bytes (read + write) per launch from one ncu capture of this workload
     # (profiles/k_*_mixed512.md); only the default workload has a capture.
-    ncu_traffic = {"interior": 6066944, "forward": 5911808, "boundary": 23650304} if args.workload == "mixed" else {}
+    # "interior" is k_interior_cached (the full kernel only takes samples without cached fragments).
+    ncu_traffic = {"interior": 40272384, "forward": 5912576, "boundary": 26743808} if args.workload == "mixed" else {}
+    ncu_file = {"interior": "k_interior_cached", "forward": "k_forward", "boundary": "k_boundary_eval"}
     prof_json = {k: {"ms_per_step": v[0] / 3.0, "calls_per_step": v[1] / 3.0} for k, v in prof.items()}
 
     line = {
@@ -479,8 +481,8 @@ def main():
                                     "fragment_slots": tuning[2], "chosen_by": "dvg_scene_autotune"}},
         "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": ncu_traffic.get(name), "peak_source": peak_src,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch "
-                                       f"(profiles/k_{'boundary_eval' if name == 'boundary' else name}_mixed512.md)"
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch, cold cache "
+                                       f"(profiles/{ncu_file.get(name, name)}_mixed512.md)"
                                        if name in ncu_traffic else None,
                      "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
                      "note": "compute-bound path (f64 root solves, divergent BVH walks); HBM roofline reported "
