@@ -17,6 +17,14 @@
 #include "kernels.cuh"
 #include "prepare.hpp"
 
+static_assert((int)dvgb::PATH_STYLED == (int)dvgb::PF_STYLED && (int)dvgb::PATH_JOIN_SHIFT == (int)dvgb::PF_JOIN_SHIFT &&
+                  (int)dvgb::PATH_CAP_SHIFT == (int)dvgb::PF_CAP_SHIFT,
+              "path style bits differ between host preparation and the kernels");
+static_assert((int)DVG_JOIN_MITER == (int)dvgb::JOIN_MITER && (int)DVG_JOIN_BEVEL == (int)dvgb::JOIN_BEVEL &&
+                  (int)DVG_JOIN_ROUND == (int)dvgb::JOIN_ROUND && (int)DVG_CAP_BUTT == (int)dvgb::CAP_BUTT &&
+                  (int)DVG_CAP_SQUARE == (int)dvgb::CAP_SQUARE && (int)DVG_CAP_ROUND == (int)dvgb::CAP_ROUND,
+              "join / cap codes differ between the ABI and the kernels");
+
 using namespace dvgb;
 
 namespace {
@@ -386,7 +394,8 @@ dvg_status dvg_scene_upload(dvg_context* ctx, const dvg_scene_desc* desc, dvg_sc
            o_gn_m = b.add(h.gn_meta), o_gl = b.add(h.gl_shapes), o_s_info = b.add(h.s_info),
            o_s_prm = b.add(h.s_params), o_s_inv = b.add(h.s_inv), o_s_x = b.add(h.s_xform),
            o_s_sw = b.add(h.s_stroke), o_s_box = b.add(h.s_box), o_s_pm = b.add(h.s_padmul),
-           o_p_shape = b.add(h.p_shape), o_p_info = b.add(h.p_info), o_pn_b = b.add(h.pn_bounds),
+           o_p_shape = b.add(h.p_shape), o_p_miter = b.add(h.p_miter), o_p_info = b.add(h.p_info),
+           o_pn_b = b.add(h.pn_bounds),
            o_pn_m = b.add(h.pn_meta), o_pl = b.add(h.pl_segs), o_seg_p = b.add(h.seg_p), o_seg_r = b.add(h.seg_r),
            o_seg_m = b.add(h.seg_meta), o_pts = b.add(h.points), o_th = b.add(h.thickness), o_ncp = b.add(h.ncp),
            o_pi = b.add(h.paint_info), o_pp = b.add(h.paint_params), o_so = b.add(h.stop_offsets),
@@ -429,6 +438,7 @@ dvg_status dvg_scene_upload(dvg_context* ctx, const dvg_scene_desc* desc, dvg_sc
     S.s_box = (const float4*)(base + o_s_box);
     S.s_padmul = (const float*)(base + o_s_pm);
     S.p_shape = (const int*)(base + o_p_shape);
+    S.p_miter = (const float*)(base + o_p_miter);
     S.p_info = (const int4*)(base + o_p_info);
     S.pn_bounds = (const float4*)(base + o_pn_b);
     S.pn_meta = (const int4*)(base + o_pn_m);

@@ -24,7 +24,8 @@ constexpr float HALF_PI_F = 1.57079632679489661923f;
 enum : int { K_CIRCLE = 0, K_RECT = 1, K_PATH = 2, K_ELLIPSE = 3 };
 enum : int { P_NONE = 0, P_SOLID = 1, P_LINEAR = 2, P_RADIAL = 3 };
 enum : int { F_BOX = 0, F_TENT = 1, F_PARABOLIC = 2, F_HANN = 3, F_GAUSSIAN = 4 };
-enum : int { PF_CLOSED = 1, PF_APPROX = 2, PF_THICK = 4 };
+enum : int { PF_CLOSED = 1, PF_APPROX = 2, PF_THICK = 4, PF_STYLED = 8, PF_JOIN_SHIFT = 4, PF_CAP_SHIFT = 6 };
+enum : int { JOIN_MITER = 0, JOIN_BEVEL = 1, JOIN_ROUND = 2, CAP_BUTT = 0, CAP_SQUARE = 1, CAP_ROUND = 2 };
 
 // Device status bits written by kernels (never a trap: the host reads them).
 enum : unsigned { ST_FRAGMENT_OVERFLOW = 1u, ST_BVH_LIMIT = 2u, ST_REFIT_LAYOUT = 4u };
@@ -57,6 +58,7 @@ struct DevScene {
     // paths
     const int4* p_info;  // 2 per path: (seg off, seg cnt, node off, node cnt), (pt off, pt cnt, ctrl off, flags)
     const int* p_shape;  // shape id per path
+    const float* p_miter;  // miter limit (>= 1) per path
     const float4* pn_bounds;
     const int4* pn_meta;
     const int* pl_segs;
@@ -587,6 +589,110 @@ __device__ __forceinline__ bool stroke_far_from_cubic(const SegGeom& s, float2 p
     return cubic_dist_lower(p.x, p.y, s.q[0], s.q[1], s.q[2], s.q[3], s.q[4], s.q[5], s.q[6], s.q[7]) > r + m;
 }
 
+// ------------------------------------------------------------------ stroke joins and caps
+// An extension: the crate strokes every path with round joins and caps (its join /
+// cap fields only pad bounds, src/renderer/prepare.rs:207-210).  A path flagged
+// PF_STYLED strokes its segment bodies as the crate does, except at vertices whose
+// join or cap is not round: there a closest point exactly at the segment's end does
+// not count, and the join or cap region is added instead.  Bevel: the triangle
+// between the vertex and the two outer offset points; miter: the quad through the
+// offset lines' intersection while that lies within miter-limit radii of the vertex
+// (else bevel); butt: nothing; square: a rectangle one radius long and two wide
+// beyond the end.  Regions are closed sets, so they meet the bodies without cracks.
+__device__ __forceinline__ bool end_excluded(int pflags, int seg, int nseg, float t) {
+    const bool at0 = t == 0.0f, at1 = t == 1.0f;
+    if (!(pflags & PF_STYLED) || !(at0 || at1)) return false;
+    const bool join = (pflags & PF_CLOSED) || (at0 ? seg > 0 : seg < nseg - 1);
+    if (join) return ((pflags >> PF_JOIN_SHIFT) & 3) != JOIN_ROUND;
+    return ((pflags >> PF_CAP_SHIFT) & 3) != CAP_ROUND;
+}
+// Tangent directions at t = 0 and t = 1 from the control points (degenerate legs
+// skipped; lines and quadratics repeat their last point).
+__device__ __forceinline__ float2 seg_dir0(float4 a, float4 b) {
+    float2 d = make_float2(a.z - a.x, a.w - a.y);
+    if (d.x == 0.0f && d.y == 0.0f) d = make_float2(b.x - a.x, b.y - a.y);
+    if (d.x == 0.0f && d.y == 0.0f) d = make_float2(b.z - a.x, b.w - a.y);
+    return d;
+}
+__device__ __forceinline__ float2 seg_dir1(float4 a, float4 b) {
+    float2 d = make_float2(b.z - b.x, b.w - b.y);
+    if (d.x == 0.0f && d.y == 0.0f) d = make_float2(b.z - a.z, b.w - a.w);
+    if (d.x == 0.0f && d.y == 0.0f) d = make_float2(b.z - a.x, b.w - a.y);
+    return d;
+}
+__device__ __forceinline__ float cross2f(float ax, float ay, float bx, float by) { return ax * by - ay * bx; }
+__device__ __forceinline__ bool in_triangle(float2 p, float2 a, float2 b, float2 c) {
+    const float d1 = cross2f(b.x - a.x, b.y - a.y, p.x - a.x, p.y - a.y);
+    const float d2 = cross2f(c.x - b.x, c.y - b.y, p.x - b.x, p.y - b.y);
+    const float d3 = cross2f(a.x - c.x, a.y - c.y, p.x - c.x, p.y - c.y);
+    const bool neg = d1 < 0.0f || d2 < 0.0f || d3 < 0.0f, pos = d1 > 0.0f || d2 > 0.0f || d3 > 0.0f;
+    return !(neg && pos);
+}
+__device__ __forceinline__ bool join_hit(float2 p, float2 v, float2 din, float2 dout, float r, int join, float limit) {
+    const float li = sqrtf(din.x * din.x + din.y * din.y), lo = sqrtf(dout.x * dout.x + dout.y * dout.y);
+    if (!(li > 0.0f) || !(lo > 0.0f) || !(r > 0.0f)) return false;
+    din = make_float2(din.x / li, din.y / li);
+    dout = make_float2(dout.x / lo, dout.y / lo);
+    const float cr = cross2f(din.x, din.y, dout.x, dout.y);
+    if (fabsf(cr) < 1.0e-6f) return false;  // straight on (no gap) or a reversal (no outer side)
+    const float sg = cr > 0.0f ? 1.0f : -1.0f;  // the outer side is right of travel on a left turn
+    const float2 a = make_float2(v.x + r * sg * din.y, v.y - r * sg * din.x);
+    const float2 b = make_float2(v.x + r * sg * dout.y, v.y - r * sg * dout.x);
+    if (join == JOIN_MITER) {
+        const float s = cross2f(b.x - a.x, b.y - a.y, dout.x, dout.y) / cr;
+        const float2 m = make_float2(a.x + s * din.x, a.y + s * din.y);
+        const float ml = sqrtf((m.x - v.x) * (m.x - v.x) + (m.y - v.y) * (m.y - v.y));
+        if (ml <= limit * r) return in_triangle(p, v, a, m) || in_triangle(p, v, m, b);
+    }
+    return in_triangle(p, v, a, b);
+}
+__device__ __forceinline__ bool square_cap_hit(float2 p, float2 v, float2 d, float r) {
+    const float l = sqrtf(d.x * d.x + d.y * d.y);
+    if (!(l > 0.0f) || !(r > 0.0f)) return false;
+    const float dx = d.x / l, dy = d.y / l, qx = p.x - v.x, qy = p.y - v.y;
+    const float s = qx * dx + qy * dy, u = qx * -dy + qy * dx;
+    return s >= 0.0f && s <= r && fabsf(u) <= r;
+}
+// The join and cap regions of a PF_STYLED path at shape-space point (px, py).  Out of
+// line, with the four tables it reads as arguments (a scene reference would make the
+// callers copy the whole scene to local memory).
+static __device__ __forceinline__ bool join_cap_hit_v(const int4* p_info, const float* p_miter, const float4* seg_p,
+                                                   const float4* seg_r, int path, float px, float py) {
+    const int4 pi = __ldg(&p_info[2 * path]);
+    const int pflags = __ldg(&p_info[2 * path + 1].w);
+    const bool closed = pflags & PF_CLOSED;
+    const int join = (pflags >> PF_JOIN_SHIFT) & 3, cap = (pflags >> PF_CAP_SHIFT) & 3;
+    const float limit = __ldg(&p_miter[path]);
+    const float reach = (join == JOIN_MITER ? limit : 1.0f) * 1.001f;  // join regions lie within reach * r of v
+    const float2 p = make_float2(px, py);
+    const int off = pi.x, n = pi.y;
+    for (int k = 0; k < n; ++k) {
+        const float4 a = __ldg(&seg_p[2 * (off + k)]), b = __ldg(&seg_p[2 * (off + k) + 1]);
+        const float2 v = make_float2(a.x, a.y);
+        const float r = __ldg(&seg_r[off + k]).x;
+        if (k > 0 || closed) {
+            if (join == JOIN_ROUND) continue;
+            const float dx = p.x - v.x, dy = p.y - v.y;
+            if (dx * dx + dy * dy > (reach * r) * (reach * r)) continue;
+            const int kin = k > 0 ? k - 1 : n - 1;
+            const float4 ia = __ldg(&seg_p[2 * (off + kin)]), ib = __ldg(&seg_p[2 * (off + kin) + 1]);
+            if (join_hit(p, v, seg_dir1(ia, ib), seg_dir0(a, b), r, join, limit)) return true;
+        } else if (cap == CAP_SQUARE) {
+            const float2 d = seg_dir0(a, b);
+            if (square_cap_hit(p, v, make_float2(-d.x, -d.y), r)) return true;
+        }
+    }
+    if (!closed && cap == CAP_SQUARE && n > 0) {
+        const float4 a = __ldg(&seg_p[2 * (off + n - 1)]), b = __ldg(&seg_p[2 * (off + n - 1) + 1]);
+        if (square_cap_hit(p, make_float2(b.z, b.w), seg_dir1(a, b), __ldg(&seg_r[off + n - 1]).w)) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ bool join_cap_hit(const DevScene& S, int path, float2 p) {
+    return join_cap_hit_v(S.p_info, S.p_miter, S.seg_p, S.seg_r, path, p.x, p.y);
+}
+
 // Nearest-segment searches keep a segment only when its distance is strictly below
 // the best so far; a cubic whose lower bound exceeds that by the culling margin
 // cannot be kept, so its exact solve is skipped (same argument as above).
@@ -637,7 +743,8 @@ __device__ __forceinline__ int winding_path_list(const DevScene& S, int path, fl
 }
 __device__ __forceinline__ bool within_path_bvh(const DevScene& S, int path, float2 p) {  // closest.rs:20-98
     int4 pi = __ldg(&S.p_info[2 * path]);
-    bool approx = __ldg(&S.p_info[2 * path + 1].w) & PF_APPROX;
+    const int pflags = __ldg(&S.p_info[2 * path + 1].w);
+    bool approx = pflags & PF_APPROX;
     int n = pi.z, end = pi.z + pi.w;
     int guard = 0;
     while (n < end && guard++ < (1 << 20)) {
@@ -649,32 +756,34 @@ __device__ __forceinline__ bool within_path_bvh(const DevScene& S, int path, flo
         }
         if (m.z > 0) {
             for (int k = m.y; k < m.y + m.z; ++k) {
+                const int sidx = __ldg(&S.pl_segs[k]);
                 SegGeom sg;
-                load_seg(S, __ldg(&S.pl_segs[k]), sg);
+                load_seg(S, sidx, sg);
                 if (stroke_misses_segment(sg, p)) continue;
                 if (sg.kind == 2 && !approx && stroke_far_from_cubic(sg, p)) continue;
                 CPRes c = seg_closest(sg, p, approx);
-                if (c.dist < seg_radius(sg, c.t)) return true;
+                if (c.dist < seg_radius(sg, c.t) && !end_excluded(pflags, sidx - pi.x, pi.y, c.t)) return true;
             }
             n = m.x;
         } else {
             n = n + 1;
         }
     }
-    return false;
+    return (pflags & PF_STYLED) && join_cap_hit(S, path, p);
 }
 __device__ __forceinline__ bool within_path_list(const DevScene& S, int path, float2 p) {  // closest.rs:228-377
     int4 pi = __ldg(&S.p_info[2 * path]);
-    bool approx = __ldg(&S.p_info[2 * path + 1].w) & PF_APPROX;
+    const int pflags = __ldg(&S.p_info[2 * path + 1].w);
+    bool approx = pflags & PF_APPROX;
     for (int k = 0; k < pi.y; ++k) {
         SegGeom sg;
         load_seg(S, pi.x + k, sg);
         if (stroke_misses_segment(sg, p)) continue;
         if (sg.kind == 2 && !approx && stroke_far_from_cubic(sg, p)) continue;
         CPRes c = seg_closest(sg, p, approx);
-        if (c.dist < seg_radius(sg, c.t)) return true;
+        if (c.dist < seg_radius(sg, c.t) && !end_excluded(pflags, k, pi.y, c.t)) return true;
     }
-    return false;
+    return (pflags & PF_STYLED) && join_cap_hit(S, path, p);
 }
 
 // ------------------------------------------------------------------ shape queries

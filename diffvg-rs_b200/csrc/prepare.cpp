@@ -16,6 +16,14 @@ namespace {
 const float kPi = 3.14159265358979323846f;
 const float kInf = std::numeric_limits<float>::infinity();
 const size_t kLeafSize = 8;  // BVH_LEAF_SIZE, src/distance/bvh.rs:12
+const float kSqrt2Up = 1.41422f;  // sqrt(2) rounded up
+
+uint32_t stroke_join_of(const dvg_scene_desc* d, uint32_t s) {  // validated: <= DVG_JOIN_ROUND
+    return d->shape_stroke_join ? d->shape_stroke_join[s] : (uint32_t)DVG_JOIN_ROUND;
+}
+uint32_t stroke_cap_of(const dvg_scene_desc* d, uint32_t s) {  // validated: <= DVG_CAP_ROUND
+    return d->shape_stroke_cap ? d->shape_stroke_cap[s] : (uint32_t)DVG_CAP_ROUND;
+}
 
 struct Box {
     float x0, y0, x1, y1;
@@ -188,6 +196,12 @@ dvg_status prepare_scene(const dvg_scene_desc* d, HostScene* out, std::string* e
         *err = "missing paint arrays";
         return DVG_ERR_INVALID_ARGUMENT;
     }
+    for (uint32_t s = 0; s < d->num_shapes; ++s)
+        if ((d->shape_stroke_join && d->shape_stroke_join[s] > (uint32_t)DVG_JOIN_ROUND) ||
+            (d->shape_stroke_cap && d->shape_stroke_cap[s] > (uint32_t)DVG_CAP_ROUND)) {
+            *err = "invalid stroke join or cap";
+            return DVG_ERR_INVALID_SCENE;
+        }
     if (d->total_points) h.points.assign(d->points, d->points + 2 * (size_t)d->total_points);
     h.thickness.assign(d->total_points, 0.0f);
     if (d->thickness && d->total_points) h.thickness.assign(d->thickness, d->thickness + d->total_points);
@@ -322,6 +336,11 @@ dvg_status prepare_scene(const dvg_scene_desc* d, HostScene* out, std::string* e
             }
             int32_t pflags = (int32_t)((closed ? DVG_PATH_CLOSED : 0) | (fl & DVG_PATH_DISTANCE_APPROX) |
                                        (thick ? DVG_PATH_HAS_THICKNESS : 0));
+            // Stroke joins / caps other than round (an extension: the crate strokes round only).
+            const uint32_t join = stroke_join_of(d, s), cap = stroke_cap_of(d, s);
+            if (join != DVG_JOIN_ROUND || (!closed && cap != DVG_CAP_ROUND))
+                pflags |= PATH_STYLED | (int32_t)(join << PATH_JOIN_SHIFT) | (int32_t)(cap << PATH_CAP_SHIFT);
+            h.p_miter.push_back(std::fmax(d->shape_miter_limit ? d->shape_miter_limit[s] : 4.0f, 1.0f));
             h.p_info.insert(h.p_info.end(), {seg_off, (int32_t)segs.size(), node_off, node_cnt, (int32_t)po,
                                              (int32_t)pc, (int32_t)co, pflags});
             h.num_paths++;
@@ -336,10 +355,13 @@ dvg_status prepare_scene(const dvg_scene_desc* d, HostScene* out, std::string* e
                 for (uint32_t k = 0; k < pc; ++k) mt = std::fmax(mt, std::fabs(d->thickness[po + k]));
                 rad = std::fmax(rad, mt * scale);
             }
-            uint32_t join = d->shape_stroke_join ? d->shape_stroke_join[s] : (uint32_t)DVG_JOIN_ROUND;
+            uint32_t join = stroke_join_of(d, s);
             float miter = d->shape_miter_limit ? d->shape_miter_limit[s] : 4.0f;
             if (join == DVG_JOIN_MITER) h.s_padmul[s] = std::fmax(miter, 1.0f);
-            if (rad > 0.0f && join == DVG_JOIN_MITER) rad *= h.s_padmul[s];
+            // a square cap's corners lie sqrt(2) radii from the end point
+            if (kind == DVG_SHAPE_PATH && !(d->path_flags[s] & DVG_PATH_CLOSED) && stroke_cap_of(d, s) == DVG_CAP_SQUARE)
+                h.s_padmul[s] = std::fmax(h.s_padmul[s], kSqrt2Up);
+            if (rad > 0.0f) rad *= h.s_padmul[s];
             shape_box[s] = inflate(gb, rad);
             flags |= SF_HAS_BOUNDS;
         }

@@ -49,12 +49,14 @@ struct HostScene {
     std::vector<float> s_xform;        // 9 per shape
     std::vector<float> s_stroke;       // 1 per shape
     std::vector<float> s_box;          // 4 per shape: padded group-space bounds (the group BVH's leaf boxes)
-    std::vector<float> s_padmul;       // 1 per shape: stroke-pad multiplier (miter limit for miter joins, else 1)
+    std::vector<float> s_padmul;       // 1 per shape: stroke-pad multiplier (miter limit for miter joins,
+                                       // at least sqrt 2 for open paths with square caps, else 1)
 
     // paths (one record per path shape)
     std::vector<int32_t> p_info;       // 8 per path: seg off, seg count, node off, node count,
                                        //             point off, point count, ctrl off, flags
     std::vector<int32_t> p_shape;      // 1 per path: its shape id
+    std::vector<float> p_miter;        // 1 per path: miter limit (>= 1) for miter joins
     std::vector<float> pn_bounds;      // 4 per path-BVH node
     std::vector<int32_t> pn_meta;      // 4 per node: skip, leaf start (into pl_segs), count, right child
     std::vector<int32_t> pl_segs;      // leaf order: global segment index
@@ -80,6 +82,14 @@ struct HostScene {
                                          // so the tables can be rebuilt in place when points move)
     std::vector<float> path_cdf, path_pmf, path_len_arr;
     std::vector<int32_t> path_pid;       // point id per cdf entry
+};
+
+// Bits of a path's flags word (the fourth int of its second p_info entry) above the
+// DVG_PATH_* bits: set when the stroke uses joins or caps other than round.
+enum PathStyle : int32_t {
+    PATH_STYLED = 8,
+    PATH_JOIN_SHIFT = 4,  // 2 bits: DVG_JOIN_*
+    PATH_CAP_SHIFT = 6,   // 2 bits: DVG_CAP_*
 };
 
 enum ShapeFlags : int32_t {

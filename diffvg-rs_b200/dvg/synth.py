@@ -22,6 +22,10 @@ PCG64 generator and a fixed seed).
 * ``large_scene``      1024x1024, 4x4 spp, 4096 closed cubic paths of 16
                        segments, 25% stroked (width U[0.5,8]), radial 3-stop
                        fills, group and shape transforms.
+* ``styled_stroke_scene`` stroked open and closed paths (lines, quadratics,
+                       cubics; some with per-point thickness) with every join
+                       (miter with limits U[1,6], bevel, round) and cap (butt,
+                       square, round), translucent solid strokes, a few filled.
 """
 from __future__ import annotations
 
@@ -31,7 +35,8 @@ from typing import List, Tuple
 import numpy as np
 
 from .scene import (Circle, Color, Ellipse, Filter, FilterType, FillRule, GradientStop, LinearGradient, Mat3,
-                    Path, PathGeometry, RadialGradient, Rect, RenderOptions, Scene, Shape, ShapeGroup)
+                    Path, PathGeometry, RadialGradient, Rect, RenderOptions, Scene, Shape, ShapeGroup, StrokeCap,
+                    StrokeJoin)
 
 
 def _closed_cubic(rng: np.random.Generator, nseg: int, lo, hi) -> Path:
@@ -251,4 +256,35 @@ def primitives_scene() -> Scene:
     g.set_shape_to_canvas(Mat3.translate(2.0, -1.0).mul(Mat3.scale(1.05, 0.95)))
     sc.groups.append(g)
     sc.groups.append(ShapeGroup([4], None, Color(0.8, 0.1, 0.5, 1.0)))
+    return sc
+
+
+def styled_stroke_scene(seed: int = 0, width: int = 96, height: int = 96, num_paths: int = 12) -> Scene:
+    """Stroked paths with every join and cap (the library's extension beyond the
+    crate's round-only stroking)."""
+    rng = np.random.default_rng(seed)
+    sc = Scene(width, height)
+    sc.background = Color(1.0, 1.0, 1.0, 1.0)
+    sc.filter = Filter(FilterType.BOX, 0.5)
+    side = float(min(width, height))
+    for i in range(num_paths):
+        closed = bool(rng.uniform() < 0.35)
+        nseg = int(rng.integers(2, 6))
+        ncp = [int(rng.integers(0, 3)) for _ in range(nseg)]
+        npts = sum(c + 1 for c in ncp) + (0 if closed else 1)
+        cx, cy = rng.uniform(0.2 * side, 0.8 * side, 2)
+        r = rng.uniform(0.1, 0.3) * side
+        pts = [(float(np.float32(cx + rng.uniform(-r, r))), float(np.float32(cy + rng.uniform(-r, r))))
+               for _ in range(npts)]
+        thick = None
+        if rng.uniform() < 0.25:
+            thick = [float(np.float32(rng.uniform(0.5, 3.0))) for _ in range(npts)]
+        sh = Shape(PathGeometry(Path(ncp, pts, thick, closed, False)))
+        sh.stroke_width = float(np.float32(rng.uniform(0.75, 4.0)))
+        sh.stroke_join = StrokeJoin(int(rng.integers(0, 3)))
+        sh.stroke_cap = StrokeCap(int(rng.integers(0, 3)))
+        sh.stroke_miter_limit = float(np.float32(rng.uniform(1.0, 6.0)))
+        sc.shapes.append(sh)
+        fill = _solid(rng) if closed and rng.uniform() < 0.5 else None
+        sc.groups.append(ShapeGroup([i], fill, _solid(rng)))
     return sc

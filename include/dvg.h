@@ -53,8 +53,15 @@ enum { DVG_FILTER_BOX = 0, DVG_FILTER_TENT = 1, DVG_FILTER_RADIAL_PARABOLIC = 2,
        DVG_FILTER_GAUSSIAN = 4 };
 /* FillRule (src/scene.rs:47-63). */
 enum { DVG_FILL_NONZERO = 0, DVG_FILL_EVENODD = 1 };
-/* StrokeJoin / StrokeCap (src/scene.rs:66-107).  Only round joins/caps are rendered,
- * as in the crate; the other values only widen bounds (miter) like the crate does. */
+/* StrokeJoin / StrokeCap (src/scene.rs:66-107).  The crate renders round joins and
+ * caps only (the other values just widen bounds); this library also renders the
+ * others for paths, in the forward pass and the interior adjoint (non-prefiltered):
+ * bevel (the outer triangle at a vertex), miter (up to shape_miter_limit radii from
+ * the vertex, else bevel), butt (the stroke ends at the end point's normal) and
+ * square (one radius beyond the end).  Round (the default) is the crate's result
+ * bit for bit.  Prefiltered coverage, the signed distance and the boundary sampling
+ * of the edge term keep the crate's round geometry (the join and cap outline edges
+ * are not sampled).  Other values are rejected as an invalid scene. */
 enum { DVG_JOIN_MITER = 0, DVG_JOIN_BEVEL = 1, DVG_JOIN_ROUND = 2 };
 enum { DVG_CAP_BUTT = 0, DVG_CAP_SQUARE = 1, DVG_CAP_ROUND = 2 };
 /* Path flags. */

@@ -180,6 +180,7 @@ struct Shape {  // scene.rs:184-197
     float stroke_width;
     uint32_t join;
     float miter;
+    uint32_t cap = DVG_CAP_ROUND;
 };
 struct Group {  // scene.rs:215-230
     std::vector<size_t> shape_ids;
@@ -226,6 +227,7 @@ static Scene decode(const dvg_scene_desc* d) {
         sh.stroke_width = d->shape_stroke_width[i];
         sh.join = d->shape_stroke_join ? d->shape_stroke_join[i] : (uint32_t)DVG_JOIN_ROUND;
         sh.miter = d->shape_miter_limit ? d->shape_miter_limit[i] : 4.0f;
+        sh.cap = d->shape_stroke_cap ? d->shape_stroke_cap[i] : (uint32_t)DVG_CAP_ROUND;
         if (sh.kind == DVG_SHAPE_PATH) {
             uint32_t co = d->path_ctrl_offset[i], cc = d->path_ctrl_count[i];
             uint32_t po = d->path_point_offset[i], pc = d->path_point_count[i];
@@ -750,7 +752,10 @@ static float max_stroke_radius(const Shape& s) {  // shape.rs:62-78
         for (float v : s.path.thick) mt = std::fmax(mt, std::fabs(v));
         radius = std::fmax(radius, mt * stroke_scale);
     }
-    if (radius > 0.0f && s.join == DVG_JOIN_MITER) radius *= std::fmax(s.miter, 1.0f);
+    float pm = s.join == DVG_JOIN_MITER ? std::fmax(s.miter, 1.0f) : 1.0f;
+    // extension: square caps reach sqrt(2) (rounded up) radii from an open path's ends
+    if (s.kind == DVG_SHAPE_PATH && !s.path.closed && s.cap == DVG_CAP_SQUARE) pm = std::fmax(pm, 1.41422f);
+    if (radius > 0.0f) radius *= pm;
     return radius;
 }
 static bool shape_bounds(const Shape& s, Bounds* out) {  // shape.rs:9-14
@@ -888,13 +893,12 @@ static Bounds segment_bounds(std::initializer_list<V2> pts, float pad) {  // sha
     }
     return inflate_bounds(b, pad);
 }
-static bool build_path_bvh(const Shape& s, PathBvh* out) {  // bvh.rs:241-381
-    if (s.kind != DVG_SHAPE_PATH) return false;
+// The path's segments in path order with per-point radii (bvh.rs:255-364).
+static std::vector<SegData> path_segments(const Shape& s, float dr) {
     const PathG& p = s.path;
-    if (p.pts.empty()) return false;
-    float dr = s.stroke_width;
     size_t point_id = 0;
     std::vector<SegData> segs;
+    if (p.pts.empty()) return segs;
     for (size_t si = 0; si < p.ncp.size(); ++si) {
         uint8_t nc = p.ncp[si];
         V2 q[4];
@@ -925,13 +929,19 @@ static bool build_path_bvh(const Shape& s, PathBvh* out) {  // bvh.rs:241-381
             break;
         }
     }
+    return segs;
+}
+static bool build_path_bvh(const Shape& s, PathBvh* out) {  // bvh.rs:241-381
+    if (s.kind != DVG_SHAPE_PATH) return false;
+    if (s.path.pts.empty()) return false;
+    std::vector<SegData> segs = path_segments(s, s.stroke_width);
     if (segs.empty()) return false;
     out->segments = segs;
     out->indices.resize(segs.size());
     for (size_t i = 0; i < segs.size(); ++i) out->indices[i] = i;
     out->nodes.clear();
     build_node(out->nodes, [&](size_t i) { return out->segments[i].bounds; }, out->indices, 0, segs.size());
-    out->approx = p.approx;
+    out->approx = s.path.approx;
     return true;
 }
 static GroupBvh build_group_bvh(const Scene& sc, const Group& g) {  // bvh.rs:156-187
@@ -976,7 +986,96 @@ static CP seg_closest(const SegData& s, V2 pt, bool approx) {
     if (s.kind == 1) return closest_point_quadratic(pt, s.p0, s.p1, s.p2, approx);
     return closest_point_cubic(pt, s.p0, s.p1, s.p2, s.p3, approx);
 }
-static bool within_distance_path_bvh(const PathBvh& pb, V2 pt) {  // closest.rs:20-98
+// ---------------------------------------------------------------- stroke joins and caps
+// Not in the crate, which strokes every path with round joins and caps (its join and
+// cap fields only pad bounds, prepare.rs:207-210): the library's extension, restated
+// with the same arithmetic as its kernels.  A path whose join (or, open, cap) is not
+// round keeps the crate's segment-body test except that a closest point exactly at
+// a segment end with such a join or cap does not count; the join or cap region is
+// added instead (bevel triangle; miter quad up to the miter limit, else bevel; butt:
+// nothing; square: a rectangle one radius long and two wide beyond the end).
+static bool style_nonround(const Shape& s) {
+    if (s.kind != DVG_SHAPE_PATH) return false;
+    return s.join != DVG_JOIN_ROUND || (!s.path.closed && s.cap != DVG_CAP_ROUND);
+}
+static bool end_excluded(const Shape& s, size_t seg, size_t nseg, float t) {
+    const bool at0 = t == 0.0f, at1 = t == 1.0f;
+    if (!style_nonround(s) || !(at0 || at1)) return false;
+    const bool join = s.path.closed || (at0 ? seg > 0 : seg + 1 < nseg);
+    return join ? s.join != DVG_JOIN_ROUND : s.cap != DVG_CAP_ROUND;
+}
+static V2 seg_dir0(const SegData& g) {
+    V2 d = g.p1 - g.p0;
+    if (d.x == 0.0f && d.y == 0.0f) d = g.p2 - g.p0;
+    if (d.x == 0.0f && d.y == 0.0f) d = g.p3 - g.p0;
+    return d;
+}
+static V2 seg_dir1(const SegData& g) {
+    V2 d = g.p3 - g.p2;
+    if (d.x == 0.0f && d.y == 0.0f) d = g.p3 - g.p1;
+    if (d.x == 0.0f && d.y == 0.0f) d = g.p3 - g.p0;
+    return d;
+}
+static float cross2f(float ax, float ay, float bx, float by) { return ax * by - ay * bx; }
+static bool in_triangle(V2 p, V2 a, V2 b, V2 c) {
+    const float d1 = cross2f(b.x - a.x, b.y - a.y, p.x - a.x, p.y - a.y);
+    const float d2 = cross2f(c.x - b.x, c.y - b.y, p.x - b.x, p.y - b.y);
+    const float d3 = cross2f(a.x - c.x, a.y - c.y, p.x - c.x, p.y - c.y);
+    const bool neg = d1 < 0.0f || d2 < 0.0f || d3 < 0.0f, pos = d1 > 0.0f || d2 > 0.0f || d3 > 0.0f;
+    return !(neg && pos);
+}
+static bool join_hit(V2 p, V2 v, V2 din, V2 dout, float r, uint32_t join, float limit) {
+    const float li = std::sqrt(din.x * din.x + din.y * din.y), lo = std::sqrt(dout.x * dout.x + dout.y * dout.y);
+    if (!(li > 0.0f) || !(lo > 0.0f) || !(r > 0.0f)) return false;
+    din = mk(din.x / li, din.y / li);
+    dout = mk(dout.x / lo, dout.y / lo);
+    const float cr = cross2f(din.x, din.y, dout.x, dout.y);
+    if (std::fabs(cr) < 1.0e-6f) return false;
+    const float sg = cr > 0.0f ? 1.0f : -1.0f;
+    const V2 a = mk(v.x + r * sg * din.y, v.y - r * sg * din.x);
+    const V2 b = mk(v.x + r * sg * dout.y, v.y - r * sg * dout.x);
+    if (join == DVG_JOIN_MITER) {
+        const float sm = cross2f(b.x - a.x, b.y - a.y, dout.x, dout.y) / cr;
+        const V2 m = mk(a.x + sm * din.x, a.y + sm * din.y);
+        const float ml = std::sqrt((m.x - v.x) * (m.x - v.x) + (m.y - v.y) * (m.y - v.y));
+        if (ml <= limit * r) return in_triangle(p, v, a, m) || in_triangle(p, v, m, b);
+    }
+    return in_triangle(p, v, a, b);
+}
+static bool square_cap_hit(V2 p, V2 v, V2 d, float r) {
+    const float l = std::sqrt(d.x * d.x + d.y * d.y);
+    if (!(l > 0.0f) || !(r > 0.0f)) return false;
+    const float dx = d.x / l, dy = d.y / l, qx = p.x - v.x, qy = p.y - v.y;
+    const float sp = qx * dx + qy * dy, u = qx * -dy + qy * dx;
+    return sp >= 0.0f && sp <= r && std::fabs(u) <= r;
+}
+// segs: the path's segments in path order (quadratics and lines repeat their last point).
+static bool join_cap_hit(const Shape& s, const std::vector<SegData>& segs, V2 p) {
+    const bool closed = s.path.closed;
+    const float limit = std::fmax(s.miter, 1.0f);
+    const float reach = (s.join == DVG_JOIN_MITER ? limit : 1.0f) * 1.001f;
+    const size_t n = segs.size();
+    for (size_t k = 0; k < n; ++k) {
+        const SegData& g = segs[k];
+        const V2 v = g.p0;
+        const float r = g.r0;
+        if (k > 0 || closed) {
+            if (s.join == DVG_JOIN_ROUND) continue;
+            const float dx = p.x - v.x, dy = p.y - v.y;
+            if (dx * dx + dy * dy > (reach * r) * (reach * r)) continue;
+            const SegData& in = segs[k > 0 ? k - 1 : n - 1];
+            if (join_hit(p, v, seg_dir1(in), seg_dir0(g), r, s.join, limit)) return true;
+        } else if (s.cap == DVG_CAP_SQUARE) {
+            const V2 d = seg_dir0(g);
+            if (square_cap_hit(p, v, mk(-d.x, -d.y), r)) return true;
+        }
+    }
+    if (!closed && s.cap == DVG_CAP_SQUARE && n > 0)
+        if (square_cap_hit(p, segs[n - 1].p3, seg_dir1(segs[n - 1]), segs[n - 1].r3)) return true;
+    return false;
+}
+
+static bool within_distance_path_bvh(const PathBvh& pb, V2 pt, const Shape* style) {  // closest.rs:20-98
     if (pb.nodes.empty()) return false;
     std::vector<size_t> stack{0};
     while (!stack.empty()) {
@@ -988,14 +1087,16 @@ static bool within_distance_path_bvh(const PathBvh& pb, V2 pt) {  // closest.rs:
             for (size_t i = n.start; i < (size_t)n.start + n.count; ++i) {
                 const SegData& s = pb.segments[pb.indices[i]];
                 CP c = seg_closest(s, pt, pb.approx);
-                if (c.dist < seg_radius(s, c.t)) return true;
+                if (c.dist < seg_radius(s, c.t) &&
+                    !(style && end_excluded(*style, pb.indices[i], pb.segments.size(), c.t)))
+                    return true;
             }
         } else {
             if (n.left != BVH_NONE) stack.push_back(n.left);
             if (n.right != BVH_NONE) stack.push_back(n.right);
         }
     }
-    return false;
+    return style && style_nonround(*style) && join_cap_hit(*style, pb.segments, pt);
 }
 struct PathHit {
     bool valid = false;
@@ -1059,6 +1160,14 @@ static bool within_distance_shape(const Shape& s, V2 pt, float r) {  // closest.
     if (s.kind == DVG_SHAPE_RECT) {
         float dist = rect_signed_distance(lp, mk(s.prm[0], s.prm[1]), mk(s.prm[2], s.prm[3]));
         return std::fabs(dist) < r;
+    }
+    if (s.kind == DVG_SHAPE_PATH && style_nonround(s)) {  // joins / caps other than round (extension)
+        std::vector<SegData> segs = path_segments(s, r);
+        for (size_t k = 0; k < segs.size(); ++k) {
+            CP c = seg_closest(segs[k], lp, s.path.approx);
+            if (c.dist < seg_radius(segs[k], c.t) && !end_excluded(s, k, segs.size(), c.t)) return true;
+        }
+        return join_cap_hit(s, segs, lp);
     }
     if (s.kind == DVG_SHAPE_PATH) {
         const PathG& p = s.path;
@@ -1259,7 +1368,7 @@ static bool within_distance_bvh(const Scene& sc, const SceneBvh& bvh, size_t gi,
                 if (s.stroke_width <= 0.0f) continue;
                 if (bs.has_path_bvh) {
                     V2 sp = xform_inv_dist(s.transform, lp);
-                    if (within_distance_path_bvh(bs.path_bvh, sp)) return true;
+                    if (within_distance_path_bvh(bs.path_bvh, sp, &s)) return true;
                 } else if (within_distance_shape(s, lp, s.stroke_width)) {
                     return true;
                 }
