@@ -172,6 +172,49 @@ def large_fit(r, dev, lib_stream, steps, warmup, rank):
             "launch_shape": {"sample_layout": tuning[0], "boundary_cell": tuning[1], "fragment_slots": tuning[2]}}
 
 
+def single_scene_sharded(r, dev, lib_stream, steps, warmup, rank, world):
+    """One large scene split over all ranks (strong scaling): every rank renders a band
+    of tiles and a range of boundary samples; NCCL sums the splat accumulators after the
+    forward and the gradients after the backward (dvg.shard.SceneShardStep)."""
+    import torch
+    import torch.distributed as dist
+
+    from dvg.shard import SceneShardStep
+
+    sc = synth.large_scene(0)  # the same scene on every rank
+    opts = RenderOptions(samples_x=4, samples_y=4, seed=0, jitter=True, use_prefiltering=False)
+    bopts = BackwardOptions(boundary_samples=sc.width * sc.height)
+    up = r.upload(sc)
+    tu = r.upload(synth.large_scene(8))
+    target = torch.empty(sc.width * sc.height * 4, device=dev)
+    tu.render_device(opts, target.data_ptr())
+    torch.cuda.synchronize(dev)
+    tu.close()
+    reduce = (lambda t: dist.all_reduce(t)) if world > 1 else (lambda t: None)
+    step = SceneShardStep(up, opts, bopts, rank, world, reduce, device=dev)
+    torch.cuda.synchronize(dev)
+    with torch.cuda.stream(lib_stream):
+        for _ in range(warmup):
+            step.step(target)
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(lib_stream)
+        for _ in range(steps):
+            step.step(target)
+        e1.record(lib_stream)
+    torch.cuda.synchronize(dev)
+    ms = max_over_ranks([e0.elapsed_time(e1) / steps], dev)[0]
+    up.close()
+    samples = sc.width * sc.height * opts.samples_x * opts.samples_y
+    return {"workload": "1024x1024, 4x4 spp, 4096 closed cubic paths x 16 segments (25% stroked), W*H boundary "
+                        "samples, one scene split over the ranks (tile bands, boundary-sample ranges)",
+            "world": world, "steps": steps, "ms_per_step": ms, "msamples_per_s": samples / (ms / 1e3) / 1e6,
+            "scaling": "strong", "tiles_of_this_rank": list(step.tiles),
+            "collectives": "NCCL all-reduce of the W*H*5 splat accumulators and of the gradient buffer per step"}
+
+
 def batched_vs_plain(r, dev, lib_stream, flush, scenes, steps, label):
     """One batched CUDA-graph step over `scenes` against the loop of single-scene
     calls doing the same work (forward + L2 + backward, then the full optimisation
@@ -306,6 +349,7 @@ def main():
     ap.add_argument("--batch-scenes", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=5)
     ap.add_argument("--large-fit-steps", type=int, default=5)
+    ap.add_argument("--shard-steps", type=int, default=3)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -420,6 +464,10 @@ def main():
         if world > 1:
             fit["ms_per_iter"] = max_over_ranks([fit["ms_per_iter"]], dev)[0]
 
+    sharded = None
+    if args.shard_steps > 0:
+        sharded = single_scene_sharded(r, dev, lib_stream, args.shard_steps, 2, rank, world)
+
     batched = None
     if args.batch_scenes > 0:
         batched = batched_vs_plain(
@@ -489,7 +537,7 @@ def main():
                              "as required, see profiles/ for the issue-slot view"},
         "kernel_ms_per_step": prof_json,
         "gpu_launches": int(timed_launches), "clocks": clocks.summary(), "e2e": e2e,
-        "batched_vs_plain": batched, "large_fit": fit,
+        "batched_vs_plain": batched, "large_fit": fit, "single_scene_sharded": sharded,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         img = out.view(H, W, 4).cpu().numpy()

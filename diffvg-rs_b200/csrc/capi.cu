@@ -113,6 +113,12 @@ struct dvg_context {
     dvg_render_options kept_opts{};
     uint64_t kept_gen = 0;
     bool kept_weights = false, kept_frag = false;
+    // The last dvg_shard_forward (its fragment codes serve the shard backward that follows).
+    const dvg_scene* shard_scene = nullptr;
+    dvg_render_options shard_opts{};
+    uint32_t shard_t0 = 0, shard_t1 = 0;
+    uint64_t shard_gen = 0;
+    bool shard_frag = false;
 };
 
 struct dvg_scene {
@@ -237,6 +243,8 @@ SampleParams sample_params(const dvg_render_options* o, int layout = 1) {
     sp.frag = nullptr;
     sp.frag_n = nullptr;
     sp.frag_slots = 0;
+    sp.tile_base = 0;
+    sp.tile_count = 0;
     return sp;
 }
 // Points sp at a fragment cache of frag_cache_bytes(tiles, spp, slots) bytes at `base`.
@@ -497,6 +505,7 @@ void dvg_scene_destroy(dvg_scene* scene) {
     if (!scene) return;
     cudaSetDevice(scene->ctx->device);
     cudaStreamSynchronize(scene->ctx->stream);
+    if (scene->ctx->shard_scene == scene) scene->ctx->shard_scene = nullptr;
     delete scene;
 }
 
@@ -589,14 +598,23 @@ static dvg_status render_host_impl(dvg_context* ctx, dvg_scene* scene, const dvg
 
 // Backward on device buffers.  `have_weights`: ctx->wsum already holds this scene's
 // weights; `frag_ready`: the forward just filled ctx->frag for these options.
+// `shard` (optional): only its tiles and boundary samples, with the weight image
+// `shard_wsum` (the sum over all shards' forwards) instead of ctx->wsum.
 static dvg_status backward_core(dvg_context* ctx, dvg_scene* sc, const dvg_render_options* opts,
                                 const dvg_backward_options* bopts, const float* d_render, const float* d_sdf,
-                                const GradPtrs& G, bool have_weights, bool frag_ready = false) {
+                                const GradPtrs& G, bool have_weights, bool frag_ready = false,
+                                const dvg_shard* shard = nullptr, const float* shard_wsum = nullptr) {
     const DevScene& S = sc->dev;
     const size_t npix = (size_t)S.width * S.height;
     if (npix == 0) return DVG_OK;
     SampleParams sp = sample_params(opts, (int)sc->tune.sample_layout);
     if (frag_ready) attach_frag(sp, ctx->frag.ptr, S.tiles_x * S.tiles_y, (int)sc->tune.fragment_slots);
+    const bool run_tiles = !shard || shard->tile_end > shard->tile_begin;  // a shard may hold samples only
+    if (shard && run_tiles) {
+        sp.tile_base = (int)shard->tile_begin;
+        sp.tile_count = (int)(shard->tile_end - shard->tile_begin);
+    }
+    const float* wsum = shard ? shard_wsum : ctx->wsum.as<float>();
     if (d_render && S.num_groups > 0) {
         if (!have_weights) {
             ++ctx->gen;
@@ -606,32 +624,33 @@ static dvg_status backward_core(dvg_context* ctx, dvg_scene* sc, const dvg_rende
             ctx->launches += launch_weights(S, sp, ctx->wsum.as<float>(), ctx->stream);
             CK(cudaGetLastError());
         }
-        {
+        if (run_tiles) {
             Prof prof_(ctx, opts->use_prefiltering ? "interior_prefilter" : "interior");
             if (opts->use_prefiltering)
                 ctx->launches +=
-                    launch_interior_prefilter(S, sp, d_render, ctx->wsum.as<float>(), G, ctx->status, ctx->stream);
+                    launch_interior_prefilter(S, sp, d_render, wsum, G, ctx->status, ctx->stream);
             else
-                ctx->launches += launch_interior(S, sp, d_render, ctx->wsum.as<float>(), G, ctx->status, ctx->stream);
+                ctx->launches += launch_interior(S, sp, d_render, wsum, G, ctx->status, ctx->stream);
         }
         CK(cudaGetLastError());
         if (S.boundary_ok && !opts->use_prefiltering) {  // src/backward/render.rs:191
             BoundaryParams bp;
             uint64_t total = (uint64_t)npix * sp.sxn * sp.syn;
-            bp.num_samples = bopts && bopts->boundary_samples ? bopts->boundary_samples : total;
-            bp.sample_base = 0;
-            bp.slot_base = 0;
+            total = bopts && bopts->boundary_samples ? bopts->boundary_samples : total;
+            bp.sample_base = shard ? std::min<uint64_t>(shard->sample_begin, total) : 0;
+            bp.num_samples = shard ? std::min<uint64_t>(std::max(shard->sample_end, shard->sample_begin), total) : total;
+            bp.slot_base = bp.sample_base;
             bp.seed = (bopts && !bopts->boundary_seed_from_options) ? bopts->boundary_seed : opts->seed;
             bp.rng = bopts ? (int)bopts->rng : 0;
             bp.cell = (int)sc->tune.boundary_cell;
-            const uint64_t cap = std::min<uint64_t>(bp.num_samples, (uint64_t)1 << 24);
+            const uint64_t cap = std::max<uint64_t>(std::min<uint64_t>(bp.num_samples - bp.sample_base, (uint64_t)1 << 24), 1);
             const int tiles = S.tiles_x * S.tiles_y;
             CK(ctx->bsamples.reserve(cap * sizeof(BSample)));
             CK(ctx->bkey.reserve(cap * sizeof(int)));
             CK(ctx->border.reserve(cap * sizeof(int)));
             CK(ctx->bcounts.reserve((2 * (size_t)tiles * BND_MAX_BUCKETS + 1) * sizeof(int)));
             Prof prof_(ctx, "boundary");
-            ctx->launches += launch_boundary(S, bp, d_render, ctx->wsum.as<float>(), G, ctx->bsamples.as<BSample>(),
+            ctx->launches += launch_boundary(S, bp, d_render, wsum, G, ctx->bsamples.as<BSample>(),
                                              ctx->bkey.as<int>(), ctx->bcounts.as<int>(), ctx->border.as<int>(), cap,
                                              ctx->stream);
             CK(cudaGetLastError());
@@ -645,9 +664,9 @@ static dvg_status backward_core(dvg_context* ctx, dvg_scene* sc, const dvg_rende
             Prof prof_(ctx, "weights");
             ctx->launches += launch_weights(S, sp, ctx->wsum.as<float>(), ctx->stream);
         }
-        {
+        if (run_tiles) {
             Prof prof_(ctx, "interior");
-            ctx->launches += launch_interior(S, sp, d_render, ctx->wsum.as<float>(), G, ctx->status, ctx->stream);
+            ctx->launches += launch_interior(S, sp, d_render, wsum, G, ctx->status, ctx->stream);
         }
         CK(cudaGetLastError());
     }
@@ -897,6 +916,113 @@ dvg_status dvg_fwd_bwd_l2_device(dvg_context* ctx, dvg_scene* scene, const dvg_r
     st = zero_grads(ctx, scene, G);
     if (st != DVG_OK) return st;
     return backward_core(ctx, scene, opts, bopts, ctx->d_render.as<float>(), nullptr, G, true, frag);
+}
+
+// ---------------------------------------------------------------------------
+// One scene split over several processes: forward per band of tiles, the caller sums
+// the accumulators, then resolve / loss on the whole image and backward per band of
+// tiles and range of boundary samples; the caller sums the gradients.
+static dvg_status check_shard(const dvg_scene* scene, const dvg_shard* shard) {
+    if (!shard) return fail(DVG_ERR_INVALID_ARGUMENT, "null shard");
+    const uint32_t tiles = (uint32_t)(scene->dev.tiles_x * scene->dev.tiles_y);
+    if (shard->tile_begin > shard->tile_end || shard->tile_end > tiles || shard->sample_begin > shard->sample_end)
+        return fail(DVG_ERR_INVALID_ARGUMENT, "shard range out of order or past the last tile");
+    return DVG_OK;
+}
+
+dvg_status dvg_scene_tile_count(const dvg_scene* scene, uint32_t* tiles) {
+    if (!scene || !tiles) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    *tiles = (uint32_t)(scene->dev.tiles_x * scene->dev.tiles_y);
+    return DVG_OK;
+}
+
+dvg_status dvg_shard_forward(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
+                             const dvg_shard* shard, float* accum_rgba, float* wsum) {
+    if (!ctx || !scene || !accum_rgba || !wsum) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    dvg_status st = check_options(opts);
+    if (st == DVG_OK) st = check_shard(scene, shard);
+    if (st != DVG_OK) return st;
+    CK(cudaSetDevice(ctx->device));
+    const DevScene& S = scene->dev;
+    const size_t npix = (size_t)S.width * S.height;
+    ++ctx->gen;
+    ctx->shard_scene = nullptr;
+    if (npix == 0) return DVG_OK;
+    CK(cudaMemsetAsync(accum_rgba, 0, npix * 4 * sizeof(float), ctx->stream));
+    CK(cudaMemsetAsync(wsum, 0, npix * sizeof(float), ctx->stream));
+    if (S.num_groups == 0 || shard->tile_end == shard->tile_begin) return DVG_OK;
+    SampleParams sp = sample_params(opts, (int)scene->tune.sample_layout);
+    sp.tile_base = (int)shard->tile_begin;
+    sp.tile_count = (int)(shard->tile_end - shard->tile_begin);
+    bool frag = false;
+    if (!opts->use_prefiltering && scene->tune.fragment_slots > 0) {
+        const int tiles = S.tiles_x * S.tiles_y, slots = (int)scene->tune.fragment_slots;
+        CK(ctx->frag.reserve(frag_cache_bytes(tiles, sp.sxn * sp.syn, slots)));
+        attach_frag(sp, ctx->frag.ptr, tiles, slots);
+        frag = true;
+    }
+    {
+        Prof prof_(ctx, opts->use_prefiltering ? "forward_prefilter" : "forward");
+        if (opts->use_prefiltering)
+            ctx->launches += launch_forward_prefilter(S, sp, accum_rgba, wsum, ctx->status, ctx->stream);
+        else
+            ctx->launches += launch_forward(S, sp, accum_rgba, wsum, ctx->status, ctx->stream);
+    }
+    CK(cudaGetLastError());
+    ctx->shard_scene = scene;
+    ctx->shard_opts = *opts;
+    ctx->shard_t0 = shard->tile_begin;
+    ctx->shard_t1 = shard->tile_end;
+    ctx->shard_gen = ctx->gen;
+    ctx->shard_frag = frag;
+    return DVG_OK;
+}
+
+dvg_status dvg_shard_resolve(dvg_context* ctx, dvg_scene* scene, const float* accum_rgba, const float* wsum,
+                             float* out_rgba) {
+    if (!ctx || !scene || !accum_rgba || !wsum || !out_rgba) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    CK(cudaSetDevice(ctx->device));
+    const DevScene& S = scene->dev;
+    if ((size_t)S.width * S.height == 0) return DVG_OK;
+    if (S.num_groups == 0) {
+        ctx->launches += launch_fill_background(S, out_rgba, ctx->stream);
+    } else {
+        Prof prof_(ctx, "resolve");
+        ctx->launches += launch_resolve(S, accum_rgba, wsum, out_rgba, ctx->stream);
+    }
+    CK(cudaGetLastError());
+    return DVG_OK;
+}
+
+dvg_status dvg_l2_device(dvg_context* ctx, const float* image, const float* target, uint64_t n, float* d_render,
+                         float* loss) {
+    if (!ctx || !image || !target || !d_render) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    CK(cudaSetDevice(ctx->device));
+    if (loss) CK(cudaMemsetAsync(loss, 0, sizeof(float), ctx->stream));
+    if (n == 0) return DVG_OK;
+    Prof prof_(ctx, "l2_loss");
+    ctx->launches += launch_l2(image, target, (size_t)n, d_render, loss, ctx->stream);
+    CK(cudaGetLastError());
+    return DVG_OK;
+}
+
+dvg_status dvg_shard_backward(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
+                              const dvg_backward_options* bopts, const dvg_shard* shard, const float* d_render,
+                              const float* wsum, dvg_grads* grads) {
+    dvg_status st = check_backward_args(ctx, scene, opts, nullptr, grads);
+    if (st == DVG_OK) st = check_shard(scene, shard);
+    if (st != DVG_OK) return st;
+    if (!d_render || !wsum) return fail(DVG_ERR_INVALID_ARGUMENT, "null d_render or weights");
+    CK(cudaSetDevice(ctx->device));
+    GradPtrs G = grads_from_user(grads);
+    if (!(bopts && bopts->compute_translation)) G.d_translation = nullptr;
+    if (!scene->dev.bg_image) G.d_background_image = nullptr;
+    st = zero_grads(ctx, scene, G);
+    if (st != DVG_OK) return st;
+    const bool frag = ctx->shard_frag && ctx->shard_scene == scene && ctx->shard_gen == ctx->gen &&
+                      ctx->shard_t0 == shard->tile_begin && ctx->shard_t1 == shard->tile_end &&
+                      std::memcmp(&ctx->shard_opts, opts, sizeof(dvg_render_options)) == 0;
+    return backward_core(ctx, scene, opts, bopts, d_render, nullptr, G, true, frag, shard, wsum);
 }
 
 }  // extern "C"

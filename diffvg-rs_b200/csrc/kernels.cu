@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(256, DVG_MINB_FWD) k_forward(DevScene S, Sampl
                                                                unsigned* status) {
     extern __shared__ float sm[];
     (void)status;
-    forward_body(S, sp, blockIdx.x, blockIdx.y, accum, wsum, sm);
+    forward_body(S, sp, sp.tile_base + blockIdx.x, blockIdx.y, accum, wsum, sm);
 }
 // Batched forward: one flat grid over every (scene, tile, sub-sample) work item.
 __global__ void __launch_bounds__(256, DVG_MINB_FWD) k_forward_batch(const BatchEntry* __restrict__ B,
@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(256, DVG_MINB_FWD) k_forward_batch(const Batch
 
 // Weight image only (rasterize_weights_f32, forward.rs:1505-1564).
 __global__ void __launch_bounds__(256) k_weights(DevScene S, SampleParams sp, float* wsum) {
-    const int tile = blockIdx.x, sub = blockIdx.y;
+    const int tile = sp.tile_base + blockIdx.x, sub = blockIdx.y;
     const int tx = tile % S.tiles_x, ty = tile / S.tiles_x;
     const int x = tx * TILE + (threadIdx.x % TILE), y = ty * TILE + (threadIdx.x / TILE);
     if (x >= S.width || y >= S.height) return;
@@ -442,12 +442,12 @@ __device__ __forceinline__ void interior_body(const DevScene& S, const SamplePar
 
 __global__ void __launch_bounds__(256, DVG_MINB_INT) k_interior(DevScene S, SampleParams sp, const float* d_render,
                                                                 const float* wsum, GradPtrs G, unsigned* status) {
-    interior_body<false>(S, sp, blockIdx.x, blockIdx.y, d_render, wsum, G, status);
+    interior_body<false>(S, sp, sp.tile_base + blockIdx.x, blockIdx.y, d_render, wsum, G, status);
 }
 __global__ void __launch_bounds__(256, DVG_MINB_LEAN) k_interior_cached(DevScene S, SampleParams sp,
                                                                         const float* d_render, const float* wsum,
                                                                         GradPtrs G, unsigned* status) {
-    interior_body<true>(S, sp, blockIdx.x, blockIdx.y, d_render, wsum, G, status);
+    interior_body<true>(S, sp, sp.tile_base + blockIdx.x, blockIdx.y, d_render, wsum, G, status);
 }
 __global__ void __launch_bounds__(256, DVG_MINB_INT) k_interior_batch(const BatchEntry* __restrict__ B,
                                                                       const int* __restrict__ item_scene,
@@ -1237,15 +1237,14 @@ int launch_binning(const DevScene& S, const float4* g_bbox, int* counts, int* of
 }
 int launch_forward(const DevScene& S, const SampleParams& sp, float* accum, float* wsum, unsigned* status,
                    cudaStream_t stream) {
-    const int tiles = S.tiles_x * S.tiles_y;
     const int hw = TILE + 2 * S.filter_ri;
     size_t smem = S.filter_ri <= MAX_SMEM_RI ? (size_t)hw * hw * 5 * sizeof(float) : 0;
-    dim3 grid(tiles, sp.sxn * sp.syn);
+    dim3 grid(launch_tiles(S, sp), sp.sxn * sp.syn);
     k_forward<<<grid, 256, smem, stream>>>(S, sp, accum, wsum, status);
     return 1;
 }
 int launch_weights(const DevScene& S, const SampleParams& sp, float* wsum, cudaStream_t stream) {
-    dim3 grid(S.tiles_x * S.tiles_y, sp.sxn * sp.syn);
+    dim3 grid(launch_tiles(S, sp), sp.sxn * sp.syn);
     k_weights<<<grid, 256, 0, stream>>>(S, sp, wsum);
     return 1;
 }
@@ -1256,7 +1255,7 @@ int launch_resolve(const DevScene& S, const float* accum, const float* wsum, flo
 }
 int launch_interior(const DevScene& S, const SampleParams& sp, const float* d_render, const float* wsum,
                     const GradPtrs& G, unsigned* status, cudaStream_t stream) {
-    dim3 grid(S.tiles_x * S.tiles_y, sp.sxn * sp.syn);
+    dim3 grid(launch_tiles(S, sp), sp.sxn * sp.syn);
     if (sp.frag) k_interior_cached<<<grid, 256, 0, stream>>>(S, sp, d_render, wsum, G, status);
     k_interior<<<grid, 256, 0, stream>>>(S, sp, d_render, wsum, G, status);
     return sp.frag ? 2 : 1;
@@ -1264,10 +1263,10 @@ int launch_interior(const DevScene& S, const SampleParams& sp, const float* d_re
 int launch_boundary(const DevScene& S, const BoundaryParams& bp, const float* d_render, const float* wsum,
                     const GradPtrs& G, BSample* samples, int* key, int* counts, int* order, uint64_t capacity,
                     cudaStream_t stream) {
-    const uint64_t n = bp.num_samples;
+    const uint64_t n = bp.num_samples;  // samples [bp.sample_base, n)
     const int tiles = S.tiles_x * S.tiles_y * bnd_buckets(bp.cell);  // sort buckets
     int launches = 0;
-    for (uint64_t base = 0; base < n; base += capacity) {
+    for (uint64_t base = bp.sample_base; base < n; base += capacity) {
         const uint64_t cnt = base + capacity < n ? capacity : n - base;
         BoundaryParams b = bp;
         b.sample_base = base;

@@ -40,7 +40,12 @@ struct SampleParams {
     uint16_t* frag;  // fragment codes (NULL: no cache)
     uint8_t* frag_n; // per-sample code count or FRAG_NONE
     int frag_slots;  // codes kept per sample (<= FRAG_MAX_SLOTS)
+    int tile_base, tile_count;  // the tiles a single-scene launch covers (count 0: all)
 };
+// Grid width of a single-scene sample launch: the tiles it covers.
+inline int launch_tiles(const DevScene& S, const SampleParams& sp) {
+    return sp.tile_count > 0 ? sp.tile_count : S.tiles_x * S.tiles_y;
+}
 // Bytes of a fragment cache with `slots` codes per sample for one scene.
 inline size_t frag_cache_bytes(int tiles, int spp, int slots) {
     const size_t samples = (size_t)tiles * spp * 256;

@@ -322,7 +322,7 @@ __device__ __forceinline__ void forward_prefilter_body(const DevScene& S, const 
 __global__ void __launch_bounds__(256, 2) k_forward_prefilter(DevScene S, SampleParams sp, float* accum, float* wsum,
                                                               unsigned* status) {
     extern __shared__ float sm[];
-    forward_prefilter_body(S, sp, blockIdx.x, blockIdx.y, accum, wsum, status, sm);
+    forward_prefilter_body(S, sp, sp.tile_base + blockIdx.x, blockIdx.y, accum, wsum, status, sm);
 }
 __global__ void __launch_bounds__(256, 2) k_forward_prefilter_batch(const BatchEntry* __restrict__ B,
                                                                     const int* __restrict__ item_scene,
@@ -927,7 +927,7 @@ __device__ __forceinline__ void interior_prefilter_body(const DevScene& S, const
 
 __global__ void __launch_bounds__(256) k_interior_prefilter(DevScene S, SampleParams sp, const float* d_render,
                                                             const float* wsum, GradPtrs G, unsigned* status) {
-    interior_prefilter_body(S, sp, blockIdx.x, blockIdx.y, d_render, wsum, G, status);
+    interior_prefilter_body(S, sp, sp.tile_base + blockIdx.x, blockIdx.y, d_render, wsum, G, status);
 }
 __global__ void __launch_bounds__(256) k_interior_prefilter_batch(const BatchEntry* __restrict__ B,
                                                                   const int* __restrict__ item_scene,
@@ -943,13 +943,13 @@ int launch_forward_prefilter(const DevScene& S, const SampleParams& sp, float* a
                              cudaStream_t stream) {
     const int hw = TILE + 2 * S.filter_ri;
     size_t smem = S.filter_ri <= MAX_SMEM_RI ? (size_t)hw * hw * 5 * sizeof(float) : 0;
-    dim3 grid(S.tiles_x * S.tiles_y, sp.sxn * sp.syn);
+    dim3 grid(launch_tiles(S, sp), sp.sxn * sp.syn);
     k_forward_prefilter<<<grid, 256, smem, stream>>>(S, sp, accum, wsum, status);
     return 1;
 }
 int launch_interior_prefilter(const DevScene& S, const SampleParams& sp, const float* d_render, const float* wsum,
                               const GradPtrs& G, unsigned* status, cudaStream_t stream) {
-    dim3 grid(S.tiles_x * S.tiles_y, sp.sxn * sp.syn);
+    dim3 grid(launch_tiles(S, sp), sp.sxn * sp.syn);
     k_interior_prefilter<<<grid, 256, 0, stream>>>(S, sp, d_render, wsum, G, status);
     return 1;
 }

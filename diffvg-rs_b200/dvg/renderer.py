@@ -52,6 +52,11 @@ EXPORTED = (
 )
 
 
+class ShardC(C.Structure):
+    _fields_ = [("tile_begin", C.c_uint32), ("tile_end", C.c_uint32), ("sample_begin", C.c_uint64),
+                ("sample_end", C.c_uint64)]
+
+
 def _tuple(t):
     return int(t.sample_layout), int(t.boundary_cell), int(t.fragment_slots)
 
@@ -122,6 +127,15 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.dvg_context_set_profiling.restype = C.c_int
     L.dvg_context_set_retain.argtypes = [vp, C.c_int]
     L.dvg_context_set_retain.restype = C.c_int
+    Sh = C.POINTER(ShardC)
+    L.dvg_scene_tile_count.argtypes = [vp, C.POINTER(C.c_uint32)]
+    L.dvg_shard_forward.argtypes = [vp, vp, R, Sh, vp, vp]
+    L.dvg_shard_resolve.argtypes = [vp, vp, vp, vp, vp]
+    L.dvg_l2_device.argtypes = [vp, vp, vp, C.c_uint64, vp, vp]
+    L.dvg_shard_backward.argtypes = [vp, vp, R, B, Sh, vp, vp, Gp]
+    for f in ("dvg_scene_tile_count", "dvg_shard_forward", "dvg_shard_resolve", "dvg_l2_device",
+              "dvg_shard_backward"):
+        getattr(L, f).restype = C.c_int
     L.dvg_context_profile.argtypes = [vp, C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.POINTER(C.c_uint64),
                                       C.c_int]
     L.dvg_context_profile.restype = C.c_int
@@ -219,12 +233,22 @@ class DeviceGrads:
         )
         self.tensors = {}
         self.c = GradsC()
+        # one device buffer (parts at 256-byte offsets), so a single collective can sum
+        # the gradients of a scene split over several processes
+        offs, total = {}, 0
         for n in GradBuffers.NAMES:
             sz = int(sizes[n])
             if n in ("d_background_image", "d_translation") and sz == 0:
+                continue
+            offs[n] = (total, max(sz, 1))
+            total += (max(sz, 1) + 63) // 64 * 64
+        self.buffer = torch.zeros(max(total, 1), dtype=torch.float32, device=torch_device)
+        for n in GradBuffers.NAMES:
+            if n not in offs:
                 setattr(self.c, n, C.cast(None, C.POINTER(C.c_float)))
                 continue
-            t = torch.zeros(max(sz, 1), dtype=torch.float32, device=torch_device)
+            o, sz = offs[n]
+            t = self.buffer[o:o + sz]
             self.tensors[n] = t
             setattr(self.c, n, C.cast(C.c_void_p(t.data_ptr()), C.POINTER(C.c_float)))
 
@@ -292,6 +316,33 @@ class UploadedScene:
                                                     C.c_void_p(target_ptr), C.byref(t)))
         return _tuple(t)
 
+    def tile_count(self) -> int:
+        """dvg_scene_tile_count: 16x16 tiles of the canvas (the unit of a shard's band)."""
+        n = C.c_uint32()
+        _check(self.renderer.lib.dvg_scene_tile_count(self.handle, C.byref(n)))
+        return int(n.value)
+
+    def shard_forward(self, options: RenderOptions, tiles, accum_ptr: int, wsum_ptr: int) -> None:
+        """dvg_shard_forward over tiles [begin, end) into zeroed device accumulators."""
+        o = render_options_c(options)
+        sh = ShardC(int(tiles[0]), int(tiles[1]), 0, 0)
+        _check(self.renderer.lib.dvg_shard_forward(self.renderer.ctx, self.handle, C.byref(o), C.byref(sh),
+                                                   C.c_void_p(accum_ptr), C.c_void_p(wsum_ptr)))
+
+    def shard_resolve(self, accum_ptr: int, wsum_ptr: int, out_ptr: int) -> None:
+        _check(self.renderer.lib.dvg_shard_resolve(self.renderer.ctx, self.handle, C.c_void_p(accum_ptr),
+                                                   C.c_void_p(wsum_ptr), C.c_void_p(out_ptr)))
+
+    def shard_backward(self, options: RenderOptions, bopts: Optional[BackwardOptions], tiles, samples,
+                       d_render_ptr: int, wsum_ptr: int, grads: "DeviceGrads") -> None:
+        """dvg_shard_backward: tiles [begin, end), boundary samples [begin, end)."""
+        o = render_options_c(options)
+        b = backward_options_c(bopts)
+        sh = ShardC(int(tiles[0]), int(tiles[1]), int(samples[0]), int(samples[1]))
+        _check(self.renderer.lib.dvg_shard_backward(self.renderer.ctx, self.handle, C.byref(o), C.byref(b),
+                                                    C.byref(sh), C.c_void_p(d_render_ptr), C.c_void_p(wsum_ptr),
+                                                    C.byref(grads.c)))
+
     def render_sdf_device(self, options: RenderOptions, out_ptr: int) -> None:
         """dvg_render_sdf_device into width*height floats of device memory."""
         o = render_options_c(options)
@@ -342,6 +393,11 @@ class Renderer:
     @property
     def stream_handle(self) -> int:
         return int(self.lib.dvg_context_stream(self.ctx) or 0)
+
+    def l2_device(self, image_ptr: int, target_ptr: int, n: int, d_render_ptr: int, loss_ptr: int = 0) -> None:
+        """dvg_l2_device: loss = sum((image - target)^2), d_render = 2 (image - target)."""
+        _check(self.lib.dvg_l2_device(self.ctx, C.c_void_p(image_ptr), C.c_void_p(target_ptr), int(n),
+                                      C.c_void_p(d_render_ptr), C.c_void_p(loss_ptr) if loss_ptr else None))
 
     def set_retain(self, enable: bool) -> None:
         """dvg_context_set_retain: keep the last render for a following render_backward."""

@@ -42,3 +42,47 @@ def weak_scaling_rate(units_per_rank: float, world: int, max_ms: float) -> float
     """Whole-job throughput in units per second when every rank did `units_per_rank`
     units and the slowest rank took `max_ms`."""
     return units_per_rank * world / (max_ms / 1e3)
+
+
+class SceneShardStep:
+    """One scene split over `world` processes: forward + L2 loss + backward of a band
+    of tiles and a range of boundary samples per process, with two sums across
+    processes (the splat accumulators after the forward, the gradients after the
+    backward).  `all_reduce(tensor)` sums a device tensor over the processes in place
+    (torch.distributed.all_reduce over NCCL on GPUs; run step() with the library's
+    stream as torch's current stream so the collectives follow its kernels).  After
+    step() every process holds the whole image, the loss and the whole scene's
+    gradients in `grads`."""
+
+    def __init__(self, scene, options, bopts, rank: int, world: int, all_reduce, device="cuda"):
+        import torch
+
+        from .renderer import DeviceGrads
+        from .scene import BackwardOptions
+
+        self.scene, self.options = scene, options
+        self.bopts = bopts or BackwardOptions()
+        self.all_reduce = all_reduce
+        w, h = scene.scene.width, scene.scene.height
+        self.npix = w * h
+        self.tiles = shard_range(scene.tile_count(), rank, world)
+        nb = self.bopts.boundary_samples or self.npix * options.samples_x * options.samples_y
+        self.samples = shard_range(nb, rank, world)
+        # accumulators in one buffer (RGBA sums, then weights): one collective
+        self.acc = torch.zeros(self.npix * 5, dtype=torch.float32, device=device)
+        self.image = torch.zeros(self.npix * 4, dtype=torch.float32, device=device)
+        self.d_render = torch.zeros(self.npix * 4, dtype=torch.float32, device=device)
+        self.loss = torch.zeros(1, dtype=torch.float32, device=device)
+        self.grads = DeviceGrads(scene.packed, device)
+
+    def step(self, target) -> None:
+        s, acc = self.scene, self.acc
+        accum_ptr, wsum_ptr = acc.data_ptr(), acc.data_ptr() + self.npix * 16
+        s.shard_forward(self.options, self.tiles, accum_ptr, wsum_ptr)
+        self.all_reduce(acc)
+        s.shard_resolve(accum_ptr, wsum_ptr, self.image.data_ptr())
+        s.renderer.l2_device(self.image.data_ptr(), target.data_ptr(), self.npix * 4, self.d_render.data_ptr(),
+                             self.loss.data_ptr())
+        s.shard_backward(self.options, self.bopts, self.tiles, self.samples, self.d_render.data_ptr(), wsum_ptr,
+                         self.grads)
+        self.all_reduce(self.grads.buffer)

@@ -299,6 +299,45 @@ dvg_status dvg_render_backward(dvg_context* ctx, const dvg_scene_desc* desc,
                                const dvg_render_options* opts, const dvg_backward_options* bopts,
                                const float* d_render, const float* d_sdf, dvg_grads* grads);
 
+/* One scene split over several processes (each usually on its own GPU), for scenes
+ * too slow for one device: each process renders a band of 16x16-pixel tiles and a
+ * range of boundary samples, and the caller sums across processes between the calls
+ * (for instance an NCCL all-reduce):
+ *   dvg_shard_forward   -> sum accum_rgba and wsum over processes
+ *   dvg_shard_resolve (+ dvg_l2_device, or any loss) on the whole image, every process
+ *   dvg_shard_backward  -> sum the gradients over processes.
+ * The sums equal a single-process render and backward up to float summation order.
+ * tile_begin / tile_end index the scene's tiles in row-major order
+ * (dvg_scene_tile_count); sample_begin / sample_end index the step's boundary
+ * samples (bopts->boundary_samples, or W*H*spp when 0; clamped to that count).
+ * No counterpart in the crate. */
+typedef struct dvg_shard {
+    uint32_t tile_begin, tile_end;
+    uint64_t sample_begin, sample_end;
+} dvg_shard;
+dvg_status dvg_scene_tile_count(const dvg_scene* scene, uint32_t* tiles);
+/* Zeroes accum_rgba (W*H*4) and wsum (W*H) device buffers, then splats the samples of
+ * the shard's tiles into them (pixels near the band's edges also receive the filter
+ * splats of the neighbouring bands' samples: only the sums are complete).  With the
+ * scene's fragment_slots > 0 it also keeps the samples' fragment codes for the
+ * dvg_shard_backward of the same scene, options and tiles that follows. */
+dvg_status dvg_shard_forward(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
+                             const dvg_shard* shard, float* accum_rgba, float* wsum);
+/* The image from summed accumulators (weighted mean, un-premultiplied; the
+ * background where no weight), W*H*4 device floats. */
+dvg_status dvg_shard_resolve(dvg_context* ctx, dvg_scene* scene, const float* accum_rgba, const float* wsum,
+                             float* out_rgba);
+/* loss = sum((image - target)^2) into *loss (device float, may be NULL) and
+ * d_render = 2 (image - target), n floats each, on device buffers. */
+dvg_status dvg_l2_device(dvg_context* ctx, const float* image, const float* target, uint64_t n, float* d_render,
+                         float* loss);
+/* Zeroes the device gradient buffers, then adds the interior adjoint of the shard's
+ * tiles and the edge-sampling term of its boundary samples; d_render (W*H*4) and
+ * wsum (W*H) are the whole image's. */
+dvg_status dvg_shard_backward(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
+                              const dvg_backward_options* bopts, const dvg_shard* shard, const float* d_render,
+                              const float* wsum, dvg_grads* grads);
+
 /* Forward + L2 loss + backward in one call on an uploaded scene (device pointers):
  * loss = sum((render - target)^2); d_render = 2*(render - target).
  * out_rgba (may be NULL), loss_out (device float, may be NULL).  No counterpart in

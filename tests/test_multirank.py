@@ -70,3 +70,90 @@ def test_shard_range_covers_everything():
             assert spans[0][0] == 0 and spans[-1][1] == n
             assert all(spans[i][1] == spans[i + 1][0] for i in range(world - 1))
             assert max(e - b for b, e in spans) - min(e - b for b, e in spans) <= 1
+
+
+class _FakeShardScene:
+    """Stands in for an uploaded scene on CPU: each shard call writes a value that
+    names the rank into the buffers it is handed, so the test sees what the step
+    summed across ranks and in which order the calls came."""
+
+    def __init__(self, scene, packed, rank, calls):
+        self.scene, self.packed, self.rank, self.calls = scene, packed, rank, calls
+        self.renderer = self
+
+    @staticmethod
+    def _view(ptr, n):
+        import ctypes
+
+        import numpy as np
+
+        return np.ctypeslib.as_array((ctypes.c_float * n).from_address(ptr))
+
+    def tile_count(self):
+        return 7
+
+    def shard_forward(self, options, tiles, accum_ptr, wsum_ptr):
+        n = self.scene.width * self.scene.height
+        self.calls.append(("forward", tuple(tiles)))
+        self._view(accum_ptr, 4 * n)[:] = 1.0 + self.rank
+        self._view(wsum_ptr, n)[:] = 10.0 * (1 + self.rank)
+
+    def shard_resolve(self, accum_ptr, wsum_ptr, out_ptr):
+        n = self.scene.width * self.scene.height
+        self.calls.append(("resolve", float(self._view(accum_ptr, 1)[0]), float(self._view(wsum_ptr, 1)[0])))
+        self._view(out_ptr, 4 * n)[:] = self._view(accum_ptr, 4 * n)
+
+    def l2_device(self, image_ptr, target_ptr, n, d_render_ptr, loss_ptr):
+        self.calls.append(("l2", n))
+
+    def shard_backward(self, options, bopts, tiles, samples, d_render_ptr, wsum_ptr, grads):
+        self.calls.append(("backward", tuple(tiles), tuple(samples)))
+        grads.tensors["d_points"][:] = 100.0 * (1 + self.rank)
+
+
+def _shard_worker(rank, world, port, out):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        from dvg import BackwardOptions, RenderOptions, synth
+        from dvg.abi import pack_scene
+        from dvg.shard import SceneShardStep
+
+        sc = synth.plain_scene(3, 32, 16, 3)
+        calls = []
+        fake = _FakeShardScene(sc, pack_scene(sc), rank, calls)
+        opts = RenderOptions(samples_x=2, samples_y=2, seed=0, jitter=True, use_prefiltering=False)
+        step = SceneShardStep(fake, opts, BackwardOptions(boundary_samples=1001), rank, world, dist.all_reduce,
+                              device="cpu")
+        step.step(torch.zeros(32 * 16 * 4))
+        out.put((rank, calls, float(step.grads.tensors["d_points"][0]), float(step.image[0])))
+    finally:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def test_single_scene_split_over_two_gloo_ranks():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_shard_worker, args=(r, WORLD, port, q)) for r in range(WORLD)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in range(WORLD))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (r0, c0, g0, i0), (r1, c1, g1, i1) = res
+    # tiles 7 -> [0, 4) + [4, 7); boundary samples 1001 -> [0, 501) + [501, 1001)
+    assert c0[0] == ("forward", (0, 4)) and c1[0] == ("forward", (4, 7))
+    assert c0[-1] == ("backward", (0, 4), (0, 501)) and c1[-1] == ("backward", (4, 7), (501, 1001))
+    # the accumulators were summed before the resolve, the gradients after the backward
+    assert c0[1] == c1[1] == ("resolve", 3.0, 30.0)
+    assert [c[0] for c in c0] == ["forward", "resolve", "l2", "backward"]
+    assert g0 == g1 == 300.0 and i0 == i1 == 3.0
