@@ -640,6 +640,7 @@ static dvg_status backward_core(dvg_context* ctx, dvg_scene* sc, const dvg_rende
             bp.sample_base = shard ? std::min<uint64_t>(shard->sample_begin, total) : 0;
             bp.num_samples = shard ? std::min<uint64_t>(std::max(shard->sample_end, shard->sample_begin), total) : total;
             bp.slot_base = bp.sample_base;
+            bp.pdf_scale = (float)((double)total / (double)((uint64_t)npix * sp.sxn * sp.syn));
             bp.seed = (bopts && !bopts->boundary_seed_from_options) ? bopts->boundary_seed : opts->seed;
             bp.rng = bopts ? (int)bopts->rng : 0;
             bp.cell = (int)sc->tune.boundary_cell;
@@ -1248,6 +1249,7 @@ extern "C" dvg_status dvg_batch_create(dvg_context* ctx, dvg_scene* const* scene
         e.b_off = b->total_bsamples;
         e.bseed = b->bopts.boundary_seed_from_options ? opts->seed : b->bopts.boundary_seed;
         e.rng = (int)b->bopts.rng;
+        e.bscale = (float)((double)e.nb / (double)((uint64_t)npix * spp));
         const int items = tiles * (int)spp;
         for (int k = 0; k < items; ++k) item_scene.push_back((int)i);
         b->items += items;

@@ -570,6 +570,285 @@ __device__ __forceinline__ float2 nrm2(float2 v) {
     float l = len2(v.x, v.y);
     return l == 0.0f ? make_float2(0.0f, 0.0f) : make_float2(v.x / l, v.y / l);
 }
+// Join and cap edges of a stroke with non-round joins or caps (the polygons
+// join_cap_hit tests), sampled as part of its boundary: uniform over the sites (the
+// non-round joins, and for open paths with non-round caps the two ends), then by
+// length along the site's edges.  Like the crate's offset-curve samples, a point
+// moves with its centreline point (the vertex): data->point_id is the vertex's path
+// point, data->t the radius derivative (p - v) . n / r (every site polygon scales
+// about v with the radius), and base_point_id = -1 marks the sample.
+__device__ float2 sample_join_cap(const DevScene& S, int path, float t, float2* normal, float* pdf, BData* data) {
+    const int4 pi = __ldg(&S.p_info[2 * path]);
+    const int4 pi2 = __ldg(&S.p_info[2 * path + 1]);
+    const bool closed = pi2.w & PF_CLOSED;
+    const int join = (pi2.w >> PF_JOIN_SHIFT) & 3, cap = (pi2.w >> PF_CAP_SHIFT) & 3;
+    const int off = pi.x, n = pi.y;
+    const int nj = join != JOIN_ROUND ? (closed ? n : n - 1) : 0;
+    const int ncap = !closed && cap != CAP_ROUND ? 2 : 0;
+    const int sites = nj + ncap;
+    if (n <= 0 || sites <= 0) {
+        *pdf = 0.0f;
+        return make_float2(0, 0);
+    }
+    int k = (int)(t * (float)sites);
+    if (k > sites - 1) k = sites - 1;
+    const float u = t * (float)sites - (float)k;
+    *pdf /= (float)sites;
+    float2 e[4], v;
+    int ne = 0, pid = 0;
+    float r = 0.0f;
+    float2 capdir = make_float2(0, 0);
+    if (k < nj) {
+        const int vb = closed ? k : k + 1, va = vb > 0 ? vb - 1 : n - 1;
+        const float4 a0 = __ldg(&S.seg_p[2 * (off + va)]), a1 = __ldg(&S.seg_p[2 * (off + va) + 1]);
+        const float4 b0 = __ldg(&S.seg_p[2 * (off + vb)]), b1 = __ldg(&S.seg_p[2 * (off + vb) + 1]);
+        v = make_float2(b0.x, b0.y);
+        r = __ldg(&S.seg_r[off + vb]).x;
+        pid = __ldg(&S.seg_meta[off + vb]).z;
+        float2 din = seg_dir1(a0, a1), dout = seg_dir0(b0, b1);
+        const float li = sqrtf(din.x * din.x + din.y * din.y), lo = sqrtf(dout.x * dout.x + dout.y * dout.y);
+        if (!(li > 0.0f) || !(lo > 0.0f) || !(r > 0.0f)) {
+            *pdf = 0.0f;
+            return make_float2(0, 0);
+        }
+        din = make_float2(din.x / li, din.y / li);
+        dout = make_float2(dout.x / lo, dout.y / lo);
+        const float cr = cross2f(din.x, din.y, dout.x, dout.y);
+        if (fabsf(cr) < 1.0e-6f) {  // no outer corner: no edge here
+            *pdf = 0.0f;
+            return make_float2(0, 0);
+        }
+        const float sg = cr > 0.0f ? 1.0f : -1.0f;
+        e[0] = make_float2(v.x + r * sg * din.y, v.y - r * sg * din.x);
+        const float2 b = make_float2(v.x + r * sg * dout.y, v.y - r * sg * dout.x);
+        ne = 1;
+        if (join == JOIN_MITER) {
+            const float sm = cross2f(b.x - e[0].x, b.y - e[0].y, dout.x, dout.y) / cr;
+            const float2 m = make_float2(e[0].x + sm * din.x, e[0].y + sm * din.y);
+            const float ml = sqrtf((m.x - v.x) * (m.x - v.x) + (m.y - v.y) * (m.y - v.y));
+            if (ml <= __ldg(&S.p_miter[path]) * r) e[ne++] = m;
+        }
+        e[ne] = b;
+    } else {
+        const bool start = k == nj;
+        const int sidx = start ? 0 : n - 1;
+        const float4 q0 = __ldg(&S.seg_p[2 * (off + sidx)]), q1 = __ldg(&S.seg_p[2 * (off + sidx) + 1]);
+        float2 d;
+        if (start) {
+            const float2 d0 = seg_dir0(q0, q1);
+            d = make_float2(-d0.x, -d0.y);
+            v = make_float2(q0.x, q0.y);
+            r = __ldg(&S.seg_r[off]).x;
+            pid = __ldg(&S.seg_meta[off]).z;
+        } else {
+            d = seg_dir1(q0, q1);
+            v = make_float2(q1.z, q1.w);
+            r = __ldg(&S.seg_r[off + n - 1]).w;
+            pid = pi2.y - 1;
+        }
+        const float l = sqrtf(d.x * d.x + d.y * d.y);
+        if (!(l > 0.0f) || !(r > 0.0f)) {
+            *pdf = 0.0f;
+            return make_float2(0, 0);
+        }
+        d = make_float2(d.x / l, d.y / l);
+        capdir = d;
+        const float2 np = make_float2(-d.y, d.x);
+        e[0] = make_float2(v.x - r * np.x, v.y - r * np.y);
+        if (cap == CAP_SQUARE) {
+            e[1] = make_float2(e[0].x + r * d.x, e[0].y + r * d.y);
+            e[2] = make_float2(v.x + r * np.x + r * d.x, v.y + r * np.y + r * d.y);
+            e[3] = make_float2(v.x + r * np.x, v.y + r * np.y);
+            ne = 3;
+        } else {
+            e[1] = make_float2(v.x + r * np.x, v.y + r * np.y);
+            ne = 1;
+        }
+    }
+    float len[3], total = 0.0f;
+    for (int i = 0; i < ne; ++i) {
+        len[i] = len2(e[i + 1].x - e[i].x, e[i + 1].y - e[i].y);
+        total += len[i];
+    }
+    if (!(total > 0.0f)) {
+        *pdf = 0.0f;
+        return make_float2(0, 0);
+    }
+    float sl = u * total;
+    int i = 0;
+    while (i < ne - 1 && sl > len[i]) sl -= len[i++];
+    const float f = len[i] > 0.0f ? fminf(sl / len[i], 1.0f) : 0.0f;
+    const float2 p = make_float2(e[i].x + f * (e[i + 1].x - e[i].x), e[i].y + f * (e[i + 1].y - e[i].y));
+    float2 nn = nrm2(make_float2(-(e[i + 1].y - e[i].y), e[i + 1].x - e[i].x));
+    const float mx = 0.5f * (e[i].x + e[i + 1].x) - v.x, my = 0.5f * (e[i].y + e[i + 1].y) - v.y;
+    const float side = (mx == 0.0f && my == 0.0f) ? nn.x * capdir.x + nn.y * capdir.y : nn.x * mx + nn.y * my;
+    if (side < 0.0f) nn = make_float2(-nn.x, -nn.y);
+    *pdf /= total;
+    *normal = nn;
+    (void)pid;
+    data->base_point_id = -1 - k;  // the site
+    data->point_id = i;            // the edge of the site's polygon
+    data->t = f;                   // the position along that edge
+    return p;
+}
+
+// Forward-mode derivative of a join / cap site's polygon with respect to its vertex
+// v, the control points that set the adjacent tangents (qa before, qb after the
+// vertex) and the radius: 7 partials (v.x, v.y, qa.x, qa.y, qb.x, qb.y, r).
+struct Dl {
+    float v;
+    float d[7];
+};
+__device__ __forceinline__ Dl dl_const(float v) {
+    Dl r;
+    r.v = v;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) r.d[k] = 0.0f;
+    return r;
+}
+__device__ __forceinline__ Dl dl_var(float v, int k) {
+    Dl r = dl_const(v);
+    r.d[k] = 1.0f;
+    return r;
+}
+__device__ __forceinline__ Dl operator+(const Dl& a, const Dl& b) {
+    Dl r;
+    r.v = a.v + b.v;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) r.d[k] = a.d[k] + b.d[k];
+    return r;
+}
+__device__ __forceinline__ Dl operator-(const Dl& a, const Dl& b) {
+    Dl r;
+    r.v = a.v - b.v;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) r.d[k] = a.d[k] - b.d[k];
+    return r;
+}
+__device__ __forceinline__ Dl operator*(const Dl& a, const Dl& b) {
+    Dl r;
+    r.v = a.v * b.v;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) r.d[k] = a.d[k] * b.v + a.v * b.d[k];
+    return r;
+}
+__device__ __forceinline__ Dl operator/(const Dl& a, const Dl& b) {
+    Dl r;
+    r.v = a.v / b.v;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) r.d[k] = (a.d[k] - r.v * b.d[k]) / b.v;
+    return r;
+}
+__device__ __forceinline__ Dl dl_sqrt(const Dl& a) {
+    Dl r;
+    r.v = sqrtf(a.v);
+#pragma unroll
+    for (int k = 0; k < 7; ++k) r.d[k] = r.v > 0.0f ? a.d[k] * (0.5f / r.v) : 0.0f;
+    return r;
+}
+struct DV {
+    Dl x, y;
+};
+__device__ __forceinline__ DV dv_add(const DV& a, const DV& b) { return DV{a.x + b.x, a.y + b.y}; }
+__device__ __forceinline__ DV dv_sub(const DV& a, const DV& b) { return DV{a.x - b.x, a.y - b.y}; }
+__device__ __forceinline__ DV dv_scale(const DV& a, const Dl& s) { return DV{a.x * s, a.y * s}; }
+__device__ __forceinline__ DV dv_unit(const DV& a) {
+    const Dl l = dl_sqrt(a.x * a.x + a.y * a.y);
+    return DV{a.x / l, a.y / l};
+}
+// Slot of the control point that seg_dir0 / seg_dir1 take (the vertex is slot 0 / 3).
+__device__ __forceinline__ int seg_dir0_slot(float4 a, float4 b) {
+    if (!(a.z - a.x == 0.0f && a.w - a.y == 0.0f)) return 1;
+    return !(b.x - a.x == 0.0f && b.y - a.y == 0.0f) ? 2 : 3;
+}
+__device__ __forceinline__ int seg_dir1_slot(float4 a, float4 b) {
+    if (!(b.z - b.x == 0.0f && b.w - b.y == 0.0f)) return 2;
+    return !(b.z - a.z == 0.0f && b.w - a.w == 0.0f) ? 1 : 0;
+}
+__device__ __forceinline__ float2 seg_slot(float4 a, float4 b, int j) {
+    return j == 0 ? make_float2(a.x, a.y) : j == 1 ? make_float2(a.z, a.w) : j == 2 ? make_float2(b.x, b.y)
+                                                                                 : make_float2(b.z, b.w);
+}
+// Path point of slot j of a segment (lines and quadratics repeat their last point).
+__device__ __forceinline__ int seg_slot_point(int4 meta, int j, bool closed, int pc) {
+    const int idx = meta.z + (j < meta.x + 1 ? j : meta.x + 1);
+    return closed ? idx % pc : idx;
+}
+// Normal velocity of the join / cap edge point sampled at (site, edge, f):
+// w[k] = dp/dtheta_k . n for theta = (v, qa, qb, r); ids = path points of v, qa, qb
+// (-1: not used).  Out of line: it runs only for those samples.
+static __device__ __noinline__ bool join_cap_velocity(const int4* p_info, const float* p_miter, const float4* seg_p,
+                                                     const float4* seg_r, const int4* seg_meta, int path, int site,
+                                                     int edge, float f, float nx, float ny, float* w, int* ids) {
+    const int4 pi = __ldg(&p_info[2 * path]);
+    const int4 pi2 = __ldg(&p_info[2 * path + 1]);
+    const bool closed = pi2.w & PF_CLOSED;
+    const int join = (pi2.w >> PF_JOIN_SHIFT) & 3, cap = (pi2.w >> PF_CAP_SHIFT) & 3;
+    const int off = pi.x, nseg = pi.y, pc = pi2.y;
+    const int nj = join != JOIN_ROUND ? (closed ? nseg : nseg - 1) : 0;
+    ids[0] = ids[1] = ids[2] = -1;
+    DV e[4];
+    int ne = 0;
+    if (site < nj) {
+        const int vb = closed ? site : site + 1, va = vb > 0 ? vb - 1 : nseg - 1;
+        const float4 a0 = __ldg(&seg_p[2 * (off + va)]), a1 = __ldg(&seg_p[2 * (off + va) + 1]);
+        const float4 b0 = __ldg(&seg_p[2 * (off + vb)]), b1 = __ldg(&seg_p[2 * (off + vb) + 1]);
+        const int sa = seg_dir1_slot(a0, a1), sb = seg_dir0_slot(b0, b1);
+        const float2 v = make_float2(b0.x, b0.y), qa = seg_slot(a0, a1, sa), qb = seg_slot(b0, b1, sb);
+        const int4 ma = __ldg(&seg_meta[off + va]), mb = __ldg(&seg_meta[off + vb]);
+        ids[0] = mb.z;
+        ids[1] = seg_slot_point(ma, sa, closed, pc);
+        ids[2] = seg_slot_point(mb, sb, closed, pc);
+        const DV V{dl_var(v.x, 0), dl_var(v.y, 1)}, QA{dl_var(qa.x, 2), dl_var(qa.y, 3)},
+            QB{dl_var(qb.x, 4), dl_var(qb.y, 5)};
+        const Dl R = dl_var(__ldg(&seg_r[off + vb]).x, 6);
+        const DV din = dv_unit(dv_sub(V, QA)), dout = dv_unit(dv_sub(QB, V));
+        const Dl cr = din.x * dout.y - din.y * dout.x;
+        if (fabsf(cr.v) < 1.0e-6f) return false;
+        const Dl sg = dl_const(cr.v > 0.0f ? 1.0f : -1.0f);
+        e[0] = DV{V.x + R * sg * din.y, V.y - R * sg * din.x};
+        const DV b{V.x + R * sg * dout.y, V.y - R * sg * dout.x};
+        ne = 1;
+        if (join == JOIN_MITER) {
+            const Dl sm = ((b.x - e[0].x) * dout.y - (b.y - e[0].y) * dout.x) / cr;
+            const DV m = dv_add(e[0], dv_scale(din, sm));
+            const float ml = sqrtf((m.x.v - v.x) * (m.x.v - v.x) + (m.y.v - v.y) * (m.y.v - v.y));
+            if (ml <= __ldg(&p_miter[path]) * R.v) e[ne++] = m;
+        }
+        e[ne] = b;
+    } else {
+        const bool start = site == nj;
+        const int si = start ? 0 : nseg - 1;
+        const float4 q0 = __ldg(&seg_p[2 * (off + si)]), q1 = __ldg(&seg_p[2 * (off + si) + 1]);
+        const int sq = start ? seg_dir0_slot(q0, q1) : seg_dir1_slot(q0, q1);
+        const float2 v = start ? make_float2(q0.x, q0.y) : make_float2(q1.z, q1.w), q = seg_slot(q0, q1, sq);
+        const int4 m = __ldg(&seg_meta[off + si]);
+        ids[0] = start ? m.z : pc - 1;
+        ids[start ? 2 : 1] = seg_slot_point(m, sq, closed, pc);
+        const DV V{dl_var(v.x, 0), dl_var(v.y, 1)};
+        const DV Q = start ? DV{dl_var(q.x, 4), dl_var(q.y, 5)} : DV{dl_var(q.x, 2), dl_var(q.y, 3)};
+        const float4 rr = __ldg(&seg_r[off + si]);
+        const Dl R = dl_var(start ? rr.x : rr.w, 6);
+        const DV d = dv_unit(dv_sub(V, Q));  // outward along the end
+        const DV np{dl_const(0.0f) - d.y, d.x};
+        e[0] = dv_sub(V, dv_scale(np, R));
+        if (cap == CAP_SQUARE) {
+            e[1] = dv_add(e[0], dv_scale(d, R));
+            e[2] = dv_add(dv_add(V, dv_scale(np, R)), dv_scale(d, R));
+            e[3] = dv_add(V, dv_scale(np, R));
+            ne = 3;
+        } else {
+            e[1] = dv_add(V, dv_scale(np, R));
+            ne = 1;
+        }
+    }
+    if (edge >= ne) return false;
+    const DV p = dv_add(e[edge], dv_scale(dv_sub(e[edge + 1], e[edge]), dl_const(f)));
+#pragma unroll
+    for (int k = 0; k < 7; ++k) w[k] = p.x.d[k] * nx + p.y.d[k] * ny;
+    return true;
+}
+
 // sample_boundary_path (boundary.rs:630-842)
 __device__ float2 sample_boundary_path(const DevScene& S, int shape, float path_len, float t, float2* normal,
                                        float* pdf, BData* data, float dir, float srad) {
@@ -584,7 +863,17 @@ __device__ float2 sample_boundary_path(const DevScene& S, int shape, float path_
         *pdf = 0.0f;
         return make_float2(0, 0);
     }
-    if (dir != 0.0f && !closed) {
+    const bool styled = dir != 0.0f && (pi2.w & PF_STYLED);
+    if (styled) {  // a share of the samples on the join / cap edges (both sides draw them)
+        const float q = JOIN_CAP_SHARE;
+        if (t < q) {
+            *pdf *= 2.0f * q;
+            return sample_join_cap(S, path, t / q, normal, pdf, data);
+        }
+        t = (t - q) / (1.0f - q);
+        *pdf *= 1.0f - q;
+    }
+    if (dir != 0.0f && !closed && (!styled || ((pi2.w >> PF_CAP_SHIFT) & 3) == CAP_ROUND)) {
         float cap = 0.0f;
         if (thick)
             cap = PI_F * (S.thickness[po] + S.thickness[po + pc - 1]);
@@ -808,11 +1097,26 @@ __device__ void accumulate_boundary(const DevScene& S, const GradPtrs& G, int sh
     }
     const bool closed = pflags & PF_CLOSED;
     int nc = 0;  // num_control_points.get(base_point_id).unwrap_or(0)
-    if (si.x == K_PATH) {
+    if (si.x == K_PATH && bd.base_point_id >= 0) {
         int ctrl_count = __ldg(&S.path_cdf_info[shape].y);
         nc = bd.base_point_id < ctrl_count ? S.ncp[co + bd.base_point_id] : 0;
     }
-    if (bd.is_stroke) {
+    if (bd.base_point_id < 0) {  // a join / cap edge sample: the exact normal velocity
+        float w[7];
+        int ids[3];
+        if (join_cap_velocity(S.p_info, S.p_miter, S.seg_p, S.seg_r, S.seg_meta, si.z, -1 - bd.base_point_id,
+                              bd.point_id, bd.t, n.x, n.y, w, ids)) {
+            for (int j = 0; j < 3; ++j)
+                if (ids[j] >= 0) {
+                    add_if(G.d_points + 2 * (po + ids[j]), w[2 * j] * contrib);
+                    add_if(G.d_points + 2 * (po + ids[j]) + 1, w[2 * j + 1] * contrib);
+                }
+            if (pflags & PF_THICK)
+                add_if(G.d_thickness + po + ids[0], w[6] * contrib);
+            else
+                add_if(G.d_shape_stroke_width + shape, w[6] * contrib);
+        }
+    } else if (bd.is_stroke) {
         if (si.x == K_PATH && (pflags & PF_THICK)) {
             float t2 = bd.t, tt = 1.0f - t2;
             int pid = bd.point_id;
@@ -847,7 +1151,7 @@ __device__ void accumulate_boundary(const DevScene& S, const GradPtrs& G, int sh
         float ang = 2.0f * PI_F * t;
         add_if(dp + 2, dvg_cosf(ang) * n.x * contrib);
         add_if(dp + 3, dvg_sinf(ang) * n.y * contrib);
-    } else if (si.x == K_PATH) {
+    } else if (si.x == K_PATH && bd.base_point_id >= 0) {
         float t2 = bd.t, tt = 1.0f - t2;
         int pid = bd.point_id;
         auto addp = [&](long idx, float w) {
@@ -908,8 +1212,8 @@ __device__ void accumulate_boundary(const DevScene& S, const GradPtrs& G, int sh
 // Boundary pass, stage 1: draw every edge sample (boundary.rs:141-175), keep
 // the valid ones with the tile of their boundary pixel as sort key.
 __device__ __forceinline__ void boundary_gen_one(const DevScene& S, uint64_t idx, uint64_t slot, uint32_t seed,
-                                                 int rng_kind, int tile_off, int scene, int cell, BSample* out,
-                                                 int* key, int* tile_counts) {
+                                                 int rng_kind, int tile_off, int scene, int cell, float pdf_scale,
+                                                 BSample* out, int* key, int* tile_counts) {
     key[slot] = -1;
     float u, t;
     if (rng_kind == 1) {
@@ -945,7 +1249,7 @@ __device__ __forceinline__ void boundary_gen_one(const DevScene& S, uint64_t idx
     const float W = (float)S.width, H = (float)S.height;
     bpt.x /= W;
     bpt.y /= H;
-    const float pdf = pmf * bpdf;
+    const float pdf = pmf * bpdf * pdf_scale;
     if (pdf <= 0.0f) return;
     const int bx = f2i(bpt.x * W), by = f2i(bpt.y * H);
     if (bx < 0 || bx >= S.width || by < 0 || by >= S.height) return;
@@ -979,7 +1283,8 @@ __global__ void __launch_bounds__(256) k_boundary_gen(DevScene S, BoundaryParams
                                                       int* tile_counts) {
     const uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + bp.sample_base;
     if (idx >= bp.num_samples) return;
-    boundary_gen_one(S, idx, idx - bp.slot_base, bp.seed, bp.rng, 0, 0, bp.cell, out, key, tile_counts);
+    boundary_gen_one(S, idx, idx - bp.slot_base, bp.seed, bp.rng, 0, 0, bp.cell, bp.pdf_scale, out, key,
+                     tile_counts);
 }
 // Batched stage 1: one flat index over all scenes' boundary samples; the scene is
 // found by binary search over the per-scene sample offsets.
@@ -999,7 +1304,7 @@ __global__ void __launch_bounds__(256) k_boundary_gen_batch(const BatchEntry* __
     const BatchEntry& E = B[lo];
     key[g] = -1;
     if (!E.S.boundary_ok || g - E.b_off >= E.nb) return;
-    boundary_gen_one(E.S, g - E.b_off, g, E.bseed, E.rng, E.tile_off, lo, cell, out, key, tile_counts);
+    boundary_gen_one(E.S, g - E.b_off, g, E.bseed, E.rng, E.tile_off, lo, cell, E.bscale, out, key, tile_counts);
 }
 // Stage 2: counting-sort scatter of sample slots by tile.
 __global__ void k_boundary_scatter(const int* key, uint64_t n, int* cursor, int* order) {

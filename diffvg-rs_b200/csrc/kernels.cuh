@@ -28,6 +28,8 @@ inline int bnd_buckets(int cell) { return (16 / cell) * (16 / cell); }
 // a warp's lanes touch consecutive halves; a count of FRAG_NONE marks a sample the
 // interior re-tests (more fragments than slots, a longer tile list, or a sample
 // point that the interior's normalise-and-rescale does not reproduce exactly).
+// Share of a styled stroke's edge samples drawn on its join and cap edges.
+constexpr float JOIN_CAP_SHARE = 0.25f;
 constexpr int FRAG_MAX_ENTRIES = 32767;
 constexpr uint8_t FRAG_NONE = 0xff;
 constexpr int FRAG_MAX_SLOTS = 64;
@@ -58,6 +60,9 @@ struct BoundaryParams {
     uint32_t seed;
     int rng;   // 0 PCG32, 1 Philox
     int cell;  // boundary sort cell edge in pixels (2, 4, 8 or 16)
+    // the step's boundary samples / (W*H*spp): the crate draws W*H*spp samples and its
+    // edge term carries no 1/N, so another count rescales each sample's pdf (1: exact)
+    float pdf_scale;
 };
 // One drawn edge sample (64 bytes), kept in scratch between the boundary stages.
 struct BSample {
@@ -88,6 +93,7 @@ struct BatchEntry {
     uint64_t nb;     // boundary samples of this scene
     uint32_t bseed;
     int rng;
+    float bscale;  // nb / (W*H*spp), as BoundaryParams::pdf_scale
 };
 
 // Per-scene state of the on-device optimisation step (Adam + scene re-preparation).

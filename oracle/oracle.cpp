@@ -2929,16 +2929,301 @@ struct BData {
     size_t base_point_id = 0, point_id = 0;
     float t = 0.0f;
     bool is_stroke = false;
+    bool join_cap = false;  // a join / cap edge sample (extension): t = (p - v) . n / r
 };
+// Share of a styled stroke's edge samples on its join and cap edges (extension).
+const float kJoinCapShare = 0.25f;
+static float len2f(float x, float y) { return std::sqrt(x * x + y * y); }
+// The join and cap edges of a stroke with non-round joins or caps: the same sites,
+// order and arithmetic as the library's kernel (sample_join_cap).
+static V2 sample_join_cap(const Shape& s, float t, V2* normal, float* pdf, BData* data) {
+    const PathG& path = s.path;
+    const std::vector<SegData> segs = path_segments(s, s.stroke_width);
+    const bool closed = path.closed;
+    const int n = (int)segs.size();
+    const int nj = s.join != DVG_JOIN_ROUND ? (closed ? n : n - 1) : 0;
+    const int ncap = !closed && s.cap != DVG_CAP_ROUND ? 2 : 0;
+    const int sites = nj + ncap;
+    if (n <= 0 || sites <= 0) {
+        *pdf = 0.0f;
+        return mk(0, 0);
+    }
+    std::vector<size_t> seg_pid(n);
+    for (int i = 0, pid = 0; i < n; ++i) {
+        seg_pid[i] = (size_t)pid;
+        pid += path.ncp[i] + 1;
+    }
+    int k = (int)(t * (float)sites);
+    if (k > sites - 1) k = sites - 1;
+    const float u = t * (float)sites - (float)k;
+    *pdf /= (float)sites;
+    V2 e[4], v = mk(0, 0), capdir = mk(0, 0);
+    int ne = 0;
+    size_t pid = 0;
+    float r = 0.0f;
+    if (k < nj) {
+        const int vb = closed ? k : k + 1, va = vb > 0 ? vb - 1 : n - 1;
+        v = segs[vb].p0;
+        r = segs[vb].r0;
+        pid = seg_pid[vb];
+        V2 din = seg_dir1(segs[va]), dout = seg_dir0(segs[vb]);
+        const float li = std::sqrt(din.x * din.x + din.y * din.y), lo = std::sqrt(dout.x * dout.x + dout.y * dout.y);
+        if (!(li > 0.0f) || !(lo > 0.0f) || !(r > 0.0f)) {
+            *pdf = 0.0f;
+            return mk(0, 0);
+        }
+        din = mk(din.x / li, din.y / li);
+        dout = mk(dout.x / lo, dout.y / lo);
+        const float cr = cross2f(din.x, din.y, dout.x, dout.y);
+        if (std::fabs(cr) < 1.0e-6f) {
+            *pdf = 0.0f;
+            return mk(0, 0);
+        }
+        const float sg = cr > 0.0f ? 1.0f : -1.0f;
+        e[0] = mk(v.x + r * sg * din.y, v.y - r * sg * din.x);
+        const V2 b = mk(v.x + r * sg * dout.y, v.y - r * sg * dout.x);
+        ne = 1;
+        if (s.join == DVG_JOIN_MITER) {
+            const float sm = cross2f(b.x - e[0].x, b.y - e[0].y, dout.x, dout.y) / cr;
+            const V2 m = mk(e[0].x + sm * din.x, e[0].y + sm * din.y);
+            const float ml = std::sqrt((m.x - v.x) * (m.x - v.x) + (m.y - v.y) * (m.y - v.y));
+            if (ml <= std::fmax(s.miter, 1.0f) * r) e[ne++] = m;
+        }
+        e[ne] = b;
+    } else {
+        const bool start = k == nj;
+        const SegData& g = segs[start ? 0 : n - 1];
+        V2 d;
+        if (start) {
+            const V2 d0 = seg_dir0(g);
+            d = mk(-d0.x, -d0.y);
+            v = g.p0;
+            r = g.r0;
+            pid = seg_pid[0];
+        } else {
+            d = seg_dir1(g);
+            v = g.p3;
+            r = g.r3;
+            pid = path.pts.size() - 1;
+        }
+        const float l = std::sqrt(d.x * d.x + d.y * d.y);
+        if (!(l > 0.0f) || !(r > 0.0f)) {
+            *pdf = 0.0f;
+            return mk(0, 0);
+        }
+        d = mk(d.x / l, d.y / l);
+        capdir = d;
+        const V2 np = mk(-d.y, d.x);
+        e[0] = mk(v.x - r * np.x, v.y - r * np.y);
+        if (s.cap == DVG_CAP_SQUARE) {
+            e[1] = mk(e[0].x + r * d.x, e[0].y + r * d.y);
+            e[2] = mk(v.x + r * np.x + r * d.x, v.y + r * np.y + r * d.y);
+            e[3] = mk(v.x + r * np.x, v.y + r * np.y);
+            ne = 3;
+        } else {
+            e[1] = mk(v.x + r * np.x, v.y + r * np.y);
+            ne = 1;
+        }
+    }
+    float len[3], total = 0.0f;
+    for (int i = 0; i < ne; ++i) {
+        len[i] = len2f(e[i + 1].x - e[i].x, e[i + 1].y - e[i].y);
+        total += len[i];
+    }
+    if (!(total > 0.0f)) {
+        *pdf = 0.0f;
+        return mk(0, 0);
+    }
+    float sl = u * total;
+    int i = 0;
+    while (i < ne - 1 && sl > len[i]) sl -= len[i++];
+    const float f = len[i] > 0.0f ? std::fmin(sl / len[i], 1.0f) : 0.0f;
+    const V2 p = mk(e[i].x + f * (e[i + 1].x - e[i].x), e[i].y + f * (e[i + 1].y - e[i].y));
+    const float ex = -(e[i + 1].y - e[i].y), ey = e[i + 1].x - e[i].x, el = len2f(ex, ey);
+    V2 nn = el > 0.0f ? mk(ex / el, ey / el) : mk(0.0f, 0.0f);
+    const float mx = 0.5f * (e[i].x + e[i + 1].x) - v.x, my = 0.5f * (e[i].y + e[i + 1].y) - v.y;
+    const float side = (mx == 0.0f && my == 0.0f) ? nn.x * capdir.x + nn.y * capdir.y : nn.x * mx + nn.y * my;
+    if (side < 0.0f) nn = mk(-nn.x, -nn.y);
+    *pdf /= total;
+    *normal = nn;
+    (void)pid;
+    data->join_cap = true;
+    data->base_point_id = (size_t)k;  // the site
+    data->point_id = (size_t)i;       // the edge of the site's polygon
+    data->t = f;                      // the position along that edge
+    return p;
+}
+
+// Forward-mode derivative of a join / cap site's polygon with respect to its vertex
+// v, the control point q that sets the adjacent tangent(s) (qa before, qb after the
+// vertex) and the radius: 7 partials (v.x, v.y, qa.x, qa.y, qb.x, qb.y, r).
+struct Dl {
+    float v;
+    float d[7];
+};
+static Dl dl_const(float v) {
+    Dl r;
+    r.v = v;
+    for (float& x : r.d) x = 0.0f;
+    return r;
+}
+static Dl dl_var(float v, int k) {
+    Dl r = dl_const(v);
+    r.d[k] = 1.0f;
+    return r;
+}
+static Dl operator+(const Dl& a, const Dl& b) {
+    Dl r;
+    r.v = a.v + b.v;
+    for (int k = 0; k < 7; ++k) r.d[k] = a.d[k] + b.d[k];
+    return r;
+}
+static Dl operator-(const Dl& a, const Dl& b) {
+    Dl r;
+    r.v = a.v - b.v;
+    for (int k = 0; k < 7; ++k) r.d[k] = a.d[k] - b.d[k];
+    return r;
+}
+static Dl operator*(const Dl& a, const Dl& b) {
+    Dl r;
+    r.v = a.v * b.v;
+    for (int k = 0; k < 7; ++k) r.d[k] = a.d[k] * b.v + a.v * b.d[k];
+    return r;
+}
+static Dl operator/(const Dl& a, const Dl& b) {
+    Dl r;
+    r.v = a.v / b.v;
+    for (int k = 0; k < 7; ++k) r.d[k] = (a.d[k] - r.v * b.d[k]) / b.v;
+    return r;
+}
+static Dl dl_sqrt(const Dl& a) {
+    Dl r;
+    r.v = std::sqrt(a.v);
+    for (int k = 0; k < 7; ++k) r.d[k] = r.v > 0.0f ? a.d[k] * (0.5f / r.v) : 0.0f;
+    return r;
+}
+struct DV {
+    Dl x, y;
+};
+static DV dv_add(const DV& a, const DV& b) { return DV{a.x + b.x, a.y + b.y}; }
+static DV dv_sub(const DV& a, const DV& b) { return DV{a.x - b.x, a.y - b.y}; }
+static DV dv_scale(const DV& a, const Dl& s) { return DV{a.x * s, a.y * s}; }
+static DV dv_unit(const DV& a) {
+    const Dl l = dl_sqrt(a.x * a.x + a.y * a.y);
+    return DV{a.x / l, a.y / l};
+}
+// Point slot j of a path segment -> path point index (lines and quadratics repeat
+// their last point; closed paths wrap).
+static size_t seg_slot_point(const PathG& p, size_t pid, int nc, int j) {
+    size_t idx = pid + (size_t)std::min(j, nc + 1);
+    return p.closed ? idx % p.pts.size() : idx;
+}
+static int seg_dir0_slot(const SegData& g) {
+    V2 d = g.p1 - g.p0;
+    if (!(d.x == 0.0f && d.y == 0.0f)) return 1;
+    d = g.p2 - g.p0;
+    return !(d.x == 0.0f && d.y == 0.0f) ? 2 : 3;
+}
+static int seg_dir1_slot(const SegData& g) {
+    V2 d = g.p3 - g.p2;
+    if (!(d.x == 0.0f && d.y == 0.0f)) return 2;
+    d = g.p3 - g.p1;
+    return !(d.x == 0.0f && d.y == 0.0f) ? 1 : 0;
+}
+static V2 seg_slot(const SegData& g, int j) { return j == 0 ? g.p0 : j == 1 ? g.p1 : j == 2 ? g.p2 : g.p3; }
+// Normal velocity of the edge point sampled at (site, edge, f): w[k] = dp/dtheta_k . n
+// for theta = (v, qa, qb, r); ids = path points of v, qa, qb (-1: not used).
+static bool join_cap_velocity(const Shape& s, size_t site, size_t edge, float f, V2 n, float w[7], long ids[3]) {
+    const PathG& path = s.path;
+    const std::vector<SegData> segs = path_segments(s, s.stroke_width);
+    const bool closed = path.closed;
+    const int nseg = (int)segs.size();
+    const int nj = s.join != DVG_JOIN_ROUND ? (closed ? nseg : nseg - 1) : 0;
+    std::vector<size_t> seg_pid(nseg);
+    for (int i = 0, pid = 0; i < nseg; ++i) {
+        seg_pid[i] = (size_t)pid;
+        pid += path.ncp[i] + 1;
+    }
+    const int k = (int)site;
+    ids[0] = ids[1] = ids[2] = -1;
+    DV e[4];
+    int ne = 0;
+    if (k < nj) {
+        const int vb = closed ? k : k + 1, va = vb > 0 ? vb - 1 : nseg - 1;
+        const int sa = seg_dir1_slot(segs[va]), sb = seg_dir0_slot(segs[vb]);
+        const V2 v = segs[vb].p0, qa = seg_slot(segs[va], sa), qb = seg_slot(segs[vb], sb);
+        ids[0] = (long)seg_pid[vb];
+        ids[1] = (long)seg_slot_point(path, seg_pid[va], path.ncp[va], sa);
+        ids[2] = (long)seg_slot_point(path, seg_pid[vb], path.ncp[vb], sb);
+        const DV V{dl_var(v.x, 0), dl_var(v.y, 1)}, QA{dl_var(qa.x, 2), dl_var(qa.y, 3)},
+            QB{dl_var(qb.x, 4), dl_var(qb.y, 5)};
+        const Dl R = dl_var(segs[vb].r0, 6);
+        const DV din = dv_unit(dv_sub(V, QA)), dout = dv_unit(dv_sub(QB, V));
+        const Dl cr = din.x * dout.y - din.y * dout.x;
+        if (std::fabs(cr.v) < 1.0e-6f) return false;
+        const Dl sg = dl_const(cr.v > 0.0f ? 1.0f : -1.0f);
+        e[0] = DV{V.x + R * sg * din.y, V.y - R * sg * din.x};
+        const DV b{V.x + R * sg * dout.y, V.y - R * sg * dout.x};
+        ne = 1;
+        if (s.join == DVG_JOIN_MITER) {
+            const Dl sm = ((b.x - e[0].x) * dout.y - (b.y - e[0].y) * dout.x) / cr;
+            const DV m = dv_add(e[0], dv_scale(din, sm));
+            const float ml = std::sqrt((m.x.v - v.x) * (m.x.v - v.x) + (m.y.v - v.y) * (m.y.v - v.y));
+            if (ml <= std::fmax(s.miter, 1.0f) * R.v) e[ne++] = m;
+        }
+        e[ne] = b;
+    } else {
+        const bool start = k == nj;
+        const int si = start ? 0 : nseg - 1;
+        const SegData& g = segs[si];
+        const int sq = start ? seg_dir0_slot(g) : seg_dir1_slot(g);
+        const V2 v = start ? g.p0 : g.p3, q = seg_slot(g, sq);
+        ids[0] = (long)(start ? seg_pid[0] : path.pts.size() - 1);
+        ids[start ? 2 : 1] = (long)seg_slot_point(path, seg_pid[si], path.ncp[si], sq);
+        const DV V{dl_var(v.x, 0), dl_var(v.y, 1)};
+        const DV Q = start ? DV{dl_var(q.x, 4), dl_var(q.y, 5)} : DV{dl_var(q.x, 2), dl_var(q.y, 3)};
+        const Dl R = dl_var(start ? g.r0 : g.r3, 6);
+        const DV d = start ? dv_unit(dv_sub(V, Q)) : dv_unit(dv_sub(V, Q));  // outward along the end
+        const DV np{dl_const(0.0f) - d.y, d.x};
+        e[0] = dv_sub(V, dv_scale(np, R));
+        if (s.cap == DVG_CAP_SQUARE) {
+            e[1] = dv_add(e[0], dv_scale(d, R));
+            e[2] = dv_add(dv_add(V, dv_scale(np, R)), dv_scale(d, R));
+            e[3] = dv_add(V, dv_scale(np, R));
+            ne = 3;
+        } else {
+            e[1] = dv_add(V, dv_scale(np, R));
+            ne = 1;
+        }
+    }
+    if ((int)edge >= ne) return false;
+    const DV& a = e[edge];
+    const DV& b = e[edge + 1];
+    const Dl F = dl_const(f);
+    const DV p = dv_add(a, dv_scale(dv_sub(b, a), F));
+    for (int j = 0; j < 7; ++j) w[j] = p.x.d[j] * n.x + p.y.d[j] * n.y;
+    return true;
+}
 static V2 sample_boundary_path(const PathG& path, const PathCdf& pc, float path_len, float t, V2* normal, float* pdf,
-                               BData* data, float stroke_direction, float stroke_radius) {  // boundary.rs:630-842
+                               BData* data, float stroke_direction, float stroke_radius,
+                               const Shape* style) {  // boundary.rs:630-842
     size_t num_points = path.pts.size();
     size_t num_base = path.ncp.size();
     if (num_points == 0 || num_base == 0) {
         *pdf = 0.0f;
         return mk(0, 0);
     }
-    if (stroke_direction != 0.0f && !path.closed) {
+    const bool styled = stroke_direction != 0.0f && style && style_nonround(*style);
+    if (styled) {  // extension: a share of the samples on the join / cap edges (both sides draw them)
+        const float q = kJoinCapShare;
+        if (t < q) {
+            *pdf *= 2.0f * q;
+            return sample_join_cap(*style, t / q, normal, pdf, data);
+        }
+        t = (t - q) / (1.0f - q);
+        *pdf *= 1.0f - q;
+    }
+    if (stroke_direction != 0.0f && !path.closed && (!styled || style->cap == DVG_CAP_ROUND)) {
         float cap_length = 0.0f;
         if (path.has_thick) {
             if (!path.thick.empty()) cap_length = PI_F * (path.thick[0] + path.thick.back());
@@ -3186,7 +3471,7 @@ static bool sample_boundary_point(const Scene& sc, size_t shape_id, size_t group
         if (!pc || !pc->valid) return false;
         if (pc->length <= 0.0f) return false;
         pt = sample_boundary_path(s.path, *pc, shape_length, local_t, &normal, &pdf, data, stroke_direction,
-                                  s.stroke_width);
+                                  s.stroke_width, &s);
     } else {
         return false;
     }
@@ -3202,7 +3487,21 @@ static void accumulate_boundary_gradient(const Shape& s, size_t shape_id, float 
     if (!std::isfinite(contrib)) return;
     const PathG& path = s.path;
     size_t pbase = path.point_base;
-    if (bd.is_stroke) {
+    if (bd.join_cap) {  // extension: exact normal velocity of a join / cap edge point
+        float w[7];
+        long ids[3];
+        if (join_cap_velocity(s, bd.base_point_id, bd.point_id, bd.t, normal, w, ids)) {
+            for (int j = 0; j < 3; ++j)
+                if (ids[j] >= 0) {
+                    g.points[2 * (pbase + (size_t)ids[j])] += w[2 * j] * contrib;
+                    g.points[2 * (pbase + (size_t)ids[j]) + 1] += w[2 * j + 1] * contrib;
+                }
+            if (path.has_thick)
+                g.thickness[pbase + (size_t)ids[0]] += w[6] * contrib;
+            else
+                g.stroke_width[shape_id] += w[6] * contrib;
+        }
+    } else if (bd.is_stroke) {
         bool has_thick = s.kind == DVG_SHAPE_PATH && path.has_thick;
         if (has_thick) {
             size_t n = path.thick.size();
@@ -3246,7 +3545,7 @@ static void accumulate_boundary_gradient(const Shape& s, size_t shape_id, float 
         float angle = 2.0f * PI_F * t;
         dp[2] += std::cos(angle) * normal.x * contrib;
         dp[3] += std::sin(angle) * normal.y * contrib;
-    } else if (s.kind == DVG_SHAPE_PATH) {
+    } else if (s.kind == DVG_SHAPE_PATH && !bd.join_cap) {
         size_t np = path.pts.size();
         auto add_point = [&](size_t idx, float w) {
             size_t index = path.closed ? idx % np : idx;
@@ -3311,9 +3610,13 @@ static BoundaryTables build_boundary_tables(const Scene& sc) {
     return bt;
 }
 // One boundary sample (boundary.rs:141-196 + render_edge_sample 845-967).
+// pdf_scale: boundary samples drawn / W*H*spp.  The crate always draws W*H*spp and its
+// edge term carries no 1/N (the weight image and the normalised coordinates hold it),
+// so another sample count rescales every sample's pdf to keep the same expectation
+// (exactly 1 for the crate's count).
 static void boundary_sample(const Scene& sc, const SceneBvh& bvh, const BoundaryTables& bt, uint64_t idx,
                             uint32_t rng_kind, uint32_t seed, const float* d_render, const std::vector<float>& wimg,
-                            Grads& g, bool compute_translation) {
+                            Grads& g, bool compute_translation, float pdf_scale) {
     float u, t;
     boundary_rng(rng_kind, idx, seed, &u, &t);
     float dummy;
@@ -3340,7 +3643,7 @@ static void boundary_sample(const Scene& sc, const SceneBvh& bvh, const Boundary
     V2 normal_canvas = xform_normal(composite_inv, normal);
     bpt.x /= (float)sc.w;
     bpt.y /= (float)sc.h;
-    float pdf = shape_pmf * bpdf;
+    float pdf = shape_pmf * bpdf * pdf_scale;
     // render_edge_sample
     int width = (int)sc.w, height = (int)sc.h;
     if (width <= 0 || height <= 0) return;
@@ -3602,9 +3905,10 @@ extern "C" int oracle_render_backward_ex(const dvg_scene_desc* desc, const dvg_r
                 uint32_t rng = bopts ? bopts->rng : 0;
                 uint32_t seed = (bopts && !bopts->boundary_seed_from_options) ? bopts->boundary_seed : opts->seed;
                 uint64_t b = sample_begin, e = sample_end ? std::min<uint64_t>(sample_end, nb) : nb;
+                const float scale = (float)((double)nb / (double)total);
                 parallel_for(b, e, nthreads, [&](int t, uint64_t lo, uint64_t hi) {
                     for (uint64_t idx = lo; idx < hi; ++idx)
-                        boundary_sample(sc, bvh, bt, idx, rng, seed, d_render, wimg, tg[t], translation);
+                        boundary_sample(sc, bvh, bt, idx, rng, seed, d_render, wimg, tg[t], translation, scale);
                 });
             }
         }
@@ -4136,9 +4440,10 @@ extern "C" unsigned long long oracle_fwd_bwd_sample(const dvg_scene_desc* desc, 
         uint64_t bstride = bcount ? nb / bcount : 1;
         uint32_t rng = bopts ? bopts->rng : 0;
         uint32_t seed = (bopts && !bopts->boundary_seed_from_options) ? bopts->boundary_seed : opts->seed;
+        const float scale = (float)((double)nb / (double)total);
         parallel_for(0, bcount, nthreads, [&](int t, uint64_t lo, uint64_t hi) {
             for (uint64_t k = lo; k < hi; ++k)
-                boundary_sample(sc, bvh, bt, k * bstride, rng, seed, d_render, wimg, tg[t], false);
+                boundary_sample(sc, bvh, bt, k * bstride, rng, seed, d_render, wimg, tg[t], false, scale);
         });
     }
     auto t2 = now();

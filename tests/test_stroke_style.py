@@ -99,3 +99,93 @@ def test_round_style_is_the_crate_test():
     sc = _scene(L_PTS, False, J.ROUND, C_.ROUND)
     for pt, want in (((-0.7, 0.7), True), ((-0.75, 0.75), False), ((10.7, -0.7), True), ((10.75, -0.75), False)):
         assert _within(sc, pt) == want, pt
+
+
+# ---- the edge-sampling term of styled strokes (join and cap outline edges)
+def _quad_scene(pts, join, radius=2.0):
+    from dvg import Filter, FilterType
+
+    sc = Scene(40, 40)
+    sc.background = Color(1.0, 1.0, 1.0, 1.0)
+    sc.filter = Filter(FilterType.BOX, 0.5)
+    sh = Shape(PathGeometry(Path([0] * len(pts), [tuple(map(float, p)) for p in pts], None, True, False)))
+    sh.stroke_width = radius
+    sh.stroke_join, sh.stroke_miter_limit = join, 6.0
+    sc.shapes.append(sh)
+    sc.groups.append(ShapeGroup([0], None, Color(0.1, 0.2, 0.8, 1.0)))
+    return sc
+
+
+def _edge_grads(sc, n_samples, seeds, base=100):
+    """Mean and standard error over seeds of the edge term alone (interior pass off),
+    with d_render = 1 on the colour channels (the loss is the summed colour)."""
+    import os
+
+    import numpy as np
+
+    from dvg import BackwardOptions, RenderOptions
+
+    w = np.ones((sc.height, sc.width, 4), np.float32)
+    w[..., 3] = 0.0
+    opts = RenderOptions(samples_x=2, samples_y=2, seed=1, jitter=True, use_prefiltering=False)
+    pts, rad = [], []
+    for s in range(seeds):
+        _, b = orc.render_backward(sc, opts, BackwardOptions(boundary_samples=n_samples, boundary_seed=base + s), w,
+                                   passes=2, threads=os.cpu_count() or 1)
+        pts.append(np.asarray(b["d_points"], np.float64).copy())
+        rad.append(float(b["d_shape_stroke_width"][0]))
+    pts, rad = np.stack(pts), np.asarray(rad)
+    return pts.mean(0), rad.mean(), rad.std(ddof=1) / np.sqrt(seeds)
+
+
+DELTA = (0.1 - 1.0) + (0.2 - 1.0) + (0.8 - 1.0)  # colour minus white background, summed
+
+
+@pytest.mark.parametrize("join", [J.BEVEL, J.MITER])
+def test_join_edges_give_the_exact_radius_gradient(join):
+    # square of side L around its centreline, radius r: stroke area 8 L r - 2 r^2 (bevel), 8 L r (miter)
+    L, r, c = 16.0, 2.0, 12.3
+    sc = _quad_scene([(c, c), (c + L, c), (c + L, c + L), (c, c + L)], join, r)
+    _, g, se = _edge_grads(sc, 100000, 12)
+    exact = DELTA * (8 * L - 4 * r if join == J.BEVEL else 8 * L)
+    assert abs(g - exact) <= 0.005 * abs(exact) + 4 * se, (g, exact, se)
+
+
+def test_mitred_vertex_gradients_match_the_area_derivative():
+    import numpy as np
+
+    r = 2.0
+    P = np.array([(11.3, 12.1), (28.4, 10.7), (29.2, 27.9), (12.6, 26.8)], np.float64)
+
+    def offset_area(Q, s):  # mitred offset polygon (every join within the limit here)
+        out = []
+        for i in range(len(Q)):
+            a, v, b = Q[i - 1], Q[i], Q[(i + 1) % len(Q)]
+            d0, d1 = (v - a) / np.linalg.norm(v - a), (b - v) / np.linalg.norm(b - v)
+            a0, a1 = v + s * np.array([d0[1], -d0[0]]), v + s * np.array([d1[1], -d1[0]])
+            cr = d0[0] * d1[1] - d0[1] * d1[0]
+            out.append(a0 + ((a1 - a0)[0] * d1[1] - (a1 - a0)[1] * d1[0]) / cr * d0)
+        x, y = np.array(out).T
+        return 0.5 * abs(np.dot(x, np.roll(y, -1)) - np.dot(y, np.roll(x, -1)))
+
+    def stroke_area(Q):
+        return abs(offset_area(Q, r) - offset_area(Q, -r))
+
+    g, _, _ = _edge_grads(_quad_scene(P, J.MITER, r), 100000, 12)
+    h = 1e-5
+    for i in range(4):
+        for c in range(2):
+            a, b = P.copy(), P.copy()
+            a[i, c] += h
+            b[i, c] -= h
+            exact = DELTA * (stroke_area(a) - stroke_area(b)) / (2 * h)
+            assert abs(g[2 * i + c] - exact) <= 0.02 * abs(exact) + 0.05, (i, c, g[2 * i + c], exact)
+
+
+def test_boundary_sample_count_keeps_the_expectation():
+    # the crate draws W*H*spp edge samples; fewer (here W*H) must estimate the same gradient
+    L, r, c = 16.0, 2.0, 12.3
+    sc = _quad_scene([(c, c), (c + L, c), (c + L, c + L), (c, c + L)], J.BEVEL, r)
+    _, g, se = _edge_grads(sc, 40 * 40, 48, base=7000)
+    exact = DELTA * (8 * L - 4 * r)
+    assert abs(g - exact) <= 4 * se + 0.005 * abs(exact), (g, exact, se)
