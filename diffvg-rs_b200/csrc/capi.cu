@@ -614,7 +614,8 @@ static dvg_status backward_core(dvg_context* ctx, dvg_scene* sc, const dvg_rende
         sp.tile_base = (int)shard->tile_begin;
         sp.tile_count = (int)(shard->tile_end - shard->tile_begin);
     }
-    const float* wsum = shard ? shard_wsum : ctx->wsum.as<float>();
+    // read at each launch: the weights pass below may (re)allocate ctx->wsum
+    auto wsum_now = [&]() -> const float* { return shard ? shard_wsum : ctx->wsum.as<float>(); };
     if (d_render && S.num_groups > 0) {
         if (!have_weights) {
             ++ctx->gen;
@@ -628,9 +629,9 @@ static dvg_status backward_core(dvg_context* ctx, dvg_scene* sc, const dvg_rende
             Prof prof_(ctx, opts->use_prefiltering ? "interior_prefilter" : "interior");
             if (opts->use_prefiltering)
                 ctx->launches +=
-                    launch_interior_prefilter(S, sp, d_render, wsum, G, ctx->status, ctx->stream);
+                    launch_interior_prefilter(S, sp, d_render, wsum_now(), G, ctx->status, ctx->stream);
             else
-                ctx->launches += launch_interior(S, sp, d_render, wsum, G, ctx->status, ctx->stream);
+                ctx->launches += launch_interior(S, sp, d_render, wsum_now(), G, ctx->status, ctx->stream);
         }
         CK(cudaGetLastError());
         if (S.boundary_ok && !opts->use_prefiltering) {  // src/backward/render.rs:191
@@ -651,7 +652,7 @@ static dvg_status backward_core(dvg_context* ctx, dvg_scene* sc, const dvg_rende
             CK(ctx->border.reserve(cap * sizeof(int)));
             CK(ctx->bcounts.reserve((2 * (size_t)tiles * BND_MAX_BUCKETS + 1) * sizeof(int)));
             Prof prof_(ctx, "boundary");
-            ctx->launches += launch_boundary(S, bp, d_render, wsum, G, ctx->bsamples.as<BSample>(),
+            ctx->launches += launch_boundary(S, bp, d_render, wsum_now(), G, ctx->bsamples.as<BSample>(),
                                              ctx->bkey.as<int>(), ctx->bcounts.as<int>(), ctx->border.as<int>(), cap,
                                              ctx->stream);
             CK(cudaGetLastError());
@@ -667,7 +668,7 @@ static dvg_status backward_core(dvg_context* ctx, dvg_scene* sc, const dvg_rende
         }
         if (run_tiles) {
             Prof prof_(ctx, "interior");
-            ctx->launches += launch_interior(S, sp, d_render, wsum, G, ctx->status, ctx->stream);
+            ctx->launches += launch_interior(S, sp, d_render, wsum_now(), G, ctx->status, ctx->stream);
         }
         CK(cudaGetLastError());
     }
