@@ -447,6 +447,7 @@ dvg_status dvg_scene_upload(dvg_context* ctx, const dvg_scene_desc* desc, dvg_sc
     S.s_padmul = (const float*)(base + o_s_pm);
     S.p_shape = (const int*)(base + o_p_shape);
     S.p_miter = (const float*)(base + o_p_miter);
+    S.styled = h.any_styled ? 1 : 0;
     S.p_info = (const int4*)(base + o_p_info);
     S.pn_bounds = (const float4*)(base + o_pn_b);
     S.pn_meta = (const int4*)(base + o_pn_m);
@@ -1123,6 +1124,7 @@ struct dvg_batch {
     uint64_t total_bsamples = 0;
     DevBuf entries, item_scene, accum, wsum, image, target, d_render, loss, grads, bsamples, bkey, border, bcounts;
     DevBuf frag;  // per-scene fragment caches (forward -> interior)
+    bool any_styled = false;  // some scene strokes with non-round joins or caps
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     uint64_t steps = 0;
@@ -1157,6 +1159,7 @@ dvg_status batch_enqueue(dvg_batch* b) {
         ctx->launches += launch_interior_batch(B, b->item_scene.as<int>(), b->items, ctx->status, ctx->stream);
     if (!pre)
         ctx->launches += launch_boundary_batch(B, n, b->total_bsamples, b->total_tiles, (int)b->tune.boundary_cell,
+                                               b->any_styled,
                                                b->bsamples.as<BSample>(),
                                                b->bkey.as<int>(), b->bcounts.as<int>(), b->border.as<int>(),
                                                ctx->stream);
@@ -1229,6 +1232,7 @@ extern "C" dvg_status dvg_batch_create(dvg_context* ctx, dvg_scene* const* scene
         if (npix == 0 || S.num_groups == 0)
             return fail(DVG_ERR_INVALID_ARGUMENT, "batch scenes need a non-empty canvas and at least one group");
         b->scenes.push_back(sc);
+        b->any_styled = b->any_styled || S.styled;
         b->pix_off.push_back(b->total_pix4);
         b->wpix_off.push_back(b->total_pix);
         b->total_pix4 += (npix * 4 + 63) & ~(size_t)63;

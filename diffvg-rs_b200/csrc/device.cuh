@@ -33,6 +33,7 @@ enum : unsigned { ST_FRAGMENT_OVERFLOW = 1u, ST_BVH_LIMIT = 2u, ST_REFIT_LAYOUT 
 struct DevScene {
     int width, height;
     int num_groups, num_shapes, num_paints, num_paths;
+    int styled;  // some path strokes with non-round joins or caps
     int filter_type;
     float filter_radius;
     int filter_ri;

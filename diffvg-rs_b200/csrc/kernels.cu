@@ -1077,6 +1077,26 @@ __device__ bool sample_boundary_point(const DevScene& S, int shape, int group, f
     *pdf_out = pdf;
     return true;
 }
+// The gradient of one join / cap edge sample (out of line with scalar arguments: the
+// boundary kernel is instruction-fetch bound and these samples are few).
+static __device__ __noinline__ void accumulate_join_cap(const int4* p_info, const float* p_miter,
+                                                       const float4* seg_p, const float4* seg_r,
+                                                       const int4* seg_meta, float* d_points, float* d_thickness,
+                                                       float* d_stroke_width, int path, int po, int site, int edge,
+                                                       float f, float nx, float ny, float contrib) {
+    float w[7];
+    int ids[3];
+    if (!join_cap_velocity(p_info, p_miter, seg_p, seg_r, seg_meta, path, site, edge, f, nx, ny, w, ids)) return;
+    for (int j = 0; j < 3; ++j)
+        if (ids[j] >= 0) {
+            add_if(d_points + 2 * (po + ids[j]), w[2 * j] * contrib);
+            add_if(d_points + 2 * (po + ids[j]) + 1, w[2 * j + 1] * contrib);
+        }
+    if (d_thickness)
+        add_if(d_thickness + po + ids[0], w[6] * contrib);
+    else
+        add_if(d_stroke_width, w[6] * contrib);
+}
 __device__ __forceinline__ void mul33(const float* a, const float* b, float* o) {  // Mat3::mul
 #pragma unroll
     for (int r = 0; r < 3; ++r)
@@ -1084,6 +1104,9 @@ __device__ __forceinline__ void mul33(const float* a, const float* b, float* o) 
         for (int c = 0; c < 3; ++c) o[3 * r + c] = a[3 * r] * b[c] + a[3 * r + 1] * b[3 + c] + a[3 * r + 2] * b[6 + c];
 }
 // accumulate_boundary_gradient (boundary.rs:970-1148)
+// STYLED: the scene has strokes with non-round joins or caps (join / cap edge samples,
+// base_point_id < 0); the kernels of other scenes carry none of that code.
+template <bool STYLED>
 __device__ void accumulate_boundary(const DevScene& S, const GradPtrs& G, int shape, int group, float contrib,
                                     float t, float2 n, const BData& bd, float2 local_pt) {
     const int4 si = __ldg(&S.s_info[shape]);
@@ -1097,25 +1120,14 @@ __device__ void accumulate_boundary(const DevScene& S, const GradPtrs& G, int sh
     }
     const bool closed = pflags & PF_CLOSED;
     int nc = 0;  // num_control_points.get(base_point_id).unwrap_or(0)
-    if (si.x == K_PATH && bd.base_point_id >= 0) {
+    if (si.x == K_PATH && (!STYLED || bd.base_point_id >= 0)) {
         int ctrl_count = __ldg(&S.path_cdf_info[shape].y);
         nc = bd.base_point_id < ctrl_count ? S.ncp[co + bd.base_point_id] : 0;
     }
-    if (bd.base_point_id < 0) {  // a join / cap edge sample: the exact normal velocity
-        float w[7];
-        int ids[3];
-        if (join_cap_velocity(S.p_info, S.p_miter, S.seg_p, S.seg_r, S.seg_meta, si.z, -1 - bd.base_point_id,
-                              bd.point_id, bd.t, n.x, n.y, w, ids)) {
-            for (int j = 0; j < 3; ++j)
-                if (ids[j] >= 0) {
-                    add_if(G.d_points + 2 * (po + ids[j]), w[2 * j] * contrib);
-                    add_if(G.d_points + 2 * (po + ids[j]) + 1, w[2 * j + 1] * contrib);
-                }
-            if (pflags & PF_THICK)
-                add_if(G.d_thickness + po + ids[0], w[6] * contrib);
-            else
-                add_if(G.d_shape_stroke_width + shape, w[6] * contrib);
-        }
+    if (STYLED && bd.base_point_id < 0) {  // a join / cap edge sample: the exact normal velocity
+        accumulate_join_cap(S.p_info, S.p_miter, S.seg_p, S.seg_r, S.seg_meta, G.d_points,
+                            (pflags & PF_THICK) ? G.d_thickness : nullptr, G.d_shape_stroke_width + shape, si.z, po,
+                            -1 - bd.base_point_id, bd.point_id, bd.t, n.x, n.y, contrib);
     } else if (bd.is_stroke) {
         if (si.x == K_PATH && (pflags & PF_THICK)) {
             float t2 = bd.t, tt = 1.0f - t2;
@@ -1151,7 +1163,7 @@ __device__ void accumulate_boundary(const DevScene& S, const GradPtrs& G, int sh
         float ang = 2.0f * PI_F * t;
         add_if(dp + 2, dvg_cosf(ang) * n.x * contrib);
         add_if(dp + 3, dvg_sinf(ang) * n.y * contrib);
-    } else if (si.x == K_PATH && bd.base_point_id >= 0) {
+    } else if (si.x == K_PATH && (!STYLED || bd.base_point_id >= 0)) {
         float t2 = bd.t, tt = 1.0f - t2;
         int pid = bd.point_id;
         auto addp = [&](long idx, float w) {
@@ -1316,6 +1328,7 @@ __global__ void k_boundary_scatter(const int* key, uint64_t n, int* cursor, int*
 }
 // Stage 3: evaluate both sides of every edge sample in tile order, so that the
 // lanes of a warp share one group list (render_edge_sample, boundary.rs:845-967).
+template <bool STYLED>
 __device__ __forceinline__ void boundary_eval_one(const DevScene& S, const BSample& r, const float* d_render,
                                                   const float* wsum, const GradPtrs& G) {
     const float W = (float)S.width, H = (float)S.height;
@@ -1380,20 +1393,22 @@ __device__ __forceinline__ void boundary_eval_one(const DevScene& S, const BSamp
     bd.point_id = r.point_id;
     bd.t = r.bt;
     bd.is_stroke = r.is_stroke != 0;
-    accumulate_boundary(S, G, r.shape, r.group, contrib, r.t, nc, bd, make_float2(r.lx, r.ly));
+    accumulate_boundary<STYLED>(S, G, r.shape, r.group, contrib, r.t, nc, bd, make_float2(r.lx, r.ly));
     if (G.d_translation) {
         add_if(G.d_translation + 2 * (size_t)r.pixel, nc.x * contrib);
         add_if(G.d_translation + 2 * (size_t)r.pixel + 1, nc.y * contrib);
     }
 }
+template <bool STYLED>
 __global__ void __launch_bounds__(128, DVG_MINB_BND) k_boundary_eval(DevScene S, const BSample* samples,
                                                                      const int* order, const int* offsets, int tiles,
                                                                      const float* d_render, const float* wsum,
                                                                      GradPtrs G) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= offsets[tiles]) return;
-    boundary_eval_one(S, samples[order[i]], d_render, wsum, G);
+    boundary_eval_one<STYLED>(S, samples[order[i]], d_render, wsum, G);
 }
+template <bool STYLED>
 __global__ void __launch_bounds__(128, DVG_MINB_BND) k_boundary_eval_batch(const BatchEntry* __restrict__ B,
                                                                            const BSample* samples, const int* order,
                                                                            const int* offsets, int tiles) {
@@ -1401,7 +1416,7 @@ __global__ void __launch_bounds__(128, DVG_MINB_BND) k_boundary_eval_batch(const
     if (i >= offsets[tiles]) return;
     const BSample r = samples[order[i]];
     const BatchEntry& E = B[r.scene];
-    boundary_eval_one(E.S, r, E.d_render, E.wsum, E.G);
+    boundary_eval_one<STYLED>(E.S, r, E.d_render, E.wsum, E.G);
 }
 
 // ------------------------------------------------------------------ background finalisation (background.rs:29-61)
@@ -1584,8 +1599,12 @@ int launch_boundary(const DevScene& S, const BoundaryParams& bp, const float* d_
         // reuse the count array as the scatter cursor (a copy of the exclusive offsets)
         cudaMemcpyAsync(counts, offsets, sizeof(int) * (size_t)tiles, cudaMemcpyDeviceToDevice, stream);
         k_boundary_scatter<<<(unsigned)((cnt + 255) / 256), 256, 0, stream>>>(key, cnt, counts, order);
-        k_boundary_eval<<<(unsigned)((cnt + 127) / 128), 128, 0, stream>>>(S, samples, order, offsets, tiles,
-                                                                            d_render, wsum, G);
+        if (S.styled)
+            k_boundary_eval<true><<<(unsigned)((cnt + 127) / 128), 128, 0, stream>>>(S, samples, order, offsets,
+                                                                                  tiles, d_render, wsum, G);
+        else
+            k_boundary_eval<false><<<(unsigned)((cnt + 127) / 128), 128, 0, stream>>>(S, samples, order, offsets,
+                                                                                   tiles, d_render, wsum, G);
         launches += 4;
     }
     return launches;
@@ -1623,7 +1642,7 @@ int launch_interior_batch(const BatchEntry* B, const int* item_scene, int items,
     k_interior_batch<<<items, 256, 0, stream>>>(B, item_scene, status);
     return 2;
 }
-int launch_boundary_batch(const BatchEntry* B, int nscenes, uint64_t total, int total_tiles, int cell,
+int launch_boundary_batch(const BatchEntry* B, int nscenes, uint64_t total, int total_tiles, int cell, bool styled,
                           BSample* samples, int* key, int* counts, int* order, cudaStream_t stream) {
     if (total == 0) return 0;
     total_tiles *= bnd_buckets(cell);  // sort buckets
@@ -1634,8 +1653,12 @@ int launch_boundary_batch(const BatchEntry* B, int nscenes, uint64_t total, int 
     k_bin_scan<<<1, 1024, 0, stream>>>(counts, total_tiles, offsets);
     cudaMemcpyAsync(counts, offsets, sizeof(int) * (size_t)total_tiles, cudaMemcpyDeviceToDevice, stream);
     k_boundary_scatter<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(key, total, counts, order);
-    k_boundary_eval_batch<<<(unsigned)((total + 127) / 128), 128, 0, stream>>>(B, samples, order, offsets,
-                                                                               total_tiles);
+    if (styled)
+        k_boundary_eval_batch<true><<<(unsigned)((total + 127) / 128), 128, 0, stream>>>(B, samples, order, offsets,
+                                                                                     total_tiles);
+    else
+        k_boundary_eval_batch<false><<<(unsigned)((total + 127) / 128), 128, 0, stream>>>(B, samples, order,
+                                                                                      offsets, total_tiles);
     return 4;
 }
 

@@ -156,7 +156,7 @@ int launch_interior_batch(const BatchEntry* B, const int* item_scene, int items,
                           cudaStream_t stream);
 int launch_interior_prefilter_batch(const BatchEntry* B, const int* item_scene, int items, unsigned* status,
                                     cudaStream_t stream);
-int launch_boundary_batch(const BatchEntry* B, int nscenes, uint64_t total, int total_tiles, int cell,
+int launch_boundary_batch(const BatchEntry* B, int nscenes, uint64_t total, int total_tiles, int cell, bool styled,
                           BSample* samples, int* key, int* counts, int* order, cudaStream_t stream);
 // Optimisation step: Adam on the selected parameters of every scene, then the
 // scene tables that depend on path points are rebuilt in place (segments, path and

@@ -338,8 +338,10 @@ dvg_status prepare_scene(const dvg_scene_desc* d, HostScene* out, std::string* e
                                        (thick ? DVG_PATH_HAS_THICKNESS : 0));
             // Stroke joins / caps other than round (an extension: the crate strokes round only).
             const uint32_t join = stroke_join_of(d, s), cap = stroke_cap_of(d, s);
-            if (join != DVG_JOIN_ROUND || (!closed && cap != DVG_CAP_ROUND))
+            if (join != DVG_JOIN_ROUND || (!closed && cap != DVG_CAP_ROUND)) {
                 pflags |= PATH_STYLED | (int32_t)(join << PATH_JOIN_SHIFT) | (int32_t)(cap << PATH_CAP_SHIFT);
+                h.any_styled = true;
+            }
             h.p_miter.push_back(std::fmax(d->shape_miter_limit ? d->shape_miter_limit[s] : 4.0f, 1.0f));
             h.p_info.insert(h.p_info.end(), {seg_off, (int32_t)segs.size(), node_off, node_cnt, (int32_t)po,
                                              (int32_t)pc, (int32_t)co, pflags});

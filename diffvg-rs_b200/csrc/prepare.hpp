@@ -57,6 +57,7 @@ struct HostScene {
                                        //             point off, point count, ctrl off, flags
     std::vector<int32_t> p_shape;      // 1 per path: its shape id
     std::vector<float> p_miter;        // 1 per path: miter limit (>= 1) for miter joins
+    bool any_styled = false;           // some path has PATH_STYLED
     std::vector<float> pn_bounds;      // 4 per path-BVH node
     std::vector<int32_t> pn_meta;      // 4 per node: skip, leaf start (into pl_segs), count, right child
     std::vector<int32_t> pl_segs;      // leaf order: global segment index
