@@ -1283,11 +1283,14 @@ __device__ __forceinline__ void boundary_gen_one(const DevScene& S, uint64_t idx
     r.is_stroke = bd.is_stroke ? 1 : 0;
     r.scene = scene;
     out[slot] = r;
-    // sort bucket: the 4x4-pixel cell of the boundary pixel inside its tile, so that a
-    // warp evaluates edge points that lie close together (coherent group walks)
+    // sort bucket: the cell of the boundary pixel inside its tile, so that a warp
+    // evaluates edge points that lie close together (coherent group walks), then the
+    // sample's class, so that it mostly runs one sampling / gradient code path
     const int tile = tile_off + (by / TILE) * S.tiles_x + (bx / TILE);
     const int per_row = TILE / cell;
-    const int bucket = tile * (per_row * per_row) + ((by % TILE) / cell) * per_row + (bx % TILE) / cell;
+    const int cls = (bd.is_stroke ? 2 : 0) + (__ldg(&S.s_info[shape]).x == K_PATH ? 1 : 0);
+    const int bucket =
+        (tile * (per_row * per_row) + ((by % TILE) / cell) * per_row + (bx % TILE) / cell) * BND_CLASSES + cls;
     key[slot] = bucket;
     atomicAdd(tile_counts + bucket, 1);
 }

@@ -15,10 +15,12 @@ constexpr int MAX_FRAGMENTS = 96;
 // Filter radii up to this (ceil) use the shared-memory tile+halo splat.
 constexpr int MAX_SMEM_RI = 8;
 // Boundary samples are counting-sorted by cell x cell-pixel cells of their tile
-// (cell in {2, 4, 8, 16}: bnd_buckets(cell) buckets per tile); scratch counts hold
+// (cell in {2, 4, 8, 16}) and, inside a cell, by class (fill or stroke, path or other
+// shape: the code they run); bnd_buckets(cell) buckets per tile; scratch counts hold
 // 2 * tiles * BND_MAX_BUCKETS + 1.
-constexpr int BND_MAX_BUCKETS = (16 / 2) * (16 / 2);
-inline int bnd_buckets(int cell) { return (16 / cell) * (16 / cell); }
+constexpr int BND_CLASSES = 4;
+constexpr int BND_MAX_BUCKETS = (16 / 2) * (16 / 2) * BND_CLASSES;
+inline int bnd_buckets(int cell) { return (16 / cell) * (16 / cell) * BND_CLASSES; }
 
 // Fragment cache of the fused forward -> interior paths: the forward stores, per
 // pixel sample, the codes (2 * tile-list entry + 0 stroke / 1 fill) of the fragments
