@@ -475,9 +475,34 @@ __global__ void __launch_bounds__(256, DVG_MINB_LEAN) k_interior_cached_batch(co
 // fragment covers pt) and whether the queried shape is the visible boundary.
 __device__ float4 edge_color(const DevScene& S, int tile, float2 pt, float4 bg, int eq_group, int eq_shape,
                              bool* hit_out) {
-    // Edge tests on the queried shape alone (within_distance_edge / is_inside_edge).
-    bool hit0 = false;
-    {
+    const int off = S.tile_offsets[tile];
+    const int n = S.tile_offsets[tile + 1] - off;
+    const int* list = S.tile_entries + off;
+    float4 acc = bg;
+    int nfrag = 0, ev = 0;  // ev: 0 none, 1 last event sets the hit, 2 last event clears it
+    for (int e = 0; e < n; ++e) {
+        const int g = __ldg(&list[e]);
+        const int4 gi = __ldg(&S.g_info[g]);
+        const float2 lp = xf9(S.g_c2s + 9 * g, pt);
+        // stroke first, then fill; one paint call site for both
+        int hitp[2];
+        hitp[0] = gi.y >= 0 && group_within(S, g, lp) ? gi.y : -1;
+        hitp[1] = gi.x >= 0 && group_inside(S, g, lp, gi.z) ? gi.x : -1;
+#pragma unroll 1
+        for (int which = 0; which < 2; ++which) {
+            if (hitp[which] < 0) continue;
+            const float4 c = paint_color(S, hitp[which], pt);
+            over(acc, c);
+            ++nfrag;
+            if (c.w >= 1.0f) ev = 2;
+            if (g == eq_group) ev = 1;
+        }
+    }
+    if (ev != 0) {
+        *hit_out = ev == 1;
+    } else {  // no deciding fragment: the edge tests on the queried shape alone
+              // (within_distance_edge / is_inside_edge)
+        bool hit0 = false;
         const int4 gi = __ldg(&S.g_info[eq_group]);
         const float2 lp = xf9(S.g_c2s + 9 * eq_group, pt);
         if (gi.y >= 0) {
@@ -488,32 +513,8 @@ __device__ float4 edge_color(const DevScene& S, int tile, float2 pt, float4 bg, 
             float2 sp = shape_local_bwd(S, eq_shape, lp);
             if (fill_hit(gi.z, winding_shape(S, eq_shape, sp, true))) hit0 = true;
         }
+        *hit_out = hit0;
     }
-    const int off = S.tile_offsets[tile];
-    const int n = S.tile_offsets[tile + 1] - off;
-    const int* list = S.tile_entries + off;
-    float4 acc = bg;
-    int nfrag = 0, ev = 0;  // ev: 0 none, 1 last event sets the hit, 2 last event clears it
-    for (int e = 0; e < n; ++e) {
-        const int g = __ldg(&list[e]);
-        const int4 gi = __ldg(&S.g_info[g]);
-        const float2 lp = xf9(S.g_c2s + 9 * g, pt);
-        if (gi.y >= 0 && group_within(S, g, lp)) {
-            float4 c = paint_color(S, gi.y, pt);
-            over(acc, c);
-            ++nfrag;
-            if (c.w >= 1.0f) ev = 2;
-            if (g == eq_group) ev = 1;
-        }
-        if (gi.x >= 0 && group_inside(S, g, lp, gi.z)) {
-            float4 c = paint_color(S, gi.x, pt);
-            over(acc, c);
-            ++nfrag;
-            if (c.w >= 1.0f) ev = 2;
-            if (g == eq_group) ev = 1;
-        }
-    }
-    *hit_out = ev == 0 ? hit0 : ev == 1;
     if (nfrag == 0) return bg;
     float fa = acc.w, fr = acc.x, fg = acc.y, fb = acc.z;
     if (fa > 1.0e-6f) {
