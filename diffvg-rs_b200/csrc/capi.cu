@@ -651,7 +651,7 @@ static dvg_status backward_core(dvg_context* ctx, dvg_scene* sc, const dvg_rende
             CK(ctx->bsamples.reserve(cap * sizeof(BSample)));
             CK(ctx->bkey.reserve(cap * sizeof(int)));
             CK(ctx->border.reserve(cap * sizeof(int)));
-            CK(ctx->bcounts.reserve((2 * (size_t)tiles * BND_MAX_BUCKETS + 1) * sizeof(int)));
+            CK(ctx->bcounts.reserve(bnd_count_ints((size_t)tiles) * sizeof(int)));
             Prof prof_(ctx, "boundary");
             ctx->launches += launch_boundary(S, bp, d_render, wsum_now(), G, ctx->bsamples.as<BSample>(),
                                              ctx->bkey.as<int>(), ctx->bcounts.as<int>(), ctx->border.as<int>(), cap,
@@ -1274,7 +1274,7 @@ extern "C" dvg_status dvg_batch_create(dvg_context* ctx, dvg_scene* const* scene
     CK(b->bsamples.reserve(nbs * sizeof(BSample)));
     CK(b->bkey.reserve(nbs * sizeof(int)));
     CK(b->border.reserve(nbs * sizeof(int)));
-    CK(b->bcounts.reserve((2 * (size_t)b->total_tiles * BND_MAX_BUCKETS + 1) * sizeof(int)));
+    CK(b->bcounts.reserve(bnd_count_ints((size_t)b->total_tiles) * sizeof(int)));
     CK(cudaMemsetAsync(b->target.ptr, 0, b->total_pix4 * sizeof(float), ctx->stream));
     float* acc = b->accum.as<float>();
     float* img = b->image.as<float>();

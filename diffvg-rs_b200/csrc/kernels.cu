@@ -92,6 +92,66 @@ __global__ void __launch_bounds__(1024) k_bin_scan(const int* counts, int n, int
     }
     if (threadIdx.x == 0) offsets[n] = carry;
 }
+// Two-level exclusive scan for long count arrays (the boundary sort's buckets): each
+// CTA scans 4096 counts and leaves its total in part[], one CTA scans the totals, a
+// third pass adds each CTA's base.  offsets[n] receives the grand total.
+constexpr int SCAN_CHUNK = 4096;
+__global__ void __launch_bounds__(1024) k_scan_chunks(const int* counts, int n, int* offsets, int* part) {
+    __shared__ int warp_sums[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int base = blockIdx.x * SCAN_CHUNK + 4 * threadIdx.x;
+    int v[4], t = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        v[k] = base + k < n ? counts[base + k] : 0;
+        t += v[k];
+    }
+    int x = t;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        int w = warp_sums[lane];
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        warp_sums[lane] = w;
+    }
+    __syncthreads();
+    int excl = (wid > 0 ? warp_sums[wid - 1] : 0) + x - t;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (base + k < n) offsets[base + k] = excl;
+        excl += v[k];
+    }
+    if (threadIdx.x == 1023) part[blockIdx.x] = warp_sums[31];
+}
+__global__ void __launch_bounds__(1024) k_scan_add(int* offsets, int n, const int* part_offsets) {
+    const int i = blockIdx.x * SCAN_CHUNK + 4 * threadIdx.x;
+    const int add = part_offsets[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (i + k < n) offsets[i + k] += add;
+}
+// Exclusive scan of counts[n] into offsets[n + 1]; part: scratch of scan_part_ints(n) ints.
+inline int scan_chunks(int n) { return (n + SCAN_CHUNK - 1) / SCAN_CHUNK; }
+int launch_scan(const int* counts, int n, int* offsets, int* part, cudaStream_t stream) {
+    const int c = scan_chunks(n);
+    if (c <= 1) {
+        k_bin_scan<<<1, 1024, 0, stream>>>(counts, n, offsets);
+        return 1;
+    }
+    k_scan_chunks<<<c, 1024, 0, stream>>>(counts, n, offsets, part);
+    k_bin_scan<<<1, 1024, 0, stream>>>(part, c, part + c);  // part + c: the chunks' bases, then the total
+    k_scan_add<<<c, 1024, 0, stream>>>(offsets, n, part + c);
+    cudaMemcpyAsync(offsets + n, part + 2 * c, sizeof(int), cudaMemcpyDeviceToDevice, stream);
+    return 3;
+}
+
 __global__ void __launch_bounds__(256) k_bin_write(DevScene S, const float4* g_bbox, const int* offsets,
                                                    int* entries) {
     __shared__ int warp_counts[8];
@@ -1599,7 +1659,7 @@ int launch_boundary(const DevScene& S, const BoundaryParams& bp, const float* d_
         cudaMemsetAsync(counts, 0, sizeof(int) * (2 * (size_t)tiles + 1), stream);
         k_boundary_gen<<<(unsigned)((cnt + 255) / 256), 256, 0, stream>>>(S, b, samples, key, counts);
         int* offsets = counts + tiles;  // tiles + 1 entries
-        k_bin_scan<<<1, 1024, 0, stream>>>(counts, tiles, offsets);
+        launches += launch_scan(counts, tiles, offsets, counts + 2 * (size_t)tiles + 1, stream);
         // reuse the count array as the scatter cursor (a copy of the exclusive offsets)
         cudaMemcpyAsync(counts, offsets, sizeof(int) * (size_t)tiles, cudaMemcpyDeviceToDevice, stream);
         k_boundary_scatter<<<(unsigned)((cnt + 255) / 256), 256, 0, stream>>>(key, cnt, counts, order);
@@ -1609,7 +1669,7 @@ int launch_boundary(const DevScene& S, const BoundaryParams& bp, const float* d_
         else
             k_boundary_eval<false><<<(unsigned)((cnt + 127) / 128), 128, 0, stream>>>(S, samples, order, offsets,
                                                                                    tiles, d_render, wsum, G);
-        launches += 4;
+        launches += 3;
     }
     return launches;
 }
@@ -1654,7 +1714,7 @@ int launch_boundary_batch(const BatchEntry* B, int nscenes, uint64_t total, int 
     k_boundary_gen_batch<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(B, nscenes, total, cell, samples,
                                                                               key, counts);
     int* offsets = counts + total_tiles;
-    k_bin_scan<<<1, 1024, 0, stream>>>(counts, total_tiles, offsets);
+    const int scans = launch_scan(counts, total_tiles, offsets, counts + 2 * (size_t)total_tiles + 1, stream);
     cudaMemcpyAsync(counts, offsets, sizeof(int) * (size_t)total_tiles, cudaMemcpyDeviceToDevice, stream);
     k_boundary_scatter<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(key, total, counts, order);
     if (styled)
@@ -1663,7 +1723,7 @@ int launch_boundary_batch(const BatchEntry* B, int nscenes, uint64_t total, int 
     else
         k_boundary_eval_batch<false><<<(unsigned)((total + 127) / 128), 128, 0, stream>>>(B, samples, order,
                                                                                       offsets, total_tiles);
-    return 4;
+    return 3 + scans;
 }
 
 int launch_fill_background(const DevScene& S, float* out, cudaStream_t stream) {

@@ -21,6 +21,12 @@ constexpr int MAX_SMEM_RI = 8;
 constexpr int BND_CLASSES = 4;
 constexpr int BND_MAX_BUCKETS = (16 / 2) * (16 / 2) * BND_CLASSES;
 inline int bnd_buckets(int cell) { return (16 / cell) * (16 / cell) * BND_CLASSES; }
+// Ints of boundary-sort scratch for `tiles` tiles: counts, offsets (+1) and the
+// two-level scan's chunk totals, bases and grand total.
+inline size_t bnd_count_ints(size_t tiles) {
+    const size_t b = tiles * BND_MAX_BUCKETS;
+    return 2 * b + 1 + 2 * ((b + 4095) / 4096) + 1;
+}
 
 // Fragment cache of the fused forward -> interior paths: the forward stores, per
 // pixel sample, the codes (2 * tile-list entry + 0 stroke / 1 fill) of the fragments
