@@ -436,6 +436,7 @@ def main():
         tgt_host = target.view(H, W, 4).cpu().numpy()
         ts = []
         img_h = None
+        d_render = np.empty_like(tgt_host)  # the L2 loss gradient, written in place every step
         for i in range(args.e2e_steps + 1):
             torch.cuda.synchronize(dev)
             e0 = torch.cuda.Event(enable_timing=True)
@@ -443,7 +444,8 @@ def main():
             e0.record(lib_stream)
             packed = synth_pack(sc)  # once per step: the scene may change between steps
             img_h = r.render(sc, opts, packed=packed).pixels
-            d_render = 2.0 * (img_h - tgt_host)
+            np.subtract(img_h, tgt_host, out=d_render)
+            d_render *= 2.0
             g = r.render_backward(sc, opts, bopts, d_render, packed=packed)
             e1.record(lib_stream)  # the calls block, so the events bracket host and device work
             torch.cuda.synchronize(dev)

@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import ctypes as C
 from dataclasses import dataclass, field
+from collections.abc import Sequence
 from typing import Dict, List, Optional
 
 import itertools
@@ -150,8 +151,7 @@ def pack_scene(scene: Scene) -> PackedScene:
     flags: List[int] = []
     ncp_l: List[int] = []
     pts_l: list = []
-    th_l: List[float] = []
-    any_thick = False
+    th_parts: List[tuple] = []  # (point offset, thickness values) of paths that have them
     zero4 = (0.0, 0.0, 0.0, 0.0)
     for sh in scene.shapes:
         g = sh.geometry
@@ -174,11 +174,7 @@ def pack_scene(scene: Scene) -> PackedScene:
             f = (PATH_CLOSED if p.is_closed else 0) | (PATH_DISTANCE_APPROX if p.use_distance_approx else 0)
             if p.thickness is not None:
                 f |= PATH_HAS_THICKNESS
-                any_thick = True
-                t = [float(x) for x in list(p.thickness)[:npt]]
-                th_l.extend(t + [0.0] * (npt - len(t)))
-            else:
-                th_l.extend([0.0] * npt)
+                th_parts.append((pt_off[-1], [float(x) for x in list(p.thickness)[:npt]]))
             flags.append(f)
             continue
         ctrl_off.append(0)
@@ -202,11 +198,15 @@ def pack_scene(scene: Scene) -> PackedScene:
     f32 = lambda v: np.asarray(v, np.float32).reshape(-1)  # noqa: E731
     kinds, sw, joins, caps, miters = u32(kinds), f32(sw), u32(joins), u32(caps), f32(miters)
     ctrl_off, ctrl_cnt, pt_off, pt_cnt, flags = u32(ctrl_off), u32(ctrl_cnt), u32(pt_off), u32(pt_cnt), u32(flags)
-    params = np.asarray(params, np.float32).reshape(ns, 4) if ns else np.zeros((0, 4), np.float32)
-    xforms = np.stack(xf).astype(np.float32, copy=False).reshape(ns, 9) if ns else np.zeros((0, 9), np.float32)
+    params = np.fromiter(itertools.chain.from_iterable(params), np.float32, 4 * ns).reshape(ns, 4)
+    # every Mat3 holds a (3, 3) float32 array, so the rows concatenate without a copy per shape
+    xforms = np.concatenate(xf).astype(np.float32, copy=False).reshape(ns, 9) if ns else np.zeros((0, 9), np.float32)
     ncp = np.asarray(ncp_l, np.int64).astype(np.uint8) if n_ncp else np.zeros(1, np.uint8)
     pts = np.fromiter(itertools.chain.from_iterable(pts_l), np.float32, 2 * n_pts) if n_pts else np.zeros(2, np.float32)
-    thick = np.asarray(th_l, np.float32) if n_pts else np.zeros(1, np.float32)
+    any_thick = bool(th_parts)
+    thick = np.zeros(max(n_pts, 1), np.float32)
+    for o, t in th_parts:
+        thick[o: o + len(t)] = t
 
     ng = len(scene.groups)
     g_off: List[int] = []
@@ -227,7 +227,7 @@ def pack_scene(scene: Scene) -> PackedScene:
     for gi, grp in enumerate(scene.groups):
         g_off.append(len(g_ids))
         g_cnt.append(len(grp.shape_indices))
-        g_ids.extend(int(s) for s in grp.shape_indices)
+        g_ids.extend(grp.shape_indices)
         g_rule.append(int(grp.fill_rule))
         s2c.append(grp.shape_to_canvas.m)
         c2s.append(grp.canvas_to_shape.m)
@@ -247,14 +247,14 @@ def pack_scene(scene: Scene) -> PackedScene:
                 s_col += [st.color.r, st.color.g, st.color.b, st.color.a]
     g_off, g_cnt, g_rule = u32(g_off), u32(g_cnt), u32(g_rule)
     g_fill, g_stroke = np.asarray(g_fill, np.int32).reshape(-1), np.asarray(g_stroke, np.int32).reshape(-1)
-    g_s2c = np.stack(s2c).astype(np.float32, copy=False).reshape(ng, 9) if ng else np.zeros((0, 9), np.float32)
-    g_c2s = np.stack(c2s).astype(np.float32, copy=False).reshape(ng, 9) if ng else np.zeros((0, 9), np.float32)
+    g_s2c = np.concatenate(s2c).astype(np.float32, copy=False).reshape(ng, 9) if ng else np.zeros((0, 9), np.float32)
+    g_c2s = np.concatenate(c2s).astype(np.float32, copy=False).reshape(ng, 9) if ng else np.zeros((0, 9), np.float32)
 
     arrays = dict(
         kinds=kinds, params=params.reshape(-1), xforms=xforms.reshape(-1), sw=sw, joins=joins, caps=caps,
         miters=miters, ctrl_off=ctrl_off, ctrl_cnt=ctrl_cnt, pt_off=pt_off, pt_cnt=pt_cnt, flags=flags,
         ncp=ncp, pts=pts, thick=thick,
-        g_off=g_off, g_cnt=g_cnt, g_ids=np.asarray(g_ids if g_ids else [0], np.uint32), g_rule=g_rule,
+        g_off=g_off, g_cnt=g_cnt, g_ids=np.asarray(g_ids if g_ids else [0], np.int64).astype(np.uint32), g_rule=g_rule,
         g_s2c=g_s2c.reshape(-1), g_c2s=g_c2s.reshape(-1), g_fill=g_fill, g_stroke=g_stroke,
         p_kind=np.asarray(p_kind if p_kind else [0], np.uint32),
         p_params=np.asarray(p_params if p_params else [[0, 0, 0, 0]], np.float32).reshape(-1),
@@ -435,48 +435,86 @@ def to_diffvg_layout(grad: "SceneGrad", scene: Scene) -> DiffvgSceneGrad:
                            grad.translation)
 
 
-def _paint_grad(kind_paint, buf: GradBuffers, pi: int, soff: int, scnt: int) -> dict:
+class LazyList(Sequence):
+    """Read-only list whose items are built on first access.  A scene of thousands of
+    shapes has thousands of small gradient records; building them all after every
+    backward pass costs more host time than the pass's own host work, and an optimiser
+    that reads the flat buffers never needs them."""
+
+    __slots__ = ("_make", "_items")
+
+    def __init__(self, n: int, make):
+        self._make = make
+        self._items = [None] * n
+
+    def __len__(self) -> int:
+        return len(self._items)
+
+    def __getitem__(self, i):
+        if isinstance(i, slice):
+            return [self[j] for j in range(*i.indices(len(self._items)))]
+        it = self._items[i]  # IndexError for out-of-range indices, as a list
+        if it is None:
+            i = int(i) + len(self._items) if i < 0 else int(i)
+            it = self._items[i] = self._make(i)
+        return it
+
+    def __iter__(self):
+        return (self[i] for i in range(len(self._items)))
+
+    def __repr__(self) -> str:
+        return repr(list(self))
+
+
+def _paint_grad(kind: int, buf: GradBuffers, pi: int, soff: int, scnt: int) -> dict:
     pp = buf["d_paint_params"][4 * pi: 4 * pi + 4].copy()
     stops = [dict(offset=float(buf["d_stop_offsets"][soff + k]), color=buf["d_stop_colors"][4 * (soff + k): 4 * (soff + k) + 4].copy())
              for k in range(scnt)]
-    if isinstance(kind_paint, Color):
+    if kind == PAINT_SOLID:
         return dict(kind="solid", color=pp)
-    if isinstance(kind_paint, LinearGradient):
+    if kind == PAINT_LINEAR:
         return dict(kind="linear", start=pp[:2], end=pp[2:], stops=stops)
     return dict(kind="radial", center=pp[:2], radius=pp[2:], stops=stops)
 
 
 def unflatten_grads(scene: Scene, packed: PackedScene, buf: GradBuffers) -> SceneGrad:
-    shapes = []
-    for i, sh in enumerate(scene.shapes):
-        g = sh.geometry
+    """Flat gradient buffers -> SceneGrad (src/grad.rs:113-126).  The per-shape and
+    per-group records are built when first read, from the packed arrays alone (editing
+    `scene` afterwards does not change them)."""
+    kinds, flags = packed.arrays["kinds"], packed.arrays["flags"]
+    p_kind = packed.arrays["p_kind"]
+    g_fill, g_stroke = packed.arrays["g_fill"], packed.arrays["g_stroke"]
+
+    def shape(i: int) -> DShape:
         sp = buf["d_shape_params"][4 * i: 4 * i + 4]
-        if isinstance(g, Circle):
+        k = int(kinds[i])
+        if k == SHAPE_CIRCLE:
             geo = dict(kind="circle", center=sp[:2].copy(), radius=float(sp[2]))
-        elif isinstance(g, Ellipse):
+        elif k == SHAPE_ELLIPSE:
             geo = dict(kind="ellipse", center=sp[:2].copy(), radius=sp[2:].copy())
-        elif isinstance(g, Rect):
+        elif k == SHAPE_RECT:
             geo = dict(kind="rect", min=sp[:2].copy(), max=sp[2:].copy())
         else:
             o, n = packed.path_point_offset[i], packed.path_point_count[i]
             pts = buf["d_points"][2 * o: 2 * (o + n)].reshape(-1, 2).copy()
-            th = buf["d_thickness"][o: o + n].copy() if g.path.thickness is not None else None
+            th = buf["d_thickness"][o: o + n].copy() if int(flags[i]) & PATH_HAS_THICKNESS else None
             geo = dict(kind="path", points=pts, thickness=th)
-        shapes.append(DShape(geo, buf["d_shape_transform"][9 * i: 9 * i + 9].reshape(3, 3).copy(),
-                             float(buf["d_shape_stroke_width"][i])))
-    groups = []
-    for gi, grp in enumerate(scene.groups):
-        fill = stroke = None
-        if grp.fill is not None:
-            pi = packed.paint_of[(gi, "fill")]
-            fill = _paint_grad(grp.fill, buf, pi, packed.stop_offset[pi], packed.stop_count[pi])
-        if grp.stroke is not None:
-            pi = packed.paint_of[(gi, "stroke")]
-            stroke = _paint_grad(grp.stroke, buf, pi, packed.stop_offset[pi], packed.stop_count[pi])
-        groups.append(DShapeGroup(buf["d_group_transform"][9 * gi: 9 * gi + 9].reshape(3, 3).copy(), fill, stroke))
+        return DShape(geo, buf["d_shape_transform"][9 * i: 9 * i + 9].reshape(3, 3).copy(),
+                      float(buf["d_shape_stroke_width"][i]))
+
+    def paint(pi: int) -> Optional[dict]:
+        if pi < 0:
+            return None
+        return _paint_grad(int(p_kind[pi]), buf, pi, packed.stop_offset[pi], packed.stop_count[pi])
+
+    def group(gi: int) -> DShapeGroup:
+        return DShapeGroup(buf["d_group_transform"][9 * gi: 9 * gi + 9].reshape(3, 3).copy(),
+                           paint(int(g_fill[gi])), paint(int(g_stroke[gi])))
+
     bgi = buf["d_background_image"]
     tr = buf["d_translation"]
-    return SceneGrad(shapes, groups, float(buf["d_filter_radius"][0]), buf["d_background"].copy(),
+    return SceneGrad(LazyList(len(scene.shapes), shape), LazyList(len(scene.groups), group),
+                     float(buf["d_filter_radius"][0]), buf["d_background"].copy(),
                      None if bgi is None else bgi.copy(), None if tr is None else tr.copy(), buf)
 
 
