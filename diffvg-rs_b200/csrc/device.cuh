@@ -1141,12 +1141,28 @@ __device__ __forceinline__ void add_if(float* p, float v) {
     if (v != 0.0f) atomicAdd(p, v);
 }
 
-// d_sample_paint for gradient paints (backward/paint.rs:91-277), per-lane atomics.
-static __device__ void d_gradient_paint(const DevScene& S, const GradPtrs& G, int p, float2 pt, float4 dc, float2* dtr) {
+// d_sample_paint for gradient paints (backward/paint.rs:91-277), split in the terms one
+// sample adds and where they go.  stop: the stop whose colour takes c0 (an interval
+// [o_stop, o_stop+1) also gives c1 to stop + 1, the two stop-offset terms when the
+// interval has a width, and the paint-parameter terms); -1: nothing to add.
+struct PaintGradTerms {
+    int stop;
+    bool interval, has_off;
+    float4 c0, c1;
+    float off0, off1;
+    float4 pp;
+};
+static __device__ __forceinline__ PaintGradTerms gradient_paint_terms(const DevScene& S, int p, float2 pt, float4 dc,
+                                                                     float2* dtr) {
+    PaintGradTerms r;
+    r.stop = -1;
+    r.interval = r.has_off = false;
+    r.c0 = r.c1 = r.pp = make_float4(0, 0, 0, 0);
+    r.off0 = r.off1 = 0.0f;
     int4 pi = __ldg(&S.paint_info[p]);
     float4 pp = __ldg(&S.paint_params[p]);
     int so = pi.y, sc = pi.z;
-    if (sc <= 0) return;
+    if (sc <= 0) return r;
     float t, denom = 0.0f, offx = 0.0f, offy = 0.0f, nx = 0.0f, ny = 0.0f;
     if (pi.x == P_LINEAR) {
         float ex = pp.z - pp.x, ey = pp.w - pp.y;
@@ -1160,36 +1176,27 @@ static __device__ void d_gradient_paint(const DevScene& S, const GradPtrs& G, in
         t = len2(nx, ny);
     }
     if (t < __ldg(&S.stop_offsets[so])) {
-        float* c = G.d_stop_colors + 4 * so;
-        add_if(c + 0, dc.x);
-        add_if(c + 1, dc.y);
-        add_if(c + 2, dc.z);
-        add_if(c + 3, dc.w);
-        return;
+        r.stop = so;
+        r.c0 = dc;
+        return r;
     }
     for (int i = 0; i + 1 < sc; ++i) {
         float o0 = __ldg(&S.stop_offsets[so + i]), o1 = __ldg(&S.stop_offsets[so + i + 1]);
         if (t >= o0 && t < o1) {
             float tt = (t - o0) / (o1 - o0);
             float4 c0 = __ldg(&S.stop_colors[so + i]), c1 = __ldg(&S.stop_colors[so + i + 1]);
-            float* a0 = G.d_stop_colors + 4 * (so + i);
-            float* a1 = a0 + 4;
-            add_if(a0 + 0, dc.x * (1.0f - tt));
-            add_if(a0 + 1, dc.y * (1.0f - tt));
-            add_if(a0 + 2, dc.z * (1.0f - tt));
-            add_if(a0 + 3, dc.w * (1.0f - tt));
-            add_if(a1 + 0, dc.x * tt);
-            add_if(a1 + 1, dc.y * tt);
-            add_if(a1 + 2, dc.z * tt);
-            add_if(a1 + 3, dc.w * tt);
+            r.stop = so + i;
+            r.interval = true;
+            r.c0 = make_float4(dc.x * (1.0f - tt), dc.y * (1.0f - tt), dc.z * (1.0f - tt), dc.w * (1.0f - tt));
+            r.c1 = make_float4(dc.x * tt, dc.y * tt, dc.z * tt, dc.w * tt);
             float d_tt = dc.x * (c1.x - c0.x) + dc.y * (c1.y - c0.y) + dc.z * (c1.z - c0.z) + dc.w * (c1.w - c0.w);
             float dof = o1 - o0;
             if (fabsf(dof) > 0.0f) {
-                add_if(G.d_stop_offsets + so + i, d_tt * (tt - 1.0f) / dof);
-                add_if(G.d_stop_offsets + so + i + 1, -d_tt * tt / dof);
+                r.has_off = true;
+                r.off0 = d_tt * (tt - 1.0f) / dof;
+                r.off1 = -d_tt * tt / dof;
             }
             float d_t = d_tt / dof;
-            float* dpp = G.d_paint_params + 4 * p;
             if (pi.x == P_LINEAR) {
                 float bx = d_t * (-(pt.x - pp.x) - (pp.z - pp.x)) / denom;
                 float by = d_t * (-(pt.y - pp.y) - (pp.w - pp.y)) / denom;
@@ -1199,15 +1206,10 @@ static __device__ void d_gradient_paint(const DevScene& S, const GradPtrs& G, in
                 float lx = pp.z - pp.x, ly = pp.w - pp.y;
                 if (lx * lx + ly * ly > 1.0e-3f) {
                     float ax = pp.x - pp.z, ay = pp.y - pp.w;
-                    add_if(dpp + 0, bx + 2.0f * d_l * ax);
-                    add_if(dpp + 1, by + 2.0f * d_l * ay);
-                    add_if(dpp + 2, ex + 2.0f * d_l * lx);
-                    add_if(dpp + 3, ey + 2.0f * d_l * ly);
+                    r.pp = make_float4(bx + 2.0f * d_l * ax, by + 2.0f * d_l * ay, ex + 2.0f * d_l * lx,
+                                       ey + 2.0f * d_l * ly);
                 } else {
-                    add_if(dpp + 0, bx);
-                    add_if(dpp + 1, by);
-                    add_if(dpp + 2, ex);
-                    add_if(dpp + 3, ey);
+                    r.pp = make_float4(bx, by, ex, ey);
                 }
                 dtr->x += bx + ex;
                 dtr->y += by + ey;
@@ -1222,23 +1224,84 @@ static __device__ void d_gradient_paint(const DevScene& S, const GradPtrs& G, in
                 }
                 float dox = dnx / pp.z, doy = dny / pp.w;
                 float drx = -dnx * offx / (pp.z * pp.z), dry = -dny * offy / (pp.w * pp.w);
-                add_if(dpp + 0, -dox);
-                add_if(dpp + 1, -doy);
-                add_if(dpp + 2, drx);
-                add_if(dpp + 3, dry);
+                r.pp = make_float4(-dox, -doy, drx, dry);
                 dtr->x += -dox;
                 dtr->y += -doy;
             }
-            return;
+            return r;
         }
     }
-    float* c = G.d_stop_colors + 4 * (so + sc - 1);
-    add_if(c + 0, dc.x);
-    add_if(c + 1, dc.y);
-    add_if(c + 2, dc.z);
-    add_if(c + 3, dc.w);
+    r.stop = so + sc - 1;
+    r.c0 = dc;
+    return r;
 }
-
+static __device__ __forceinline__ void add4_if(float* d, float4 v) {
+    add_if(d + 0, v.x);
+    add_if(d + 1, v.y);
+    add_if(d + 2, v.z);
+    add_if(d + 3, v.w);
+}
+static __device__ __forceinline__ void add_paint_terms(const GradPtrs& G, int p, const PaintGradTerms& r) {
+    if (r.stop < 0) return;
+    float* a0 = G.d_stop_colors + 4 * r.stop;
+    add4_if(a0, r.c0);
+    if (!r.interval) return;
+    add4_if(a0 + 4, r.c1);
+    if (r.has_off) {
+        add_if(G.d_stop_offsets + r.stop, r.off0);
+        add_if(G.d_stop_offsets + r.stop + 1, r.off1);
+    }
+    add4_if(G.d_paint_params + 4 * p, r.pp);
+}
+// Per-lane atomics.
+static __device__ void d_gradient_paint(const DevScene& S, const GradPtrs& G, int p, float2 pt, float4 dc, float2* dtr) {
+    add_paint_terms(G, p, gradient_paint_terms(S, p, pt, dc, dtr));
+}
+__device__ __forceinline__ float4 warp_sum4(float4 v) {
+    return make_float4(warp_sum(v.x), warp_sum(v.y), warp_sum(v.z), warp_sum(v.w));
+}
+// The same for a whole warp whose lanes share paint p (all 32 lanes call it; `has`:
+// this lane has a contribution).  When every contributing lane adds to the same stop
+// (or stop interval) the terms are summed over the warp and one lane adds them: 1
+// atomic per term instead of one per lane, all of them on one cache line.  The same
+// terms, summed in another order.
+static __device__ void d_gradient_paint_warp(const DevScene& S, const GradPtrs& G, int p, float2 pt, float4 dc,
+                                             bool has, float2* dtr) {
+    PaintGradTerms r;
+    r.stop = -1;
+    if (has) r = gradient_paint_terms(S, p, pt, dc, dtr);
+    const int key = r.stop < 0 ? -1 : 2 * r.stop + (r.interval ? 1 : 0);
+    const int kmax = __reduce_max_sync(0xffffffffu, key);
+    const int kmin = __reduce_min_sync(0xffffffffu, key < 0 ? 0x7fffffff : key);
+    if (kmax < 0) return;
+    if (kmin != kmax) {  // lanes in different stop intervals
+        add_paint_terms(G, p, r);
+        return;
+    }
+    if (r.stop < 0) {
+        r.c0 = r.c1 = r.pp = make_float4(0, 0, 0, 0);
+        r.off0 = r.off1 = 0.0f;
+    }
+    const bool interval = (kmax & 1) != 0;
+    const float4 c0 = warp_sum4(r.c0);
+    float4 c1 = make_float4(0, 0, 0, 0), pp4 = make_float4(0, 0, 0, 0);
+    float o0 = 0.0f, o1 = 0.0f;
+    if (interval) {
+        c1 = warp_sum4(r.c1);
+        pp4 = warp_sum4(r.pp);
+        o0 = warp_sum(r.off0);
+        o1 = warp_sum(r.off1);
+    }
+    if ((threadIdx.x & 31) != 0) return;
+    const int stop = kmax >> 1;
+    float* a0 = G.d_stop_colors + 4 * stop;
+    add4_if(a0, c0);
+    if (!interval) return;
+    add4_if(a0 + 4, c1);
+    add_if(G.d_stop_offsets + stop, o0);  // zero sums (an interval without width) add nothing
+    add_if(G.d_stop_offsets + stop + 1, o1);
+    add4_if(G.d_paint_params + 4 * p, pp4);
+}
 
 // ------------------------------------------------------------------ filtered splat / gather
 // Adds the sample's premultiplied colour times the filter weight (and the weight)

@@ -473,10 +473,10 @@ __device__ __forceinline__ void interior_body(const DevScene& S, const SamplePar
                 add_if(d + 2, s2);
                 add_if(d + 3, s3);
             }
-        } else if (has) {
+        } else {
             float2 dtr = make_float2(0.0f, 0.0f);
-            d_gradient_paint(S, G, p, pt, dv, &dtr);
-            if (G.d_translation) {
+            d_gradient_paint_warp(S, G, p, pt, dv, has, &dtr);
+            if (has && G.d_translation) {
                 add_if(G.d_translation + 2 * (size_t)pixel, dtr.x);
                 add_if(G.d_translation + 2 * (size_t)pixel + 1, dtr.y);
             }
