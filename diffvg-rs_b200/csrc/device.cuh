@@ -1253,15 +1253,11 @@ static __device__ __forceinline__ void add_paint_terms(const GradPtrs& G, int p,
     }
     add4_if(G.d_paint_params + 4 * p, r.pp);
 }
-// Per-lane atomics.
-static __device__ void d_gradient_paint(const DevScene& S, const GradPtrs& G, int p, float2 pt, float4 dc, float2* dtr) {
-    add_paint_terms(G, p, gradient_paint_terms(S, p, pt, dc, dtr));
-}
 __device__ __forceinline__ float4 warp_sum4(float4 v) {
     return make_float4(warp_sum(v.x), warp_sum(v.y), warp_sum(v.z), warp_sum(v.w));
 }
-// The same for a whole warp whose lanes share paint p (all 32 lanes call it; `has`:
-// this lane has a contribution).  When every contributing lane adds to the same stop
+// d_sample_paint of a gradient paint for a whole warp whose lanes share paint p (all
+// 32 lanes call it; `has`: this lane has a contribution).  When every contributing lane adds to the same stop
 // (or stop interval) the terms are summed over the warp and one lane adds them: 1
 // atomic per term instead of one per lane, all of them on one cache line.  The same
 // terms, summed in another order.

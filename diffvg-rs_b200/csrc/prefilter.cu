@@ -878,9 +878,9 @@ __device__ __forceinline__ void interior_prefilter_body(const DevScene& S, const
                     add_if(d + 3, s3);
                 }
             }
-            if (!has || w == 0.0f) continue;
             float2 tdelta = make_float2(0.0f, 0.0f);
-            if (kind != P_SOLID) d_gradient_paint(S, G, p, pt, dv, &tdelta);
+            if (kind != P_SOLID) d_gradient_paint_warp(S, G, p, pt, dv, has && w != 0.0f, &tdelta);
+            if (!has || w == 0.0f) continue;
             const float d = fdist[i];
             float d_d;
             bool geom = true;
