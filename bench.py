@@ -436,7 +436,8 @@ def main():
         tgt_host = target.view(H, W, 4).cpu().numpy()
         ts = []
         img_h = None
-        d_render = np.empty_like(tgt_host)  # the L2 loss gradient, written in place every step
+        # the L2 loss gradient, written in place every step, in page-locked memory
+        d_render = torch.empty(tgt_host.shape, dtype=torch.float32, pin_memory=True).numpy()
         for i in range(args.e2e_steps + 1):
             torch.cuda.synchronize(dev)
             e0 = torch.cuda.Event(enable_timing=True)
@@ -457,8 +458,9 @@ def main():
         e2e = {"value": samples * world / e2e_s / 1e6, "unit": UNIT,
                "h2d_bytes_per_step": int(desc_bytes + d_render.nbytes),
                "d2h_bytes_per_step": int(img_h.nbytes + grad_bytes), "ms_per_step": e2e_s * 1e3,
-               "path": "pack_scene + dvg_render + dvg_render_backward per step (host buffers; the backward "
-                       "reuses the scene, weights and fragment codes dvg_render retained)"}
+               "path": "pack_scene + dvg_render + dvg_render_backward per step (host buffers: the image "
+                       "and the loss gradient in page-locked memory; the backward reuses the scene, weights "
+                       "and fragment codes dvg_render retained)"}
 
     fit = None
     if args.large_fit_steps > 0:

@@ -423,6 +423,15 @@ class Renderer:
         packing again (e.g. after editing its arrays in place)."""
         return UploadedScene(self, scene, packed)
 
+    def _host_image(self, shape) -> np.ndarray:
+        """An uninitialised float32 host array in page-locked memory (torch's caching
+        host allocator: a freed image's block is reused by the next one), so that the
+        device-to-host copy of the image runs at DMA speed instead of through the
+        driver's staging buffer."""
+        import torch
+
+        return torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
+
     def render(self, scene: Scene, options: RenderOptions = None, packed: Optional[PackedScene] = None) -> Image:
         """Renderer::render (src/renderer/renderer.rs:39-545).  `packed`: pack_scene(scene)
         made by the caller (one packing for a render and the render_backward after it)."""
@@ -433,7 +442,7 @@ class Renderer:
         if scene.width == 0 or scene.height == 0:
             return Image(scene.width, scene.height, np.zeros((0,), np.float32))
         packed = packed or pack_scene(scene)
-        out = np.empty((scene.height, scene.width, 4), np.float32)
+        out = self._host_image((scene.height, scene.width, 4))
         o = render_options_c(options)
         _check(self.lib.dvg_render(self.ctx, packed.ref(), C.byref(o), _fp(out)))
         return Image(scene.width, scene.height, out)
