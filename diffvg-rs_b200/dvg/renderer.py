@@ -423,11 +423,15 @@ class Renderer:
         packing again (e.g. after editing its arrays in place)."""
         return UploadedScene(self, scene, packed)
 
+    PINNED_IMAGE_BYTES = 256 << 20
+
     def _host_image(self, shape) -> np.ndarray:
-        """An uninitialised float32 host array in page-locked memory (torch's caching
-        host allocator: a freed image's block is reused by the next one), so that the
-        device-to-host copy of the image runs at DMA speed instead of through the
-        driver's staging buffer."""
+        """An uninitialised float32 host array, page-locked up to PINNED_IMAGE_BYTES
+        (torch's caching host allocator: a freed image's block is reused by the next
+        one), so that the device-to-host copy of the image runs at DMA speed instead of
+        through the driver's staging buffer; larger images use ordinary memory."""
+        if int(np.prod(shape)) * 4 > self.PINNED_IMAGE_BYTES:
+            return np.empty(shape, np.float32)
         import torch
 
         return torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
