@@ -13,7 +13,10 @@ from dataclasses import dataclass, field
 from collections.abc import Sequence
 from typing import Dict, List, Optional
 
+import importlib
 import itertools
+import os
+import subprocess
 
 import numpy as np
 
@@ -133,9 +136,61 @@ def _paint_record(p):
     raise TypeError(f"unsupported paint {type(p)!r}")
 
 
+_PACKER = None
+
+
+def _packer():
+    """The native packer module (csrc/pack.cpp, built by `make -C diffvg-rs_b200 pack`
+    on first use when missing) and the classes it tests against."""
+    global _PACKER
+    if _PACKER is None:
+        try:
+            from . import _dvgpack
+        except ImportError:
+            pkg = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+            subprocess.run(["make", "-s", "-C", pkg, "pack"], check=True)
+            importlib.invalidate_caches()
+            from . import _dvgpack
+
+        def as_f32(m):
+            return np.ascontiguousarray(np.asarray(m, np.float32).reshape(-1))
+
+        _PACKER = (_dvgpack, (PathGeometry, Circle, Ellipse, Rect, Color, LinearGradient, RadialGradient, as_f32))
+    return _PACKER
+
+
 def pack_scene(scene: Scene) -> PackedScene:
-    """Scene -> dvg_scene_desc arrays (one Python pass collecting plain lists, one
-    numpy conversion per array)."""
+    """Scene -> dvg_scene_desc arrays, in one native pass over the scene objects."""
+    mod, types = _packer()
+    raw, any_thick, paint_of = mod.pack(scene, types)
+
+    def arr(k, dt, default=None):
+        a = np.frombuffer(raw[k], dt)
+        return a if a.size or default is None else np.asarray(default, dt)
+
+    u32, f32 = np.uint32, np.float32
+    n_pts = len(raw["pts"]) // 8
+    g_ids = arr("g_ids", np.int64)
+    arrays = dict(
+        kinds=arr("kinds", u32), params=arr("params", f32), xforms=arr("xforms", f32), sw=arr("sw", f32),
+        joins=arr("joins", u32), caps=arr("caps", u32), miters=arr("miters", f32), ctrl_off=arr("ctrl_off", u32),
+        ctrl_cnt=arr("ctrl_cnt", u32), pt_off=arr("pt_off", u32), pt_cnt=arr("pt_cnt", u32),
+        flags=arr("flags", u32), ncp=arr("ncp", np.uint8, [0]), pts=arr("pts", f32, [0.0, 0.0]),
+        thick=arr("thick", f32, [0.0]),
+        g_off=arr("g_off", u32), g_cnt=arr("g_cnt", u32), g_ids=(g_ids if g_ids.size else np.zeros(1, np.int64)).astype(u32),
+        g_rule=arr("g_rule", u32), g_s2c=arr("g_s2c", f32), g_c2s=arr("g_c2s", f32),
+        g_fill=arr("g_fill", np.int32), g_stroke=arr("g_stroke", np.int32),
+        p_kind=arr("p_kind", u32, [0]), p_params=arr("p_params", f32, [0.0] * 4), p_soff=arr("p_soff", u32, [0]),
+        p_scnt=arr("p_scnt", u32, [0]), s_off=arr("s_off", f32, [0.0]), s_col=arr("s_col", f32, [0.0] * 4),
+    )
+    counts = dict(ctrl=len(raw["ncp"]), points=n_pts, group_shapes=int(g_ids.size), paints=len(raw["p_kind"]) // 4,
+                  stops=len(raw["s_off"]) // 4)
+    return _describe(scene, arrays, counts, bool(any_thick), paint_of)
+
+
+def pack_scene_python(scene: Scene) -> PackedScene:
+    """pack_scene in plain Python (one pass collecting lists, one numpy conversion per
+    array): the reference the native packer is tested against, byte for byte."""
     ns = len(scene.shapes)
     kinds: List[int] = []
     params: List[tuple] = []
@@ -263,6 +318,13 @@ def pack_scene(scene: Scene) -> PackedScene:
         s_off=np.asarray(s_off if s_off else [0.0], np.float32),
         s_col=np.asarray(s_col if s_col else [0.0] * 4, np.float32),
     )
+    counts = dict(ctrl=n_ncp, points=n_pts, group_shapes=len(g_ids), paints=len(p_kind), stops=len(s_off))
+    return _describe(scene, arrays, counts, any_thick, paint_of)
+
+
+def _describe(scene: Scene, arrays: Dict[str, np.ndarray], counts: Dict[str, int], any_thick: bool,
+              paint_of: dict) -> PackedScene:
+    """The dvg_scene_desc over packed arrays (shared by both packers)."""
     bg_img = None
     if scene.background_image is not None:
         bg_img = np.ascontiguousarray(np.asarray(scene.background_image, np.float32).reshape(-1))
@@ -275,7 +337,7 @@ def pack_scene(scene: Scene) -> PackedScene:
     d.background_image = _ptr(bg_img, C.c_float)
     d.filter_type = int(scene.filter.filter_type)
     d.filter_radius = float(scene.filter.radius)
-    d.num_shapes = ns
+    d.num_shapes = len(scene.shapes)
     d.shape_kind = _ptr(arrays["kinds"], C.c_uint32)
     d.shape_params = _ptr(arrays["params"], C.c_float)
     d.shape_transform = _ptr(arrays["xforms"], C.c_float)
@@ -291,27 +353,29 @@ def pack_scene(scene: Scene) -> PackedScene:
     d.num_control_points = _ptr(arrays["ncp"], C.c_uint8)
     d.points = _ptr(arrays["pts"], C.c_float)
     d.thickness = _ptr(arrays["thick"], C.c_float) if any_thick else C.cast(None, _fp)
-    d.total_ctrl = n_ncp
-    d.total_points = n_pts
-    d.num_groups = ng
-    d.group_shape_offset = _ptr(g_off, C.c_uint32)
-    d.group_shape_count = _ptr(g_cnt, C.c_uint32)
+    d.total_ctrl = counts['ctrl']
+    d.total_points = counts['points']
+    d.num_groups = len(scene.groups)
+    d.group_shape_offset = _ptr(arrays["g_off"], C.c_uint32)
+    d.group_shape_count = _ptr(arrays["g_cnt"], C.c_uint32)
     d.group_shape_ids = _ptr(arrays["g_ids"], C.c_uint32)
-    d.total_group_shapes = len(g_ids)
-    d.group_fill_rule = _ptr(g_rule, C.c_uint32)
+    d.total_group_shapes = counts['group_shapes']
+    d.group_fill_rule = _ptr(arrays["g_rule"], C.c_uint32)
     d.group_shape_to_canvas = _ptr(arrays["g_s2c"], C.c_float)
     d.group_canvas_to_shape = _ptr(arrays["g_c2s"], C.c_float)
-    d.group_fill_paint = _ptr(g_fill, C.c_int32)
-    d.group_stroke_paint = _ptr(g_stroke, C.c_int32)
-    d.num_paints = len(p_kind)
+    d.group_fill_paint = _ptr(arrays["g_fill"], C.c_int32)
+    d.group_stroke_paint = _ptr(arrays["g_stroke"], C.c_int32)
+    d.num_paints = counts['paints']
     d.paint_kind = _ptr(arrays["p_kind"], C.c_uint32)
     d.paint_params = _ptr(arrays["p_params"], C.c_float)
     d.paint_stop_offset = _ptr(arrays["p_soff"], C.c_uint32)
     d.paint_stop_count = _ptr(arrays["p_scnt"], C.c_uint32)
     d.stop_offsets = _ptr(arrays["s_off"], C.c_float)
     d.stop_colors = _ptr(arrays["s_col"], C.c_float)
-    d.total_stops = len(s_off)
-    return PackedScene(d, arrays, paint_of, pt_off.tolist(), pt_cnt.tolist(), p_soff, p_scnt)
+    d.total_stops = counts['stops']
+    soff = arrays["p_soff"][: counts["paints"]].tolist()
+    scnt = arrays["p_scnt"][: counts["paints"]].tolist()
+    return PackedScene(d, arrays, paint_of, arrays["pt_off"].tolist(), arrays["pt_cnt"].tolist(), soff, scnt)
 
 
 class GradBuffers:
