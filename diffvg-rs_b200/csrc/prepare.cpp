@@ -88,49 +88,75 @@ struct Seg {
 };
 
 // Preorder median-split BVH (src/distance/bvh.rs:190-238) emitted with skip links.
-struct BvhOut {
-    std::vector<Box> bounds;
-    std::vector<int32_t> left, right, start, count;
-};
-template <typename BoundsOf>
-int32_t build_bvh(BvhOut& out, BoundsOf bounds_of, std::vector<int32_t>& idx, size_t start, size_t end) {
-    Box b = empty_box();
-    for (size_t i = start; i < end; ++i) grow(b, bounds_of(idx[i]));
-    size_t count = end - start;
-    int32_t node = (int32_t)out.bounds.size();
-    out.bounds.push_back(b);
-    out.left.push_back(-1);
-    out.right.push_back(-1);
-    out.start.push_back((int32_t)start);
-    out.count.push_back((int32_t)count);
-    if (count <= kLeafSize) return node;
-    int axis = (b.x1 - b.x0) >= (b.y1 - b.y0) ? 0 : 1;
-    std::stable_sort(idx.begin() + start, idx.begin() + end, [&](int32_t a, int32_t c) {
-        Box ba = bounds_of(a), bc = bounds_of(c);
-        float va = axis == 0 ? (ba.x0 + ba.x1) * 0.5f : (ba.y0 + ba.y1) * 0.5f;
-        float vc = axis == 0 ? (bc.x0 + bc.x1) * 0.5f : (bc.y0 + bc.y1) * 0.5f;
-        return va < vc;
-    });
-    size_t mid = start + count / 2;
-    int32_t l = build_bvh(out, bounds_of, idx, start, mid);
-    int32_t r = build_bvh(out, bounds_of, idx, mid, end);
-    out.left[node] = l;
-    out.right[node] = r;
-    out.count[node] = 0;
-    return node;
-}
-// Subtree sizes -> skip link = first node after the subtree (preorder layout).
-std::vector<int32_t> skip_links(const BvhOut& b) {
-    size_t n = b.bounds.size();
-    std::vector<int32_t> size(n, 1);
-    for (size_t i = n; i-- > 0;) {
-        if (b.left[i] >= 0) size[i] += size[b.left[i]];
-        if (b.right[i] >= 0) size[i] += size[b.right[i]];
+// One builder serves every path and group of a scene: its arrays keep their capacity
+// from one BVH to the next instead of being allocated per BVH.
+struct BvhBuilder {
+    std::vector<Box> item;                              // item bounds (filled by the caller)
+    std::vector<int32_t> idx;                           // item order; leaves are ranges of it
+    std::vector<Box> bounds;                            // per node
+    std::vector<int32_t> left, right, start, count, skip;
+    std::vector<float> cx, cy;                          // item centres: the split keys
+
+    void build() {
+        const size_t n = item.size();
+        idx.resize(n);
+        std::iota(idx.begin(), idx.end(), 0);
+        cx.resize(n);
+        cy.resize(n);
+        for (size_t i = 0; i < n; ++i) {
+            cx[i] = (item[i].x0 + item[i].x1) * 0.5f;
+            cy[i] = (item[i].y0 + item[i].y1) * 0.5f;
+        }
+        bounds.clear();
+        left.clear();
+        right.clear();
+        start.clear();
+        count.clear();
+        if (n) node(0, n);
+        // subtree sizes -> skip link = first node after the subtree (preorder layout)
+        const size_t nn = bounds.size();
+        skip.assign(nn, 1);
+        for (size_t k = nn; k-- > 0;) {
+            if (left[k] >= 0) skip[k] += skip[left[k]];
+            if (right[k] >= 0) skip[k] += skip[right[k]];
+        }
+        for (size_t k = 0; k < nn; ++k) skip[k] += (int32_t)k;
     }
-    std::vector<int32_t> skip(n);
-    for (size_t i = 0; i < n; ++i) skip[i] = (int32_t)i + size[i];
-    return skip;
-}
+
+  private:
+    int32_t node(size_t s, size_t e) {
+        Box b = empty_box();
+        for (size_t i = s; i < e; ++i) grow(b, item[idx[i]]);
+        const size_t n = e - s;
+        const int32_t id = (int32_t)bounds.size();
+        bounds.push_back(b);
+        left.push_back(-1);
+        right.push_back(-1);
+        start.push_back((int32_t)s);
+        count.push_back((int32_t)n);
+        if (n <= kLeafSize) return id;
+        // stable sort of the range by centre along the longer axis: ties keep their order
+        const float* key = (b.x1 - b.x0) >= (b.y1 - b.y0) ? cx.data() : cy.data();
+        if (n <= 64) {
+            for (size_t i = s + 1; i < e; ++i) {
+                const int32_t v = idx[i];
+                const float kv = key[v];
+                size_t j = i;
+                for (; j > s && kv < key[idx[j - 1]]; --j) idx[j] = idx[j - 1];
+                idx[j] = v;
+            }
+        } else {
+            std::stable_sort(idx.begin() + s, idx.begin() + e, [key](int32_t a, int32_t c) { return key[a] < key[c]; });
+        }
+        const size_t mid = s + n / 2;
+        const int32_t l = node(s, mid);
+        const int32_t r = node(mid, e);
+        left[id] = l;
+        right[id] = r;
+        count[id] = 0;
+        return id;
+    }
+};
 
 bool path_point(const dvg_scene_desc* d, uint32_t po, uint32_t pc, bool closed, size_t index, float* x, float* y) {
     if (pc == 0) return false;  // src/path_utils.rs:7-16
@@ -216,6 +242,8 @@ dvg_status prepare_scene(const dvg_scene_desc* d, HostScene* out, std::string* e
     h.s_stroke.assign(S, 0.0f);
     h.s_padmul.assign(S, 1.0f);
     std::vector<Box> shape_box(S, empty_box());
+    BvhBuilder bvh;          // reused by every path and group BVH below
+    std::vector<Seg> segs;   // one path's segments, reused from path to path
     for (uint32_t s = 0; s < S; ++s) {
         uint32_t kind = d->shape_kind[s];
         if (kind > DVG_SHAPE_ELLIPSE) {
@@ -281,7 +309,7 @@ dvg_status prepare_scene(const dvg_scene_desc* d, HostScene* out, std::string* e
             path_index = (int32_t)(h.p_info.size() / 8);
             h.p_shape.push_back((int32_t)s);
             // Segments in path order (src/distance/bvh.rs:255-364).
-            std::vector<Seg> segs;
+            segs.clear();
             size_t pid = 0;
             float dr = d->shape_stroke_width[s];
             for (uint32_t k = 0; k < cc; ++k) {
@@ -314,17 +342,16 @@ dvg_status prepare_scene(const dvg_scene_desc* d, HostScene* out, std::string* e
             int32_t node_off = (int32_t)(h.pn_meta.size() / 4);
             int32_t node_cnt = 0;
             if (!segs.empty()) {
-                std::vector<int32_t> idx(segs.size());
-                std::iota(idx.begin(), idx.end(), 0);
-                BvhOut bo;
-                build_bvh(bo, [&](int32_t i) { return segs[i].bounds; }, idx, 0, segs.size());
-                std::vector<int32_t> skip = skip_links(bo);
+                BvhBuilder& bo = bvh;
+                bo.item.clear();
+                for (const Seg& sg : segs) bo.item.push_back(sg.bounds);
+                bo.build();
                 int32_t leaf_base = (int32_t)h.pl_segs.size();
-                for (int32_t i : idx) h.pl_segs.push_back(seg_off + i);
+                for (int32_t i : bo.idx) h.pl_segs.push_back(seg_off + i);
                 for (size_t n = 0; n < bo.bounds.size(); ++n) {
                     const Box& b = bo.bounds[n];
                     h.pn_bounds.insert(h.pn_bounds.end(), {b.x0, b.y0, b.x1, b.y1});
-                    h.pn_meta.insert(h.pn_meta.end(), {node_off + skip[n], leaf_base + bo.start[n], bo.count[n],
+                    h.pn_meta.insert(h.pn_meta.end(), {node_off + bo.skip[n], leaf_base + bo.start[n], bo.count[n],
                                                        bo.right[n] >= 0 ? node_off + bo.right[n] : -1});
                 }
                 node_cnt = (int32_t)bo.bounds.size();
@@ -445,17 +472,16 @@ dvg_status prepare_scene(const dvg_scene_desc* d, HostScene* out, std::string* e
         int32_t node_off = (int32_t)(h.gn_meta.size() / 4), node_cnt = 0;
         Box root = empty_box();
         if (!with_bounds.empty()) {  // GroupBvh::build (src/distance/bvh.rs:156-187)
-            std::vector<int32_t> idx(with_bounds.size());
-            std::iota(idx.begin(), idx.end(), 0);
-            BvhOut bo;
-            build_bvh(bo, [&](int32_t i) { return shape_box[with_bounds[i]]; }, idx, 0, with_bounds.size());
-            std::vector<int32_t> skip = skip_links(bo);
+            BvhBuilder& bo = bvh;
+            bo.item.clear();
+            for (int32_t sid : with_bounds) bo.item.push_back(shape_box[sid]);
+            bo.build();
             int32_t leaf_base = (int32_t)h.gl_shapes.size();
-            for (int32_t i : idx) h.gl_shapes.push_back(with_bounds[i]);
+            for (int32_t i : bo.idx) h.gl_shapes.push_back(with_bounds[i]);
             for (size_t n = 0; n < bo.bounds.size(); ++n) {
                 const Box& b = bo.bounds[n];
                 h.gn_bounds.insert(h.gn_bounds.end(), {b.x0, b.y0, b.x1, b.y1});
-                h.gn_meta.insert(h.gn_meta.end(), {node_off + skip[n], leaf_base + bo.start[n], bo.count[n],
+                h.gn_meta.insert(h.gn_meta.end(), {node_off + bo.skip[n], leaf_base + bo.start[n], bo.count[n],
                                                    bo.right[n] >= 0 ? node_off + bo.right[n] : -1});
             }
             node_cnt = (int32_t)bo.bounds.size();
