@@ -23,7 +23,7 @@
 #define DVG_MINB_INT 2
 #endif
 #ifndef DVG_MINB_BND
-#define DVG_MINB_BND 6
+#define DVG_MINB_BND 8  // 64 registers: more warps for the two-sided edge evaluation outweigh its spills
 #endif
 #ifndef DVG_MINB_LEAN
 #define DVG_MINB_LEAN 4
