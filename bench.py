@@ -518,7 +518,7 @@ def main():
     # DRAM bytes (read + write) per launch from one ncu capture of this workload
     # (profiles/k_*_mixed512.md); only the default workload has a capture.
     # "interior" is k_interior_cached (the full kernel only takes samples without cached fragments).
-    ncu_traffic = {"interior": 40036608, "forward": 5965312, "boundary": 26230784} if args.workload == "mixed" else {}
+    ncu_traffic = {"interior": 40369408, "forward": 5965312, "boundary": 36529408} if args.workload == "mixed" else {}
     ncu_file = {"interior": "k_interior_cached", "forward": "k_forward", "boundary": "k_boundary_eval"}
     prof_json = {k: {"ms_per_step": v[0] / 3.0, "calls_per_step": v[1] / 3.0} for k, v in prof.items()}
 
