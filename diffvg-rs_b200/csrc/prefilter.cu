@@ -10,6 +10,16 @@
 // Built with -fmad=false like kernels.cu.
 #include "device.cuh"
 #include "kernels.cuh"
+// Minimum resident CTAs per SM of the prefiltered forward and interior kernels, by
+// measurement on B200 (mixed 512x512 scene, 4x4 spp): the forward at 4 (64 registers,
+// spilling) 42.0 -> 36.4 ms against 2; the interior at 1 (168 registers, no spills)
+// 64.7 -> 62.6 ms against the compiler's own choice of 128.
+#ifndef DVG_MINB_PF_FWD
+#define DVG_MINB_PF_FWD 4
+#endif
+#ifndef DVG_MINB_PF_INT
+#define DVG_MINB_PF_INT 1
+#endif
 
 namespace dvgb {
 
@@ -319,12 +329,12 @@ __device__ __forceinline__ void forward_prefilter_body(const DevScene& S, const 
     __syncthreads();
     flush_splat(S, tx, ty, ri, HW, sm, accum, wsum);
 }
-__global__ void __launch_bounds__(256, 2) k_forward_prefilter(DevScene S, SampleParams sp, float* accum, float* wsum,
+__global__ void __launch_bounds__(256, DVG_MINB_PF_FWD) k_forward_prefilter(DevScene S, SampleParams sp, float* accum, float* wsum,
                                                               unsigned* status) {
     extern __shared__ float sm[];
     forward_prefilter_body(S, sp, sp.tile_base + blockIdx.x, blockIdx.y, accum, wsum, status, sm);
 }
-__global__ void __launch_bounds__(256, 2) k_forward_prefilter_batch(const BatchEntry* __restrict__ B,
+__global__ void __launch_bounds__(256, DVG_MINB_PF_FWD) k_forward_prefilter_batch(const BatchEntry* __restrict__ B,
                                                                     const int* __restrict__ item_scene,
                                                                     unsigned* status) {
     extern __shared__ float sm[];
@@ -925,11 +935,11 @@ __device__ __forceinline__ void interior_prefilter_body(const DevScene& S, const
     }
 }
 
-__global__ void __launch_bounds__(256) k_interior_prefilter(DevScene S, SampleParams sp, const float* d_render,
+__global__ void __launch_bounds__(256, DVG_MINB_PF_INT) k_interior_prefilter(DevScene S, SampleParams sp, const float* d_render,
                                                             const float* wsum, GradPtrs G, unsigned* status) {
     interior_prefilter_body(S, sp, sp.tile_base + blockIdx.x, blockIdx.y, d_render, wsum, G, status);
 }
-__global__ void __launch_bounds__(256) k_interior_prefilter_batch(const BatchEntry* __restrict__ B,
+__global__ void __launch_bounds__(256, DVG_MINB_PF_INT) k_interior_prefilter_batch(const BatchEntry* __restrict__ B,
                                                                   const int* __restrict__ item_scene,
                                                                   unsigned* status) {
     const int item = blockIdx.x;
