@@ -119,6 +119,7 @@ struct dvg_context {
     uint32_t shard_t0 = 0, shard_t1 = 0;
     uint64_t shard_gen = 0;
     bool shard_frag = false;
+    dvg_tuning shard_tune{};  // the scene's launch shape when its fragment codes were written
 };
 
 struct dvg_scene {
@@ -476,6 +477,7 @@ dvg_status dvg_scene_upload(dvg_context* ctx, const dvg_scene_desc* desc, dvg_sc
     S.path_len = (const float*)(base + o_plen);
     sc->g_bbox = (const float4*)(base + o_g_bbox);
     S.g_bbox = sc->g_bbox;
+    S.status = ctx->status;
     // tile binning
     S.tiles_x = (S.width + TILE - 1) / TILE;
     S.tiles_y = (S.height + TILE - 1) / TILE;
@@ -978,6 +980,7 @@ dvg_status dvg_shard_forward(dvg_context* ctx, dvg_scene* scene, const dvg_rende
     ctx->shard_t1 = shard->tile_end;
     ctx->shard_gen = ctx->gen;
     ctx->shard_frag = frag;
+    ctx->shard_tune = scene->tune;
     return DVG_OK;
 }
 
@@ -1022,9 +1025,12 @@ dvg_status dvg_shard_backward(dvg_context* ctx, dvg_scene* scene, const dvg_rend
     if (!scene->dev.bg_image) G.d_background_image = nullptr;
     st = zero_grads(ctx, scene, G);
     if (st != DVG_OK) return st;
+    // The codes are laid out by the tuning's slot count and sample layout: a
+    // dvg_scene_set_tuning between the two calls makes them unusable.
     const bool frag = ctx->shard_frag && ctx->shard_scene == scene && ctx->shard_gen == ctx->gen &&
                       ctx->shard_t0 == shard->tile_begin && ctx->shard_t1 == shard->tile_end &&
-                      std::memcmp(&ctx->shard_opts, opts, sizeof(dvg_render_options)) == 0;
+                      std::memcmp(&ctx->shard_opts, opts, sizeof(dvg_render_options)) == 0 &&
+                      std::memcmp(&ctx->shard_tune, &scene->tune, sizeof(dvg_tuning)) == 0;
     return backward_core(ctx, scene, opts, bopts, d_render, nullptr, G, true, frag, shard, wsum);
 }
 

@@ -92,6 +92,7 @@ struct DevScene {
     int tiles_x, tiles_y;
     const int* tile_offsets;
     const int* tile_entries;
+    unsigned* status;  // the owning context's status word (ST_* bits), or null
 };
 
 // ------------------------------------------------------------------ small math
@@ -704,18 +705,27 @@ __device__ __forceinline__ bool cubic_cannot_beat(const SegGeom& s, float2 p, bo
 }
 
 // ------------------------------------------------------------------ path queries
+// Preorder walks with skip links move strictly forward: a node's skip link points
+// past its subtree and a descent goes to node + 1, so a walk ends after at most
+// the tree's node count.  A skip link that does not point forward (a corrupt
+// table) ends the walk and raises ST_BVH_LIMIT, which the host reports as
+// DVG_ERR_DEVICE_LIMIT, instead of looping.
+__device__ __forceinline__ int bvh_skip(const DevScene& S, int n, int skip) {
+    if (skip > n) return skip;
+    if (S.status) atomicOr(S.status, ST_BVH_LIMIT);
+    return 0x7fffffff;
+}
 // Walks the path's BVH (preorder with skip links).  Node tests are exactly the
 // crate's: ray test for winding (winding.rs:117-126), containment for strokes.
 __device__ __forceinline__ int winding_path(const DevScene& S, int path, float2 p) {
     int4 pi = __ldg(&S.p_info[2 * path]);
     int n = pi.z, end = pi.z + pi.w;
     int w = 0;
-    int guard = 0;
-    while (n < end && guard++ < (1 << 20)) {
+    while (n < end) {
         float4 b = __ldg(&S.pn_bounds[n]);
         int4 m = __ldg(&S.pn_meta[n]);
         if (p.y < b.y || p.y > b.w || p.x > b.z) {
-            n = m.x;
+            n = bvh_skip(S, n, m.x);
             continue;
         }
         if (m.z > 0) {
@@ -724,7 +734,7 @@ __device__ __forceinline__ int winding_path(const DevScene& S, int path, float2 
                 load_seg(S, __ldg(&S.pl_segs[k]), sg);
                 if (!ray_misses_segment(sg, p)) w += winding_segment(sg, p);
             }
-            n = m.x;
+            n = bvh_skip(S, n, m.x);
         } else {
             n = n + 1;
         }
@@ -747,12 +757,11 @@ __device__ __forceinline__ bool within_path_bvh(const DevScene& S, int path, flo
     const int pflags = __ldg(&S.p_info[2 * path + 1].w);
     bool approx = pflags & PF_APPROX;
     int n = pi.z, end = pi.z + pi.w;
-    int guard = 0;
-    while (n < end && guard++ < (1 << 20)) {
+    while (n < end) {
         float4 b = __ldg(&S.pn_bounds[n]);
         int4 m = __ldg(&S.pn_meta[n]);
         if (!(p.x >= b.x && p.x <= b.z && p.y >= b.y && p.y <= b.w)) {
-            n = m.x;
+            n = bvh_skip(S, n, m.x);
             continue;
         }
         if (m.z > 0) {
@@ -765,7 +774,7 @@ __device__ __forceinline__ bool within_path_bvh(const DevScene& S, int path, flo
                 CPRes c = seg_closest(sg, p, approx);
                 if (c.dist < seg_radius(sg, c.t) && !end_excluded(pflags, sidx - pi.x, pi.y, c.t)) return true;
             }
-            n = m.x;
+            n = bvh_skip(S, n, m.x);
         } else {
             n = n + 1;
         }
@@ -882,12 +891,11 @@ __device__ __forceinline__ bool group_within(const DevScene& S, int g, float2 lp
         return false;
     }
     int n = gb.x, end = gb.x + gb.y;
-    int guard = 0;
-    while (n < end && guard++ < (1 << 20)) {
+    while (n < end) {
         float4 b = __ldg(&S.gn_bounds[n]);
         int4 m = __ldg(&S.gn_meta[n]);
         if (!(lp.x >= b.x && lp.x <= b.z && lp.y >= b.y && lp.y <= b.w)) {
-            n = m.x;
+            n = bvh_skip(S, n, m.x);
             continue;
         }
         if (m.z > 0) {
@@ -902,7 +910,7 @@ __device__ __forceinline__ bool group_within(const DevScene& S, int g, float2 lp
                     return true;
                 }
             }
-            n = m.x;
+            n = bvh_skip(S, n, m.x);
         } else {
             n = n + 1;
         }
@@ -925,12 +933,11 @@ __device__ __forceinline__ bool group_inside(const DevScene& S, int g, float2 lp
         if (!(lp.x >= b.x && lp.x <= b.z && lp.y >= b.y && lp.y <= b.w)) return false;
     }
     int n = gb.x, end = gb.x + gb.y;
-    int guard = 0;
-    while (n < end && guard++ < (1 << 20)) {
+    while (n < end) {
         float4 b = __ldg(&S.gn_bounds[n]);
         int4 m = __ldg(&S.gn_meta[n]);
         if (!(lp.x >= b.x && lp.x <= b.z && lp.y >= b.y && lp.y <= b.w)) {
-            n = m.x;
+            n = bvh_skip(S, n, m.x);
             continue;
         }
         if (m.z > 0) {
@@ -938,7 +945,7 @@ __device__ __forceinline__ bool group_inside(const DevScene& S, int g, float2 lp
                 int s = __ldg(&S.gl_shapes[k]);
                 w += winding_shape(S, s, shape_local_dist(S, s, lp), true);
             }
-            n = m.x;
+            n = bvh_skip(S, n, m.x);
         } else {
             n = n + 1;
         }

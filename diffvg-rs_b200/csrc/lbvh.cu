@@ -8,7 +8,7 @@
 //   4. bounds bottom-up: the second child to arrive at a parent unions both.
 // Every step is integer work or exact min / max, and the codes use f32 arithmetic
 // without contraction, so the tree is bit-for-bit the one a CPU build of the same
-// steps produces (the oracle's lbvh build; tests/test_gpu_lbvh.py).
+// steps produces (the oracle's lbvh build; tests/test_lbvh.py).
 //
 // Layout: internal nodes 0 .. n-2 (root 0), leaves n-1 .. 2n-2 in sorted order;
 // children[i] = (left, right) node ids; leaf k holds box key[k] & 0xffffffff.

@@ -281,7 +281,10 @@ dvg_status dvg_eval_positions_backward(dvg_context* ctx, const dvg_scene_desc* d
  * larger canvases return DVG_ERR_INVALID_ARGUMENT and launch nothing.  All calls on
  * a device share that array (each call clears it first); calls that overlap on the
  * GPU race on it.  The first call on a device looks up the array's address (with
- * the device current); make that first call before any stream capture begins. */
+ * the device current); make that first call before any stream capture begins.
+ * The address is kept for the life of the process: after a cudaDeviceReset of
+ * that device (which rebuilds its context and the array) do not call this entry
+ * point again in the same process. */
 dvg_status dvg_render_device_noalloc(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
                                      float* out_rgba);
 

@@ -3784,57 +3784,92 @@ extern "C" int oracle_sample_premultiplied(const dvg_scene_desc* desc, const dvg
 // Forward image with the crate's GPU semantics: rasterize_weights_f32, rasterize_splat_f32
 // and resolve_splat_f32 (src/gpu/kernels/forward.rs:1505-1735, 294-334), with the early
 // outs of Renderer::render (src/renderer/renderer.rs:40-66).
-extern "C" int oracle_render(const dvg_scene_desc* desc, const dvg_render_options* opts, float* out) {
+//
+// oracle_render_window restricts the same computation to the pixels [x0,x1) x [y0,y1):
+// a pixel's weight and colour sums receive only the samples of pixels within
+// ceil(radius) of it, visited in increasing sample index as in the full render, so the
+// window's pixels come out bit for bit as in the full image.  `threads` > 1 evaluates
+// the per-sample colours on that many host threads; the weight and splat sums stay
+// serial in sample order (same result for any thread count).
+extern "C" int oracle_render_window(const dvg_scene_desc* desc, const dvg_render_options* opts, uint32_t x0,
+                                    uint32_t y0, uint32_t x1, uint32_t y1, int threads, float* out) {
     Scene sc = decode(desc);
     if (sc.w == 0 || sc.h == 0) return 0;
-    size_t npix = (size_t)sc.w * sc.h;
+    x1 = std::min<uint32_t>(x1, sc.w);
+    y1 = std::min<uint32_t>(y1, sc.h);
+    if (x0 >= x1 || y0 >= y1) return 0;
+    const int width = (int)sc.w, height = (int)sc.h;
+    const int ww = (int)(x1 - x0), wh = (int)(y1 - y0);
+    const size_t wpix = (size_t)ww * wh;
     if (sc.groups.empty()) {
-        for (size_t i = 0; i < npix; ++i)
-            if (sc.has_bg_img)
-                for (int k = 0; k < 4; ++k) out[4 * i + k] = sc.bg_img[4 * i + k];
-            else {
-                out[4 * i] = sc.bg.r;
-                out[4 * i + 1] = sc.bg.g;
-                out[4 * i + 2] = sc.bg.b;
-                out[4 * i + 3] = sc.bg.a;
+        for (int y = (int)y0; y < (int)y1; ++y)
+            for (int x = (int)x0; x < (int)x1; ++x) {
+                const size_t i = (size_t)y * width + x, o = (size_t)(y - (int)y0) * ww + (x - (int)x0);
+                if (sc.has_bg_img)
+                    for (int k = 0; k < 4; ++k) out[4 * o + k] = sc.bg_img[4 * i + k];
+                else {
+                    out[4 * o] = sc.bg.r;
+                    out[4 * o + 1] = sc.bg.g;
+                    out[4 * o + 2] = sc.bg.b;
+                    out[4 * o + 3] = sc.bg.a;
+                }
             }
         return 0;
     }
     SampleSpec sp = make_spec(opts);
     SceneBvh bvh = build_scene_bvh(sc);
-    std::vector<float> wimg((size_t)npix, 0.0f);
-    uint64_t total = (uint64_t)npix * sp.sx_n * sp.sy_n;
     int ri = to_i32(std::ceil(sc.filter_radius));
     if (ri < 0) ri = 0;
-    int width = (int)sc.w, height = (int)sc.h;
-    for (uint64_t idx = 0; idx < total; ++idx) {
-        V2 pt;
-        size_t pix;
-        sample_position(sc, sp, idx, &pt, &pix);
-        int x = (int)(pix % sc.w), y = (int)(pix / sc.w);
+    const uint64_t spp = (uint64_t)sp.sx_n * sp.sy_n;
+    // pixels whose samples can reach the window
+    const int ex0 = std::max(0, (int)x0 - ri), ey0 = std::max(0, (int)y0 - ri);
+    const int ex1 = std::min(width, (int)x1 + ri), ey1 = std::min(height, (int)y1 + ri);
+    const int ew = ex1 - ex0, eh = ey1 - ey0;
+    const uint64_t esamples = (uint64_t)ew * eh * spp;
+    auto sample_idx = [&](uint64_t k) {  // k-th sample of the extended window, in sample-index order
+        const uint64_t s = k % spp, p = k / spp;
+        const int x = ex0 + (int)(p % (uint64_t)ew), y = ey0 + (int)(p / (uint64_t)ew);
+        return ((uint64_t)y * width + x) * spp + s;
+    };
+    std::vector<V4> colors(esamples);
+    std::vector<V2> pts(esamples);
+    parallel_for(0, esamples, threads, [&](int, uint64_t lo, uint64_t hi) {
+        for (uint64_t k = lo; k < hi; ++k) {
+            V2 pt;
+            size_t pix;
+            sample_position(sc, sp, sample_idx(k), &pt, &pix);
+            pts[k] = pt;
+            colors[k] = sp.prefilter ? eval_premultiplied_prefiltered(sc, bvh, pt, sample_background(sc, pix))
+                                     : eval_premultiplied(sc, bvh, pt, sample_background(sc, pix));
+        }
+    });
+    auto in_window = [&](int xx, int yy) { return xx >= (int)x0 && yy >= (int)y0 && xx < (int)x1 && yy < (int)y1; };
+    std::vector<float> wimg(wpix, 0.0f);
+    for (uint64_t k = 0; k < esamples; ++k) {
+        const uint64_t p = k / spp;
+        const int x = ex0 + (int)(p % (uint64_t)ew), y = ey0 + (int)(p / (uint64_t)ew);
+        const V2 pt = pts[k];
         for (int dy = -ri; dy <= ri; ++dy)
             for (int dx = -ri; dx <= ri; ++dx) {
                 int xx = x + dx, yy = y + dy;
-                if (xx >= 0 && yy >= 0 && xx < width && yy < height) {
+                if (xx >= 0 && yy >= 0 && xx < width && yy < height && in_window(xx, yy)) {
                     float w = compute_filter_weight(sc.filter_type, sc.filter_radius, (float)xx + 0.5f - pt.x,
                                                     (float)yy + 0.5f - pt.y);
-                    if (w > 0.0f) wimg[(size_t)yy * width + xx] += w;
+                    if (w > 0.0f) wimg[(size_t)(yy - (int)y0) * ww + (xx - (int)x0)] += w;
                 }
             }
     }
-    std::vector<float> acc(npix * 4, 0.0f);
-    for (uint64_t idx = 0; idx < total; ++idx) {
-        V2 pt;
-        size_t pix;
-        sample_position(sc, sp, idx, &pt, &pix);
-        int x = (int)(pix % sc.w), y = (int)(pix / sc.w);
-        V4 c = sp.prefilter ? eval_premultiplied_prefiltered(sc, bvh, pt, sample_background(sc, pix))
-                            : eval_premultiplied(sc, bvh, pt, sample_background(sc, pix));
+    std::vector<float> acc(wpix * 4, 0.0f);
+    for (uint64_t k = 0; k < esamples; ++k) {
+        const uint64_t p = k / spp;
+        const int x = ex0 + (int)(p % (uint64_t)ew), y = ey0 + (int)(p / (uint64_t)ew);
+        const V2 pt = pts[k];
+        const V4 c = colors[k];
         for (int dy = -ri; dy <= ri; ++dy)
             for (int dx = -ri; dx <= ri; ++dx) {
                 int xx = x + dx, yy = y + dy;
-                if (xx >= 0 && yy >= 0 && xx < width && yy < height) {
-                    size_t b = (size_t)yy * width + xx;
+                if (xx >= 0 && yy >= 0 && xx < width && yy < height && in_window(xx, yy)) {
+                    size_t b = (size_t)(yy - (int)y0) * ww + (xx - (int)x0);
                     float ws = wimg[b];
                     if (ws > 0.0f) {
                         float w = compute_filter_weight(sc.filter_type, sc.filter_radius, (float)xx + 0.5f - pt.x,
@@ -3850,7 +3885,7 @@ extern "C" int oracle_render(const dvg_scene_desc* desc, const dvg_render_option
                 }
             }
     }
-    for (size_t i = 0; i < npix; ++i) {
+    for (size_t i = 0; i < wpix; ++i) {
         float r = sc.bg.r, g = sc.bg.g, b = sc.bg.b, a = sc.bg.a;
         if (wimg[i] > 0.0f) {
             r = acc[4 * i];
@@ -3869,6 +3904,10 @@ extern "C" int oracle_render(const dvg_scene_desc* desc, const dvg_render_option
         out[4 * i + 3] = a;
     }
     return 0;
+}
+
+extern "C" int oracle_render(const dvg_scene_desc* desc, const dvg_render_options* opts, float* out) {
+    return oracle_render_window(desc, opts, 0, 0, desc->width, desc->height, 1, out);
 }
 
 extern "C" int oracle_render_backward_ex(const dvg_scene_desc* desc, const dvg_render_options* opts,

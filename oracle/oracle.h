@@ -24,6 +24,11 @@ extern "C" {
 
 /* Forward image with the crate's GPU pipeline semantics (weights -> splat -> resolve). */
 int oracle_render(const dvg_scene_desc* desc, const dvg_render_options* opts, float* out_rgba);
+/* The same image restricted to pixels [x0,x1) x [y0,y1) (out: (x1-x0)*(y1-y0)*4 floats,
+ * row-major over the window), bit-identical to those pixels of oracle_render; the
+ * per-sample colours run on `threads` host threads. */
+int oracle_render_window(const dvg_scene_desc* desc, const dvg_render_options* opts, uint32_t x0, uint32_t y0,
+                         uint32_t x1, uint32_t y1, int threads, float* out_rgba);
 
 /* Per-sample premultiplied colour at canvas point (px,py) (eval_scene semantics). */
 int oracle_sample_premultiplied(const dvg_scene_desc* desc, const dvg_render_options* opts,

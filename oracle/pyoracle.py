@@ -52,6 +52,7 @@ def lib() -> C.CDLL:
         B = C.POINTER(BackwardOptionsC)
         fp = C.POINTER(C.c_float)
         L.oracle_render.argtypes = [D, R, fp]
+        L.oracle_render_window.argtypes = [D, R, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, fp]
         L.oracle_render_differentiated.argtypes = [D, R, fp]
         L.oracle_render_sdf.argtypes = [D, R, fp]
         L.oracle_lbvh_build.argtypes = [fp, C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(C.c_int32), fp]
@@ -87,6 +88,18 @@ def render(scene: Scene, options: RenderOptions) -> np.ndarray:
     o = render_options_c(options)
     lib().oracle_render(ps.ref(), C.byref(o), _fp(out))
     return out.reshape(int(scene.height), int(scene.width), 4)
+
+
+def render_window(scene: Scene, options: RenderOptions, x0: int, y0: int, x1: int, y1: int,
+                  threads: int = 0) -> np.ndarray:
+    """Pixels [x0,x1) x [y0,y1) of render() ([y1-y0, x1-x0, 4], bit-identical), the
+    per-sample colours on `threads` host threads (0: every core)."""
+    ps = pack_scene(scene)
+    x1, y1 = min(x1, int(scene.width)), min(y1, int(scene.height))
+    out = np.zeros(max(x1 - x0, 0) * max(y1 - y0, 0) * 4, np.float32)
+    o = render_options_c(options)
+    lib().oracle_render_window(ps.ref(), C.byref(o), x0, y0, x1, y1, threads or (os.cpu_count() or 1), _fp(out))
+    return out.reshape(max(y1 - y0, 0), max(x1 - x0, 0), 4)
 
 
 def render_differentiated(scene: Scene, options: RenderOptions) -> np.ndarray:

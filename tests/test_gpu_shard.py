@@ -84,6 +84,47 @@ def test_shards_sum_to_the_whole_step(scene):
         r.close()
 
 
+def test_tuning_change_between_shard_calls():
+    """dvg_scene_set_tuning between dvg_shard_forward and dvg_shard_backward: the
+    forward's fragment codes were laid out for the old slot count and sample layout,
+    so the backward must rebuild the fragments instead of reading them; its
+    gradients equal a fresh fused step under the new tuning."""
+    r = Renderer(0)
+    try:
+        sc = synth.mixed_scene(4, 96, 80, scale=0.1, size_scale=0.3)
+        opts = RenderOptions(samples_x=2, samples_y=2, seed=3, jitter=True, use_prefiltering=False)
+        nb = 5000
+        bo = BackwardOptions(boundary_samples=nb)
+        up = r.upload(sc)
+        tgt = torch.rand(sc.width * sc.height * 4, device="cuda")
+        tiles = up.tile_count()
+        npix = sc.width * sc.height
+        for before, after in (((1, 4, 8), (1, 4, 32)), ((1, 4, 16), (0, 4, 16)), ((0, 2, 32), (1, 8, 0))):
+            up.set_tuning(*after)
+            ref_img, _, ref_g = _full(up, opts, bo, tgt)
+            up.set_tuning(*before)
+            acc = torch.empty(npix * 5, device="cuda")
+            torch.cuda.synchronize()
+            up.shard_forward(opts, (0, tiles), acc.data_ptr(), acc.data_ptr() + npix * 16)
+            img = torch.empty(npix * 4, device="cuda")
+            d_render = torch.empty(npix * 4, device="cuda")
+            up.shard_resolve(acc.data_ptr(), acc.data_ptr() + npix * 16, img.data_ptr())
+            r.l2_device(img.data_ptr(), tgt.data_ptr(), npix * 4, d_render.data_ptr(), 0)
+            up.set_tuning(*after)
+            g = DeviceGrads(up.packed, "cuda")
+            torch.cuda.synchronize()
+            up.shard_backward(opts, bo, (0, tiles), (0, nb), d_render.data_ptr(), acc.data_ptr() + npix * 16, g)
+            torch.cuda.synchronize()
+            assert float(torch.max(torch.abs(img - ref_img))) <= 2e-6
+            for k, v in ref_g.tensors.items():
+                a, b = g.tensors[k].cpu().numpy(), v.cpu().numpy()
+                scale = float(np.max(np.abs(b))) if b.size else 0.0
+                assert float(np.max(np.abs(a - b))) <= 1e-4 * (scale + 1e-6) + 1e-6, (before, after, k)
+        up.close()
+    finally:
+        r.close()
+
+
 def test_shard_ranges_are_checked():
     from dvg.renderer import RenderError
 
