@@ -24,6 +24,18 @@
 
 namespace orc {
 
+// Work accounting for the compute roofline (built only into oracle/_build/liboracle_ops.so,
+// -DORACLE_COUNT_OPS; a no-op in the oracle proper).  OPS(n) adds the floating-point
+// operations of the straight-line block it follows: one per f32 or f64 add, subtract,
+// multiply, divide and square root, one per libm call (acos, cos, pow, sin, atan2);
+// negation, comparisons, abs, min / max and conversions count zero.
+#ifdef ORACLE_COUNT_OPS
+static thread_local uint64_t g_ops = 0;
+#define OPS(n) (g_ops += (uint64_t)(n))
+#else
+#define OPS(n) ((void)0)
+#endif
+
 static const float PI_F = 3.14159265358979323846f;       // core::f32::consts::PI
 static const float FRAC_PI_2_F = 1.57079632679489661923f;  // core::f32::consts::FRAC_PI_2
 static const float INF_F = std::numeric_limits<float>::infinity();
@@ -328,34 +340,41 @@ static bool solve_quadratic(double a, double b, double c, double t[2]) {
     if (std::fabs(a) < eps) {
         if (std::fabs(b) < eps) return false;
         double root = -c / b;
+        OPS(1);
         t[0] = root;
         t[1] = root;
         return true;
     }
     double discrim = b * b - 4.0 * a * c;
+    OPS(4);
     if (discrim < 0.0) return false;
     double root = std::sqrt(discrim);
+    OPS(1);
     if (std::fabs(root) < eps) {
         double r = -0.5 * b / a;
+        OPS(2);
         t[0] = r;
         t[1] = r;
         return true;
     }
     double q = (b < 0.0) ? -0.5 * (b - root) : -0.5 * (b + root);
+    OPS(2);
     if (std::fabs(q) < eps) {
         double inv = 0.5 / a;
         t[0] = (-b - root) * inv;
         t[1] = (-b + root) * inv;
+        OPS(5);
     } else {
         t[0] = q / a;
         t[1] = c / q;
+        OPS(2);
     }
     if (t[0] > t[1]) std::swap(t[0], t[1]);
     return true;
 }
 static double cbrt_ref(double x) {  // distance/utils.rs:115-123
-    if (x > 0.0) return std::pow(x, 1.0 / 3.0);
-    if (x < 0.0) return -std::pow(-x, 1.0 / 3.0);
+    if (x > 0.0) return OPS(1), std::pow(x, 1.0 / 3.0);
+    if (x < 0.0) return OPS(1), -std::pow(-x, 1.0 / 3.0);
     return 0.0;
 }
 static int solve_cubic(double a, double b, double c, double d, double t[3]) {
@@ -373,17 +392,20 @@ static int solve_cubic(double a, double b, double c, double d, double t[3]) {
     d = d / a;
     double q = (b * b - 3.0 * c) / 9.0;
     double r = (2.0 * b * b * b - 9.0 * b * c + 27.0 * d) / 54.0;
+    OPS(3 + 4 + 9 + 3);  // normalise, q, r, the discriminant test r*r < q*q*q
     if (r * r < q * q * q) {
         double theta = std::acos(r / std::sqrt(q * q * q));
         t[0] = -2.0 * std::sqrt(q) * std::cos(theta / 3.0) - b / 3.0;
         t[1] = -2.0 * std::sqrt(q) * std::cos((theta + 2.0 * M_PI) / 3.0) - b / 3.0;
         t[2] = -2.0 * std::sqrt(q) * std::cos((theta - 2.0 * M_PI) / 3.0) - b / 3.0;
+        OPS(5 + 7 + 8 + 8);
         return 3;
     }
     double a_root = (r > 0.0) ? -cbrt_ref(r + std::sqrt(r * r - q * q * q))
                               : cbrt_ref(-r + std::sqrt(r * r - q * q * q));
-    double b_root = (std::fabs(a_root) > 1.0e-6) ? q / a_root : 0.0;
+    double b_root = (std::fabs(a_root) > 1.0e-6) ? (OPS(1), q / a_root) : 0.0;
     t[0] = (a_root + b_root) - b / 3.0;
+    OPS(6 + 3);  // r*r - q*q*q, sqrt, +-r; (a + b) - b/3
     return 1;
 }
 
@@ -396,8 +418,10 @@ struct CP {  // (closest point, t, dist)
 static inline void distance_to_segment(V2 pt, V2 a, V2 b, float* dist, V2* cp, float* t) {
     V2 ab = b - a;  // curve.rs:10-21
     float denom = dot(ab, ab);
+    OPS(5);
     if (denom <= 1.0e-10f) {
         *dist = length(pt - a);
+        OPS(6);
         *cp = a;
         *t = 0.0f;
         return;
@@ -405,6 +429,7 @@ static inline void distance_to_segment(V2 pt, V2 a, V2 b, float* dist, V2* cp, f
     float tt = clampf(dot(pt - a, ab) / denom, 0.0f, 1.0f);
     V2 c = a + ab * tt;
     *dist = length(pt - c);
+    OPS(6 + 4 + 6);
     *cp = c;
     *t = tt;
 }
@@ -420,16 +445,19 @@ static void quadratic_closest_pt_approx(V2 p0, V2 p1, V2 p2, V2 pt, V2* cp_out, 
     gf = mk(gf.y, -gf.x);
     float t = 0.0f;
     float denom = dot(gf, gf);
+    OPS(6 + 3 + 4 + 4 + 3 + 6 + 10 + 2 + 3);
     if (denom > 1.0e-8f) {
         V2 pp = gf * (-f / denom);
         V2 d0p = b0 - pp;
         float ap = cross(d0p, d20);
         float bp = 2.0f * cross(d10, d0p);
         float denom2 = 2.0f * a + b + d;
-        if (std::fabs(denom2) > 1.0e-8f) t = clampf((ap + bp) / denom2, 0.0f, 1.0f);
+        OPS(3 + 2 + 3 + 4 + 3);
+        if (std::fabs(denom2) > 1.0e-8f) t = (OPS(2), clampf((ap + bp) / denom2, 0.0f, 1.0f));
     }
     float tt = 1.0f - t;
     *cp_out = p0 * (tt * tt) + p1 * (2.0f * tt * t) + p2 * (t * t);
+    OPS(1 + 14);
     *t_out = t;
 }
 static CP closest_point_quadratic(V2 pt, V2 p0, V2 p1, V2 p2, bool approx) {  // curve.rs:26-78
@@ -437,6 +465,7 @@ static CP closest_point_quadratic(V2 pt, V2 p0, V2 p1, V2 p2, bool approx) {  //
         V2 cp;
         float t;
         quadratic_closest_pt_approx(p0, p1, p2, pt, &cp, &t);
+        OPS(6);
         return CP{cp, t, length(pt - cp)};
     }
     float best_t = 0.0f;
@@ -458,6 +487,7 @@ static CP closest_point_quadratic(V2 pt, V2 p0, V2 p1, V2 p2, bool approx) {  //
     double b = 3.0 * (ax * bx + ay * by);
     double c = 2.0 * (bx * bx + by * by) + (ax * cx + ay * cy);
     double d = bx * cx + by * cy;
+    OPS(12 + 10 + 18);  // end-point distances, coefficients, the cubic's coefficients
     double roots[3] = {0, 0, 0};
     int num = solve_cubic(a, b, c, d, roots);
     for (int i = 0; i < num; ++i) {
@@ -467,6 +497,7 @@ static CP closest_point_quadratic(V2 pt, V2 p0, V2 p1, V2 p2, bool approx) {  //
             float tt = 1.0f - t32;
             V2 cp = (p0 * (tt * tt)) + (p1 * (2.0f * tt * t32)) + (p2 * (t32 * t32));
             float dist = length(pt - cp);
+            OPS(1 + 14 + 6);
             if (dist < best_dist) {
                 best_dist = dist;
                 best_pt = cp;
@@ -484,6 +515,7 @@ static CP closest_point_cubic_approx(V2 pt, V2 p0, V2 p1, V2 p2, V2 p3) {  // cu
     V2 best_pt = p0;
     float best_t = 0.0f;
     float best_dist = length(pt - p0);
+    OPS(6);
     for (int i = 1; i <= steps; ++i) {
         float t = (float)i * inv;
         float tt = 1.0f - t;
@@ -494,6 +526,7 @@ static CP closest_point_cubic_approx(V2 pt, V2 p0, V2 p1, V2 p2, V2 p3) {  // cu
         V2 cp;
         distance_to_segment(pt, prev, curr, &dist, &cp, &seg_t);
         float local_t = prev_t + seg_t * (t - prev_t);
+        OPS(10 + 14 + 3);
         if (dist < best_dist) {
             best_dist = dist;
             best_pt = cp;
@@ -524,7 +557,9 @@ static CP closest_point_cubic(V2 pt, V2 p0, V2 p1, V2 p2, V2 p3, bool approx) { 
     double dx = (double)(p0.x - pt.x);
     double dy = (double)(p0.y - pt.y);
     double a = 3.0 * (ax * ax + ay * ay);
+    OPS(12 + 28 + 4);  // end-point distances, coefficients, leading term
     if (std::fabs(a) < 1.0e-10) return CP{best_pt, best_t, best_dist};
+    OPS(32 + 5 + 16);  // b..f, their normalisation, the deflated cubic and -b/5
     double b = 5.0 * (ax * bx + ay * by);
     double c = 4.0 * (ax * cx + ay * cy) + 2.0 * (bx * bx + by * by);
     double d = 3.0 * ((bx * cx + by * cy) + (ax * dx + ay * dy));
@@ -563,6 +598,7 @@ static CP closest_point_cubic(V2 pt, V2 p0, V2 p1, V2 p2, V2 p3, bool approx) { 
         double upper = (j < num_intervals) ? std::fmin(intervals[j], 1.0) : 1.0;
         double lb = lower, ub = upper;
         double lb_eval = eval_poly(lb), ub_eval = eval_poly(ub);
+        OPS(19);
         if (lb_eval * ub_eval > 0.0) {
             lower = upper;
             continue;
@@ -572,9 +608,11 @@ static CP closest_point_cubic(V2 pt, V2 p0, V2 p1, V2 p2, V2 p3, bool approx) { 
             std::swap(lb_eval, ub_eval);
         }
         double t = 0.5 * (lb + ub);
+        OPS(2);
         for (int it = 0; it < 20; ++it) {
-            if (!(t >= lb && t <= ub)) t = 0.5 * (lb + ub);
+            if (!(t >= lb && t <= ub)) t = (OPS(2), 0.5 * (lb + ub));
             double value = eval_poly(t);
+            OPS(9);
             if (std::fabs(value) < 1.0e-5 || it == 19) break;
             if (value > 0.0)
                 ub = t;
@@ -582,6 +620,7 @@ static CP closest_point_cubic(V2 pt, V2 p0, V2 p1, V2 p2, V2 p3, bool approx) { 
                 lb = t;
             double derivative = eval_deriv(t);
             t -= value / derivative;
+            OPS(11 + 2);
         }
         if (t >= 0.0 && t <= 1.0) {
             float t32 = (float)t;
@@ -589,6 +628,7 @@ static CP closest_point_cubic(V2 pt, V2 p0, V2 p1, V2 p2, V2 p3, bool approx) { 
             V2 cp = (p0 * (tt * tt * tt)) + (p1 * (3.0f * tt * tt * t32)) +
                     (p2 * (3.0f * tt * t32 * t32)) + (p3 * (t32 * t32 * t32));
             float dist = length(pt - cp);
+            OPS(25 + 6);
             if (dist < best_dist) {
                 best_dist = dist;
                 best_pt = cp;
@@ -605,10 +645,13 @@ static CP closest_point_cubic(V2 pt, V2 p0, V2 p1, V2 p2, V2 p3, bool approx) { 
 static int winding_number_segment(uint8_t kind, V2 p0, V2 p1, V2 p2, V2 p3, V2 pt) {
     if (kind == 0) {
         float dy = p1.y - p0.y;
+        OPS(1);
         if (std::fabs(dy) <= 1.0e-8f) return 0;
         float t = (pt.y - p0.y) / dy;
+        OPS(2);
         if (t >= 0.0f && t <= 1.0f) {
             float tp = p0.x - pt.x + t * (p1.x - p0.x);
+            OPS(4);
             if (tp >= 0.0f) return dy > 0.0f ? 1 : -1;
         }
         return 0;
@@ -617,11 +660,13 @@ static int winding_number_segment(uint8_t kind, V2 p0, V2 p1, V2 p2, V2 p3, V2 p
         double a = (double)(p0.y - 2.0f * p1.y + p2.y);
         double b = (double)(-2.0f * p0.y + 2.0f * p1.y);
         double c = (double)(p0.y - pt.y);
+        OPS(7);
         double roots[2] = {0, 0};
         int num_roots = 0;
         if (std::fabs(a) < 1.0e-12) {
             if (std::fabs(b) > 1.0e-12) {
                 roots[0] = -c / b;
+                OPS(1);
                 num_roots = 1;
             }
         } else if (solve_quadratic(a, b, c, roots)) {
@@ -631,12 +676,15 @@ static int winding_number_segment(uint8_t kind, V2 p0, V2 p1, V2 p2, V2 p3, V2 p
         double ax = (double)(p0.x - 2.0f * p1.x + p2.x);
         double bx = (double)(-2.0f * p0.x + 2.0f * p1.x);
         double cx = (double)(p0.x - pt.x);
+        OPS(7);
         for (int i = 0; i < num_roots; ++i) {
             double t = roots[i];
             if (t >= 0.0 && t <= 1.0) {
                 double tp = ax * t * t + bx * t + cx;
+                OPS(5);
                 if (tp > 0.0) {
                     double deriv = 2.0 * a * t + b;
+                    OPS(3);
                     winding += deriv > 0.0 ? 1 : -1;
                 }
             }
@@ -648,19 +696,23 @@ static int winding_number_segment(uint8_t kind, V2 p0, V2 p1, V2 p2, V2 p3, V2 p
         double b = (double)(3.0f * p0.y - 6.0f * p1.y + 3.0f * p2.y);
         double c = (double)(-3.0f * p0.y + 3.0f * p1.y);
         double d = (double)(p0.y - pt.y);
+        OPS(14);
         double roots[3] = {0, 0, 0};
         int num_roots = solve_cubic(a, b, c, d, roots);
         double ax = (double)(-p0.x + 3.0f * p1.x - 3.0f * p2.x + p3.x);
         double bx = (double)(3.0f * p0.x - 6.0f * p1.x + 3.0f * p2.x);
         double cx = (double)(-3.0f * p0.x + 3.0f * p1.x);
         double dx = (double)(p0.x - pt.x);
+        OPS(14);
         int winding = 0;
         for (int i = 0; i < num_roots; ++i) {
             double t = roots[i];
             if (t >= 0.0 && t <= 1.0) {
                 double tp = ax * t * t * t + bx * t * t + cx * t + dx;
+                OPS(9);
                 if (tp > 0.0) {
                     double deriv = 3.0 * a * t * t + 2.0 * b * t + c;
+                    OPS(7);
                     winding += deriv > 0.0 ? 1 : -1;
                 }
             }
@@ -783,14 +835,17 @@ static V2 closest_point_ellipse(V2 c, V2 radius, V2 pt) {  // shape.rs:116-164
     dx = std::fabs(dx);
     dy = std::fabs(dy);
     float t = std::atan2(dy * rx, dx * ry);
+    OPS(2 + 3);
     const int max_iter = 20;
     const float tol = 1.0e-6f;
     for (int i = 0; i < max_iter; ++i) {
         float s = std::sin(t), co = std::cos(t);
         float g = rx * dx * s - ry * dy * co + (ry * ry - rx * rx) * s * co;
         float g_t = rx * dx * co + ry * dy * s + (ry * ry - rx * rx) * (co * co - s * s);
+        OPS(2 + 11 + 12);
         if (std::fabs(g_t) < 1.0e-12f) break;
         float next = clampf(t - g / g_t, 0.0f, FRAC_PI_2_F);
+        OPS(3);
         if (std::fabs(next - t) < tol) {
             t = next;
             break;
@@ -798,6 +853,7 @@ static V2 closest_point_ellipse(V2 c, V2 radius, V2 pt) {  // shape.rs:116-164
         t = next;
     }
     float s = std::sin(t), co = std::cos(t);
+    OPS(2 + 6);
     return mk(c.x + sign_x * rx * co, c.y + sign_y * ry * s);
 }
 static V2 closest_point_rect(V2 mn, V2 mx, V2 pt) {  // shape.rs:167-185
@@ -814,6 +870,7 @@ static float rect_signed_distance(V2 pt, V2 mn, V2 mx) {  // shape.rs:188-201
     float dy = std::fmax(std::fmax(mn.y - pt.y, 0.0f), pt.y - mx.y);
     float outside = std::sqrt(dx * dx + dy * dy);
     float inside = std::fmin(std::fmin(std::fmin(pt.x - mn.x, mx.x - pt.x), pt.y - mn.y), mx.y - pt.y);
+    OPS(4 + 4 + 4);
     return outside > 0.0f ? outside : -inside;
 }
 static float ellipse_signed_distance(V2 pt, V2 c, V2 radius) {  // shape.rs:204-212
@@ -823,6 +880,7 @@ static float ellipse_signed_distance(V2 pt, V2 c, V2 radius) {  // shape.rs:204-
     bool inside = (local.x / rx) * (local.x / rx) + (local.y / ry) * (local.y / ry) <= 1.0f;
     V2 closest = closest_point_ellipse(c, mk(rx, ry), pt);
     float dist = length(pt - closest);
+    OPS(2 + 7 + 6);
     return inside ? -dist : dist;
 }
 
@@ -972,10 +1030,10 @@ static SceneBvh build_scene_bvh(const Scene& sc) {  // bvh.rs:21-30
 
 // ---------------------------------------------------------------- closest / within (distance/closest.rs)
 static float seg_radius(const SegData& s, float t) {  // closest.rs:66-79
-    if (s.kind == 0) return s.r0 + t * (s.r1 - s.r0);
+    if (s.kind == 0) return OPS(3), s.r0 + t * (s.r1 - s.r0);
     float tt = 1.0f - t;
-    if (s.kind == 1) return tt * tt * s.r0 + 2.0f * tt * t * s.r1 + t * t * s.r2;
-    return tt * tt * tt * s.r0 + 3.0f * tt * tt * t * s.r1 + 3.0f * tt * t * t * s.r2 + t * t * t * s.r3;
+    if (s.kind == 1) return OPS(10), tt * tt * s.r0 + 2.0f * tt * t * s.r1 + t * t * s.r2;
+    return OPS(18), tt * tt * tt * s.r0 + 3.0f * tt * tt * t * s.r1 + 3.0f * tt * t * t * s.r2 + t * t * t * s.r3;
 }
 static CP seg_closest(const SegData& s, V2 pt, bool approx) {
     if (s.kind == 0) {
@@ -1151,6 +1209,7 @@ static bool within_distance_shape(const Shape& s, V2 pt, float r) {  // closest.
     V2 lp = xform_inv_dist(s.transform, pt);
     if (s.kind == DVG_SHAPE_CIRCLE) {
         float dist = length(lp - mk(s.prm[0], s.prm[1])) - std::fabs(s.prm[2]);
+        OPS(7);
         return std::fabs(dist) < r;
     }
     if (s.kind == DVG_SHAPE_ELLIPSE) {
@@ -1293,12 +1352,14 @@ static int winding_number_path_bvh(const PathBvh& pb, V2 pt) {  // winding.rs:73
 static int winding_number_shape(const Shape& s, const PathBvh* pb, V2 pt) {  // winding.rs:13-48
     if (s.kind == DVG_SHAPE_CIRCLE) {
         float r = std::fabs(s.prm[2]);
+        OPS(6);
         return length_sq(pt - mk(s.prm[0], s.prm[1])) < r * r ? 1 : 0;
     }
     if (s.kind == DVG_SHAPE_ELLIPSE) {
         float rx = std::fmax(std::fabs(s.prm[2]), 1.0e-6f);
         float ry = std::fmax(std::fabs(s.prm[3]), 1.0e-6f);
         float dx = (pt.x - s.prm[0]) / rx, dy = (pt.y - s.prm[1]) / ry;
+        OPS(7);
         return dx * dx + dy * dy < 1.0f ? 1 : 0;
     }
     if (s.kind == DVG_SHAPE_RECT) {
@@ -4381,36 +4442,92 @@ extern "C" int oracle_path_bvh(const dvg_scene_desc* desc, uint32_t shape, float
     return n;
 }
 
-extern "C" int oracle_count_segment_tests(const dvg_scene_desc* desc, const dvg_render_options* opts,
-                                          unsigned long long* out3) {
-    // out3[0..2]: fill ray-test passes per segment kind (line, quad, cubic);
-    // out3[3..5]: stroke padded-bounds hits per kind.
+// Work of one forward pass, for the compute roofline: every test the crate's BVH
+// queries reach when evaluated without early exits (is_inside_bvh, api.rs:259-309,
+// within_distance_bvh, api.rs:79-135), for every pixel sample of the options.  A shape
+// is reached when its group-space bounds (padded by the stroke radius, shape.rs:9-14)
+// contain the sample; a path segment when its padded bounds pass the +x ray test (fill,
+// winding.rs:117-126) or contain the sample (stroke, closest.rs:20-98).  Kinds: 0-2
+// fill line / quadratic / cubic segment, 3-5 stroke line / quadratic / cubic segment,
+// 6-8 fill circle / ellipse / rect, 9-11 stroke circle / ellipse / rect.  counts[k] =
+// tests of kind k; flops[k] = the floating-point operations the crate's arithmetic
+// executes for them (the winding solve, or the closest point plus radius), counted by
+// OPS().  Needs the counting build (-DORACLE_COUNT_OPS); returns -1 otherwise.
+extern "C" int oracle_count_work(const dvg_scene_desc* desc, const dvg_render_options* opts, int threads,
+                                 unsigned long long* counts, unsigned long long* flops) {
+    for (int i = 0; i < 12; ++i) counts[i] = flops[i] = 0;
+#ifndef ORACLE_COUNT_OPS
+    (void)desc;
+    (void)opts;
+    (void)threads;
+    return -1;
+#else
     Scene sc = decode(desc);
     SampleSpec sp = make_spec(opts);
-    for (int i = 0; i < 6; ++i) out3[i] = 0;
-    std::vector<PathBvh> pbs(sc.shapes.size());
-    std::vector<char> has(sc.shapes.size(), 0);
-    for (size_t i = 0; i < sc.shapes.size(); ++i) has[i] = build_path_bvh(sc.shapes[i], &pbs[i]);
-    uint64_t total = (uint64_t)sc.w * sc.h * sp.sx_n * sp.sy_n;
-    for (uint64_t idx = 0; idx < total; ++idx) {
-        V2 pt;
-        size_t pix;
-        sample_position(sc, sp, idx, &pt, &pix);
-        for (const Group& g : sc.groups) {
-            V2 lp = xform_pt(g.c2s, pt);
-            for (size_t si : g.shape_ids) {
-                if (si >= sc.shapes.size() || !has[si]) continue;
-                V2 spt = xform_inv_dist(sc.shapes[si].transform, lp);
-                for (const SegData& s : pbs[si].segments) {
-                    if (g.fill >= 0 && !(spt.y < s.bounds.min.y || spt.y > s.bounds.max.y || spt.x > s.bounds.max.x))
-                        out3[s.kind] += 1;
-                    if (g.stroke >= 0 && sc.shapes[si].stroke_width > 0.0f && s.bounds.contains(spt))
-                        out3[3 + s.kind] += 1;
+    SceneBvh bvh = build_scene_bvh(sc);
+    const uint64_t total = (uint64_t)sc.w * sc.h * sp.sx_n * sp.sy_n;
+    const int nt = threads > 1 ? threads : 1;
+    std::vector<std::vector<uint64_t>> tc(nt, std::vector<uint64_t>(24, 0));
+    parallel_for(0, total, nt, [&](int t, uint64_t lo, uint64_t hi) {
+        uint64_t* c = tc[t].data();
+        uint64_t* f = c + 12;
+        for (uint64_t idx = lo; idx < hi; ++idx) {
+            V2 pt;
+            size_t pix;
+            sample_position(sc, sp, idx, &pt, &pix);
+            for (size_t gi = 0; gi < sc.groups.size(); ++gi) {
+                const Group& g = sc.groups[gi];
+                if (g.fill < 0 && g.stroke < 0) continue;
+                const V2 lp = xform_pt(g.c2s, pt);
+                for (const BvhShape& bs : bvh.groups[gi].shapes) {
+                    if (!bs.bounds.contains(lp)) continue;
+                    const Shape& s = sc.shapes[bs.shape_index];
+                    const bool stroke = g.stroke >= 0 && s.stroke_width > 0.0f;
+                    if (s.kind == DVG_SHAPE_PATH) {
+                        if (!bs.has_path_bvh) continue;
+                        const V2 spt = xform_inv_dist(s.transform, lp);
+                        for (const SegData& seg : bs.path_bvh.segments) {
+                            const Bounds& b = seg.bounds;
+                            if (g.fill >= 0 && !(spt.y < b.min.y || spt.y > b.max.y || spt.x > b.max.x)) {
+                                g_ops = 0;
+                                winding_number_segment(seg.kind, seg.p0, seg.p1, seg.p2, seg.p3, spt);
+                                c[seg.kind] += 1;
+                                f[seg.kind] += g_ops;
+                            }
+                            if (stroke && b.contains(spt)) {
+                                g_ops = 0;
+                                const CP cp = seg_closest(seg, spt, bs.path_bvh.approx);
+                                seg_radius(seg, cp.t);
+                                c[3 + seg.kind] += 1;
+                                f[3 + seg.kind] += g_ops;
+                            }
+                        }
+                        continue;
+                    }
+                    const int k = s.kind == DVG_SHAPE_CIRCLE ? 0 : s.kind == DVG_SHAPE_ELLIPSE ? 1 : 2;
+                    if (g.fill >= 0) {
+                        g_ops = 0;
+                        winding_number_shape(s, nullptr, xform_inv_dist(s.transform, lp));
+                        c[6 + k] += 1;
+                        f[6 + k] += g_ops;
+                    }
+                    if (stroke) {
+                        g_ops = 0;
+                        within_distance_shape(s, lp, s.stroke_width);
+                        c[9 + k] += 1;
+                        f[9 + k] += g_ops;
+                    }
                 }
             }
         }
-    }
+    });
+    for (const auto& v : tc)
+        for (int i = 0; i < 12; ++i) {
+            counts[i] += v[i];
+            flops[i] += v[12 + i];
+        }
     return 0;
+#endif
 }
 
 // Bounded-sample forward + backward for CPU timing: `count` samples spread evenly

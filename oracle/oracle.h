@@ -94,8 +94,6 @@ void oracle_philox_floats(unsigned long long idx, unsigned int seed, float* out2
 int oracle_path_bvh(const dvg_scene_desc* desc, uint32_t shape, float* nodes, int node_cap,
                     int* indices, int index_cap, int* num_indices);
 
-/* Work units: number of (sample, path segment) pairs whose padded segment bounds
- * contain the sample in shape space, split by segment kind (line, quad, cubic). */
 /* Bounded-sample CPU forward + backward (timing workload): `count` samples spread
  * evenly over the sample sequence plus the proportional share of boundary samples,
  * on `threads` threads; times[0] = set-up seconds, times[1] = sample-loop seconds. */
@@ -103,8 +101,14 @@ unsigned long long oracle_fwd_bwd_sample(const dvg_scene_desc* desc, const dvg_r
                                          const dvg_backward_options* bopts, const float* d_render,
                                          unsigned long long count, int threads, double* times);
 
-int oracle_count_segment_tests(const dvg_scene_desc* desc, const dvg_render_options* opts,
-                               unsigned long long* out3);
+/* Work of one forward pass for the compute roofline: counts[12] tests reached by the
+ * crate's BVH queries without early exits (kinds 0-2 fill line / quadratic / cubic
+ * segment, 3-5 stroke segment, 6-8 fill circle / ellipse / rect, 9-11 stroke circle /
+ * ellipse / rect) and flops[12] the floating-point operations of those tests in the
+ * crate's arithmetic.  Only the counting build (liboracle_ops.so) counts; the oracle
+ * proper returns -1. */
+int oracle_count_work(const dvg_scene_desc* desc, const dvg_render_options* opts, int threads,
+                      unsigned long long* counts, unsigned long long* flops);
 
 #ifdef __cplusplus
 }

@@ -71,7 +71,6 @@ def lib() -> C.CDLL:
         L.oracle_pcg32_floats.argtypes = [C.c_ulonglong, C.c_ulonglong, C.c_int, fp]
         L.oracle_philox_floats.argtypes = [C.c_ulonglong, C.c_uint, fp]
         L.oracle_path_bvh.argtypes = [D, C.c_uint32, fp, C.c_int, C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int)]
-        L.oracle_count_segment_tests.argtypes = [D, R, C.POINTER(C.c_ulonglong)]
         L.oracle_fwd_bwd_sample.argtypes = [D, R, B, fp, C.c_ulonglong, C.c_int, C.POINTER(C.c_double)]
         L.oracle_fwd_bwd_sample.restype = C.c_ulonglong
         _lib = L
@@ -251,12 +250,28 @@ def path_bvh(scene: Scene, shape: int):
     return nodes[: 8 * n].reshape(-1, 8), idx[: ni.value]
 
 
-def count_segment_tests(scene: Scene, options: RenderOptions) -> np.ndarray:
+WORK_KINDS = ("fill_line", "fill_quad", "fill_cubic", "stroke_line", "stroke_quad", "stroke_cubic",
+              "fill_circle", "fill_ellipse", "fill_rect", "stroke_circle", "stroke_ellipse", "stroke_rect")
+_ops_lib: Optional[C.CDLL] = None
+
+
+def count_work(scene: Scene, options: RenderOptions, threads: int = 0):
+    """Forward-pass work for the compute roofline: {kind: (tests, flops)} from the
+    counting build of the oracle (liboracle_ops.so; see oracle_count_work)."""
+    global _ops_lib
+    if _ops_lib is None:
+        build()
+        _ops_lib = C.CDLL(os.path.join(_HERE, "_build", "liboracle_ops.so"))
+        _ops_lib.oracle_count_work.argtypes = [C.POINTER(SceneDesc), C.POINTER(RenderOptionsC), C.c_int,
+                                               C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)]
     ps = pack_scene(scene)
-    out = (C.c_ulonglong * 6)()
     o = render_options_c(options)
-    lib().oracle_count_segment_tests(ps.ref(), C.byref(o), out)
-    return np.array(list(out), np.uint64)
+    counts = (C.c_ulonglong * 12)()
+    flops = (C.c_ulonglong * 12)()
+    rc = _ops_lib.oracle_count_work(ps.ref(), C.byref(o), threads or (os.cpu_count() or 1), counts, flops)
+    if rc != 0:
+        raise RuntimeError("liboracle_ops.so was not built with operation counting")
+    return {k: (int(counts[i]), int(flops[i])) for i, k in enumerate(WORK_KINDS)}
 
 
 def fwd_bwd_sample(scene: Scene, options: RenderOptions, bopts: Optional[BackwardOptions], d_render: np.ndarray,
