@@ -19,6 +19,7 @@ no collective in the data path); timing is the max over ranks.
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import subprocess
@@ -47,16 +48,29 @@ def workload(name: str, seed: int):
                             "(128 cubic fills, 64 strokes, 32 circles, 32 ellipses), W*H boundary samples",
                    width=512, height=512, spp=16, shapes=256)
         target = synth.mixed_scene(seed + 1000)
-    elif name == "plain":
+        return sc, target, opts, BackwardOptions(boundary_samples=sc.width * sc.height), cfg
+    if name == "plain":
         sc = synth.plain_scene(seed)
         opts = synth.plain_options()
-        cfg = dict(workload="plain scene 256x256, 2x2 spp, box r=0.5, 16 closed cubic paths", width=256,
-                   height=256, spp=4, shapes=16)
-        target = synth.plain_scene(seed + 1000)
+        cfg = dict(workload="plain scene 256x256, 2x2 spp, box r=0.5, 16 closed cubic paths, target = the seed+1 "
+                            "scene, W*H*spp boundary samples", width=256, height=256, spp=4, shapes=16)
+        target = synth.plain_scene(seed + 1)
+    elif name == "adjoint":
+        sc = synth.adjoint_scene(seed)
+        opts = synth.adjoint_options()
+        cfg = dict(workload="adjoint-check scene 128x128, 4x4 spp, 4 filled cubic + 4 stroked quadratic paths, "
+                            "W*H*spp boundary samples", width=128, height=128, spp=16, shapes=8)
+        target = synth.adjoint_scene(seed + 1)
+    elif name == "large":
+        sc = synth.large_scene(seed)
+        opts = RenderOptions(samples_x=4, samples_y=4, seed=0, jitter=True, use_prefiltering=False)
+        cfg = dict(workload="large scene 1024x1024, 4x4 spp, 4096 closed cubic paths x 16 segments, 25% stroked, "
+                            "radial 3-stop fills, W*H*spp boundary samples", width=1024, height=1024, spp=16,
+                   shapes=4096)
+        target = synth.large_scene(seed + 7)
     else:
         raise SystemExit(f"unknown workload {name}")
-    bopts = BackwardOptions(boundary_samples=sc.width * sc.height)
-    return sc, target, opts, bopts, cfg
+    return sc, target, opts, BackwardOptions(), cfg
 
 
 class ClockSampler:
@@ -110,12 +124,12 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
-def cpu_baseline(sc, opts, bopts, target_img, img, seconds: float):
-    """CPU port of the crate's path (the oracle), bounded sample, all host threads."""
+def cpu_baseline(sc, opts, bopts, target_img, img, seconds: float, threads: int = 0):
+    """CPU port of the crate's path (the oracle), bounded sample, `threads` host threads (0: all)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
 
-    threads = os.cpu_count() or 1
+    threads = threads or os.cpu_count() or 1
     d_render = 2.0 * (img - target_img)
     total = sc.width * sc.height * opts.samples_x * opts.samples_y
     count = 4096
@@ -127,8 +141,167 @@ def cpu_baseline(sc, opts, bopts, target_img, img, seconds: float):
     t = loop + setup * n / total  # per-call set-up amortised over the sample's share of the step
     return {"value": n / t / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{n} of {total} pixel samples spread evenly over the image (+ the same fraction of the "
-                      f"{bopts.boundary_samples} boundary samples); set-up {setup:.2f}s amortised by that fraction",
+                      f"{bopts.boundary_samples or total} boundary samples); set-up {setup:.2f}s amortised by that "
+                      "fraction",
             "ms_per_step_extrapolated": t * total / n * 1e3}
+
+
+def source_digest() -> str:
+    """Digest of the library's kernel sources; ncu figures captured from other sources are stale."""
+    h = hashlib.sha256()
+    csrc = os.path.join(ROOT, "diffvg-rs_b200", "csrc")
+    for n in sorted(os.listdir(csrc)):
+        with open(os.path.join(csrc, n), "rb") as f:
+            h.update(n.encode())
+            h.update(f.read())
+    return h.hexdigest()[:16]
+
+
+def ncu_figures(workload: str):
+    """Per-kernel ncu counters of one step of `workload` (profiles/ncu_step_<workload>.json, see
+    ncu_import), whether they were captured from the current kernel sources, and the file."""
+    path = os.path.join(ROOT, "profiles", f"ncu_step_{workload}.json")
+    if not os.path.exists(path):
+        return {}, False, None
+    with open(path) as f:
+        d = json.load(f)
+    return d.get("kernels", {}), d.get("source_digest") == source_digest(), os.path.relpath(path, ROOT)
+
+
+NCU_STEP_METRICS = ("gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum,"
+                    "lts__t_sectors_op_red.sum,lts__t_sectors_op_atom.sum")
+
+
+def ncu_import(csv_path: str, workload: str) -> None:
+    """Per-kernel sums over the launches of one captured step, keyed by kernel name, with the digest of
+    the kernel sources they were captured from.  Capture (one GPU; warm-up outside the range):
+      ncu --clock-control none --nvtx --nvtx-include dvg_step/ --metrics <NCU_STEP_METRICS> --csv
+          --print-units base --log-file step.csv python bench.py --ncu-step --workload <w>"""
+    import csv
+
+    with open(csv_path) as f:
+        rows = list(csv.DictReader(line for line in f if line.startswith('"')))
+    names = {"gpu__time_duration.sum": "ns", "dram__bytes_read.sum": "dram_read", "dram__bytes_write.sum":
+             "dram_write", "lts__t_sectors_op_red.sum": "red_sectors", "lts__t_sectors_op_atom.sum": "atom_sectors"}
+    per = {}
+    for row in rows:
+        key = names.get(row["Metric Name"])
+        if key is None:
+            continue
+        kname = row["Kernel Name"].replace("void ", "").split("(")[0].replace("dvgb::", "")
+        per.setdefault(kname, {}).setdefault(row["ID"], {})[key] = float(row["Metric Value"].replace(",", ""))
+    kernels = {}
+    for kname, launches in per.items():
+        s = {k: sum(l.get(k, 0.0) for l in launches.values()) for k in names.values()}
+        kernels[kname] = {"launches": len(launches), "ms": s["ns"] / 1e6,
+                          "dram_bytes": int(s["dram_read"] + s["dram_write"]),
+                          "red_sectors": int(s["red_sectors"]), "atom_sectors": int(s["atom_sectors"])}
+    out = {"workload": workload, "source_digest": source_digest(),
+           "what": "one fused step (forward + L2 + backward) captured by ncu after warm-up, L2 flushed before it; "
+                   "per kernel, summed over its launches in the step; times are ncu's (serialised launches): "
+                   "compare shares, not absolutes",
+           "command": "ncu --clock-control none --nvtx --nvtx-include dvg_step/ --metrics " + NCU_STEP_METRICS +
+                      " --csv --print-units base --log-file step.csv python bench.py --ncu-step --workload "
+                      + workload + " --e2e-steps 0; python bench.py --ncu-import step.csv --workload " + workload,
+           "kernels": dict(sorted(kernels.items(), key=lambda kv: -kv[1]["ms"]))}
+    path = os.path.join(ROOT, "profiles", f"ncu_step_{workload}.json")
+    with open(path, "w") as f:
+        json.dump(out, f, indent=1)
+        f.write("\n")
+    print(f"wrote {os.path.relpath(path, ROOT)}: {len(kernels)} kernels")
+
+
+def compute_roofline(workload, prof, up, W, H, dev, clocks):
+    """Compute roofline of the forward kernel: the crate's arithmetic for every test its BVH queries
+    reach (profiles/roofline_work.json, counted by the oracle's counting build) over the kernel's
+    average CUDA-event launch time, against the FP32 issue rate (SMs x 128 lanes x max SM clock, one
+    unfused operation per lane per clock: the kernels are built without multiply-add contraction so
+    that their decisions match the crate's).  The HBM figure is kept as a secondary field."""
+    import torch
+
+    with open(os.path.join(ROOT, "profiles", "roofline_work.json")) as f:
+        work = json.load(f)["workloads"].get(workload)
+    ms_tot, calls = prof.get("forward", (0.0, 1))
+    avg_ms = ms_tot / max(calls, 1)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    mhz = clocks.get("sm_max_mhz") or 1965.0
+    peak = sms * 128 * mhz * 1e6 / 1e12
+    achieved = work["total_flops"] / (avg_ms / 1e3) / 1e12 if work and avg_ms > 0 else None
+    kernels, fresh, src = ncu_figures(workload)
+    fk = kernels.get("k_forward", {})
+    step_ms = sum(v[0] for v in prof.values())
+    # HBM view of the same kernel: image-sized accumulators and weights, scene tables once
+    npix = W * H
+    scene_bytes = sum(a.nbytes for a in up.packed.arrays.values())
+    alg_bytes = npix * (16 + 4) * 2 + scene_bytes
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    hbm_peak, hbm_src = 6650.0, "fallback"
+    if os.path.exists(peaks_path):
+        with open(peaks_path) as f:
+            hbm_peak, hbm_src = float(json.load(f).get("hbm_gbs", hbm_peak)), "measured"
+    hbm_achieved = alg_bytes / (avg_ms / 1e3) / 1e9 if avg_ms > 0 else None
+    return {
+        "bound": "fp32_issue", "kernel": "k_forward", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+        "frac": achieved / peak if achieved is not None else None,
+        "traffic": fk.get("dram_bytes") if fresh else None,
+        "traffic_source": (f"{src}: ncu dram__bytes_read.sum + dram__bytes_write.sum of its one launch in a step"
+                           if fresh and fk else "no ncu capture from the current kernel sources"),
+        "peak_source": f"nominal: {sms} SMs x 128 FP32 lanes x {mhz:.0f} MHz (max SM clock sampled during the run)",
+        "avg_launch_ms": avg_ms, "share_of_step": ms_tot / step_ms if step_ms else None,
+        "work": {"flops_per_launch": work["total_flops"] if work else None,
+                 "tests_per_launch": work["total_tests"] if work else None,
+                 "source": "profiles/roofline_work.json (python oracle/count_work.py)"},
+        "hbm": {"achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s", "peak_source": hbm_src,
+                "frac": hbm_achieved / hbm_peak if hbm_achieved else None, "algorithmic_bytes_per_launch": alg_bytes},
+        "note": "the FP32 figure counts the crate's arithmetic per test (a libm call as one operation) and none of "
+                "the per-sample jitter, transform, paint, compositing and splat work; the kernel skips tests the "
+                "crate runs (exact culling), and its root solves run in f64 as the crate's do",
+    }
+
+
+def l2_atomic_probe(dev) -> float:
+    """Measured rate of single-float atomic adds on this GPU: torch index_add_ of 2^26 values into 2^24
+    floats at random int32 indices (one L2 reduction per value, plus the 8 bytes of index and value it
+    reads), median of 5 timed runs, in G adds/s."""
+    import torch
+
+    n, m = 1 << 26, 1 << 24
+    g = torch.Generator(device=dev)
+    g.manual_seed(0)
+    idx = torch.randint(0, m, (n,), device=dev, dtype=torch.int32, generator=g)
+    src = torch.ones(n, device=dev)
+    dst = torch.zeros(m, device=dev)
+    for _ in range(2):
+        dst.index_add_(0, idx, src)
+    ts = []
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dst.index_add_(0, idx, src)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ts.append(e0.elapsed_time(e1))
+    del idx, src, dst
+    return n / (float(np.median(ts)) / 1e3) / 1e9
+
+
+def l2_atomic_summary(workload, prof, dev):
+    """L2 reduction sectors of one step (ncu, per kernel) against the measured atomic-add rate."""
+    kernels, fresh, src = ncu_figures(workload)
+    probe = l2_atomic_probe(dev)
+    out = {"probe_gadds_per_s": probe,
+           "probe": "torch index_add_ of 2^26 floats at random indices into 2^24 (one L2 reduction each)"}
+    if not fresh:
+        out["step"] = None
+        out["note"] = "no ncu capture from the current kernel sources"
+        return out
+    step_ms = sum(v[0] for v in prof.values()) / 3.0
+    per = {name: k.get("red_sectors", 0) + k.get("atom_sectors", 0) for name, k in kernels.items()}
+    sectors = sum(per.values())
+    rate = sectors / (step_ms / 1e3) / 1e9
+    out["step"] = {"sectors": sectors, "gsectors_per_s_over_step": rate, "frac_of_probe": rate / probe,
+                   "kernels": {k: v for k, v in per.items() if v > 0}, "source": src}
+    return out
 
 
 def large_fit(r, dev, lib_stream, steps, warmup, rank):
@@ -316,13 +489,14 @@ def run_reference(args):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
 
-    img = pyoracle.render(sc, opts)  # untimed inputs for the backward
-    tgt = pyoracle.render(target, opts)
+    # untimed inputs for the backward
+    img = pyoracle.render_window(sc, opts, 0, 0, sc.width, sc.height, args.cpu_threads)
+    tgt = pyoracle.render_window(target, opts, 0, 0, sc.width, sc.height, args.cpu_threads)
     vals = []
     for _ in range(args.warmup):
-        cpu_baseline(sc, opts, bopts, tgt, img, args.cpu_seconds / 4)
+        cpu_baseline(sc, opts, bopts, tgt, img, args.cpu_seconds / 4, args.cpu_threads)
     for _ in range(args.steps):
-        vals.append(cpu_baseline(sc, opts, bopts, tgt, img, args.cpu_seconds / 2))
+        vals.append(cpu_baseline(sc, opts, bopts, tgt, img, args.cpu_seconds / 2, args.cpu_threads))
     v = float(np.median([b["value"] for b in vals]))
     samples = cfg["width"] * cfg["height"] * cfg["spp"]
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
@@ -350,7 +524,15 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=5)
     ap.add_argument("--large-fit-steps", type=int, default=5)
     ap.add_argument("--shard-steps", type=int, default=3)
+    ap.add_argument("--cpu-threads", type=int, default=0, help="host threads of the CPU baseline (0: all)")
+    ap.add_argument("--ncu-step", action="store_true",
+                    help="run the warm-up steps and one step inside the NVTX range dvg_step, then exit")
+    ap.add_argument("--ncu-import", metavar="CSV",
+                    help="turn an ncu --csv --print-units base capture of one --ncu-step step into "
+                         "profiles/ncu_step_<workload>.json, then exit")
     args = ap.parse_args()
+    if args.ncu_import:
+        return ncu_import(args.ncu_import, args.workload)
     if args.impl == "reference":
         return run_reference(args)
 
@@ -394,6 +576,22 @@ def main():
         step()
     torch.cuda.synchronize(dev)
     warm_launches = r.launch_count - launches0
+
+    if args.ncu_step:
+        # exactly one step inside the NVTX range "dvg_step" (L2 flushed before it), for an ncu capture
+        # restricted to that range (ncu --nvtx --nvtx-include dvg_step/); no timing, no JSON line
+        with torch.cuda.stream(lib_stream):
+            flush.zero_()
+        torch.cuda.synchronize(dev)
+        torch.cuda.nvtx.range_push("dvg_step")
+        step()
+        torch.cuda.synchronize(dev)
+        torch.cuda.nvtx.range_pop()
+        print(f"ncu step of workload {args.workload}, kernel sources {source_digest()}", flush=True)
+        up.close()
+        tgt_up.close()
+        r.close()
+        return
 
     if world > 1:
         dist.barrier()
@@ -499,27 +697,9 @@ def main():
             batched["scenes_per_s_plain_loop"] = n / (batched["plain_ms_per_step"] / 1e3)
             batched["speedup"] = batched["plain_ms_per_step"] / batched["batched_ms_per_step"]
 
-    dominant = max(prof.items(), key=lambda kv: kv[1][0]) if prof else ("none", (0.0, 1))
-    name, (ms_tot, calls) = dominant
-    avg_ms = ms_tot / max(calls, 1)
-    npix = W * H
-    # algorithmic HBM bytes per launch of the dominant launcher (per-pixel image traffic + scene tables)
-    scene_bytes = sum(a.nbytes for a in up.packed.arrays.values())
-    alg_bytes = {"forward": npix * (16 + 4) * 2 + scene_bytes, "interior": npix * (16 + 4) + scene_bytes,
-                 "boundary": npix * (16 + 4) + scene_bytes + bopts.boundary_samples * 64 * 3}.get(
-        name, npix * 16 + scene_bytes)
-    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    peak = 6650.0
-    peak_src = "fallback"
-    if os.path.exists(peaks_path):
-        peak = float(json.load(open(peaks_path)).get("hbm_gbs", peak))
-        peak_src = "measured"
-    achieved = alg_bytes / (avg_ms / 1e3) / 1e9
-    # DRAM bytes (read + write) per launch from one ncu capture of this workload
-    # (profiles/k_*_mixed512.md); only the default workload has a capture.
-    # "interior" is k_interior_cached (the full kernel only takes samples without cached fragments).
-    ncu_traffic = {"interior": 40369408, "forward": 5965312, "boundary": 36529408} if args.workload == "mixed" else {}
-    ncu_file = {"interior": "k_interior_cached", "forward": "k_forward", "boundary": "k_boundary_eval"}
+    clock_summary = clocks.summary()
+    roofline = compute_roofline(args.workload, prof, up, W, H, dev, clock_summary)
+    roofline["l2_atomics"] = l2_atomic_summary(args.workload, prof, dev)
     prof_json = {k: {"ms_per_step": v[0] / 3.0, "calls_per_step": v[1] / 3.0} for k, v in prof.items()}
 
     line = {
@@ -531,22 +711,15 @@ def main():
                    "(256 MiB write outside the timed events)", "parallelism": f"weak, {world} independent scene(s)",
                    "launch_shape": {"sample_layout": tuning[0], "boundary_cell": tuning[1],
                                     "fragment_slots": tuning[2], "chosen_by": "dvg_scene_autotune"}},
-        "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": ncu_traffic.get(name), "peak_source": peak_src,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch, cold cache "
-                                       f"(profiles/{ncu_file.get(name, name)}_mixed512.md)"
-                                       if name in ncu_traffic else None,
-                     "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
-                     "note": "compute-bound path (f64 root solves, divergent BVH walks); HBM roofline reported "
-                             "as required, see profiles/ for the issue-slot view"},
+        "roofline": roofline,
         "kernel_ms_per_step": prof_json,
-        "gpu_launches": int(timed_launches), "clocks": clocks.summary(), "e2e": e2e,
+        "gpu_launches": int(timed_launches), "clocks": clock_summary, "e2e": e2e,
         "batched_vs_plain": batched, "large_fit": fit, "single_scene_sharded": sharded,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         img = out.view(H, W, 4).cpu().numpy()
         line["cpu_baseline"] = cpu_baseline(sc, opts, bopts, target.view(H, W, 4).cpu().numpy(), img,
-                                            args.cpu_seconds)
+                                            args.cpu_seconds, args.cpu_threads)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
