@@ -941,6 +941,20 @@ dvg_status dvg_scene_tile_count(const dvg_scene* scene, uint32_t* tiles) {
     return DVG_OK;
 }
 
+dvg_status dvg_scene_tile_groups(const dvg_scene* scene, uint32_t* groups, uint32_t n) {
+    if (!scene || !groups) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");
+    const uint32_t tiles = (uint32_t)(scene->dev.tiles_x * scene->dev.tiles_y);
+    if (n < tiles) return fail(DVG_ERR_INVALID_ARGUMENT, "buffer holds fewer entries than the scene has tiles");
+    if (tiles == 0) return DVG_OK;
+    CK(cudaSetDevice(scene->ctx->device));
+    std::vector<int> off(tiles + 1, 0);
+    CK(cudaMemcpyAsync(off.data(), scene->dev.tile_offsets, (tiles + 1) * sizeof(int), cudaMemcpyDeviceToHost,
+                       scene->ctx->stream));
+    CK(cudaStreamSynchronize(scene->ctx->stream));
+    for (uint32_t t = 0; t < tiles; ++t) groups[t] = (uint32_t)(off[t + 1] - off[t]);
+    return DVG_OK;
+}
+
 dvg_status dvg_shard_forward(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
                              const dvg_shard* shard, float* accum_rgba, float* wsum) {
     if (!ctx || !scene || !accum_rgba || !wsum) return fail(DVG_ERR_INVALID_ARGUMENT, "null argument");

@@ -129,11 +129,12 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.dvg_context_set_retain.restype = C.c_int
     Sh = C.POINTER(ShardC)
     L.dvg_scene_tile_count.argtypes = [vp, C.POINTER(C.c_uint32)]
+    L.dvg_scene_tile_groups.argtypes = [vp, C.POINTER(C.c_uint32), C.c_uint32]
     L.dvg_shard_forward.argtypes = [vp, vp, R, Sh, vp, vp]
     L.dvg_shard_resolve.argtypes = [vp, vp, vp, vp, vp]
     L.dvg_l2_device.argtypes = [vp, vp, vp, C.c_uint64, vp, vp]
     L.dvg_shard_backward.argtypes = [vp, vp, R, B, Sh, vp, vp, Gp]
-    for f in ("dvg_scene_tile_count", "dvg_shard_forward", "dvg_shard_resolve", "dvg_l2_device",
+    for f in ("dvg_scene_tile_count", "dvg_scene_tile_groups", "dvg_shard_forward", "dvg_shard_resolve", "dvg_l2_device",
               "dvg_shard_backward"):
         getattr(L, f).restype = C.c_int
     L.dvg_context_profile.argtypes = [vp, C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.POINTER(C.c_uint64),
@@ -321,6 +322,13 @@ class UploadedScene:
         n = C.c_uint32()
         _check(self.renderer.lib.dvg_scene_tile_count(self.handle, C.byref(n)))
         return int(n.value)
+
+    def tile_groups(self) -> np.ndarray:
+        """dvg_scene_tile_groups: groups binned to each tile (the per-tile work estimate)."""
+        n = self.tile_count()
+        out = np.zeros(max(n, 1), np.uint32)
+        _check(self.renderer.lib.dvg_scene_tile_groups(self.handle, out.ctypes.data_as(C.POINTER(C.c_uint32)), n))
+        return out[:n]
 
     def shard_forward(self, options: RenderOptions, tiles, accum_ptr: int, wsum_ptr: int) -> None:
         """dvg_shard_forward over tiles [begin, end) into zeroed device accumulators."""

@@ -319,6 +319,9 @@ typedef struct dvg_shard {
     uint64_t sample_begin, sample_end;
 } dvg_shard;
 dvg_status dvg_scene_tile_count(const dvg_scene* scene, uint32_t* tiles);
+/* Number of groups binned to each tile (row-major; groups[n], n >= the tile count), the
+ * per-tile work estimate for splitting the tiles by cost instead of by count.  Synchronises. */
+dvg_status dvg_scene_tile_groups(const dvg_scene* scene, uint32_t* groups, uint32_t n);
 /* Zeroes accum_rgba (W*H*4) and wsum (W*H) device buffers, then splats the samples of
  * the shard's tiles into them (pixels near the band's edges also receive the filter
  * splats of the neighbouring bands' samples: only the sums are complete).  With the

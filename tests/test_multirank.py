@@ -72,6 +72,28 @@ def test_shard_range_covers_everything():
             assert max(e - b for b, e in spans) - min(e - b for b, e in spans) <= 1
 
 
+def test_cost_range_covers_everything_and_balances():
+    import numpy as np
+
+    from dvg.shard import cost_range, shard_range
+
+    rng = np.random.default_rng(0)
+    for n in (0, 1, 7, 64, 257):
+        for world in (1, 2, 3, 8):
+            for costs in (rng.integers(1, 50, n), rng.pareto(1.5, n) + 1.0, np.zeros(n), np.ones(n)):
+                spans = [cost_range(list(costs), r, world) for r in range(world)]
+                assert spans[0][0] == 0 and spans[-1][1] == n
+                assert all(spans[i][1] == spans[i + 1][0] for i in range(world - 1))
+                assert all(b <= e for b, e in spans)
+                total = float(np.sum(costs))
+                if total > 0:
+                    # every rank's cost is within one unit's cost of an equal share
+                    for b, e in spans:
+                        assert abs(float(np.sum(costs[b:e])) - total / world) <= float(np.max(costs)) + 1e-9
+                else:
+                    assert spans == [shard_range(n, r, world) for r in range(world)]
+
+
 class _FakeShardScene:
     """Stands in for an uploaded scene on CPU: each shard call writes a value that
     names the rank into the buffers it is handed, so the test sees what the step
@@ -91,6 +113,9 @@ class _FakeShardScene:
 
     def tile_count(self):
         return 7
+
+    def tile_groups(self):  # uneven work: the first tile holds most of the groups
+        return [9, 0, 0, 1, 1, 1, 2]
 
     def shard_forward(self, options, tiles, accum_ptr, wsum_ptr):
         n = self.scene.width * self.scene.height
@@ -150,9 +175,10 @@ def test_single_scene_split_over_two_gloo_ranks():
         p.join(timeout=60)
         assert p.exitcode == 0
     (r0, c0, g0, i0), (r1, c1, g1, i1) = res
-    # tiles 7 -> [0, 4) + [4, 7); boundary samples 1001 -> [0, 501) + [501, 1001)
-    assert c0[0] == ("forward", (0, 4)) and c1[0] == ("forward", (4, 7))
-    assert c0[-1] == ("backward", (0, 4), (0, 501)) and c1[-1] == ("backward", (4, 7), (501, 1001))
+    # tiles split by cost (groups + 1 = 10,1,1,2,2,2,3: half of 21 falls in tile 1) -> [0, 1) + [1, 7);
+    # boundary samples 1001 -> [0, 501) + [501, 1001)
+    assert c0[0] == ("forward", (0, 1)) and c1[0] == ("forward", (1, 7))
+    assert c0[-1] == ("backward", (0, 1), (0, 501)) and c1[-1] == ("backward", (1, 7), (501, 1001))
     # the accumulators were summed before the resolve, the gradients after the backward
     assert c0[1] == c1[1] == ("resolve", 3.0, 30.0)
     assert [c[0] for c in c0] == ["forward", "resolve", "l2", "backward"]
