@@ -38,6 +38,7 @@ from dvg.shard import max_over_ranks, rank_seed, weak_scaling_rate  # noqa: E402
 
 METRIC = "fwd+bwd Msamples/s (ms/iter), plain single-scene launch loop on one B200"
 UNIT = "Msamples/s"
+LARGE_FIT_LR = 0.1  # Adam step on path points (pixels) and paint parameters of the large fitting loop
 
 
 def workload(name: str, seed: int):
@@ -304,11 +305,13 @@ def l2_atomic_summary(workload, prof, dev):
     return out
 
 
-def large_fit(r, dev, lib_stream, steps, warmup, rank):
+def large_fit(r, dev, lib_stream, steps, warmup, rank, lr=LARGE_FIT_LR):
     """Large fitting loop: 1024x1024, 4x4 spp, 4096 closed cubic paths of 16 segments
-    (25 % stroked, radial 3-stop fills, group and shape transforms); every iteration
-    is one CUDA-graph replay of forward + L2 + backward + Adam (lr 1e-2 on points) +
-    on-device scene re-preparation, with no host work between iterations."""
+    (25 % stroked, radial 3-stop fills, group and shape transforms) fitted to the render
+    of another seeded scene of the same structure; every iteration is one CUDA-graph
+    replay of forward + L2 + backward + Adam (on path points and paint parameters) +
+    on-device scene re-preparation, with no host work between iterations.  The loss of
+    every 50th iteration is read back (a host synchronisation between two replays)."""
     import torch
 
     sc = synth.large_scene(rank_seed(0, rank))
@@ -322,26 +325,29 @@ def large_fit(r, dev, lib_stream, steps, warmup, rank):
     torch.cuda.synchronize(dev)
     tu.close()
     tuning = batch.autotune()
-    batch.set_adam(1e-2, (0.9, 0.999), 1e-8, points=True)
-    for _ in range(warmup):
+    batch.set_adam(lr, (0.9, 0.999), 1e-8, points=True, paints=True)
+    batch.step(True)
+    traj = [(1, float(batch.losses()[0]))]  # iteration 1: the loss of the initial scene
+    for _ in range(warmup - 1):
         batch.step(True)
-    first = float(batch.losses()[0])
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(lib_stream)
-    for _ in range(steps):
+    for i in range(1, steps + 1):
         batch.step(True)
+        if i % 50 == 0 or i == steps:
+            traj.append((warmup + i, float(batch.losses()[0])))
     e1.record(lib_stream)
     torch.cuda.synchronize(dev)
     ms = e0.elapsed_time(e1) / steps
-    last = float(batch.losses()[0])
     samples = sc.width * sc.height * 16
     batch.close()
     up.close()
     return {"workload": "1024x1024, 4x4 spp, 4096 closed cubic paths x 16 segments, 25% stroked, radial 3-stop "
-                        "fills, W*H*spp boundary samples; fwd + L2 + bwd + Adam + re-preparation per graph replay",
+                        "fills, W*H*spp boundary samples, fitted to the render of another seeded scene; fwd + L2 + "
+                        f"bwd + Adam (lr {lr}, points and paint parameters) + re-preparation per graph replay",
             "iterations": steps, "warmup": warmup, "ms_per_iter": ms, "msamples_per_s": samples / (ms / 1e3) / 1e6,
-            "loss_after_warmup": first, "loss_last": last,
+            "loss_first": traj[0][1], "loss_last": traj[-1][1], "loss_trajectory": traj,
             "launch_shape": {"sample_layout": tuning[0], "boundary_cell": tuning[1], "fragment_slots": tuning[2]}}
 
 
@@ -432,6 +438,19 @@ def batched_vs_plain(r, dev, lib_stream, flush, scenes, steps, label):
     tuning = batch.autotune()
     t_plain = timed(plain_step)
     t_batch = timed(lambda: batch.step(True))
+    # What batching can remove from the plain loop: the time its stream is not running a kernel
+    # (launch latency and host work between the per-scene calls).  Kernel time from the library's
+    # per-launcher CUDA events over one plain loop; launches per scene from its launch counter.
+    torch.cuda.synchronize(dev)
+    l0 = r.launch_count
+    r.set_profiling(True)
+    r.profile(reset=True)
+    plain_step()
+    prof = r.profile(reset=True)
+    r.set_profiling(False)
+    launches_per_scene = (r.launch_count - l0) / count
+    kernel_ms = sum(v[0] for v in prof.values())
+    gap_ms = max(t_plain - kernel_ms, 0.0)
 
     # Full optimisation step (forward, L2, backward, Adam lr 1e-2 on path points).
     # Batched: Adam and the scene re-preparation run on device inside the graph.
@@ -467,6 +486,13 @@ def batched_vs_plain(r, dev, lib_stream, flush, scenes, steps, label):
            "batched_ms_per_step": t_batch, "plain_ms_per_step": t_plain,
            "scenes_per_s_batched_graph": count / (t_batch / 1e3), "scenes_per_s_plain_loop": count / (t_plain / 1e3),
            "msamples_per_s_batched": samples / (t_batch / 1e3) / 1e6, "speedup": t_plain / t_batch,
+           "plain_loop_accounting": {
+               "kernel_ms": kernel_ms, "not_in_a_kernel_ms": gap_ms, "launches_per_scene": launches_per_scene,
+               "amdahl_bound_speedup": t_plain / max(t_plain - gap_ms, 1e-9),
+               "what": "kernel_ms: sum of the library's per-launcher CUDA-event times over one plain loop; the "
+                       "rest of the loop's time is launch latency and host work between calls, all that one "
+                       "batched launch per stage can remove (besides filling the GPU better for small scenes), "
+                       "hence the bound plain / (plain - not_in_a_kernel)"},
            "optimisation_step": {
                "batched_graph_ms": t_batch_opt, "plain_loop_ms": t_plain_opt,
                "scenes_per_s_batched_graph": count / (t_batch_opt / 1e3),
@@ -522,7 +548,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-scenes", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=5)
-    ap.add_argument("--large-fit-steps", type=int, default=5)
+    ap.add_argument("--large-fit-steps", type=int, default=200)
     ap.add_argument("--shard-steps", type=int, default=3)
     ap.add_argument("--cpu-threads", type=int, default=0, help="host threads of the CPU baseline (0: all)")
     ap.add_argument("--ncu-step", action="store_true",
