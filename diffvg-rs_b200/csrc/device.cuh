@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include "prepare.hpp"  // ShapeFlags shared with the host preparation
+#include "winding_f32.cuh"
 
 namespace dvgb {
 
@@ -493,6 +494,10 @@ static __device__ __noinline__ int winding_segment_v(int kind, float a0, float a
             }
         }
         return w;
+    }
+    {  // the f32 solve decides whenever its margins prove the f64 one decides the same
+        const int w32 = winding_cubic_f32(q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], pt.x, pt.y);
+        if (w32 != WIND_UNSURE) return w32;
     }
     double a = (double)(-q[1] + 3.0f * q[3] - 3.0f * q[5] + q[7]);
     double b = (double)(3.0f * q[1] - 6.0f * q[3] + 3.0f * q[5]);

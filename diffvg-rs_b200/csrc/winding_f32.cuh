@@ -1,0 +1,112 @@
+// winding_f32.cuh — certified f32 winding contribution of a cubic segment.
+//
+// The crate computes the +x-ray crossings of a cubic segment in f64 (winding.rs:170-192:
+// solve_cubic on the y polynomial, then x(t) > px and the sign of y'(t) at every root
+// in [0, 1]).  This header computes the same crossings in f32 and returns them only
+// when margins prove that the f64 computation takes the same decisions; otherwise it
+// returns WIND_UNSURE and the caller runs the f64 computation.  The margins are ~100x
+// the error bound of the f32 path, derived below:
+//
+//  * the crate takes its cubic branch (|a| >= 1e-6) and the normalised cubic is well
+//    scaled: |a| >= 1e-3 and |a| >= max(|b|, |c|, |d|) / 16, so that |b/a|, |c/a|,
+//    |d/a| <= 16, q <= 34, |r| <= 203;
+//  * the number of real roots is the same in f32 and f64: |r^2 - q^3| exceeds
+//    1e-3 (r^2 + |q|^3) + 1e-4 (|r| + q^2) + 1e-6, while the f32 error of r^2 - q^3 is
+//    below 2.4e-5 |r| + 6e-6 q^2 (relative rounding 6e-8 on terms of at most 203 and
+//    34);
+//  * every root within 0.5 of [0, 1] is refined by two Newton steps on the f32
+//    polynomial, where |y'| must exceed 1e-2 (|a| + |b| + |c|) (the trigonometric or
+//    Cardano root is within ~5e-4 given the margin above; after two steps the root is
+//    within ~1e-5 of the exact one, as is the crate's f64 root); the last step must be
+//    below 1e-4; a refined root within 1e-3 of 0 or 1 is undecided (the crate's
+//    t in [0, 1] test is inclusive);
+//  * at a root in [0, 1], x(t) - px must exceed 1e-3 (1 + |px| + max |x_k|) in
+//    magnitude (the root error moves x(t) by at most 6e-5 max |x_k|) and y'(t) must
+//    exceed 1e-2 (|a| + |b| + |c|) in magnitude.
+// The coefficients a, b, c, d (and those of x) are the crate's f32 expressions,
+// evaluated in the same order without contraction, so both paths start from the same
+// numbers.  tests/test_winding_f32.py holds the decisions to the oracle's f64 ones on
+// random and adversarial segments.
+#pragma once
+
+#ifndef __CUDACC__
+#include <cmath>
+#ifndef __host__
+#define __host__
+#endif
+#ifndef __device__
+#define __device__
+#endif
+#endif
+
+namespace dvgb {
+
+constexpr int WIND_UNSURE = 0x7fff;
+
+__host__ __device__ inline int winding_cubic_f32(float x0, float y0, float x1, float y1, float x2, float y2, float x3,
+                                                 float y3, float px, float py) {
+    const float a = -y0 + 3.0f * y1 - 3.0f * y2 + y3;
+    const float b = 3.0f * y0 - 6.0f * y1 + 3.0f * y2;
+    const float c = -3.0f * y0 + 3.0f * y1;
+    const float d = y0 - py;
+    const float fa = fabsf(a);
+    const float mcoef = fmaxf(fmaxf(fabsf(b), fabsf(c)), fabsf(d));
+    if (!(fa >= 1.0e-3f) || !(fa * 16.0f >= mcoef)) return WIND_UNSURE;
+    const float B = b / a, C = c / a, D = d / a;
+    const float q = (B * B - 3.0f * C) / 9.0f;
+    const float r = (2.0f * B * B * B - 9.0f * B * C + 27.0f * D) / 54.0f;
+    const float q3 = q * q * q, r2 = r * r;
+    const float disc = r2 - q3;
+    if (!(fabsf(disc) > 1.0e-3f * (r2 + fabsf(q3)) + 1.0e-4f * (fabsf(r) + q * q) + 1.0e-6f)) return WIND_UNSURE;
+    float t[3];
+    int n;
+    if (disc < 0.0f) {  // three real roots (q > 0 here)
+        const float th = acosf(r / sqrtf(q3));
+        const float s = -2.0f * sqrtf(q);
+        t[0] = s * cosf(th / 3.0f) - B / 3.0f;
+        t[1] = s * cosf((th + 6.28318530717958648f) / 3.0f) - B / 3.0f;
+        t[2] = s * cosf((th - 6.28318530717958648f) / 3.0f) - B / 3.0f;
+        n = 3;
+    } else {
+        const float e = sqrtf(disc);
+        const float ar = r > 0.0f ? -cbrtf(r + e) : cbrtf(-r + e);
+        const float br = fabsf(ar) > 1.0e-6f ? q / ar : 0.0f;
+        t[0] = (ar + br) - B / 3.0f;
+        n = 1;
+    }
+    const float ax = -x0 + 3.0f * x1 - 3.0f * x2 + x3;
+    const float bx = 3.0f * x0 - 6.0f * x1 + 3.0f * x2;
+    const float cx = -3.0f * x0 + 3.0f * x1;
+    const float dx = x0 - px;
+    const float xm = fmaxf(fmaxf(fabsf(x0), fabsf(x1)), fmaxf(fabsf(x2), fabsf(x3)));
+    const float ex = 1.0e-3f * (1.0f + fabsf(px) + xm);
+    const float ed = 1.0e-2f * (fa + fabsf(b) + fabsf(c));
+    int w = 0;
+    for (int i = 0; i < n; ++i) {
+        float u = t[i];
+        if (!(u > -0.5f && u < 1.5f)) continue;  // far outside [0, 1]: no crossing either way
+        // two Newton steps on a u^3 + b u^2 + c u + d (|y'| > ed keeps them well defined)
+        float step = 0.0f, moved = 0.0f;
+        for (int k = 0; k < 2; ++k) {
+            const float f = ((a * u + b) * u + c) * u + d;
+            const float fp = (3.0f * a * u + 2.0f * b) * u + c;
+            if (!(fabsf(fp) > ed)) return WIND_UNSURE;  // a flat crossing near [0, 1]
+            step = f / fp;
+            u -= step;
+            moved += fabsf(step);
+        }
+        if (!(fabsf(step) < 1.0e-4f) || !(moved < 1.0e-2f)) return WIND_UNSURE;
+        if (u < -1.0e-3f || u > 1.0f + 1.0e-3f) continue;  // outside [0, 1] by the margin
+        if (u <= 1.0e-3f || u >= 1.0f - 1.0e-3f) return WIND_UNSURE;
+        const float tp = ((ax * u + bx) * u + cx) * u + dx;
+        if (!(fabsf(tp) > ex)) return WIND_UNSURE;
+        if (tp > 0.0f) {
+            const float dy = (3.0f * a * u + 2.0f * b) * u + c;
+            if (!(fabsf(dy) > ed)) return WIND_UNSURE;
+            w += dy > 0.0f ? 1 : -1;
+        }
+    }
+    return w;
+}
+
+}  // namespace dvgb
