@@ -1142,7 +1142,7 @@ struct dvg_batch {
     size_t total_pix4 = 0, total_pix = 0, total_grads = 0, max_pixels = 0;
     int items = 0, total_tiles = 0, max_ri = 0;
     uint64_t total_bsamples = 0;
-    DevBuf entries, item_scene, accum, wsum, image, target, d_render, loss, grads, bsamples, bkey, border, bcounts;
+    DevBuf entries, work, accum, wsum, image, target, d_render, loss, grads, bsamples, bkey, border, bcounts;
     DevBuf frag;  // per-scene fragment caches (forward -> interior)
     bool any_styled = false;  // some scene strokes with non-round joins or caps
     cudaGraph_t graph = nullptr;
@@ -1167,16 +1167,16 @@ dvg_status batch_enqueue(dvg_batch* b) {
     CK(cudaMemsetAsync(b->grads.ptr, 0, b->total_grads * sizeof(float), ctx->stream));
     const bool pre = b->opts.use_prefiltering != 0;
     if (pre)
-        ctx->launches += launch_forward_prefilter_batch(B, b->item_scene.as<int>(), b->items, b->max_ri, ctx->status,
+        ctx->launches += launch_forward_prefilter_batch(B, b->work.as<int2>(), b->items, b->max_ri, ctx->status,
                                                         ctx->stream);
     else
-        ctx->launches += launch_forward_batch(B, b->item_scene.as<int>(), b->items, b->max_ri, ctx->stream);
+        ctx->launches += launch_forward_batch(B, b->work.as<int2>(), b->items, b->max_ri, ctx->stream);
     ctx->launches += launch_pixels_batch(B, n, b->max_pixels, 0, ctx->stream);
     ctx->launches += launch_pixels_batch(B, n, b->max_pixels, 1, ctx->stream);
     if (pre)
-        ctx->launches += launch_interior_prefilter_batch(B, b->item_scene.as<int>(), b->items, ctx->status, ctx->stream);
+        ctx->launches += launch_interior_prefilter_batch(B, b->work.as<int2>(), b->items, ctx->status, ctx->stream);
     else
-        ctx->launches += launch_interior_batch(B, b->item_scene.as<int>(), b->items, ctx->status, ctx->stream);
+        ctx->launches += launch_interior_batch(B, b->work.as<int2>(), b->items, ctx->status, ctx->stream);
     if (!pre)
         ctx->launches += launch_boundary_batch(B, n, b->total_bsamples, b->total_tiles, (int)b->tune.boundary_cell,
                                                b->any_styled,
@@ -1243,7 +1243,14 @@ extern "C" dvg_status dvg_batch_create(dvg_context* ctx, dvg_scene* const* scene
         b->bopts.boundary_seed_from_options = 1;
     }
     const SampleParams sp = sample_params(opts);
-    std::vector<int> item_scene;
+    // Work items (scene, tile + tiles * sub-sample round), one CTA each, listed heaviest
+    // first: the hardware hands out CTAs in list order as SMs free up, so the longest
+    // items start first and the stage's tail is made of short ones.  Weight: the groups
+    // binned to the item's tile + 1 (its sampling and splat).
+    struct Item {
+        int weight, scene, local;
+    };
+    std::vector<Item> work;
     for (uint32_t i = 0; i < count; ++i) {
         dvg_scene* sc = scenes[i];
         if (!sc || sc->ctx != ctx) return fail(DVG_ERR_INVALID_ARGUMENT, "batch scene is null or from another context");
@@ -1276,7 +1283,11 @@ extern "C" dvg_status dvg_batch_create(dvg_context* ctx, dvg_scene* const* scene
         e.rng = (int)b->bopts.rng;
         e.bscale = (float)((double)e.nb / (double)((uint64_t)npix * spp));
         const int items = tiles * (int)spp;
-        for (int k = 0; k < items; ++k) item_scene.push_back((int)i);
+        std::vector<int> off(tiles + 1, 0);
+        CK(cudaMemcpyAsync(off.data(), S.tile_offsets, (tiles + 1) * sizeof(int), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        for (int k = 0; k < items; ++k) work.push_back(Item{off[k % tiles + 1] - off[k % tiles] + 1, (int)i, k});
         b->items += items;
         b->total_tiles += tiles;
         b->total_bsamples += e.nb;
@@ -1289,7 +1300,10 @@ extern "C" dvg_status dvg_batch_create(dvg_context* ctx, dvg_scene* const* scene
     CK(b->wsum.reserve(b->total_pix * sizeof(float)));
     CK(b->loss.reserve(count * sizeof(float)));
     CK(b->grads.reserve(std::max<size_t>(b->total_grads, 64) * sizeof(float)));
-    CK(b->item_scene.reserve(item_scene.size() * sizeof(int)));
+    std::stable_sort(work.begin(), work.end(), [](const Item& x, const Item& y) { return x.weight > y.weight; });
+    std::vector<int2> work2(work.size());
+    for (size_t k = 0; k < work.size(); ++k) work2[k] = make_int2(work[k].scene, work[k].local);
+    CK(b->work.reserve(work2.size() * sizeof(int2)));
     const uint64_t nbs = std::max<uint64_t>(b->total_bsamples, 1);
     CK(b->bsamples.reserve(nbs * sizeof(BSample)));
     CK(b->bkey.reserve(nbs * sizeof(int)));
@@ -1331,7 +1345,7 @@ extern "C" dvg_status dvg_batch_create(dvg_context* ctx, dvg_scene* const* scene
     CK(b->entries.reserve(count * sizeof(BatchEntry)));
     CK(cudaMemcpyAsync(b->entries.ptr, b->host_entries.data(), count * sizeof(BatchEntry), cudaMemcpyHostToDevice,
                        ctx->stream));
-    CK(cudaMemcpyAsync(b->item_scene.ptr, item_scene.data(), item_scene.size() * sizeof(int), cudaMemcpyHostToDevice,
+    CK(cudaMemcpyAsync(b->work.ptr, work2.data(), work2.size() * sizeof(int2), cudaMemcpyHostToDevice,
                        ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     *out = b.release();

@@ -244,11 +244,11 @@ __global__ void __launch_bounds__(256, DVG_MINB_FWD) k_forward(DevScene S, Sampl
 }
 // Batched forward: one flat grid over every (scene, tile, sub-sample) work item.
 __global__ void __launch_bounds__(256, DVG_MINB_FWD) k_forward_batch(const BatchEntry* __restrict__ B,
-                                                                     const int* __restrict__ item_scene) {
+                                                                     const int2* __restrict__ work) {
     extern __shared__ float sm[];
-    const int item = blockIdx.x;
-    const BatchEntry& E = B[item_scene[item]];
-    const int local = item - E.item_off;
+    const int2 wk = work[blockIdx.x];  // (scene, tile + tiles * sub-sample round)
+    const BatchEntry& E = B[wk.x];
+    const int local = wk.y;
     const int tiles = E.S.tiles_x * E.S.tiles_y;
     forward_body(E.S, E.sp, local % tiles, local / tiles, E.accum, E.wsum, sm);
 }
@@ -510,21 +510,21 @@ __global__ void __launch_bounds__(256, DVG_MINB_LEAN) k_interior_cached(DevScene
     interior_body<true>(S, sp, sp.tile_base + blockIdx.x, blockIdx.y, d_render, wsum, G, status);
 }
 __global__ void __launch_bounds__(256, DVG_MINB_INT) k_interior_batch(const BatchEntry* __restrict__ B,
-                                                                      const int* __restrict__ item_scene,
+                                                                      const int2* __restrict__ work,
                                                                       unsigned* status) {
-    const int item = blockIdx.x;
-    const BatchEntry& E = B[item_scene[item]];
-    const int local = item - E.item_off;
+    const int2 wk = work[blockIdx.x];  // (scene, tile + tiles * sub-sample round)
+    const BatchEntry& E = B[wk.x];
+    const int local = wk.y;
     const int tiles = E.S.tiles_x * E.S.tiles_y;
     interior_body<false>(E.S, E.sp, local % tiles, local / tiles, E.d_render, E.wsum, E.G, status);
 }
 __global__ void __launch_bounds__(256, DVG_MINB_LEAN) k_interior_cached_batch(const BatchEntry* __restrict__ B,
-                                                                              const int* __restrict__ item_scene,
+                                                                              const int2* __restrict__ work,
                                                                               unsigned* status) {
-    const int item = blockIdx.x;
-    const BatchEntry& E = B[item_scene[item]];
+    const int2 wk = work[blockIdx.x];  // (scene, tile + tiles * sub-sample round)
+    const BatchEntry& E = B[wk.x];
     if (!E.sp.frag) return;  // uniform per CTA
-    const int local = item - E.item_off;
+    const int local = wk.y;
     const int tiles = E.S.tiles_x * E.S.tiles_y;
     interior_body<true>(E.S, E.sp, local % tiles, local / tiles, E.d_render, E.wsum, E.G, status);
 }
@@ -1679,10 +1679,10 @@ int launch_finalize_background(const DevScene& S, const GradPtrs& G, cudaStream_
     return 1;
 }
 // Batched step launchers (one launch per stage for all scenes).
-int launch_forward_batch(const BatchEntry* B, const int* item_scene, int items, int max_ri, cudaStream_t stream) {
+int launch_forward_batch(const BatchEntry* B, const int2* work, int items, int max_ri, cudaStream_t stream) {
     const int hw = TILE + 2 * max_ri;
     size_t smem = max_ri <= MAX_SMEM_RI ? (size_t)hw * hw * 5 * sizeof(float) : 0;
-    k_forward_batch<<<items, 256, smem, stream>>>(B, item_scene);
+    k_forward_batch<<<items, 256, smem, stream>>>(B, work);
     return 1;
 }
 int launch_pixels_batch(const BatchEntry* B, int nscenes, size_t max_pixels, int which, cudaStream_t stream) {
@@ -1700,10 +1700,10 @@ int launch_pixels_batch(const BatchEntry* B, int nscenes, size_t max_pixels, int
     }
     return 1;
 }
-int launch_interior_batch(const BatchEntry* B, const int* item_scene, int items, unsigned* status,
+int launch_interior_batch(const BatchEntry* B, const int2* work, int items, unsigned* status,
                           cudaStream_t stream) {
-    k_interior_cached_batch<<<items, 256, 0, stream>>>(B, item_scene, status);
-    k_interior_batch<<<items, 256, 0, stream>>>(B, item_scene, status);
+    k_interior_cached_batch<<<items, 256, 0, stream>>>(B, work, status);
+    k_interior_batch<<<items, 256, 0, stream>>>(B, work, status);
     return 2;
 }
 int launch_boundary_batch(const BatchEntry* B, int nscenes, uint64_t total, int total_tiles, int cell, bool styled,

@@ -154,15 +154,16 @@ int launch_boundary(const DevScene& S, const BoundaryParams& bp, const float* d_
                     cudaStream_t stream);
 int launch_finalize_background(const DevScene& S, const GradPtrs& G, cudaStream_t stream);
 int launch_fill_background(const DevScene& S, float* out, cudaStream_t stream);
-// Batched launchers: B (device) holds one BatchEntry per scene; item_scene maps each
-// (scene, tile, sub-sample) work item to its scene.  which: 0 resolve, 1 L2, 2 background.
-int launch_forward_batch(const BatchEntry* B, const int* item_scene, int items, int max_ri, cudaStream_t stream);
-int launch_forward_prefilter_batch(const BatchEntry* B, const int* item_scene, int items, int max_ri,
+// Batched launchers: B (device) holds one BatchEntry per scene; work[i] = (scene, tile +
+// tiles * sub-sample round) is the i-th CTA's item, in any order (the batch lists the
+// heaviest tiles first).  which: 0 resolve, 1 L2, 2 background.
+int launch_forward_batch(const BatchEntry* B, const int2* work, int items, int max_ri, cudaStream_t stream);
+int launch_forward_prefilter_batch(const BatchEntry* B, const int2* work, int items, int max_ri,
                                    unsigned* status, cudaStream_t stream);
 int launch_pixels_batch(const BatchEntry* B, int nscenes, size_t max_pixels, int which, cudaStream_t stream);
-int launch_interior_batch(const BatchEntry* B, const int* item_scene, int items, unsigned* status,
+int launch_interior_batch(const BatchEntry* B, const int2* work, int items, unsigned* status,
                           cudaStream_t stream);
-int launch_interior_prefilter_batch(const BatchEntry* B, const int* item_scene, int items, unsigned* status,
+int launch_interior_prefilter_batch(const BatchEntry* B, const int2* work, int items, unsigned* status,
                                     cudaStream_t stream);
 int launch_boundary_batch(const BatchEntry* B, int nscenes, uint64_t total, int total_tiles, int cell, bool styled,
                           BSample* samples, int* key, int* counts, int* order, cudaStream_t stream);

@@ -342,12 +342,12 @@ __global__ void __launch_bounds__(256, DVG_MINB_PF_FWD) k_forward_prefilter(DevS
     forward_prefilter_body(S, sp, sp.tile_base + blockIdx.x, blockIdx.y, accum, wsum, status, sm);
 }
 __global__ void __launch_bounds__(256, DVG_MINB_PF_FWD) k_forward_prefilter_batch(const BatchEntry* __restrict__ B,
-                                                                    const int* __restrict__ item_scene,
+                                                                    const int2* __restrict__ work,
                                                                     unsigned* status) {
     extern __shared__ float sm[];
-    const int item = blockIdx.x;
-    const BatchEntry& E = B[item_scene[item]];
-    const int local = item - E.item_off;
+    const int2 wk = work[blockIdx.x];  // (scene, tile + tiles * sub-sample round)
+    const BatchEntry& E = B[wk.x];
+    const int local = wk.y;
     const int tiles = E.S.tiles_x * E.S.tiles_y;
     forward_prefilter_body(E.S, E.sp, local % tiles, local / tiles, E.accum, E.wsum, status, sm);
 }
@@ -947,11 +947,11 @@ __global__ void __launch_bounds__(256, DVG_MINB_PF_INT) k_interior_prefilter(Dev
     interior_prefilter_body(S, sp, sp.tile_base + blockIdx.x, blockIdx.y, d_render, wsum, G, status);
 }
 __global__ void __launch_bounds__(256, DVG_MINB_PF_INT) k_interior_prefilter_batch(const BatchEntry* __restrict__ B,
-                                                                  const int* __restrict__ item_scene,
+                                                                  const int2* __restrict__ work,
                                                                   unsigned* status) {
-    const int item = blockIdx.x;
-    const BatchEntry& E = B[item_scene[item]];
-    const int local = item - E.item_off;
+    const int2 wk = work[blockIdx.x];  // (scene, tile + tiles * sub-sample round)
+    const BatchEntry& E = B[wk.x];
+    const int local = wk.y;
     const int tiles = E.S.tiles_x * E.S.tiles_y;
     interior_prefilter_body(E.S, E.sp, local % tiles, local / tiles, E.d_render, E.wsum, E.G, status);
 }
@@ -971,16 +971,16 @@ int launch_interior_prefilter(const DevScene& S, const SampleParams& sp, const f
     return 1;
 }
 
-int launch_forward_prefilter_batch(const BatchEntry* B, const int* item_scene, int items, int max_ri,
+int launch_forward_prefilter_batch(const BatchEntry* B, const int2* work, int items, int max_ri,
                                    unsigned* status, cudaStream_t stream) {
     const int hw = TILE + 2 * max_ri;
     size_t smem = max_ri <= MAX_SMEM_RI ? (size_t)hw * hw * 5 * sizeof(float) : 0;
-    k_forward_prefilter_batch<<<items, 256, smem, stream>>>(B, item_scene, status);
+    k_forward_prefilter_batch<<<items, 256, smem, stream>>>(B, work, status);
     return 1;
 }
-int launch_interior_prefilter_batch(const BatchEntry* B, const int* item_scene, int items, unsigned* status,
+int launch_interior_prefilter_batch(const BatchEntry* B, const int2* work, int items, unsigned* status,
                                     cudaStream_t stream) {
-    k_interior_prefilter_batch<<<items, 256, 0, stream>>>(B, item_scene, status);
+    k_interior_prefilter_batch<<<items, 256, 0, stream>>>(B, work, status);
     return 1;
 }
 
