@@ -1807,18 +1807,24 @@ dvg_status autotune_loop(dvg_context* ctx, dvg_tuning* tune, bool try_slots, App
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
+    // a candidate's time: the median of three timed runs after one warm run
     auto time_of = [&](dvg_tuning t, float* ms) -> dvg_status {
         *tune = t;
         dvg_status st = apply();
         if (st != DVG_OK) return st;
         st = run();  // warm
         if (st != DVG_OK) return st;
-        CK(cudaEventRecord(e0, ctx->stream));
-        st = run();
-        if (st != DVG_OK) return st;
-        CK(cudaEventRecord(e1, ctx->stream));
-        CK(cudaEventSynchronize(e1));
-        CK(cudaEventElapsedTime(ms, e0, e1));
+        float runs[3];
+        for (int k = 0; k < 3; ++k) {
+            CK(cudaEventRecord(e0, ctx->stream));
+            st = run();
+            if (st != DVG_OK) return st;
+            CK(cudaEventRecord(e1, ctx->stream));
+            CK(cudaEventSynchronize(e1));
+            CK(cudaEventElapsedTime(&runs[k], e0, e1));
+        }
+        std::sort(runs, runs + 3);
+        *ms = runs[1];
         return DVG_OK;
     };
     const uint32_t slots0 = try_slots ? 16 : 0;
