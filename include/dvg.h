@@ -397,9 +397,10 @@ dvg_status dvg_batch_set_adam(dvg_batch* batch, const dvg_adam_options* opts);
 dvg_status dvg_batch_scene_params(dvg_batch* batch, uint32_t index, float* host_points, float* host_paint_params);
 
 /* Launch-shape tuning of an uploaded scene (see dvg_tuning).  dvg_scene_autotune times
- * dvg_fwd_bwd_l2_device on the scene with each warp layout and each boundary cell
- * (device target image, width*height*4 floats; the scene's own gradient buffers are
- * used as scratch), keeps the fastest for later calls and returns it.  Synchronises. */
+ * dvg_fwd_bwd_l2_device on the scene with each warp layout, each boundary cell and each
+ * fragment-cache size (device target image, width*height*4 floats; the scene's own
+ * gradient buffers are used as scratch; a candidate's time is the median of three runs
+ * after a warm one), keeps the fastest for later calls and returns it.  Synchronises. */
 dvg_status dvg_scene_set_tuning(dvg_scene* scene, const dvg_tuning* tuning);
 dvg_status dvg_scene_get_tuning(const dvg_scene* scene, dvg_tuning* tuning);
 dvg_status dvg_scene_autotune(dvg_context* ctx, dvg_scene* scene, const dvg_render_options* opts,
