@@ -1,6 +1,11 @@
-// winding_f32.cuh — certified f32 winding contribution of a cubic segment.
+// certified_f32.cuh — decisions the crate makes with f64 root solves, made in f32
+// whenever margins prove the f64 computation decides the same: the winding contribution
+// of a cubic segment (winding_cubic_f32) and the stroke test of a quadratic segment of
+// constant radius (within_quad_f32).  Both return *_UNSURE otherwise, and the caller
+// runs the f64 computation.  tests/test_winding_f32.py holds both to the oracle's f64
+// decisions on random and adversarial inputs.
 //
-// The crate computes the +x-ray crossings of a cubic segment in f64 (winding.rs:170-192:
+// Winding.  The crate computes the +x-ray crossings of a cubic segment in f64 (winding.rs:170-192:
 // solve_cubic on the y polynomial, then x(t) > px and the sign of y'(t) at every root
 // in [0, 1]).  This header computes the same crossings in f32 and returns them only
 // when margins prove that the f64 computation takes the same decisions; otherwise it
@@ -107,6 +112,78 @@ __host__ __device__ inline int winding_cubic_f32(float x0, float y0, float x1, f
         }
     }
     return w;
+}
+
+// Stroke test of a quadratic segment with the same radius r at its three control points
+// (closest.rs:20-98 with closest_point_quadratic, curve.rs:26-78): the crate keeps the
+// closest of p0, p2 and the curve points at the roots in [0, 1] of the cubic
+// A t^3 + B t^2 + C t + D (the derivative of the squared distance, solved in f64) and
+// tests dist < r(t) (r(t) = r up to rounding).  Here: the same coefficients in f32, the
+// same root formulas, one Newton step, every root clamped to [0, 1] (a root just outside
+// gives the end point's distance, which the crate has as a candidate anyway), and the
+// smallest candidate distance d.  Decided when |d - r| > 1e-3 (1 + |p| + max |p_k| + r):
+// the candidates agree with the crate's up to the root error (~1e-4) times |B'| (at most
+// twice the control polygon's extent), and the distance is stationary at interior
+// roots.  Same scaling and discriminant margins as the winding (the crate's cubic
+// branch, |A| >= 1e-6; a well-scaled normalised cubic; a root count that f32 and f64
+// agree on).
+constexpr int WITHIN_UNSURE = 2;
+
+__host__ __device__ inline int within_quad_f32(float x0, float y0, float x1, float y1, float x2, float y2, float r,
+                                               float px, float py) {
+    const float ax = x0 - 2.0f * x1 + x2, ay = y0 - 2.0f * y1 + y2;
+    const float bx = -x0 + x1, by = -y0 + y1;
+    const float cx = x0 - px, cy = y0 - py;
+    const float A = ax * ax + ay * ay;
+    const float B = 3.0f * (ax * bx + ay * by);
+    const float C = 2.0f * (bx * bx + by * by) + (ax * cx + ay * cy);
+    const float D = bx * cx + by * cy;
+    const float mcoef = fmaxf(fmaxf(fabsf(B), fabsf(C)), fabsf(D));
+    if (!(A >= 1.0e-3f) || !(A * 16.0f >= mcoef)) return WITHIN_UNSURE;
+    const float Bn = B / A, Cn = C / A, Dn = D / A;
+    const float q = (Bn * Bn - 3.0f * Cn) / 9.0f;
+    const float rr = (2.0f * Bn * Bn * Bn - 9.0f * Bn * Cn + 27.0f * Dn) / 54.0f;
+    const float q3 = q * q * q, r2 = rr * rr;
+    const float disc = r2 - q3;
+    if (!(fabsf(disc) > 1.0e-3f * (r2 + fabsf(q3)) + 1.0e-4f * (fabsf(rr) + q * q) + 1.0e-6f)) return WITHIN_UNSURE;
+    float t[3];
+    int n;
+    if (disc < 0.0f) {
+        const float th = acosf(rr / sqrtf(q3));
+        const float s = -2.0f * sqrtf(q);
+        t[0] = s * cosf(th / 3.0f) - Bn / 3.0f;
+        t[1] = s * cosf((th + 6.28318530717958648f) / 3.0f) - Bn / 3.0f;
+        t[2] = s * cosf((th - 6.28318530717958648f) / 3.0f) - Bn / 3.0f;
+        n = 3;
+    } else {
+        const float e = sqrtf(disc);
+        const float ar = rr > 0.0f ? -cbrtf(rr + e) : cbrtf(-rr + e);
+        const float br = fabsf(ar) > 1.0e-6f ? q / ar : 0.0f;
+        t[0] = (ar + br) - Bn / 3.0f;
+        n = 1;
+    }
+    const float d0x = px - x0, d0y = py - y0, d2x = px - x2, d2y = py - y2;
+    float d = fminf(sqrtf(d0x * d0x + d0y * d0y), sqrtf(d2x * d2x + d2y * d2y));
+    for (int i = 0; i < n; ++i) {
+        float u = t[i];
+        if (!(u > -0.5f && u < 1.5f)) continue;  // far outside [0, 1]: not a candidate either way
+        const float fp = (3.0f * A * u + 2.0f * B) * u + C;
+        if (fabsf(fp) > 0.0f) {
+            const float step = (((A * u + B) * u + C) * u + D) / fp;
+            if (fabsf(step) < 0.25f) u -= step;
+        }
+        u = fminf(fmaxf(u, 0.0f), 1.0f);
+        const float tt = 1.0f - u;
+        const float w0 = tt * tt, w1 = 2.0f * tt * u, w2 = u * u;
+        const float ex = (x0 * w0 + x1 * w1) + x2 * w2 - px, ey = (y0 * w0 + y1 * w1) + y2 * w2 - py;
+        d = fminf(d, sqrtf(ex * ex + ey * ey));
+    }
+    const float pm = fmaxf(fmaxf(fmaxf(fabsf(x0), fabsf(y0)), fmaxf(fabsf(x1), fabsf(y1))),
+                           fmaxf(fabsf(x2), fabsf(y2)));
+    const float margin = 1.0e-3f * (1.0f + fmaxf(fabsf(px), fabsf(py)) + pm + r);
+    if (d < r - margin) return 1;
+    if (d > r + margin) return 0;
+    return WITHIN_UNSURE;
 }
 
 }  // namespace dvgb

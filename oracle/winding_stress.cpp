@@ -1,11 +1,11 @@
 // winding_stress.cpp — test infrastructure: the certified f32 cubic winding of the
-// library (diffvg-rs_b200/csrc/winding_f32.cuh) against the oracle's restatement of
+// library (diffvg-rs_b200/csrc/certified_f32.cuh) against the oracle's restatement of
 // the crate's f64 computation (winding_number_segment, winding.rs:170-192), on random
 // and adversarial segments.  Built into oracle/_build/libwinding_stress.so by the
 // Makefile; driven by tests/test_winding_f32.py.
 #include "oracle.cpp"
 
-#include "../diffvg-rs_b200/csrc/winding_f32.cuh"
+#include "../diffvg-rs_b200/csrc/certified_f32.cuh"
 
 namespace {
 struct SplitMix {
@@ -92,6 +92,57 @@ extern "C" void winding_stress(int mode, uint64_t seed, uint64_t n, unsigned lon
         const int fast = dvgb::winding_cubic_f32(p[0].x, p[0].y, p[1].x, p[1].y, p[2].x, p[2].y, p[3].x, p[3].y, q.x, q.y);
         out[0] += 1;
         if (fast != dvgb::WIND_UNSURE) {
+            out[1] += 1;
+            if (fast != ref) out[2] += 1;
+        }
+    }
+}
+
+// The certified f32 stroke test of a quadratic segment (within_quad_f32) against the
+// oracle's closest_point_quadratic (curve.rs:26-78) and the radius test (closest.rs:66-79).
+// mode 0: control points uniform in [-64, 64]^2, radius U[0.5, 8], query points at
+//         distance r + 10^U[-6, 1] (random sign) from a random curve point's normal;
+// mode 1: nearly straight quadratics (p1 on the chord plus 10^U[-7, 0]);
+// mode 2: degenerate ones (p1 = p0, p1 = p2, p0 = p2);
+// mode 3: coordinates scaled up to 4096;
+// mode 4: the tests a scene makes: query points uniform over the radius-padded box.
+// out[0] = cases, out[1] = certified, out[2] = certified and different from f64.
+extern "C" void within_stress(int mode, uint64_t seed, uint64_t n, unsigned long long* out) {
+    SplitMix rng{seed * 0x9e3779b97f4a7c15ull + 77 + (uint64_t)mode};
+    out[0] = out[1] = out[2] = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        const float scale = mode == 3 ? rng.range(64.0f, 4096.0f) : 64.0f;
+        V2 p[3];
+        for (int k = 0; k < 3; ++k) p[k] = mk(rng.range(-1.0f, 1.0f) * scale, rng.range(-1.0f, 1.0f) * scale);
+        const float r = rng.range(0.5f, 8.0f) * (scale / 64.0f);
+        if (mode == 1)
+            p[1] = lerp(p[0], p[2], (float)rng.uni()) +
+                   mk(rng.range(-1, 1), rng.range(-1, 1)) * (float)std::pow(10.0, -7.0 + 7.0 * rng.uni());
+        if (mode == 2) {
+            const int k = (int)(rng.next() % 3);
+            if (k == 0) p[1] = p[0];
+            if (k == 1) p[1] = p[2];
+            if (k == 2) p[2] = p[0];
+        }
+        V2 q;
+        if (mode == 4) {
+            V2 lo = vmin(vmin(p[0], p[1]), p[2]), hi = vmax(vmax(p[0], p[1]), p[2]);
+            q = mk(rng.range(lo.x - r, hi.x + r), rng.range(lo.y - r, hi.y + r));
+        } else {
+            const float t = (float)rng.uni(), u = 1.0f - t;
+            const V2 on = p[0] * (u * u) + p[1] * (2.0f * u * t) + p[2] * (t * t);
+            V2 tg = (p[1] - p[0]) * (2.0f * u) + (p[2] - p[1]) * (2.0f * t);
+            float tl = length(tg);
+            V2 nrm = tl > 0.0f ? mk(-tg.y / tl, tg.x / tl) : mk(1.0f, 0.0f);
+            const float off = r + (rng.next() % 2 ? 1.0f : -1.0f) * (float)std::pow(10.0, -6.0 + 7.0 * rng.uni());
+            q = on + nrm * off;
+        }
+        const CP c = closest_point_quadratic(q, p[0], p[1], p[2], false);
+        const float tt = 1.0f - c.t;
+        const int ref = c.dist < tt * tt * r + 2.0f * tt * c.t * r + c.t * c.t * r ? 1 : 0;
+        const int fast = dvgb::within_quad_f32(p[0].x, p[0].y, p[1].x, p[1].y, p[2].x, p[2].y, r, q.x, q.y);
+        out[0] += 1;
+        if (fast != dvgb::WITHIN_UNSURE) {
             out[1] += 1;
             if (fast != ref) out[2] += 1;
         }

@@ -1,10 +1,12 @@
-"""The certified f32 cubic winding (diffvg-rs_b200/csrc/winding_f32.cuh, used by every
-kernel's winding solve before the f64 one) against the oracle's restatement of the
-crate's f64 computation: on random segments with query points near the curve, integer
+"""The certified f32 decisions (diffvg-rs_b200/csrc/certified_f32.cuh, used by every
+kernel before the f64 solves) against the oracle's restatement of the crate's f64
+computations.  Cubic winding: random segments with query points near the curve, integer
 alignments, near-degenerate cubics (elevated quadratics, lines, cusps, tiny loops),
-query rows exactly at end points and extrema, large coordinates, and the tests a
-scene makes, it never returns a decision that differs from the f64 one; and it
-decides most of a scene's tests (so the f64 solve runs rarely)."""
+query rows exactly at end points and extrema, large coordinates, scene-like tests.
+Quadratic stroke test: query points at the stroke's edge (radius +- 10^U[-6, 1]),
+nearly straight and degenerate quadratics, large coordinates, scene-like tests.  Never
+a decision that differs from the f64 one; most of a scene's tests decided in f32 (so
+the f64 solves run rarely)."""
 import ctypes as C
 import os
 import subprocess
@@ -24,18 +26,32 @@ def stress():
     L = C.CDLL(LIB)
     L.winding_stress.argtypes = [C.c_int, C.c_uint64, C.c_uint64, C.POINTER(C.c_ulonglong)]
     L.winding_stress.restype = None
+    L.within_stress.argtypes = [C.c_int, C.c_uint64, C.c_uint64, C.POINTER(C.c_ulonglong)]
+    L.within_stress.restype = None
 
-    def run(mode, seed, n):
+    def run(fn, mode, seed, n):
         out = (C.c_ulonglong * 3)()
-        L.winding_stress(mode, seed, n, out)
+        getattr(L, fn)(mode, seed, n, out)
         return list(out)
     return run
 
 
 @pytest.mark.parametrize("mode", range(len(MODES)), ids=MODES)
 def test_certified_f32_winding_never_disagrees(stress, mode):
-    cases, certified, wrong = stress(mode, 11, 2_000_000)
+    cases, certified, wrong = stress("winding_stress", mode, 11, 2_000_000)
     assert cases == 2_000_000
     assert wrong == 0, f"{wrong} certified decisions differ from the f64 ones ({MODES[mode]})"
     if mode == 5:
+        assert certified >= 0.9 * cases, f"only {certified / cases:.3f} of a scene's tests decided in f32"
+
+
+WITHIN_MODES = ("at the stroke edge", "nearly straight", "degenerate", "large coordinates", "scene tests")
+
+
+@pytest.mark.parametrize("mode", range(len(WITHIN_MODES)), ids=WITHIN_MODES)
+def test_certified_f32_quadratic_stroke_never_disagrees(stress, mode):
+    cases, certified, wrong = stress("within_stress", mode, 12, 2_000_000)
+    assert cases == 2_000_000
+    assert wrong == 0, f"{wrong} certified decisions differ from the f64 ones ({WITHIN_MODES[mode]})"
+    if mode == 4:
         assert certified >= 0.9 * cases, f"only {certified / cases:.3f} of a scene's tests decided in f32"
