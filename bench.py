@@ -348,7 +348,8 @@ def large_fit(r, dev, lib_stream, steps, warmup, rank, lr=LARGE_FIT_LR):
                         f"bwd + Adam (lr {lr}, points and paint parameters) + re-preparation per graph replay",
             "iterations": steps, "warmup": warmup, "ms_per_iter": ms, "msamples_per_s": samples / (ms / 1e3) / 1e6,
             "loss_first": traj[0][1], "loss_last": traj[-1][1], "loss_trajectory": traj,
-            "launch_shape": {"sample_layout": tuning[0], "boundary_cell": tuning[1], "fragment_slots": tuning[2]}}
+            "launch_shape": {"sample_layout": tuning[0], "boundary_cell": tuning[1], "fragment_slots": tuning[2],
+                             "work_queue": "persistent CTAs" if tuning[3] else "one CTA per item"}}
 
 
 def single_scene_sharded(r, dev, lib_stream, steps, warmup, rank, world):
@@ -500,7 +501,8 @@ def batched_vs_plain(r, dev, lib_stream, flush, scenes, steps, label):
                "what": "fwd + L2 + bwd + Adam(lr 1e-2) on path points per scene; batched = one graph replay with "
                        "on-device Adam and scene re-preparation; plain = per scene host preparation + upload, "
                        "fused device call, gradient read-back, host Adam"},
-           "workload": label, "launch_shape": {"sample_layout": tuning[0], "boundary_cell": tuning[1], "fragment_slots": tuning[2]}}
+           "workload": label, "launch_shape": {"sample_layout": tuning[0], "boundary_cell": tuning[1], "fragment_slots": tuning[2],
+                             "work_queue": "persistent CTAs" if tuning[3] else "one CTA per item"}}
     batch.close()
     for u in ups + tgts:
         u.close()

@@ -134,7 +134,7 @@ struct dvg_scene {
     size_t grad_floats = 0;
     size_t arena_bytes = 0;  // bytes of prepared tables in `arena`
     const float4* g_bbox = nullptr;
-    dvg_tuning tune{1, 4, 16};  // launch shape (dvg_scene_set_tuning / dvg_scene_autotune)
+    dvg_tuning tune{1, 4, 16, 0};  // launch shape (dvg_scene_set_tuning / dvg_scene_autotune)
 };
 
 namespace {
@@ -1142,13 +1142,13 @@ struct dvg_batch {
     size_t total_pix4 = 0, total_pix = 0, total_grads = 0, max_pixels = 0;
     int items = 0, total_tiles = 0, max_ri = 0;
     uint64_t total_bsamples = 0;
-    DevBuf entries, work, accum, wsum, image, target, d_render, loss, grads, bsamples, bkey, border, bcounts;
+    DevBuf entries, work, queue, accum, wsum, image, target, d_render, loss, grads, bsamples, bkey, border, bcounts;
     DevBuf frag;  // per-scene fragment caches (forward -> interior)
     bool any_styled = false;  // some scene strokes with non-round joins or caps
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     uint64_t steps = 0;
-    dvg_tuning tune{1, 4, 16};  // launch shape (dvg_batch_autotune)
+    dvg_tuning tune{1, 4, 16, 0};  // launch shape (dvg_batch_autotune)
     // on-device optimisation step (dvg_batch_set_adam)
     bool adam = false;
     AdamParams ap{};
@@ -1166,17 +1166,25 @@ dvg_status batch_enqueue(dvg_batch* b) {
     CK(cudaMemsetAsync(b->loss.ptr, 0, (size_t)n * sizeof(float), ctx->stream));
     CK(cudaMemsetAsync(b->grads.ptr, 0, b->total_grads * sizeof(float), ctx->stream));
     const bool pre = b->opts.use_prefiltering != 0;
+    int* queue = nullptr;  // persistent CTAs: three zeroed item counters (forward, 2 interior kernels)
+    if (b->tune.work_queue) {
+        CK(b->queue.reserve(4 * sizeof(int)));
+        CK(cudaMemsetAsync(b->queue.ptr, 0, 4 * sizeof(int), ctx->stream));
+        queue = b->queue.as<int>();
+    }
     if (pre)
-        ctx->launches += launch_forward_prefilter_batch(B, b->work.as<int2>(), b->items, b->max_ri, ctx->status,
-                                                        ctx->stream);
+        ctx->launches += launch_forward_prefilter_batch(B, b->work.as<int2>(), b->items, queue, b->max_ri,
+                                                        ctx->status, ctx->stream);
     else
-        ctx->launches += launch_forward_batch(B, b->work.as<int2>(), b->items, b->max_ri, ctx->stream);
+        ctx->launches += launch_forward_batch(B, b->work.as<int2>(), b->items, queue, b->max_ri, ctx->stream);
     ctx->launches += launch_pixels_batch(B, n, b->max_pixels, 0, ctx->stream);
     ctx->launches += launch_pixels_batch(B, n, b->max_pixels, 1, ctx->stream);
     if (pre)
-        ctx->launches += launch_interior_prefilter_batch(B, b->work.as<int2>(), b->items, ctx->status, ctx->stream);
+        ctx->launches += launch_interior_prefilter_batch(B, b->work.as<int2>(), b->items, queue ? queue + 1 : nullptr,
+                                                         ctx->status, ctx->stream);
     else
-        ctx->launches += launch_interior_batch(B, b->work.as<int2>(), b->items, ctx->status, ctx->stream);
+        ctx->launches += launch_interior_batch(B, b->work.as<int2>(), b->items, queue ? queue + 1 : nullptr,
+                                               ctx->status, ctx->stream);
     if (!pre)
         ctx->launches += launch_boundary_batch(B, n, b->total_bsamples, b->total_tiles, (int)b->tune.boundary_cell,
                                                b->any_styled,
@@ -1797,13 +1805,15 @@ namespace {
 bool tuning_valid(const dvg_tuning* t) {
     return t && t->sample_layout <= 1 &&
            (t->boundary_cell == 2 || t->boundary_cell == 4 || t->boundary_cell == 8 || t->boundary_cell == 16) &&
-           t->fragment_slots <= (uint32_t)FRAG_MAX_SLOTS;
+           t->fragment_slots <= (uint32_t)FRAG_MAX_SLOTS && t->work_queue <= 1;
 }
 // The candidates: both warp layouts with the default cell and cache, then every cell
 // with the better layout (the boundary pass does not depend on the layout), then the
-// fragment-cache sizes (`try_slots`: only where the cache is used, non-prefiltered).
+// fragment-cache sizes (`try_slots`: only where the cache is used, non-prefiltered),
+// then persistent CTAs for the batch stages (`try_queue`).
 template <typename Apply, typename Run>
-dvg_status autotune_loop(dvg_context* ctx, dvg_tuning* tune, bool try_slots, Apply apply, Run run) {
+dvg_status autotune_loop(dvg_context* ctx, dvg_tuning* tune, bool try_slots, Apply apply, Run run,
+                         bool try_queue = false) {
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -1849,6 +1859,7 @@ dvg_status autotune_loop(dvg_context* ctx, dvg_tuning* tune, bool try_slots, App
         const dvg_tuning b2 = best;
         for (int k = 0; k < 3; ++k) consider(dvg_tuning{b2.sample_layout, b2.boundary_cell, slots[k]});
     }
+    if (try_queue) consider(dvg_tuning{best.sample_layout, best.boundary_cell, best.fragment_slots, 1});
     *tune = best;
     if (st == DVG_OK) st = apply();
     cudaEventDestroy(e0);
@@ -1924,7 +1935,7 @@ extern "C" dvg_status dvg_batch_autotune(dvg_batch* b, dvg_tuning* out) {
     b->adam = false;  // time forward + loss + backward only: the parameters must not move
     dvg_status st = autotune_loop(
         ctx, &t, b->opts.use_prefiltering == 0, [&]() { return dvg_batch_set_tuning(b, &t); },
-        [&]() { return batch_enqueue(b); });
+        [&]() { return batch_enqueue(b); }, true);
     b->adam = adam;
     if (st != DVG_OK) return st;
     if (out) *out = b->tune;

@@ -11,6 +11,8 @@
 //   k_l2           L2 loss and d_render
 //
 // Built with -fmad=false (see device.cuh).
+#include <algorithm>
+
 #include "device.cuh"
 #include "kernels.cuh"
 
@@ -244,13 +246,15 @@ __global__ void __launch_bounds__(256, DVG_MINB_FWD) k_forward(DevScene S, Sampl
 }
 // Batched forward: one flat grid over every (scene, tile, sub-sample) work item.
 __global__ void __launch_bounds__(256, DVG_MINB_FWD) k_forward_batch(const BatchEntry* __restrict__ B,
-                                                                     const int2* __restrict__ work) {
+                                                                     const int2* __restrict__ work, int items,
+                                                                     int* counter) {
     extern __shared__ float sm[];
-    const int2 wk = work[blockIdx.x];  // (scene, tile + tiles * sub-sample round)
-    const BatchEntry& E = B[wk.x];
-    const int local = wk.y;
-    const int tiles = E.S.tiles_x * E.S.tiles_y;
-    forward_body(E.S, E.sp, local % tiles, local / tiles, E.accum, E.wsum, sm);
+    for_each_item(items, counter, [&](int i) {
+        const int2 wk = work[i];  // (scene, tile + tiles * sub-sample round)
+        const BatchEntry& E = B[wk.x];
+        const int tiles = E.S.tiles_x * E.S.tiles_y;
+        forward_body(E.S, E.sp, wk.y % tiles, wk.y / tiles, E.accum, E.wsum, sm);
+    });
 }
 
 // Weight image only (rasterize_weights_f32, forward.rs:1505-1564).
@@ -510,23 +514,25 @@ __global__ void __launch_bounds__(256, DVG_MINB_LEAN) k_interior_cached(DevScene
     interior_body<true>(S, sp, sp.tile_base + blockIdx.x, blockIdx.y, d_render, wsum, G, status);
 }
 __global__ void __launch_bounds__(256, DVG_MINB_INT) k_interior_batch(const BatchEntry* __restrict__ B,
-                                                                      const int2* __restrict__ work,
-                                                                      unsigned* status) {
-    const int2 wk = work[blockIdx.x];  // (scene, tile + tiles * sub-sample round)
-    const BatchEntry& E = B[wk.x];
-    const int local = wk.y;
-    const int tiles = E.S.tiles_x * E.S.tiles_y;
-    interior_body<false>(E.S, E.sp, local % tiles, local / tiles, E.d_render, E.wsum, E.G, status);
+                                                                      const int2* __restrict__ work, int items,
+                                                                      int* counter, unsigned* status) {
+    for_each_item(items, counter, [&](int i) {
+        const int2 wk = work[i];  // (scene, tile + tiles * sub-sample round)
+        const BatchEntry& E = B[wk.x];
+        const int tiles = E.S.tiles_x * E.S.tiles_y;
+        interior_body<false>(E.S, E.sp, wk.y % tiles, wk.y / tiles, E.d_render, E.wsum, E.G, status);
+    });
 }
 __global__ void __launch_bounds__(256, DVG_MINB_LEAN) k_interior_cached_batch(const BatchEntry* __restrict__ B,
-                                                                              const int2* __restrict__ work,
-                                                                              unsigned* status) {
-    const int2 wk = work[blockIdx.x];  // (scene, tile + tiles * sub-sample round)
-    const BatchEntry& E = B[wk.x];
-    if (!E.sp.frag) return;  // uniform per CTA
-    const int local = wk.y;
-    const int tiles = E.S.tiles_x * E.S.tiles_y;
-    interior_body<true>(E.S, E.sp, local % tiles, local / tiles, E.d_render, E.wsum, E.G, status);
+                                                                              const int2* __restrict__ work, int items,
+                                                                              int* counter, unsigned* status) {
+    for_each_item(items, counter, [&](int i) {
+        const int2 wk = work[i];  // (scene, tile + tiles * sub-sample round)
+        const BatchEntry& E = B[wk.x];
+        if (!E.sp.frag) return;  // uniform per item
+        const int tiles = E.S.tiles_x * E.S.tiles_y;
+        interior_body<true>(E.S, E.sp, wk.y % tiles, wk.y / tiles, E.d_render, E.wsum, E.G, status);
+    });
 }
 
 // ------------------------------------------------------------------ boundary sampling
@@ -1679,10 +1685,21 @@ int launch_finalize_background(const DevScene& S, const GradPtrs& G, cudaStream_
     return 1;
 }
 // Batched step launchers (one launch per stage for all scenes).
-int launch_forward_batch(const BatchEntry* B, const int2* work, int items, int max_ri, cudaStream_t stream) {
+// CTAs of a persistent launch: as many as the GPU holds at once (and no more than items).
+template <typename K>
+int persistent_grid(K kernel, size_t smem, int items) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, smem);
+    return std::max(1, std::min(items, std::max(per_sm, 1) * std::max(sms, 1)));
+}
+int launch_forward_batch(const BatchEntry* B, const int2* work, int items, int* counter, int max_ri,
+                         cudaStream_t stream) {
     const int hw = TILE + 2 * max_ri;
     size_t smem = max_ri <= MAX_SMEM_RI ? (size_t)hw * hw * 5 * sizeof(float) : 0;
-    k_forward_batch<<<items, 256, smem, stream>>>(B, work);
+    const int grid = counter ? persistent_grid(k_forward_batch, smem, items) : items;
+    k_forward_batch<<<grid, 256, smem, stream>>>(B, work, items, counter);
     return 1;
 }
 int launch_pixels_batch(const BatchEntry* B, int nscenes, size_t max_pixels, int which, cudaStream_t stream) {
@@ -1700,10 +1717,14 @@ int launch_pixels_batch(const BatchEntry* B, int nscenes, size_t max_pixels, int
     }
     return 1;
 }
-int launch_interior_batch(const BatchEntry* B, const int2* work, int items, unsigned* status,
+int launch_interior_batch(const BatchEntry* B, const int2* work, int items, int* counters, unsigned* status,
                           cudaStream_t stream) {
-    k_interior_cached_batch<<<items, 256, 0, stream>>>(B, work, status);
-    k_interior_batch<<<items, 256, 0, stream>>>(B, work, status);
+    int* c0 = counters ? counters : nullptr;
+    int* c1 = counters ? counters + 1 : nullptr;
+    k_interior_cached_batch<<<c0 ? persistent_grid(k_interior_cached_batch, 0, items) : items, 256, 0, stream>>>(
+        B, work, items, c0, status);
+    k_interior_batch<<<c1 ? persistent_grid(k_interior_batch, 0, items) : items, 256, 0, stream>>>(B, work, items, c1,
+                                                                                                  status);
     return 2;
 }
 int launch_boundary_batch(const BatchEntry* B, int nscenes, uint64_t total, int total_tiles, int cell, bool styled,

@@ -52,6 +52,29 @@ struct SampleParams {
     int frag_slots;  // codes kept per sample (<= FRAG_MAX_SLOTS)
     int tile_base, tile_count;  // the tiles a single-scene launch covers (count 0: all)
 };
+// Work items of a batched stage (work[i] = (scene, tile + tiles * sub-sample round),
+// heaviest first).  counter == nullptr: one CTA per item, item = blockIdx.x.  Otherwise
+// the CTAs are persistent (as many as the GPU holds at once) and take the next item from
+// *counter until the list is done; the counter is zeroed before the launch.  Every CTA
+// makes at most items / gridDim.x + 2 atomic increments, so the loop always ends.
+#ifdef __CUDACC__
+template <typename F>
+__device__ __forceinline__ void for_each_item(int items, int* counter, F&& body) {
+    if (!counter) {
+        if ((int)blockIdx.x < items) body((int)blockIdx.x);
+        return;
+    }
+    __shared__ int s_item;
+    for (;;) {
+        __syncthreads();  // the previous item is done with shared memory and s_item
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int i = s_item;
+        if (i >= items) return;
+        body(i);
+    }
+}
+#endif
 // Grid width of a single-scene sample launch: the tiles it covers.
 inline int launch_tiles(const DevScene& S, const SampleParams& sp) {
     return sp.tile_count > 0 ? sp.tile_count : S.tiles_x * S.tiles_y;
@@ -155,15 +178,18 @@ int launch_boundary(const DevScene& S, const BoundaryParams& bp, const float* d_
 int launch_finalize_background(const DevScene& S, const GradPtrs& G, cudaStream_t stream);
 int launch_fill_background(const DevScene& S, float* out, cudaStream_t stream);
 // Batched launchers: B (device) holds one BatchEntry per scene; work[i] = (scene, tile +
-// tiles * sub-sample round) is the i-th CTA's item, in any order (the batch lists the
-// heaviest tiles first).  which: 0 resolve, 1 L2, 2 background.
-int launch_forward_batch(const BatchEntry* B, const int2* work, int items, int max_ri, cudaStream_t stream);
-int launch_forward_prefilter_batch(const BatchEntry* B, const int2* work, int items, int max_ri,
+// tiles * sub-sample round) is the i-th work item, in any order (the batch lists the
+// heaviest tiles first).  counter(s): null for one CTA per item, else zeroed device ints
+// for persistent CTAs (see for_each_item; launch_interior_batch takes two, one per
+// kernel).  which: 0 resolve, 1 L2, 2 background.
+int launch_forward_batch(const BatchEntry* B, const int2* work, int items, int* counter, int max_ri,
+                         cudaStream_t stream);
+int launch_forward_prefilter_batch(const BatchEntry* B, const int2* work, int items, int* counter, int max_ri,
                                    unsigned* status, cudaStream_t stream);
 int launch_pixels_batch(const BatchEntry* B, int nscenes, size_t max_pixels, int which, cudaStream_t stream);
-int launch_interior_batch(const BatchEntry* B, const int2* work, int items, unsigned* status,
+int launch_interior_batch(const BatchEntry* B, const int2* work, int items, int* counters, unsigned* status,
                           cudaStream_t stream);
-int launch_interior_prefilter_batch(const BatchEntry* B, const int2* work, int items, unsigned* status,
+int launch_interior_prefilter_batch(const BatchEntry* B, const int2* work, int items, int* counter, unsigned* status,
                                     cudaStream_t stream);
 int launch_boundary_batch(const BatchEntry* B, int nscenes, uint64_t total, int total_tiles, int cell, bool styled,
                           BSample* samples, int* key, int* counts, int* order, cudaStream_t stream);

@@ -8,6 +8,8 @@
 // (closer child first, src/distance/api.rs:138-236, closest.rs:104-199): the
 // order only matters for exact distance ties, which it resolves the same way.
 // Built with -fmad=false like kernels.cu.
+#include <algorithm>
+
 #include "device.cuh"
 #include "kernels.cuh"
 // Minimum resident CTAs per SM of the prefiltered forward and interior kernels, by
@@ -342,14 +344,15 @@ __global__ void __launch_bounds__(256, DVG_MINB_PF_FWD) k_forward_prefilter(DevS
     forward_prefilter_body(S, sp, sp.tile_base + blockIdx.x, blockIdx.y, accum, wsum, status, sm);
 }
 __global__ void __launch_bounds__(256, DVG_MINB_PF_FWD) k_forward_prefilter_batch(const BatchEntry* __restrict__ B,
-                                                                    const int2* __restrict__ work,
-                                                                    unsigned* status) {
+                                                                    const int2* __restrict__ work, int items,
+                                                                    int* counter, unsigned* status) {
     extern __shared__ float sm[];
-    const int2 wk = work[blockIdx.x];  // (scene, tile + tiles * sub-sample round)
-    const BatchEntry& E = B[wk.x];
-    const int local = wk.y;
-    const int tiles = E.S.tiles_x * E.S.tiles_y;
-    forward_prefilter_body(E.S, E.sp, local % tiles, local / tiles, E.accum, E.wsum, status, sm);
+    for_each_item(items, counter, [&](int i) {
+        const int2 wk = work[i];  // (scene, tile + tiles * sub-sample round)
+        const BatchEntry& E = B[wk.x];
+        const int tiles = E.S.tiles_x * E.S.tiles_y;
+        forward_prefilter_body(E.S, E.sp, wk.y % tiles, wk.y / tiles, E.accum, E.wsum, status, sm);
+    });
 }
 
 // ------------------------------------------------------------------ distance adjoint (backward/distance.rs)
@@ -947,13 +950,14 @@ __global__ void __launch_bounds__(256, DVG_MINB_PF_INT) k_interior_prefilter(Dev
     interior_prefilter_body(S, sp, sp.tile_base + blockIdx.x, blockIdx.y, d_render, wsum, G, status);
 }
 __global__ void __launch_bounds__(256, DVG_MINB_PF_INT) k_interior_prefilter_batch(const BatchEntry* __restrict__ B,
-                                                                  const int2* __restrict__ work,
-                                                                  unsigned* status) {
-    const int2 wk = work[blockIdx.x];  // (scene, tile + tiles * sub-sample round)
-    const BatchEntry& E = B[wk.x];
-    const int local = wk.y;
-    const int tiles = E.S.tiles_x * E.S.tiles_y;
-    interior_prefilter_body(E.S, E.sp, local % tiles, local / tiles, E.d_render, E.wsum, E.G, status);
+                                                                  const int2* __restrict__ work, int items,
+                                                                  int* counter, unsigned* status) {
+    for_each_item(items, counter, [&](int i) {
+        const int2 wk = work[i];  // (scene, tile + tiles * sub-sample round)
+        const BatchEntry& E = B[wk.x];
+        const int tiles = E.S.tiles_x * E.S.tiles_y;
+        interior_prefilter_body(E.S, E.sp, wk.y % tiles, wk.y / tiles, E.d_render, E.wsum, E.G, status);
+    });
 }
 
 int launch_forward_prefilter(const DevScene& S, const SampleParams& sp, float* accum, float* wsum, unsigned* status,
@@ -971,16 +975,32 @@ int launch_interior_prefilter(const DevScene& S, const SampleParams& sp, const f
     return 1;
 }
 
-int launch_forward_prefilter_batch(const BatchEntry* B, const int2* work, int items, int max_ri,
+int launch_forward_prefilter_batch(const BatchEntry* B, const int2* work, int items, int* counter, int max_ri,
                                    unsigned* status, cudaStream_t stream) {
     const int hw = TILE + 2 * max_ri;
     size_t smem = max_ri <= MAX_SMEM_RI ? (size_t)hw * hw * 5 * sizeof(float) : 0;
-    k_forward_prefilter_batch<<<items, 256, smem, stream>>>(B, work, status);
+    int grid = items;
+    if (counter) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_forward_prefilter_batch, 256, smem);
+        grid = std::max(1, std::min(items, std::max(per_sm, 1) * std::max(sms, 1)));
+    }
+    k_forward_prefilter_batch<<<grid, 256, smem, stream>>>(B, work, items, counter, status);
     return 1;
 }
-int launch_interior_prefilter_batch(const BatchEntry* B, const int2* work, int items, unsigned* status,
+int launch_interior_prefilter_batch(const BatchEntry* B, const int2* work, int items, int* counter, unsigned* status,
                                     cudaStream_t stream) {
-    k_interior_prefilter_batch<<<items, 256, 0, stream>>>(B, work, status);
+    int grid = items;
+    if (counter) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_interior_prefilter_batch, 256, 0);
+        grid = std::max(1, std::min(items, std::max(per_sm, 1) * std::max(sms, 1)));
+    }
+    k_interior_prefilter_batch<<<grid, 256, 0, stream>>>(B, work, items, counter, status);
     return 1;
 }
 

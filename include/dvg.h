@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define DVG_ABI_VERSION 1
+#define DVG_ABI_VERSION 2
 
 typedef enum dvg_status {
     DVG_OK = 0,
@@ -190,11 +190,16 @@ typedef struct dvg_scene dvg_scene;
  *                adjoint, which then skips its own hit tests for samples with at most
  *                this many fragments; 0 disables the cache, at most 64, default 16.
  *                Device memory: (2 * slots + 1) bytes per pixel sample of the scene
- *                (W * H * spp, rounded up to whole 16x16 tiles). */
+ *                (W * H * spp, rounded up to whole 16x16 tiles).
+ * work_queue:    batches only: 0 = the forward and interior stages launch one CTA per
+ *                work item (scene, tile, sub-sample), heaviest tiles first (default);
+ *                1 = they launch as many persistent CTAs as the GPU holds at once, which
+ *                take the items from a device counter in the same order. */
 typedef struct dvg_tuning {
     uint32_t sample_layout;
     uint32_t boundary_cell;
     uint32_t fragment_slots;
+    uint32_t work_queue;
 } dvg_tuning;
 
 /* Version of this ABI (DVG_ABI_VERSION). */

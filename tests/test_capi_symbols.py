@@ -48,7 +48,7 @@ def test_abi_version_and_no_device_error():
         pytest.skip("a CUDA device is present; the no-device path is not reachable")
     lib = C.CDLL(LIB)
     lib.dvg_abi_version.restype = C.c_uint32
-    assert lib.dvg_abi_version() == 1
+    assert lib.dvg_abi_version() == 2
     ctx = C.c_void_p()
     lib.dvg_context_create.argtypes = [C.c_int, C.POINTER(C.c_void_p)]
     st = lib.dvg_context_create(0, C.byref(ctx))
