@@ -30,8 +30,23 @@ struct SplitMix {
 // mode 3: query rows exactly at the end-point y values and at the y extrema;
 // mode 4: coordinates scaled to |x| up to 4096;
 // mode 5: the tests a scene makes: query points uniform over the control points' box.
+// perturb > 0: every initial root is moved by up to +-perturb before the refinement
+// and the certificate (the largest error of the GPU's fast root formulas is ~5e-4).
 // out[0] = cases, out[1] = certified, out[2] = certified and different from f64.
-extern "C" void winding_stress(int mode, uint64_t seed, uint64_t n, unsigned long long* out) {
+static int winding_perturbed(const V2* p, V2 q, float perturb, SplitMix& rng) {
+    const float a = -p[0].y + 3.0f * p[1].y - 3.0f * p[2].y + p[3].y;
+    const float b = 3.0f * p[0].y - 6.0f * p[1].y + 3.0f * p[2].y;
+    const float c = -3.0f * p[0].y + 3.0f * p[1].y;
+    const float d = p[0].y - q.y;
+    const float mcoef = std::fmax(std::fmax(std::fabs(b), std::fabs(c)), std::fabs(d));
+    if (!(std::fabs(a) >= 1.0e-3f) || !(std::fabs(a) * 16.0f >= mcoef)) return dvgb::WIND_UNSURE;
+    float t[3];
+    const int n = dvgb::cubic_roots_f32(b / a, c / a, d / a, t);
+    if (n < 0) return dvgb::WIND_UNSURE;
+    for (int i = 0; i < n; ++i) t[i] += rng.range(-perturb, perturb);
+    return dvgb::winding_from_roots(a, b, c, d, t, n, p[0].x, p[1].x, p[2].x, p[3].x, q.x);
+}
+extern "C" void winding_stress(int mode, uint64_t seed, uint64_t n, float perturb, unsigned long long* out) {
     SplitMix rng{seed * 0x2545f4914f6cdd1dull + (uint64_t)mode};
     out[0] = out[1] = out[2] = 0;
     for (uint64_t i = 0; i < n; ++i) {
@@ -89,7 +104,10 @@ extern "C" void winding_stress(int mode, uint64_t seed, uint64_t n, unsigned lon
             }
         }
         const int ref = winding_number_segment(2, p[0], p[1], p[2], p[3], q);
-        const int fast = dvgb::winding_cubic_f32(p[0].x, p[0].y, p[1].x, p[1].y, p[2].x, p[2].y, p[3].x, p[3].y, q.x, q.y);
+        const int fast = perturb > 0.0f
+                             ? winding_perturbed(p, q, perturb, rng)
+                             : dvgb::winding_cubic_f32(p[0].x, p[0].y, p[1].x, p[1].y, p[2].x, p[2].y, p[3].x, p[3].y,
+                                                       q.x, q.y);
         out[0] += 1;
         if (fast != dvgb::WIND_UNSURE) {
             out[1] += 1;
@@ -106,8 +124,25 @@ extern "C" void winding_stress(int mode, uint64_t seed, uint64_t n, unsigned lon
 // mode 2: degenerate ones (p1 = p0, p1 = p2, p0 = p2);
 // mode 3: coordinates scaled up to 4096;
 // mode 4: the tests a scene makes: query points uniform over the radius-padded box.
+// perturb > 0: initial roots moved by up to +-perturb, as for the winding.
 // out[0] = cases, out[1] = certified, out[2] = certified and different from f64.
-extern "C" void within_stress(int mode, uint64_t seed, uint64_t n, unsigned long long* out) {
+static int within_perturbed(const V2* p, float r, V2 q, float perturb, SplitMix& rng) {
+    const float ax = p[0].x - 2.0f * p[1].x + p[2].x, ay = p[0].y - 2.0f * p[1].y + p[2].y;
+    const float bx = -p[0].x + p[1].x, by = -p[0].y + p[1].y;
+    const float cx = p[0].x - q.x, cy = p[0].y - q.y;
+    const float A = ax * ax + ay * ay;
+    const float B = 3.0f * (ax * bx + ay * by);
+    const float C = 2.0f * (bx * bx + by * by) + (ax * cx + ay * cy);
+    const float D = bx * cx + by * cy;
+    const float mcoef = std::fmax(std::fmax(std::fabs(B), std::fabs(C)), std::fabs(D));
+    if (!(A >= 1.0e-3f) || !(A * 16.0f >= mcoef)) return dvgb::WITHIN_UNSURE;
+    float t[3];
+    const int n = dvgb::cubic_roots_f32(B / A, C / A, D / A, t);
+    if (n < 0) return dvgb::WITHIN_UNSURE;
+    for (int i = 0; i < n; ++i) t[i] += rng.range(-perturb, perturb);
+    return dvgb::within_quad_from_roots(t, n, p[0].x, p[0].y, p[1].x, p[1].y, p[2].x, p[2].y, r, q.x, q.y, A, B, C, D);
+}
+extern "C" void within_stress(int mode, uint64_t seed, uint64_t n, float perturb, unsigned long long* out) {
     SplitMix rng{seed * 0x9e3779b97f4a7c15ull + 77 + (uint64_t)mode};
     out[0] = out[1] = out[2] = 0;
     for (uint64_t i = 0; i < n; ++i) {
@@ -140,7 +175,9 @@ extern "C" void within_stress(int mode, uint64_t seed, uint64_t n, unsigned long
         const CP c = closest_point_quadratic(q, p[0], p[1], p[2], false);
         const float tt = 1.0f - c.t;
         const int ref = c.dist < tt * tt * r + 2.0f * tt * c.t * r + c.t * c.t * r ? 1 : 0;
-        const int fast = dvgb::within_quad_f32(p[0].x, p[0].y, p[1].x, p[1].y, p[2].x, p[2].y, r, q.x, q.y);
+        const int fast = perturb > 0.0f ? within_perturbed(p, r, q, perturb, rng)
+                                        : dvgb::within_quad_f32(p[0].x, p[0].y, p[1].x, p[1].y, p[2].x, p[2].y, r, q.x,
+                                                                q.y);
         out[0] += 1;
         if (fast != dvgb::WITHIN_UNSURE) {
             out[1] += 1;
