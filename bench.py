@@ -173,7 +173,7 @@ NCU_STEP_METRICS = ("gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_wri
                     "lts__t_sectors_op_red.sum,lts__t_sectors_op_atom.sum")
 
 
-def ncu_import(csv_path: str, workload: str) -> None:
+def ncu_import(csv_path: str, workload: str, digest: str = "") -> None:
     """Per-kernel sums over the launches of one captured step, keyed by kernel name, with the digest of
     the kernel sources they were captured from.  Capture (one GPU; warm-up outside the range):
       ncu --clock-control none --nvtx --nvtx-include dvg_step/ --metrics <NCU_STEP_METRICS> --csv
@@ -197,7 +197,7 @@ def ncu_import(csv_path: str, workload: str) -> None:
         kernels[kname] = {"launches": len(launches), "ms": s["ns"] / 1e6,
                           "dram_bytes": int(s["dram_read"] + s["dram_write"]),
                           "red_sectors": int(s["red_sectors"]), "atom_sectors": int(s["atom_sectors"])}
-    out = {"workload": workload, "source_digest": source_digest(),
+    out = {"workload": workload, "source_digest": digest or source_digest(),
            "what": "one fused step (forward + L2 + backward) captured by ncu after warm-up, L2 flushed before it; "
                    "per kernel, summed over its launches in the step; times are ncu's (serialised launches): "
                    "compare shares, not absolutes",
@@ -558,9 +558,11 @@ def main():
     ap.add_argument("--ncu-import", metavar="CSV",
                     help="turn an ncu --csv --print-units base capture of one --ncu-step step into "
                          "profiles/ncu_step_<workload>.json, then exit")
+    ap.add_argument("--ncu-digest", default="",
+                    help="kernel-source digest the --ncu-step run printed (default: the current sources')")
     args = ap.parse_args()
     if args.ncu_import:
-        return ncu_import(args.ncu_import, args.workload)
+        return ncu_import(args.ncu_import, args.workload, args.ncu_digest)
     if args.impl == "reference":
         return run_reference(args)
 
