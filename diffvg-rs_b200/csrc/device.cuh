@@ -899,6 +899,15 @@ __device__ __forceinline__ int winding_shape(const DevScene& S, int s, float2 sp
 __device__ __forceinline__ bool fill_hit(int rule, int w) { return rule == 1 ? ((w < 0 ? -w : w) % 2) == 1 : w != 0; }
 
 // ------------------------------------------------------------------ group queries (distance/api.rs)
+// A point outside a group's conservative canvas box (its group-space root box mapped to
+// the canvas in f64 and padded by half a pixel plus 1e-4 of the coordinates) cannot hit
+// the group's stroke or fill without prefiltering: both tests begin with that root box
+// (within_distance_bvh api.rs:79-135, is_inside_bvh api.rs:259-309), which the point's
+// group-space image misses by far more than the f32 rounding of the transform.
+__device__ __forceinline__ bool outside_group_box(const DevScene& S, int g, float2 pt) {
+    const float4 b = __ldg(&S.g_bbox[g]);
+    return pt.x < b.x || pt.x > b.z || pt.y < b.y || pt.y > b.w;
+}
 // within_distance_bvh (api.rs:79-135) with the brute-force fallback (api.rs:15-33).
 __device__ __forceinline__ bool group_within(const DevScene& S, int g, float2 lp) {
     int4 gb = __ldg(&S.g_bvh[g]);

@@ -215,12 +215,14 @@ __device__ __forceinline__ void forward_body(const DevScene& S, const SamplePara
         float4 acc = background_premul(S, y * S.width + x);
         for (int e = 0; e < n; ++e) {
             const int g = __ldg(&list[e]);
-            const int4 gi = __ldg(&S.g_info[g]);
-            const float2 lp = xf9(S.g_c2s + 9 * g, pt);
             // stroke first, then fill; one paint call site for both
-            int hitp[2];
-            hitp[0] = gi.y >= 0 && group_within(S, g, lp) ? gi.y : -1;
-            hitp[1] = gi.x >= 0 && group_inside(S, g, lp, gi.z) ? gi.x : -1;
+            int hitp[2] = {-1, -1};
+            if (!outside_group_box(S, g, pt)) {
+                const int4 gi = __ldg(&S.g_info[g]);
+                const float2 lp = xf9(S.g_c2s + 9 * g, pt);
+                hitp[0] = gi.y >= 0 && group_within(S, g, lp) ? gi.y : -1;
+                hitp[1] = gi.x >= 0 && group_inside(S, g, lp, gi.z) ? gi.x : -1;
+            }
 #pragma unroll 1
             for (int which = 0; which < 2; ++which)
                 if (hitp[which] >= 0) {
@@ -364,10 +366,13 @@ __device__ __forceinline__ void interior_body(const DevScene& S, const SamplePar
             } else {
                 e = k;
                 const int g = __ldg(&list[e]);
-                const int4 gi = __ldg(&S.g_info[g]);
-                const float2 lp = xf9(S.g_c2s + 9 * g, pt);
-                hitp[0] = gi.y >= 0 && group_within(S, g, lp) ? gi.y : -1;
-                hitp[1] = gi.x >= 0 && group_inside(S, g, lp, gi.z) ? gi.x : -1;
+                hitp[0] = hitp[1] = -1;
+                if (!outside_group_box(S, g, pt)) {
+                    const int4 gi = __ldg(&S.g_info[g]);
+                    const float2 lp = xf9(S.g_c2s + 9 * g, pt);
+                    hitp[0] = gi.y >= 0 && group_within(S, g, lp) ? gi.y : -1;
+                    hitp[1] = gi.x >= 0 && group_inside(S, g, lp, gi.z) ? gi.x : -1;
+                }
             }
 #pragma unroll 1
             for (int which = 0; which < 2; ++which) {
@@ -548,12 +553,14 @@ __device__ float4 edge_color(const DevScene& S, int tile, float2 pt, float4 bg, 
     int nfrag = 0, ev = 0;  // ev: 0 none, 1 last event sets the hit, 2 last event clears it
     for (int e = 0; e < n; ++e) {
         const int g = __ldg(&list[e]);
-        const int4 gi = __ldg(&S.g_info[g]);
-        const float2 lp = xf9(S.g_c2s + 9 * g, pt);
         // stroke first, then fill; one paint call site for both
-        int hitp[2];
-        hitp[0] = gi.y >= 0 && group_within(S, g, lp) ? gi.y : -1;
-        hitp[1] = gi.x >= 0 && group_inside(S, g, lp, gi.z) ? gi.x : -1;
+        int hitp[2] = {-1, -1};
+        if (!outside_group_box(S, g, pt)) {
+            const int4 gi = __ldg(&S.g_info[g]);
+            const float2 lp = xf9(S.g_c2s + 9 * g, pt);
+            hitp[0] = gi.y >= 0 && group_within(S, g, lp) ? gi.y : -1;
+            hitp[1] = gi.x >= 0 && group_inside(S, g, lp, gi.z) ? gi.x : -1;
+        }
 #pragma unroll 1
         for (int which = 0; which < 2; ++which) {
             if (hitp[which] < 0) continue;
