@@ -13,7 +13,6 @@
 #include <cuda_runtime.h>
 
 #include "prepare.hpp"  // ShapeFlags shared with the host preparation
-#include "certified_f32.cuh"
 
 namespace dvgb {
 
@@ -495,10 +494,6 @@ static __device__ __noinline__ int winding_segment_v(int kind, float a0, float a
         }
         return w;
     }
-    {  // the f32 solve decides whenever its margins prove the f64 one decides the same
-        const int w32 = winding_cubic_f32(q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], pt.x, pt.y);
-        if (w32 != WIND_UNSURE) return w32;
-    }
     double a = (double)(-q[1] + 3.0f * q[3] - 3.0f * q[5] + q[7]);
     double b = (double)(3.0f * q[1] - 6.0f * q[3] + 3.0f * q[5]);
     double c = (double)(-3.0f * q[1] + 3.0f * q[3]);
@@ -757,12 +752,6 @@ __device__ __forceinline__ int winding_path_list(const DevScene& S, int path, fl
     }
     return w;
 }
-// A quadratic segment whose stroke test within_quad_f32 can take: exact closest point
-// (not the crate's approximation), the same radius at its three control points, no
-// non-round join or cap (whose end-point exclusion needs the closest point's t).
-__device__ __forceinline__ bool quad_plain_radius(const SegGeom& sg, bool approx, int pflags) {
-    return sg.kind == 1 && !approx && !(pflags & PF_STYLED) && sg.r[0] == sg.r[1] && sg.r[1] == sg.r[2];
-}
 __device__ __forceinline__ bool within_path_bvh(const DevScene& S, int path, float2 p) {  // closest.rs:20-98
     int4 pi = __ldg(&S.p_info[2 * path]);
     const int pflags = __ldg(&S.p_info[2 * path + 1].w);
@@ -782,11 +771,6 @@ __device__ __forceinline__ bool within_path_bvh(const DevScene& S, int path, flo
                 load_seg(S, sidx, sg);
                 if (stroke_misses_segment(sg, p)) continue;
                 if (sg.kind == 2 && !approx && stroke_far_from_cubic(sg, p)) continue;
-                if (quad_plain_radius(sg, approx, pflags)) {  // decided in f32 when certain
-                    const int w = within_quad_f32(sg.q[0], sg.q[1], sg.q[2], sg.q[3], sg.q[4], sg.q[5], sg.r[0], p.x, p.y);
-                    if (w == 1) return true;
-                    if (w == 0) continue;
-                }
                 CPRes c = seg_closest(sg, p, approx);
                 if (c.dist < seg_radius(sg, c.t) && !end_excluded(pflags, sidx - pi.x, pi.y, c.t)) return true;
             }
@@ -806,11 +790,6 @@ __device__ __forceinline__ bool within_path_list(const DevScene& S, int path, fl
         load_seg(S, pi.x + k, sg);
         if (stroke_misses_segment(sg, p)) continue;
         if (sg.kind == 2 && !approx && stroke_far_from_cubic(sg, p)) continue;
-        if (quad_plain_radius(sg, approx, pflags)) {  // decided in f32 when certain
-            const int w = within_quad_f32(sg.q[0], sg.q[1], sg.q[2], sg.q[3], sg.q[4], sg.q[5], sg.r[0], p.x, p.y);
-            if (w == 1) return true;
-            if (w == 0) continue;
-        }
         CPRes c = seg_closest(sg, p, approx);
         if (c.dist < seg_radius(sg, c.t) && !end_excluded(pflags, k, pi.y, c.t)) return true;
     }

@@ -3675,13 +3675,14 @@ static BoundaryTables build_boundary_tables(const Scene& sc) {
 // edge term carries no 1/N (the weight image and the normalised coordinates hold it),
 // so another sample count rescales every sample's pdf to keep the same expectation
 // (exactly 1 for the crate's count).
-static void boundary_sample(const Scene& sc, const SceneBvh& bvh, const BoundaryTables& bt, uint64_t idx,
-                            uint32_t rng_kind, uint32_t seed, const float* d_render, const std::vector<float>& wimg,
-                            Grads& g, bool compute_translation, float pdf_scale) {
-    float u, t;
-    boundary_rng(rng_kind, idx, seed, &u, &t);
-    float dummy;
-    size_t sample_id = sample_cdf(bt.cdf.cdf, u, &dummy);
+//
+// boundary_eval is the part after the two draws: the edge term of the boundary point at
+// parameter t of shape-cdf entry sample_id.  Its contribution is multiplied by `weight`
+// (1 for a drawn sample) and its colours are taken `offset` (normalised canvas units; the
+// crate's 1e-4) either side of the point along the canvas normal.
+static void boundary_eval(const Scene& sc, const SceneBvh& bvh, const BoundaryTables& bt, size_t sample_id, float t,
+                          const float* d_render, const std::vector<float>& wimg, Grads& g, bool compute_translation,
+                          float pdf_scale, float weight, float offset) {
     if (sample_id >= bt.cdf.shape_ids.size()) return;
     size_t shape_id = bt.cdf.shape_ids[sample_id];
     size_t group_id = bt.cdf.group_ids[sample_id];
@@ -3715,8 +3716,8 @@ static void boundary_sample(const Scene& sc, const SceneBvh& bvh, const Boundary
     V4 bg = sample_background(sc, pixel_index);
     EdgeQuery iq{group_id, shape_id, false}, oq{group_id, shape_id, false};
     V2 n = normal_canvas;
-    V4 ci = sample_color(sc, bvh, bpt - n * 1.0e-4f, &bg, nullptr, &iq, nullptr, -1, pixel_index);
-    V4 co = sample_color(sc, bvh, bpt + n * 1.0e-4f, &bg, nullptr, &oq, nullptr, -1, pixel_index);
+    V4 ci = sample_color(sc, bvh, bpt - n * offset, &bg, nullptr, &iq, nullptr, -1, pixel_index);
+    V4 co = sample_color(sc, bvh, bpt + n * offset, &bg, nullptr, &oq, nullptr, -1, pixel_index);
     if (!iq.hit && !oq.hit) return;
     if (!iq.hit) {
         n = n * -1.0f;
@@ -3734,6 +3735,7 @@ static void boundary_sample(const Scene& sc, const SceneBvh& bvh, const Boundary
     V4 diff{ci.x - co.x, ci.y - co.y, ci.z - co.z, ci.w - co.w};
     float contrib = dot4(diff, dc) / pdf;
     if (!std::isfinite(contrib)) return;
+    contrib *= weight;
     accumulate_boundary_gradient(shp, shape_id, contrib, t, n, data, g, grp.s2c, local_pt, group_id);
     if (compute_translation && g.has_translation) {
         size_t ti = pixel_index * 2;
@@ -3742,6 +3744,16 @@ static void boundary_sample(const Scene& sc, const SceneBvh& bvh, const Boundary
             g.translation[ti + 1] += n.y * contrib;
         }
     }
+}
+
+static void boundary_sample(const Scene& sc, const SceneBvh& bvh, const BoundaryTables& bt, uint64_t idx,
+                            uint32_t rng_kind, uint32_t seed, const float* d_render, const std::vector<float>& wimg,
+                            Grads& g, bool compute_translation, float pdf_scale) {
+    float u, t;
+    boundary_rng(rng_kind, idx, seed, &u, &t);
+    float dummy;
+    size_t sample_id = sample_cdf(bt.cdf.cdf, u, &dummy);
+    boundary_eval(sc, bvh, bt, sample_id, t, d_render, wimg, g, compute_translation, pdf_scale, 1.0f, 1.0e-4f);
 }
 
 // Interior sample (render.rs:95-169).
@@ -4015,6 +4027,46 @@ extern "C" int oracle_render_backward_ex(const dvg_scene_desc* desc, const dvg_r
         for (auto& g : tg) grads.add(g);
     }
     finalize_background_gradients(sc, grads);
+    export_grads(grads, out, desc);
+    return 0;
+}
+
+// Deterministic expectation of the boundary pass: the crate draws N = W*H*spp samples,
+// each a shape-cdf entry s (probability pmf_s) and a parameter t ~ U[0,1), so its boundary
+// gradients average over seeds to N * sum_s pmf_s * integral_0^1 edge(s, t) dt.  The
+// integral is taken by the midpoint rule, t_j = (j + 1/2) / m, every term through the same
+// boundary_eval as a drawn sample.  offset as in boundary_eval (1e-4 for the crate).
+extern "C" int oracle_boundary_integral(const dvg_scene_desc* desc, const dvg_render_options* opts,
+                                        const float* d_render, uint32_t m, float offset, int threads, dvg_grads* out) {
+    Scene sc = decode(desc);
+    Grads grads;
+    grads.init(sc, desc, false, false);
+    SampleSpec sp = make_spec(opts);
+    if (sc.w == 0 || sc.h == 0 || m == 0 || !d_render || sp.prefilter) {
+        export_grads(grads, out, desc);
+        return 0;
+    }
+    SceneBvh bvh = build_scene_bvh(sc);
+    std::vector<float> wimg = build_weight_image(sc, sp);
+    BoundaryTables bt = build_boundary_tables(sc);
+    if (bt.ok) {
+        const double n_samples = (double)sc.w * sc.h * sp.sx_n * sp.sy_n;
+        const uint64_t entries = bt.cdf.shape_ids.size();
+        int nthreads = threads > 1 ? threads : 1;
+        std::vector<Grads> tg(nthreads);
+        for (auto& g : tg) g.init(sc, desc, false, false);
+        parallel_for(0, entries * m, nthreads, [&](int th, uint64_t lo, uint64_t hi) {
+            for (uint64_t k = lo; k < hi; ++k) {
+                const size_t e = (size_t)(k / m);
+                const float pmf = e < bt.cdf.pmf.size() ? bt.cdf.pmf[e] : 0.0f;
+                if (pmf <= 0.0f) continue;
+                const float t = (float)(((double)(k % m) + 0.5) / m);
+                boundary_eval(sc, bvh, bt, e, t, d_render, wimg, tg[th], false, 1.0f,
+                              (float)(n_samples * pmf / m), offset);
+            }
+        });
+        for (auto& g : tg) grads.add(g);
+    }
     export_grads(grads, out, desc);
     return 0;
 }

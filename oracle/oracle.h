@@ -67,6 +67,15 @@ int oracle_render_backward_ex(const dvg_scene_desc* desc, const dvg_render_optio
                               dvg_grads* grads, int passes, int threads,
                               unsigned long long sample_begin, unsigned long long sample_end);
 
+/* Deterministic expectation of the boundary pass over boundary seeds (no interior
+ * pass): the edge term at the midpoints of m equal steps of every shape's boundary
+ * parameter, weighted by the shape's pmf and the crate's sample count.  offset: the
+ * colour-sampling offset along the normal in normalised canvas units (1e-4 in the
+ * crate, boundary.rs:880-902).  Test infrastructure for the boundary estimators. */
+int oracle_boundary_integral(const dvg_scene_desc* desc, const dvg_render_options* opts,
+                             const float* d_render, uint32_t m, float offset, int threads,
+                             dvg_grads* grads);
+
 /* Weight image (build_weight_image, src/backward/filters.rs:11-67). */
 int oracle_weight_image(const dvg_scene_desc* desc, const dvg_render_options* opts, float* out_w);
 

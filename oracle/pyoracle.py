@@ -64,6 +64,7 @@ def lib() -> C.CDLL:
         L.oracle_render_backward_ex.argtypes = [D, R, B, fp, C.POINTER(GradsC), C.c_int, C.c_int,
                                                 C.c_ulonglong, C.c_ulonglong]
         L.oracle_weight_image.argtypes = [D, R, fp]
+        L.oracle_boundary_integral.argtypes = [D, R, fp, C.c_uint32, C.c_float, C.c_int, C.POINTER(GradsC)]
         L.oracle_compute_distance.argtypes = [D, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_int, fp]
         L.oracle_within_distance.argtypes = [D, C.c_uint32, C.c_float, C.c_float, C.c_int]
         L.oracle_is_inside.argtypes = [D, C.c_uint32, C.c_float, C.c_float, C.c_int]
@@ -144,6 +145,21 @@ def render_backward(scene: Scene, options: RenderOptions, bopts: Optional[Backwa
     lib().oracle_render_backward_ex(ps.ref(), C.byref(o), C.byref(b),
                                     _fp(dr) if dr is not None else C.cast(None, C.POINTER(C.c_float)),
                                     C.byref(buf.c), passes, threads, sample_begin, sample_end)
+    return unflatten_grads(scene, ps, buf), buf
+
+
+def boundary_integral(scene: Scene, options: RenderOptions, d_render: np.ndarray, m: int,
+                      offset: float = 1.0e-4, threads: int = 0):
+    """Expectation over boundary seeds of the crate's boundary gradients (midpoint rule
+    with m steps of every shape's boundary parameter; see oracle_boundary_integral).
+    offset: the colour-sampling offset in normalised canvas units.  Returns
+    (SceneGrad, GradBuffers) as render_backward."""
+    ps = pack_scene(scene)
+    buf = GradBuffers(ps, background_image=False, translation=False)
+    o = render_options_c(options)
+    dr = np.ascontiguousarray(np.asarray(d_render, np.float32).reshape(-1))
+    lib().oracle_boundary_integral(ps.ref(), C.byref(o), _fp(dr), m, offset, threads or (os.cpu_count() or 1),
+                                   C.byref(buf.c))
     return unflatten_grads(scene, ps, buf), buf
 
 

@@ -1,56 +1,112 @@
-"""Boundary-sampled gradients against finite differences, in expectation.
+"""Boundary-sampled gradients in expectation.
 
 Without prefiltering a pixel sample is either inside a fill or not, so the control
-points and the transforms of a filled path receive gradient only from the boundary
-term (edge samples drawn in proportion to length, colour jump over the pdf,
-src/backward/boundary.rs:113-1148).  Its expectation over the edge samples is the
-derivative of the expected image: the image averaged over the jitter of the pixel
-samples.
+points, stroke widths and transforms receive gradient only from the boundary term
+(edge samples drawn in proportion to length, colour jump over the pdf,
+src/backward/boundary.rs:113-1148).  Two checks of its expectation over boundary seeds:
 
-Left: the mean of 64 runs with Philox4x32-10 boundary seeds (W*H edge samples each)
-and its standard error.  Right: central finite differences of L = sum(d_render *
-image) in f64, with common random numbers (the same jitter seed on both sides of a
-difference), averaged over 256 jitter seeds, and their standard error.  Steps: 0.1
-pixel for points and translations, 0.1 pixel / 64 for the linear entries of the
-transforms (they move points up to ~64 px from the canvas centre about which the
-transforms are built).  Bar, as for the Philox-against-PCG32 test: per element
-z = |left - right| / sqrt(se_left^2 + se_right^2); at least 97 % of the elements
-within 3 sigma, none beyond 6 sigma, mean z^2 <= 2.
+1. Against the crate's own integral.  The oracle's boundary_integral takes the edge
+   term of every boundary point of every shape (midpoint rule over the boundary
+   parameter, the same per-point evaluation as a drawn sample), which is what the
+   crate's boundary gradients average to over seeds.  Left: the mean of 128 runs with
+   Philox4x32-10 seeds (W*H edge samples each) and its standard error.  Scenes: the
+   128x128, 4x4-spp adjoint-verification scene as generated (four filled cubic paths
+   that cross themselves and each other, four stroked quadratic paths) and the same
+   scene with rotations and translations on every shape and group; every control
+   point, stroke width and affine transform entry.
 
-Scenes: the 128x128, 4x4-spp adjoint-verification scene as generated (identity
-transforms) for every control point of its four filled cubic paths, and the same
-scene with rotations and translations on every shape and group for the six affine
-entries of those paths' shape and group transforms.
+2. Against finite differences of the rendered image.  Right: central differences of
+   L = sum(d_render * image) in f64 with common random numbers (the same jitter seed
+   on both sides), averaged over 256 jitter seeds.  Steps: 0.1 pixel for points and
+   translations, 0.1 pixel / 64 for the linear transform entries.  Scene: four smooth
+   closed cubic outlines, one per quadrant, whose boundaries cross neither themselves
+   nor each other (see below), untransformed for the control points and rotated about
+   their own centres for the transform entries.
 
-Crate behaviour kept for parity and measured here instead: the edge term gives a
-transformed shape's control points the canvas-space normal (render_edge_sample passes
-it to accumulate_boundary_gradient, src/backward/boundary.rs:882-967, 970-1148), not
-its pull-back to shape space, so under rotations their gradients are biased (the z
-scores of the rotated scene's control points are far from the 3-sigma bar).  Also left
-out: the projective row of the transforms (the forward applies them as affine maps,
-the adjoint differentiates a projective one) and the stroked paths (the crate's edge
-term samples the stroke bodies but not their round join and cap arcs).
+Bar for both: per element z = |left - right| / (combined standard error); at least
+97 % of the elements within 3 sigma, none beyond 6 sigma, mean z^2 <= 2.
+
+Crate behaviour kept for parity, measured here instead of passed over:
+- The colours either side of an edge point are sampled 1e-4 of the canvas size away
+  along the normal (render_edge_sample, boundary.rs:880-902; 0.0128 px on 128x128).
+  Where the edge crosses another colour edge at a shallow angle, both offset points
+  straddle that edge too for a stretch of about 2 * offset / sin(angle), and the term
+  picks up the other edge's colour jump there.  The crossings of the adjoint scene
+  move its control-point gradients by up to ~12 % from the derivative of the image,
+  which is why the finite-difference check runs on a scene without crossings
+  (tests/test_boundary_integral.py measures the offset's effect on both scenes).
+- The edge term gives a transformed shape's control points the canvas-space normal
+  (render_edge_sample passes it to accumulate_boundary_gradient, boundary.rs:882-967,
+  970-1148), not its pull-back to shape space: under rotations their gradients are
+  biased (the last test measures it against finite differences).
+Also outside the finite-difference check: the projective row of the transforms (the
+forward applies them as affine maps, the adjoint differentiates a projective one).
 """
 import numpy as np
 import pytest
 
-from dvg import BackwardOptions, RenderOptions, Rng, synth
+from dvg import BackwardOptions, Color, Filter, FilterType, Mat3, Path, PathGeometry, RenderOptions, Rng, Scene, \
+    Shape, ShapeGroup, synth
 from test_fd import _rigid_transforms
 
 pytestmark = pytest.mark.gpu
 
 PHILOX_SEEDS = 64
+INTEGRAL_SEEDS = 128
 JITTER_SEEDS = 256
 H_PX = 0.1
+INTEGRAL_STEPS = 400_000  # midpoint steps of each shape's boundary parameter
+INTEGRAL_REL = 1e-3  # allowance for the midpoint rule, relative to the integral
 
 
 def _opts(seed):
     return RenderOptions(samples_x=4, samples_y=4, seed=seed, jitter=True, use_prefiltering=False)
 
 
+def separated_blobs(width=128, height=128, seed=0):
+    """Four smooth closed cubic outlines (5-7 segments about a circle of radius 0.3 of
+    a quadrant, tangent handles of a third of the chord), one per quadrant, opaque or
+    semi-transparent solid fills: no boundary crosses another or itself."""
+    rng = np.random.default_rng(seed)
+    sc = Scene(width, height)
+    sc.background = Color(1.0, 1.0, 1.0, 1.0)
+    sc.filter = Filter(FilterType.BOX, 0.5)
+    r0 = 0.3 * min(width, height) / 2
+    for qy in range(2):
+        for qx in range(2):
+            c = np.array([(qx + 0.5) * width / 2, (qy + 0.5) * height / 2])
+            n = int(rng.integers(5, 8))
+            ang = 2 * np.pi * (np.arange(n) + rng.uniform(-0.2, 0.2, n)) / n
+            rad = r0 * (1.0 + rng.uniform(-0.2, 0.2, n))
+            a = c + rad[:, None] * np.stack([np.cos(ang), np.sin(ang)], 1)
+            tan = np.stack([-np.sin(ang), np.cos(ang)], 1)
+            pts = []
+            for k in range(n):
+                k1 = (k + 1) % n
+                hl = np.linalg.norm(a[k1] - a[k]) / 3.0
+                pts += [a[k], a[k] + hl * tan[k], a[k1] - hl * tan[k1]]
+            pts = np.asarray(pts, np.float32)
+            sc.shapes.append(Shape(PathGeometry(Path([2] * n, [tuple(map(float, p)) for p in pts], None, True,
+                                                     False))))
+            rgb = np.float32(rng.uniform(0.0, 1.0, 3))
+            alpha = float(rng.choice([1.0, 0.6]))
+            sc.groups.append(ShapeGroup([len(sc.shapes) - 1], Color(*map(float, rgb), alpha), None))
+    return sc
+
+
+def _rigid_about_centres(sc):
+    """Each shape rotated about its own centre and moved by a pixel or two; each group
+    rotated the other way about the same centre: no two outlines come to cross."""
+    for i, (s, g) in enumerate(zip(sc.shapes, sc.groups)):
+        c = np.mean(np.asarray(s.geometry.path.points, np.float64), 0)
+        s.transform = Mat3.translate(*c).mul(Mat3.rotate(0.3 * (i + 1))).mul(Mat3.translate(*(-c)))
+        g.set_shape_to_canvas(Mat3.translate(1.5 - 0.5 * i, -1.0 + 0.5 * i).mul(Mat3.translate(*c)).mul(
+            Mat3.rotate(-0.2 * (i + 1))).mul(Mat3.translate(*(-c))))
+    return sc
+
+
 def _params(sc, points=True, xforms=True):
     """(array, flat index, getter, setter, h) for the filled cubic paths."""
-    from dvg import Mat3
     from dvg.abi import pack_scene
 
     packed = pack_scene(sc)
@@ -109,22 +165,31 @@ def _losses(r, sc, dr, n_seeds):
     return (imgs.double() @ dr).cpu().numpy()
 
 
-def _z_scores(r, sc, params):
+def _d_render(r, sc, target_sc):
+    target = r.render(target_sc, _opts(0)).pixels
+    img = r.render(sc, _opts(0)).pixels
+    return (2.0 * (img - target)).astype(np.float32)
+
+
+def _boundary_runs(r, sc, dr, names, n_seeds):
+    """Boundary-sampled gradients of n_seeds Philox seeds: {name: (n_seeds, size)}."""
+    runs = {n: [] for n in names}
+    for b in range(n_seeds):
+        g = r.render_backward(sc, _opts(0), BackwardOptions(rng=Rng.PHILOX, boundary_seed=1000 + b,
+                                                             boundary_samples=sc.width * sc.height), dr).buffers
+        for n in names:
+            runs[n].append(np.asarray(g[n], np.float64).copy())
+    return {n: np.asarray(v) for n, v in runs.items()}
+
+
+def _z_scores_fd(r, sc, target_sc, params):
     """Per parameter: |mean boundary-sampled gradient - mean finite difference| over the
     combined standard error (see the module docstring)."""
     import torch
 
-    target_sc = synth.adjoint_scene(1, sc.width, sc.height)
-    target = r.render(target_sc, _opts(0)).pixels
-    img = r.render(sc, _opts(0)).pixels
-    dr = (2.0 * (img - target)).astype(np.float32)
+    dr = _d_render(r, sc, target_sc)
     dr_dev = torch.from_numpy(dr.reshape(-1).astype(np.float64)).cuda()
-    left = {}
-    for b in range(PHILOX_SEEDS):
-        g = r.render_backward(sc, _opts(0), BackwardOptions(rng=Rng.PHILOX, boundary_seed=1000 + b,
-                                                             boundary_samples=sc.width * sc.height), dr).buffers
-        for name, idx, _, _, _ in params:
-            left.setdefault((name, idx), []).append(float(g[name][idx]))
+    runs = _boundary_runs(r, sc, dr, sorted({p[0] for p in params}), PHILOX_SEEDS)
     z = []
     for name, idx, get, put, h in params:
         v = get()
@@ -135,7 +200,7 @@ def _z_scores(r, sc, params):
         lm = _losses(r, sc, dr_dev, JITTER_SEEDS)
         put(v)
         fd = (lp - lm) / (hp - hm)
-        a = np.asarray(left[(name, idx)])
+        a = runs[name][:, idx]
         se = np.sqrt(a.var(ddof=1) / a.size + fd.var(ddof=1) / fd.size)
         diff = abs(a.mean() - fd.mean())
         if se == 0.0:
@@ -145,6 +210,27 @@ def _z_scores(r, sc, params):
     return np.asarray(z)
 
 
+def _z_scores_integral(r, sc, target_sc, names):
+    """Per gradient element: |mean boundary-sampled gradient - the oracle's integral of
+    the crate's edge term| over the standard error of the mean (plus the integral's
+    allowance)."""
+    import pyoracle
+
+    dr = _d_render(r, sc, target_sc)
+    runs = _boundary_runs(r, sc, dr, names, INTEGRAL_SEEDS)
+    _, integral = pyoracle.boundary_integral(sc, _opts(0), dr, INTEGRAL_STEPS)
+    z = []
+    for n in names:
+        a = runs[n]
+        ref = np.asarray(integral[n], np.float64)[: a.shape[1]]
+        se = np.sqrt(a.var(0, ddof=1) / a.shape[0] + (INTEGRAL_REL * np.abs(ref)) ** 2)
+        diff = np.abs(a.mean(0) - ref)
+        live = se > 0.0
+        assert np.all(diff[~live] <= 1e-6 * max(1.0, float(np.abs(ref).max()))), n
+        z.append(diff[live] / se[live])
+    return np.concatenate(z)
+
+
 def _assert_within_3_sigma(z, at_least):
     assert z.size >= at_least
     assert float(np.mean(z <= 3.0)) >= 0.97, f"{int(np.sum(z > 3.0))} of {z.size} beyond 3 sigma"
@@ -152,13 +238,31 @@ def _assert_within_3_sigma(z, at_least):
     assert float(np.mean(z * z)) <= 2.0, f"mean z^2 {float(np.mean(z * z)):.2f}"
 
 
-def test_cuda_boundary_point_gradients_match_fd_in_expectation():
+INTEGRAL_NAMES = ("d_points", "d_shape_stroke_width", "d_shape_transform", "d_group_transform")
+
+
+@pytest.mark.parametrize("rotated", [False, True], ids=["as generated", "rotated"])
+def test_cuda_boundary_gradients_match_crate_integral(rotated):
     from dvg import Renderer
 
     r = Renderer(0)
     try:
         sc = synth.adjoint_scene(0, 128, 128)
-        _assert_within_3_sigma(_z_scores(r, sc, _params(sc, points=True, xforms=False)), 100)
+        if rotated:
+            sc = _rigid_transforms(sc)
+        _assert_within_3_sigma(_z_scores_integral(r, sc, synth.adjoint_scene(1, 128, 128), INTEGRAL_NAMES), 250)
+    finally:
+        r.close()
+
+
+def test_cuda_boundary_point_gradients_match_fd_in_expectation():
+    from dvg import Renderer
+
+    r = Renderer(0)
+    try:
+        sc = separated_blobs(seed=0)
+        _assert_within_3_sigma(_z_scores_fd(r, sc, separated_blobs(seed=1), _params(sc, points=True, xforms=False)),
+                               100)
     finally:
         r.close()
 
@@ -168,22 +272,23 @@ def test_cuda_boundary_transform_gradients_match_fd_in_expectation():
 
     r = Renderer(0)
     try:
-        sc = _rigid_transforms(synth.adjoint_scene(0, 128, 128))
-        _assert_within_3_sigma(_z_scores(r, sc, _params(sc, points=False, xforms=True)), 40)
+        sc = _rigid_about_centres(separated_blobs(seed=0))
+        _assert_within_3_sigma(_z_scores_fd(r, sc, separated_blobs(seed=1), _params(sc, points=False, xforms=True)),
+                               40)
     finally:
         r.close()
 
 
 def test_cuda_boundary_points_of_rotated_shapes_measured_exclusion():
     """The crate's canvas-space normal on shape-space control points: on the rotated
-    scene the control points' z scores are far outside the bar the untransformed scene
-    meets (mean z^2 well above 2)."""
+    outlines the control points' z scores against finite differences are far outside
+    the bar the untransformed outlines meet (mean z^2 well above 2)."""
     from dvg import Renderer
 
     r = Renderer(0)
     try:
-        sc = _rigid_transforms(synth.adjoint_scene(0, 128, 128))
-        z = _z_scores(r, sc, _params(sc, points=True, xforms=False)[::3])
+        sc = _rigid_about_centres(separated_blobs(seed=0))
+        z = _z_scores_fd(r, sc, separated_blobs(seed=1), _params(sc, points=True, xforms=False)[::3])
         assert float(np.mean(z * z)) > 4.0, f"mean z^2 {float(np.mean(z * z)):.2f}"
     finally:
         r.close()
