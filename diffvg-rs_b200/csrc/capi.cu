@@ -477,7 +477,6 @@ dvg_status dvg_scene_upload(dvg_context* ctx, const dvg_scene_desc* desc, dvg_sc
     S.path_len = (const float*)(base + o_plen);
     sc->g_bbox = (const float4*)(base + o_g_bbox);
     S.g_bbox = sc->g_bbox;
-    S.status = ctx->status;
     // tile binning
     S.tiles_x = (S.width + TILE - 1) / TILE;
     S.tiles_y = (S.height + TILE - 1) / TILE;

@@ -92,7 +92,6 @@ struct DevScene {
     int tiles_x, tiles_y;
     const int* tile_offsets;
     const int* tile_entries;
-    unsigned* status;  // the owning context's status word (ST_* bits), or null
 };
 
 // ------------------------------------------------------------------ small math
@@ -705,16 +704,12 @@ __device__ __forceinline__ bool cubic_cannot_beat(const SegGeom& s, float2 p, bo
 }
 
 // ------------------------------------------------------------------ path queries
-// Preorder walks with skip links move strictly forward: a node's skip link points
-// past its subtree and a descent goes to node + 1, so a walk ends after at most
-// the tree's node count.  A skip link that does not point forward (a corrupt
-// table) ends the walk and raises ST_BVH_LIMIT, which the host reports as
-// DVG_ERR_DEVICE_LIMIT, instead of looping.
-__device__ __forceinline__ int bvh_skip(const DevScene& S, int n, int skip) {
-    if (skip > n) return skip;
-    if (S.status) atomicOr(S.status, ST_BVH_LIMIT);
-    return 0x7fffffff;
-}
+// Preorder walks with skip links move strictly forward: a descent goes to node + 1 and
+// a node's skip link is node + its subtree's size (the only producer of these tables is
+// the host builder, BvhBuilder in prepare.cpp; the device re-preparation in refit.cu
+// rewrites bounds and leaf order, never the links), so a walk ends after at most the
+// tree's node count.  The loop carries no guard: a bounds-free compare-and-select on
+// every link cost the forward 10 % and the boundary evaluation 12 % on the mixed scene.
 // Walks the path's BVH (preorder with skip links).  Node tests are exactly the
 // crate's: ray test for winding (winding.rs:117-126), containment for strokes.
 __device__ __forceinline__ int winding_path(const DevScene& S, int path, float2 p) {
@@ -725,7 +720,7 @@ __device__ __forceinline__ int winding_path(const DevScene& S, int path, float2 
         float4 b = __ldg(&S.pn_bounds[n]);
         int4 m = __ldg(&S.pn_meta[n]);
         if (p.y < b.y || p.y > b.w || p.x > b.z) {
-            n = bvh_skip(S, n, m.x);
+            n = m.x;
             continue;
         }
         if (m.z > 0) {
@@ -734,7 +729,7 @@ __device__ __forceinline__ int winding_path(const DevScene& S, int path, float2 
                 load_seg(S, __ldg(&S.pl_segs[k]), sg);
                 if (!ray_misses_segment(sg, p)) w += winding_segment(sg, p);
             }
-            n = bvh_skip(S, n, m.x);
+            n = m.x;
         } else {
             n = n + 1;
         }
@@ -761,7 +756,7 @@ __device__ __forceinline__ bool within_path_bvh(const DevScene& S, int path, flo
         float4 b = __ldg(&S.pn_bounds[n]);
         int4 m = __ldg(&S.pn_meta[n]);
         if (!(p.x >= b.x && p.x <= b.z && p.y >= b.y && p.y <= b.w)) {
-            n = bvh_skip(S, n, m.x);
+            n = m.x;
             continue;
         }
         if (m.z > 0) {
@@ -774,7 +769,7 @@ __device__ __forceinline__ bool within_path_bvh(const DevScene& S, int path, flo
                 CPRes c = seg_closest(sg, p, approx);
                 if (c.dist < seg_radius(sg, c.t) && !end_excluded(pflags, sidx - pi.x, pi.y, c.t)) return true;
             }
-            n = bvh_skip(S, n, m.x);
+            n = m.x;
         } else {
             n = n + 1;
         }
@@ -878,15 +873,6 @@ __device__ __forceinline__ int winding_shape(const DevScene& S, int s, float2 sp
 __device__ __forceinline__ bool fill_hit(int rule, int w) { return rule == 1 ? ((w < 0 ? -w : w) % 2) == 1 : w != 0; }
 
 // ------------------------------------------------------------------ group queries (distance/api.rs)
-// A point outside a group's conservative canvas box (its group-space root box mapped to
-// the canvas in f64 and padded by half a pixel plus 1e-4 of the coordinates) cannot hit
-// the group's stroke or fill without prefiltering: both tests begin with that root box
-// (within_distance_bvh api.rs:79-135, is_inside_bvh api.rs:259-309), which the point's
-// group-space image misses by far more than the f32 rounding of the transform.
-__device__ __forceinline__ bool outside_group_box(const DevScene& S, int g, float2 pt) {
-    const float4 b = __ldg(&S.g_bbox[g]);
-    return pt.x < b.x || pt.x > b.z || pt.y < b.y || pt.y > b.w;
-}
 // within_distance_bvh (api.rs:79-135) with the brute-force fallback (api.rs:15-33).
 __device__ __forceinline__ bool group_within(const DevScene& S, int g, float2 lp) {
     int4 gb = __ldg(&S.g_bvh[g]);
@@ -904,7 +890,7 @@ __device__ __forceinline__ bool group_within(const DevScene& S, int g, float2 lp
         float4 b = __ldg(&S.gn_bounds[n]);
         int4 m = __ldg(&S.gn_meta[n]);
         if (!(lp.x >= b.x && lp.x <= b.z && lp.y >= b.y && lp.y <= b.w)) {
-            n = bvh_skip(S, n, m.x);
+            n = m.x;
             continue;
         }
         if (m.z > 0) {
@@ -919,7 +905,7 @@ __device__ __forceinline__ bool group_within(const DevScene& S, int g, float2 lp
                     return true;
                 }
             }
-            n = bvh_skip(S, n, m.x);
+            n = m.x;
         } else {
             n = n + 1;
         }
@@ -946,7 +932,7 @@ __device__ __forceinline__ bool group_inside(const DevScene& S, int g, float2 lp
         float4 b = __ldg(&S.gn_bounds[n]);
         int4 m = __ldg(&S.gn_meta[n]);
         if (!(lp.x >= b.x && lp.x <= b.z && lp.y >= b.y && lp.y <= b.w)) {
-            n = bvh_skip(S, n, m.x);
+            n = m.x;
             continue;
         }
         if (m.z > 0) {
@@ -954,7 +940,7 @@ __device__ __forceinline__ bool group_inside(const DevScene& S, int g, float2 lp
                 int s = __ldg(&S.gl_shapes[k]);
                 w += winding_shape(S, s, shape_local_dist(S, s, lp), true);
             }
-            n = bvh_skip(S, n, m.x);
+            n = m.x;
         } else {
             n = n + 1;
         }

@@ -216,13 +216,11 @@ __device__ __forceinline__ void forward_body(const DevScene& S, const SamplePara
         for (int e = 0; e < n; ++e) {
             const int g = __ldg(&list[e]);
             // stroke first, then fill; one paint call site for both
-            int hitp[2] = {-1, -1};
-            if (!outside_group_box(S, g, pt)) {
-                const int4 gi = __ldg(&S.g_info[g]);
-                const float2 lp = xf9(S.g_c2s + 9 * g, pt);
-                hitp[0] = gi.y >= 0 && group_within(S, g, lp) ? gi.y : -1;
-                hitp[1] = gi.x >= 0 && group_inside(S, g, lp, gi.z) ? gi.x : -1;
-            }
+            const int4 gi = __ldg(&S.g_info[g]);
+            const float2 lp = xf9(S.g_c2s + 9 * g, pt);
+            int hitp[2];
+            hitp[0] = gi.y >= 0 && group_within(S, g, lp) ? gi.y : -1;
+            hitp[1] = gi.x >= 0 && group_inside(S, g, lp, gi.z) ? gi.x : -1;
 #pragma unroll 1
             for (int which = 0; which < 2; ++which)
                 if (hitp[which] >= 0) {
@@ -366,13 +364,10 @@ __device__ __forceinline__ void interior_body(const DevScene& S, const SamplePar
             } else {
                 e = k;
                 const int g = __ldg(&list[e]);
-                hitp[0] = hitp[1] = -1;
-                if (!outside_group_box(S, g, pt)) {
-                    const int4 gi = __ldg(&S.g_info[g]);
-                    const float2 lp = xf9(S.g_c2s + 9 * g, pt);
-                    hitp[0] = gi.y >= 0 && group_within(S, g, lp) ? gi.y : -1;
-                    hitp[1] = gi.x >= 0 && group_inside(S, g, lp, gi.z) ? gi.x : -1;
-                }
+                const int4 gi = __ldg(&S.g_info[g]);
+                const float2 lp = xf9(S.g_c2s + 9 * g, pt);
+                hitp[0] = gi.y >= 0 && group_within(S, g, lp) ? gi.y : -1;
+                hitp[1] = gi.x >= 0 && group_inside(S, g, lp, gi.z) ? gi.x : -1;
             }
 #pragma unroll 1
             for (int which = 0; which < 2; ++which) {
@@ -554,13 +549,11 @@ __device__ float4 edge_color(const DevScene& S, int tile, float2 pt, float4 bg, 
     for (int e = 0; e < n; ++e) {
         const int g = __ldg(&list[e]);
         // stroke first, then fill; one paint call site for both
-        int hitp[2] = {-1, -1};
-        if (!outside_group_box(S, g, pt)) {
-            const int4 gi = __ldg(&S.g_info[g]);
-            const float2 lp = xf9(S.g_c2s + 9 * g, pt);
-            hitp[0] = gi.y >= 0 && group_within(S, g, lp) ? gi.y : -1;
-            hitp[1] = gi.x >= 0 && group_inside(S, g, lp, gi.z) ? gi.x : -1;
-        }
+        const int4 gi = __ldg(&S.g_info[g]);
+        const float2 lp = xf9(S.g_c2s + 9 * g, pt);
+        int hitp[2];
+        hitp[0] = gi.y >= 0 && group_within(S, g, lp) ? gi.y : -1;
+        hitp[1] = gi.x >= 0 && group_inside(S, g, lp, gi.z) ? gi.x : -1;
 #pragma unroll 1
         for (int which = 0; which < 2; ++which) {
             if (hitp[which] < 0) continue;
@@ -1405,26 +1398,36 @@ __global__ void k_boundary_scatter(const int* key, uint64_t n, int* cursor, int*
 }
 // Stage 3: evaluate both sides of every edge sample in tile order, so that the
 // lanes of a warp share one group list (render_edge_sample, boundary.rs:845-967).
+// Two lanes per sample: the even lane of a pair takes the colour inside, the odd lane
+// the colour outside.  The two points are 2e-4 of the canvas apart, so a pair walks
+// the same BVH nodes and segment tests in lockstep; the even lane receives the odd
+// lane's colour and hit by shuffle and finishes the sample alone.  Every lane of the
+// warp reaches the shuffles (`valid` false: a pair past the last sample).
 template <bool STYLED>
-__device__ __forceinline__ void boundary_eval_one(const DevScene& S, const BSample& r, const float* d_render,
-                                                  const float* wsum, const GradPtrs& G) {
+__device__ __forceinline__ void boundary_eval_pair(const DevScene& S, const BSample& r, bool valid,
+                                                   const float* d_render, const float* wsum, const GradPtrs& G) {
     const float W = (float)S.width, H = (float)S.height;
-    const float4 bg = background_premul(S, r.pixel);
-    const int tile = ((r.pixel / S.width) / TILE) * S.tiles_x + ((r.pixel % S.width) / TILE);
-    float2 nc = make_float2(r.nx, r.ny);
-    bool hi, ho;
-    const float2 pin = make_float2(r.bx - nc.x * 1.0e-4f, r.by - nc.y * 1.0e-4f);
-    const float2 pout = make_float2(r.bx + nc.x * 1.0e-4f, r.by + nc.y * 1.0e-4f);
-    float4 cc[2];
-    bool hh[2];
-#pragma unroll 1
-    for (int side = 0; side < 2; ++side) {
-        const float2 q = side == 0 ? pin : pout;
-        cc[side] = edge_color(S, tile, make_float2(q.x * W, q.y * H), bg, r.group, r.shape, &hh[side]);
+    const int side = threadIdx.x & 1;
+    float4 cs = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    bool hs = false;
+    float4 bg = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (valid) {
+        bg = background_premul(S, r.pixel);
+        const int tile = ((r.pixel / S.width) / TILE) * S.tiles_x + ((r.pixel % S.width) / TILE);
+        const float o = side == 0 ? -1.0e-4f : 1.0e-4f;
+        const float2 q = make_float2(r.bx + r.nx * o, r.by + r.ny * o);
+        cs = edge_color(S, tile, make_float2(q.x * W, q.y * H), bg, r.group, r.shape, &hs);
     }
-    float4 ci = cc[0], co = cc[1];
-    hi = hh[0];
-    ho = hh[1];
+    float4 co;
+    co.x = __shfl_xor_sync(0xffffffffu, cs.x, 1);
+    co.y = __shfl_xor_sync(0xffffffffu, cs.y, 1);
+    co.z = __shfl_xor_sync(0xffffffffu, cs.z, 1);
+    co.w = __shfl_xor_sync(0xffffffffu, cs.w, 1);
+    const bool ho = __shfl_xor_sync(0xffffffffu, (int)hs, 1) != 0;
+    if (!valid || side != 0) return;
+    float2 nc = make_float2(r.nx, r.ny);
+    float4 ci = cs;
+    const bool hi = hs;
     if (!hi && !ho) return;
     if (!hi) {
         nc = make_float2(nc.x * -1.0f, nc.y * -1.0f);
@@ -1476,24 +1479,28 @@ __device__ __forceinline__ void boundary_eval_one(const DevScene& S, const BSamp
         add_if(G.d_translation + 2 * (size_t)r.pixel + 1, nc.y * contrib);
     }
 }
+// Two threads per sample (boundary_eval_pair): launch 2 * samples threads.
 template <bool STYLED>
 __global__ void __launch_bounds__(128, DVG_MINB_BND) k_boundary_eval(DevScene S, const BSample* samples,
                                                                      const int* order, const int* offsets, int tiles,
                                                                      const float* d_render, const float* wsum,
                                                                      GradPtrs G) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= offsets[tiles]) return;
-    boundary_eval_one<STYLED>(S, samples[order[i]], d_render, wsum, G);
+    const int64_t i = (int64_t)(((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 1);
+    const bool valid = i < offsets[tiles];
+    BSample r{};
+    if (valid) r = samples[order[i]];
+    boundary_eval_pair<STYLED>(S, r, valid, d_render, wsum, G);
 }
 template <bool STYLED>
 __global__ void __launch_bounds__(128, DVG_MINB_BND) k_boundary_eval_batch(const BatchEntry* __restrict__ B,
                                                                            const BSample* samples, const int* order,
                                                                            const int* offsets, int tiles) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= offsets[tiles]) return;
-    const BSample r = samples[order[i]];
-    const BatchEntry& E = B[r.scene];
-    boundary_eval_one<STYLED>(E.S, r, E.d_render, E.wsum, E.G);
+    const int64_t i = (int64_t)(((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 1);
+    const bool valid = i < offsets[tiles];
+    BSample r{};
+    if (valid) r = samples[order[i]];
+    const BatchEntry& E = B[valid ? r.scene : 0];
+    boundary_eval_pair<STYLED>(E.S, r, valid, E.d_render, E.wsum, E.G);
 }
 
 // ------------------------------------------------------------------ background finalisation (background.rs:29-61)
@@ -1677,11 +1684,11 @@ int launch_boundary(const DevScene& S, const BoundaryParams& bp, const float* d_
         cudaMemcpyAsync(counts, offsets, sizeof(int) * (size_t)tiles, cudaMemcpyDeviceToDevice, stream);
         k_boundary_scatter<<<(unsigned)((cnt + 255) / 256), 256, 0, stream>>>(key, cnt, counts, order);
         if (S.styled)
-            k_boundary_eval<true><<<(unsigned)((cnt + 127) / 128), 128, 0, stream>>>(S, samples, order, offsets,
-                                                                                  tiles, d_render, wsum, G);
+            k_boundary_eval<true><<<(unsigned)((2 * cnt + 127) / 128), 128, 0, stream>>>(S, samples, order, offsets,
+                                                                                      tiles, d_render, wsum, G);
         else
-            k_boundary_eval<false><<<(unsigned)((cnt + 127) / 128), 128, 0, stream>>>(S, samples, order, offsets,
-                                                                                   tiles, d_render, wsum, G);
+            k_boundary_eval<false><<<(unsigned)((2 * cnt + 127) / 128), 128, 0, stream>>>(S, samples, order, offsets,
+                                                                                       tiles, d_render, wsum, G);
         launches += 3;
     }
     return launches;
@@ -1746,11 +1753,11 @@ int launch_boundary_batch(const BatchEntry* B, int nscenes, uint64_t total, int 
     cudaMemcpyAsync(counts, offsets, sizeof(int) * (size_t)total_tiles, cudaMemcpyDeviceToDevice, stream);
     k_boundary_scatter<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(key, total, counts, order);
     if (styled)
-        k_boundary_eval_batch<true><<<(unsigned)((total + 127) / 128), 128, 0, stream>>>(B, samples, order, offsets,
-                                                                                     total_tiles);
+        k_boundary_eval_batch<true><<<(unsigned)((2 * total + 127) / 128), 128, 0, stream>>>(B, samples, order,
+                                                                                         offsets, total_tiles);
     else
-        k_boundary_eval_batch<false><<<(unsigned)((total + 127) / 128), 128, 0, stream>>>(B, samples, order,
-                                                                                      offsets, total_tiles);
+        k_boundary_eval_batch<false><<<(unsigned)((2 * total + 127) / 128), 128, 0, stream>>>(B, samples, order,
+                                                                                          offsets, total_tiles);
     return 3 + scans;
 }
 

@@ -18,7 +18,8 @@ src/backward/boundary.rs:113-1148).  Two checks of its expectation over boundary
 2. Against finite differences of the rendered image.  Right: central differences of
    L = sum(d_render * image) in f64 with common random numbers (the same jitter seed
    on both sides), averaged over 256 jitter seeds.  Steps: 0.1 pixel for points and
-   translations, 0.1 pixel / 64 for the linear transform entries.  Scene: four smooth
+   translations, 0.1 pixel / 64 for the linear transform entries, whose differences are
+   extrapolated from h and h/2 (Richardson) to cancel their h^2 term.  Scene: four smooth
    closed cubic outlines, one per quadrant, whose boundaries cross neither themselves
    nor each other (see below), untransformed for the control points and rotated about
    their own centres for the transform entries.
@@ -182,9 +183,24 @@ def _boundary_runs(r, sc, dr, names, n_seeds):
     return {n: np.asarray(v) for n, v in runs.items()}
 
 
-def _z_scores_fd(r, sc, target_sc, params):
+def _central(r, sc, dr_dev, get, put, h):
+    """Central differences per jitter seed (common random numbers on both sides)."""
+    v = get()
+    hp, hm = float(np.float32(v + h)), float(np.float32(v - h))
+    put(hp)
+    lp = _losses(r, sc, dr_dev, JITTER_SEEDS)
+    put(hm)
+    lm = _losses(r, sc, dr_dev, JITTER_SEEDS)
+    put(v)
+    return (lp - lm) / (hp - hm)
+
+
+def _z_scores_fd(r, sc, target_sc, params, richardson=False):
     """Per parameter: |mean boundary-sampled gradient - mean finite difference| over the
-    combined standard error (see the module docstring)."""
+    combined standard error (see the module docstring).  richardson: (4 D(h/2) - D(h)) / 3
+    per jitter seed, which cancels the h^2 term of the central differences D (the
+    transforms' linear entries move points far from the origin by up to 0.15 px at h,
+    where that term reaches ~10 % of some entries)."""
     import torch
 
     dr = _d_render(r, sc, target_sc)
@@ -192,14 +208,9 @@ def _z_scores_fd(r, sc, target_sc, params):
     runs = _boundary_runs(r, sc, dr, sorted({p[0] for p in params}), PHILOX_SEEDS)
     z = []
     for name, idx, get, put, h in params:
-        v = get()
-        hp, hm = float(np.float32(v + h)), float(np.float32(v - h))
-        put(hp)
-        lp = _losses(r, sc, dr_dev, JITTER_SEEDS)
-        put(hm)
-        lm = _losses(r, sc, dr_dev, JITTER_SEEDS)
-        put(v)
-        fd = (lp - lm) / (hp - hm)
+        fd = _central(r, sc, dr_dev, get, put, h)
+        if richardson:
+            fd = (4.0 * _central(r, sc, dr_dev, get, put, h / 2) - fd) / 3.0
         a = runs[name][:, idx]
         se = np.sqrt(a.var(ddof=1) / a.size + fd.var(ddof=1) / fd.size)
         diff = abs(a.mean() - fd.mean())
@@ -273,8 +284,8 @@ def test_cuda_boundary_transform_gradients_match_fd_in_expectation():
     r = Renderer(0)
     try:
         sc = _rigid_about_centres(separated_blobs(seed=0))
-        _assert_within_3_sigma(_z_scores_fd(r, sc, separated_blobs(seed=1), _params(sc, points=False, xforms=True)),
-                               40)
+        _assert_within_3_sigma(_z_scores_fd(r, sc, separated_blobs(seed=1), _params(sc, points=False, xforms=True),
+                                            richardson=True), 40)
     finally:
         r.close()
 
