@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include "prepare.hpp"  // ShapeFlags shared with the host preparation
+#include "winding_newton.cuh"
 
 namespace dvgb {
 
@@ -453,6 +454,21 @@ __device__ __forceinline__ float seg_radius(const SegGeom& s, float t) {  // clo
     if (s.kind == 1) return tt * tt * s.r[0] + 2.0f * tt * t * s.r[1] + t * t * s.r[2];
     return tt * tt * tt * s.r[0] + 3.0f * tt * tt * t * s.r[1] + 3.0f * tt * t * t * s.r[2] + t * t * t * s.r[3];
 }
+// The crate's cubic crossings: its f64 roots (solve_cubic) and decisions (winding.rs:170-192).
+static __device__ __noinline__ int winding_cubic_exact(double a, double b, double c, double d, double ax, double bx,
+                                                       double cx, double dx) {
+    double r[3];
+    int nr = solve_cubic(a, b, c, d, r);
+    int w = 0;
+    for (int i = 0; i < nr; ++i) {
+        double t = r[i];
+        if (t >= 0.0 && t <= 1.0) {
+            double tp = ax * t * t * t + bx * t * t + cx * t + dx;
+            if (tp > 0.0) w += (3.0 * a * t * t + 2.0 * b * t + c) > 0.0 ? 1 : -1;
+        }
+    }
+    return w;
+}
 // winding.rs:118-192
 static __device__ __noinline__ int winding_segment_v(int kind, float a0, float a1, float a2, float a3, float a4, float a5, float a6, float a7, float2 pt) {
     const float q[8] = {a0, a1, a2, a3, a4, a5, a6, a7};
@@ -497,21 +513,13 @@ static __device__ __noinline__ int winding_segment_v(int kind, float a0, float a
     double b = (double)(3.0f * q[1] - 6.0f * q[3] + 3.0f * q[5]);
     double c = (double)(-3.0f * q[1] + 3.0f * q[3]);
     double d = (double)(q[1] - pt.y);
-    double r[3];
-    int nr = solve_cubic(a, b, c, d, r);
     double ax = (double)(-q[0] + 3.0f * q[2] - 3.0f * q[4] + q[6]);
     double bx = (double)(3.0f * q[0] - 6.0f * q[2] + 3.0f * q[4]);
     double cx = (double)(-3.0f * q[0] + 3.0f * q[2]);
     double dx = (double)(q[0] - pt.x);
-    int w = 0;
-    for (int i = 0; i < nr; ++i) {
-        double t = r[i];
-        if (t >= 0.0 && t <= 1.0) {
-            double tp = ax * t * t * t + bx * t * t + cx * t + dx;
-            if (tp > 0.0) w += (3.0 * a * t * t + 2.0 * b * t + c) > 0.0 ? 1 : -1;
-        }
-    }
-    return w;
+    // the crate's decisions without its f64 acos / cos / pow whenever they provably agree
+    const int wn = winding_cubic_newton(a, b, c, d, ax, bx, cx, dx);
+    return wn != WIND_UNSURE ? wn : winding_cubic_exact(a, b, c, d, ax, bx, cx, dx);
 }
 __device__ __forceinline__ int winding_segment(const SegGeom& s, float2 pt) {
     return winding_segment_v(s.kind, s.q[0], s.q[1], s.q[2], s.q[3], s.q[4], s.q[5], s.q[6], s.q[7], pt);
