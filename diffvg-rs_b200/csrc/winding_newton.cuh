@@ -149,18 +149,22 @@ DVG_WN_HD int winding_cubic_newton(double a, double b, double c, double d, doubl
     if (!(aq3 < 1.0e30f && ar2 < 1.0e30f)) return WIND_UNSURE;
     int w = 0;
     if (rr < q3) {  // three roots
-        // 1 - x^2 for the crate's x = r / sqrt(q^3), without its sqrt
-        if (!(q3 - rr >= 1.0e-8 * q3)) return WIND_UNSURE;  // near a double root
-        const float q3f = (float)q3;
+        // 1 - x^2 >= 1e-6 for the crate's x = r / sqrt(q^3) (without its sqrt)
+        if (!(q3 - rr >= 1.0e-6 * q3)) return WIND_UNSURE;  // near a double root
         const float sq = std::sqrt((float)q);
         if (!(sq > 1.0e-30f && sq < 1.0e12f)) return WIND_UNSURE;
-        const float rs = wn_rsqrt(q3f);
-        const float th = std::acos(std::fmin(std::fmax((float)r * rs, -1.0f), 1.0f));
-        // the crate's rounding: acos(x) within (4 eps / sqrt(1 - x^2) + 8 eps) of the exact
-        // angle (x carries the rounding of sqrt, q^3 and the division), the cosines and
-        // products a few eps more; 2 sqrt(q) times that bounds its root, doubled.
-        const float sep_rs = wn_rsqrt((float)(q3 - rr)) * (q3f * rs);  // 1 / sqrt(1 - x^2)
-        const float ec = 4.0f * sq * (float)WN_EPS * (8.2f * sep_rs + 32.0f);
+        const float th = std::acos(std::fmin(std::fmax((float)r * wn_rsqrt((float)q3), -1.0f), 1.0f));
+        // the crate's rounding: acos(x) within 4 eps / sqrt(1 - x^2) + 8 eps (<= 4008 eps) of
+        // the exact angle (x carries the rounding of sqrt, q^3 and the division), the cosines
+        // and products a few eps more; 2 sqrt(q) times that bounds its root, doubled.
+        const float ec = 3.7e-12f * sq;
+        // the f32 estimates: x within 5e-7 of its value (casts, rsqrt, product), acos within
+        // 2 ulp, so the angle within 5e-4 (1 / sqrt(1 - x^2) <= 1e3), the cosine (fast, 2^-21
+        // absolute) and sqrt(q) a little more: each estimate within 3.4e-4 sqrt(q) of the
+        // crate's root of the same index; 2e-3 sqrt(q) allowed.  A root whose estimate lies
+        // farther than that outside [0, 1] is outside for the crate too and needs no Newton step.
+        const float e0 = 2.0e-3f * sq;
+        const float fb3 = (float)b3;
         // g is monotone between its stationary points -sqrt(q), sqrt(q): the crate's roots
         // k = 0, 2, 1 are the one root in (-inf, -sqrt q), (-sqrt q, sqrt q), (sqrt q, inf);
         // a certified root strictly inside its interval is the crate's k-th root.
@@ -170,6 +174,10 @@ DVG_WN_HD int winding_cubic_newton(double a, double b, double c, double d, doubl
             const float phi = (th + (k == 0 ? 0.0f : (k == 1 ? 6.2831853f : -6.2831853f))) * (1.0f / 3.0f);
             float y0 = -2.0f * sq * wn_cos(phi);
             if (perturb) y0 += perturb[k] * 2.0f * sq;
+            {
+                const float t0 = y0 - fb3, e = e0 + 2.4e-7f * (std::fabs(y0) + std::fabs(fb3));
+                if (t0 + e < 0.0f || t0 - e > 1.0f) continue;
+            }
             float u;
             const double y = wn_newton(y0, q3x, r2x, q, aq3, ar2, &u);
             if (u < 0.0f) return WIND_UNSURE;

@@ -4,10 +4,13 @@ the crate's f64 computation (winding_number_segment, src/distance/winding.rs:170
 Random segments with query points near the curve, integer alignments, near-degenerate
 cubics (elevated quadratics, lines, cusps, tiny loops), query rows exactly at end points
 and extrema, large coordinates, scene-like tests and rows within 1e-12..1e-2 of a y
-extremum (near double roots); the f32 root estimates also moved by up to 1e-5 and 1e-4
-of their formula's scale (the device's fast cosine errs by about 2^-21).  Never a
-decision that differs from the crate's; nearly all of a scene's tests decided without
-the crate's formula."""
+extremum (near double roots); the f32 root estimates also moved by up to 1e-5, 1e-4 and
+8e-4 of their formula's scale 2 sqrt(q) (the device's estimates are within 1.7e-4 of it:
+fast cosine, f32 acos of a rounded argument); the library skips the Newton step of a root
+whose estimate lies more than 2e-3 sqrt(q) outside [0, 1], and a harness run with larger
+moves (2.5e-3 of the scale) does find wrong decisions, so the cases reach that test.
+Never a decision that differs from the crate's; nearly all of a scene's tests decided
+without the crate's formula."""
 import ctypes as C
 import os
 import subprocess
@@ -35,11 +38,18 @@ def stress():
     return run
 
 
-@pytest.mark.parametrize("perturb", [0.0, 1e-5, 1e-4])
+@pytest.mark.parametrize("perturb", [0.0, 1e-5, 1e-4, 8e-4])
 @pytest.mark.parametrize("mode", range(len(MODES)), ids=MODES)
 def test_newton_winding_never_disagrees(stress, mode, perturb):
     cases, decided, wrong = stress(mode, 11, 2_000_000, perturb)
     assert cases == 2_000_000
     assert wrong == 0, f"{wrong} decisions differ from the crate's ({MODES[mode]})"
-    if mode == 5:
-        assert decided >= 0.999 * cases, f"only {decided / cases:.4f} of a scene's tests decided"
+    if mode == 5 and perturb <= 1e-4:  # the device's estimates err by ~1e-7 of the scale, rarely more
+        bar = 0.999 if perturb <= 1e-5 else 0.995
+        assert decided >= bar * cases, f"only {decided / cases:.4f} of a scene's tests decided"
+
+
+def test_harness_finds_wrong_decisions_beyond_the_estimate_bound(stress):
+    """Estimates moved past the 2e-3 sqrt(q) skip bound: the harness must see wrong decisions."""
+    wrong = sum(stress(mode, 5, 1_000_000, 2.5e-3)[2] for mode in range(len(MODES)))
+    assert wrong > 0
