@@ -134,7 +134,7 @@ struct dvg_scene {
     size_t grad_floats = 0;
     size_t arena_bytes = 0;  // bytes of prepared tables in `arena`
     const float4* g_bbox = nullptr;
-    dvg_tuning tune{1, 4, 16, 0};  // launch shape (dvg_scene_set_tuning / dvg_scene_autotune)
+    dvg_tuning tune{1, 4, 16, 0, 0};  // launch shape (dvg_scene_set_tuning / dvg_scene_autotune)
 };
 
 namespace {
@@ -234,9 +234,10 @@ dvg_status check_options(const dvg_render_options* o) {
     if (!o) return fail(DVG_ERR_INVALID_ARGUMENT, "null render options");
     return DVG_OK;
 }
-SampleParams sample_params(const dvg_render_options* o, int layout = 1) {
+SampleParams sample_params(const dvg_render_options* o, const dvg_tuning& tune) {
     SampleParams sp;
-    sp.layout = layout;
+    sp.layout = (int)tune.sample_layout;
+    sp.fwd_occ = (int)tune.forward_occupancy;
     sp.sxn = o->samples_x > 0 ? (int)o->samples_x : 1;
     sp.syn = o->samples_y > 0 ? (int)o->samples_y : 1;
     sp.seed = o->seed;
@@ -531,7 +532,7 @@ static dvg_status render_into(dvg_context* ctx, dvg_scene* sc, const dvg_render_
         return DVG_OK;
     }
     ++ctx->gen;  // accum, wsum and the fragment cache are rewritten below
-    SampleParams sp = sample_params(opts, (int)sc->tune.sample_layout);
+    SampleParams sp = sample_params(opts, sc->tune);
     if (frag_out && !opts->use_prefiltering && sc->tune.fragment_slots > 0) {
         const int tiles = S.tiles_x * S.tiles_y, slots = (int)sc->tune.fragment_slots;
         CK(ctx->frag.reserve(frag_cache_bytes(tiles, sp.sxn * sp.syn, slots)));
@@ -609,7 +610,7 @@ static dvg_status backward_core(dvg_context* ctx, dvg_scene* sc, const dvg_rende
     const DevScene& S = sc->dev;
     const size_t npix = (size_t)S.width * S.height;
     if (npix == 0) return DVG_OK;
-    SampleParams sp = sample_params(opts, (int)sc->tune.sample_layout);
+    SampleParams sp = sample_params(opts, sc->tune);
     if (frag_ready) attach_frag(sp, ctx->frag.ptr, S.tiles_x * S.tiles_y, (int)sc->tune.fragment_slots);
     const bool run_tiles = !shard || shard->tile_end > shard->tile_begin;  // a shard may hold samples only
     if (shard && run_tiles) {
@@ -969,7 +970,7 @@ dvg_status dvg_shard_forward(dvg_context* ctx, dvg_scene* scene, const dvg_rende
     CK(cudaMemsetAsync(accum_rgba, 0, npix * 4 * sizeof(float), ctx->stream));
     CK(cudaMemsetAsync(wsum, 0, npix * sizeof(float), ctx->stream));
     if (S.num_groups == 0 || shard->tile_end == shard->tile_begin) return DVG_OK;
-    SampleParams sp = sample_params(opts, (int)scene->tune.sample_layout);
+    SampleParams sp = sample_params(opts, scene->tune);
     sp.tile_base = (int)shard->tile_begin;
     sp.tile_count = (int)(shard->tile_end - shard->tile_begin);
     bool frag = false;
@@ -1116,7 +1117,7 @@ extern "C" dvg_status dvg_render_device_noalloc(dvg_context* ctx, dvg_scene* sce
     float* accum = scratch;            // 4 floats per pixel (float4 aligned: 256-byte base)
     float* wsum = scratch + 4 * npix;  // 1 float per pixel
     CK(cudaMemsetAsync(scratch, 0, 5 * npix * sizeof(float), ctx->stream));
-    const SampleParams sp = sample_params(opts, (int)scene->tune.sample_layout);
+    const SampleParams sp = sample_params(opts, scene->tune);
     if (opts->use_prefiltering)
         ctx->launches += launch_forward_prefilter(S, sp, accum, wsum, ctx->status, ctx->stream);
     else
@@ -1147,7 +1148,7 @@ struct dvg_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     uint64_t steps = 0;
-    dvg_tuning tune{1, 4, 16, 0};  // launch shape (dvg_batch_autotune)
+    dvg_tuning tune{1, 4, 16, 0, 0};  // launch shape (dvg_batch_autotune)
     // on-device optimisation step (dvg_batch_set_adam)
     bool adam = false;
     AdamParams ap{};
@@ -1175,7 +1176,8 @@ dvg_status batch_enqueue(dvg_batch* b) {
         ctx->launches += launch_forward_prefilter_batch(B, b->work.as<int2>(), b->items, queue, b->max_ri,
                                                         ctx->status, ctx->stream);
     else
-        ctx->launches += launch_forward_batch(B, b->work.as<int2>(), b->items, queue, b->max_ri, ctx->stream);
+        ctx->launches += launch_forward_batch(B, b->work.as<int2>(), b->items, queue, b->max_ri,
+                                              (int)b->tune.forward_occupancy, ctx->stream);
     ctx->launches += launch_pixels_batch(B, n, b->max_pixels, 0, ctx->stream);
     ctx->launches += launch_pixels_batch(B, n, b->max_pixels, 1, ctx->stream);
     if (pre)
@@ -1220,6 +1222,7 @@ dvg_status batch_apply_tuning(dvg_batch* b) {
     for (size_t i = 0; i < b->host_entries.size(); ++i) {
         BatchEntry& e = b->host_entries[i];
         e.sp.layout = (int)b->tune.sample_layout;
+        e.sp.fwd_occ = (int)b->tune.forward_occupancy;
         e.sp.frag = nullptr;
         e.sp.frag_n = nullptr;
         e.sp.frag_slots = 0;
@@ -1249,7 +1252,7 @@ extern "C" dvg_status dvg_batch_create(dvg_context* ctx, dvg_scene* const* scene
     else {
         b->bopts.boundary_seed_from_options = 1;
     }
-    const SampleParams sp = sample_params(opts);
+    const SampleParams sp = sample_params(opts, dvg_tuning{1, 4, 16, 0, 0});
     // Work items (scene, tile + tiles * sub-sample round), one CTA each, listed heaviest
     // first: the hardware hands out CTAs in list order as SMs free up, so the longest
     // items start first and the stage's tail is made of short ones.  Weight: the groups
@@ -1591,7 +1594,7 @@ extern "C" dvg_status dvg_render_sdf_device(dvg_context* ctx, dvg_scene* scene, 
     }
     {
         Prof prof_(ctx, "render_sdf");
-        ctx->launches += launch_render_sdf(S, sample_params(opts), out, ctx->status, ctx->stream);
+        ctx->launches += launch_render_sdf(S, sample_params(opts, dvg_tuning{1, 4, 16, 0, 0}), out, ctx->status, ctx->stream);
     }
     CK(cudaGetLastError());
     return DVG_OK;
@@ -1804,12 +1807,14 @@ namespace {
 bool tuning_valid(const dvg_tuning* t) {
     return t && t->sample_layout <= 1 &&
            (t->boundary_cell == 2 || t->boundary_cell == 4 || t->boundary_cell == 8 || t->boundary_cell == 16) &&
-           t->fragment_slots <= (uint32_t)FRAG_MAX_SLOTS && t->work_queue <= 1;
+           t->fragment_slots <= (uint32_t)FRAG_MAX_SLOTS && t->work_queue <= 1 &&
+           t->forward_occupancy <= 1;
 }
 // The candidates: both warp layouts with the default cell and cache, then every cell
 // with the better layout (the boundary pass does not depend on the layout), then the
 // fragment-cache sizes (`try_slots`: only where the cache is used, non-prefiltered),
-// then persistent CTAs for the batch stages (`try_queue`).
+// then persistent CTAs for the batch stages (`try_queue`), then the forward kernel at
+// 3 CTAs per SM.
 template <typename Apply, typename Run>
 dvg_status autotune_loop(dvg_context* ctx, dvg_tuning* tune, bool try_slots, Apply apply, Run run,
                          bool try_queue = false) {
@@ -1858,7 +1863,8 @@ dvg_status autotune_loop(dvg_context* ctx, dvg_tuning* tune, bool try_slots, App
         const dvg_tuning b2 = best;
         for (int k = 0; k < 3; ++k) consider(dvg_tuning{b2.sample_layout, b2.boundary_cell, slots[k]});
     }
-    if (try_queue) consider(dvg_tuning{best.sample_layout, best.boundary_cell, best.fragment_slots, 1});
+    if (try_queue) consider(dvg_tuning{best.sample_layout, best.boundary_cell, best.fragment_slots, 1, 0});
+    consider(dvg_tuning{best.sample_layout, best.boundary_cell, best.fragment_slots, best.work_queue, 1});
     *tune = best;
     if (st == DVG_OK) st = apply();
     cudaEventDestroy(e0);

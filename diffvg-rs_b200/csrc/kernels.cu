@@ -18,14 +18,12 @@
 
 // Minimum resident CTAs per SM for the scene-evaluation kernels (register cap =
 // 65536 / (threads * value)); chosen by measurement on B200.
-#ifndef DVG_MINB_FWD
-#define DVG_MINB_FWD 2
-#endif
+// (the non-prefiltered forward is compiled for 2 and for 3, see dvg_tuning.forward_occupancy)
 #ifndef DVG_MINB_INT
 #define DVG_MINB_INT 2
 #endif
 #ifndef DVG_MINB_BND
-#define DVG_MINB_BND 8  // 64 registers: more warps for the two-sided edge evaluation outweigh its spills
+#define DVG_MINB_BND 12  // 40 registers: more warps for the two-lane edge evaluation outweigh its spills
 #endif
 #ifndef DVG_MINB_LEAN
 #define DVG_MINB_LEAN 4
@@ -238,16 +236,17 @@ __device__ __forceinline__ void forward_body(const DevScene& S, const SamplePara
     __syncthreads();
     flush_splat(S, tx, ty, ri, HW, sm, accum, wsum);
 }
-__global__ void __launch_bounds__(256, DVG_MINB_FWD) k_forward(DevScene S, SampleParams sp, float* accum, float* wsum,
-                                                               unsigned* status) {
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_forward(DevScene S, SampleParams sp, float* accum, float* wsum,
+                                                       unsigned* status) {
     extern __shared__ float sm[];
     (void)status;
     forward_body(S, sp, sp.tile_base + blockIdx.x, blockIdx.y, accum, wsum, sm);
 }
 // Batched forward: one flat grid over every (scene, tile, sub-sample) work item.
-__global__ void __launch_bounds__(256, DVG_MINB_FWD) k_forward_batch(const BatchEntry* __restrict__ B,
-                                                                     const int2* __restrict__ work, int items,
-                                                                     int* counter) {
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_forward_batch(const BatchEntry* __restrict__ B,
+                                                             const int2* __restrict__ work, int items, int* counter) {
     extern __shared__ float sm[];
     for_each_item(items, counter, [&](int i) {
         const int2 wk = work[i];  // (scene, tile + tiles * sub-sample round)
@@ -1644,7 +1643,10 @@ int launch_forward(const DevScene& S, const SampleParams& sp, float* accum, floa
     const int hw = TILE + 2 * S.filter_ri;
     size_t smem = S.filter_ri <= MAX_SMEM_RI ? (size_t)hw * hw * 5 * sizeof(float) : 0;
     dim3 grid(launch_tiles(S, sp), sp.sxn * sp.syn);
-    k_forward<<<grid, 256, smem, stream>>>(S, sp, accum, wsum, status);
+    if (sp.fwd_occ == 1)
+        k_forward<3><<<grid, 256, smem, stream>>>(S, sp, accum, wsum, status);
+    else
+        k_forward<2><<<grid, 256, smem, stream>>>(S, sp, accum, wsum, status);
     return 1;
 }
 int launch_weights(const DevScene& S, const SampleParams& sp, float* wsum, cudaStream_t stream) {
@@ -1708,12 +1710,17 @@ int persistent_grid(K kernel, size_t smem, int items) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, smem);
     return std::max(1, std::min(items, std::max(per_sm, 1) * std::max(sms, 1)));
 }
-int launch_forward_batch(const BatchEntry* B, const int2* work, int items, int* counter, int max_ri,
+int launch_forward_batch(const BatchEntry* B, const int2* work, int items, int* counter, int max_ri, int occ,
                          cudaStream_t stream) {
     const int hw = TILE + 2 * max_ri;
     size_t smem = max_ri <= MAX_SMEM_RI ? (size_t)hw * hw * 5 * sizeof(float) : 0;
-    const int grid = counter ? persistent_grid(k_forward_batch, smem, items) : items;
-    k_forward_batch<<<grid, 256, smem, stream>>>(B, work, items, counter);
+    if (occ == 1) {
+        const int grid = counter ? persistent_grid(k_forward_batch<3>, smem, items) : items;
+        k_forward_batch<3><<<grid, 256, smem, stream>>>(B, work, items, counter);
+    } else {
+        const int grid = counter ? persistent_grid(k_forward_batch<2>, smem, items) : items;
+        k_forward_batch<2><<<grid, 256, smem, stream>>>(B, work, items, counter);
+    }
     return 1;
 }
 int launch_pixels_batch(const BatchEntry* B, int nscenes, size_t max_pixels, int which, cudaStream_t stream) {

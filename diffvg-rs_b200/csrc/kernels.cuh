@@ -51,6 +51,7 @@ struct SampleParams {
     uint8_t* frag_n; // per-sample code count or FRAG_NONE
     int frag_slots;  // codes kept per sample (<= FRAG_MAX_SLOTS)
     int tile_base, tile_count;  // the tiles a single-scene launch covers (count 0: all)
+    int fwd_occ;  // dvg_tuning.forward_occupancy: 0 = k_forward at 2 CTAs per SM, 1 = at 3
 };
 // Work items of a batched stage (work[i] = (scene, tile + tiles * sub-sample round),
 // heaviest first).  counter == nullptr: one CTA per item, item = blockIdx.x.  Otherwise
@@ -182,7 +183,7 @@ int launch_fill_background(const DevScene& S, float* out, cudaStream_t stream);
 // heaviest tiles first).  counter(s): null for one CTA per item, else zeroed device ints
 // for persistent CTAs (see for_each_item; launch_interior_batch takes two, one per
 // kernel).  which: 0 resolve, 1 L2, 2 background.
-int launch_forward_batch(const BatchEntry* B, const int2* work, int items, int* counter, int max_ri,
+int launch_forward_batch(const BatchEntry* B, const int2* work, int items, int* counter, int max_ri, int occ,
                          cudaStream_t stream);
 int launch_forward_prefilter_batch(const BatchEntry* B, const int2* work, int items, int* counter, int max_ri,
                                    unsigned* status, cudaStream_t stream);

@@ -58,12 +58,13 @@ class ShardC(C.Structure):
 
 
 def _tuple(t):
-    return int(t.sample_layout), int(t.boundary_cell), int(t.fragment_slots), int(t.work_queue)
+    return (int(t.sample_layout), int(t.boundary_cell), int(t.fragment_slots), int(t.work_queue),
+            int(t.forward_occupancy))
 
 
 class TuningC(C.Structure):
     _fields_ = [("sample_layout", C.c_uint32), ("boundary_cell", C.c_uint32), ("fragment_slots", C.c_uint32),
-                ("work_queue", C.c_uint32)]
+                ("work_queue", C.c_uint32), ("forward_occupancy", C.c_uint32)]
 
 
 class AdamOptionsC(C.Structure):
@@ -300,13 +301,15 @@ class UploadedScene:
                                                             C.c_void_p(d_render_ptr), None, C.byref(grads.c)))
 
     def tuning(self):
-        """(sample_layout, boundary_cell, fragment_slots, work_queue) used by this scene's launches."""
+        """(sample_layout, boundary_cell, fragment_slots, work_queue, forward_occupancy) used by this
+        scene's launches."""
         t = TuningC()
         _check(self.renderer.lib.dvg_scene_get_tuning(self.handle, C.byref(t)))
         return _tuple(t)
 
-    def set_tuning(self, sample_layout: int, boundary_cell: int, fragment_slots: int = 16, work_queue: int = 0) -> None:
-        t = TuningC(sample_layout, boundary_cell, fragment_slots, work_queue)
+    def set_tuning(self, sample_layout: int, boundary_cell: int, fragment_slots: int = 16, work_queue: int = 0,
+                   forward_occupancy: int = 0) -> None:
+        t = TuningC(sample_layout, boundary_cell, fragment_slots, work_queue, forward_occupancy)
         _check(self.renderer.lib.dvg_scene_set_tuning(self.handle, C.byref(t)))
 
     def autotune(self, options: RenderOptions, bopts: Optional[BackwardOptions], target_ptr: int):
@@ -579,13 +582,15 @@ class Batch:
         return out
 
     def autotune(self):
-        """dvg_batch_autotune: returns the chosen (sample_layout, boundary_cell, fragment_slots, work_queue)."""
+        """dvg_batch_autotune: returns the chosen (sample_layout, boundary_cell, fragment_slots, work_queue,
+        forward_occupancy)."""
         t = TuningC()
         _check(self.renderer.lib.dvg_batch_autotune(self.handle, C.byref(t)))
         return _tuple(t)
 
-    def set_tuning(self, sample_layout: int, boundary_cell: int, fragment_slots: int = 16, work_queue: int = 0) -> None:
-        t = TuningC(sample_layout, boundary_cell, fragment_slots, work_queue)
+    def set_tuning(self, sample_layout: int, boundary_cell: int, fragment_slots: int = 16, work_queue: int = 0,
+                   forward_occupancy: int = 0) -> None:
+        t = TuningC(sample_layout, boundary_cell, fragment_slots, work_queue, forward_occupancy)
         _check(self.renderer.lib.dvg_batch_set_tuning(self.handle, C.byref(t)))
 
     def set_adam(self, lr: float = 1e-2, betas=(0.9, 0.999), eps: float = 1e-8, points: bool = True,

@@ -194,12 +194,16 @@ typedef struct dvg_scene dvg_scene;
  * work_queue:    batches only: 0 = the forward and interior stages launch one CTA per
  *                work item (scene, tile, sub-sample), heaviest tiles first (default);
  *                1 = they launch as many persistent CTAs as the GPU holds at once, which
- *                take the items from a device counter in the same order. */
+ *                take the items from a device counter in the same order.
+ * forward_occupancy: the non-prefiltered forward kernel's register budget: 0 = 2 CTAs of
+ *                256 threads per SM (128 registers, default), 1 = 3 CTAs (85 registers:
+ *                more resident warps to cover its latencies, some spills). */
 typedef struct dvg_tuning {
     uint32_t sample_layout;
     uint32_t boundary_cell;
     uint32_t fragment_slots;
     uint32_t work_queue;
+    uint32_t forward_occupancy;
 } dvg_tuning;
 
 /* Version of this ABI (DVG_ABI_VERSION). */

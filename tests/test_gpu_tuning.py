@@ -11,8 +11,9 @@ from dvg import BackwardOptions, Batch, DeviceGrads, Renderer, RenderOptions, sy
 
 pytestmark = pytest.mark.gpu
 
+# (sample_layout, boundary_cell, fragment_slots[, work_queue, forward_occupancy])
 SHAPES = [(1, 4, 16), (0, 4, 16), (1, 2, 16), (1, 8, 16), (1, 16, 16), (0, 16, 16), (1, 4, 0), (0, 4, 0),
-          (1, 4, 1), (0, 4, 2), (1, 4, 8), (1, 4, 64)]
+          (1, 4, 1), (0, 4, 2), (1, 4, 8), (1, 4, 64), (1, 4, 16, 0, 1), (0, 2, 0, 0, 1)]
 
 
 def _run(up, opts, bo, tgt):
@@ -40,7 +41,7 @@ def test_every_launch_shape_gives_the_same_result(prefilter):
         ref_img, ref_g = _run(up, opts, bo, tgt)
         for shape in SHAPES:
             up.set_tuning(*shape)
-            assert up.tuning()[:3] == tuple(shape)
+            assert up.tuning()[:len(shape)] == tuple(shape)
             img, g = _run(up, opts, bo, tgt)
             assert float(np.max(np.abs(img - ref_img))) <= 2e-6, shape
             for k, v in ref_g.items():
@@ -85,13 +86,14 @@ def test_batch_autotune_keeps_results():
         ref = b.losses().copy()
         chosen = b.autotune()
         assert chosen[0] in (0, 1) and chosen[1] in (2, 4, 8, 16) and chosen[2] in (0, 8, 16, 32)
-        assert chosen[3] in (0, 1)
+        assert chosen[3] in (0, 1) and chosen[4] in (0, 1)
         b.step(True)
         assert np.allclose(b.losses(), ref, rtol=1e-5, atol=1e-6)
-        # gradients with and without the fragment cache, one CTA per work item or persistent CTAs
+        # gradients with and without the fragment cache, one CTA per work item or persistent CTAs,
+        # the forward at 2 or 3 CTAs per SM
         grads = []
-        for slots, queue in ((0, 0), (2, 0), (16, 0), (16, 1), (0, 1)):
-            b.set_tuning(1, 4, slots, queue)
+        for slots, queue, occ in ((0, 0, 0), (2, 0, 0), (16, 0, 0), (16, 1, 0), (0, 1, 0), (16, 0, 1), (16, 1, 1)):
+            b.set_tuning(1, 4, slots, queue, occ)
             b.step(True)
             b.losses()
             grads.append([(lambda g: (g[0].copy(), g[1].copy()))(_batch_grads(b, i, ups)) for i in range(3)])
