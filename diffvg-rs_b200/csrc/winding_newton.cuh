@@ -78,7 +78,8 @@ DVG_WN_HD float wn_log2_bound(float x) {
 // exists and is unique when h = |g''| |step| / |g'(y0)| <= 1/4 (Kantorovich: <= 1/2);
 // then Newton's error is at most (|g''| / (2|g'|)) (2|step|)^2 = 2 h |step|.  *u < 0: no
 // bound.  q3x = 3q, r2x = 2r, aqr = 3|q| and 2|r| for the residual's rounding.
-DVG_WN_HD double wn_newton(float y0f, double q3x, double r2x, double q, float aq3, float ar2, float* u) {
+DVG_WN_HD double wn_newton(float y0f, double q3x, double r2x, double q, float aq3, float ar2, float dq, float dr,
+                           float* u) {
     const double y0 = (double)y0f;
     const double y2 = y0 * y0;
     const double g = (y2 - q3x) * y0 + r2x;
@@ -102,7 +103,10 @@ DVG_WN_HD double wn_newton(float y0f, double q3x, double r2x, double q, float aq
     const float gabs = (ay * ay + aq3) * ay + ar2;
     // Newton + the f64 residual's rounding + the f32 reciprocal's (2 ulp + the f32 g') + the
     // update's rounding
-    *u = (2.0f * h * as + 16.0f * (float)WN_EPS * gabs * ai + as * 2.5e-6f + 8.0f * (float)WN_EPS * ay) * 1.01f;
+    // + the distance to the root of the crate's g (its q and r differ by dq, dr): twice the
+    // first-order shift, g' varying by less than half over the ball
+    *u = (2.0f * h * as + (16.0f * (float)WN_EPS * gabs + 2.0f * (3.0f * ay * dq + 2.0f * dr)) * ai + as * 2.5e-6f +
+          8.0f * (float)WN_EPS * ay) * 1.01f;
     return y1;
 }
 
@@ -116,7 +120,7 @@ DVG_WN_HD int wn_decide(double y, float uy, double b3, double a, double b, doubl
                         double dx) {
     const double t = y - b3;
     // the crate's t = fl(y_crate - b3) against ours: both roots' bounds and both roundings
-    const double ut = ((double)uy + 4.5e-16 * (std::fabs(y) + std::fabs(b3))) * 1.001;
+    const double ut = ((double)uy + 4.5e-16 * std::fabs(y) + 9.0e-16 * std::fabs(b3)) * 1.001;
     if (!(ut < 1.0e-3)) return WIND_UNSURE;
     if (t + ut < 0.0 || t - ut > 1.0) return 0;  // outside [0, 1] for both
     if (!(t - ut >= 0.0 && t + ut <= 1.0)) return WIND_UNSURE;
@@ -139,14 +143,28 @@ DVG_WN_HD int wn_decide(double y, float uy, double b3, double a, double b, doubl
 DVG_WN_HD int winding_cubic_newton(double a, double b, double c, double d, double ax, double bx, double cx, double dx,
                                    const float* perturb = nullptr) {
     if (std::fabs(a) < 1.0e-6) return WIND_UNSURE;  // the crate's quadratic branch
-    const double bn = b / a, cn = c / a, dn = d / a;
-    const double q = (bn * bn - 3.0 * cn) / 9.0;
-    const double r = (2.0 * bn * bn * bn - 9.0 * bn * cn + 27.0 * dn) / 54.0;
-    const double b3 = bn / 3.0;
+    // The crate divides: b/a, c/a, d/a, /9, /54, /3.  One reciprocal and products give
+    // values within a few eps of its own; g below has roots within dy of the crate's g (its
+    // q and r), which the bounds carry (qa, ra: the sums of |terms| of q and r).
+    const double ia = 1.0 / a;
+    const double bn = b * ia, cn = c * ia, dn = d * ia;
+    const double q = (bn * bn - 3.0 * cn) * (1.0 / 9.0);
+    const double r = (2.0 * bn * bn * bn - 9.0 * bn * cn + 27.0 * dn) * (1.0 / 54.0);
+    const double b3 = bn * (1.0 / 3.0);
     const double q3 = q * q * q, rr = r * r;
     const double q3x = 3.0 * q, r2x = 2.0 * r;
     const float aq3 = (float)std::fabs(q3x), ar2 = (float)std::fabs(r2x);
     if (!(aq3 < 1.0e30f && ar2 < 1.0e30f)) return WIND_UNSURE;
+    // |our q - the crate's q| <= 16 eps (b^2 + 3|c|) / 9 + 3 eps |q| and |our r - the crate's r|
+    // <= 19 eps (2|b|^3 + 9|b c| + 27|d|) / 54 + 3 eps |r| (inputs within 3 eps, both roundings),
+    // taken with a margin of 2.5 or more
+    float dq, dr;
+    {
+        const float fb = (float)std::fabs(bn), fc = (float)std::fabs(cn), fd = (float)std::fabs(dn);
+        if (!(fb < 1.0e12f && fc < 1.0e24f && fd < 1.0e30f)) return WIND_UNSURE;
+        dq = 2.0e-15f * (fb * fb + 3.0f * fc);
+        dr = 1.0e-16f * ((2.0f * fb * fb + 9.0f * fc) * fb + 27.0f * fd) + 1.0e-15f * (float)std::fabs(r);
+    }
     int w = 0;
     if (rr < q3) {  // three roots
         // 1 - x^2 >= 1e-6 for the crate's x = r / sqrt(q^3) (without its sqrt)
@@ -179,7 +197,7 @@ DVG_WN_HD int winding_cubic_newton(double a, double b, double c, double d, doubl
                 if (t0 + e < 0.0f || t0 - e > 1.0f) continue;
             }
             float u;
-            const double y = wn_newton(y0, q3x, r2x, q, aq3, ar2, &u);
+            const double y = wn_newton(y0, q3x, r2x, q, aq3, ar2, dq, dr, &u);
             if (u < 0.0f) return WIND_UNSURE;
             const float uy = u + ec;
             const float yf = (float)y;
@@ -206,7 +224,7 @@ DVG_WN_HD int winding_cubic_newton(double a, double b, double c, double d, doubl
     float y0 = arf + brf;
     if (perturb) y0 += perturb[0] * (std::fabs(arf) + std::fabs(brf));
     float u;
-    const double y = wn_newton(y0, q3x, r2x, q, aq3, ar2, &u);
+    const double y = wn_newton(y0, q3x, r2x, q, aq3, ar2, dq, dr, &u);
     if (u < 0.0f) return WIND_UNSURE;
     // the crate's ar = +-pow(m, 1/3): the exponent's rounding (|ln m| eps / 3), pow's own
     // ulp and the error of s (< 1e-9 / 3 of ar); br = q / ar follows ar
