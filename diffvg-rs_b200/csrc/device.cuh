@@ -247,6 +247,15 @@ static __device__ __noinline__ CPRes closest_quad_approx_v(float2 pt, float a0, 
     float cx = q[0] * w0 + q[2] * w1 + q[4] * w2, cy = q[1] * w0 + q[3] * w1 + q[5] * w2;
     return CPRes{cx, cy, t, len2(pt.x - cx, pt.y - cy)};
 }
+// The crate's candidates: its f64 roots (solve_cubic) in [0, 1], as f32 parameters.
+static __device__ __noinline__ int closest_quad_candidates_exact(double A, double B, double C, double D, float* t32) {
+    double r[3];
+    const int nr = solve_cubic(A, B, C, D, r);
+    int n = 0;
+    for (int i = 0; i < nr; ++i)
+        if (r[i] >= 0.0 && r[i] <= 1.0) t32[n++] = (float)r[i];
+    return n;
+}
 static __device__ __noinline__ CPRes closest_quad_v(float2 pt, float a0, float a1, float a2, float a3, float a4, float a5, float a6, float a7, bool approx);
 __device__ __forceinline__ CPRes closest_quad(float2 pt, const float* q, bool approx) {
     return closest_quad_v(pt, q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], approx);
@@ -273,23 +282,23 @@ static __device__ __noinline__ CPRes closest_quad_v(float2 pt, float a0, float a
     double B = 3.0 * (ax * bbx + ay * bby);
     double Cc = 2.0 * (bbx * bbx + bby * bby) + (ax * cx + ay * cy);
     double D = bbx * cx + bby * cy;
-    double r[3];
-    int n = solve_cubic(A, B, Cc, D, r);
+    // the crate's candidates t32 = (float)t of the roots in [0, 1]: certified without its
+    // acos / cos / pow when their side of 0 and 1 and their f32 rounding provably agree
+    float cand[3];
+    int n = closest_quad_roots_newton(A, B, Cc, D, cand);
+    if (n < 0) n = closest_quad_candidates_exact(A, B, Cc, D, cand);
     for (int i = 0; i < n; ++i) {
-        double t = r[i];
-        if (t >= 0.0 && t <= 1.0) {
-            float t32 = (float)t;
-            float tt = 1.0f - t32;
-            float w0 = tt * tt, w1 = 2.0f * tt * t32, w2 = t32 * t32;
-            float px = (q[0] * w0 + q[2] * w1) + q[4] * w2;
-            float py = (q[1] * w0 + q[3] * w1) + q[5] * w2;
-            float dist = len2(pt.x - px, pt.y - py);
-            if (dist < best) {
-                best = dist;
-                bx = px;
-                by = py;
-                best_t = t32;
-            }
+        float t32 = cand[i];
+        float tt = 1.0f - t32;
+        float w0 = tt * tt, w1 = 2.0f * tt * t32, w2 = t32 * t32;
+        float px = (q[0] * w0 + q[2] * w1) + q[4] * w2;
+        float py = (q[1] * w0 + q[3] * w1) + q[5] * w2;
+        float dist = len2(pt.x - px, pt.y - py);
+        if (dist < best) {
+            best = dist;
+            bx = px;
+            by = py;
+            best_t = t32;
         }
     }
     return CPRes{bx, by, best_t, best};

@@ -138,10 +138,18 @@ DVG_WN_HD int wn_decide(double y, float uy, double b3, double a, double b, doubl
     return dy > 0.0 ? 1 : -1;
 }
 
+// The roots of the crate's solve_cubic(a, b, c, d) that can fall in [0, 1], certified: for
+// each of them, in the crate's order, per_root(y, uy, b3) with y a root of g and uy the
+// bound on its distance to the crate's root (t = y - b3); roots whose estimate lies clearly
+// outside [0, 1] are skipped.  Returns the sum of per_root's results, or WIND_UNSURE (also
+// when per_root returns it).
 // perturb: host stress harness only — each f32 estimate moves by perturb[k] times the
 // scale of its formula (2 sqrt(q), or |ar| + |q / ar|).
-DVG_WN_HD int winding_cubic_newton(double a, double b, double c, double d, double ax, double bx, double cx, double dx,
-                                   const float* perturb = nullptr) {
+// tight: bound the crate's three-root rounding from this cubic's 1 - x^2 (one more rsqrt)
+// instead of its worst case 1e-6 (needed where the roots' f32 rounding must be certain).
+template <bool tight = false, typename PerRoot>
+DVG_WN_HD int cubic_roots_certified(double a, double b, double c, double d, PerRoot&& per_root,
+                                    const float* perturb) {
     if (std::fabs(a) < 1.0e-6) return WIND_UNSURE;  // the crate's quadratic branch
     // The crate divides: b/a, c/a, d/a, /9, /54, /3.  One reciprocal and products give
     // values within a few eps of its own; g below has roots within dy of the crate's g (its
@@ -175,7 +183,9 @@ DVG_WN_HD int winding_cubic_newton(double a, double b, double c, double d, doubl
         // the crate's rounding: acos(x) within 4 eps / sqrt(1 - x^2) + 8 eps (<= 4008 eps) of
         // the exact angle (x carries the rounding of sqrt, q^3 and the division), the cosines
         // and products a few eps more; 2 sqrt(q) times that bounds its root, doubled.
-        const float ec = 3.7e-12f * sq;
+        const float ec = tight ? 4.0f * sq * (float)WN_EPS *
+                                     (8.2f * wn_rsqrt((float)(q3 - rr)) * ((float)q * sq) + 32.0f)
+                               : 3.7e-12f * sq;
         // the f32 estimates: x within 5e-7 of its value (casts, rsqrt, product), acos within
         // 2 ulp, so the angle within 5e-4 (1 / sqrt(1 - x^2) <= 1e3), the cosine (fast, 2^-21
         // absolute) and sqrt(q) a little more: each estimate within 3.4e-4 sqrt(q) of the
@@ -203,7 +213,7 @@ DVG_WN_HD int winding_cubic_newton(double a, double b, double c, double d, doubl
             const float yf = (float)y;
             const bool inside = k == 0 ? yf + uy < -hi : (k == 1 ? yf - uy > hi : std::fabs(yf) + uy < lo);
             if (!inside) return WIND_UNSURE;
-            const int dk = wn_decide(y, uy, b3, a, b, c, ax, bx, cx, dx);
+            const int dk = per_root(y, uy, b3);
             if (dk == WIND_UNSURE) return WIND_UNSURE;
             w += dk;
         }
@@ -213,9 +223,10 @@ DVG_WN_HD int winding_cubic_newton(double a, double b, double c, double d, doubl
     const double disc = rr - q3;
     const double s = std::sqrt(disc);
     const double m = std::fabs(r) + s;  // |cbrt argument| of the crate
-    // the crate's s: sqrt of a difference carrying 3 eps (r^2 + |q^3|) of rounding; kept below
-    // 1e-9 of s (so below 1e-9 of m)
+    // the crate's s: sqrt of a difference carrying 3 eps (r^2 + |q^3|) of rounding, so within
+    // 1.5 eps (r^2 + |q^3|) / (r^2 - q^3) of itself; kept below 1e-9 of s (so of m)
     if (!(3.0 * WN_EPS * (rr + std::fabs(q3)) < 1.0e-9 * s * s)) return WIND_UNSURE;
+    const float rel_s = tight ? (float)(1.6 * WN_EPS * ((rr + std::fabs(q3)) / disc)) : 3.4e-10f;
     const float mf = (float)m;
     if (!(mf > 1.0e-30f && mf < 1.0e30f)) return WIND_UNSURE;
     const float arf = (r > 0.0 ? -1.0f : 1.0f) * std::cbrt(mf);
@@ -227,10 +238,42 @@ DVG_WN_HD int winding_cubic_newton(double a, double b, double c, double d, doubl
     const double y = wn_newton(y0, q3x, r2x, q, aq3, ar2, dq, dr, &u);
     if (u < 0.0f) return WIND_UNSURE;
     // the crate's ar = +-pow(m, 1/3): the exponent's rounding (|ln m| eps / 3), pow's own
-    // ulp and the error of s (< 1e-9 / 3 of ar); br = q / ar follows ar
-    const float rel = (float)WN_EPS * (0.7f * wn_log2_bound(mf) + 16.0f) + 3.4e-10f;
+    // ulp and the error of s (rel_s of s, so of m; a third of that on ar); br = q / ar follows ar
+    const float rel = (float)WN_EPS * (0.7f * wn_log2_bound(mf) + 16.0f) + rel_s;
     const float uy = u + 4.04f * (std::fabs(arf) + std::fabs(brf)) * rel;
-    return wn_decide(y, uy, b3, a, b, c, ax, bx, cx, dx);
+    return per_root(y, uy, b3);
+}
+
+// The winding contribution of a cubic segment (the crate's decisions), or WIND_UNSURE.
+DVG_WN_HD int winding_cubic_newton(double a, double b, double c, double d, double ax, double bx, double cx, double dx,
+                                   const float* perturb = nullptr) {
+    return cubic_roots_certified(
+        a, b, c, d, [&](double y, float uy, double b3) { return wn_decide(y, uy, b3, a, b, c, ax, bx, cx, dx); },
+        perturb);
+}
+
+// The crate's candidates of the closest point on a quadratic segment (closest_point_quadratic,
+// curve.rs:26-78): the roots in [0, 1] of its stationarity cubic A t^3 + B t^2 + C t + D,
+// as the f32 parameters t32 = (float)t the crate evaluates, in the crate's order.  Returns
+// the count, or -1 when a root's side of 0 or 1 or its f32 rounding is not certain.
+DVG_WN_HD int closest_quad_roots_newton(double A, double B, double C, double D, float* t32,
+                                        const float* perturb = nullptr) {
+    int n = 0;
+    const int st = cubic_roots_certified<true>(
+        A, B, C, D,
+        [&](double y, float uy, double b3) -> int {
+            const double t = y - b3;
+            const double ut = ((double)uy + 4.5e-16 * std::fabs(y) + 9.0e-16 * std::fabs(b3)) * 1.001;
+            if (!(ut < 1.0e-3)) return WIND_UNSURE;
+            if (t + ut < 0.0 || t - ut > 1.0) return 0;  // not a candidate, for both
+            if (!(t - ut >= 0.0 && t + ut <= 1.0)) return WIND_UNSURE;
+            const float f = (float)t;
+            if (!((float)(t - ut) == f && (float)(t + ut) == f)) return WIND_UNSURE;  // rounds alike
+            t32[n++] = f;
+            return 0;
+        },
+        perturb);
+    return st == WIND_UNSURE ? -1 : n;
 }
 
 }  // namespace dvgb

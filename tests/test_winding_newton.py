@@ -10,7 +10,14 @@ fast cosine, f32 acos of a rounded argument); the library skips the Newton step 
 whose estimate lies more than 2e-3 sqrt(q) outside [0, 1], and a harness run with larger
 moves (2.5e-3 of the scale) does find wrong decisions, so the cases reach that test.
 Never a decision that differs from the crate's; nearly all of a scene's tests decided
-without the crate's formula."""
+without the crate's formula.
+
+The same certified roots give the quadratic closest point's candidates (the stationarity
+cubic's roots in [0, 1] as the f32 parameters the crate evaluates): against the oracle's
+closest_point_quadratic (curve.rs:26-78), bit-identical point, parameter and distance on
+random segments with query points near the curve, integer alignments, nearly straight and
+degenerate segments, points near a centre of curvature (merging stationary points) and
+scene tests."""
 import ctypes as C
 import os
 import subprocess
@@ -53,3 +60,31 @@ def test_harness_finds_wrong_decisions_beyond_the_estimate_bound(stress):
     """Estimates moved past the 2e-3 sqrt(q) skip bound: the harness must see wrong decisions."""
     wrong = sum(stress(mode, 5, 1_000_000, 2.5e-3)[2] for mode in range(len(MODES)))
     assert wrong > 0
+
+
+QUAD_MODES = ("near the curve", "integer alignments", "nearly straight and degenerate", "near the evolute",
+              "scene tests")
+
+
+@pytest.fixture(scope="module")
+def quad_stress():
+    subprocess.run(["make", "-s", "-C", ORACLE], check=True)
+    L = C.CDLL(LIB)
+    L.closest_quad_stress.argtypes = [C.c_int, C.c_uint64, C.c_uint64, C.c_float, C.POINTER(C.c_ulonglong)]
+    L.closest_quad_stress.restype = None
+
+    def run(mode, seed, n, perturb):
+        out = (C.c_ulonglong * 3)()
+        L.closest_quad_stress(mode, seed, n, perturb, out)
+        return list(out)
+    return run
+
+
+@pytest.mark.parametrize("perturb", [0.0, 1e-5, 1e-4])
+@pytest.mark.parametrize("mode", range(len(QUAD_MODES)), ids=QUAD_MODES)
+def test_newton_closest_quadratic_is_bit_identical(quad_stress, mode, perturb):
+    cases, decided, wrong = quad_stress(mode, 7, 1_000_000, perturb)
+    assert cases >= 900_000
+    assert wrong == 0, f"{wrong} closest points differ from the crate's ({QUAD_MODES[mode]})"
+    if mode == 4 and perturb == 0.0:
+        assert decided >= 0.999 * cases, f"only {decided / cases:.4f} of a scene's tests decided"
