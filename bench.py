@@ -229,7 +229,9 @@ def compute_roofline(workload, prof, up, W, H, dev, clocks):
     peak = sms * 128 * mhz * 1e6 / 1e12
     achieved = work["total_flops"] / (avg_ms / 1e3) / 1e12 if work and avg_ms > 0 else None
     kernels, fresh, src = ncu_figures(workload)
-    fk = kernels.get("k_forward", {})
+    # the forward kernel is a template over its resident CTAs per SM (k_forward<2>, k_forward<3>);
+    # the captured step ran the shape the autotuner picked
+    fk = next((v for k, v in kernels.items() if k == "k_forward" or k.startswith("k_forward<")), {})
     step_ms = sum(v[0] for v in prof.values())
     # HBM view of the same kernel: image-sized accumulators and weights, scene tables once
     npix = W * H
@@ -256,7 +258,8 @@ def compute_roofline(workload, prof, up, W, H, dev, clocks):
                 "frac": hbm_achieved / hbm_peak if hbm_achieved else None, "algorithmic_bytes_per_launch": alg_bytes},
         "note": "the FP32 figure counts the crate's arithmetic per test (a libm call as one operation) and none of "
                 "the per-sample jitter, transform, paint, compositing and splat work; the kernel skips tests the "
-                "crate runs (exact culling), and its root solves run in f64 as the crate's do",
+                "crate runs (exact culling), and it takes the crate's root decisions from f32 estimates polished "
+                "by one f64 Newton step where bounds prove them equal (the crate's f64 formula otherwise)",
     }
 
 
