@@ -1808,13 +1808,13 @@ bool tuning_valid(const dvg_tuning* t) {
     return t && t->sample_layout <= 1 &&
            (t->boundary_cell == 2 || t->boundary_cell == 4 || t->boundary_cell == 8 || t->boundary_cell == 16) &&
            t->fragment_slots <= (uint32_t)FRAG_MAX_SLOTS && t->work_queue <= 1 &&
-           t->forward_occupancy <= 1;
+           t->forward_occupancy <= 2;
 }
 // The candidates: both warp layouts with the default cell and cache, then every cell
 // with the better layout (the boundary pass does not depend on the layout), then the
 // fragment-cache sizes (`try_slots`: only where the cache is used, non-prefiltered),
 // then persistent CTAs for the batch stages (`try_queue`), then the forward kernel at
-// 3 CTAs per SM.
+// 3 and at 4 CTAs per SM.
 template <typename Apply, typename Run>
 dvg_status autotune_loop(dvg_context* ctx, dvg_tuning* tune, bool try_slots, Apply apply, Run run,
                          bool try_queue = false) {
@@ -1864,7 +1864,11 @@ dvg_status autotune_loop(dvg_context* ctx, dvg_tuning* tune, bool try_slots, App
         for (int k = 0; k < 3; ++k) consider(dvg_tuning{b2.sample_layout, b2.boundary_cell, slots[k]});
     }
     if (try_queue) consider(dvg_tuning{best.sample_layout, best.boundary_cell, best.fragment_slots, 1, 0});
-    consider(dvg_tuning{best.sample_layout, best.boundary_cell, best.fragment_slots, best.work_queue, 1});
+    {
+        const dvg_tuning b3 = best;
+        for (uint32_t occ = 1; occ <= 2; ++occ)
+            consider(dvg_tuning{b3.sample_layout, b3.boundary_cell, b3.fragment_slots, b3.work_queue, occ});
+    }
     *tune = best;
     if (st == DVG_OK) st = apply();
     cudaEventDestroy(e0);

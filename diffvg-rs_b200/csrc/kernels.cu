@@ -18,12 +18,12 @@
 
 // Minimum resident CTAs per SM for the scene-evaluation kernels (register cap =
 // 65536 / (threads * value)); chosen by measurement on B200.
-// (the non-prefiltered forward is compiled for 2 and for 3, see dvg_tuning.forward_occupancy)
+// (the non-prefiltered forward is compiled for 2, 3 and 4, see dvg_tuning.forward_occupancy)
 #ifndef DVG_MINB_INT
 #define DVG_MINB_INT 2
 #endif
 #ifndef DVG_MINB_BND
-#define DVG_MINB_BND 12  // 40 registers: more warps for the two-lane edge evaluation outweigh its spills
+#define DVG_MINB_BND 16  // 32 registers: more warps for the two-lane edge evaluation outweigh its spills
 #endif
 #ifndef DVG_MINB_LEAN
 #define DVG_MINB_LEAN 4
@@ -1643,7 +1643,9 @@ int launch_forward(const DevScene& S, const SampleParams& sp, float* accum, floa
     const int hw = TILE + 2 * S.filter_ri;
     size_t smem = S.filter_ri <= MAX_SMEM_RI ? (size_t)hw * hw * 5 * sizeof(float) : 0;
     dim3 grid(launch_tiles(S, sp), sp.sxn * sp.syn);
-    if (sp.fwd_occ == 1)
+    if (sp.fwd_occ == 2)
+        k_forward<4><<<grid, 256, smem, stream>>>(S, sp, accum, wsum, status);
+    else if (sp.fwd_occ == 1)
         k_forward<3><<<grid, 256, smem, stream>>>(S, sp, accum, wsum, status);
     else
         k_forward<2><<<grid, 256, smem, stream>>>(S, sp, accum, wsum, status);
@@ -1714,7 +1716,10 @@ int launch_forward_batch(const BatchEntry* B, const int2* work, int items, int* 
                          cudaStream_t stream) {
     const int hw = TILE + 2 * max_ri;
     size_t smem = max_ri <= MAX_SMEM_RI ? (size_t)hw * hw * 5 * sizeof(float) : 0;
-    if (occ == 1) {
+    if (occ == 2) {
+        const int grid = counter ? persistent_grid(k_forward_batch<4>, smem, items) : items;
+        k_forward_batch<4><<<grid, 256, smem, stream>>>(B, work, items, counter);
+    } else if (occ == 1) {
         const int grid = counter ? persistent_grid(k_forward_batch<3>, smem, items) : items;
         k_forward_batch<3><<<grid, 256, smem, stream>>>(B, work, items, counter);
     } else {

@@ -196,8 +196,9 @@ typedef struct dvg_scene dvg_scene;
  *                1 = they launch as many persistent CTAs as the GPU holds at once, which
  *                take the items from a device counter in the same order.
  * forward_occupancy: the non-prefiltered forward kernel's register budget: 0 = 2 CTAs of
- *                256 threads per SM (128 registers, default), 1 = 3 CTAs (85 registers:
- *                more resident warps to cover its latencies, some spills). */
+ *                256 threads per SM (128 registers, default), 1 = 3 CTAs (80 registers),
+ *                2 = 4 CTAs (64 registers): more resident warps to cover its latencies,
+ *                more spills. */
 typedef struct dvg_tuning {
     uint32_t sample_layout;
     uint32_t boundary_cell;
