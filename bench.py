@@ -353,7 +353,7 @@ def large_fit(r, dev, lib_stream, steps, warmup, rank, lr=LARGE_FIT_LR):
             "loss_first": traj[0][1], "loss_last": traj[-1][1], "loss_trajectory": traj,
             "launch_shape": {"sample_layout": tuning[0], "boundary_cell": tuning[1], "fragment_slots": tuning[2],
                              "work_queue": "persistent CTAs" if tuning[3] else "one CTA per item",
-                             "forward_ctas_per_sm": 2 + tuning[4]}}
+                             "forward_ctas_per_sm": 4 - tuning[4]}}
 
 
 def single_scene_sharded(r, dev, lib_stream, steps, warmup, rank, world):
@@ -511,7 +511,7 @@ def batched_vs_plain(r, dev, lib_stream, flush, scenes, steps, label):
                        "fused device call, gradient read-back, host Adam"},
            "workload": label, "launch_shape": {"sample_layout": tuning[0], "boundary_cell": tuning[1], "fragment_slots": tuning[2],
                              "work_queue": "persistent CTAs" if tuning[3] else "one CTA per item",
-                             "forward_ctas_per_sm": 2 + tuning[4]}}
+                             "forward_ctas_per_sm": 4 - tuning[4]}}
     batch.close()
     for u in ups + tgts:
         u.close()
@@ -749,7 +749,7 @@ def main():
         "config": {**cfg, "boundary_samples": bopts.boundary_samples, "l2": "flushed between timed steps "
                    "(256 MiB write outside the timed events)", "parallelism": f"weak, {world} independent scene(s)",
                    "launch_shape": {"sample_layout": tuning[0], "boundary_cell": tuning[1],
-                                    "fragment_slots": tuning[2], "forward_ctas_per_sm": 2 + tuning[4],
+                                    "fragment_slots": tuning[2], "forward_ctas_per_sm": 4 - tuning[4],
                                     "chosen_by": "dvg_scene_autotune"}},
         "roofline": roofline,
         "kernel_ms_per_step": prof_json,

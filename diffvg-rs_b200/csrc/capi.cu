@@ -1814,7 +1814,7 @@ bool tuning_valid(const dvg_tuning* t) {
 // with the better layout (the boundary pass does not depend on the layout), then the
 // fragment-cache sizes (`try_slots`: only where the cache is used, non-prefiltered),
 // then persistent CTAs for the batch stages (`try_queue`), then the forward kernel at
-// 3 and at 4 CTAs per SM.
+// 3 and at 2 CTAs per SM.
 template <typename Apply, typename Run>
 dvg_status autotune_loop(dvg_context* ctx, dvg_tuning* tune, bool try_slots, Apply apply, Run run,
                          bool try_queue = false) {

@@ -1644,11 +1644,11 @@ int launch_forward(const DevScene& S, const SampleParams& sp, float* accum, floa
     size_t smem = S.filter_ri <= MAX_SMEM_RI ? (size_t)hw * hw * 5 * sizeof(float) : 0;
     dim3 grid(launch_tiles(S, sp), sp.sxn * sp.syn);
     if (sp.fwd_occ == 2)
-        k_forward<4><<<grid, 256, smem, stream>>>(S, sp, accum, wsum, status);
+        k_forward<2><<<grid, 256, smem, stream>>>(S, sp, accum, wsum, status);
     else if (sp.fwd_occ == 1)
         k_forward<3><<<grid, 256, smem, stream>>>(S, sp, accum, wsum, status);
     else
-        k_forward<2><<<grid, 256, smem, stream>>>(S, sp, accum, wsum, status);
+        k_forward<4><<<grid, 256, smem, stream>>>(S, sp, accum, wsum, status);
     return 1;
 }
 int launch_weights(const DevScene& S, const SampleParams& sp, float* wsum, cudaStream_t stream) {
@@ -1717,14 +1717,14 @@ int launch_forward_batch(const BatchEntry* B, const int2* work, int items, int* 
     const int hw = TILE + 2 * max_ri;
     size_t smem = max_ri <= MAX_SMEM_RI ? (size_t)hw * hw * 5 * sizeof(float) : 0;
     if (occ == 2) {
-        const int grid = counter ? persistent_grid(k_forward_batch<4>, smem, items) : items;
-        k_forward_batch<4><<<grid, 256, smem, stream>>>(B, work, items, counter);
+        const int grid = counter ? persistent_grid(k_forward_batch<2>, smem, items) : items;
+        k_forward_batch<2><<<grid, 256, smem, stream>>>(B, work, items, counter);
     } else if (occ == 1) {
         const int grid = counter ? persistent_grid(k_forward_batch<3>, smem, items) : items;
         k_forward_batch<3><<<grid, 256, smem, stream>>>(B, work, items, counter);
     } else {
-        const int grid = counter ? persistent_grid(k_forward_batch<2>, smem, items) : items;
-        k_forward_batch<2><<<grid, 256, smem, stream>>>(B, work, items, counter);
+        const int grid = counter ? persistent_grid(k_forward_batch<4>, smem, items) : items;
+        k_forward_batch<4><<<grid, 256, smem, stream>>>(B, work, items, counter);
     }
     return 1;
 }

@@ -51,7 +51,7 @@ struct SampleParams {
     uint8_t* frag_n; // per-sample code count or FRAG_NONE
     int frag_slots;  // codes kept per sample (<= FRAG_MAX_SLOTS)
     int tile_base, tile_count;  // the tiles a single-scene launch covers (count 0: all)
-    int fwd_occ;  // dvg_tuning.forward_occupancy: k_forward at 2 + fwd_occ CTAs per SM
+    int fwd_occ;  // dvg_tuning.forward_occupancy: k_forward at 4 - fwd_occ CTAs per SM
 };
 // Work items of a batched stage (work[i] = (scene, tile + tiles * sub-sample round),
 // heaviest first).  counter == nullptr: one CTA per item, item = blockIdx.x.  Otherwise

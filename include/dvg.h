@@ -195,10 +195,9 @@ typedef struct dvg_scene dvg_scene;
  *                work item (scene, tile, sub-sample), heaviest tiles first (default);
  *                1 = they launch as many persistent CTAs as the GPU holds at once, which
  *                take the items from a device counter in the same order.
- * forward_occupancy: the non-prefiltered forward kernel's register budget: 0 = 2 CTAs of
- *                256 threads per SM (128 registers, default), 1 = 3 CTAs (80 registers),
- *                2 = 4 CTAs (64 registers): more resident warps to cover its latencies,
- *                more spills. */
+ * forward_occupancy: the non-prefiltered forward kernel's register budget: 0 = 4 CTAs of
+ *                256 threads per SM (64 registers, default), 1 = 3 CTAs (80 registers),
+ *                2 = 2 CTAs (128 registers): fewer resident warps, fewer spills. */
 typedef struct dvg_tuning {
     uint32_t sample_layout;
     uint32_t boundary_cell;
