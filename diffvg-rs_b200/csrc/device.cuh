@@ -13,6 +13,15 @@
 #include <cuda_runtime.h>
 
 #include "prepare.hpp"  // ShapeFlags shared with the host preparation
+// Set by a translation unit before including this header: DVG_EXACT_ROOT_SOLVES, the cubic
+// winding runs the crate's root formula; DVG_EXACT_CLOSEST_QUAD, the quadratic closest
+// point does (both also without them whenever the certified shortcut is not sure).
+#ifndef DVG_EXACT_ROOT_SOLVES
+#define DVG_EXACT_ROOT_SOLVES 0
+#endif
+#ifndef DVG_EXACT_CLOSEST_QUAD
+#define DVG_EXACT_CLOSEST_QUAD DVG_EXACT_ROOT_SOLVES
+#endif
 #include "winding_newton.cuh"
 
 namespace dvgb {
@@ -285,8 +294,12 @@ static __device__ __noinline__ CPRes closest_quad_v(float2 pt, float a0, float a
     // the crate's candidates t32 = (float)t of the roots in [0, 1]: certified without its
     // acos / cos / pow when their side of 0 and 1 and their f32 rounding provably agree
     float cand[3];
+#if DVG_EXACT_CLOSEST_QUAD
+    const int n = closest_quad_candidates_exact(A, B, Cc, D, cand);
+#else
     int n = closest_quad_roots_newton(A, B, Cc, D, cand);
     if (n < 0) n = closest_quad_candidates_exact(A, B, Cc, D, cand);
+#endif
     for (int i = 0; i < n; ++i) {
         float t32 = cand[i];
         float tt = 1.0f - t32;
@@ -526,9 +539,13 @@ static __device__ __noinline__ int winding_segment_v(int kind, float a0, float a
     double bx = (double)(3.0f * q[0] - 6.0f * q[2] + 3.0f * q[4]);
     double cx = (double)(-3.0f * q[0] + 3.0f * q[2]);
     double dx = (double)(q[0] - pt.x);
+#if DVG_EXACT_ROOT_SOLVES
+    return winding_cubic_exact(a, b, c, d, ax, bx, cx, dx);
+#else
     // the crate's decisions without its f64 acos / cos / pow whenever they provably agree
     const int wn = winding_cubic_newton(a, b, c, d, ax, bx, cx, dx);
     return wn != WIND_UNSURE ? wn : winding_cubic_exact(a, b, c, d, ax, bx, cx, dx);
+#endif
 }
 __device__ __forceinline__ int winding_segment(const SegGeom& s, float2 pt) {
     return winding_segment_v(s.kind, s.q[0], s.q[1], s.q[2], s.q[3], s.q[4], s.q[5], s.q[6], s.q[7], pt);

@@ -7,7 +7,13 @@
 // search walks the crate's BVHs with an explicit stack in the crate's order
 // (closer child first, src/distance/api.rs:138-236, closest.rs:104-199): the
 // order only matters for exact distance ties, which it resolves the same way.
-// Built with -fmad=false like kernels.cu.
+// Built with -fmad=false like kernels.cu.  The quadratic closest point runs the crate's
+// root formula here (DVG_EXACT_CLOSEST_QUAD): these kernels call it for every segment
+// within the distance search, and its certified shortcut measured slower in them (mixed
+// 512x512 scene, 4x4 spp: prefiltered interior 65.8 ms without it, 66.9 with it).
+#ifndef DVG_EXACT_CLOSEST_QUAD
+#define DVG_EXACT_CLOSEST_QUAD 1
+#endif
 #include <algorithm>
 
 #include "device.cuh"
@@ -50,7 +56,7 @@ struct ClosestD {
 };
 
 // closest_point_path_bvh (closest.rs:104-199); cp in shape space.
-__device__ bool closest_path_bvh(const DevScene& S, int path, float2 p, float2* cp, int* seg, float* tt,
+static __device__ bool closest_path_bvh(const DevScene& S, int path, float2 p, float2* cp, int* seg, float* tt,
                                  unsigned* status) {
     const int4 pi = __ldg(&S.p_info[2 * path]);
     if (pi.w == 0) return false;
@@ -115,7 +121,7 @@ __device__ __forceinline__ float2 closest_point_rect(float4 r, float2 p) {  // s
 }
 
 // closest_point_shape (closest.rs:386-456); lp and the result in group space.
-__device__ bool closest_shape(const DevScene& S, int s, float2 lp, float2* out, int* seg, float* t) {
+static __device__ bool closest_shape(const DevScene& S, int s, float2 lp, float2* out, int* seg, float* t) {
     const float2 p = shape_local_dist(S, s, lp);
     const int4 si = __ldg(&S.s_info[s]);
     const float4 prm = __ldg(&S.s_params[s]);
@@ -168,7 +174,7 @@ __device__ bool closest_shape(const DevScene& S, int s, float2 lp, float2* out, 
 }
 
 // compute_distance_bvh (api.rs:138-236) with the brute-force fallback compute_distance (api.rs:36-76).
-__device__ bool compute_distance_group(const DevScene& S, int g, float2 pt, float max_radius, ClosestD* best,
+static __device__ bool compute_distance_group(const DevScene& S, int g, float2 pt, float max_radius, ClosestD* best,
                                        unsigned* status) {
     const int4 gb = __ldg(&S.g_bvh[g]);
     const float* s2c = S.g_s2c + 9 * g;
@@ -338,6 +344,9 @@ __device__ __forceinline__ void forward_prefilter_body(const DevScene& S, const 
     __syncthreads();
     flush_splat(S, tx, ty, ri, HW, sm, accum, wsum);
 }
+// The prefiltered forward kernels and their launchers are compiled in prefilter_fwd.cu
+// (DVG_PREFILTER_FORWARD, with the crate's root formulas); everything else here.
+#if DVG_PREFILTER_FORWARD
 __global__ void __launch_bounds__(256, DVG_MINB_PF_FWD) k_forward_prefilter(DevScene S, SampleParams sp, float* accum, float* wsum,
                                                               unsigned* status) {
     extern __shared__ float sm[];
@@ -354,6 +363,30 @@ __global__ void __launch_bounds__(256, DVG_MINB_PF_FWD) k_forward_prefilter_batc
         forward_prefilter_body(E.S, E.sp, wk.y % tiles, wk.y / tiles, E.accum, E.wsum, status, sm);
     });
 }
+int launch_forward_prefilter(const DevScene& S, const SampleParams& sp, float* accum, float* wsum, unsigned* status,
+                             cudaStream_t stream) {
+    const int hw = TILE + 2 * S.filter_ri;
+    size_t smem = S.filter_ri <= MAX_SMEM_RI ? (size_t)hw * hw * 5 * sizeof(float) : 0;
+    dim3 grid(launch_tiles(S, sp), sp.sxn * sp.syn);
+    k_forward_prefilter<<<grid, 256, smem, stream>>>(S, sp, accum, wsum, status);
+    return 1;
+}
+int launch_forward_prefilter_batch(const BatchEntry* B, const int2* work, int items, int* counter, int max_ri,
+                                   unsigned* status, cudaStream_t stream) {
+    const int hw = TILE + 2 * max_ri;
+    size_t smem = max_ri <= MAX_SMEM_RI ? (size_t)hw * hw * 5 * sizeof(float) : 0;
+    int grid = items;
+    if (counter) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_forward_prefilter_batch, 256, smem);
+        grid = std::max(1, std::min(items, std::max(per_sm, 1) * std::max(sms, 1)));
+    }
+    k_forward_prefilter_batch<<<grid, 256, smem, stream>>>(B, work, items, counter, status);
+    return 1;
+}
+#else
 
 // ------------------------------------------------------------------ distance adjoint (backward/distance.rs)
 __device__ __forceinline__ void d_xform_pt(const float* m, float2 p, float2 d_out, float* dm, float2* d_p) {
@@ -385,7 +418,7 @@ __device__ __forceinline__ float2 add2(float2 a, float2 b) { return make_float2(
 __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ float2 mul2(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 
-__device__ void add_point_grad(const GradPtrs& G, int po, int pc, bool closed, long idx, float2 d) {
+static __device__ void add_point_grad(const GradPtrs& G, int po, int pc, bool closed, long idx, float2 d) {
     long i = closed ? idx % pc : idx;
     if (i < pc) {
         add_if(G.d_points + 2 * (po + i), d.x);
@@ -393,7 +426,7 @@ __device__ void add_point_grad(const GradPtrs& G, int po, int pc, bool closed, l
     }
 }
 // d_closest_point_path (distance.rs:190-394)
-__device__ void d_closest_point_path(const DevScene& S, const GradPtrs& G, int s, float2 pt, float2 d_cp, int seg,
+static __device__ void d_closest_point_path(const DevScene& S, const GradPtrs& G, int s, float2 pt, float2 d_cp, int seg,
                                      float min_t, float2* d_pt) {
     const int path = __ldg(&S.s_info[s].z);
     const int4 pi = __ldg(&S.p_info[2 * path]);
@@ -533,7 +566,7 @@ __device__ void d_closest_point_path(const DevScene& S, const GradPtrs& G, int s
     }
 }
 // d_closest_point_ellipse (distance.rs:479-561)
-__device__ void d_closest_point_ellipse(float4 prm, float2 pt, float2 d_cp, float2* dc, float2* dr, float2* d_pt) {
+static __device__ void d_closest_point_ellipse(float4 prm, float2 pt, float2 d_cp, float2* dc, float2* dr, float2* d_pt) {
     float rx = fabsf(prm.z), ry = fabsf(prm.w);
     const float eps = 1.0e-6f;
     float lx = pt.x - prm.x, ly = pt.y - prm.y;
@@ -596,7 +629,7 @@ __device__ void d_closest_point_ellipse(float4 prm, float2 pt, float2 d_cp, floa
     }
 }
 // d_closest_point_rect (distance.rs:397-476)
-__device__ void d_closest_point_rect(float4 r, float2 pt, float2 d_cp, float2* d_min, float2* d_max, float2* d_pt) {
+static __device__ void d_closest_point_rect(float4 r, float2 pt, float2 d_cp, float2* d_min, float2* d_max, float2* d_pt) {
     auto dist_to_seg = [&](float2 p0, float2 p1) {
         float2 e = sub2(p1, p0);
         float t = dot2(sub2(pt, p0), e) / dot2(e, e);
@@ -665,7 +698,7 @@ __device__ void d_closest_point_rect(float4 r, float2 pt, float2 d_cp, float2* d
 }
 // d_compute_distance (distance.rs:50-136): geometry, shape and group transform
 // gradients by atomics; returns d_pt (for the translation adjoint).
-__device__ float2 d_compute_distance(const DevScene& S, const GradPtrs& G, int g, int s, float2 pt, float2 cp,
+static __device__ float2 d_compute_distance(const DevScene& S, const GradPtrs& G, int g, int s, float2 pt, float2 cp,
                                      int seg, float seg_t, float d_dist) {
     float dx = pt.x - cp.x, dy = pt.y - cp.y;
     if (dx * dx + dy * dy < 1.0e-10f) return make_float2(0.0f, 0.0f);
@@ -960,14 +993,6 @@ __global__ void __launch_bounds__(256, DVG_MINB_PF_INT) k_interior_prefilter_bat
     });
 }
 
-int launch_forward_prefilter(const DevScene& S, const SampleParams& sp, float* accum, float* wsum, unsigned* status,
-                             cudaStream_t stream) {
-    const int hw = TILE + 2 * S.filter_ri;
-    size_t smem = S.filter_ri <= MAX_SMEM_RI ? (size_t)hw * hw * 5 * sizeof(float) : 0;
-    dim3 grid(launch_tiles(S, sp), sp.sxn * sp.syn);
-    k_forward_prefilter<<<grid, 256, smem, stream>>>(S, sp, accum, wsum, status);
-    return 1;
-}
 int launch_interior_prefilter(const DevScene& S, const SampleParams& sp, const float* d_render, const float* wsum,
                               const GradPtrs& G, unsigned* status, cudaStream_t stream) {
     dim3 grid(launch_tiles(S, sp), sp.sxn * sp.syn);
@@ -975,21 +1000,6 @@ int launch_interior_prefilter(const DevScene& S, const SampleParams& sp, const f
     return 1;
 }
 
-int launch_forward_prefilter_batch(const BatchEntry* B, const int2* work, int items, int* counter, int max_ri,
-                                   unsigned* status, cudaStream_t stream) {
-    const int hw = TILE + 2 * max_ri;
-    size_t smem = max_ri <= MAX_SMEM_RI ? (size_t)hw * hw * 5 * sizeof(float) : 0;
-    int grid = items;
-    if (counter) {
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_forward_prefilter_batch, 256, smem);
-        grid = std::max(1, std::min(items, std::max(per_sm, 1) * std::max(sms, 1)));
-    }
-    k_forward_prefilter_batch<<<grid, 256, smem, stream>>>(B, work, items, counter, status);
-    return 1;
-}
 int launch_interior_prefilter_batch(const BatchEntry* B, const int2* work, int items, int* counter, unsigned* status,
                                     cudaStream_t stream) {
     int grid = items;
@@ -1016,7 +1026,7 @@ int launch_interior_prefilter_batch(const BatchEntry* B, const int2* work, int i
 // bound; the loop therefore keeps the crate's order.  A group whose conservative
 // canvas box is farther than the bound is skipped without its transform (it cannot
 // return a point within the bound, which is all the crate's search would accept).
-__device__ bool sdf_closest(const DevScene& S, const float4* g_bbox, float2 pt, float init, ClosestD* best,
+static __device__ bool sdf_closest(const DevScene& S, const float4* g_bbox, float2 pt, float init, ClosestD* best,
                             int* group, unsigned* status) {
     float best_dist = init;
     bool found = false;
@@ -1037,7 +1047,7 @@ __device__ __forceinline__ bool sdf_inside(const DevScene& S, int g, float2 pt) 
     const int4 gi = __ldg(&S.g_info[g]);
     return gi.x >= 0 && group_inside(S, g, xf9(S.g_c2s + 9 * g, pt), gi.z);
 }
-__device__ float sdf_signed(const DevScene& S, float2 pt, unsigned* status) {
+static __device__ float sdf_signed(const DevScene& S, float2 pt, unsigned* status) {
     ClosestD b;
     int g = 0;
     if (!sdf_closest(S, S.g_bbox, pt, 1.0e20f, &b, &g, status)) return 0.0f;
@@ -1149,4 +1159,5 @@ int launch_positions_backward(const DevScene& S, const float2* pos, uint64_t n, 
     return 1;
 }
 
+#endif  // DVG_PREFILTER_FORWARD
 }  // namespace dvgb
