@@ -256,8 +256,15 @@ static __device__ __noinline__ CPRes closest_quad_approx_v(float2 pt, float a0, 
     float cx = q[0] * w0 + q[2] * w1 + q[4] * w2, cy = q[1] * w0 + q[3] * w1 + q[5] * w2;
     return CPRes{cx, cy, t, len2(pt.x - cx, pt.y - cy)};
 }
-// The crate's candidates: its f64 roots (solve_cubic) in [0, 1], as f32 parameters.
-static __device__ __noinline__ int closest_quad_candidates_exact(double A, double B, double C, double D, float* t32) {
+// The crate's candidates: its f64 roots (solve_cubic) in [0, 1], as f32 parameters (inline
+// where it is the only path, as for the winding).
+#if DVG_EXACT_CLOSEST_QUAD
+#define DVG_QUAD_EXACT_ATTR __forceinline__
+#else
+#define DVG_QUAD_EXACT_ATTR __noinline__
+#endif
+static __device__ DVG_QUAD_EXACT_ATTR int closest_quad_candidates_exact(double A, double B, double C, double D,
+                                                                        float* t32) {
     double r[3];
     const int nr = solve_cubic(A, B, C, D, r);
     int n = 0;
@@ -477,8 +484,15 @@ __device__ __forceinline__ float seg_radius(const SegGeom& s, float t) {  // clo
     return tt * tt * tt * s.r[0] + 3.0f * tt * tt * t * s.r[1] + 3.0f * tt * t * t * s.r[2] + t * t * t * s.r[3];
 }
 // The crate's cubic crossings: its f64 roots (solve_cubic) and decisions (winding.rs:170-192).
-static __device__ __noinline__ int winding_cubic_exact(double a, double b, double c, double d, double ax, double bx,
-                                                       double cx, double dx) {
+// Out of line where it is the certified path's fallback (rarely run), inline where it is
+// the only path.
+#if DVG_EXACT_ROOT_SOLVES
+#define DVG_WIND_EXACT_ATTR __forceinline__
+#else
+#define DVG_WIND_EXACT_ATTR __noinline__
+#endif
+static __device__ DVG_WIND_EXACT_ATTR int winding_cubic_exact(double a, double b, double c, double d, double ax,
+                                                              double bx, double cx, double dx) {
     double r[3];
     int nr = solve_cubic(a, b, c, d, r);
     int w = 0;
