@@ -356,6 +356,41 @@ def large_fit(r, dev, lib_stream, steps, warmup, rank, lr=LARGE_FIT_LR):
                              "forward_ctas_per_sm": 4 - tuning[4]}}
 
 
+def prefiltered_step(r, dev, lib_stream, flush, steps, warmup, rank):
+    """The crate's default mode: the mixed scene at 2x2 spp with prefiltering (smoothstep
+    coverage from the signed distance, no boundary pass), one fused forward + L2 + backward
+    per step, L2 flushed between steps, CUDA events on the library's stream."""
+    import torch
+
+    sc = synth.mixed_scene(rank_seed(0, rank))
+    opts = RenderOptions(samples_x=2, samples_y=2, seed=0, jitter=True, use_prefiltering=True)
+    bopts = BackwardOptions()
+    up, tu = r.upload(sc), r.upload(synth.mixed_scene(rank_seed(0, rank) + 1000))
+    n = sc.width * sc.height * 4
+    tgt, img = torch.empty(n, device=dev), torch.empty(n, device=dev)
+    loss = torch.zeros(1, device=dev)
+    tu.render_device(opts, tgt.data_ptr())
+    g = DeviceGrads(up.packed, dev)
+    for _ in range(warmup):
+        up.fwd_bwd_l2_device(opts, bopts, tgt.data_ptr(), img.data_ptr(), loss.data_ptr(), g)
+    ts = []
+    for _ in range(steps):
+        with torch.cuda.stream(lib_stream):
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(lib_stream)
+        up.fwd_bwd_l2_device(opts, bopts, tgt.data_ptr(), img.data_ptr(), loss.data_ptr(), g)
+        e1.record(lib_stream)
+        torch.cuda.synchronize(dev)
+        ts.append(e0.elapsed_time(e1))
+    up.close()
+    tu.close()
+    ms = float(np.median(ts))
+    samples = sc.width * sc.height * 4
+    return {"workload": "mixed-primitive scene 512x512, 2x2 spp, prefiltered (the crate's default RenderOptions), "
+                        "fwd + L2 + bwd", "steps": steps, "ms_per_step": ms, "msamples_per_s": samples / ms / 1e3}
+
+
 def single_scene_sharded(r, dev, lib_stream, steps, warmup, rank, world):
     """One large scene split over all ranks (strong scaling): every rank renders a band
     of tiles and a range of boundary samples; NCCL sums the splat accumulators after the
@@ -561,6 +596,8 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=5)
     ap.add_argument("--large-fit-steps", type=int, default=200)
     ap.add_argument("--shard-steps", type=int, default=3)
+    ap.add_argument("--prefilter-steps", type=int, default=5,
+                    help="steps of the prefiltered leg (the crate's default mode; 0: skip)")
     ap.add_argument("--cpu-threads", type=int, default=0, help="host threads of the CPU baseline (0: all)")
     ap.add_argument("--ncu-step", action="store_true",
                     help="run the warm-up steps and one step inside the NVTX range dvg_step, then exit")
@@ -709,6 +746,12 @@ def main():
     if args.shard_steps > 0:
         sharded = single_scene_sharded(r, dev, lib_stream, args.shard_steps, 2, rank, world)
 
+    prefiltered = None
+    if args.prefilter_steps > 0:
+        prefiltered = prefiltered_step(r, dev, lib_stream, flush, args.prefilter_steps, 3, rank)
+        if world > 1:
+            prefiltered["ms_per_step"] = max_over_ranks([prefiltered["ms_per_step"]], dev)[0]
+
     batched = None
     if args.batch_scenes > 0:
         batched = batched_vs_plain(
@@ -755,6 +798,7 @@ def main():
         "kernel_ms_per_step": prof_json,
         "gpu_launches": int(timed_launches), "clocks": clock_summary, "e2e": e2e,
         "batched_vs_plain": batched, "large_fit": fit, "single_scene_sharded": sharded,
+        "prefiltered": prefiltered,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         img = out.view(H, W, 4).cpu().numpy()
