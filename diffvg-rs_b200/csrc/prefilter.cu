@@ -306,6 +306,52 @@ __device__ __forceinline__ PFragD prefilter_frag(const DevScene& S, int g, int w
     return f;
 }
 
+// Prefiltered coverage reaches past a group's geometry: smoothstep(d) of a fill is
+// non-zero for signed distances above -1 pixel, a stroke's for canvas distances below
+// its width + 1 (sampling.rs:240-300 visits every group at every sample).  The scene's
+// tile lists bin the point-sampled coverage, whose group boxes carry 0.5 pixel of
+// slack only, so the prefiltered kernels bin each tile again, in group order, against
+// the group box grown by that reach (stroke widths are those of the group's shapes).
+__device__ __forceinline__ bool pf_group_reaches(const DevScene& S, int tile, int g) {
+    const int4 gi = __ldg(&S.g_info[g]);
+    if (gi.x < 0 && gi.y < 0) return false;
+    float reach = 1.0f;
+    if (gi.y >= 0) {
+        const int4 gb = __ldg(&S.g_bvh[g]);
+        for (int k = 0; k < gb.w; ++k)
+            reach = fmaxf(reach, 1.0f + fabsf(__ldg(&S.s_stroke[__ldg(&S.g_shape_list[gb.z + k])])));
+    }
+    reach = reach * 1.001f + 0.01f;
+    const float4 b = __ldg(&S.g_bbox[g]);
+    const int tx = tile % S.tiles_x, ty = tile / S.tiles_x;
+    // edge tiles extend to infinity, as in the scene's binning
+    const float x0 = tx == 0 ? -INF_F : (float)(tx * TILE), y0 = ty == 0 ? -INF_F : (float)(ty * TILE);
+    const float x1 = tx == S.tiles_x - 1 ? INF_F : (float)((tx + 1) * TILE);
+    const float y1 = ty == S.tiles_y - 1 ? INF_F : (float)((ty + 1) * TILE);
+    return !(b.z + reach < x0 || b.x - reach > x1 || b.w + reach < y0 || b.y - reach > y1);
+}
+// Groups [base, base + 256) that reach the tile, in order, into list; returns their
+// count.  Called by all 256 threads of the CTA; list is valid until the next call.
+__device__ __forceinline__ int pf_bin_chunk(const DevScene& S, int tile, int base, int* list, int* warp_cnt) {
+    __syncthreads();  // the previous chunk's list is consumed
+    const int g = base + (int)threadIdx.x;
+    const bool hit = g < S.num_groups && pf_group_reaches(S, tile, g);
+    const unsigned m = __ballot_sync(0xffffffffu, hit);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) warp_cnt[wid] = __popc(m);
+    __syncthreads();
+    int off = 0, total = 0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+        const int c = warp_cnt[w];
+        off += w < wid ? c : 0;
+        total += c;
+    }
+    if (hit) list[off + __popc(m & ((1u << lane) - 1u))] = g;
+    __syncthreads();
+    return total;
+}
+
 // ------------------------------------------------------------------ forward
 __device__ __forceinline__ void forward_prefilter_body(const DevScene& S, const SampleParams& sp, int tile, int round,
                                                        float* accum, float* wsum, unsigned* status, float* sm) {
@@ -317,18 +363,22 @@ __device__ __forceinline__ void forward_prefilter_body(const DevScene& S, const 
     const int s_in_tile = round * 256 + (int)threadIdx.x;
     const int pix = sp.layout ? s_in_tile / spp : (int)threadIdx.x, sub = sp.layout ? s_in_tile % spp : round;
     const int x = tx * TILE + (pix % TILE), y = ty * TILE + (pix / TILE);
+    __shared__ int list[256], warp_cnt[8];
     if (use_sm)
         for (int i = threadIdx.x; i < HW * HW * 5; i += blockDim.x) sm[i] = 0.0f;
-    __syncthreads();
-    const int off = S.tile_offsets[tile];
-    const int n = S.tile_offsets[tile + 1] - off;
-    const int* list = S.tile_entries + off;
-    if (x < S.width && y < S.height) {
+    const bool valid = x < S.width && y < S.height;
+    float2 pt = make_float2(0.0f, 0.0f);
+    float4 acc = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (valid) {
         const int sx = sub % sp.sxn, sy = sub / sp.sxn;
-        const float2 pt = sample_pos(x, y, sx, sy, sp.sxn, sp.syn, S.width, sp.seed, false);
-        float4 acc = background_premul(S, y * S.width + x);
+        pt = sample_pos(x, y, sx, sy, sp.sxn, sp.syn, S.width, sp.seed, false);
+        acc = background_premul(S, y * S.width + x);
+    }
+    for (int base = 0; base < S.num_groups; base += 256) {
+        const int n = pf_bin_chunk(S, tile, base, list, warp_cnt);  // also orders the smem clear above
+        if (!valid) continue;
         for (int e = 0; e < n; ++e) {
-            const int g = __ldg(&list[e]);
+            const int g = list[e];
             const int4 gi = __ldg(&S.g_info[g]);
 #pragma unroll 1
             for (int which = 0; which < 2; ++which) {
@@ -338,8 +388,9 @@ __device__ __forceinline__ void forward_prefilter_body(const DevScene& S, const 
                 if (f.hit) over(acc, f.c);
             }
         }
-        splat_sample(S, x, y, tx, ty, ri, HW, use_sm, pt, acc, sm, accum, wsum);
     }
+    __syncthreads();  // the splat tile is cleared even without groups
+    if (valid) splat_sample(S, x, y, tx, ty, ri, HW, use_sm, pt, acc, sm, accum, wsum);
     if (!use_sm) return;
     __syncthreads();
     flush_splat(S, tx, ty, ri, HW, sm, accum, wsum);
@@ -792,9 +843,7 @@ __device__ __forceinline__ void interior_prefilter_body(const DevScene& S, const
     const int x = tx * TILE + (pix % TILE), y = ty * TILE + (pix / TILE);
     const bool valid = x < S.width && y < S.height;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int off = S.tile_offsets[tile];
-    const int n = S.tile_offsets[tile + 1] - off;
-    const int* list = S.tile_entries + off;
+    __shared__ int list[256], warp_cnt[8];
     const int W = S.width, H = S.height;
     float2 ps = make_float2(0.0f, 0.0f), pt = ps;
     int pixel = 0;
@@ -814,9 +863,11 @@ __device__ __forceinline__ void interior_prefilter_body(const DevScene& S, const
     int nf = 0;
     bool overflow = false;
     float4 acc = bg;
-    if (valid) {
+    for (int base = 0; base < S.num_groups; base += 256) {
+        const int n = pf_bin_chunk(S, tile, base, list, warp_cnt);
+        if (!valid) continue;
         for (int e = 0; e < n; ++e) {
-            const int g = __ldg(&list[e]);
+            const int g = list[e];
             const int4 gi = __ldg(&S.g_info[g]);
 #pragma unroll 1
             for (int which = 0; which < 2; ++which) {
@@ -826,7 +877,7 @@ __device__ __forceinline__ void interior_prefilter_body(const DevScene& S, const
                 if (!f.hit) continue;
                 over(acc, f.c);
                 if (nf < MAX_PF) {
-                    code[nf] = 2 * e + which;
+                    code[nf] = 2 * g + which;
                     tr[nf] = f.c.w;
                     fshape[nf] = f.shape;
                     fdist[nf] = f.dist;
@@ -890,8 +941,7 @@ __device__ __forceinline__ void interior_prefilter_body(const DevScene& S, const
         const int mine = cur < nf ? code[cur] : 0x7fffffff;
         const int nxt = __reduce_min_sync(0xffffffffu, mine);
         if (nxt == 0x7fffffff) break;
-        const int e = nxt >> 1, which = nxt & 1;  // code = 2 * entry + (0 stroke, 1 fill)
-        const int g = __ldg(&list[e]);
+        const int g = nxt >> 1, which = nxt & 1;  // code = 2 * group + (0 stroke, 1 fill)
         const int4 gi = __ldg(&S.g_info[g]);
         const int p = which == 0 ? gi.y : gi.x;
         const bool has = mine == nxt;

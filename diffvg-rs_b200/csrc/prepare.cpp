@@ -218,6 +218,10 @@ dvg_status prepare_scene(const dvg_scene_desc* d, HostScene* out, std::string* e
         *err = "missing group arrays";
         return DVG_ERR_INVALID_ARGUMENT;
     }
+    if (d->num_groups >= (1u << 30)) {  // fragment codes pack 2 * group + stroke/fill into an int
+        *err = "too many groups";
+        return DVG_ERR_INVALID_SCENE;
+    }
     if (d->num_paints && (!d->paint_kind || !d->paint_params)) {
         *err = "missing paint arrays";
         return DVG_ERR_INVALID_ARGUMENT;

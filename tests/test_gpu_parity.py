@@ -166,3 +166,40 @@ def test_backward_prefilter_mixed_matches_oracle(renderer):
     sc = synth.mixed_scene(7, 80, 80, scale=0.08, size_scale=0.25)
     gpu, ref = _backward_case(renderer, sc, _prefilter_opts())
     _grad_check(gpu, ref)
+
+
+def _reach_scene():
+    """48x48 (3x3 tiles of 16 pixels), each shape ending 0.4-0.65 pixel short of a
+    tile edge: prefiltered coverage (smoothstep of the distance, 1 pixel past a fill
+    and stroke width + 1 past a stroke) crosses into the next tile, where the
+    point-sampled tile binning does not list the group."""
+    from dvg import Circle, Ellipse, Path, PathGeometry, Shape, ShapeGroup
+
+    sc = Scene(48, 48)
+    sc.background = Color(1.0, 1.0, 1.0, 1.0)
+    geoms = [
+        (Circle((8.0, 24.0), 7.35), 0.0),  # right edge x = 15.35, next tile from x = 16
+        (Ellipse((40.0, 40.0), (7.4, 5.0)), 0.0),  # left edge x = 32.6, previous tile to x = 32
+        (PathGeometry(Path([0], [(20.0, 29.45), (28.0, 29.45)], None, False, False)), 2.0),  # y + 2 + 1 > 32
+    ]
+    for k, (geom, sw) in enumerate(geoms):
+        shape = Shape(geom)
+        shape.stroke_width = sw
+        sc.shapes.append(shape)
+        paint = Color(0.9 * (k == 0), 0.8 * (k == 1), 0.7 * (k == 2), 1.0)
+        sc.groups.append(ShapeGroup([k], None, paint) if sw > 0 else ShapeGroup([k], paint, None))
+    return sc
+
+
+def test_prefilter_coverage_reaches_past_tile_edges(renderer):
+    """Prefiltered image and gradients where coverage crosses tile edges that the
+    groups' point-sampled boxes stop short of."""
+    sc = _reach_scene()
+    opts = _prefilter_opts()
+    ref = orc.render(sc, opts)
+    # the oracle covers the pixels across each edge (the case is exercised)
+    for x, y in ((16, 24), (31, 40), (24, 32)):
+        assert np.max(np.abs(ref[y, x, :3] - 1.0)) > 1e-3, (x, y)
+    assert _img_err(renderer.render(sc, opts).pixels, ref) <= IMG_TOL
+    gpu, gref = _backward_case(renderer, sc, opts, BackwardOptions(compute_translation=True))
+    _grad_check(gpu, gref)

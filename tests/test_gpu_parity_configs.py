@@ -5,6 +5,7 @@
             crate's default W*H*spp PCG32 boundary samples).
 * mixed     512x512, 4x4 spp, Gaussian r=1, 256 shapes: image, and the gradients
             with W*H PCG32 boundary samples.
+* mixed, the crate's default options (prefiltered, 2x2 spp): image and gradients.
 * adjoint   128x128, 4x4 spp, 8 paths, through the fused device call with the
             fragment cache off (fragment_slots = 0: every fragment list is rebuilt
             from the BVHs, nothing stored between the passes).
@@ -80,6 +81,14 @@ def test_mixed_512_full_size(renderer):
     sc = synth.mixed_scene(0)
     _image_and_grads(renderer, sc, synth.mixed_scene(1), synth.mixed_options(),
                      BackwardOptions(boundary_samples=sc.width * sc.height))
+
+
+def test_mixed_512_crate_default_options(renderer):
+    """The crate's default RenderOptions (prefiltered coverage, 2x2 spp, jitter, seed 0) on
+    the mixed scene: the prefiltered forward (its own translation unit, the crate's root
+    formulas) and the prefiltered interior adjoint (no boundary pass in this mode)."""
+    sc = synth.mixed_scene(0)
+    _image_and_grads(renderer, sc, synth.mixed_scene(1), RenderOptions(), BackwardOptions())
 
 
 def test_adjoint_128_recompute_path(renderer):
