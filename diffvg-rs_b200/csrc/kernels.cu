@@ -758,88 +758,6 @@ __device__ float2 sample_join_cap(const DevScene& S, int path, float t, float2* 
     return p;
 }
 
-// Forward-mode derivative of a join / cap site's polygon with respect to its vertex
-// v, the control points that set the adjacent tangents (qa before, qb after the
-// vertex) and the radius: 7 partials (v.x, v.y, qa.x, qa.y, qb.x, qb.y, r).
-struct Dl {
-    float v;
-    float d[7];
-};
-__device__ __forceinline__ Dl dl_const(float v) {
-    Dl r;
-    r.v = v;
-#pragma unroll
-    for (int k = 0; k < 7; ++k) r.d[k] = 0.0f;
-    return r;
-}
-__device__ __forceinline__ Dl dl_var(float v, int k) {
-    Dl r = dl_const(v);
-    r.d[k] = 1.0f;
-    return r;
-}
-__device__ __forceinline__ Dl operator+(const Dl& a, const Dl& b) {
-    Dl r;
-    r.v = a.v + b.v;
-#pragma unroll
-    for (int k = 0; k < 7; ++k) r.d[k] = a.d[k] + b.d[k];
-    return r;
-}
-__device__ __forceinline__ Dl operator-(const Dl& a, const Dl& b) {
-    Dl r;
-    r.v = a.v - b.v;
-#pragma unroll
-    for (int k = 0; k < 7; ++k) r.d[k] = a.d[k] - b.d[k];
-    return r;
-}
-__device__ __forceinline__ Dl operator*(const Dl& a, const Dl& b) {
-    Dl r;
-    r.v = a.v * b.v;
-#pragma unroll
-    for (int k = 0; k < 7; ++k) r.d[k] = a.d[k] * b.v + a.v * b.d[k];
-    return r;
-}
-__device__ __forceinline__ Dl operator/(const Dl& a, const Dl& b) {
-    Dl r;
-    r.v = a.v / b.v;
-#pragma unroll
-    for (int k = 0; k < 7; ++k) r.d[k] = (a.d[k] - r.v * b.d[k]) / b.v;
-    return r;
-}
-__device__ __forceinline__ Dl dl_sqrt(const Dl& a) {
-    Dl r;
-    r.v = sqrtf(a.v);
-#pragma unroll
-    for (int k = 0; k < 7; ++k) r.d[k] = r.v > 0.0f ? a.d[k] * (0.5f / r.v) : 0.0f;
-    return r;
-}
-struct DV {
-    Dl x, y;
-};
-__device__ __forceinline__ DV dv_add(const DV& a, const DV& b) { return DV{a.x + b.x, a.y + b.y}; }
-__device__ __forceinline__ DV dv_sub(const DV& a, const DV& b) { return DV{a.x - b.x, a.y - b.y}; }
-__device__ __forceinline__ DV dv_scale(const DV& a, const Dl& s) { return DV{a.x * s, a.y * s}; }
-__device__ __forceinline__ DV dv_unit(const DV& a) {
-    const Dl l = dl_sqrt(a.x * a.x + a.y * a.y);
-    return DV{a.x / l, a.y / l};
-}
-// Slot of the control point that seg_dir0 / seg_dir1 take (the vertex is slot 0 / 3).
-__device__ __forceinline__ int seg_dir0_slot(float4 a, float4 b) {
-    if (!(a.z - a.x == 0.0f && a.w - a.y == 0.0f)) return 1;
-    return !(b.x - a.x == 0.0f && b.y - a.y == 0.0f) ? 2 : 3;
-}
-__device__ __forceinline__ int seg_dir1_slot(float4 a, float4 b) {
-    if (!(b.z - b.x == 0.0f && b.w - b.y == 0.0f)) return 2;
-    return !(b.z - a.z == 0.0f && b.w - a.w == 0.0f) ? 1 : 0;
-}
-__device__ __forceinline__ float2 seg_slot(float4 a, float4 b, int j) {
-    return j == 0 ? make_float2(a.x, a.y) : j == 1 ? make_float2(a.z, a.w) : j == 2 ? make_float2(b.x, b.y)
-                                                                                 : make_float2(b.z, b.w);
-}
-// Path point of slot j of a segment (lines and quadratics repeat their last point).
-__device__ __forceinline__ int seg_slot_point(int4 meta, int j, bool closed, int pc) {
-    const int idx = meta.z + (j < meta.x + 1 ? j : meta.x + 1);
-    return closed ? idx % pc : idx;
-}
 // Normal velocity of the join / cap edge point sampled at (site, edge, f):
 // w[k] = dp/dtheta_k . n for theta = (v, qa, qb, r); ids = path points of v, qa, qb
 // (-1: not used).  Out of line: it runs only for those samples.

@@ -261,6 +261,135 @@ __device__ __forceinline__ float d_smoothstep(float d, float d_ret) {  // backwa
     return d_t * 0.5f;
 }
 
+// ------------------------------------------------------------------ styled strokes (an extension)
+// The crate's prefiltered stroke coverage is round: smoothstep(|d| + sw) - smoothstep(|d| - sw)
+// (sampling.rs:240-260).  For a PF_STYLED path whose closest point is a segment end with a
+// non-round join or cap (the ends the point-sampled stroke excludes, end_excluded), the
+// coverage is smoothstep(s + 2 sw) - smoothstep(s), s the signed distance (canvas space,
+// negative inside) to the outer edges of that join or cap region; s = |d| - sw elsewhere
+// gives the crate's formula back.  The region is the point-sampled one, built in canvas
+// space from the canvas images of the vertex and of the control points that set its
+// tangents, with the stroke width as radius (the prefiltered stroke's own units): the bevel
+// edge, the two miter edges within the limit, a butt end's flat end, a square cap's three
+// outer box edges.  A reversal ends both bodies flat; a straight join (|cross| < 1e-6)
+// keeps the round formula.  sd->d: partials with respect to (v, qa, qb) in canvas space and
+// sw; ids: the path points of v, qa, qb (-1: unused); q: their shape-space positions.
+static __device__ __noinline__ bool styled_end_sd(const DevScene& S, int g, int s, int seg, float t, float2 pt, Dl* sd,
+                                                  int* ids, float2* q) {
+    const int4 si = __ldg(&S.s_info[s]);
+    if (si.x != K_PATH || si.z < 0) return false;
+    const float sw = __ldg(&S.s_stroke[s]);
+    if (!(sw > 0.0f)) return false;
+    const int path = si.z;
+    const int4 pi = __ldg(&S.p_info[2 * path]);
+    const int4 pi2 = __ldg(&S.p_info[2 * path + 1]);
+    const int pflags = pi2.w, off = pi.x, n = pi.y, pc = pi2.y;
+    if (seg < 0 || seg >= n || !end_excluded(pflags, seg, n, t)) return false;
+    const bool closed = pflags & PF_CLOSED;
+    const int join = (pflags >> PF_JOIN_SHIFT) & 3, cap = (pflags >> PF_CAP_SHIFT) & 3;
+    const float* X = S.s_xform + 9 * s;
+    const float* s2c = S.g_s2c + 9 * g;
+    ids[0] = ids[1] = ids[2] = -1;
+    const bool at1 = t == 1.0f;
+    const bool is_join = closed || (at1 ? seg + 1 < n : seg > 0);
+    const Dl R = dl_var(sw, 6);
+    DV V, e[4];
+    int ne = 1;
+    bool fan = false, rect = false;
+    if (is_join) {
+        const int vb = at1 ? (seg + 1) % n : seg, va = vb > 0 ? vb - 1 : n - 1;
+        const float4 a0 = __ldg(&S.seg_p[2 * (off + va)]), a1 = __ldg(&S.seg_p[2 * (off + va) + 1]);
+        const float4 b0 = __ldg(&S.seg_p[2 * (off + vb)]), b1 = __ldg(&S.seg_p[2 * (off + vb) + 1]);
+        const int sa = seg_dir1_slot(a0, a1), sb = seg_dir0_slot(b0, b1);
+        q[0] = make_float2(b0.x, b0.y);
+        q[1] = seg_slot(a0, a1, sa);
+        q[2] = seg_slot(b0, b1, sb);
+        const int4 ma = __ldg(&S.seg_meta[off + va]), mb = __ldg(&S.seg_meta[off + vb]);
+        ids[0] = mb.z;
+        ids[1] = seg_slot_point(ma, sa, closed, pc);
+        ids[2] = seg_slot_point(mb, sb, closed, pc);
+        const float2 vc = xf9(s2c, xf9(X, q[0])), ac = xf9(s2c, xf9(X, q[1])), bc = xf9(s2c, xf9(X, q[2]));
+        if ((vc.x == ac.x && vc.y == ac.y) || (vc.x == bc.x && vc.y == bc.y)) return false;
+        V = DV{dl_var(vc.x, 0), dl_var(vc.y, 1)};
+        const DV QA{dl_var(ac.x, 2), dl_var(ac.y, 3)}, QB{dl_var(bc.x, 4), dl_var(bc.y, 5)};
+        const DV din = dv_unit(dv_sub(V, QA)), dout = dv_unit(dv_sub(QB, V));
+        const Dl cr = din.x * dout.y - din.y * dout.x;
+        if (fabsf(cr.v) < 1.0e-6f) {
+            if (din.x.v * dout.x.v + din.y.v * dout.y.v > 0.0f) return false;  // straight on: the bodies meet
+            const DV np{dl_const(0.0f) - din.y, din.x};                        // a reversal: both end flat at v
+            e[0] = dv_sub(V, dv_scale(np, R));
+            e[1] = dv_add(V, dv_scale(np, R));
+        } else {
+            const Dl sg = dl_const(cr.v > 0.0f ? 1.0f : -1.0f);
+            e[0] = DV{V.x + R * sg * din.y, V.y - R * sg * din.x};
+            const DV b{V.x + R * sg * dout.y, V.y - R * sg * dout.x};
+            if (join == JOIN_MITER) {
+                const Dl sm = ((b.x - e[0].x) * dout.y - (b.y - e[0].y) * dout.x) / cr;
+                const DV m = dv_add(e[0], dv_scale(din, sm));
+                const float ml = sqrtf((m.x.v - vc.x) * (m.x.v - vc.x) + (m.y.v - vc.y) * (m.y.v - vc.y));
+                if (ml <= __ldg(&S.p_miter[path]) * R.v) e[ne++] = m;
+            }
+            e[ne] = b;
+            fan = true;
+        }
+    } else {
+        const bool start = !at1;
+        const int sj = start ? 0 : n - 1;
+        const float4 q0 = __ldg(&S.seg_p[2 * (off + sj)]), q1 = __ldg(&S.seg_p[2 * (off + sj) + 1]);
+        const int sq = start ? seg_dir0_slot(q0, q1) : seg_dir1_slot(q0, q1);
+        const int4 m = __ldg(&S.seg_meta[off + sj]);
+        q[0] = start ? make_float2(q0.x, q0.y) : make_float2(q1.z, q1.w);
+        q[start ? 2 : 1] = seg_slot(q0, q1, sq);
+        ids[0] = seg_slot_point(m, start ? 0 : 3, closed, pc);
+        ids[start ? 2 : 1] = seg_slot_point(m, sq, closed, pc);
+        const float2 vc = xf9(s2c, xf9(X, q[0])), qc = xf9(s2c, xf9(X, q[start ? 2 : 1]));
+        if (vc.x == qc.x && vc.y == qc.y) return false;
+        V = DV{dl_var(vc.x, 0), dl_var(vc.y, 1)};
+        const DV Q = start ? DV{dl_var(qc.x, 4), dl_var(qc.y, 5)} : DV{dl_var(qc.x, 2), dl_var(qc.y, 3)};
+        const DV d = dv_unit(dv_sub(V, Q));  // outward along the end
+        const DV np{dl_const(0.0f) - d.y, d.x};
+        e[0] = dv_sub(V, dv_scale(np, R));
+        if (cap == CAP_SQUARE) {
+            e[1] = dv_add(e[0], dv_scale(d, R));
+            e[2] = dv_add(dv_add(V, dv_scale(np, R)), dv_scale(d, R));
+            e[3] = dv_add(V, dv_scale(np, R));
+            ne = 3;
+            rect = true;
+        } else {
+            e[1] = dv_add(V, dv_scale(np, R));
+        }
+    }
+    // squared distance to the closest outer edge e[i] -> e[i + 1]
+    Dl best = dl_const(0.0f);
+    for (int i = 0; i < ne; ++i) {
+        const DV ex = dv_sub(e[i + 1], e[i]);
+        const Dl ee = ex.x * ex.x + ex.y * ex.y;
+        DV c = e[i];
+        if (ee.v > 0.0f) {
+            const Dl tt = ((dl_const(pt.x) - e[i].x) * ex.x + (dl_const(pt.y) - e[i].y) * ex.y) / ee;
+            if (tt.v >= 1.0f)
+                c = e[i + 1];
+            else if (tt.v > 0.0f)
+                c = dv_add(e[i], dv_scale(ex, tt));
+        }
+        const Dl dx = dl_const(pt.x) - c.x, dy = dl_const(pt.y) - c.y;
+        const Dl d2 = dx * dx + dy * dy;
+        if (i == 0 || d2.v < best.v) best = d2;
+    }
+    const Dl dist = dl_sqrt(best);
+    bool inside = false;
+    const float2 v0 = make_float2(V.x.v, V.y.v);
+    auto val = [](const DV& a) { return make_float2(a.x.v, a.y.v); };
+    if (fan)
+        for (int i = 0; i < ne; ++i) inside = inside || in_triangle(pt, v0, val(e[i]), val(e[i + 1]));
+    if (rect)
+        inside = in_triangle(pt, val(e[0]), val(e[1]), val(e[2])) || in_triangle(pt, val(e[0]), val(e[2]), val(e[3]));
+    *sd = inside ? dl_const(0.0f) - dist : dist;
+    return true;
+}
+// A closest point that can be an excluded segment end (the styled test's only callers).
+__device__ __forceinline__ bool maybe_styled_end(int seg, float t) { return seg >= 0 && (t == 0.0f || t == 1.0f); }
+
 // One prefiltered fragment (sampling.rs:240-300).
 struct PFragD {
     bool hit;
@@ -285,7 +414,13 @@ __device__ __forceinline__ PFragD prefilter_frag(const DevScene& S, int g, int w
         if (!have) return f;
         const float sw = __ldg(&S.s_stroke[h.shape]);
         d = h.dist;
-        w = smoothstep1(fabsf(d) + sw) - smoothstep1(fabsf(d) - sw);
+        Dl sd;
+        int ids[3];
+        float2 q[3];
+        if (maybe_styled_end(h.seg, h.t) && styled_end_sd(S, g, h.shape, h.seg, h.t, pt, &sd, ids, q))
+            w = smoothstep1(sd.v + 2.0f * sw) - smoothstep1(sd.v);
+        else
+            w = smoothstep1(fabsf(d) + sw) - smoothstep1(fabsf(d) - sw);
     } else {
         const bool inside = group_inside(S, g, xf9(S.g_c2s + 9 * g, pt), rule);
         if (!have && !inside) return f;
@@ -747,6 +882,34 @@ static __device__ void d_closest_point_rect(float4 r, float2 pt, float2 d_cp, fl
     d_max->y += dlb.y;
     *d_max = add2(*d_max, drb);
 }
+// Adjoint of styled_end_sd: d_s times its partials, through the shape and group
+// transforms, into the path points, the shape and the group transform; returns d_pt
+// (the region moves with its three points, so d/dpt = -(the sum of their partials)).
+static __device__ __noinline__ float2 d_styled_end(const DevScene& S, const GradPtrs& G, int g, int s, const Dl& sd,
+                                                   float d_s, const int* ids, const float2* q) {
+    const float* X = S.s_xform + 9 * s;
+    const float* s2c = S.g_s2c + 9 * g;
+    const int4 pi2 = __ldg(&S.p_info[2 * __ldg(&S.s_info[s].z) + 1]);
+    const int po = pi2.x, pc = pi2.y;
+    const bool closed = pi2.w & PF_CLOSED;
+    float d_s2c[9] = {0}, d_st[9] = {0};
+    float2 sum = make_float2(0.0f, 0.0f);
+    for (int j = 0; j < 3; ++j) {
+        if (ids[j] < 0) continue;
+        const float2 gc = make_float2(d_s * sd.d[2 * j], d_s * sd.d[2 * j + 1]);
+        sum = add2(sum, gc);
+        const float2 qg = xf9(X, q[j]);
+        float2 g_qg = make_float2(0.0f, 0.0f), g_q = g_qg;
+        d_xform_pt(s2c, qg, gc, d_s2c, &g_qg);
+        d_xform_pt(X, q[j], g_qg, d_st, &g_q);
+        add_point_grad(G, po, pc, closed, ids[j], g_q);
+    }
+    for (int k = 0; k < 9; ++k) {
+        add_if(G.d_group_transform + 9 * g + k, d_s2c[k]);
+        add_if(G.d_shape_transform + 9 * s + k, d_st[k]);
+    }
+    return make_float2(-sum.x, -sum.y);
+}
 // d_compute_distance (distance.rs:50-136): geometry, shape and group transform
 // gradients by atomics; returns d_pt (for the translation adjoint).
 static __device__ float2 d_compute_distance(const DevScene& S, const GradPtrs& G, int g, int s, float2 pt, float2 cp,
@@ -949,12 +1112,19 @@ __device__ __forceinline__ void interior_prefilter_body(const DevScene& S, const
             float4 dv = make_float4(0, 0, 0, 0);
             int i = cur;
             float w = 0.0f, d_w = 0.0f;
+            bool styled = false;
+            Dl sd;
+            int sids[3];
+            float2 sq[3];
             if (has) {
                 float4 c = paint_color(S, p, pt);
                 const float d = fdist[i];
                 if (which == 0) {
                     const float sw = __ldg(&S.s_stroke[fshape[i]]);
-                    w = smoothstep1(fabsf(d) + sw) - smoothstep1(fabsf(d) - sw);
+                    styled = maybe_styled_end(fseg[i], ft[i]) &&
+                             styled_end_sd(S, g, fshape[i], fseg[i], ft[i], pt, &sd, sids, sq);
+                    w = styled ? smoothstep1(sd.v + 2.0f * sw) - smoothstep1(sd.v)
+                               : smoothstep1(fabsf(d) + sw) - smoothstep1(fabsf(d) - sw);
                 } else {
                     w = smoothstep1(d);
                 }
@@ -987,7 +1157,17 @@ __device__ __forceinline__ void interior_prefilter_body(const DevScene& S, const
             const float d = fdist[i];
             float d_d;
             bool geom = true;
-            if (which == 0) {
+            if (which == 0 && styled) {
+                const float sw = __ldg(&S.s_stroke[fshape[i]]);
+                const float dp = d_smoothstep(sd.v + 2.0f * sw, d_w), dm = d_smoothstep(sd.v, d_w);
+                const float d_s = dp - dm;
+                add_if(G.d_shape_stroke_width + fshape[i], 2.0f * dp + d_s * sd.d[6]);
+                const float2 dpt = d_styled_end(S, G, g, fshape[i], sd, d_s, sids, sq);
+                tdelta.x += -dpt.x;
+                tdelta.y += -dpt.y;
+                d_d = 0.0f;
+                geom = false;
+            } else if (which == 0) {
                 const float sw = __ldg(&S.s_stroke[fshape[i]]);
                 const float ap = fabsf(d) + sw, am = fabsf(d) - sw;
                 const float dap = d_smoothstep(ap, d_w), dam = -d_smoothstep(am, d_w);

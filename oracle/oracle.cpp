@@ -2639,6 +2639,9 @@ struct PFrag {  // types.rs:118-136
     PathInfo pinfo;
     bool within, is_stroke;
 };
+static bool styled_end_value(const Group& grp, const Shape& s, size_t seg, float t, V2 pt, float* sd);
+static bool styled_end_backward(const Group& grp, size_t group_id, const Shape& s, size_t shape_id, size_t seg, float t,
+                                V2 pt, float d_s, Grads& g, float* d_sw, V2* d_pt);
 static void collect_prefiltered(const Scene& sc, const SceneBvh& bvh, V2 pt, std::vector<PFrag>& frags) {
     frags.clear();
     for (size_t gi = 0; gi < sc.groups.size(); ++gi) {
@@ -2648,7 +2651,12 @@ static void collect_prefiltered(const Scene& sc, const SceneBvh& bvh, V2 pt, std
             if (compute_distance_bvh(sc, bvh, gi, pt, INF_F, &hit)) {
                 const Shape& shp = sc.shapes[hit.shape_index];
                 float d = hit.distance;
-                float w = smoothstep(std::fabs(d) + shp.stroke_width) - smoothstep(std::fabs(d) - shp.stroke_width);
+                float sd = 0.0f, w;
+                if (hit.path.valid && (hit.path.t == 0.0f || hit.path.t == 1.0f) &&
+                    styled_end_value(g, shp, hit.path.segment_index, hit.path.t, pt, &sd))
+                    w = smoothstep(sd + 2.0f * shp.stroke_width) - smoothstep(sd);
+                else
+                    w = smoothstep(std::fabs(d) + shp.stroke_width) - smoothstep(std::fabs(d) - shp.stroke_width);
                 if (w > 0.0f) {
                     V4 c = paint_color(sc.paints[g.stroke], pt);
                     c.w *= w;
@@ -2758,8 +2766,24 @@ static V4 sample_color_prefiltered(const Scene& sc, const SceneBvh& bvh, V2 scre
                 const Shape& shp = sc.shapes[f.shape_id];
                 float d = f.distance;
                 float abs_plus = std::fabs(d) + shp.stroke_width, abs_minus = std::fabs(d) - shp.stroke_width;
-                float w = smoothstep(abs_plus) - smoothstep(abs_minus);
-                if (w != 0.0f) {
+                float sd = 0.0f;
+                const bool styled = f.pinfo.valid && (f.pinfo.t == 0.0f || f.pinfo.t == 1.0f) &&
+                                    styled_end_value(grp, shp, f.pinfo.base_point_id, f.pinfo.t, pt, &sd);
+                float w = styled ? smoothstep(sd + 2.0f * shp.stroke_width) - smoothstep(sd)
+                                 : smoothstep(abs_plus) - smoothstep(abs_minus);
+                if (w != 0.0f && styled) {
+                    float d_w = w > 0.0f ? (f.a / w) * d_alpha_i : 0.0f;
+                    float dai = d_alpha_i * w;
+                    V2 tdelta = mk(0, 0);
+                    if (grp.stroke >= 0) d_sample_paint(sc, grp.stroke, *grads, pt, V4{dci_r, dci_g, dci_b, dai}, &tdelta);
+                    float dp = d_smoothstep(sd + 2.0f * shp.stroke_width, d_w), dm = d_smoothstep(sd, d_w);
+                    float d_s = dp - dm, d_sw = 0.0f;
+                    V2 d_pt = mk(0, 0);
+                    styled_end_backward(grp, f.group_id, shp, f.shape_id, f.pinfo.base_point_id, f.pinfo.t, pt, d_s,
+                                        *grads, &d_sw, &d_pt);
+                    grads->stroke_width[f.shape_id] += 2.0f * dp + d_sw;
+                    accumulate_translation(*grads, translation_index, tdelta + d_pt * -1.0f);
+                } else if (w != 0.0f) {
                     float d_w = w > 0.0f ? (f.a / w) * d_alpha_i : 0.0f;
                     float dai = d_alpha_i * w;
                     V2 tdelta = mk(0, 0);
@@ -3192,6 +3216,164 @@ static int seg_dir1_slot(const SegData& g) {
     return !(d.x == 0.0f && d.y == 0.0f) ? 1 : 0;
 }
 static V2 seg_slot(const SegData& g, int j) { return j == 0 ? g.p0 : j == 1 ? g.p1 : j == 2 ? g.p2 : g.p3; }
+// Prefiltered stroke of a styled path (the library's extension; the crate's prefiltered
+// stroke coverage is round, smoothstep(|d| + sw) - smoothstep(|d| - sw), sampling.rs:
+// 240-260).  Where the closest point is a segment end that the point-sampled stroke
+// excludes (end_excluded), the coverage is smoothstep(s + 2 sw) - smoothstep(s), s the
+// signed distance (canvas space, negative inside) to the outer edges of that join or cap
+// region, built in canvas space from the canvas images of the vertex and of the control
+// points that set its tangents with the stroke width as radius: bevel edge; the two miter
+// edges within the limit; a butt end's flat end; a square cap's three outer box edges.
+// A reversal ends both bodies flat; a straight join (|cross| < 1e-6) keeps the round
+// formula (returns false).  sd->d: partials with respect to (v, qa, qb) in canvas space
+// and sw; ids: path points of v, qa, qb (-1: unused); q: their shape-space positions.
+static bool styled_end_sd(const Group& grp, const Shape& s, size_t seg, float t, V2 pt, Dl* sd, long ids[3],
+                          V2 q[3]) {
+    if (s.kind != DVG_SHAPE_PATH || !(s.stroke_width > 0.0f)) return false;
+    const PathG& path = s.path;
+    const std::vector<SegData> segs = path_segments(s, s.stroke_width);
+    const size_t n = segs.size();
+    if (seg >= n || !end_excluded(s, seg, n, t)) return false;
+    const bool closed = path.closed;
+    std::vector<size_t> seg_pid(n);
+    for (size_t i = 0, pid = 0; i < n; ++i) {
+        seg_pid[i] = pid;
+        pid += path.ncp[i] + 1;
+    }
+    auto canvas = [&](V2 p) { return xform_pt(grp.s2c, xform_pt(s.transform, p)); };
+    ids[0] = ids[1] = ids[2] = -1;
+    const bool at1 = t == 1.0f;
+    const bool is_join = closed || (at1 ? seg + 1 < n : seg > 0);
+    const Dl R = dl_var(s.stroke_width, 6);
+    DV V, e[4];
+    int ne = 1;
+    bool fan = false, rect = false;
+    if (is_join) {
+        const size_t vb = at1 ? (seg + 1) % n : seg, va = vb > 0 ? vb - 1 : n - 1;
+        const int sa = seg_dir1_slot(segs[va]), sb = seg_dir0_slot(segs[vb]);
+        q[0] = segs[vb].p0;
+        q[1] = seg_slot(segs[va], sa);
+        q[2] = seg_slot(segs[vb], sb);
+        ids[0] = (long)seg_pid[vb];
+        ids[1] = (long)seg_slot_point(path, seg_pid[va], path.ncp[va], sa);
+        ids[2] = (long)seg_slot_point(path, seg_pid[vb], path.ncp[vb], sb);
+        const V2 vc = canvas(q[0]), ac = canvas(q[1]), bc = canvas(q[2]);
+        if ((vc.x == ac.x && vc.y == ac.y) || (vc.x == bc.x && vc.y == bc.y)) return false;
+        V = DV{dl_var(vc.x, 0), dl_var(vc.y, 1)};
+        const DV QA{dl_var(ac.x, 2), dl_var(ac.y, 3)}, QB{dl_var(bc.x, 4), dl_var(bc.y, 5)};
+        const DV din = dv_unit(dv_sub(V, QA)), dout = dv_unit(dv_sub(QB, V));
+        const Dl cr = din.x * dout.y - din.y * dout.x;
+        if (std::fabs(cr.v) < 1.0e-6f) {
+            if (din.x.v * dout.x.v + din.y.v * dout.y.v > 0.0f) return false;
+            const DV np{dl_const(0.0f) - din.y, din.x};
+            e[0] = dv_sub(V, dv_scale(np, R));
+            e[1] = dv_add(V, dv_scale(np, R));
+        } else {
+            const Dl sg = dl_const(cr.v > 0.0f ? 1.0f : -1.0f);
+            e[0] = DV{V.x + R * sg * din.y, V.y - R * sg * din.x};
+            const DV b{V.x + R * sg * dout.y, V.y - R * sg * dout.x};
+            if (s.join == DVG_JOIN_MITER) {
+                const Dl sm = ((b.x - e[0].x) * dout.y - (b.y - e[0].y) * dout.x) / cr;
+                const DV m = dv_add(e[0], dv_scale(din, sm));
+                const float ml = std::sqrt((m.x.v - vc.x) * (m.x.v - vc.x) + (m.y.v - vc.y) * (m.y.v - vc.y));
+                if (ml <= std::fmax(s.miter, 1.0f) * R.v) e[ne++] = m;
+            }
+            e[ne] = b;
+            fan = true;
+        }
+    } else {
+        const bool start = !at1;
+        const size_t sj = start ? 0 : n - 1;
+        const SegData& g = segs[sj];
+        const int sq = start ? seg_dir0_slot(g) : seg_dir1_slot(g);
+        q[0] = start ? g.p0 : g.p3;
+        q[start ? 2 : 1] = seg_slot(g, sq);
+        ids[0] = (long)seg_slot_point(path, seg_pid[sj], path.ncp[sj], start ? 0 : 3);
+        ids[start ? 2 : 1] = (long)seg_slot_point(path, seg_pid[sj], path.ncp[sj], sq);
+        const V2 vc = canvas(q[0]), qc = canvas(q[start ? 2 : 1]);
+        if (vc.x == qc.x && vc.y == qc.y) return false;
+        V = DV{dl_var(vc.x, 0), dl_var(vc.y, 1)};
+        const DV Q = start ? DV{dl_var(qc.x, 4), dl_var(qc.y, 5)} : DV{dl_var(qc.x, 2), dl_var(qc.y, 3)};
+        const DV d = dv_unit(dv_sub(V, Q));
+        const DV np{dl_const(0.0f) - d.y, d.x};
+        e[0] = dv_sub(V, dv_scale(np, R));
+        if (s.cap == DVG_CAP_SQUARE) {
+            e[1] = dv_add(e[0], dv_scale(d, R));
+            e[2] = dv_add(dv_add(V, dv_scale(np, R)), dv_scale(d, R));
+            e[3] = dv_add(V, dv_scale(np, R));
+            ne = 3;
+            rect = true;
+        } else {
+            e[1] = dv_add(V, dv_scale(np, R));
+        }
+    }
+    Dl best = dl_const(0.0f);
+    for (int i = 0; i < ne; ++i) {
+        const DV ex = dv_sub(e[i + 1], e[i]);
+        const Dl ee = ex.x * ex.x + ex.y * ex.y;
+        DV c = e[i];
+        if (ee.v > 0.0f) {
+            const Dl tt = ((dl_const(pt.x) - e[i].x) * ex.x + (dl_const(pt.y) - e[i].y) * ex.y) / ee;
+            if (tt.v >= 1.0f)
+                c = e[i + 1];
+            else if (tt.v > 0.0f)
+                c = dv_add(e[i], dv_scale(ex, tt));
+        }
+        const Dl dx = dl_const(pt.x) - c.x, dy = dl_const(pt.y) - c.y;
+        const Dl d2 = dx * dx + dy * dy;
+        if (i == 0 || d2.v < best.v) best = d2;
+    }
+    const Dl dist = dl_sqrt(best);
+    auto val = [](const DV& a) { return mk(a.x.v, a.y.v); };
+    bool inside = false;
+    if (fan)
+        for (int i = 0; i < ne; ++i) inside = inside || in_triangle(pt, val(V), val(e[i]), val(e[i + 1]));
+    if (rect) inside = in_triangle(pt, val(e[0]), val(e[1]), val(e[2])) || in_triangle(pt, val(e[0]), val(e[2]), val(e[3]));
+    *sd = inside ? dl_const(0.0f) - dist : dist;
+    return true;
+}
+static bool styled_end_value(const Group& grp, const Shape& s, size_t seg, float t, V2 pt, float* sd) {
+    Dl d;
+    long ids[3];
+    V2 q[3];
+    if (!styled_end_sd(grp, s, seg, t, pt, &d, ids, q)) return false;
+    *sd = d.v;
+    return true;
+}
+// Adjoint of styled_end_sd: d_s times its partials through the shape and group
+// transforms into the path points and both transforms; returns d_pt (the region moves
+// with its three points, so d/dpt = -(the sum of their partials)).
+static V2 d_styled_end(const Group& grp, size_t group_id, const Shape& s, size_t shape_id, const Dl& sd, float d_s,
+                       const long ids[3], const V2 q[3], Grads& g) {
+    M3 d_s2c = zero3(), d_st = zero3();
+    V2 sum = mk(0, 0);
+    for (int j = 0; j < 3; ++j) {
+        if (ids[j] < 0) continue;
+        const V2 gc = mk(d_s * sd.d[2 * j], d_s * sd.d[2 * j + 1]);
+        sum = sum + gc;
+        const V2 qg = xform_pt(s.transform, q[j]);
+        V2 g_qg = mk(0, 0), g_q = mk(0, 0);
+        d_xform_pt(grp.s2c, qg, gc, &d_s2c, &g_qg);
+        d_xform_pt(s.transform, q[j], g_qg, &d_st, &g_q);
+        g.points[2 * (s.path.point_base + (size_t)ids[j])] += g_q.x;
+        g.points[2 * (s.path.point_base + (size_t)ids[j]) + 1] += g_q.y;
+    }
+    add_group_transform(g, group_id, d_s2c);
+    add_shape_transform(g, shape_id, d_st);
+    return sum * -1.0f;
+}
+// The styled prefiltered stroke's adjoint for d_s = dL/ds: geometry and transforms into
+// g, the stroke-width part of ds/dsw * d_s into *d_sw, dL/dpt into *d_pt.
+static bool styled_end_backward(const Group& grp, size_t group_id, const Shape& s, size_t shape_id, size_t seg, float t,
+                                V2 pt, float d_s, Grads& g, float* d_sw, V2* d_pt) {
+    Dl sd;
+    long ids[3];
+    V2 q[3];
+    if (!styled_end_sd(grp, s, seg, t, pt, &sd, ids, q)) return false;
+    *d_sw = d_s * sd.d[6];
+    *d_pt = d_styled_end(grp, group_id, s, shape_id, sd, d_s, ids, q, g);
+    return true;
+}
 // Normal velocity of the edge point sampled at (site, edge, f): w[k] = dp/dtheta_k . n
 // for theta = (v, qa, qb, r); ids = path points of v, qa, qb (-1: not used).
 static bool join_cap_velocity(const Shape& s, size_t site, size_t edge, float f, V2 n, float w[7], long ids[3]) {

@@ -80,3 +80,33 @@ def test_styled_fused_step_uses_the_same_fragments(renderer):
         scale = float(np.max(np.abs(v))) if v.size else 0.0
         assert float(np.max(np.abs(outs[1][1][k] - v))) <= 1e-4 * (scale + 1e-6) + 1e-6, k
     up.close()
+
+
+# ---------------------------------------------------------------- prefiltered coverage
+def _pf_opts():
+    return RenderOptions(samples_x=2, samples_y=2, seed=0, jitter=False, use_prefiltering=True)
+
+
+@pytest.mark.parametrize("seed", SEEDS[:2])
+def test_styled_prefiltered_matches_oracle(renderer, seed):
+    """Prefiltered coverage at excluded join / cap ends (the signed distance to the region's
+    outer edges): image and every gradient array against the oracle."""
+    sc = synth.styled_stroke_scene(seed)
+    opts = _pf_opts()
+    img = renderer.render(sc, opts).pixels
+    ref = orc.render(sc, opts)
+    assert float(np.max(np.abs(img - ref))) <= 1e-5
+    for s in sc.shapes:  # the styled coverage is in use
+        s.stroke_join, s.stroke_cap = StrokeJoin.ROUND, StrokeCap.ROUND
+    assert float(np.max(np.abs(orc.render(sc, opts) - ref))) > 1e-2
+    sc = synth.styled_stroke_scene(seed)
+    d_render = np.random.default_rng(seed).standard_normal((sc.height, sc.width, 4)).astype(np.float32)
+    bo = BackwardOptions(compute_translation=True)
+    g = renderer.render_backward(sc, opts, bo, d_render)
+    _, rb = orc.render_backward(sc, opts, bo, d_render)
+    for name in rb.NAMES:
+        a, b = g.buffers[name], rb[name]
+        if a is None or b is None or not b.size:
+            continue
+        scale = float(np.max(np.abs(b)))
+        assert float(np.max(np.abs(a - b))) <= 1e-4 * (scale + 1e-6) + 1e-6, name
