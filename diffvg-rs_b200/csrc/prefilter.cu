@@ -387,8 +387,13 @@ static __device__ __noinline__ bool styled_end_sd(const DevScene& S, int g, int 
     *sd = inside ? dl_const(0.0f) - dist : dist;
     return true;
 }
-// A closest point that can be an excluded segment end (the styled test's only callers).
-__device__ __forceinline__ bool maybe_styled_end(int seg, float t) { return seg >= 0 && (t == 0.0f || t == 1.0f); }
+// A closest point at a segment end of a PF_STYLED path: the only case styled_end_sd can
+// change, tested inline so that other strokes make no call.
+__device__ __forceinline__ bool maybe_styled_end(const DevScene& S, int s, int seg, float t) {
+    if (seg < 0 || !(t == 0.0f || t == 1.0f)) return false;
+    const int path = __ldg(&S.s_info[s].z);
+    return path >= 0 && (__ldg(&S.p_info[2 * path + 1].w) & PF_STYLED);
+}
 
 // One prefiltered fragment (sampling.rs:240-300).
 struct PFragD {
@@ -417,7 +422,7 @@ __device__ __forceinline__ PFragD prefilter_frag(const DevScene& S, int g, int w
         Dl sd;
         int ids[3];
         float2 q[3];
-        if (maybe_styled_end(h.seg, h.t) && styled_end_sd(S, g, h.shape, h.seg, h.t, pt, &sd, ids, q))
+        if (maybe_styled_end(S, h.shape, h.seg, h.t) && styled_end_sd(S, g, h.shape, h.seg, h.t, pt, &sd, ids, q))
             w = smoothstep1(sd.v + 2.0f * sw) - smoothstep1(sd.v);
         else
             w = smoothstep1(fabsf(d) + sw) - smoothstep1(fabsf(d) - sw);
@@ -1121,7 +1126,7 @@ __device__ __forceinline__ void interior_prefilter_body(const DevScene& S, const
                 const float d = fdist[i];
                 if (which == 0) {
                     const float sw = __ldg(&S.s_stroke[fshape[i]]);
-                    styled = maybe_styled_end(fseg[i], ft[i]) &&
+                    styled = maybe_styled_end(S, fshape[i], fseg[i], ft[i]) &&
                              styled_end_sd(S, g, fshape[i], fseg[i], ft[i], pt, &sd, sids, sq);
                     w = styled ? smoothstep1(sd.v + 2.0f * sw) - smoothstep1(sd.v)
                                : smoothstep1(fabsf(d) + sw) - smoothstep1(fabsf(d) - sw);
