@@ -72,6 +72,17 @@ def test_joins_known_answers(join, expect):
         assert _alpha(sc, x, y) == pytest.approx(w, abs=2e-6), (join, x, y)
 
 
+def test_reversal_ends_flat_and_straight_join_stays_round():
+    # a reversal at V = (24, 16.5) (out and straight back): both bodies end flat at V
+    sc = Scene(40, 32)
+    _stroke(sc, [(8.0, 16.5), (24.0, 16.5), (10.0, 16.5)], False, J.MITER, C_.ROUND, 2.0)
+    assert _alpha(sc, 24, 16) == pytest.approx(_w(0.5, 2.0), abs=2e-6)
+    # a straight join at V = (16.5, 16.5): the bodies meet, the round formula holds
+    sc = Scene(40, 32)
+    _stroke(sc, [(8.0, 16.5), (16.5, 16.5), (24.0, 16.5)], False, J.BEVEL, C_.ROUND, 2.5)
+    assert _alpha(sc, 16, 19) == pytest.approx(_smooth(3.0 + 2.5) - _smooth(3.0 - 2.5), abs=2e-6)
+
+
 def test_miter_limit_falls_back_to_bevel():
     # a right angle has miter ratio sqrt(2): limit 1.2 bevels
     sc = Scene(32, 32)
